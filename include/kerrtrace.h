@@ -1,0 +1,178 @@
+/*
+ * kerrtrace.h -- C ABI of the B200-native geodesic renderer.
+ *
+ * This is the drop-in boundary for the reference renderer's backend dispatch
+ * (render_image, main.cpp:2209-2478).  The reference routes one frame either
+ * to its CPU two-phase path (trace_geodesics main.cpp:2014-2206, then
+ * colorize_buffer main.cpp:1817-1866) or to `cuda_render`
+ * (gpu/cuda/tracer.cuh:23-26).  The entry points below replace both with
+ * plain C: pointers, sizes and status codes, no C++ types, no exceptions.
+ *
+ *   kt_frame_desc   <- FrameParams (main.cpp:1885-1893) + IntegratorControls
+ *                      (main.cpp:193-197) + trace_geodesics' arguments
+ *                      (main.cpp:2014-2027): chart, integrator, bundles,
+ *                      solver mode, pixel offsets, M, Q, Lambda.
+ *   kt_frame_derive <- the per-frame host work of trace_geodesics
+ *                      (main.cpp:2033-2082): chart fallback rules, r_horizon,
+ *                      r_isco, disk bounds, escape radius, camera angles.
+ *   kt_trace        <- trace_geodesics' per-pixel loop (main.cpp:2098-2183):
+ *                      fills a per-pixel SoA (GeoPixel main.cpp:84-94, in
+ *                      float64 instead of float32).
+ *   kt_colorize     <- colorize_buffer (main.cpp:1817-1866) with the
+ *                      blackbody palette (disk_colour main.cpp:1799-1814) and
+ *                      the equirectangular background (main.cpp:153-170).
+ *   kt_render_host  <- render_image's CPU branch (main.cpp:2468-2476):
+ *                      trace + colorize, host buffers in and out.
+ *   kt_kgeo_write / kt_kgeo_read <- save_kgeo / load_kgeo (main.cpp:96-137).
+ *
+ * Threading: a kt_context belongs to one host thread at a time.  Device
+ * pointers passed to the asynchronous calls belong to the caller; the
+ * context owns its scratch (queue counters) only.  Every call returns a
+ * kt_status; kt_last_error() gives the message of the last failure.
+ */
+#ifndef KERRTRACE_H
+#define KERRTRACE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KT_ABI_VERSION 1
+
+typedef enum kt_status {
+  KT_OK = 0,
+  KT_ERR_INVALID_ARGUMENT = 1, /* bad sizes, NaN parameters, NULL pointers */
+  KT_ERR_UNSUPPORTED = 2,      /* a mode this backend does not run */
+  KT_ERR_CUDA = 3,             /* a CUDA runtime call failed */
+  KT_ERR_OUT_OF_MEMORY = 4,
+  KT_ERR_NO_DEVICE = 5,
+  KT_ERR_IO = 6,               /* .kgeo read/write failure */
+  KT_ERR_INTERNAL = 7
+} kt_status;
+
+/* Coordinate chart (CoordinateChart, main.cpp:175). */
+enum { KT_CHART_KS = 0, KT_CHART_BL = 1 };
+/* Integrator (Integrator, geodesic.hpp:417). */
+enum { KT_RK4_DOUBLING = 0, KT_DOPRI5 = 1 };
+/* Ray solver (RaySolverMode, main.cpp:176); only STANDARD runs here. */
+enum { KT_SOLVER_STANDARD = 0, KT_SOLVER_SEMI_ANALYTIC = 1, KT_SOLVER_ELLIPTIC_CLOSED = 2 };
+/* Arithmetic of the trace. */
+enum { KT_PREC_FP64 = 0, KT_PREC_MIXED = 1 };
+/* Per-pixel outcome codes (GeoPixel::outcome, main.cpp:85). */
+enum { KT_OUT_ESCAPED = 0, KT_OUT_DISK = 1, KT_OUT_HORIZON = 2 };
+/* Per-pixel status (extension: why a ray stopped). */
+enum {
+  KT_RAY_EVENT = 0,      /* stopped at a disk / horizon / escape event */
+  KT_RAY_STEP_CAP = 1,   /* max_steps accepted steps without an event */
+  KT_RAY_REJECT_CAP = 2, /* more than 64 consecutive rejected attempts */
+  KT_RAY_NONFINITE = 3   /* step size became non-finite */
+};
+
+typedef struct kt_frame_desc {
+  /* metric (M_bh, fp.a, Q_bh, Lam) */
+  double M, a, Q, Lambda;
+  /* camera and disk (FrameParams; angles in degrees as on the CLI) */
+  double theta_deg, phi_deg, r_obs, disk_out, fov_deg;
+  int32_t width, height;
+  double pixel_offset_x, pixel_offset_y;
+  /* integrator (requested; kt_frame_derive applies the fallback rules) */
+  int32_t chart, integrator, bundles, solver_mode;
+  int32_t max_steps, precision;
+  double step_init, tol;
+  uint32_t flags; /* reserved, must be 0 */
+  int32_t reserved0;
+} kt_frame_desc;
+
+typedef struct kt_frame_derived {
+  int32_t chart;      /* effective chart: KS+Lambda!=0 -> BL, bundles -> BL */
+  int32_t integrator; /* effective integrator: the KS chart always uses RK4 */
+  double r_horizon, rh_cut, r_isco, r_disk_in, r_disk_out, r_escape;
+  double r_obs, theta_obs, phi_obs, fov_h; /* radians */
+  double dlam0;       /* max(step_init, 1e-10) */
+  int32_t max_steps;  /* max(1, max_steps) */
+  int32_t reserved0;
+  double tol;
+  double bundle_eps;  /* fov_h / width * 0.5 (ray_bundle.hpp:282) */
+} kt_frame_derived;
+
+/* Per-pixel results, struct of arrays, width*height entries, row-major
+ * (index = py*width + px).  Slot meaning is the reference's GeoPixel. */
+typedef struct kt_geo_soa {
+  uint8_t* outcome;
+  double* r;
+  double* redshift;
+  double* magnif;
+  double* phi_disk;
+  double* theta_esc;
+  double* phi_esc;
+  uint8_t* status;    /* optional (NULL): KT_RAY_* */
+  uint32_t* steps;    /* optional (NULL): accepted steps */
+  uint32_t* attempts; /* optional (NULL): adaptive attempts (accepted+rejected) */
+} kt_geo_soa;
+
+/* ColorParams (main.cpp:72-81), blackbody palette. */
+typedef struct kt_color_params {
+  double exposure, gamma, temp_scale;
+  int32_t palette; /* 0 = blackbody; 1 = interstellar (not implemented) */
+  int32_t reserved0;
+} kt_color_params;
+
+typedef struct kt_context kt_context;
+
+int kt_abi_version(void);
+const char* kt_status_string(kt_status s);
+
+kt_status kt_create(kt_context** ctx, int device);
+void kt_destroy(kt_context* ctx);
+const char* kt_last_error(const kt_context* ctx);
+
+/* Host-side frame preparation; needs no GPU. */
+kt_status kt_frame_derive(const kt_frame_desc* desc, kt_frame_derived* out);
+void kt_frame_desc_defaults(kt_frame_desc* desc);
+void kt_color_params_defaults(kt_color_params* cp);
+
+/* Trace one frame into caller-owned device buffers, asynchronously on
+ * `stream` (a cudaStream_t, NULL = legacy default stream). */
+kt_status kt_trace(kt_context* ctx, const kt_frame_desc* desc,
+                   const kt_geo_soa* out, void* stream);
+
+/* Trace only the pixels listed in pix[0..n) (index py*width+px) into
+ * compact device outputs out[i] (used for sampling and tile sharding). */
+kt_status kt_trace_pixels(kt_context* ctx, const kt_frame_desc* desc,
+                          const uint32_t* pix_dev, int64_t n,
+                          const kt_geo_soa* out, void* stream);
+
+/* Same as kt_trace but with host buffers: copies in and out inside the
+ * call and returns after the results are on the host. */
+kt_status kt_trace_host(kt_context* ctx, const kt_frame_desc* desc,
+                        const kt_geo_soa* out_host);
+
+/* Phase 2 on the device: SoA -> RGB8 (width*height*3 bytes).  bg_rgb is a
+ * device RGB8 equirectangular image (bg_w*bg_h*3) or NULL for black. */
+kt_status kt_colorize(kt_context* ctx, const kt_frame_desc* desc,
+                      const kt_geo_soa* geo, const kt_color_params* cp,
+                      const uint8_t* bg_rgb, int32_t bg_w, int32_t bg_h,
+                      uint8_t* rgb_out, void* stream);
+
+/* render_image equivalent: trace + colorize, host buffers in and out. */
+kt_status kt_render_host(kt_context* ctx, const kt_frame_desc* desc,
+                         const kt_color_params* cp, const uint8_t* bg_rgb_host,
+                         int32_t bg_w, int32_t bg_h, uint8_t* rgb_out_host);
+
+/* .kgeo two-phase cache (main.cpp:96-137): 4-byte magic, u32 version, the
+ * 88-byte KGeoMeta, then width*height 28-byte float32 GeoPixel records. */
+kt_status kt_kgeo_write(const char* path, const kt_frame_desc* desc,
+                        const kt_geo_soa* geo_host);
+kt_status kt_kgeo_read_header(const char* path, int32_t* width, int32_t* height,
+                              double meta[10]);
+kt_status kt_kgeo_read(const char* path, const kt_geo_soa* geo_host,
+                       int64_t capacity);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KERRTRACE_H */

@@ -1,0 +1,174 @@
+"""ctypes bindings of the oracle libraries (test infrastructure).
+
+  port   : oracle/_build/liboracle_port.so  -- the C restatement (kt_oracle.c)
+  strict : oracle/_ref/libktref_strict.so   -- the reference compiled with the
+                                               renderer's libm, no contraction
+  stock  : oracle/_ref/libktref_stock.so    -- the reference as shipped (-O3
+                                               -ffast-math, glibc libm)
+  ieee   : oracle/_ref/libktref_ieee.so     -- the reference at -O3 without
+                                               -ffast-math, glibc libm
+
+Only tests, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from kerrtracecpp2_b200.abi import FrameDerived, FrameDesc
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PORT_PATH = os.path.join(ROOT, "oracle", "_build", "liboracle_port.so")
+REF_PATHS = {
+    "strict": os.path.join(ROOT, "oracle", "_ref", "libktref_strict.so"),
+    "stock": os.path.join(ROOT, "oracle", "_ref", "libktref_stock.so"),
+    "ieee": os.path.join(ROOT, "oracle", "_ref", "libktref_ieee.so"),
+}
+
+_P = ctypes.c_void_p
+_D = ctypes.c_double
+_cache = {}
+
+
+def _ptr(a):
+    return a.ctypes.data_as(_P) if a is not None else None
+
+
+def port():
+    if "port" not in _cache:
+        if not os.path.exists(PORT_PATH):
+            raise FileNotFoundError(f"{PORT_PATH} missing: run python oracle/build.py")
+        L = ctypes.CDLL(PORT_PATH)
+        L.orc_trace_pixels.argtypes = [ctypes.POINTER(FrameDesc), ctypes.c_int64, _P] + [_P] * 9 + [ctypes.c_int]
+        L.orc_trace_pixels.restype = None
+        L.orc_frame_derive.argtypes = [ctypes.POINTER(FrameDesc), ctypes.POINTER(FrameDerived)]
+        L.orc_colorize.argtypes = [ctypes.POINTER(FrameDesc), ctypes.c_int64] + [_P] * 6 + [_D] * 3 + [_P, ctypes.c_int, ctypes.c_int, _P]
+        L.orc_colorize.restype = None
+        for f in ("orc_r_horizon", "orc_r_isco"):
+            getattr(L, f).argtypes = [_D] * 4
+            getattr(L, f).restype = _D
+        _cache["port"] = L
+    return _cache["port"]
+
+
+def ref_available(flavour="strict"):
+    return os.path.exists(REF_PATHS[flavour])
+
+
+def ref(flavour="strict"):
+    key = "ref_" + flavour
+    if key not in _cache:
+        path = REF_PATHS[flavour]
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} missing: run python oracle/build.py (needs the reference tree)")
+        L = ctypes.CDLL(path)
+        L.ref_trace_pixels.argtypes = [ctypes.POINTER(FrameDesc), ctypes.c_int64, _P] + [_P] * 7 + [ctypes.c_int]
+        L.ref_trace_pixels.restype = None
+        L.ref_trace_geodesics.argtypes = [ctypes.POINTER(FrameDesc), _P, ctypes.c_int]
+        L.ref_colorize.argtypes = [_P, ctypes.c_int, ctypes.c_int, _D, _D, _D, _P, ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, _P]
+        L.ref_colorize.restype = None
+        for f in ("ref_r_horizon", "ref_r_isco"):
+            getattr(L, f).argtypes = [_D] * 4
+            getattr(L, f).restype = _D
+        L.ref_libm_probe_cos.argtypes = [_D]
+        L.ref_libm_probe_cos.restype = _D
+        L.ref_contravariant_BL.argtypes = [_D] * 6 + [_P]
+        L.ref_covariant_BL.argtypes = [_D] * 6 + [_P]
+        L.ref_angle_ray.argtypes = [_D] * 8 + [ctypes.c_int, ctypes.c_int, _D, _D, _P]
+        L.ref_hamiltonian.argtypes = [_D] * 4 + [_P]
+        L.ref_hamiltonian.restype = _D
+        L.ref_adaptive_step.argtypes = [_D] * 4 + [_P, _P, ctypes.c_int, _P, _D]
+        L.ref_adaptive_step.restype = ctypes.c_int
+        L.ref_keplerian_omega.argtypes = [_D] * 5
+        L.ref_keplerian_omega.restype = _D
+        L.ref_bl_to_ks.argtypes = [_D] * 4 + [_P]
+        L.ref_ks_to_bl.argtypes = [_D] * 4 + [_P]
+        L.ref_r_ks.argtypes = [_D] * 4
+        L.ref_r_ks.restype = _D
+        _cache[key] = L
+    return _cache[key]
+
+
+def all_pixels(desc):
+    return np.arange(desc.width * desc.height, dtype=np.uint32)
+
+
+def _alloc(n):
+    return {
+        "outcome": np.zeros(n, np.uint8), "r": np.zeros(n), "redshift": np.zeros(n),
+        "magnif": np.zeros(n), "phi_disk": np.zeros(n), "theta_esc": np.zeros(n),
+        "phi_esc": np.zeros(n),
+    }
+
+
+def trace_port(desc, pix=None, nthreads=0, counters=False):
+    pix = all_pixels(desc) if pix is None else np.ascontiguousarray(pix, np.uint32)
+    n = len(pix)
+    out = _alloc(n)
+    steps = np.zeros(n, np.uint32) if counters else None
+    att = np.zeros(n, np.uint32) if counters else None
+    port().orc_trace_pixels(ctypes.byref(desc), n, _ptr(pix), *[_ptr(out[k]) for k in
+                            ("outcome", "r", "redshift", "magnif", "phi_disk", "theta_esc", "phi_esc")],
+                            _ptr(steps), _ptr(att), nthreads)
+    if counters:
+        out["steps"], out["attempts"] = steps, att
+    return out
+
+
+def trace_ref(desc, flavour="strict", pix=None, nthreads=0):
+    pix = all_pixels(desc) if pix is None else np.ascontiguousarray(pix, np.uint32)
+    n = len(pix)
+    out = _alloc(n)
+    ref(flavour).ref_trace_pixels(ctypes.byref(desc), n, _ptr(pix), *[_ptr(out[k]) for k in
+                                  ("outcome", "r", "redshift", "magnif", "phi_disk", "theta_esc", "phi_esc")],
+                                  nthreads)
+    return out
+
+
+GEOPIXEL_DTYPE = np.dtype([("outcome", "u1"), ("pad", "u1", 3), ("r", "<f4"), ("redshift", "<f4"),
+                           ("magnif", "<f4"), ("phi_disk", "<f4"), ("theta_esc", "<f4"),
+                           ("phi_esc", "<f4")])
+
+
+def trace_geodesics_ref(desc, flavour="strict", nthreads=0):
+    """The reference's own frame loop: GeoPixel records (float32)."""
+    out = np.zeros(desc.width * desc.height, GEOPIXEL_DTYPE)
+    ref(flavour).ref_trace_geodesics(ctypes.byref(desc), _ptr(out), nthreads)
+    return out
+
+
+def colorize_port(desc, geo, bg=None, exposure=1.0, gamma=2.2, temp_scale=1.0):
+    n = len(geo["outcome"])
+    rgb = np.zeros((n, 3), np.uint8)
+    bw, bh = (bg.shape[1], bg.shape[0]) if bg is not None else (0, 0)
+    bgc = np.ascontiguousarray(bg) if bg is not None else None
+    port().orc_colorize(ctypes.byref(desc), n, *[_ptr(np.ascontiguousarray(geo[k])) for k in
+                        ("outcome", "r", "redshift", "magnif", "theta_esc", "phi_esc")],
+                        exposure, gamma, temp_scale, _ptr(bgc), bw, bh, _ptr(rgb))
+    return rgb
+
+
+def colorize_ref(desc, geopixels, r_isco, bg=None, exposure=1.0, gamma=2.2, temp_scale=1.0,
+                 flavour="strict"):
+    n = desc.width * desc.height
+    rgb = np.zeros((n, 3), np.uint8)
+    bw, bh = (bg.shape[1], bg.shape[0]) if bg is not None else (0, 0)
+    bgc = np.ascontiguousarray(bg) if bg is not None else None
+    ref(flavour).ref_colorize(_ptr(geopixels), desc.width, desc.height, exposure, gamma, temp_scale,
+                              _ptr(bgc), bw, bh, desc.M, r_isco, r_isco, desc.disk_out, _ptr(rgb))
+    return rgb
+
+
+def to_geopixels(geo):
+    """float64 SoA -> GeoPixel records, as trace_geodesics stores them."""
+    n = len(geo["outcome"])
+    g = np.zeros(n, GEOPIXEL_DTYPE)
+    for k in ("outcome", "r", "redshift", "magnif", "phi_disk", "theta_esc", "phi_esc"):
+        g[k] = geo[k]
+    return g
+
+
+def derive_port(desc):
+    d = FrameDerived()
+    port().orc_frame_derive(ctypes.byref(desc), ctypes.byref(d))
+    return d
