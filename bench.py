@@ -1,0 +1,335 @@
+#!/usr/bin/env python
+"""Headline benchmark: primary rays traced per second (Mrays/s) at 1280x720.
+
+Workload (default): Kerr-Newman-de Sitter, BL chart, a=0.9, Q=0.3,
+Lambda=1e-4, r_obs=60, theta=85 deg, fov=30 deg, disk ISCO..20, DOPRI5 at
+tol 1e-10, plain FP64 (bit-identical to the reference CPU path).  A step is
+one full 1280x720 frame traced by kt_trace into device-resident SoA
+buffers.  Inputs are frame parameters only; between steps a 256 MB buffer
+is written to flush L2 (the 55 MB of outputs would otherwise stay cached).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N>1 runs under torchrun, one process per GPU: every rank traces its own
+720p frame (an orbit of the camera, phi = 360*rank/N deg), no data-path
+collective, scaling "weak"; time = max over ranks.  `--impl reference`
+times the reference renderer's own CPU path (compiled from its sources,
+oracle/_ref) on the host cores for the same metric.
+"""
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mrays/s 720p: plain FP64 vs mixed-precision at stated error; adjoint ms/frame"
+
+WORKLOADS = {
+    "knds_bl_dopri5_720p": dict(chart=1, integrator=1, tol=1e-10, a=0.9, Q=0.3, Lambda=1e-4,
+                                r_obs=60.0, theta_deg=85.0, phi_deg=0.0, fov_deg=30.0,
+                                disk_out=20.0, width=1280, height=720),
+    "kerr_ks_rk4_320x180": dict(chart=0, a=0.5, r_obs=40.0, theta_deg=80.0, phi_deg=0.0,
+                                fov_deg=45.0, disk_out=12.0, width=320, height=180),
+    "bundles_bl_1080p": dict(chart=1, bundles=1, a=0.998, theta_deg=60.0, width=1920, height=1080),
+    "kn_ks_rk4_512": dict(chart=0, a=0.7, Q=0.1, theta_deg=70.0, r_obs=50.0, disk_out=15.0,
+                          width=512, height=512),
+}
+
+# Algorithmic FP64 operations (+, -, *, / and sqrt = 1, fma = 2), counted
+# from the reference's arithmetic as kt_physics.cuh evaluates it:
+#   BL RHS (geodesic_rhs + dphi_vel): 3 sincos (70 each incl. reduction),
+#   5 g^{mu nu} evaluations (34 full, 26 at the centre, 24 when only theta
+#   changes), 4 Hamiltonians (16), FD differences -> 453.
+#   DOPRI5 attempt: 6 RHS + stage sums (189) + y5/y4 (117) + error norm (26)
+#   + controller with pow (115) -> 6 RHS + 447.
+#   RK4 doubling attempt: 10 RHS + stage inputs/sums (207) + error (13)
+#   + controller (115) -> 10 RHS + 335; one more RHS per accepted step.
+FLOPS_BL_RHS = 453.0
+FLOPS_DOPRI5_ATTEMPT = 447.0
+FLOPS_RK4_ATTEMPT = 335.0
+
+
+def env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def start_clock_sampler(path):
+    cmd = ["nvidia-smi",
+           "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+           "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+           "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+           "--format=csv,noheader,nounits", "-lms", "200"]
+    try:
+        f = open(path, "w")
+        return subprocess.Popen(cmd, stdout=f, stderr=subprocess.DEVNULL), f
+    except (OSError, FileNotFoundError):
+        return None, None
+
+
+def stop_clock_sampler(proc, f, path, gpu_index):
+    if proc is None:
+        return None
+    proc.terminate()
+    try:
+        proc.wait(timeout=5)
+    except subprocess.TimeoutExpired:
+        proc.kill()
+    f.close()
+    sm, mx, reasons = [], [], set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for line in open(path):
+        parts = [p.strip() for p in line.split(",")]
+        if len(parts) < 9 or parts[0] != str(gpu_index):
+            continue
+        try:
+            sm.append(float(parts[1]))
+            mx.append(float(parts[2]))
+        except ValueError:
+            continue
+        for n, v in zip(names, parts[5:9]):
+            if v.lower() == "active":
+                reasons.add(n)
+    if not sm:
+        return None
+    return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "samples": len(sm),
+            "reasons": sorted(reasons)}
+
+
+def ray_flops(desc, steps, attempts):
+    """Algorithmic FP64 flops of one traced frame from the kernel's counters."""
+    if desc.bundles or desc.chart == 0 and abs(desc.Lambda) <= 1e-15:
+        return None  # counted only for the BL single-ray integrators
+    n = desc.width * desc.height
+    if desc.integrator == 1:
+        rhs = n + 6.0 * attempts
+        return rhs * FLOPS_BL_RHS + attempts * FLOPS_DOPRI5_ATTEMPT
+    rhs = n + 10.0 * attempts + steps
+    return rhs * FLOPS_BL_RHS + attempts * FLOPS_RK4_ATTEMPT
+
+
+def cpu_reference_sample(desc, seconds, flavour="ieee"):
+    """Time the reference's CPU path on a strided sample of the frame.
+
+    Returns (rays_per_s, n_pixels, threads, kind, sample, results)."""
+    import oracle_lib as O  # noqa: E402  (tests/oracle_lib.py)
+
+    n = desc.width * desc.height
+    threads = os.cpu_count() or 1
+    use_ref = O.ref_available(flavour)
+    kind = "reference" if use_ref else "port"
+
+    def trace(pix):
+        if use_ref:
+            return O.trace_ref(desc, flavour, pix=pix, nthreads=threads)
+        return O.trace_port(desc, pix=pix, nthreads=threads)
+
+    # calibrate on ~0.2% of the frame, then size the sample to `seconds`
+    stride = max(1, n // max(512, threads * 16))
+    pix = np.arange(0, n, stride, dtype=np.uint32)
+    t0 = time.perf_counter()
+    trace(pix)
+    rate = len(pix) / max(time.perf_counter() - t0, 1e-6)
+    want = int(min(n, max(len(pix), rate * seconds)))
+    stride = max(1, n // want)
+    pix = np.arange(0, n, stride, dtype=np.uint32)
+    t0 = time.perf_counter()
+    res = trace(pix)
+    dt = time.perf_counter() - t0
+    sample = f"{len(pix)} of {n} pixels (every {stride}th, row-major) of the same frame"
+    return len(pix) / dt, pix, threads, kind, sample, res
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="knds_bl_dopri5_720p", choices=sorted(WORKLOADS))
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+    rank = env_int("RANK", 0)
+    world = env_int("WORLD_SIZE", 1)
+    local_rank = env_int("LOCAL_RANK", 0)
+    from kerrtracecpp2_b200 import abi
+
+    wl = dict(WORKLOADS[args.workload])
+    base_cfg = {"workload": args.workload, "width": wl["width"], "height": wl["height"],
+                "chart": "BL" if wl.get("chart", 0) == 1 else "KS",
+                "integrator": "DOPRI5" if wl.get("integrator", 0) == 1 else "RK4-doubling",
+                "tol": wl.get("tol", 1e-7), "a": wl.get("a"), "Q": wl.get("Q", 0.0),
+                "Lambda": wl.get("Lambda", 0.0), "bundles": bool(wl.get("bundles", 0)),
+                "parallelism": f"frames{args.gpus}", "l2": "256 MB flush between steps"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        desc = abi.frame_desc(**wl)
+        per_step = max(2.0, 120.0 / max(1, args.steps + args.warmup))
+        for _ in range(args.warmup):
+            cpu_reference_sample(desc, per_step)
+        rates = []
+        info = None
+        for _ in range(args.steps):
+            rate, pix, threads, kind, sample, _ = cpu_reference_sample(desc, per_step)
+            rates.append(rate)
+            info = (threads, kind, sample)
+        v = float(np.mean(rates)) / 1e6
+        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "Mrays/s",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1e3 * wl["width"] * wl["height"] / (v * 1e6),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (procedural camera frame; no dataset)", "config": base_cfg,
+                "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": info[0], "kind": info[1],
+                                 "sample": info[2] + ("; reference built -O3 without -ffast-math, "
+                                                      "glibc libm" if info[1] == "reference" else "")},
+                "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return 0
+
+    import torch
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist  # noqa: F811
+        from datetime import timedelta
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    device = torch.device("cuda", local_rank)
+    torch.cuda.set_device(device)
+    import kerrtracecpp2_b200 as kt
+
+    R = kt.Renderer(local_rank)
+    if world > 1:
+        wl["phi_deg"] = 360.0 * rank / world
+    desc = abi.frame_desc(**wl)
+    n = desc.width * desc.height
+    out = R.alloc(n, counters=True)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=device)
+    stream = torch.cuda.current_stream(device)
+
+    def step():
+        flush.fill_(1)
+        R.trace(desc, out, stream)
+
+    for _ in range(max(args.warmup, 1)):
+        step()
+    torch.cuda.synchronize(device)
+
+    clk_path = os.path.join(tempfile.gettempdir(), f"kt_clocks_{os.getpid()}.csv")
+    proc, fh = start_clock_sampler(clk_path)
+    time.sleep(0.3)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(device)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * args.steps + 2)]
+    ev[0].record(stream)
+    for i in range(args.steps):
+        flush.fill_(1)
+        ev[2 + 2 * i].record(stream)
+        R.trace(desc, out, stream)
+        ev[3 + 2 * i].record(stream)
+    ev[1].record(stream)
+    torch.cuda.synchronize(device)
+    if dist:
+        dist.barrier()
+    clocks = stop_clock_sampler(proc, fh, clk_path, local_rank)
+    total_ms = ev[0].elapsed_time(ev[1])
+    kern_ms = [ev[2 + 2 * i].elapsed_time(ev[3 + 2 * i]) for i in range(args.steps)]
+    t = torch.tensor([total_ms, float(np.mean(kern_ms))], dtype=torch.float64, device=device)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms, kernel_ms = float(t[0]), float(t[1])
+    value = world * args.steps * n / (total_ms * 1e-3) / 1e6
+
+    steps_sum = float(out["steps"].to(torch.int64).sum())
+    att_sum = float(out["attempts"].to(torch.int64).sum())
+    flops = ray_flops(desc, steps_sum, att_sum)
+    peak_gflops = R.fp64_peak_gflops()
+    roofline = None
+    if flops is not None:
+        achieved = flops / (kernel_ms * 1e-3) / 1e12
+        peak = peak_gflops / 1e3
+        roofline = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                    "frac": achieved / peak, "traffic": None,
+                    "peak_source": "measured in this run: kt_measure_fp64_peak (dependent FMA chains, all SMs)",
+                    "flops_per_frame": flops, "rhs_per_ray": (n + 6.0 * att_sum) / n
+                    if desc.integrator == 1 else (n + 10.0 * att_sum + steps_sum) / n,
+                    "kernel_ms": kernel_ms}
+
+    # end to end through the public host-buffer call (kt_trace_host): the
+    # frame parameters go in, the per-pixel results come back to pinned host
+    # memory inside the timed region.
+    host = {k: torch.empty(n, dtype={"u1": torch.uint8, "f8": torch.float64}[dt],
+                           pin_memory=True).numpy()
+            for k, dt in abi.GEO_FIELDS if dt in ("u1", "f8") and k != "status"}
+    soa = abi.GeoSoA()
+    for k, _ in abi.GEO_FIELDS:
+        setattr(soa, k, host[k].ctypes.data_as(ctypes.c_void_p) if k in host else None)
+    L = kt.load_library()
+    for _ in range(1):
+        L.kt_trace_host(R.ctx, ctypes.byref(desc), ctypes.byref(soa))
+    e2e_ms = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize(device)
+        t0 = time.perf_counter()
+        st = L.kt_trace_host(R.ctx, ctypes.byref(desc), ctypes.byref(soa))
+        e2e_ms.append(1e3 * (time.perf_counter() - t0))
+        if st != 0:
+            raise RuntimeError(L.kt_last_error(R.ctx).decode())
+    et = torch.tensor([sum(e2e_ms)], dtype=torch.float64, device=device)
+    if dist:
+        dist.all_reduce(et, op=dist.ReduceOp.MAX)
+    e2e_value = world * args.steps * n / (float(et[0]) * 1e-3) / 1e6
+    d2h = sum(host[k].nbytes for k in host)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, pix, threads, kind, sample, res = cpu_reference_sample(desc, args.cpu_seconds)
+        got_out = out["outcome"].cpu().numpy()[pix]
+        got_g = out["redshift"].cpu().numpy()[pix]
+        disk = (got_out == 1) & (res["outcome"] == 1)
+        rel = np.abs(got_g[disk] - res["redshift"][disk]) / np.maximum(np.abs(res["redshift"][disk]), 1e-300)
+        cpu = {"value": rate / 1e6, "unit": "Mrays/s", "cores": threads, "kind": kind,
+               "sample": sample + ("; reference built -O3 without -ffast-math, glibc libm"
+                                   if kind == "reference" else ""),
+               "class_mismatch_vs_gpu": int(np.sum(got_out != res["outcome"])),
+               "g_rel_diff_vs_gpu_median": float(np.median(rel)) if rel.size else None}
+
+    line = {"metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (procedural camera frame; no dataset)", "config": base_cfg,
+            "mode": "plain FP64, bit-identical to the reference CPU path",
+            "roofline": roofline, "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": ctypes.sizeof(desc),
+                    "d2h_bytes_per_step": d2h, "call": "kt_trace_host"},
+            "clocks": clocks, "gpu_launches": args.steps * (2 if desc.chart == 0 and not desc.bundles
+                                                            and abs(desc.Lambda) <= 1e-15 else 1)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    R.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

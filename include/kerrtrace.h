@@ -61,6 +61,10 @@ enum { KT_RK4_DOUBLING = 0, KT_DOPRI5 = 1 };
 enum { KT_SOLVER_STANDARD = 0, KT_SOLVER_SEMI_ANALYTIC = 1, KT_SOLVER_ELLIPTIC_CLOSED = 2 };
 /* Arithmetic of the trace. */
 enum { KT_PREC_FP64 = 0, KT_PREC_MIXED = 1 };
+/* kt_frame_desc.flags: theta_deg, phi_deg and fov_deg hold radians (the
+ * reference's CameraParams_CUDA carries radians, gpu/cuda/tracer.cuh:16-20). */
+#define KT_FLAG_ANGLES_RADIANS 1u
+
 /* Per-pixel outcome codes (GeoPixel::outcome, main.cpp:85). */
 enum { KT_OUT_ESCAPED = 0, KT_OUT_DISK = 1, KT_OUT_HORIZON = 2 };
 /* Per-pixel status (extension: why a ray stopped). */
@@ -82,7 +86,7 @@ typedef struct kt_frame_desc {
   int32_t chart, integrator, bundles, solver_mode;
   int32_t max_steps, precision;
   double step_init, tol;
-  uint32_t flags; /* reserved, must be 0 */
+  uint32_t flags; /* KT_FLAG_* bits, 0 by default */
   int32_t reserved0;
 } kt_frame_desc;
 
@@ -124,6 +128,9 @@ typedef struct kt_context kt_context;
 
 int kt_abi_version(void);
 const char* kt_status_string(kt_status s);
+/* sizeof of kt_frame_desc, kt_frame_derived, kt_geo_soa, kt_color_params
+ * (lets bindings check their struct layout); returns the count written. */
+int kt_abi_struct_sizes(size_t* sizes, int n);
 
 kt_status kt_create(kt_context** ctx, int device);
 void kt_destroy(kt_context* ctx);
@@ -161,6 +168,15 @@ kt_status kt_colorize(kt_context* ctx, const kt_frame_desc* desc,
 kt_status kt_render_host(kt_context* ctx, const kt_frame_desc* desc,
                          const kt_color_params* cp, const uint8_t* bg_rgb_host,
                          int32_t bg_w, int32_t bg_h, uint8_t* rgb_out_host);
+
+/* Measured FP64 FMA throughput of the context's device (GFLOP/s, 2 flops
+ * per FMA): the non-tensor FP64 peak the trace kernels are bounded by. */
+kt_status kt_measure_fp64_peak(kt_context* ctx, double* gflops);
+
+/* Deterministic procedural equirectangular star field (RGB8, w*h*3 bytes),
+ * the stand-in for the reference's background photographs, which are not in
+ * its tree.  Same seed, same image, on any host. */
+kt_status kt_starfield(uint64_t seed, int32_t w, int32_t h, uint8_t* rgb);
 
 /* .kgeo two-phase cache (main.cpp:96-137): 4-byte magic, u32 version, the
  * 88-byte KGeoMeta, then width*height 28-byte float32 GeoPixel records. */

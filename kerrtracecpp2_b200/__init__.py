@@ -1,0 +1,312 @@
+"""kerrtracecpp2_b200 -- B200-native per-pixel null-geodesic renderer.
+
+Python host side over the C ABI of libkerrtrace.so (include/kerrtrace.h).
+The functions mirror the reference renderer's frame interface:
+
+  trace_geodesics(W, H, fp, use_bundles, chart, intg, ctl, ...)  main.cpp:2014
+  colorize_buffer(geo, W, H, cp, bg, ...)                          main.cpp:1817
+  render_image(W, H, fp, bg, use_bundles, chart, intg, ctl, ...)   main.cpp:2209
+
+with the same argument meaning (FrameParams in degrees, IntegratorControls,
+pixel offsets, M, Q, Lambda).  Tracing runs on the GPU only: loading the
+package without the built library, or tracing without a CUDA device, raises.
+"""
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import abi
+from .abi import (ColorParams, FrameDerived, FrameDesc, GeoSoA, color_params, frame_desc,
+                  KT_CHART_BL, KT_CHART_KS, KT_DOPRI5, KT_RK4_DOUBLING, KT_OK)
+
+__all__ = ["FrameParams", "IntegratorControls", "Renderer", "load_library", "trace_geodesics",
+           "colorize_buffer", "render_image", "frame_derive", "starfield", "KerrTraceError",
+           "frame_desc", "color_params", "FrameDesc", "ColorParams"]
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libkerrtrace.so")
+_lib = None
+
+
+class KerrTraceError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"{message} (status {status})")
+        self.status = status
+
+
+def load_library():
+    """Load the in-tree libkerrtrace.so; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with python kerrtracecpp2_b200/build.py")
+    L = ctypes.CDLL(LIB_PATH)
+    P, D, I32 = ctypes.c_void_p, ctypes.c_double, ctypes.c_int32
+    PD = ctypes.POINTER(FrameDesc)
+    L.kt_abi_version.restype = ctypes.c_int
+    L.kt_status_string.restype = ctypes.c_char_p
+    L.kt_status_string.argtypes = [ctypes.c_int]
+    L.kt_abi_struct_sizes.argtypes = [ctypes.POINTER(ctypes.c_size_t), ctypes.c_int]
+    L.kt_abi_struct_sizes.restype = ctypes.c_int
+    L.kt_create.argtypes = [ctypes.POINTER(P), ctypes.c_int]
+    L.kt_create.restype = ctypes.c_int
+    L.kt_destroy.argtypes = [P]
+    L.kt_destroy.restype = None
+    L.kt_last_error.argtypes = [P]
+    L.kt_last_error.restype = ctypes.c_char_p
+    L.kt_frame_derive.argtypes = [PD, ctypes.POINTER(FrameDerived)]
+    L.kt_frame_derive.restype = ctypes.c_int
+    L.kt_frame_desc_defaults.argtypes = [PD]
+    L.kt_frame_desc_defaults.restype = None
+    L.kt_color_params_defaults.argtypes = [ctypes.POINTER(ColorParams)]
+    L.kt_color_params_defaults.restype = None
+    L.kt_trace.argtypes = [P, PD, ctypes.POINTER(GeoSoA), P]
+    L.kt_trace.restype = ctypes.c_int
+    L.kt_trace_pixels.argtypes = [P, PD, P, ctypes.c_int64, ctypes.POINTER(GeoSoA), P]
+    L.kt_trace_pixels.restype = ctypes.c_int
+    L.kt_trace_host.argtypes = [P, PD, ctypes.POINTER(GeoSoA)]
+    L.kt_trace_host.restype = ctypes.c_int
+    L.kt_colorize.argtypes = [P, PD, ctypes.POINTER(GeoSoA), ctypes.POINTER(ColorParams), P, I32,
+                              I32, P, P]
+    L.kt_colorize.restype = ctypes.c_int
+    L.kt_render_host.argtypes = [P, PD, ctypes.POINTER(ColorParams), P, I32, I32, P]
+    L.kt_render_host.restype = ctypes.c_int
+    L.kt_measure_fp64_peak.argtypes = [P, ctypes.POINTER(D)]
+    L.kt_measure_fp64_peak.restype = ctypes.c_int
+    L.kt_starfield.argtypes = [ctypes.c_uint64, I32, I32, P]
+    L.kt_starfield.restype = ctypes.c_int
+    L.kt_kgeo_write.argtypes = [ctypes.c_char_p, PD, ctypes.POINTER(GeoSoA)]
+    L.kt_kgeo_write.restype = ctypes.c_int
+    L.kt_kgeo_read_header.argtypes = [ctypes.c_char_p, ctypes.POINTER(I32), ctypes.POINTER(I32),
+                                      ctypes.POINTER(D)]
+    L.kt_kgeo_read_header.restype = ctypes.c_int
+    L.kt_kgeo_read.argtypes = [ctypes.c_char_p, ctypes.POINTER(GeoSoA), ctypes.c_int64]
+    L.kt_kgeo_read.restype = ctypes.c_int
+    if L.kt_abi_version() != abi.KT_ABI_VERSION:
+        raise ImportError("libkerrtrace.so ABI version mismatch")
+    _lib = L
+    return L
+
+
+def _check(status, what, ctx=None):
+    if status != KT_OK:
+        L = load_library()
+        msg = L.kt_last_error(ctx).decode() if ctx else L.kt_status_string(status).decode()
+        raise KerrTraceError(status, f"{what}: {msg}")
+
+
+@dataclass
+class FrameParams:
+    """FrameParams (main.cpp:1885-1893); angles in degrees."""
+
+    a: float = 0.998
+    theta: float = 80.0
+    phi: float = 0.0
+    r_obs: float = 40.0
+    disk_out: float = 12.0
+    fov: float = 30.0
+
+
+@dataclass
+class IntegratorControls:
+    """IntegratorControls (main.cpp:193-197)."""
+
+    max_steps: int = 500000
+    step_init: float = 1.0
+    tol: float = 1e-7
+
+
+def make_desc(W, H, fp, use_bundles=False, chart=KT_CHART_KS, intg=KT_RK4_DOUBLING, ctl=None,
+              pixel_offset_x=0.0, pixel_offset_y=0.0, M=1.0, Q=0.0, Lam=0.0):
+    ctl = ctl or IntegratorControls()
+    return frame_desc(M=M, a=fp.a, Q=Q, Lambda=Lam, theta_deg=fp.theta, phi_deg=fp.phi,
+                      r_obs=fp.r_obs, disk_out=fp.disk_out, fov_deg=fp.fov, width=W, height=H,
+                      pixel_offset_x=pixel_offset_x, pixel_offset_y=pixel_offset_y, chart=chart,
+                      integrator=intg, bundles=int(bool(use_bundles)), max_steps=ctl.max_steps,
+                      step_init=ctl.step_init, tol=ctl.tol)
+
+
+def frame_derive(desc):
+    """kt_frame_derive: per-frame constants (r_+, ISCO, chart fallback...)."""
+    L = load_library()
+    out = FrameDerived()
+    _check(L.kt_frame_derive(ctypes.byref(desc), ctypes.byref(out)), "kt_frame_derive")
+    return out
+
+
+def starfield(seed=0, w=2048, h=1024):
+    """Deterministic procedural equirectangular star field, (h, w, 3) uint8."""
+    L = load_library()
+    img = np.zeros((h, w, 3), np.uint8)
+    _check(L.kt_starfield(seed, w, h, img.ctypes.data_as(ctypes.c_void_p)), "kt_starfield")
+    return img
+
+
+def _np_soa(n, counters=True):
+    out = {k: np.zeros(n, dt) for k, dt in abi.GEO_FIELDS}
+    if not counters:
+        for k in ("status", "steps", "attempts"):
+            out[k] = None
+    return out
+
+
+def _soa_struct(arrays, ptr):
+    s = GeoSoA()
+    for k, _ in abi.GEO_FIELDS:
+        a = arrays.get(k)
+        setattr(s, k, ptr(a) if a is not None else None)
+    return s
+
+
+def _np_ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _torch_ptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class Renderer:
+    """One kt_context on one CUDA device."""
+
+    def __init__(self, device=0):
+        self.L = load_library()
+        self.ctx = ctypes.c_void_p()
+        _check(self.L.kt_create(ctypes.byref(self.ctx), device), "kt_create")
+        self.device = device
+
+    def close(self):
+        if self.ctx:
+            self.L.kt_destroy(self.ctx)
+            self.ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- device-buffer entry points (torch tensors as device memory) --------
+    def alloc(self, n, counters=True):
+        import torch
+
+        dev = torch.device("cuda", self.device)
+        tdt = {"u1": torch.uint8, "f8": torch.float64, "u4": torch.int32}
+        out = {k: torch.empty(n, dtype=tdt[dt], device=dev) for k, dt in abi.GEO_FIELDS}
+        if not counters:
+            for k in ("status", "steps", "attempts"):
+                out[k] = None
+        return out
+
+    def trace(self, desc, out=None, stream=None):
+        """kt_trace into torch device tensors (allocated if out is None)."""
+        n = desc.width * desc.height
+        out = out if out is not None else self.alloc(n)
+        st = self._stream(stream)
+        _check(self.L.kt_trace(self.ctx, ctypes.byref(desc), ctypes.byref(_soa_struct(out, _torch_ptr)),
+                               st), "kt_trace", self.ctx)
+        return out
+
+    def trace_pixels(self, desc, pix, out=None, stream=None):
+        n = int(pix.numel())
+        out = out if out is not None else self.alloc(n)
+        _check(self.L.kt_trace_pixels(self.ctx, ctypes.byref(desc), _torch_ptr(pix), n,
+                                      ctypes.byref(_soa_struct(out, _torch_ptr)), self._stream(stream)),
+               "kt_trace_pixels", self.ctx)
+        return out
+
+    def colorize(self, desc, geo, cp=None, bg=None, rgb=None, stream=None):
+        import torch
+
+        cp = cp or color_params()
+        n = desc.width * desc.height
+        if rgb is None:
+            rgb = torch.empty(n * 3, dtype=torch.uint8, device=torch.device("cuda", self.device))
+        bw, bh = (bg.shape[1], bg.shape[0]) if bg is not None else (0, 0)
+        _check(self.L.kt_colorize(self.ctx, ctypes.byref(desc), ctypes.byref(_soa_struct(geo, _torch_ptr)),
+                                  ctypes.byref(cp), _torch_ptr(bg) if bg is not None else None, bw, bh,
+                                  _torch_ptr(rgb), self._stream(stream)), "kt_colorize", self.ctx)
+        return rgb
+
+    @staticmethod
+    def _stream(stream):
+        if stream is None:
+            try:
+                import torch
+
+                return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+            except Exception:
+                return None
+        return ctypes.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
+
+    def fp64_peak_gflops(self):
+        """Measured FP64 FMA throughput of this device (GFLOP/s)."""
+        v = ctypes.c_double()
+        _check(self.L.kt_measure_fp64_peak(self.ctx, ctypes.byref(v)), "kt_measure_fp64_peak", self.ctx)
+        return v.value
+
+    # -- host-buffer entry points --------------------------------------------
+    def trace_host(self, desc, counters=True):
+        out = _np_soa(desc.width * desc.height, counters)
+        _check(self.L.kt_trace_host(self.ctx, ctypes.byref(desc), ctypes.byref(_soa_struct(out, _np_ptr))),
+               "kt_trace_host", self.ctx)
+        return out
+
+    def render_host(self, desc, cp=None, bg=None):
+        cp = cp or color_params()
+        rgb = np.zeros((desc.height, desc.width, 3), np.uint8)
+        bgc = np.ascontiguousarray(bg) if bg is not None else None
+        bw, bh = (bg.shape[1], bg.shape[0]) if bg is not None else (0, 0)
+        _check(self.L.kt_render_host(self.ctx, ctypes.byref(desc), ctypes.byref(cp),
+                                     _np_ptr(bgc) if bgc is not None else None, bw, bh, _np_ptr(rgb)),
+               "kt_render_host", self.ctx)
+        return rgb
+
+
+_default = {}
+
+
+def _renderer(device=0):
+    if device not in _default:
+        _default[device] = Renderer(device)
+    return _default[device]
+
+
+def trace_geodesics(W, H, fp, use_bundles=False, chart=KT_CHART_KS, intg=KT_RK4_DOUBLING, ctl=None,
+                    pixel_offset_x=0.0, pixel_offset_y=0.0, M_bh=1.0, Q_bh=0.0, Lam=0.0, device=0):
+    """Phase 1 (main.cpp:2014): per-pixel results as float64 numpy arrays."""
+    desc = make_desc(W, H, fp, use_bundles, chart, intg, ctl, pixel_offset_x, pixel_offset_y, M_bh,
+                     Q_bh, Lam)
+    return _renderer(device).trace_host(desc)
+
+
+def render_image(W, H, fp, bg=None, use_bundles=False, chart=KT_CHART_KS, intg=KT_RK4_DOUBLING,
+                 ctl=None, M_bh=1.0, Q_bh=0.0, Lam=0.0, cp=None, pixel_offset_x=0.0,
+                 pixel_offset_y=0.0, device=0):
+    """render_image (main.cpp:2209): trace + colorize; (H, W, 3) uint8."""
+    desc = make_desc(W, H, fp, use_bundles, chart, intg, ctl, pixel_offset_x, pixel_offset_y, M_bh,
+                     Q_bh, Lam)
+    return _renderer(device).render_host(desc, cp, bg)
+
+
+def colorize_buffer(geo, desc, cp=None, bg=None, device=0):
+    """colorize_buffer (main.cpp:1817) of host results from trace_geodesics."""
+    import torch
+
+    r = _renderer(device)
+    dev = torch.device("cuda", device)
+    g = {k: (torch.from_numpy(np.ascontiguousarray(v)).to(dev) if v is not None else None)
+         for k, v in geo.items()}
+    bgt = torch.from_numpy(np.ascontiguousarray(bg)).to(dev) if bg is not None else None
+    rgb = r.colorize(desc, g, cp, bgt)
+    torch.cuda.synchronize(dev)
+    return rgb.cpu().numpy().reshape(desc.height, desc.width, 3)

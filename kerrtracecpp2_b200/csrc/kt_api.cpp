@@ -1,0 +1,428 @@
+// kt_api.cpp -- the C ABI (include/kerrtrace.h) over the CUDA kernels.
+//
+// No exceptions cross the boundary: every entry point returns a kt_status
+// and records a message readable with kt_last_error().  There is no CPU
+// tracing path: without a CUDA device the trace calls fail with
+// KT_ERR_NO_DEVICE.
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <new>
+#include <string>
+
+#include "../../include/kerrtrace.h"
+#include "kt_frame.h"
+#include "kt_internal.h"
+
+struct kt_context {
+  int device = 0;
+  std::string err;
+  uint32_t* d_counters = nullptr;  // [0] ray queue, [1] fallback queue, [2] fallback count
+  uint32_t* d_fb = nullptr;        // fallback list: pix[cap] then slot[cap]
+  size_t fb_cap = 0;
+  // device staging for the host-buffer entry points
+  unsigned char* d_stage = nullptr;
+  size_t stage_cap = 0;
+  unsigned char* d_bg = nullptr;
+  size_t bg_cap = 0;
+  cudaStream_t stream = nullptr;
+  kt::LaunchShape shapes[kt::kNumModes];
+  bool shape_ok[kt::kNumModes] = {false, false, false, false};
+};
+
+namespace {
+
+// Makes the context's device current for the duration of a call.
+struct DeviceGuard {
+  int prev = -1;
+  bool ok = false;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    ok = cudaSetDevice(dev) == cudaSuccess;
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+kt_status fail(kt_context* ctx, kt_status st, const std::string& msg) {
+  if (ctx) ctx->err = msg;
+  return st;
+}
+
+kt_status cuda_fail(kt_context* ctx, cudaError_t e, const char* what) {
+  kt_status st = KT_ERR_CUDA;
+  if (e == cudaErrorMemoryAllocation) st = KT_ERR_OUT_OF_MEMORY;
+  if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) st = KT_ERR_NO_DEVICE;
+  return fail(ctx, st, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define KT_CUDA(ctx, call, what)                   \
+  do {                                             \
+    cudaError_t _e = (call);                       \
+    if (_e != cudaSuccess) return cuda_fail(ctx, _e, what); \
+  } while (0)
+
+kt_status ensure(kt_context* ctx, void** buf, size_t* cap, size_t need, const char* what) {
+  if (*cap >= need && *buf) return KT_OK;
+  if (*buf) cudaFree(*buf);
+  *buf = nullptr;
+  *cap = 0;
+  cudaError_t e = cudaMalloc(buf, need);
+  if (e != cudaSuccess) {
+    *buf = nullptr;
+    return cuda_fail(ctx, e, what);
+  }
+  *cap = need;
+  return KT_OK;
+}
+
+kt::Mode mode_of(const kt::Frame& f) {
+  if (f.bundles) return kt::kModeBundle;
+  if (f.chart == KT_CHART_KS) return kt::kModeKSRk4;
+  return f.intg == KT_DOPRI5 ? kt::kModeBLDopri5 : kt::kModeBLRk4;
+}
+
+kt_status shape(kt_context* ctx, kt::Mode m, kt::LaunchShape* s) {
+  if (!ctx->shape_ok[m]) {
+    KT_CUDA(ctx, kt::launch_shape(m, ctx->device, &ctx->shapes[m]), "occupancy query");
+    ctx->shape_ok[m] = true;
+  }
+  *s = ctx->shapes[m];
+  return KT_OK;
+}
+
+kt::OutSoA to_out(const kt_geo_soa* o) {
+  kt::OutSoA s;
+  s.outcome = o->outcome;
+  s.r = o->r;
+  s.red = o->redshift;
+  s.magnif = o->magnif;
+  s.phi_disk = o->phi_disk;
+  s.th_esc = o->theta_esc;
+  s.ph_esc = o->phi_esc;
+  s.status = o->status;
+  s.steps = o->steps;
+  s.attempts = o->attempts;
+  return s;
+}
+
+bool out_complete(const kt_geo_soa* o) {
+  return o && o->outcome && o->r && o->redshift && o->magnif && o->phi_disk && o->theta_esc &&
+         o->phi_esc;
+}
+
+// Launch the trace of rl (and, in the KS chart, the BL pass over the rays
+// whose KS initialisation failed, main.cpp:1537-1538).
+kt_status run_trace(kt_context* ctx, const kt::Frame& f, const kt::OutSoA& out,
+                    const kt::RayList& rl, uint64_t n_max, cudaStream_t st) {
+  const kt::Mode m = mode_of(f);
+  kt::LaunchShape s;
+  kt_status r = shape(ctx, m, &s);
+  if (r != KT_OK) return r;
+  KT_CUDA(ctx, cudaMemsetAsync(ctx->d_counters, 0, 4 * sizeof(uint32_t), st), "reset queue");
+  kt::Fallback fb = {nullptr, nullptr, ctx->d_counters + 2};
+  if (m == kt::kModeKSRk4) {
+    r = ensure(ctx, (void**)&ctx->d_fb, &ctx->fb_cap, 2 * n_max * sizeof(uint32_t), "fallback list");
+    if (r != KT_OK) return r;
+    fb.pix = ctx->d_fb;
+    fb.slot = ctx->d_fb + n_max;
+  }
+  KT_CUDA(ctx, kt::launch_trace(m, f, out, rl, ctx->d_counters, fb, s, st), "trace kernel launch");
+  if (m == kt::kModeKSRk4) {
+    const kt::Mode bm = f.intg == KT_DOPRI5 ? kt::kModeBLDopri5 : kt::kModeBLRk4;
+    kt::LaunchShape bs;
+    r = shape(ctx, bm, &bs);
+    if (r != KT_OK) return r;
+    kt::RayList fl = {fb.pix, fb.slot, fb.count, 0};
+    KT_CUDA(ctx, kt::launch_trace(bm, f, out, fl, ctx->d_counters + 1, fb, bs, st),
+            "fallback kernel launch");
+  }
+  return KT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int kt_abi_version(void) { return KT_ABI_VERSION; }
+
+const char* kt_status_string(kt_status s) {
+  switch (s) {
+    case KT_OK: return "ok";
+    case KT_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case KT_ERR_UNSUPPORTED: return "unsupported";
+    case KT_ERR_CUDA: return "CUDA error";
+    case KT_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case KT_ERR_NO_DEVICE: return "no CUDA device";
+    case KT_ERR_IO: return "I/O error";
+    case KT_ERR_INTERNAL: return "internal error";
+  }
+  return "unknown status";
+}
+
+int kt_abi_struct_sizes(size_t* sizes, int n) {
+  const size_t v[4] = {sizeof(kt_frame_desc), sizeof(kt_frame_derived), sizeof(kt_geo_soa),
+                       sizeof(kt_color_params)};
+  int k = 0;
+  for (; k < n && k < 4; ++k) sizes[k] = v[k];
+  return k;
+}
+
+void kt_frame_desc_defaults(kt_frame_desc* d) {
+  if (!d) return;
+  memset(d, 0, sizeof *d);
+  // main.cpp:2505-2517 and 2709-2716
+  d->M = 1.0;
+  d->a = 0.998;
+  d->theta_deg = 80.0;
+  d->r_obs = 40.0;
+  d->disk_out = 12.0;
+  d->fov_deg = 30.0;
+  d->width = 1920;
+  d->height = 1080;
+  d->chart = KT_CHART_KS;
+  d->integrator = KT_RK4_DOUBLING;
+  d->max_steps = 500000;
+  d->step_init = 1.0;
+  d->tol = 1e-7;
+}
+
+void kt_color_params_defaults(kt_color_params* cp) {
+  if (!cp) return;
+  memset(cp, 0, sizeof *cp);
+  cp->exposure = 1.0;
+  cp->gamma = 2.2;
+  cp->temp_scale = 1.0;
+}
+
+kt_status kt_frame_derive(const kt_frame_desc* desc, kt_frame_derived* out) {
+  if (!out) return KT_ERR_INVALID_ARGUMENT;
+  kt::Frame f;
+  std::string err;
+  return kt::prepare_frame(desc, &f, out, &err);
+}
+
+kt_status kt_create(kt_context** pctx, int device) {
+  if (!pctx) return KT_ERR_INVALID_ARGUMENT;
+  *pctx = nullptr;
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) return KT_ERR_NO_DEVICE;
+  if (device < 0 || device >= count) return KT_ERR_INVALID_ARGUMENT;
+  kt_context* ctx = new (std::nothrow) kt_context();
+  if (!ctx) return KT_ERR_OUT_OF_MEMORY;
+  ctx->device = device;
+  DeviceGuard g(device);
+  if (!g.ok) {
+    delete ctx;
+    return KT_ERR_NO_DEVICE;
+  }
+  int major = 0;
+  cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device);
+  if (major != 10) {
+    delete ctx;
+    return KT_ERR_UNSUPPORTED;  // kernels are built for sm_100a only
+  }
+  if (cudaMalloc((void**)&ctx->d_counters, 4 * sizeof(uint32_t)) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    kt_destroy(ctx);
+    return KT_ERR_OUT_OF_MEMORY;
+  }
+  *pctx = ctx;
+  return KT_OK;
+}
+
+void kt_destroy(kt_context* ctx) {
+  if (!ctx) return;
+  DeviceGuard g(ctx->device);
+  if (ctx->stream) {
+    cudaStreamSynchronize(ctx->stream);
+    cudaStreamDestroy(ctx->stream);
+  }
+  cudaFree(ctx->d_counters);
+  cudaFree(ctx->d_fb);
+  cudaFree(ctx->d_stage);
+  cudaFree(ctx->d_bg);
+  delete ctx;
+}
+
+const char* kt_last_error(const kt_context* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+kt_status kt_trace(kt_context* ctx, const kt_frame_desc* desc, const kt_geo_soa* out,
+                   void* stream) {
+  if (!ctx) return KT_ERR_INVALID_ARGUMENT;
+  if (!out_complete(out)) return fail(ctx, KT_ERR_INVALID_ARGUMENT, "kt_trace: output pointer is NULL");
+  kt::Frame f;
+  kt_status r = kt::prepare_frame(desc, &f, nullptr, &ctx->err);
+  if (r != KT_OK) return r;
+  DeviceGuard g(ctx->device);
+  const uint64_t n = (uint64_t)desc->width * (uint64_t)desc->height;
+  kt::RayList rl = {nullptr, nullptr, nullptr, (uint32_t)n};
+  return run_trace(ctx, f, to_out(out), rl, n, (cudaStream_t)stream);
+}
+
+kt_status kt_trace_pixels(kt_context* ctx, const kt_frame_desc* desc, const uint32_t* pix_dev,
+                          int64_t n, const kt_geo_soa* out, void* stream) {
+  if (!ctx) return KT_ERR_INVALID_ARGUMENT;
+  if (n < 0 || n > 0x7fffffff) return fail(ctx, KT_ERR_INVALID_ARGUMENT, "kt_trace_pixels: bad n");
+  if (n > 0 && (!pix_dev || !out_complete(out)))
+    return fail(ctx, KT_ERR_INVALID_ARGUMENT, "kt_trace_pixels: NULL pointer");
+  kt::Frame f;
+  kt_status r = kt::prepare_frame(desc, &f, nullptr, &ctx->err);
+  if (r != KT_OK) return r;
+  if (n == 0) return KT_OK;
+  DeviceGuard g(ctx->device);
+  kt::RayList rl = {pix_dev, nullptr, nullptr, (uint32_t)n};
+  return run_trace(ctx, f, to_out(out), rl, (uint64_t)n, (cudaStream_t)stream);
+}
+
+kt_status kt_trace_host(kt_context* ctx, const kt_frame_desc* desc, const kt_geo_soa* out_host) {
+  if (!ctx) return KT_ERR_INVALID_ARGUMENT;
+  if (!out_complete(out_host)) return fail(ctx, KT_ERR_INVALID_ARGUMENT, "kt_trace_host: NULL output");
+  kt::Frame f;
+  kt_status r = kt::prepare_frame(desc, &f, nullptr, &ctx->err);
+  if (r != KT_OK) return r;
+  DeviceGuard g(ctx->device);
+  const size_t n = (size_t)desc->width * (size_t)desc->height;
+  // 6 float64 arrays, attempts, steps, outcome, status
+  const size_t need = n * (6 * 8 + 4 + 4 + 1 + 1) + 256;
+  r = ensure(ctx, (void**)&ctx->d_stage, &ctx->stage_cap, need, "staging buffer");
+  if (r != KT_OK) return r;
+  unsigned char* p = ctx->d_stage;
+  kt_geo_soa d;
+  d.r = (double*)p; p += 8 * n;
+  d.redshift = (double*)p; p += 8 * n;
+  d.magnif = (double*)p; p += 8 * n;
+  d.phi_disk = (double*)p; p += 8 * n;
+  d.theta_esc = (double*)p; p += 8 * n;
+  d.phi_esc = (double*)p; p += 8 * n;
+  d.steps = (uint32_t*)p; p += 4 * n;
+  d.attempts = (uint32_t*)p; p += 4 * n;
+  d.outcome = p; p += n;
+  d.status = p;
+  if (!out_host->status) d.status = nullptr;
+  if (!out_host->steps) d.steps = nullptr;
+  if (!out_host->attempts) d.attempts = nullptr;
+  kt::RayList rl = {nullptr, nullptr, nullptr, (uint32_t)n};
+  r = run_trace(ctx, f, to_out(&d), rl, n, ctx->stream);
+  if (r != KT_OK) return r;
+  struct { void* dst; const void* src; size_t bytes; } cp[] = {
+      {out_host->outcome, d.outcome, n}, {out_host->r, d.r, 8 * n},
+      {out_host->redshift, d.redshift, 8 * n}, {out_host->magnif, d.magnif, 8 * n},
+      {out_host->phi_disk, d.phi_disk, 8 * n}, {out_host->theta_esc, d.theta_esc, 8 * n},
+      {out_host->phi_esc, d.phi_esc, 8 * n}, {out_host->status, d.status, n},
+      {out_host->steps, d.steps, 4 * n}, {out_host->attempts, d.attempts, 4 * n}};
+  for (auto& c : cp)
+    if (c.dst && c.src)
+      KT_CUDA(ctx, cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToHost, ctx->stream),
+              "copy results to host");
+  KT_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "trace");
+  return KT_OK;
+}
+
+kt_status kt_colorize(kt_context* ctx, const kt_frame_desc* desc, const kt_geo_soa* geo,
+                      const kt_color_params* cp, const uint8_t* bg_rgb, int32_t bg_w,
+                      int32_t bg_h, uint8_t* rgb_out, void* stream) {
+  if (!ctx) return KT_ERR_INVALID_ARGUMENT;
+  if (!geo || !geo->outcome || !geo->r || !geo->redshift || !geo->magnif || !geo->theta_esc ||
+      !geo->phi_esc || !cp || !rgb_out)
+    return fail(ctx, KT_ERR_INVALID_ARGUMENT, "kt_colorize: NULL pointer");
+  if (bg_rgb && (bg_w < 1 || bg_h < 1))
+    return fail(ctx, KT_ERR_INVALID_ARGUMENT, "kt_colorize: background size must be >= 1");
+  if (cp->palette != 0) return fail(ctx, KT_ERR_UNSUPPORTED, "only the blackbody palette is implemented");
+  kt::Frame f;
+  kt_status r = kt::prepare_frame(desc, &f, nullptr, &ctx->err);
+  if (r != KT_OK) return r;
+  DeviceGuard g(ctx->device);
+  const kt::ColourConst cc = kt::make_colour(f, *cp);
+  const int64_t n = (int64_t)desc->width * desc->height;
+  KT_CUDA(ctx, kt::launch_colorize(cc, n, geo->outcome, geo->r, geo->redshift, geo->magnif,
+                                   geo->theta_esc, geo->phi_esc, bg_rgb, bg_w, bg_h, rgb_out,
+                                   (cudaStream_t)stream),
+          "colorize kernel launch");
+  return KT_OK;
+}
+
+kt_status kt_render_host(kt_context* ctx, const kt_frame_desc* desc, const kt_color_params* cp,
+                         const uint8_t* bg_rgb_host, int32_t bg_w, int32_t bg_h,
+                         uint8_t* rgb_out_host) {
+  if (!ctx) return KT_ERR_INVALID_ARGUMENT;
+  if (!cp || !rgb_out_host) return fail(ctx, KT_ERR_INVALID_ARGUMENT, "kt_render_host: NULL pointer");
+  if (bg_rgb_host && (bg_w < 1 || bg_h < 1))
+    return fail(ctx, KT_ERR_INVALID_ARGUMENT, "kt_render_host: background size must be >= 1");
+  kt::Frame f;
+  kt_status r = kt::prepare_frame(desc, &f, nullptr, &ctx->err);
+  if (r != KT_OK) return r;
+  DeviceGuard g(ctx->device);
+  const size_t n = (size_t)desc->width * (size_t)desc->height;
+  const size_t need = n * (6 * 8 + 1 + 3) + 256;
+  r = ensure(ctx, (void**)&ctx->d_stage, &ctx->stage_cap, need, "staging buffer");
+  if (r != KT_OK) return r;
+  unsigned char* p = ctx->d_stage;
+  kt_geo_soa d;
+  memset(&d, 0, sizeof d);
+  d.r = (double*)p; p += 8 * n;
+  d.redshift = (double*)p; p += 8 * n;
+  d.magnif = (double*)p; p += 8 * n;
+  d.phi_disk = (double*)p; p += 8 * n;
+  d.theta_esc = (double*)p; p += 8 * n;
+  d.phi_esc = (double*)p; p += 8 * n;
+  d.outcome = p; p += n;
+  uint8_t* d_rgb = p;
+  const uint8_t* d_bg = nullptr;
+  if (bg_rgb_host) {
+    const size_t bb = (size_t)bg_w * (size_t)bg_h * 3;
+    r = ensure(ctx, (void**)&ctx->d_bg, &ctx->bg_cap, bb, "background buffer");
+    if (r != KT_OK) return r;
+    KT_CUDA(ctx, cudaMemcpyAsync(ctx->d_bg, bg_rgb_host, bb, cudaMemcpyHostToDevice, ctx->stream),
+            "copy background");
+    d_bg = ctx->d_bg;
+  }
+  kt::RayList rl = {nullptr, nullptr, nullptr, (uint32_t)n};
+  r = run_trace(ctx, f, to_out(&d), rl, n, ctx->stream);
+  if (r != KT_OK) return r;
+  const kt::ColourConst cc = kt::make_colour(f, *cp);
+  if (cp->palette != 0) return fail(ctx, KT_ERR_UNSUPPORTED, "only the blackbody palette is implemented");
+  KT_CUDA(ctx, kt::launch_colorize(cc, (int64_t)n, d.outcome, d.r, d.redshift, d.magnif, d.theta_esc,
+                                   d.phi_esc, d_bg, bg_w, bg_h, d_rgb, ctx->stream),
+          "colorize kernel launch");
+  KT_CUDA(ctx, cudaMemcpyAsync(rgb_out_host, d_rgb, 3 * n, cudaMemcpyDeviceToHost, ctx->stream),
+          "copy image to host");
+  KT_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "render");
+  return KT_OK;
+}
+
+kt_status kt_measure_fp64_peak(kt_context* ctx, double* gflops) {
+  if (!ctx || !gflops) return KT_ERR_INVALID_ARGUMENT;
+  DeviceGuard g(ctx->device);
+  int sms = 0;
+  KT_CUDA(ctx, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device), "attr");
+  const int block = 256, grid = sms * 8, n_iter = 4096;
+  double* d_sink = nullptr;
+  KT_CUDA(ctx, cudaMalloc((void**)&d_sink, grid * sizeof(double)), "probe buffer");
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best_ms = 1e30f;
+  cudaError_t err = cudaSuccess;
+  for (int rep = 0; rep < 4 && err == cudaSuccess; ++rep) {
+    cudaEventRecord(e0, ctx->stream);
+    err = kt::launch_fp64_probe(d_sink, n_iter, grid, block, ctx->stream);
+    cudaEventRecord(e1, ctx->stream);
+    if (err == cudaSuccess) err = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    if (err == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess && rep > 0 && ms < best_ms)
+      best_ms = ms;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(d_sink);
+  if (err != cudaSuccess) return cuda_fail(ctx, err, "FP64 probe");
+  const double fmas = (double)grid * block * n_iter * 8.0;
+  *gflops = 2.0 * fmas / (best_ms * 1e-3) / 1e9;
+  return KT_OK;
+}
+
+}  // extern "C"

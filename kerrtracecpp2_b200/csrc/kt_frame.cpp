@@ -1,0 +1,253 @@
+// kt_frame.cpp -- host-side frame preparation (the per-frame part of the
+// reference's trace_geodesics, main.cpp:2014-2082).
+//
+// Validates a kt_frame_desc, applies the reference's chart fallback rules and
+// argument clamps, and computes the frame constants the kernels use: outer
+// horizon r_+ (knds_metric.hpp:237-315), ISCO (knds_metric.hpp:318-349),
+// disk bounds, escape radius, and the observer's metric for the camera.  The
+// arithmetic is the reference's, evaluated with the renderer's libm so that
+// every derived constant is bit-identical to what the reference computes.
+// Compile with -ffp-contract=off.
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+
+#include "kt_frame.h"
+
+namespace kt {
+
+static double delta_r(const Metric& g, double r) { return bl_delta_r(g, r, r * r + g.a2); }
+
+// r_horizon (knds_metric.hpp:237-315): closed form for Lambda = 0, else a
+// 20000-point logarithmic scan of Delta_r with 160-step bisection; for
+// Lambda > 0 the largest root is cosmological and the next one is taken.
+double host_r_horizon(const Metric& g) {
+  const double M = g.M, a = g.a, Q = g.Q, L = g.L;
+  if (fabs(L) < 1e-15) {
+    const double disc = (M * M - a * a) - Q * Q;
+    return M + sqrt(dmax(disc, 0.0));
+  }
+  const double scale = dmax(fabs(M), 1.0);
+  const double rmin = dmax(1e-6 * scale, 1e-9);
+  double rmax;
+  if (L > 0.0)
+    rmax = dmax(20.0 * scale, 1.25 * sqrt(3.0 / L));
+  else
+    rmax = (200.0 * scale + 20.0 * fabs(a)) + 20.0 * fabs(Q);
+  if (!(rmax > rmin)) rmax = rmin * 10.0;
+
+  auto bisect = [&](double lo, double hi) -> double {
+    double flo = delta_r(g, lo), fhi = delta_r(g, hi);
+    if (!finite(flo) || !finite(fhi)) return ktm_nan();
+    for (int i = 0; i < 160; ++i) {
+      const double mid = 0.5 * (lo + hi);
+      const double fmid = delta_r(g, mid);
+      if (!finite(fmid)) break;
+      if ((flo > 0.0 && fmid < 0.0) || (flo < 0.0 && fmid > 0.0)) {
+        hi = mid;
+        fhi = fmid;
+      } else {
+        lo = mid;
+        flo = fmid;
+      }
+    }
+    (void)fhi;
+    return 0.5 * (lo + hi);
+  };
+  double roots[16];
+  int nroots = 0;
+  auto push_root = [&](double rr) {
+    if (!finite(rr) || rr <= 0.0) return;
+    for (int i = 0; i < nroots; ++i) {
+      double rel = 1.0;
+      if (rel < fabs(roots[i])) rel = fabs(roots[i]);
+      if (rel < fabs(rr)) rel = fabs(rr);
+      if (fabs(roots[i] - rr) <= 1e-8 * rel) return;
+    }
+    if (nroots < 16) roots[nroots++] = rr;
+  };
+  const int samples = 20000;
+  const double log_span = ktm_log(rmax / rmin);
+  double prev_r = rmin;
+  double prev_f = delta_r(g, prev_r);
+  for (int i = 1; i <= samples; ++i) {
+    const double t = (double)i / (double)samples;
+    const double r = rmin * ktm_exp(log_span * t);
+    const double f = delta_r(g, r);
+    if (finite(prev_f) && finite(f)) {
+      if (prev_f == 0.0) push_root(prev_r);
+      if (f == 0.0) push_root(r);
+      if ((prev_f > 0.0 && f < 0.0) || (prev_f < 0.0 && f > 0.0)) push_root(bisect(prev_r, r));
+    }
+    prev_r = r;
+    prev_f = f;
+  }
+  if (nroots == 0) {
+    const double disc = (M * M - a * a) - Q * Q;
+    return M + sqrt(dmax(disc, 0.0));
+  }
+  std::sort(roots, roots + nroots);
+  if (L > 0.0 && nroots >= 2) return roots[nroots - 2];
+  return roots[nroots - 1];
+}
+
+// r_isco (knds_metric.hpp:318-349): Bardeen-Press-Teukolsky closed form for
+// Kerr; otherwise the first radius (1e-4 M steps from 1.05 r_+) where the
+// circular-orbit angular momentum stops decreasing.
+double host_r_isco(const Metric& g) {
+  const double M = g.M, a = g.a;
+  if (fabs(g.L) < 1e-15 && fabs(g.Q) < 1e-15) {
+    if (fabs(a) < 1e-10) return 6.0 * M;
+    const double ap = a / M;
+    const double z1 = 1.0 + ktm_cbrt(1.0 - ap * ap) * (ktm_cbrt(1.0 + ap) + ktm_cbrt(1.0 - ap));
+    const double z2 = sqrt((3.0 * ap) * ap + z1 * z1);
+    return M * ((3.0 + z2) - sqrt((3.0 - z1) * ((3.0 + z1) + 2.0 * z2)));
+  }
+  const Ang eq = bl_ang(g, kHalfPi);
+  auto L_circ = [&](double rr) -> double {
+    const double Om = kepler_omega(g, rr);
+    const Cov G = bl_cov(g, rr, eq);
+    const double N2 = -((G.tt + (2.0 * G.tp) * Om) + (G.pp * Om) * Om);
+    if (N2 <= 0.0) return -1e30;
+    const double ut = 1.0 / sqrt(N2);
+    return -(G.tp + G.pp * Om) * ut;
+  };
+  const double rh = host_r_horizon(g);
+  double r = rh * 1.05;
+  const double dr = 1e-4 * M;
+  double L_prev = L_circ(r);
+  for (; r < 30.0 * M; r += dr) {
+    const double Lc = L_circ(r + dr);
+    if (Lc < L_prev && L_prev > 0.0) return r;
+    L_prev = Lc;
+  }
+  return r;
+}
+
+static bool all_finite(std::initializer_list<double> xs) {
+  for (double x : xs)
+    if (!finite(x)) return false;
+  return true;
+}
+
+kt_status prepare_frame(const kt_frame_desc* d, Frame* f, kt_frame_derived* dv, std::string* err) {
+  if (d == nullptr) {
+    *err = "frame descriptor is NULL";
+    return KT_ERR_INVALID_ARGUMENT;
+  }
+  if (d->width < 1 || d->height < 1) {
+    *err = "width and height must be >= 1";
+    return KT_ERR_INVALID_ARGUMENT;
+  }
+  if ((int64_t)d->width * (int64_t)d->height > (int64_t)0x7fffffff) {
+    *err = "width*height exceeds 2^31-1 pixels";
+    return KT_ERR_INVALID_ARGUMENT;
+  }
+  if (!all_finite({d->M, d->a, d->Q, d->Lambda, d->theta_deg, d->phi_deg, d->r_obs, d->disk_out,
+                   d->fov_deg, d->pixel_offset_x, d->pixel_offset_y, d->step_init, d->tol})) {
+    *err = "non-finite frame parameter";
+    return KT_ERR_INVALID_ARGUMENT;
+  }
+  if (d->chart != KT_CHART_KS && d->chart != KT_CHART_BL) {
+    *err = "chart must be KT_CHART_KS or KT_CHART_BL";
+    return KT_ERR_INVALID_ARGUMENT;
+  }
+  if (d->integrator != KT_RK4_DOUBLING && d->integrator != KT_DOPRI5) {
+    *err = "integrator must be KT_RK4_DOUBLING or KT_DOPRI5";
+    return KT_ERR_INVALID_ARGUMENT;
+  }
+  if (d->bundles != 0 && d->bundles != 1) {
+    *err = "bundles must be 0 or 1";
+    return KT_ERR_INVALID_ARGUMENT;
+  }
+  if (d->solver_mode != KT_SOLVER_STANDARD) {
+    *err = "only --solver-mode standard runs on this backend";
+    return KT_ERR_UNSUPPORTED;
+  }
+  if (d->precision != KT_PREC_FP64) {
+    *err = "only KT_PREC_FP64 is implemented";
+    return KT_ERR_UNSUPPORTED;
+  }
+  if ((d->flags & ~(uint32_t)KT_FLAG_ANGLES_RADIANS) != 0) {
+    *err = "unknown bits in flags";
+    return KT_ERR_INVALID_ARGUMENT;
+  }
+  if (!(d->r_obs > 0.0) || !(d->M > 0.0)) {
+    *err = "r_obs and M must be positive";
+    return KT_ERR_INVALID_ARGUMENT;
+  }
+
+  Frame fr;
+  memset(&fr, 0, sizeof fr);
+  fr.g = make_metric(d->M, d->a, d->Q, d->Lambda);
+  // Chart fallback rules (main.cpp:2033-2049).
+  int chart = d->chart;
+  if (chart == KT_CHART_KS && fabs(d->Lambda) > 1e-15) chart = KT_CHART_BL;
+  if (d->bundles && chart == KT_CHART_KS) chart = KT_CHART_BL;
+  fr.chart = chart;
+  fr.intg = d->integrator;
+  fr.bundles = d->bundles;
+  // Camera (camera.hpp:32-35): degrees -> radians as theta_deg * M_PI / 180.
+  double th, ph, fov;
+  if (d->flags & KT_FLAG_ANGLES_RADIANS) {
+    th = d->theta_deg;
+    ph = d->phi_deg;
+    fov = d->fov_deg;
+  } else {
+    th = (d->theta_deg * kPi) / 180.0;
+    ph = (d->phi_deg * kPi) / 180.0;
+    fov = (d->fov_deg * kPi) / 180.0;
+  }
+  fr.cam = make_camera(fr.g, d->r_obs, th, ph, fov, d->width, d->height, d->pixel_offset_x,
+                       d->pixel_offset_y);
+  fr.eq = bl_ang(fr.g, kHalfPi);
+  // Controls with main()'s clamps (main.cpp:2683-2686) and the tracers' own
+  // max(step_init, 1e-10) / max(1, max_steps).
+  fr.max_steps = std::max(1, (int)d->max_steps);
+  fr.dlam0 = dmax(dmax(1e-10, d->step_init), 1e-10);
+  fr.tol = dmax(1e-10, d->tol);
+  const double rh = host_r_horizon(fr.g);
+  const double r_isco = host_r_isco(fr.g);
+  fr.rh_cut = rh * 1.03;
+  fr.r_in = r_isco;
+  fr.r_out = d->disk_out;
+  fr.r_esc = d->r_obs * 1.05;
+  fr.bundle_eps = (fov / (double)d->width) * 0.5;
+  *f = fr;
+  if (dv) {
+    memset(dv, 0, sizeof *dv);
+    dv->chart = chart;
+    dv->integrator = (chart == KT_CHART_KS) ? KT_RK4_DOUBLING : d->integrator;
+    dv->r_horizon = rh;
+    dv->rh_cut = fr.rh_cut;
+    dv->r_isco = r_isco;
+    dv->r_disk_in = fr.r_in;
+    dv->r_disk_out = fr.r_out;
+    dv->r_escape = fr.r_esc;
+    dv->r_obs = d->r_obs;
+    dv->theta_obs = th;
+    dv->phi_obs = ph;
+    dv->fov_h = fov;
+    dv->dlam0 = fr.dlam0;
+    dv->max_steps = fr.max_steps;
+    dv->tol = fr.tol;
+    dv->bundle_eps = fr.bundle_eps;
+  }
+  return KT_OK;
+}
+
+ColourConst make_colour(const Frame& f, const kt_color_params& cp) {
+  ColourConst cc;
+  cc.M = f.g.M;
+  cc.r_isco = f.r_in;
+  cc.exposure = cp.exposure;
+  cc.gamma = cp.gamma;
+  cc.temp_scale = cp.temp_scale;
+  cc.log10_50 = ktm_log10(4e4 / 800.0);
+  cc.pt_peak = page_thorne(3.0 * f.r_in, f.r_in);
+  return cc;
+}
+
+}  // namespace kt

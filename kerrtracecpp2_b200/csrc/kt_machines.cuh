@@ -1,0 +1,880 @@
+// kt_machines.cuh -- per-ray integrators as "one RHS per step" state machines.
+//
+// Each machine advances one ray by exactly one right-hand-side evaluation
+// per call: input() gives the point at which the next RHS is needed,
+// consume() takes the RHS there and does the bookkeeping (stage sums, error
+// control, accept/reject, events, termination).  The persistent kernel runs
+// input -> RHS -> consume in a loop, so the heavy RHS code appears once in
+// the kernel, every lane evaluates one RHS per iteration whatever stage its
+// ray is in, and a lane whose ray finished is refilled from the ray queue
+// on the next iteration.
+//
+// Arithmetic and control flow follow the reference renderer:
+//   BL  RK4 step doubling : trace_single + rk4_adaptive (main.cpp:343-434,
+//                           geodesic.hpp:169-257)
+//   BL  DOPRI5            : trace_single + dopri5_adaptive (geodesic.hpp:284-414)
+//   KS  RK4 step doubling : trace_single_ks (main.cpp:1456-1660)
+//   BL  Jacobi bundle     : trace_bundle (ray_bundle.hpp:137-436)
+// The reference evaluates f(s0) twice per step-doubling attempt and f at
+// both ends of an accepted step for the event test; these are the same
+// inputs, so the machines evaluate each once and reuse it (bit-identical).
+#pragma once
+
+#include "kt_physics.cuh"
+
+namespace kt {
+
+enum : int { kOutEscaped = 0, kOutDisk = 1, kOutHorizon = 2 };
+enum : int { kStEvent = 0, kStStepCap = 1, kStRejectCap = 2, kStNonfinite = 3 };
+enum : int { kEvNone = 0, kEvDisk = 1, kEvHorizon = 2, kEvEscape = 3 };
+
+struct Frame {
+  Metric g;
+  CamConst cam;
+  Ang eq;  // bl_ang at theta = pi/2 (disk redshift)
+  double r_in, r_out, r_esc, rh_cut;
+  double dlam0, tol;
+  double bundle_eps;
+  int max_steps;
+  int chart, intg, bundles;
+};
+
+struct RayResult {
+  double r, red, magnif, phi_disk, th_esc, ph_esc;
+  uint32_t steps, attempts;
+  int outcome, status;
+};
+
+KT_HD void set_result(RayResult* o, int outcome, int status, double r, double red, double magnif,
+                      double phi_disk, double th_esc, double ph_esc) {
+  o->outcome = outcome;
+  o->status = status;
+  o->r = r;
+  o->red = red;
+  o->magnif = magnif;
+  o->phi_disk = phi_disk;
+  o->th_esc = th_esc;
+  o->ph_esc = ph_esc;
+}
+
+// Step-size update shared by the step-doubling controllers (geodesic.hpp:226-256,
+// main.cpp:1507-1527, ray_bundle.hpp:235-262): returns 1 accepted, 0
+// rejected, -1 non-finite error.
+KT_HD int doubling_update(double err, double tol, double* dlam) {
+  if (!finite(err)) {
+    *dlam = (finite(*dlam) && *dlam > 1e-10) ? *dlam * 0.5 : 1e-6;
+    if (*dlam < 1e-10) *dlam = 1e-10;
+    return -1;
+  }
+  const int accepted = (err < tol || *dlam < 1e-10);
+  if (accepted) {
+    const double scale = (err > 1e-14) ? 0.9 * ktm_pow(tol / err, 0.2) : 4.0;
+    double hnew = *dlam * scale;
+    if (!finite(hnew)) hnew = *dlam;
+    *dlam = hnew;
+    if (*dlam > 100.0) *dlam = 100.0;
+    if (*dlam < 1e-10) *dlam = 1e-10;
+  } else {
+    const double half = *dlam * 0.5;
+    double hnew = (*dlam * 0.9) * ktm_pow(tol / err, 0.25);
+    if (!finite(hnew)) hnew = half;
+    *dlam = hnew;
+    if (*dlam > half) *dlam = half;
+    if (*dlam < 1e-10) *dlam = 1e-10;
+  }
+  return accepted;
+}
+
+// After a rejected attempt: the reference's `!isfinite(dlam) || ++rejects > 64`.
+KT_HD bool reject_cap(double h, int* rejects, int* status) {
+  if (!finite(h)) {
+    *status = kStNonfinite;
+    return true;
+  }
+  if (++*rejects > 64) {
+    *status = kStRejectCap;
+    return true;
+  }
+  return false;
+}
+
+// Horizon and escape tests of one accepted step (main.cpp:398-418); updates
+// best_alpha / ev when the crossing comes first.
+KT_HD void horizon_escape(double r_prev, double r_now, double rh_cut, double r_esc,
+                          double* best_alpha, int* ev) {
+  if (r_now <= rh_cut) {
+    const double denom_h = r_prev - r_now;
+    double alpha_h = (fabs(denom_h) > 1e-12) ? ((r_prev - rh_cut) / denom_h) : 0.0;
+    alpha_h = dclamp(alpha_h, 0.0, 1.0);
+    if (alpha_h < *best_alpha) {
+      *best_alpha = alpha_h;
+      *ev = kEvHorizon;
+    }
+  }
+  if (r_now >= r_esc) {
+    const double denom_e = r_now - r_prev;
+    double alpha_e = (fabs(denom_e) > 1e-12) ? ((r_esc - r_prev) / denom_e) : 1.0;
+    alpha_e = dclamp(alpha_e, 0.0, 1.0);
+    if (alpha_e < *best_alpha) {
+      *best_alpha = alpha_e;
+      *ev = kEvEscape;
+    }
+  }
+}
+
+// ------------------------------------------------------- BL, single ray
+// Shared state of the BL single-ray machines.
+struct BLBase {
+  double r, th, ph, pr, pth, pt, pphi;  // GeodesicState
+  double h;                             // dlam
+  double k1[5];                         // f(s) = {dr, dth, dpr, dpth, dphi}
+  double step_used;
+  int slot, it, rejects;
+  uint32_t attempts;
+
+  KT_HD void init_state(const Frame& f, const Geo& s) {
+    r = s.r;
+    th = s.th;
+    ph = s.ph;
+    pr = s.pr;
+    pth = s.pth;
+    pt = s.pt;
+    pphi = s.pphi;
+    h = f.dlam0;
+    step_used = h;
+    slot = -1;
+    it = 0;
+    rejects = 0;
+    attempts = 0;
+  }
+
+  // Events of trace_single (main.cpp:364-433) for the accepted step
+  // (sp_*) -> (current state), with f at both ends.  Returns true when the
+  // ray stops.
+  KT_HD bool events(const Frame& f, double sp_r, double sp_th, double sp_ph, double k0_r,
+                    double k0_th, RayResult* o) {
+    double best_alpha = 2.0;
+    int ev = kEvNone;
+    double disk_r = 0.0, disk_red = 1.0, disk_phi = 0.0;
+    const double q0 = sp_th - kHalfPi;
+    const double q1 = th - kHalfPi;
+    if (sign_change(q0, q1) || (dmin(fabs(q0), fabs(q1)) < 0.35)) {
+      double alpha = 0.0;
+      if (first_event(sp_th, th, k0_th, k1[1], step_used, kHalfPi, &alpha)) {
+        const double r_hit = hermite(sp_r, r, k0_r, k1[0], step_used, alpha);
+        if (r_hit >= f.r_in && r_hit <= f.r_out) {
+          disk_r = r_hit;
+          disk_red = dclamp(disk_redshift(f.g, f.eq, r_hit, pt, pphi), 0.0, 20.0);
+          disk_phi = sp_ph + alpha * (ph - sp_ph);
+          best_alpha = alpha;
+          ev = kEvDisk;
+        }
+      }
+    }
+    horizon_escape(sp_r, r, f.rh_cut, f.r_esc, &best_alpha, &ev);
+    if (ev == kEvNone) return false;
+    o->steps = (uint32_t)it + 1;
+    o->attempts = attempts;
+    if (ev == kEvDisk) {
+      set_result(o, kOutDisk, kStEvent, disk_r, disk_red, 1.0, disk_phi, 0.0, 0.0);
+    } else if (ev == kEvHorizon) {
+      set_result(o, kOutHorizon, kStEvent, sp_r + best_alpha * (r - sp_r), 0.0, 1.0, 0.0, 0.0, 0.0);
+    } else {
+      const double th_esc = sp_th + best_alpha * (th - sp_th);
+      const double ph_esc = sp_ph + best_alpha * (ph - sp_ph);
+      // TraceResult{ESCAPED, r_escape, 1.0, th_esc, ph_esc}: theta lands in
+      // the phi_disk slot and phi in theta_esc (main.cpp:430-432).
+      set_result(o, kOutEscaped, kStEvent, f.r_esc, 1.0, 1.0, th_esc, ph_esc, 0.0);
+    }
+    return true;
+  }
+
+  // {ESCAPED, s.r, 1.0, s.theta, s.phi} (main.cpp:359-360, 433).
+  KT_HD void stop_here(int status, uint32_t steps, RayResult* o) {
+    o->steps = steps;
+    o->attempts = attempts;
+    set_result(o, kOutEscaped, status, r, 1.0, 1.0, th, ph, 0.0);
+  }
+
+  // After an accepted step without event: next step or the step cap.
+  KT_HD bool next_step(const Frame& f, RayResult* o) {
+    ++it;
+    rejects = 0;
+    slot = 0;
+    if (it >= f.max_steps) {
+      stop_here(kStStepCap, (uint32_t)it, o);
+      return true;
+    }
+    return false;
+  }
+};
+
+// RK4 step doubling.  Slots per attempt (h = step, hb = h/2):
+//   0..2  path A  (one step h from s):     f(s + c k_prev), c = h/2, h/2, h
+//   3..5  path B1 (half step from s):      c = hb/2, hb/2, hb
+//   6     path B2 first stage:             f(B1)
+//   7..9  path B2 (half step from B1):     c = hb/2, hb/2, hb
+//   10    after acceptance:                f(B) = next k1 and the event RHS
+// slot -1 computes k1 = f(s) of a new ray.
+struct BLRk4 : BLBase {
+  double sum[5];
+  double kp[4];
+  double A[4];   // path A result (r, th, pr, pth); after acceptance: s_prev
+  double B1[5];  // r, th, ph, pr, pth
+  double sp_ph;
+
+  KT_HD void init(const Frame& f, const Geo& s) { init_state(f, s); }
+
+  KT_HD void input(double y[4]) const {
+    if (slot == -1 || slot == 10) {
+      y[0] = r; y[1] = th; y[2] = pr; y[3] = pth;
+      return;
+    }
+    if (slot == 6) {
+      y[0] = B1[0]; y[1] = B1[1]; y[2] = B1[3]; y[3] = B1[4];
+      return;
+    }
+    // slots 0-5 start from s, 7-9 from B1; the first stage of a path uses k1
+    const double hb = 0.5 * h;
+    const bool on_s = slot < 6;
+    const int j = (slot < 3) ? slot : (slot < 6) ? slot - 3 : slot - 6;
+    const double hs = (slot < 3) ? h : hb;
+    // stage 4 of a path takes the full step, stages 2-3 half of it
+    const double c = (on_s ? (j == 2) : (slot == 9)) ? hs : 0.5 * hs;
+    const bool use_k1 = on_s && j == 0;
+    y[0] = (on_s ? r : B1[0]) + c * (use_k1 ? k1[0] : kp[0]);
+    y[1] = (on_s ? th : B1[1]) + c * (use_k1 ? k1[1] : kp[1]);
+    y[2] = (on_s ? pr : B1[3]) + c * (use_k1 ? k1[2] : kp[2]);
+    y[3] = (on_s ? pth : B1[4]) + c * (use_k1 ? k1[3] : kp[3]);
+  }
+
+  // Returns true when the ray is finished (o filled).
+  KT_HD bool consume(const Frame& f, const double k[5], RayResult* o) {
+    switch (slot) {
+      case -1:
+        for (int i = 0; i < 5; ++i) k1[i] = k[i];
+        slot = 0;
+        return false;
+      case 0:
+      case 3:
+        for (int i = 0; i < 5; ++i) sum[i] = k1[i] + 2.0 * k[i];
+        for (int i = 0; i < 4; ++i) kp[i] = k[i];
+        ++slot;
+        return false;
+      case 1:
+      case 4:
+      case 7:
+      case 8:
+        for (int i = 0; i < 5; ++i) sum[i] = sum[i] + 2.0 * k[i];
+        for (int i = 0; i < 4; ++i) kp[i] = k[i];
+        ++slot;
+        return false;
+      case 6:
+        for (int i = 0; i < 5; ++i) sum[i] = k[i];
+        for (int i = 0; i < 4; ++i) kp[i] = k[i];
+        slot = 7;
+        return false;
+      case 2: {
+        const double w = h / 6.0;
+        A[0] = r + w * (sum[0] + k[0]);
+        A[1] = th + w * (sum[1] + k[1]);
+        A[2] = pr + w * (sum[2] + k[2]);
+        A[3] = pth + w * (sum[3] + k[3]);
+        slot = 3;
+        return false;
+      }
+      case 5: {
+        const double w = (0.5 * h) / 6.0;
+        B1[0] = r + w * (sum[0] + k[0]);
+        B1[1] = th + w * (sum[1] + k[1]);
+        B1[2] = ph + w * (sum[4] + k[4]);
+        B1[3] = pr + w * (sum[2] + k[2]);
+        B1[4] = pth + w * (sum[3] + k[3]);
+        slot = 6;
+        return false;
+      }
+      case 9: {
+        const double w = (0.5 * h) / 6.0;
+        const double Br = B1[0] + w * (sum[0] + k[0]);
+        const double Bth = B1[1] + w * (sum[1] + k[1]);
+        const double Bph = B1[2] + w * (sum[4] + k[4]);
+        const double Bpr = B1[3] + w * (sum[2] + k[2]);
+        const double Bpth = B1[4] + w * (sum[3] + k[3]);
+        const double e0 = A[0] - Br, e1 = A[1] - Bth, e2 = A[2] - Bpr, e3 = A[3] - Bpth;
+        const double err = sqrt(((e0 * e0 + e1 * e1) + e2 * e2) + e3 * e3) / 15.0;
+        step_used = h;
+        ++attempts;
+        const int acc = doubling_update(err, f.tol, &h);
+        if (acc == 1) {
+          A[0] = r;  // s_prev
+          A[1] = th;
+          sp_ph = ph;
+          kp[0] = k1[0];  // f(s_prev): dr, dth
+          kp[1] = k1[1];
+          r = Br;
+          th = Bth;
+          ph = Bph;
+          pr = Bpr;
+          pth = Bpth;
+          slot = 10;
+          return false;
+        }
+        int st;
+        if (reject_cap(h, &rejects, &st)) {
+          stop_here(st, (uint32_t)it, o);
+          return true;
+        }
+        slot = 0;
+        return false;
+      }
+      default: {  // 10: k = f(s_new)
+        for (int i = 0; i < 5; ++i) k1[i] = k[i];
+        if (events(f, A[0], A[1], sp_ph, kp[0], kp[1], o)) return true;
+        return next_step(f, o);
+      }
+    }
+  }
+};
+
+// DOPRI5 (Dormand-Prince 5(4), FSAL).  Slots: -1 -> k1 = f(s) of a new ray;
+// 0..4 -> k2..k6; 5 -> k7 = f(y5), then error control.  Phi is not advanced
+// (the reference's `advance` updates r, theta, p_r, p_theta only).
+struct BLDopri5 : BLBase {
+  double kk[7][4];
+
+  KT_HD void init(const Frame& f, const Geo& s) { init_state(f, s); }
+
+  // advance (geodesic.hpp:300-310): y = s + sum_i (h w_i) k_i, in order.
+  template <int N>
+  KT_HD void adv(const double* w, double y[4]) const {
+    y[0] = r; y[1] = th; y[2] = pr; y[3] = pth;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      const double hw = h * w[i];
+      y[0] += hw * kk[i][0];
+      y[1] += hw * kk[i][1];
+      y[2] += hw * kk[i][2];
+      y[3] += hw * kk[i][3];
+    }
+  }
+
+  KT_HD void input(double y[4]) const {
+    const double a2[1] = {1.0 / 5.0};
+    const double a3[2] = {3.0 / 40.0, 9.0 / 40.0};
+    const double a4[3] = {44.0 / 45.0, -56.0 / 15.0, 32.0 / 9.0};
+    const double a5[4] = {19372.0 / 6561.0, -25360.0 / 2187.0, 64448.0 / 6561.0, -212.0 / 729.0};
+    const double a6[5] = {9017.0 / 3168.0, -355.0 / 33.0, 46732.0 / 5247.0, 49.0 / 176.0,
+                          -5103.0 / 18656.0};
+    const double b5[6] = {35.0 / 384.0, 0.0, 500.0 / 1113.0, 125.0 / 192.0, -2187.0 / 6784.0,
+                          11.0 / 84.0};
+    switch (slot) {
+      case 0: adv<1>(a2, y); break;
+      case 1: adv<2>(a3, y); break;
+      case 2: adv<3>(a4, y); break;
+      case 3: adv<4>(a5, y); break;
+      case 4: adv<5>(a6, y); break;
+      case 5: adv<6>(b5, y); break;
+      default: y[0] = r; y[1] = th; y[2] = pr; y[3] = pth; break;
+    }
+  }
+
+  KT_HD bool consume(const Frame& f, const double k[5], RayResult* o) {
+    if (slot < 0) {
+      for (int i = 0; i < 4; ++i) kk[0][i] = k[i];
+      slot = 0;
+      return false;
+    }
+    if (slot < 5) {
+      switch (slot) {  // constant indices keep kk in registers
+        case 0: for (int i = 0; i < 4; ++i) kk[1][i] = k[i]; break;
+        case 1: for (int i = 0; i < 4; ++i) kk[2][i] = k[i]; break;
+        case 2: for (int i = 0; i < 4; ++i) kk[3][i] = k[i]; break;
+        case 3: for (int i = 0; i < 4; ++i) kk[4][i] = k[i]; break;
+        default: for (int i = 0; i < 4; ++i) kk[5][i] = k[i]; break;
+      }
+      ++slot;
+      return false;
+    }
+    for (int i = 0; i < 4; ++i) kk[6][i] = k[i];
+    const double b5[6] = {35.0 / 384.0, 0.0, 500.0 / 1113.0, 125.0 / 192.0, -2187.0 / 6784.0,
+                          11.0 / 84.0};
+    const double b4[7] = {5179.0 / 57600.0, 0.0, 7571.0 / 16695.0, 393.0 / 640.0,
+                          -92097.0 / 339200.0, 187.0 / 2100.0, 1.0 / 40.0};
+    double y5[4], y4[4];
+    adv<6>(b5, y5);
+    adv<7>(b4, y4);
+    const double ref[4] = {r, th, pr, pth};
+    double err2 = 0.0;
+    for (int i = 0; i < 4; ++i) {
+      const double ratio = (y5[i] - y4[i]) / (f.tol * (1.0 + fabs(ref[i])));
+      err2 += ratio * ratio;
+    }
+    const double err = sqrt(err2 / 4.0);
+    step_used = h;
+    ++attempts;
+    slot = 0;
+    if (!finite(err)) {
+      h = (finite(h) && h > 1e-10) ? h * 0.5 : 1e-6;
+      if (h < 1e-10) h = 1e-10;
+    } else if (err <= 1.0 || h < 1e-10) {
+      const double fac = (err > 1e-12) ? 0.9 * ktm_pow(1.0 / err, 0.2) : 4.0;
+      double hnew = h * fac;
+      if (!finite(hnew)) hnew = h;
+      if (hnew > 100.0) hnew = 100.0;
+      if (hnew < 1e-10) hnew = 1e-10;
+      h = hnew;
+      const double sp_r = r, sp_th = th;
+      const double k0_r = kk[0][0], k0_th = kk[0][1];
+      r = y5[0];
+      th = y5[1];
+      pr = y5[2];
+      pth = y5[3];
+      for (int i = 0; i < 4; ++i) kk[0][i] = kk[6][i];  // FSAL
+      k1[0] = kk[0][0];
+      k1[1] = kk[0][1];
+      if (events(f, sp_r, sp_th, ph, k0_r, k0_th, o)) return true;
+      return next_step(f, o);
+    } else {
+      double hnew = (h * 0.9) * ktm_pow(1.0 / err, 0.25);
+      if (!finite(hnew)) hnew = h * 0.5;
+      h = dmax(hnew, 1e-10);
+    }
+    int st;
+    if (reject_cap(h, &rejects, &st)) {
+      stop_here(st, (uint32_t)it, o);
+      return true;
+    }
+    return false;
+  }
+};
+
+// ------------------------------------------------------------- KS chart
+// trace_single_ks (main.cpp:1530-1660), RK4 step doubling in (X,Y,Z,p).
+struct KSRk4 {
+  double s[6];   // X, Y, Z, pX, pY, pZ
+  double pT;
+  double h;
+  double k1[6];
+  double sum[6], kp[6];
+  double A[6];   // path A; after acceptance: s_prev
+  double B1[6];
+  double step_used;
+  double prev_r;  // r_KS at the start of the step
+  int slot, it, rejects;
+  uint32_t attempts;
+
+  // Returns false when init_ks_state fails: the reference then traces the
+  // ray in the BL chart (main.cpp:1537-1538).
+  KT_HD bool init(const Frame& f, const Geo& sb) {
+    KSState k;
+    if (!init_ks_state(f.g, sb, &k)) return false;
+    s[0] = k.X; s[1] = k.Y; s[2] = k.Z; s[3] = k.pX; s[4] = k.pY; s[5] = k.pZ;
+    pT = k.pT;
+    h = f.dlam0;
+    step_used = h;
+    prev_r = r_ks(f.g, s[0], s[1], s[2]);
+    slot = -1;
+    it = 0;
+    rejects = 0;
+    attempts = 0;
+    return true;
+  }
+
+  KT_HD void input(double y[6]) const {
+    if (slot == -1 || slot == 10) {
+      for (int i = 0; i < 6; ++i) y[i] = s[i];
+      return;
+    }
+    if (slot == 6) {
+      for (int i = 0; i < 6; ++i) y[i] = B1[i];
+      return;
+    }
+    const double hb = 0.5 * h;
+    const bool on_s = slot < 6;
+    const int j = (slot < 3) ? slot : (slot < 6) ? slot - 3 : slot - 6;
+    const double hs = (slot < 3) ? h : hb;
+    // stage 4 of a path takes the full step, stages 2-3 half of it
+    const double c = (on_s ? (j == 2) : (slot == 9)) ? hs : 0.5 * hs;
+    const bool use_k1 = on_s && j == 0;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) y[i] = (on_s ? s[i] : B1[i]) + c * (use_k1 ? k1[i] : kp[i]);
+  }
+
+  KT_HD void stop_at(const Frame& f, const double* x, int status, uint32_t steps, RayResult* o) {
+    double rr, tt, pp;
+    ks_to_bl(f.g, x[0], x[1], x[2], &rr, &tt, &pp);
+    o->steps = steps;
+    o->attempts = attempts;
+    // TraceResult{ESCAPED, r, 1.0, th, ph}: slot quirk as in the BL tracer.
+    set_result(o, kOutEscaped, status, rr, 1.0, 1.0, tt, pp, 0.0);
+  }
+
+  KT_HD bool consume(const Frame& f, const double k[6], RayResult* o) {
+    switch (slot) {
+      case -1:
+        for (int i = 0; i < 6; ++i) k1[i] = k[i];
+        slot = 0;
+        return false;
+      case 0:
+      case 3:
+        for (int i = 0; i < 6; ++i) {
+          sum[i] = k1[i] + 2.0 * k[i];
+          kp[i] = k[i];
+        }
+        ++slot;
+        return false;
+      case 1:
+      case 4:
+      case 7:
+      case 8:
+        for (int i = 0; i < 6; ++i) {
+          sum[i] = sum[i] + 2.0 * k[i];
+          kp[i] = k[i];
+        }
+        ++slot;
+        return false;
+      case 6:
+        for (int i = 0; i < 6; ++i) {
+          sum[i] = k[i];
+          kp[i] = k[i];
+        }
+        slot = 7;
+        return false;
+      case 2: {
+        const double w = h / 6.0;
+        for (int i = 0; i < 6; ++i) A[i] = s[i] + w * (sum[i] + k[i]);
+        slot = 3;
+        return false;
+      }
+      case 5: {
+        const double w = (0.5 * h) / 6.0;
+        for (int i = 0; i < 6; ++i) B1[i] = s[i] + w * (sum[i] + k[i]);
+        slot = 6;
+        return false;
+      }
+      case 9: {
+        const double w = (0.5 * h) / 6.0;
+        double B[6];
+        for (int i = 0; i < 6; ++i) B[i] = B1[i] + w * (sum[i] + k[i]);
+        double e2 = 0.0;
+        {
+          const double e0 = A[0] - B[0], e1 = A[1] - B[1], ez = A[2] - B[2];
+          const double e3 = A[3] - B[3], e4 = A[4] - B[4], e5 = A[5] - B[5];
+          e2 = ((((e0 * e0 + e1 * e1) + ez * ez) + e3 * e3) + e4 * e4) + e5 * e5;
+        }
+        const double err = sqrt(e2) / 15.0;
+        step_used = h;
+        ++attempts;
+        const int acc = doubling_update(err, f.tol, &h);
+        if (acc == 1) {
+          for (int i = 0; i < 6; ++i) {
+            A[i] = s[i];   // s_prev
+            kp[i] = k1[i];  // f(s_prev)
+            s[i] = B[i];
+          }
+          slot = 10;
+          return false;
+        }
+        int st;
+        if (reject_cap(h, &rejects, &st)) {
+          stop_at(f, s, st, (uint32_t)it, o);
+          return true;
+        }
+        slot = 0;
+        return false;
+      }
+      default: {  // 10: k = f(s_new); events (main.cpp:1570-1657)
+        for (int i = 0; i < 6; ++i) k1[i] = k[i];
+        const double* sp = A;
+        const double* d0 = kp;
+        const double r_now = r_ks(f.g, s[0], s[1], s[2]);
+        double best_alpha = 2.0;
+        int ev = kEvNone;
+        double disk_r = 0.0, disk_red = 1.0, disk_phi = 0.0;
+        if (sign_change(sp[2], s[2]) || (dmin(fabs(sp[2]), fabs(s[2])) < 0.35)) {
+          double alpha = 0.0;
+          bool hit = first_event(sp[2], s[2], d0[2], k1[2], step_used, 0.0, &alpha);
+          if (!hit && sign_change(sp[2], s[2])) {
+            const double denom = sp[2] - s[2];
+            alpha = (fabs(denom) > 1e-12) ? (sp[2] / denom) : 0.5;
+            alpha = dclamp(alpha, 0.0, 1.0);
+            hit = true;
+          }
+          if (hit) {
+            double xh[6];
+            for (int i = 0; i < 6; ++i) xh[i] = hermite(sp[i], s[i], d0[i], k1[i], step_used, alpha);
+            double r_hit, th_hit, ph_hit;
+            ks_to_bl(f.g, xh[0], xh[1], xh[2], &r_hit, &th_hit, &ph_hit);
+            if (r_hit >= f.r_in && r_hit <= f.r_out) {
+              const double pphi_bl = ks_pphi_bl(r_hit, th_hit, ph_hit, f.g.a, xh[3], xh[4], xh[5]);
+              disk_r = r_hit;
+              disk_red = dclamp(disk_redshift(f.g, f.eq, r_hit, pT, pphi_bl), 0.0, 20.0);
+              disk_phi = ph_hit;
+              best_alpha = alpha;
+              ev = kEvDisk;
+            }
+          }
+        }
+        horizon_escape(prev_r, r_now, f.rh_cut, f.r_esc, &best_alpha, &ev);
+        if (ev != kEvNone) {
+          o->steps = (uint32_t)it + 1;
+          o->attempts = attempts;
+          if (ev == kEvDisk) {
+            set_result(o, kOutDisk, kStEvent, disk_r, disk_red, 1.0, disk_phi, 0.0, 0.0);
+          } else if (ev == kEvHorizon) {
+            set_result(o, kOutHorizon, kStEvent, prev_r + best_alpha * (r_now - prev_r), 0.0, 1.0,
+                       0.0, 0.0, 0.0);
+          } else {
+            double xe[3];
+            for (int i = 0; i < 3; ++i) xe[i] = sp[i] + best_alpha * (s[i] - sp[i]);
+            double re, te, pe;
+            ks_to_bl(f.g, xe[0], xe[1], xe[2], &re, &te, &pe);
+            set_result(o, kOutEscaped, kStEvent, re, 1.0, 1.0, te, pe, 0.0);
+          }
+          return true;
+        }
+        prev_r = r_now;
+        ++it;
+        rejects = 0;
+        slot = 0;
+        if (it >= f.max_steps) {
+          stop_at(f, s, kStStepCap, (uint32_t)it, o);
+          return true;
+        }
+        return false;
+      }
+    }
+  }
+};
+
+// ---------------------------------------------------- BL Jacobi bundle
+// trace_bundle (ray_bundle.hpp:301-436): RK4 step doubling of the geodesic
+// and the 4x2 deviation matrix W; error control on the geodesic only.
+struct Bundle {
+  double r, th, ph, pr, pth, pt, pphi;
+  double W[8];
+  double h;
+  double k1[5], kW1[8];  // f(s, W)
+  double sum[5], sumW[8], kp[4], kpW[8];
+  double A[4];            // path A geodesic; after acceptance: s_prev (r, th, ph)
+  double B1[5], B1W[8];
+  double Wprev[8];
+  double step_used, sp_ph;
+  int slot, it, rejects;
+  uint32_t attempts;
+
+  KT_HD void init(const Frame& f, int px, int py) {
+    double al, be;
+    pixel_angles(f.cam, px, py, &al, &be);
+    const Geo s = angle_ray(f.cam, al, be);
+    r = s.r; th = s.th; ph = s.ph; pr = s.pr; pth = s.pth; pt = s.pt; pphi = s.pphi;
+    // init_bundle (ray_bundle.hpp:278-298)
+    const double eps = f.bundle_eps;
+    const Geo ap = angle_ray(f.cam, al + eps, be);
+    const Geo am = angle_ray(f.cam, al - eps, be);
+    const Geo bp = angle_ray(f.cam, al, be + eps);
+    const Geo bm = angle_ray(f.cam, al, be - eps);
+    W[0] = (ap.r - am.r) / (2.0 * eps);
+    W[2] = (ap.th - am.th) / (2.0 * eps);
+    W[4] = (ap.pr - am.pr) / (2.0 * eps);
+    W[6] = (ap.pth - am.pth) / (2.0 * eps);
+    W[1] = (bp.r - bm.r) / (2.0 * eps);
+    W[3] = (bp.th - bm.th) / (2.0 * eps);
+    W[5] = (bp.pr - bm.pr) / (2.0 * eps);
+    W[7] = (bp.pth - bm.pth) / (2.0 * eps);
+    h = f.dlam0;
+    step_used = h;
+    slot = -1;
+    it = 0;
+    rejects = 0;
+    attempts = 0;
+  }
+
+  // point (geodesic y[4] and W yW[8]) of the next bundle RHS
+  KT_HD void input(double y[4], double yW[8]) const {
+    if (slot == -1 || slot == 10) {
+      y[0] = r; y[1] = th; y[2] = pr; y[3] = pth;
+#pragma unroll
+      for (int i = 0; i < 8; ++i) yW[i] = W[i];
+      return;
+    }
+    if (slot == 6) {
+      y[0] = B1[0]; y[1] = B1[1]; y[2] = B1[3]; y[3] = B1[4];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) yW[i] = B1W[i];
+      return;
+    }
+    const double hb = 0.5 * h;
+    const bool on_s = slot < 6;
+    const int j = (slot < 3) ? slot : (slot < 6) ? slot - 3 : slot - 6;
+    const double hs = (slot < 3) ? h : hb;
+    // stage 4 of a path takes the full step, stages 2-3 half of it
+    const double c = (on_s ? (j == 2) : (slot == 9)) ? hs : 0.5 * hs;
+    const bool use_k1 = on_s && j == 0;
+    y[0] = (on_s ? r : B1[0]) + c * (use_k1 ? k1[0] : kp[0]);
+    y[1] = (on_s ? th : B1[1]) + c * (use_k1 ? k1[1] : kp[1]);
+    y[2] = (on_s ? pr : B1[3]) + c * (use_k1 ? k1[2] : kp[2]);
+    y[3] = (on_s ? pth : B1[4]) + c * (use_k1 ? k1[3] : kp[3]);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) yW[i] = (on_s ? W[i] : B1W[i]) + c * (use_k1 ? kW1[i] : kpW[i]);
+  }
+
+  KT_HD bool consume(const Frame& f, const double k[5], const double kW[8], RayResult* o) {
+    switch (slot) {
+      case -1:
+        for (int i = 0; i < 5; ++i) k1[i] = k[i];
+        for (int i = 0; i < 8; ++i) kW1[i] = kW[i];
+        slot = 0;
+        return false;
+      case 0:
+      case 3:
+        for (int i = 0; i < 5; ++i) sum[i] = k1[i] + 2.0 * k[i];
+        for (int i = 0; i < 8; ++i) sumW[i] = kW1[i] + 2.0 * kW[i];
+        for (int i = 0; i < 4; ++i) kp[i] = k[i];
+        for (int i = 0; i < 8; ++i) kpW[i] = kW[i];
+        ++slot;
+        return false;
+      case 1:
+      case 4:
+      case 7:
+      case 8:
+        for (int i = 0; i < 5; ++i) sum[i] = sum[i] + 2.0 * k[i];
+        for (int i = 0; i < 8; ++i) sumW[i] = sumW[i] + 2.0 * kW[i];
+        for (int i = 0; i < 4; ++i) kp[i] = k[i];
+        for (int i = 0; i < 8; ++i) kpW[i] = kW[i];
+        ++slot;
+        return false;
+      case 6:
+        for (int i = 0; i < 5; ++i) sum[i] = k[i];
+        for (int i = 0; i < 8; ++i) sumW[i] = kW[i];
+        for (int i = 0; i < 4; ++i) kp[i] = k[i];
+        for (int i = 0; i < 8; ++i) kpW[i] = kW[i];
+        slot = 7;
+        return false;
+      case 2: {
+        const double w = h / 6.0;
+        A[0] = r + w * (sum[0] + k[0]);
+        A[1] = th + w * (sum[1] + k[1]);
+        A[2] = pr + w * (sum[2] + k[2]);
+        A[3] = pth + w * (sum[3] + k[3]);
+        slot = 3;
+        return false;
+      }
+      case 5: {
+        const double w = (0.5 * h) / 6.0;
+        B1[0] = r + w * (sum[0] + k[0]);
+        B1[1] = th + w * (sum[1] + k[1]);
+        B1[2] = ph + w * (sum[4] + k[4]);
+        B1[3] = pr + w * (sum[2] + k[2]);
+        B1[4] = pth + w * (sum[3] + k[3]);
+        for (int i = 0; i < 8; ++i) B1W[i] = W[i] + w * (sumW[i] + kW[i]);
+        slot = 6;
+        return false;
+      }
+      case 9: {
+        const double w = (0.5 * h) / 6.0;
+        const double Br = B1[0] + w * (sum[0] + k[0]);
+        const double Bth = B1[1] + w * (sum[1] + k[1]);
+        const double Bph = B1[2] + w * (sum[4] + k[4]);
+        const double Bpr = B1[3] + w * (sum[2] + k[2]);
+        const double Bpth = B1[4] + w * (sum[3] + k[3]);
+        const double e0 = A[0] - Br, e1 = A[1] - Bth, e2 = A[2] - Bpr, e3 = A[3] - Bpth;
+        const double err = sqrt(((e0 * e0 + e1 * e1) + e2 * e2) + e3 * e3) / 15.0;
+        step_used = h;
+        ++attempts;
+        const int acc = doubling_update(err, f.tol, &h);
+        if (acc == 1) {
+          A[0] = r;
+          A[1] = th;
+          sp_ph = ph;
+          kp[0] = k1[0];
+          kp[1] = k1[1];
+          for (int i = 0; i < 8; ++i) {
+            Wprev[i] = W[i];
+            W[i] = B1W[i] + w * (sumW[i] + kW[i]);
+          }
+          r = Br;
+          th = Bth;
+          ph = Bph;
+          pr = Bpr;
+          pth = Bpth;
+          slot = 10;
+          return false;
+        }
+        int st;
+        if (reject_cap(h, &rejects, &st)) {
+          // trace_bundle returns BundleResult{} (ray_bundle.hpp:320)
+          o->steps = (uint32_t)it;
+          o->attempts = attempts;
+          set_result(o, kOutEscaped, st, 0.0, 1.0, 1.0, 0.0, 0.0, 0.0);
+          return true;
+        }
+        slot = 0;
+        return false;
+      }
+      default: {  // 10
+        for (int i = 0; i < 5; ++i) k1[i] = k[i];
+        for (int i = 0; i < 8; ++i) kW1[i] = kW[i];
+        const double sp_r = A[0], sp_th = A[1];
+        double best_alpha = 2.0;
+        int ev = kEvNone;
+        double disk_r = 0.0, disk_red = 1.0, disk_det = 1.0, disk_phi = 0.0;
+        bool skip = false;
+        const double q0 = sp_th - kHalfPi;
+        const double q1 = th - kHalfPi;
+        if (sign_change(q0, q1) || (dmin(fabs(q0), fabs(q1)) < 0.35)) {
+          double alpha = 0.0;
+          if (!first_event(sp_th, th, kp[1], k1[1], step_used, kHalfPi, &alpha)) {
+            skip = true;  // ray_bundle.hpp:352-356 `continue`
+          } else {
+            const double r_hit = hermite(sp_r, r, kp[0], k1[0], step_used, alpha);
+            if (r_hit >= f.r_in && r_hit <= f.r_out) {
+              const double J00 = Wprev[0] + alpha * (W[0] - Wprev[0]);
+              const double J01 = Wprev[1] + alpha * (W[1] - Wprev[1]);
+              const double J10 = Wprev[2] + alpha * (W[2] - Wprev[2]);
+              const double J11 = Wprev[3] + alpha * (W[3] - Wprev[3]);
+              double det = fabs(J00 * J11 - J01 * J10);
+              det = det < 1e-12 ? 1e-12 : det;
+              disk_r = r_hit;
+              disk_red = bundle_redshift(f.g, f.eq, r_hit, pt, pphi);
+              disk_det = det;
+              disk_phi = sp_ph + alpha * (ph - sp_ph);
+              best_alpha = alpha;
+              ev = kEvDisk;
+            }
+          }
+        }
+        if (!skip) {
+          horizon_escape(sp_r, r, f.rh_cut, f.r_esc, &best_alpha, &ev);
+          if (ev != kEvNone) {
+            o->steps = (uint32_t)it + 1;
+            o->attempts = attempts;
+            if (ev == kEvDisk) {
+              set_result(o, kOutDisk, kStEvent, disk_r, disk_red, disk_det, disk_phi, 0.0, 0.0);
+            } else if (ev == kEvHorizon) {
+              // BundleResult{}: the pixel reads as escaped toward (0, 0)
+              set_result(o, kOutEscaped, kStEvent, 0.0, 1.0, 1.0, 0.0, 0.0, 0.0);
+            } else {
+              const double th_esc = sp_th + best_alpha * (th - sp_th);
+              const double ph_esc = sp_ph + best_alpha * (ph - sp_ph);
+              set_result(o, kOutEscaped, kStEvent, 0.0, 1.0, 1.0, 0.0, th_esc, ph_esc);
+            }
+            return true;
+          }
+        }
+        ++it;
+        rejects = 0;
+        slot = 0;
+        if (it >= f.max_steps) {
+          o->steps = (uint32_t)it;
+          o->attempts = attempts;
+          set_result(o, kOutEscaped, kStStepCap, 0.0, 1.0, 1.0, 0.0, 0.0, 0.0);
+          return true;
+        }
+        return false;
+      }
+    }
+  }
+};
+
+}  // namespace kt

@@ -1,0 +1,748 @@
+// kt_physics.cuh -- FP64 physics of the geodesic path, host+device.
+//
+// The functions reproduce the reference renderer's floating-point operation
+// order exactly (the parity bar is bit equality with the reference's CPU
+// FP64 path); they are organised for the GPU:
+//   * the angular part of the BL inverse metric (one sincos) is shared by
+//     every evaluation at the same theta, so one RHS costs 3 sincos instead
+//     of the reference's 15 trig calls, with identical values;
+//   * frame constants (a^2, Xi^2, the observer's metric for the camera) are
+//     computed once on the host with the same code;
+//   * no function allocates or loops over unknown bounds.
+// Compile device code with --fmad=false and host code with
+// -ffp-contract=off: a fused multiply-add changes the rounding of the
+// reference's separate multiply and add.
+#pragma once
+
+#include <math.h>
+#include <stdint.h>
+
+#include "ktmath.h"
+
+#if defined(__CUDACC__)
+#define KT_HD __host__ __device__ __forceinline__
+#else
+#define KT_HD inline
+#endif
+
+namespace kt {
+
+constexpr double kPi = 3.14159265358979323846;  // M_PI
+constexpr double kHalfPi = kPi / 2.0;           // M_PI/2.0 (exact halving)
+
+// std::max / std::min / clamp semantics of the reference (NaN included).
+KT_HD double dmax(double a, double b) { return (a < b) ? b : a; }
+KT_HD double dmin(double a, double b) { return (b < a) ? b : a; }
+KT_HD double dclamp(double v, double lo, double hi) { return v < lo ? lo : v > hi ? hi : v; }
+KT_HD bool finite(double x) { return !ktm_isnan(x) && !ktm_isinf(x); }
+
+// KNdSMetric parameters plus products the reference recomputes inline.
+struct Metric {
+  double M, a, Q, L;
+  double a2;    // a*a
+  double fa2;   // 4.0*a2        (r_KS, knds_metric.hpp:154)
+  double Laa;   // (L*a)*a        (Delta_theta, Xi)
+  double xi2;   // Xi()*Xi()
+  double axi2;  // a*xi2
+  double twoM;  // 2.0*M
+  double Q2;    // Q*Q
+};
+
+KT_HD Metric make_metric(double M, double a, double Q, double L) {
+  Metric g;
+  g.M = M;
+  g.a = a;
+  g.Q = Q;
+  g.L = L;
+  g.a2 = a * a;
+  g.fa2 = 4.0 * g.a2;
+  g.Laa = (L * a) * a;
+  const double xi = 1.0 + g.Laa / 3.0;
+  g.xi2 = xi * xi;
+  g.axi2 = a * g.xi2;
+  g.twoM = 2.0 * M;
+  g.Q2 = Q * Q;
+  return g;
+}
+
+// ---------------------------------------------------------------- BL chart
+// knds_metric.hpp:45-132
+
+// theta-dependent factors: cos, sin^2, a^2 cos^2 (in Sigma), Delta_theta.
+struct Ang {
+  double ct, st2, Ath, dth;
+};
+
+KT_HD Ang bl_ang(const Metric& g, double th) {
+  double st, ct;
+  ktm_sincos(th, &st, &ct);
+  Ang A;
+  A.ct = ct;
+  A.st2 = st * st;
+  A.Ath = (g.a2 * ct) * ct;
+  A.dth = 1.0 + ((g.Laa * ct) * ct) / 3.0;
+  return A;
+}
+
+// Delta_r, knds_metric.hpp:51
+KT_HD double bl_delta_r(const Metric& g, double r, double r2a2) {
+  return ((r2a2 * (1.0 - ((g.L * r) * r) / 3.0)) - g.twoM * r) + g.Q2;
+}
+
+// Non-zero entries of g^{mu nu} (contravariant_BL, knds_metric.hpp:99-117).
+struct Inv {
+  double tt, tp, rr, hh, pp;  // g^tt, g^tphi, g^rr, g^thth, g^phiphi
+};
+
+KT_HD Inv bl_inv(const Metric& g, double r, const Ang& A) {
+  const double r_sq = r * r;
+  const double sig = r_sq + A.Ath;
+  const double r2a2 = r_sq + g.a2;
+  const double dr = bl_delta_r(g, r, r2a2);
+  const double dth = A.dth;
+  const double pre = (sig * dr) * dth;
+  Inv U;
+  U.tt = ((-g.xi2) * ((dth * r2a2) * r2a2 - ((dr * g.a) * g.a) * A.st2)) / pre;
+  U.tp = (g.axi2 * (dr - dth * r2a2)) / pre;
+  U.rr = dr / sig;
+  U.hh = dth / sig;
+  U.pp = (A.st2 > 1e-14) ? (g.xi2 * (dr - ((dth * g.a) * g.a) * A.st2)) / (pre * A.st2) : 0.0;
+  return U;
+}
+
+// hamiltonian, knds_metric.hpp:122-132
+KT_HD double bl_ham(const Inv& U, double pr, double pth, double pt, double pphi) {
+  return 0.5 * (((((U.tt * pt) * pt + ((2.0 * U.tp) * pt) * pphi) + (U.rr * pr) * pr) +
+                 (U.hh * pth) * pth) +
+                (U.pp * pphi) * pphi);
+}
+
+// Non-zero entries of g_{mu nu} (covariant_BL, knds_metric.hpp:71-88).
+struct Cov {
+  double tt, tp, rr, hh, pp;
+};
+
+KT_HD Cov bl_cov(const Metric& g, double r, const Ang& A) {
+  const double r_sq = r * r;
+  const double sig = r_sq + A.Ath;
+  const double r2a2 = r_sq + g.a2;
+  const double dr = bl_delta_r(g, r, r2a2);
+  const double dth = A.dth;
+  const double pre = sig * g.xi2;
+  Cov G;
+  G.tt = (-dr + ((dth * g.a) * g.a) * A.st2) / pre;
+  G.tp = ((g.a * A.st2) * (dr - dth * r2a2)) / pre;
+  G.rr = sig / dr;
+  G.hh = sig / dth;
+  G.pp = (A.st2 * ((dth * r2a2) * r2a2 - ((dr * g.a) * g.a) * A.st2)) / pre;
+  return G;
+}
+
+// Geodesic right-hand side (geodesic_rhs, geodesic.hpp:143-166) together with
+// dphi/dlambda (dphi_vel, geodesic.hpp:40-45): the reference evaluates
+// dphi_vel at the same (r, theta) as the RHS, so it is the same g^{mu nu}.
+// k = {dr, dtheta, dp_r, dp_theta, dphi}.
+KT_HD void bl_rhs(const Metric& g, double r, double th, double pr, double pth, double pt,
+                  double pphi, double k[5]) {
+  const Ang A0 = bl_ang(g, th);
+  const Inv U0 = bl_inv(g, r, A0);
+  k[0] = U0.rr * pr;
+  k[1] = U0.hh * pth;
+  k[4] = U0.tp * pt + U0.pp * pphi;
+  const double eps_r = 1e-5 * dmax(fabs(r), 0.01);
+  const double eps_th = 1e-6;
+  const double hp = bl_ham(bl_inv(g, r + eps_r, A0), pr, pth, pt, pphi);
+  const double hm = bl_ham(bl_inv(g, r - eps_r, A0), pr, pth, pt, pphi);
+  k[2] = -(hp - hm) / (2.0 * eps_r);
+  const double tp = bl_ham(bl_inv(g, r, bl_ang(g, th + eps_th)), pr, pth, pt, pphi);
+  const double tm = bl_ham(bl_inv(g, r, bl_ang(g, th - eps_th)), pr, pth, pt, pphi);
+  k[3] = -(tp - tm) / (2.0 * eps_th);
+}
+
+// keplerian_omega, knds_metric.hpp:354-363
+KT_HD double kepler_omega(const Metric& g, double r) {
+  const double s = (g.a < 0.0) ? 1.0 : -1.0;
+  const double Meff = (g.M - g.Q2 / (2.0 * r)) + (((g.L * g.a) * r) * r) / 3.0;
+  const double sq = sqrt(dmax(Meff, 0.0));
+  const double den = r * sqrt(r) + (s * g.a) * sq;
+  if (fabs(den) < 1e-14) return 0.0;
+  return (s * sq) / den;
+}
+
+// disk_redshift, main.cpp:329-341 (equatorial metric: Ang at pi/2 given).
+KT_HD double disk_redshift(const Metric& g, const Ang& eq, double r, double pt, double pphi) {
+  const double Om = kepler_omega(g, r);
+  const double b = (-pphi) / (-pt);
+  const Cov G = bl_cov(g, r, eq);
+  const double d2 = -((G.tt + (2.0 * G.tp) * Om) + (G.pp * Om) * Om);
+  if (d2 <= 0.0) return 1.0;
+  const double dv = fabs(1.0 - Om * b);
+  if (dv < 1e-8) return 20.0;
+  const double red = sqrt(d2) / dv;
+  return finite(red) ? red : 1.0;
+}
+
+// Bundle-mode redshift (ray_bundle.hpp:367-378): signed Doppler factor.
+KT_HD double bundle_redshift(const Metric& g, const Ang& eq, double r, double pt, double pphi) {
+  const double Om = kepler_omega(g, r);
+  const double b = (-pphi) / (-pt);
+  const Cov G = bl_cov(g, r, eq);
+  const double d2 = -((G.tt + (2.0 * G.tp) * Om) + (G.pp * Om) * Om);
+  const double dv = 1.0 - Om * b;
+  double red = (d2 > 0.0 && fabs(dv) > 1e-10) ? sqrt(d2) / dv : 1.0;
+  red = red < 0.0 ? 0.0 : red > 20.0 ? 20.0 : red;
+  return red;
+}
+
+// ------------------------------------------------------------------ events
+// geodesic.hpp:49-140
+
+KT_HD double clamp01(double x) {
+  if (x < 0.0) return 0.0;
+  if (x > 1.0) return 1.0;
+  return x;
+}
+
+KT_HD double hermite(double y0, double y1, double dy0, double dy1, double h, double alpha) {
+  alpha = clamp01(alpha);
+  const double a2 = alpha * alpha;
+  const double a3 = a2 * alpha;
+  const double h00 = (2.0 * a3 - 3.0 * a2) + 1.0;
+  const double h10 = (a3 - 2.0 * a2) + alpha;
+  const double h01 = -2.0 * a3 + 3.0 * a2;
+  const double h11 = a3 - a2;
+  return ((h00 * y0 + h10 * (h * dy0)) + h01 * y1) + h11 * (h * dy1);
+}
+
+KT_HD bool sign_change(double f0, double f1) {
+  return ((f0 <= 0.0 && f1 >= 0.0) || (f0 >= 0.0 && f1 <= 0.0));
+}
+
+// first_event_alpha_hermite with 8 bins x 8 bisections (geodesic.hpp:98-140).
+KT_HD bool first_event(double y0, double y1, double dy0, double dy1, double h, double target,
+                       double* alpha_out) {
+  const double f_eps = 1e-12;
+  double a0 = 0.0;
+  double f0 = y0 - target;
+  if (fabs(f0) <= f_eps) {
+    *alpha_out = 0.0;
+    return true;
+  }
+  for (int i = 1; i <= 8; ++i) {
+    const double a1 = (double)i / 8.0;
+    const double f1 = (i == 8) ? (y1 - target) : (hermite(y0, y1, dy0, dy1, h, a1) - target);
+    if (fabs(f1) <= f_eps) {
+      *alpha_out = a1;
+      return true;
+    }
+    if (sign_change(f0, f1)) {
+      double lo = a0, hi = a1;
+      for (int k = 0; k < 8; ++k) {
+        const double mid = 0.5 * (lo + hi);
+        const double fm = hermite(y0, y1, dy0, dy1, h, mid) - target;
+        if (sign_change(f0, fm))
+          hi = mid;
+        else
+          lo = mid;
+      }
+      *alpha_out = 0.5 * (lo + hi);
+      return true;
+    }
+    a0 = a1;
+    f0 = f1;
+  }
+  return false;
+}
+
+// ------------------------------------------------------------------ camera
+// camera.hpp:38-145.  The observer's metric is a frame constant.
+struct CamConst {
+  double r_obs, theta_obs, phi_obs, fov_h;
+  int W, H;
+  double half_wm1, half_hm1, span;  // 0.5*(W-1), 0.5*(H-1), (double)span
+  double offx, offy;
+  double gtt, gtphi, grr, gthth, gphph;  // g_{mu nu} at the observer
+  double Utt, Utp, Urr, Uhh, Upp;        // g^{mu nu} at the observer
+  double sqrt_grr, sqrt_gthth, inv_guard_grr, inv_guard_gthth, sqrt_gphph_guard;
+  double ut, ephi_p, ephi_t;
+  int tetrad_ok;
+  int pad0;
+};
+
+KT_HD CamConst make_camera(const Metric& g, double r_obs, double theta_obs, double phi_obs,
+                           double fov_h, int W, int H, double offx, double offy) {
+  CamConst c;
+  c.r_obs = r_obs;
+  c.theta_obs = theta_obs;
+  c.phi_obs = phi_obs;
+  c.fov_h = fov_h;
+  c.W = W;
+  c.H = H;
+  c.half_wm1 = 0.5 * (double)(W - 1);
+  c.half_hm1 = 0.5 * (double)(H - 1);
+  c.span = (double)((W > 1) ? (W - 1) : 1);
+  c.offx = offx;
+  c.offy = offy;
+  const Ang A = bl_ang(g, theta_obs);
+  const Cov G = bl_cov(g, r_obs, A);
+  const Inv U = bl_inv(g, r_obs, A);
+  c.gtt = G.tt;
+  c.gtphi = G.tp;
+  c.grr = G.rr;
+  c.gthth = G.hh;
+  c.gphph = G.pp;
+  c.Utt = U.tt;
+  c.Utp = U.tp;
+  c.Urr = U.rr;
+  c.Uhh = U.hh;
+  c.Upp = U.pp;
+  c.sqrt_grr = sqrt(fabs(G.rr));
+  c.sqrt_gthth = sqrt(fabs(G.hh));
+  c.inv_guard_grr = dmax(c.sqrt_grr, 1e-14);
+  c.inv_guard_gthth = dmax(c.sqrt_gthth, 1e-14);
+  c.sqrt_gphph_guard = sqrt(dmax(fabs(G.pp), 1e-14));
+  const double denom_phi = G.pp - (G.tp * G.tp) / G.tt;
+  c.tetrad_ok = (G.tt < -1e-14) && finite(denom_phi) && (denom_phi > 1e-14) &&
+                finite(c.sqrt_grr) && (c.sqrt_grr > 1e-14) && finite(c.sqrt_gthth) &&
+                (c.sqrt_gthth > 1e-14);
+  c.ut = 1.0 / sqrt(-G.tt);
+  c.ephi_p = 1.0 / sqrt(denom_phi);
+  c.ephi_t = ((-G.tp) / G.tt) * c.ephi_p;
+  c.pad0 = 0;
+  return c;
+}
+
+// pixel_ray's angles (camera.hpp:38-47).
+KT_HD void pixel_angles(const CamConst& c, int px, int py, double* alpha, double* beta) {
+  const double x = (double)px + c.offx;
+  const double y = (double)py + c.offy;
+  *alpha = (c.fov_h * (x - c.half_wm1)) / c.span;
+  *beta = (c.fov_h * (c.half_hm1 - y)) / c.span;
+}
+
+// GeodesicState (geodesic.hpp:33-37)
+struct Geo {
+  double r, th, ph, pr, pth, pt, pphi;
+};
+
+// angle_ray (camera.hpp:50-145)
+KT_HD Geo angle_ray(const CamConst& c, double alpha, double beta) {
+  double sa, ca, sb, cb;
+  ktm_sincos(alpha, &sa, &ca);
+  ktm_sincos(beta, &sb, &cb);
+  double pUt = 1.0;
+  double pUr = ((-ca) * cb) / c.inv_guard_grr;
+  double pUth = (-sb) / c.inv_guard_gthth;
+  double pUphi = ((-sa) * cb) / c.sqrt_gphph_guard;
+  if (c.tetrad_ok) {
+    const double n_r = (-ca) * cb;
+    const double n_th = -sb;
+    const double n_ph = (-sa) * cb;
+    pUt = c.ut + n_ph * c.ephi_t;
+    pUr = n_r / c.sqrt_grr;
+    pUth = n_th / c.sqrt_gthth;
+    pUphi = n_ph * c.ephi_p;
+  }
+  double pt = c.gtt * pUt + c.gtphi * pUphi;
+  const double pr = c.grr * pUr;
+  const double pth = c.gthth * pUth;
+  const double pphi = c.gtphi * pUt + c.gphph * pUphi;
+  const double A = c.Utt;
+  const double B = (2.0 * c.Utp) * pphi;
+  const double C = ((c.Urr * pr) * pr + (c.Uhh * pth) * pth) + (c.Upp * pphi) * pphi;
+  const double disc = B * B - (4.0 * A) * C;
+  if (disc >= 0.0 && fabs(A) > 1e-15) {
+    const double sq = sqrt(disc);
+    const double pt1 = (-B - sq) / (2.0 * A);
+    const double pt2 = (-B + sq) / (2.0 * A);
+    pt = (pt1 < 0.0) ? pt1 : pt2;
+    if (pt > 0.0) pt = dmin(pt1, pt2);
+  }
+  Geo s;
+  s.r = c.r_obs;
+  s.th = c.theta_obs;
+  s.ph = c.phi_obs;
+  s.pr = pr;
+  s.pth = pth;
+  s.pt = pt;
+  s.pphi = pphi;
+  return s;
+}
+
+// ---------------------------------------------------------------- KS chart
+// knds_metric.hpp:150-230 (ingoing, Lambda = 0), main.cpp:1306-1454
+
+KT_HD double r_ks(const Metric& g, double X, double Y, double Z) {
+  const double R2 = (X * X + Y * Y) + Z * Z;
+  const double b = R2 - g.a2;
+  return sqrt(0.5 * (b + sqrt(b * b + (g.fa2 * Z) * Z)));
+}
+
+// g^{ab} = eta^{ab} - H l^a l^b, all 16 entries in the reference's
+// evaluation order (the product (H l^a) l^b is not symmetric in rounding).
+KT_HD void ks_inv(const Metric& g, double X, double Y, double Z, double G[16]) {
+  const double r = r_ks(g, X, Y, Z);
+  const double r_sq = r * r;
+  const double rho2 = r_sq + ((g.a2 * Z) * Z) / r_sq;
+  const double H = (g.twoM * r - g.Q2) / rho2;
+  const double r2a2 = r_sq + g.a2;
+  const double lU[4] = {-1.0, (r * X + g.a * Y) / r2a2, (r * Y - g.a * X) / r2a2, Z / r};
+#pragma unroll
+  for (int mu = 0; mu < 4; ++mu) {
+    const double hl = H * lU[mu];
+#pragma unroll
+    for (int nu = 0; nu < 4; ++nu) {
+      const double eta = (mu != nu) ? 0.0 : (mu == 0 ? -1.0 : 1.0);
+      G[4 * mu + nu] = eta - hl * lU[nu];
+    }
+  }
+}
+
+KT_HD double ks_ham(const double G[16], const double p[4]) {
+  double H = 0.0;
+#pragma unroll
+  for (int mu = 0; mu < 4; ++mu)
+#pragma unroll
+    for (int nu = 0; nu < 4; ++nu) H += (G[4 * mu + nu] * p[mu]) * p[nu];
+  return 0.5 * H;
+}
+
+struct KSState {
+  double X, Y, Z, pX, pY, pZ, pT;
+};
+
+// geodesic_rhs_ks, main.cpp:1432-1454.  k = {dX, dY, dZ, dpX, dpY, dpZ}.
+KT_HD void ks_rhs(const Metric& g, double X, double Y, double Z, double pX, double pY, double pZ,
+                  double pT, double k[6]) {
+  double G[16];
+  ks_inv(g, X, Y, Z, G);
+  k[0] = ((G[4] * pT + G[5] * pX) + G[6] * pY) + G[7] * pZ;
+  k[1] = ((G[8] * pT + G[9] * pX) + G[10] * pY) + G[11] * pZ;
+  k[2] = ((G[12] * pT + G[13] * pX) + G[14] * pY) + G[15] * pZ;
+  const double p[4] = {pT, pX, pY, pZ};
+  const double eX = 1e-5 * (fabs(X) + 0.1);
+  const double eY = 1e-5 * (fabs(Y) + 0.1);
+  const double eZ = 1e-5 * (fabs(Z) + 0.1);
+  double Gp[16], Gm[16];
+  ks_inv(g, X + eX, Y, Z, Gp);
+  ks_inv(g, X - eX, Y, Z, Gm);
+  k[3] = -(ks_ham(Gp, p) - ks_ham(Gm, p)) / (2.0 * eX);
+  ks_inv(g, X, Y + eY, Z, Gp);
+  ks_inv(g, X, Y - eY, Z, Gm);
+  k[4] = -(ks_ham(Gp, p) - ks_ham(Gm, p)) / (2.0 * eY);
+  ks_inv(g, X, Y, Z + eZ, Gp);
+  ks_inv(g, X, Y, Z - eZ, Gm);
+  k[5] = -(ks_ham(Gp, p) - ks_ham(Gm, p)) / (2.0 * eZ);
+}
+
+// BL_to_KS_spatial (knds_metric.hpp:368-387) from precomputed sin/cos.
+KT_HD void bl_to_ks_sc(double r, double st, double ct, double sf, double cf, double a, double* X,
+                       double* Y, double* Z) {
+  *X = st * (r * cf - a * sf);
+  *Y = st * (r * sf + a * cf);
+  *Z = r * ct;
+}
+
+// KS_to_BL_spatial (knds_metric.hpp:390-411); the reference's first atan2
+// results are overwritten before use.
+KT_HD void ks_to_bl(const Metric& g, double X, double Y, double Z, double* r, double* th,
+                    double* ph) {
+  const double rr = r_ks(g, X, Y, Z);
+  *r = rr;
+  const double Zr = Z / rr;
+  *th = ktm_acos(Zr < -1.0 ? -1.0 : Zr > 1.0 ? 1.0 : Zr);
+  const double st_val = sqrt(dmax(1.0 - (Z * Z) / (rr * rr), 0.0));
+  const double r2a2 = rr * rr + g.a2;
+  if (st_val > 1e-10) {
+    const double cf = (X * rr + Y * g.a) / (st_val * r2a2);
+    const double sf = (Y * rr - X * g.a) / (st_val * r2a2);
+    *ph = ktm_atan2(sf, cf);
+  } else {
+    *ph = 0.0;
+  }
+}
+
+// jacobian_bl_to_ks, main.cpp:1348-1371: J[i][j] = d(X,Y,Z)_i / d(r,th,ph)_j.
+KT_HD void jacobian_bl_to_ks(double r, double th, double ph, double a, double J[3][3]) {
+  const double er = 1e-6 * (fabs(r) + 1.0);
+  const double eth = 1e-6;
+  const double eph = 1e-6;
+  double st, ct, sf, cf, st_p, ct_p, st_m, ct_m, sf_p, cf_p, sf_m, cf_m;
+  ktm_sincos(th, &st, &ct);
+  ktm_sincos(ph, &sf, &cf);
+  ktm_sincos(th + eth, &st_p, &ct_p);
+  ktm_sincos(th - eth, &st_m, &ct_m);
+  ktm_sincos(ph + eph, &sf_p, &cf_p);
+  ktm_sincos(ph - eph, &sf_m, &cf_m);
+  double p[6][3];
+  bl_to_ks_sc(r + er, st, ct, sf, cf, a, &p[0][0], &p[0][1], &p[0][2]);
+  bl_to_ks_sc(r - er, st, ct, sf, cf, a, &p[1][0], &p[1][1], &p[1][2]);
+  bl_to_ks_sc(r, st_p, ct_p, sf, cf, a, &p[2][0], &p[2][1], &p[2][2]);
+  bl_to_ks_sc(r, st_m, ct_m, sf, cf, a, &p[3][0], &p[3][1], &p[3][2]);
+  bl_to_ks_sc(r, st, ct, sf_p, cf_p, a, &p[4][0], &p[4][1], &p[4][2]);
+  bl_to_ks_sc(r, st, ct, sf_m, cf_m, a, &p[5][0], &p[5][1], &p[5][2]);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    J[i][0] = (p[0][i] - p[1][i]) / (2.0 * er);
+    J[i][1] = (p[2][i] - p[3][i]) / (2.0 * eth);
+    J[i][2] = (p[4][i] - p[5][i]) / (2.0 * eph);
+  }
+}
+
+// solve_3x3 with partial pivoting, main.cpp:1314-1346.
+KT_HD bool solve_3x3(const double Ain[3][3], const double bin[3], double x[3]) {
+  double A[3][4];
+  for (int i = 0; i < 3; ++i) {
+    for (int j = 0; j < 3; ++j) A[i][j] = Ain[i][j];
+    A[i][3] = bin[i];
+  }
+  for (int col = 0; col < 3; ++col) {
+    int piv = col;
+    double best = fabs(A[piv][col]);
+    for (int r = col + 1; r < 3; ++r) {
+      const double v = fabs(A[r][col]);
+      if (v > best) {
+        best = v;
+        piv = r;
+      }
+    }
+    if (best < 1e-14) return false;
+    if (piv != col) {
+      for (int k = col; k < 4; ++k) {
+        const double t = A[col][k];
+        A[col][k] = A[piv][k];
+        A[piv][k] = t;
+      }
+    }
+    const double inv = 1.0 / A[col][col];
+    for (int k = col; k < 4; ++k) A[col][k] *= inv;
+    for (int r = 0; r < 3; ++r) {
+      if (r == col) continue;
+      const double fr = A[r][col];
+      for (int k = col; k < 4; ++k) A[r][k] -= fr * A[col][k];
+    }
+  }
+  x[0] = A[0][3];
+  x[1] = A[1][3];
+  x[2] = A[2][3];
+  return true;
+}
+
+// init_ks_state, main.cpp:1404-1430.  Lambda = 0 is checked by the caller.
+KT_HD bool init_ks_state(const Metric& g, const Geo& sb, KSState* k) {
+  double st, ct, sf, cf;
+  ktm_sincos(sb.th, &st, &ct);
+  ktm_sincos(sb.ph, &sf, &cf);
+  bl_to_ks_sc(sb.r, st, ct, sf, cf, g.a, &k->X, &k->Y, &k->Z);
+  double J[3][3], A3[3][3];
+  jacobian_bl_to_ks(sb.r, sb.th, sb.ph, g.a, J);
+  for (int j = 0; j < 3; ++j)
+    for (int i = 0; i < 3; ++i) A3[j][i] = J[i][j];
+  const double b3[3] = {sb.pr, sb.pth, sb.pphi};
+  double x3[3];
+  if (!solve_3x3(A3, b3, x3)) return false;
+  k->pX = x3[0];
+  k->pY = x3[1];
+  k->pZ = x3[2];
+  double G[16];
+  ks_inv(g, k->X, k->Y, k->Z, G);
+  const double A = G[0];
+  const double B = 2.0 * ((G[1] * k->pX + G[2] * k->pY) + G[3] * k->pZ);
+  const double C = (((((G[5] * k->pX) * k->pX + (G[10] * k->pY) * k->pY) + (G[15] * k->pZ) * k->pZ) +
+                     ((2.0 * G[6]) * k->pX) * k->pY) +
+                    ((2.0 * G[7]) * k->pX) * k->pZ) +
+                   ((2.0 * G[11]) * k->pY) * k->pZ;
+  const double disc = B * B - (4.0 * A) * C;
+  if (disc < 0.0 || fabs(A) < 1e-15) return false;
+  const double sq = sqrt(disc);
+  const double pT1 = (-B - sq) / (2.0 * A);
+  const double pT2 = (-B + sq) / (2.0 * A);
+  k->pT = (pT1 < 0.0) ? pT1 : pT2;
+  if (k->pT > 0.0) k->pT = dmin(pT1, pT2);
+  return finite(k->pT);
+}
+
+// ks_covector_to_bl's p_phi component (main.cpp:1391-1402).
+KT_HD double ks_pphi_bl(double r, double th, double ph, double a, double pX, double pY,
+                        double pZ) {
+  double J[3][3];
+  jacobian_bl_to_ks(r, th, ph, a, J);
+  double s = 0.0;
+  s += J[0][2] * pX;
+  s += J[1][2] * pY;
+  s += J[2][2] * pZ;
+  return s;
+}
+
+// --------------------------------------------------------------- bundles
+// ray_bundle.hpp:56-214.  Hessian of H by central differences: the 33
+// evaluations fall on 9 distinct (r, theta) points, so 9 g^{mu nu}.
+KT_HD void bundle_hessian(const Metric& g, double r, double th, double pr, double pth, double pt,
+                          double pphi, const Ang& A0, double Hs[4][4]) {
+  const double e0 = 1e-5 * (fabs(r) + 0.1);
+  const double e1 = 1e-5;
+  const double e2 = 1e-5 * (fabs(pr) + 1e-3);
+  const double e3 = 1e-5 * (fabs(pth) + 1e-3);
+  const Ang Ap = bl_ang(g, th + e1);
+  const Ang Am = bl_ang(g, th + (-e1));
+  const double rp = r + e0, rm = r + (-e0);
+  const double prp = pr + e2, prm = pr + (-e2);
+  const double pthp = pth + e3, pthm = pth + (-e3);
+  // g^{mu nu} at (r + {0,+,-}e0, theta + {0,+,-}e1)
+  const Inv U00 = bl_inv(g, r, A0), Up0 = bl_inv(g, rp, A0), Um0 = bl_inv(g, rm, A0);
+  const Inv U0p = bl_inv(g, r, Ap), U0m = bl_inv(g, r, Am);
+  const Inv Upp = bl_inv(g, rp, Ap), Upm = bl_inv(g, rp, Am);
+  const Inv Ump = bl_inv(g, rm, Ap), Umm = bl_inv(g, rm, Am);
+  const double H0 = bl_ham(U00, pr, pth, pt, pphi);
+  const double e[4] = {e0, e1, e2, e3};
+  double vp[4], vm[4];
+  vp[0] = bl_ham(Up0, pr, pth, pt, pphi);
+  vm[0] = bl_ham(Um0, pr, pth, pt, pphi);
+  vp[1] = bl_ham(U0p, pr, pth, pt, pphi);
+  vm[1] = bl_ham(U0m, pr, pth, pt, pphi);
+  vp[2] = bl_ham(U00, prp, pth, pt, pphi);
+  vm[2] = bl_ham(U00, prm, pth, pt, pphi);
+  vp[3] = bl_ham(U00, pr, pthp, pt, pphi);
+  vm[3] = bl_ham(U00, pr, pthm, pt, pphi);
+#pragma unroll
+  for (int a = 0; a < 4; ++a) Hs[a][a] = ((vp[a] - 2.0 * H0) + vm[a]) / (e[a] * e[a]);
+  // cross(a,b) = (pp - pm - mp + mm) / (4 e_a e_b)
+#define KT_CROSS(a, b, pp, pm, mp, mm) \
+  Hs[a][b] = Hs[b][a] = ((((pp) - (pm)) - (mp)) + (mm)) / ((4.0 * e[a]) * e[b])
+  KT_CROSS(0, 1, bl_ham(Upp, pr, pth, pt, pphi), bl_ham(Upm, pr, pth, pt, pphi),
+           bl_ham(Ump, pr, pth, pt, pphi), bl_ham(Umm, pr, pth, pt, pphi));
+  KT_CROSS(0, 2, bl_ham(Up0, prp, pth, pt, pphi), bl_ham(Up0, prm, pth, pt, pphi),
+           bl_ham(Um0, prp, pth, pt, pphi), bl_ham(Um0, prm, pth, pt, pphi));
+  KT_CROSS(0, 3, bl_ham(Up0, pr, pthp, pt, pphi), bl_ham(Up0, pr, pthm, pt, pphi),
+           bl_ham(Um0, pr, pthp, pt, pphi), bl_ham(Um0, pr, pthm, pt, pphi));
+  KT_CROSS(1, 2, bl_ham(U0p, prp, pth, pt, pphi), bl_ham(U0p, prm, pth, pt, pphi),
+           bl_ham(U0m, prp, pth, pt, pphi), bl_ham(U0m, prm, pth, pt, pphi));
+  KT_CROSS(1, 3, bl_ham(U0p, pr, pthp, pt, pphi), bl_ham(U0p, pr, pthm, pt, pphi),
+           bl_ham(U0m, pr, pthp, pt, pphi), bl_ham(U0m, pr, pthm, pt, pphi));
+  KT_CROSS(2, 3, bl_ham(U00, prp, pthp, pt, pphi), bl_ham(U00, prp, pthm, pt, pphi),
+           bl_ham(U00, prm, pthp, pt, pphi), bl_ham(U00, prm, pthm, pt, pphi));
+#undef KT_CROSS
+}
+
+// bundle_rhs (ray_bundle.hpp:130-156): geodesic RHS (k[0..4] as bl_rhs) and
+// dW = J_s Hess W (dW[i][k], 4x2).
+KT_HD void bundle_rhs(const Metric& g, double r, double th, double pr, double pth, double pt,
+                      double pphi, const double W[8], double k[5], double dW[8]) {
+  bl_rhs(g, r, th, pr, pth, pt, pphi, k);
+  const Ang A0 = bl_ang(g, th);
+  double Hs[4][4];
+  bundle_hessian(g, r, th, pr, pth, pt, pphi, A0, Hs);
+  double M[4][4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    M[0][j] = Hs[2][j];
+    M[1][j] = Hs[3][j];
+    M[2][j] = -Hs[0][j];
+    M[3][j] = -Hs[1][j];
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      double s = 0.0;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) s += M[i][j] * W[2 * j + c];
+      dW[2 * i + c] = s;
+    }
+}
+
+// ------------------------------------------------------------------ colour
+// main.cpp:153-170, 1663-1687, 1799-1814
+
+// (uint8_t)(double) as g++ on x86-64 performs it: truncate toward zero to a
+// 32-bit integer and keep the low byte (values outside [0,256) occur when
+// the background interpolation extrapolates).
+KT_HD uint8_t to_u8(double v) { return (uint8_t)(int32_t)v; }
+
+KT_HD void blackbody(double T, double log10_50, uint8_t c[3]) {
+  T = dclamp(T, 800.0, 4e4);
+  const double t = ktm_log10(T / 800.0) / log10_50;
+  double R, G, B;
+  if (t < 0.25) {
+    R = 1;
+    G = (t / 0.25) * 0.4;
+    B = 0;
+  } else if (t < 0.5) {
+    const double f = (t - 0.25) / 0.25;
+    R = 1;
+    G = 0.4 + f * 0.4;
+    B = f * 0.3;
+  } else if (t < 0.75) {
+    const double f = (t - 0.5) / 0.25;
+    R = 1;
+    G = 0.8 + f * 0.2;
+    B = 0.3 + f * 0.5;
+  } else {
+    const double f = (t - 0.75) / 0.25;
+    R = 1 - f * 0.2;
+    G = 1;
+    B = 0.8 + f * 0.2;
+  }
+  c[0] = to_u8(dclamp(R, 0.0, 1.0) * 255);
+  c[1] = to_u8(dclamp(G, 0.0, 1.0) * 255);
+  c[2] = to_u8(dclamp(B, 0.0, 1.0) * 255);
+}
+
+KT_HD double page_thorne(double r, double r_isco) {
+  if (r <= r_isco) return 0.0;
+  const double x = sqrt(r_isco / r);
+  return (1.0 - x) / ((r * r) * r);
+}
+
+KT_HD double tonemap(double x, double exposure, double gamma) {
+  x = x * exposure;
+  x = x / (1.0 + x);
+  return ktm_pow(dclamp(x, 0.0, 1.0), 1.0 / gamma);
+}
+
+struct ColourConst {
+  double M, r_isco, exposure, gamma, temp_scale;
+  double log10_50;  // log10(4e4/800.0), a per-frame constant
+  double pt_peak;   // page_thorne(3 r_isco, r_isco)
+};
+
+KT_HD void disk_colour(const ColourConst& cc, double r, double red, double magnif, uint8_t out[3]) {
+  const double T = ((6500.0 * cc.temp_scale) * sqrt((6.0 * cc.M) / r)) * dclamp(red, 0.2, 5.0);
+  const double pt_norm = page_thorne(r, cc.r_isco);
+  double I = (cc.pt_peak > 0.0) ? pt_norm / cc.pt_peak : 0.0;
+  const double red_c = dclamp(red, 0.1, 10.0);
+  const double lift = 1.0 + 0.85 * dclamp(1.0 - red_c, 0.0, 1.0);
+  I *= ktm_pow(red_c, 4.0) * lift;
+  I *= dclamp(1.0 / magnif, 0.05, 5.0);
+  uint8_t c[3];
+  blackbody(T, cc.log10_50, c);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) out[k] = to_u8(tonemap((c[k] / 255.0) * I, cc.exposure, cc.gamma) * 255);
+}
+
+KT_HD int iclamp(int v, int lo, int hi) { return v < lo ? lo : v > hi ? hi : v; }
+
+// BackgroundImage::sample (main.cpp:153-170) on an RGB8 image.
+KT_HD void bg_sample(const uint8_t* px, int w, int h, double theta, double phi, uint8_t out[3]) {
+  double pw = fmod(phi, 2.0 * kPi);
+  if (pw < 0) pw += 2.0 * kPi;
+  const double uf = (pw / (2.0 * kPi)) * (double)(w - 1);
+  const double vf = (theta / kPi) * (double)(h - 1);
+  const int u0 = (int)uf, u1 = (w > 1) ? ((u0 + 1) % w) : 0;
+  const int v0 = (int)vf, v1 = (v0 + 1 < h - 1) ? v0 + 1 : h - 1;
+  const double fu = uf - u0, fv = vf - v0;
+  const int r0 = iclamp(v0, 0, h - 1) * w, r1 = iclamp(v1, 0, h - 1) * w;
+  const int c0 = iclamp(u0, 0, w - 1), c1 = iclamp(u1, 0, w - 1);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const double c00 = px[3 * (r0 + c0) + k];
+    const double c10 = px[3 * (r0 + c1) + k];
+    const double c01 = px[3 * (r1 + c0) + k];
+    const double c11 = px[3 * (r1 + c1) + k];
+    const double top = c00 + fu * (c10 - c00);
+    const double bot = c01 + fu * (c11 - c01);
+    out[k] = to_u8(top + fv * (bot - top));
+  }
+}
+
+}  // namespace kt

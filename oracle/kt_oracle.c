@@ -1421,3 +1421,61 @@ void orc_colorize(const kt_frame_desc* d, int64_t n, const uint8_t* outcome, con
     rgb[3 * i + 2] = c[2];
   }
 }
+
+/* ------------------------------------------------- known-answer helpers
+ * Entry points for the checks of tests/core_tests.cpp:18-96 in the
+ * reference (metric inverse, camera null condition, one adaptive step,
+ * Omega_K sign, KS radius recovery). */
+void orc_metric_bl(double M, double a, double Q, double L, double r, double th, double* cov16,
+                   double* con16) {
+  const Metric g = {M, a, Q, L};
+  double A[4][4], B[4][4];
+  m_cov_bl(&g, r, th, A);
+  m_con_bl(&g, r, th, B);
+  memcpy(cov16, A, sizeof A);
+  memcpy(con16, B, sizeof B);
+}
+
+double orc_hamiltonian(double M, double a, double Q, double L, const double* s7) {
+  const Metric g = {M, a, Q, L};
+  return m_ham(&g, s7[0], s7[1], s7[3], s7[4], s7[5], s7[6]);
+}
+
+void orc_angle_ray(double M, double a, double Q, double L, double r_obs, double th_deg,
+                   double ph_deg, double fov_deg, int W, int H, double alpha, double beta,
+                   double* s7) {
+  const Metric g = {M, a, Q, L};
+  Cam c = {r_obs, (th_deg * ORC_PI) / 180.0, (ph_deg * ORC_PI) / 180.0, (fov_deg * ORC_PI) / 180.0,
+           W, H};
+  const Geo s = cam_angle_ray(&c, alpha, beta, &g);
+  const double v[7] = {s.r, s.th, s.ph, s.pr, s.pth, s.pt, s.pphi};
+  memcpy(s7, v, sizeof v);
+}
+
+int orc_adaptive_step(double M, double a, double Q, double L, double* s7, double* h, int dopri5,
+                      double* fsal4, double tol) {
+  const Metric g = {M, a, Q, L};
+  Geo s = {s7[0], s7[1], s7[2], s7[3], s7[4], s7[5], s7[6]};
+  int acc;
+  if (dopri5) {
+    Vec4 f = {{fsal4[0], fsal4[1], fsal4[2], fsal4[3]}};
+    acc = dopri5_adaptive(&g, &s, h, &f, tol);
+    memcpy(fsal4, f.v, sizeof f.v);
+  } else {
+    acc = rk4_adaptive(&g, &s, h, tol);
+  }
+  const double v[7] = {s.r, s.th, s.ph, s.pr, s.pth, s.pt, s.pphi};
+  memcpy(s7, v, sizeof v);
+  return acc;
+}
+
+double orc_keplerian_omega(double M, double a, double Q, double L, double r) {
+  const Metric g = {M, a, Q, L};
+  return m_kepler(&g, r);
+}
+
+void orc_bl_to_ks(double r, double th, double ph, double a, double* xyz) {
+  m_bl_to_ks(r, th, ph, a, &xyz[0], &xyz[1], &xyz[2]);
+}
+
+double orc_r_ks(double X, double Y, double Z, double a) { return m_r_ks(X, Y, Z, a); }

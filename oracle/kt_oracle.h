@@ -39,6 +39,19 @@ void orc_colorize(const kt_frame_desc* d, int64_t n, const uint8_t* outcome, con
                   const double* phi_esc, double exposure, double gamma, double temp_scale,
                   const uint8_t* bg, int bg_w, int bg_h, uint8_t* rgb);
 
+/* Known-answer helpers (tests/core_tests.cpp of the reference). */
+void orc_metric_bl(double M, double a, double Q, double L, double r, double th, double* cov16,
+                   double* con16);
+double orc_hamiltonian(double M, double a, double Q, double L, const double* s7);
+void orc_angle_ray(double M, double a, double Q, double L, double r_obs, double th_deg,
+                   double ph_deg, double fov_deg, int W, int H, double alpha, double beta,
+                   double* s7);
+int orc_adaptive_step(double M, double a, double Q, double L, double* s7, double* h, int dopri5,
+                      double* fsal4, double tol);
+double orc_keplerian_omega(double M, double a, double Q, double L, double r);
+void orc_bl_to_ks(double r, double th, double ph, double a, double* xyz);
+double orc_r_ks(double X, double Y, double Z, double a);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,43 @@
+"""Access to tests/golden/frames.npz (fixtures made by make_golden.py from
+the reference renderer compiled here)."""
+import json
+import os
+
+import numpy as np
+
+from kerrtracecpp2_b200 import abi
+
+PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "frames.npz")
+FIELDS = ("outcome", "r", "redshift", "magnif", "phi_disk", "theta_esc", "phi_esc")
+_z = None
+
+
+def data():
+    global _z
+    if _z is None:
+        _z = dict(np.load(PATH))
+    return _z
+
+
+def cases():
+    return json.loads(bytes(data()["meta_json"]).decode())
+
+
+def desc(name):
+    return abi.frame_desc(**cases()[name])
+
+
+def result(name):
+    z = data()
+    return {k: z[f"{name}/{k}"] for k in FIELDS}
+
+
+def bits(a):
+    a = np.ascontiguousarray(a)
+    return a.view({1: np.uint8, 4: np.uint32, 8: np.uint64}[a.dtype.itemsize])
+
+
+def mismatches(got, want, fields=FIELDS):
+    """Per-field count of entries whose bits differ."""
+    return {k: int(np.sum(bits(np.asarray(got[k], dtype=want[k].dtype)) != bits(want[k])))
+            for k in fields}

@@ -1,0 +1,93 @@
+// kt_hostcheck.cpp -- TEST-ONLY host build of the GPU kernels' per-ray code.
+//
+// The kernels' state machines (kt_machines.cuh) are written for host and
+// device.  This file runs them on the CPU, one ray after another, exactly as
+// the persistent kernel does for one lane, so the CPU test suite can check
+// their arithmetic against the oracle without a GPU.  It is not a fallback:
+// the product library has no CPU tracing path and nothing outside tests/
+// loads this library.  Built by tests/conftest.py with -ffp-contract=off.
+#include <stdint.h>
+
+#include <string>
+
+#include "../include/kerrtrace.h"
+#include "../kerrtracecpp2_b200/csrc/kt_frame.h"
+
+using namespace kt;
+
+namespace {
+
+Geo camera_ray(const Frame& f, uint32_t pix) {
+  const int px = (int)(pix % (uint32_t)f.cam.W);
+  const int py = (int)(pix / (uint32_t)f.cam.W);
+  double al, be;
+  pixel_angles(f.cam, px, py, &al, &be);
+  return angle_ray(f.cam, al, be);
+}
+
+template <class M>
+RayResult run_bl(const Frame& f, const Geo& s) {
+  M m;
+  m.init(f, s);
+  RayResult res;
+  for (;;) {
+    double y[4], k[5];
+    m.input(y);
+    bl_rhs(f.g, y[0], y[1], y[2], y[3], m.pt, m.pphi, k);
+    if (m.consume(f, k, &res)) return res;
+  }
+}
+
+RayResult run_ray(const Frame& f, uint32_t pix) {
+  if (f.bundles) {
+    Bundle m;
+    m.init(f, (int)(pix % (uint32_t)f.cam.W), (int)(pix / (uint32_t)f.cam.W));
+    RayResult res;
+    for (;;) {
+      double y[4], yW[8], k[5], kW[8];
+      m.input(y, yW);
+      bundle_rhs(f.g, y[0], y[1], y[2], y[3], m.pt, m.pphi, yW, k, kW);
+      if (m.consume(f, k, kW, &res)) return res;
+    }
+  }
+  const Geo s = camera_ray(f, pix);
+  if (f.chart == KT_CHART_KS) {
+    KSRk4 m;
+    if (m.init(f, s)) {
+      RayResult res;
+      for (;;) {
+        double y[6], k[6];
+        m.input(y);
+        ks_rhs(f.g, y[0], y[1], y[2], y[3], y[4], y[5], m.pT, k);
+        if (m.consume(f, k, &res)) return res;
+      }
+    }
+  }
+  return f.intg == KT_DOPRI5 ? run_bl<BLDopri5>(f, s) : run_bl<BLRk4>(f, s);
+}
+
+}  // namespace
+
+extern "C" int hc_trace_pixels(const kt_frame_desc* d, int64_t n, const uint32_t* pix,
+                               uint8_t* outcome, double* r, double* red, double* magnif,
+                               double* phi_disk, double* th_esc, double* ph_esc, uint8_t* status,
+                               uint32_t* steps, uint32_t* attempts) {
+  Frame f;
+  std::string err;
+  if (prepare_frame(d, &f, nullptr, &err) != KT_OK) return 1;
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int64_t i = 0; i < n; ++i) {
+    const RayResult o = run_ray(f, pix[i]);
+    outcome[i] = (uint8_t)o.outcome;
+    r[i] = o.r;
+    red[i] = o.red;
+    magnif[i] = o.magnif;
+    phi_disk[i] = o.phi_disk;
+    th_esc[i] = o.th_esc;
+    ph_esc[i] = o.ph_esc;
+    if (status) status[i] = (uint8_t)o.status;
+    if (steps) steps[i] = o.steps;
+    if (attempts) attempts[i] = o.attempts;
+  }
+  return 0;
+}

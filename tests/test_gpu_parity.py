@@ -1,0 +1,138 @@
+"""GPU parity: the CUDA kernels against the reference renderer (golden
+fixtures made from its own code) and the oracle, bit for bit, through the
+C ABI.  Full-size frames are checked through properties that do not need
+the CPU to trace the whole frame: determinism, pixel-subset consistency,
+agreement on a strided sample, valid ranges."""
+import numpy as np
+import pytest
+
+import golden_lib as G
+import oracle_lib as O
+from kerrtracecpp2_b200 import abi
+
+pytestmark = pytest.mark.gpu
+
+
+def to_np(out):
+    return {k: (v.cpu().numpy() if v is not None else None) for k, v in out.items()}
+
+
+def trace(renderer, d):
+    import torch
+
+    out = renderer.trace(d)
+    torch.cuda.synchronize()
+    got = to_np(out)
+    got["steps"] = got["steps"].view(np.uint32)
+    got["attempts"] = got["attempts"].view(np.uint32)
+    return got
+
+
+@pytest.mark.parametrize("name", sorted(G.cases()))
+def test_kernel_matches_reference_fixtures(renderer, name):
+    got = trace(renderer, G.desc(name))
+    assert G.mismatches(got, G.result(name)) == {k: 0 for k in G.FIELDS}
+
+
+@pytest.mark.parametrize("kw", [
+    dict(chart=0, a=0.5, width=320, height=180, r_obs=40.0, theta_deg=80.0, fov_deg=45.0,
+         disk_out=12.0),                                                        # config 1, full
+    dict(chart=1, integrator=1, tol=1e-10, a=0.9, Q=0.3, Lambda=1e-4, r_obs=60.0, theta_deg=85.0,
+         fov_deg=30.0, disk_out=20.0, width=160, height=90),                    # config 2 at 1/64
+    dict(chart=1, bundles=1, a=0.998, theta_deg=60.0, width=96, height=54),    # config 3 at 1/400
+    dict(chart=0, a=0.7, Q=0.1, theta_deg=70.0, r_obs=50.0, disk_out=15.0, width=128,
+         height=128),                                                           # config 5 at 1/16
+], ids=["cfg1_full", "cfg2_160x90", "cfg3_96x54", "cfg5_128"])
+def test_kernel_matches_oracle_medium(renderer, kw):
+    d = abi.frame_desc(**kw)
+    got = trace(renderer, d)
+    want = O.trace_port(d, counters=True)
+    assert G.mismatches(got, want) == {k: 0 for k in G.FIELDS}
+    assert np.array_equal(got["steps"], want["steps"])
+    assert np.array_equal(got["attempts"], want["attempts"])
+
+
+def test_full_720p_frame_properties(renderer):
+    """Config 2 at full size: deterministic, valid ranges, and a strided
+    sample bit-identical to the oracle."""
+    d = abi.frame_desc(chart=1, integrator=1, tol=1e-10, a=0.9, Q=0.3, Lambda=1e-4, r_obs=60.0,
+                       theta_deg=85.0, fov_deg=30.0, disk_out=20.0, width=1280, height=720)
+    a = trace(renderer, d)
+    b = trace(renderer, d)
+    assert G.mismatches(a, b) == {k: 0 for k in G.FIELDS}
+    assert set(np.unique(a["outcome"])) <= {0, 1, 2}
+    disk = a["outcome"] == 1
+    assert disk.any() and (a["outcome"] == 2).any() and (a["outcome"] == 0).any()
+    assert np.all((a["redshift"][disk] >= 0) & (a["redshift"][disk] <= 20))
+    assert np.all((a["r"][disk] >= 1.0) & (a["r"][disk] <= 20.0))
+    pix = np.arange(0, d.width * d.height, 997, dtype=np.uint32)
+    want = O.trace_port(d, pix=pix)
+    sub = {k: a[k][pix] for k in G.FIELDS}
+    assert G.mismatches(sub, want) == {k: 0 for k in G.FIELDS}
+
+
+def test_trace_pixels_equals_frame(renderer):
+    import torch
+
+    d = G.desc("cfg5_ks")
+    full = trace(renderer, d)
+    pix = np.array([5, 0, 2303, 17, 1000, 1001, 999], np.uint32)
+    out = renderer.trace_pixels(d, torch.from_numpy(pix.astype(np.int32)).cuda())
+    torch.cuda.synchronize()
+    sub = to_np(out)
+    for k in G.FIELDS:
+        assert np.array_equal(G.bits(sub[k]), G.bits(full[k][pix])), k
+
+
+def test_trace_host_equals_device(renderer):
+    d = G.desc("cfg2_bl_dopri5")
+    dev = trace(renderer, d)
+    host = renderer.trace_host(d)
+    assert G.mismatches(host, dev) == {k: 0 for k in G.FIELDS}
+
+
+@pytest.mark.parametrize("name", ["cfg1_ks_rk4", "cfg2_bl_dopri5", "cfg3_bundles", "cfg5_ks",
+                                  "seven_by_three", "retrograde", "ads_lambda", "offsets"])
+def test_render_matches_reference_colour(renderer, name):
+    z = G.data()
+    d = G.desc(name)
+    rgb = renderer.render_host(d, bg=z["bg"])
+    assert np.array_equal(rgb.reshape(-1, 3), z[f"{name}/rgb"])
+
+
+def test_colorize_device_entry(renderer):
+    import torch
+
+    z = G.data()
+    d = G.desc("cfg1_ks_rk4")
+    out = renderer.trace(d)
+    bg = torch.from_numpy(np.ascontiguousarray(z["bg"])).cuda()
+    rgb = renderer.colorize(d, out, bg=bg)
+    torch.cuda.synchronize()
+    assert np.array_equal(rgb.cpu().numpy().reshape(-1, 3), z["cfg1_ks_rk4/rgb"])
+
+
+def test_status_and_counters(renderer):
+    got = trace(renderer, G.desc("step_cap"))
+    assert np.all(got["status"] == abi.KT_RAY_STEP_CAP) and np.all(got["steps"] == 7)
+    got = trace(renderer, G.desc("cfg1_ks_rk4"))
+    assert np.all(got["status"] == abi.KT_RAY_EVENT)
+
+
+def test_errors_are_status_codes(renderer):
+    import kerrtracecpp2_b200 as kt
+
+    with pytest.raises(kt.KerrTraceError) as e:
+        renderer.trace(abi.frame_desc(width=0, height=10))
+    assert e.value.status == abi.KT_ERR_INVALID_ARGUMENT
+    with pytest.raises(kt.KerrTraceError) as e:
+        renderer.trace(abi.frame_desc(width=8, height=8, solver_mode=abi.KT_SOLVER_SEMI_ANALYTIC))
+    assert e.value.status == abi.KT_ERR_UNSUPPORTED
+    # the context stays usable after an error
+    got = trace(renderer, G.desc("one_pixel"))
+    assert G.mismatches(got, G.result("one_pixel")) == {k: 0 for k in G.FIELDS}
+
+
+def test_fp64_peak_probe(renderer):
+    g = renderer.fp64_peak_gflops()
+    assert 1e3 < g < 1e6

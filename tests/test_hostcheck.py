@@ -1,0 +1,69 @@
+"""The GPU kernels' per-ray code (kt_machines.cuh / kt_physics.cuh) compiled
+for the host: bit-identical to the reference fixtures on every path.  This
+pins the kernels' operation order on the CPU; the GPU tests repeat the
+comparison with the device build."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import golden_lib as G
+import testlibs
+from kerrtracecpp2_b200.abi import FrameDesc, frame_desc
+
+P = ctypes.c_void_p
+
+
+@pytest.fixture(scope="module")
+def hc():
+    L = ctypes.CDLL(testlibs.HOSTCHECK)
+    L.hc_trace_pixels.argtypes = [ctypes.POINTER(FrameDesc), ctypes.c_int64, P] + [P] * 10
+    L.hc_trace_pixels.restype = ctypes.c_int
+    return L
+
+
+def run(hc, d, pix=None):
+    n = d.width * d.height
+    pix = np.arange(n, dtype=np.uint32) if pix is None else pix
+    n = len(pix)
+    o = {k: np.zeros(n, dt) for k, dt in [("outcome", np.uint8), ("r", "f8"), ("redshift", "f8"),
+                                           ("magnif", "f8"), ("phi_disk", "f8"), ("theta_esc", "f8"),
+                                           ("phi_esc", "f8"), ("status", np.uint8),
+                                           ("steps", np.uint32), ("attempts", np.uint32)]}
+    keys = ["outcome", "r", "redshift", "magnif", "phi_disk", "theta_esc", "phi_esc", "status",
+            "steps", "attempts"]
+    assert hc.hc_trace_pixels(ctypes.byref(d), n, pix.ctypes.data_as(P),
+                              *[o[k].ctypes.data_as(P) for k in keys]) == 0
+    return o
+
+
+@pytest.mark.parametrize("name", sorted(G.cases()))
+def test_kernel_code_matches_reference(hc, name):
+    got = run(hc, G.desc(name))
+    assert G.mismatches(got, G.result(name)) == {k: 0 for k in G.FIELDS}
+
+
+def test_step_counters_match_oracle(hc):
+    import oracle_lib as O
+
+    d = G.desc("cfg2_bl_dopri5")
+    got = run(hc, d)
+    want = O.trace_port(d, counters=True)
+    assert np.array_equal(got["steps"], want["steps"])
+    assert np.array_equal(got["attempts"], want["attempts"])
+
+
+def test_status_codes(hc):
+    got = run(hc, G.desc("step_cap"))
+    assert np.all(got["status"] == 1) and np.all(got["steps"] == 7)
+    got = run(hc, G.desc("cfg1_ks_rk4"))
+    assert np.all(got["status"] == 0)
+
+
+def test_pixel_subset_equals_frame(hc):
+    d = G.desc("cfg5_ks")
+    full = run(hc, d)
+    pix = np.array([0, 7, 100, 1151, 2303, 5], np.uint32)
+    sub = run(hc, d, pix)
+    for k in G.FIELDS:
+        assert np.array_equal(G.bits(sub[k]), G.bits(full[k][pix]))
