@@ -164,6 +164,14 @@ kt_status kt_colorize(kt_context* ctx, const kt_frame_desc* desc,
                       const uint8_t* bg_rgb, int32_t bg_w, int32_t bg_h,
                       uint8_t* rgb_out, void* stream);
 
+/* colorize_buffer (main.cpp:1817) on host buffers: the per-pixel records of
+ * a width x height frame (e.g. read from a .kgeo file), black-hole mass M and
+ * the ISCO radius recorded with them; RGB8 out (width*height*3 bytes). */
+kt_status kt_colorize_host(kt_context* ctx, const kt_geo_soa* geo_host, int32_t width,
+                           int32_t height, double M, double r_isco,
+                           const kt_color_params* cp, const uint8_t* bg_rgb_host,
+                           int32_t bg_w, int32_t bg_h, uint8_t* rgb_out_host);
+
 /* render_image equivalent: trace + colorize, host buffers in and out. */
 kt_status kt_render_host(kt_context* ctx, const kt_frame_desc* desc,
                          const kt_color_params* cp, const uint8_t* bg_rgb_host,

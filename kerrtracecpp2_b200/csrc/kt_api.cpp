@@ -394,6 +394,63 @@ kt_status kt_render_host(kt_context* ctx, const kt_frame_desc* desc, const kt_co
   return KT_OK;
 }
 
+kt_status kt_colorize_host(kt_context* ctx, const kt_geo_soa* g, int32_t width, int32_t height,
+                           double M, double r_isco, const kt_color_params* cp,
+                           const uint8_t* bg_rgb_host, int32_t bg_w, int32_t bg_h,
+                           uint8_t* rgb_out_host) {
+  if (!ctx) return KT_ERR_INVALID_ARGUMENT;
+  if (!g || !g->outcome || !g->r || !g->redshift || !g->magnif || !g->theta_esc || !g->phi_esc ||
+      !cp || !rgb_out_host)
+    return fail(ctx, KT_ERR_INVALID_ARGUMENT, "kt_colorize_host: NULL pointer");
+  if (width < 1 || height < 1 || (int64_t)width * height > 0x7fffffff)
+    return fail(ctx, KT_ERR_INVALID_ARGUMENT, "kt_colorize_host: bad frame size");
+  if (bg_rgb_host && (bg_w < 1 || bg_h < 1))
+    return fail(ctx, KT_ERR_INVALID_ARGUMENT, "kt_colorize_host: background size must be >= 1");
+  if (cp->palette != 0) return fail(ctx, KT_ERR_UNSUPPORTED, "only the blackbody palette is implemented");
+  DeviceGuard guard(ctx->device);
+  const size_t n = (size_t)width * (size_t)height;
+  const size_t need = n * (5 * 8 + 1 + 3) + 256;
+  kt_status r = ensure(ctx, (void**)&ctx->d_stage, &ctx->stage_cap, need, "staging buffer");
+  if (r != KT_OK) return r;
+  unsigned char* p = ctx->d_stage;
+  double* d_r = (double*)p; p += 8 * n;
+  double* d_red = (double*)p; p += 8 * n;
+  double* d_mag = (double*)p; p += 8 * n;
+  double* d_th = (double*)p; p += 8 * n;
+  double* d_ph = (double*)p; p += 8 * n;
+  uint8_t* d_out = p; p += n;
+  uint8_t* d_rgb = p;
+  const struct { void* dst; const void* src; size_t bytes; } cps[] = {
+      {d_r, g->r, 8 * n}, {d_red, g->redshift, 8 * n}, {d_mag, g->magnif, 8 * n},
+      {d_th, g->theta_esc, 8 * n}, {d_ph, g->phi_esc, 8 * n}, {d_out, g->outcome, n}};
+  for (const auto& c : cps)
+    KT_CUDA(ctx, cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyHostToDevice, ctx->stream), "copy in");
+  const uint8_t* d_bg = nullptr;
+  if (bg_rgb_host) {
+    const size_t bb = (size_t)bg_w * (size_t)bg_h * 3;
+    r = ensure(ctx, (void**)&ctx->d_bg, &ctx->bg_cap, bb, "background buffer");
+    if (r != KT_OK) return r;
+    KT_CUDA(ctx, cudaMemcpyAsync(ctx->d_bg, bg_rgb_host, bb, cudaMemcpyHostToDevice, ctx->stream),
+            "copy background");
+    d_bg = ctx->d_bg;
+  }
+  kt::ColourConst cc;
+  cc.M = M;
+  cc.r_isco = r_isco;
+  cc.exposure = cp->exposure;
+  cc.gamma = cp->gamma;
+  cc.temp_scale = cp->temp_scale;
+  cc.log10_50 = ktm_log10(4e4 / 800.0);
+  cc.pt_peak = kt::page_thorne(3.0 * r_isco, r_isco);
+  KT_CUDA(ctx, kt::launch_colorize(cc, (int64_t)n, d_out, d_r, d_red, d_mag, d_th, d_ph, d_bg, bg_w,
+                                   bg_h, d_rgb, ctx->stream),
+          "colorize kernel launch");
+  KT_CUDA(ctx, cudaMemcpyAsync(rgb_out_host, d_rgb, 3 * n, cudaMemcpyDeviceToHost, ctx->stream),
+          "copy image to host");
+  KT_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "colorize");
+  return KT_OK;
+}
+
 kt_status kt_measure_fp64_peak(kt_context* ctx, double* gflops) {
   if (!ctx || !gflops) return KT_ERR_INVALID_ARGUMENT;
   DeviceGuard g(ctx->device);

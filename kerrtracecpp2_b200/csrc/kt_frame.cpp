@@ -245,7 +245,7 @@ ColourConst make_colour(const Frame& f, const kt_color_params& cp) {
   cc.exposure = cp.exposure;
   cc.gamma = cp.gamma;
   cc.temp_scale = cp.temp_scale;
-  cc.log10_50 = ktm_log10(4e4 / 800.0);
+  cc.log10_50 = ktm_log10(4e4 / 800.0);  // blackbody's log10(4e4/800.0), main.cpp:1665
   cc.pt_peak = page_thorne(3.0 * f.r_in, f.r_in);
   return cc;
 }
