@@ -42,8 +42,9 @@ struct Fallback {
 enum Mode : int { kModeBLRk4 = 0, kModeBLDopri5 = 1, kModeKSRk4 = 2, kModeBundle = 3, kNumModes = 4 };
 
 struct LaunchShape {
-  int block;   // threads per block
-  int grid;    // persistent blocks
+  int block;    // threads per block
+  int grid;     // persistent blocks
+  size_t smem;  // dynamic shared memory per block (ray machines)
 };
 
 // Occupancy-derived persistent grid for one mode (cached per device).

@@ -1,12 +1,12 @@
 // kt_kernels.cu -- persistent geodesic-tracing kernels for sm_100a.
 //
-// One CUDA thread carries one ray at a time through a per-ray state machine
-// (kt_machines.cuh).  Each loop iteration every active lane evaluates one
-// Hamiltonian right-hand side at its own stage, then does the cheap
-// bookkeeping; a lane whose ray finished takes the next ray from a device
-// queue (one atomicAdd per warp for all its idle lanes).  Rays differ in
-// length by 3-10x, so refilling per lane keeps the FP64 pipes busy until the
-// queue runs dry; the grid is sized to the resident capacity of the GPU
+// One CUDA thread carries one ray at a time through a per-ray machine
+// (kt_machines.cuh); the 32 rays of a warp advance through the slots of an
+// adaptive attempt in lockstep, one Hamiltonian right-hand side per slot.
+// At every attempt boundary the lanes whose rays finished take new rays from
+// a device queue (one atomicAdd per warp for all its idle lanes).  Rays
+// differ in length by 3-50x, so refilling keeps the FP64 pipes busy until
+// the queue runs dry; the grid is sized to the resident capacity of the GPU
 // (persistent kernel).  State lives in registers; results go out as SoA.
 //
 // The kernels do no waiting on other threads: the only inter-thread
@@ -33,7 +33,7 @@ __device__ __forceinline__ void write_result(const OutSoA& o, uint32_t s, const 
   if (o.attempts) o.attempts[s] = r.attempts;
 }
 
-// ---- per-mode start (new ray) and step (one RHS) -------------------------
+// ---- per-mode start (new ray) and one slot (one RHS) ---------------------
 
 __device__ __forceinline__ Geo camera_ray(const Frame& f, uint32_t pix) {
   const int px = (int)(pix % (uint32_t)f.cam.W);
@@ -43,74 +43,111 @@ __device__ __forceinline__ Geo camera_ray(const Frame& f, uint32_t pix) {
   return angle_ray(f.cam, al, be);
 }
 
+// Each mode keeps its ray machine in shared memory (one record per thread,
+// record size an odd number of 8-byte words so a warp's accesses spread over
+// the banks): the machine is touched only between RHS evaluations, so the
+// registers are left to the RHS working set and more warps fit per SM.
+template <class M>
+struct alignas(8) SmemRecord {
+  M m;
+  double pad[((sizeof(M) + 7) / 8) % 2 == 0 ? 1 : 2];
+};
+
 struct ModeBLRk4 {
-  BLRk4 m;
+  using Machine = BLRk4;
+  static constexpr int kSlots = BLRk4::kSlots;
+  BLRk4* m;
+  __device__ __forceinline__ bool needs_k1() const { return m->needs_k1(); }
   __device__ __forceinline__ bool start(const Frame& f, uint32_t pix, uint32_t, const Fallback&) {
-    m.init(f, camera_ray(f, pix));
+    m->init(f, camera_ray(f, pix));
     return true;
   }
-  __device__ __forceinline__ bool step(const Frame& f, RayResult* res) {
+  __device__ __forceinline__ bool slot(const Frame& f, int s, RayResult* res) {
     double y[4], k[5];
-    m.input(y);
-    bl_rhs(f.g, y[0], y[1], y[2], y[3], m.pt, m.pphi, k);
-    return m.consume(f, k, res);
+    m->input(s, y);
+    bl_rhs(f.g, y[0], y[1], y[2], y[3], m->pt, m->pphi, k);
+    return m->consume(f, s, k, res);
   }
 };
 
 struct ModeBLDopri5 {
-  BLDopri5 m;
+  using Machine = BLDopri5;
+  static constexpr int kSlots = BLDopri5::kSlots;
+  BLDopri5* m;
+  __device__ __forceinline__ bool needs_k1() const { return m->needs_k1(); }
   __device__ __forceinline__ bool start(const Frame& f, uint32_t pix, uint32_t, const Fallback&) {
-    m.init(f, camera_ray(f, pix));
+    m->init(f, camera_ray(f, pix));
     return true;
   }
-  __device__ __forceinline__ bool step(const Frame& f, RayResult* res) {
+  __device__ __forceinline__ bool slot(const Frame& f, int s, RayResult* res) {
     double y[4], k[5];
-    m.input(y);
-    bl_rhs(f.g, y[0], y[1], y[2], y[3], m.pt, m.pphi, k);
-    return m.consume(f, k, res);
+    m->input(s, y);
+    bl_rhs(f.g, y[0], y[1], y[2], y[3], m->pt, m->pphi, k);
+    return m->consume(f, s, k, res);
   }
 };
 
 struct ModeKSRk4 {
-  KSRk4 m;
-  __device__ __forceinline__ bool start(const Frame& f, uint32_t pix, uint32_t slot,
+  using Machine = KSRk4;
+  static constexpr int kSlots = KSRk4::kSlots;
+  KSRk4* m;
+  __device__ __forceinline__ bool needs_k1() const { return m->needs_k1(); }
+  __device__ __forceinline__ bool start(const Frame& f, uint32_t pix, uint32_t out_slot,
                                         const Fallback& fb) {
-    if (m.init(f, camera_ray(f, pix))) return true;
+    if (m->init(f, camera_ray(f, pix))) return true;
     // init_ks_state failed: the ray is traced in the BL chart by a second
     // launch over the fallback list.
     const uint32_t i = atomicAdd(fb.count, 1u);
     fb.pix[i] = pix;
-    fb.slot[i] = slot;
+    fb.slot[i] = out_slot;
     return false;
   }
-  __device__ __forceinline__ bool step(const Frame& f, RayResult* res) {
+  __device__ __forceinline__ bool slot(const Frame& f, int s, RayResult* res) {
     double y[6], k[6];
-    m.input(y);
-    ks_rhs(f.g, y[0], y[1], y[2], y[3], y[4], y[5], m.pT, k);
-    return m.consume(f, k, res);
+    m->input(s, y);
+    ks_rhs(f.g, y[0], y[1], y[2], y[3], y[4], y[5], m->pT, k);
+    return m->consume(f, s, k, res);
   }
 };
 
 struct ModeBundle {
-  Bundle m;
+  using Machine = Bundle;
+  static constexpr int kSlots = Bundle::kSlots;
+  Bundle* m;
+  __device__ __forceinline__ bool needs_k1() const { return m->needs_k1(); }
   __device__ __forceinline__ bool start(const Frame& f, uint32_t pix, uint32_t, const Fallback&) {
-    m.init(f, (int)(pix % (uint32_t)f.cam.W), (int)(pix / (uint32_t)f.cam.W));
+    m->init(f, (int)(pix % (uint32_t)f.cam.W), (int)(pix / (uint32_t)f.cam.W));
     return true;
   }
-  __device__ __forceinline__ bool step(const Frame& f, RayResult* res) {
+  __device__ __forceinline__ bool slot(const Frame& f, int s, RayResult* res) {
     double y[4], yW[8], k[5], kW[8];
-    m.input(y, yW);
-    bundle_rhs(f.g, y[0], y[1], y[2], y[3], m.pt, m.pphi, yW, k, kW);
-    return m.consume(f, k, kW, res);
+    m->input(s, y, yW);
+    bundle_rhs(f.g, y[0], y[1], y[2], y[3], m->pt, m->pphi, yW, k, kW);
+    return m->consume(f, s, k, kW, res);
   }
 };
 
+template <class ModeT>
+constexpr size_t smem_bytes(int block) {
+  return sizeof(SmemRecord<typename ModeT::Machine>) * (size_t)block;
+}
+
 // ---- the persistent loop ---------------------------------------------------
+// One iteration of the outer loop is one adaptive attempt for every ray of
+// the warp.  At its start, idle lanes take new rays from the queue (one
+// atomicAdd per warp).  Slot -1 runs only if some lane needs it (new rays,
+// f at the end of an accepted step); slots 0..kSlots-1 run for every active
+// lane.  All lanes of the warp see the same slot index, so the bookkeeping
+// after each RHS runs converged; a lane whose ray ends mid-attempt idles to
+// the end of the attempt.
 
 template <class ModeT>
 __global__ void __launch_bounds__(kBlock) k_trace(const Frame f, const OutSoA out, const RayList rl,
                                                   uint32_t* __restrict__ queue, const Fallback fb) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  using Rec = SmemRecord<typename ModeT::Machine>;
   ModeT mode;
+  mode.m = &reinterpret_cast<Rec*>(smem)[threadIdx.x].m;
   bool active = false;
   uint32_t out_slot = 0;
   const uint32_t n = rl.n_dev ? *rl.n_dev : rl.n;
@@ -136,16 +173,20 @@ __global__ void __launch_bounds__(kBlock) k_trace(const Frame f, const OutSoA ou
         }
       }
     }
-    const bool any = __any_sync(kFull, active);
-    if (!any) {
+    if (!__any_sync(kFull, active)) {
       if (exhausted) break;
       continue;
     }
-    if (active) {
-      RayResult res;
-      if (mode.step(f, &res)) {
-        write_result(out, out_slot, res);
-        active = false;
+    KT_ROLLED
+    for (int s = -1; s < ModeT::kSlots; ++s) {
+      const bool part = active && (s >= 0 || mode.needs_k1());
+      if (s < 0 && !__any_sync(kFull, part)) continue;
+      if (part) {
+        RayResult res;
+        if (mode.slot(f, s, &res)) {
+          write_result(out, out_slot, res);
+          active = false;
+        }
       }
     }
   }
@@ -156,11 +197,15 @@ static cudaError_t shape_for(int device, LaunchShape* shape) {
   int sms = 0, per_sm = 0;
   cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   if (e != cudaSuccess) return e;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace<ModeT>, kBlock, 0);
+  const size_t smem = smem_bytes<ModeT>(kBlock);
+  e = cudaFuncSetAttribute(k_trace<ModeT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace<ModeT>, kBlock, smem);
   if (e != cudaSuccess) return e;
   if (per_sm < 1) per_sm = 1;
   shape->block = kBlock;
   shape->grid = sms * per_sm;
+  shape->smem = smem;
   return cudaSuccess;
 }
 
@@ -178,10 +223,10 @@ cudaError_t launch_trace(Mode mode, const Frame& f, const OutSoA& out, const Ray
                          uint32_t* queue, const Fallback& fb, const LaunchShape& s,
                          cudaStream_t stream) {
   switch (mode) {
-    case kModeBLRk4: k_trace<ModeBLRk4><<<s.grid, s.block, 0, stream>>>(f, out, rl, queue, fb); break;
-    case kModeBLDopri5: k_trace<ModeBLDopri5><<<s.grid, s.block, 0, stream>>>(f, out, rl, queue, fb); break;
-    case kModeKSRk4: k_trace<ModeKSRk4><<<s.grid, s.block, 0, stream>>>(f, out, rl, queue, fb); break;
-    case kModeBundle: k_trace<ModeBundle><<<s.grid, s.block, 0, stream>>>(f, out, rl, queue, fb); break;
+    case kModeBLRk4: k_trace<ModeBLRk4><<<s.grid, s.block, s.smem, stream>>>(f, out, rl, queue, fb); break;
+    case kModeBLDopri5: k_trace<ModeBLDopri5><<<s.grid, s.block, s.smem, stream>>>(f, out, rl, queue, fb); break;
+    case kModeKSRk4: k_trace<ModeKSRk4><<<s.grid, s.block, s.smem, stream>>>(f, out, rl, queue, fb); break;
+    case kModeBundle: k_trace<ModeBundle><<<s.grid, s.block, s.smem, stream>>>(f, out, rl, queue, fb); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();

@@ -1,13 +1,16 @@
-// kt_machines.cuh -- per-ray integrators as "one RHS per step" state machines.
+// kt_machines.cuh -- per-ray integrators as "one RHS per slot" machines.
 //
-// Each machine advances one ray by exactly one right-hand-side evaluation
-// per call: input() gives the point at which the next RHS is needed,
-// consume() takes the RHS there and does the bookkeeping (stage sums, error
-// control, accept/reject, events, termination).  The persistent kernel runs
-// input -> RHS -> consume in a loop, so the heavy RHS code appears once in
-// the kernel, every lane evaluates one RHS per iteration whatever stage its
-// ray is in, and a lane whose ray finished is refilled from the ray queue
-// on the next iteration.
+// An adaptive attempt is a fixed sequence of kSlots right-hand-side
+// evaluations (slots 0..kSlots-1).  input(slot) gives the point at which the
+// slot's RHS is needed, consume(slot) takes the RHS there and does the
+// bookkeeping (stage sums; after the last slot: error control,
+// accept/reject, events, termination).  Slot -1 is an extra RHS a ray needs
+// only sometimes: f(s) of a new ray, and for step doubling f at the end of
+// an accepted step (the next attempt's first stage and the event test).
+// The persistent kernel runs all lanes of a warp through the same slot
+// sequence together, so the bookkeeping after each slot executes converged
+// and the kernel holds a single copy of the RHS; rays that finished are
+// replaced at the next attempt boundary.
 //
 // Arithmetic and control flow follow the reference renderer:
 //   BL  RK4 step doubling : trace_single + rk4_adaptive (main.cpp:343-434,
@@ -129,8 +132,9 @@ struct BLBase {
   double h;                             // dlam
   double k1[5];                         // f(s) = {dr, dth, dpr, dpth, dphi}
   double step_used;
-  int slot, it, rejects;
+  int it, rejects;
   uint32_t attempts;
+  bool need_k1;
 
   KT_HD void init_state(const Frame& f, const Geo& s) {
     r = s.r;
@@ -142,11 +146,13 @@ struct BLBase {
     pphi = s.pphi;
     h = f.dlam0;
     step_used = h;
-    slot = -1;
     it = 0;
     rejects = 0;
     attempts = 0;
+    need_k1 = true;
   }
+
+  KT_HD bool needs_k1() const { return need_k1; }
 
   // Events of trace_single (main.cpp:364-433) for the accepted step
   // (sp_*) -> (current state), with f at both ends.  Returns true when the
@@ -200,7 +206,6 @@ struct BLBase {
   KT_HD bool next_step(const Frame& f, RayResult* o) {
     ++it;
     rejects = 0;
-    slot = 0;
     if (it >= f.max_steps) {
       stop_here(kStStepCap, (uint32_t)it, o);
       return true;
@@ -209,24 +214,34 @@ struct BLBase {
   }
 };
 
-// RK4 step doubling.  Slots per attempt (h = step, hb = h/2):
-//   0..2  path A  (one step h from s):     f(s + c k_prev), c = h/2, h/2, h
-//   3..5  path B1 (half step from s):      c = hb/2, hb/2, hb
-//   6     path B2 first stage:             f(B1)
-//   7..9  path B2 (half step from B1):     c = hb/2, hb/2, hb
-//   10    after acceptance:                f(B) = next k1 and the event RHS
-// slot -1 computes k1 = f(s) of a new ray.
+// Stage coefficient and base of step-doubling slots 0..9 (h = step,
+// hb = h/2): path A (0-2) = one step h from s, path B1 (3-5) = half step
+// from s, path B2 (6-9) = half step from B1 (slot 6 is its first stage).
+// Returns the multiplier c of the previous stage's k in y = base + c k.
+KT_HD double doubling_coeff(int slot, double h) {
+  const double hb = 0.5 * h;
+  if (slot < 3) return (slot == 2) ? h : 0.5 * h;
+  if (slot < 6) return (slot == 5) ? hb : 0.5 * hb;
+  return (slot == 9) ? hb : 0.5 * hb;
+}
+
+// RK4 step doubling (rk4_adaptive, geodesic.hpp:204-257), kSlots = 10.
 struct BLRk4 : BLBase {
+  static constexpr int kSlots = 10;
   double sum[5];
   double kp[4];
   double A[4];   // path A result (r, th, pr, pth); after acceptance: s_prev
   double B1[5];  // r, th, ph, pr, pth
   double sp_ph;
+  bool pending;  // accepted step waiting for f(s_new) and its events
 
-  KT_HD void init(const Frame& f, const Geo& s) { init_state(f, s); }
+  KT_HD void init(const Frame& f, const Geo& s) {
+    init_state(f, s);
+    pending = false;
+  }
 
-  KT_HD void input(double y[4]) const {
-    if (slot == -1 || slot == 10) {
+  KT_HD void input(int slot, double y[4]) const {
+    if (slot < 0) {
       y[0] = r; y[1] = th; y[2] = pr; y[3] = pth;
       return;
     }
@@ -234,14 +249,9 @@ struct BLRk4 : BLBase {
       y[0] = B1[0]; y[1] = B1[1]; y[2] = B1[3]; y[3] = B1[4];
       return;
     }
-    // slots 0-5 start from s, 7-9 from B1; the first stage of a path uses k1
-    const double hb = 0.5 * h;
+    const double c = doubling_coeff(slot, h);
     const bool on_s = slot < 6;
-    const int j = (slot < 3) ? slot : (slot < 6) ? slot - 3 : slot - 6;
-    const double hs = (slot < 3) ? h : hb;
-    // stage 4 of a path takes the full step, stages 2-3 half of it
-    const double c = (on_s ? (j == 2) : (slot == 9)) ? hs : 0.5 * hs;
-    const bool use_k1 = on_s && j == 0;
+    const bool use_k1 = (slot == 0 || slot == 3);
     y[0] = (on_s ? r : B1[0]) + c * (use_k1 ? k1[0] : kp[0]);
     y[1] = (on_s ? th : B1[1]) + c * (use_k1 ? k1[1] : kp[1]);
     y[2] = (on_s ? pr : B1[3]) + c * (use_k1 ? k1[2] : kp[2]);
@@ -249,17 +259,20 @@ struct BLRk4 : BLBase {
   }
 
   // Returns true when the ray is finished (o filled).
-  KT_HD bool consume(const Frame& f, const double k[5], RayResult* o) {
+  KT_HD bool consume(const Frame& f, int slot, const double k[5], RayResult* o) {
+    if (slot < 0) {
+      for (int i = 0; i < 5; ++i) k1[i] = k[i];
+      need_k1 = false;
+      if (!pending) return false;
+      pending = false;
+      if (events(f, A[0], A[1], sp_ph, kp[0], kp[1], o)) return true;
+      return next_step(f, o);
+    }
     switch (slot) {
-      case -1:
-        for (int i = 0; i < 5; ++i) k1[i] = k[i];
-        slot = 0;
-        return false;
       case 0:
       case 3:
         for (int i = 0; i < 5; ++i) sum[i] = k1[i] + 2.0 * k[i];
         for (int i = 0; i < 4; ++i) kp[i] = k[i];
-        ++slot;
         return false;
       case 1:
       case 4:
@@ -267,12 +280,10 @@ struct BLRk4 : BLBase {
       case 8:
         for (int i = 0; i < 5; ++i) sum[i] = sum[i] + 2.0 * k[i];
         for (int i = 0; i < 4; ++i) kp[i] = k[i];
-        ++slot;
         return false;
       case 6:
         for (int i = 0; i < 5; ++i) sum[i] = k[i];
         for (int i = 0; i < 4; ++i) kp[i] = k[i];
-        slot = 7;
         return false;
       case 2: {
         const double w = h / 6.0;
@@ -280,7 +291,6 @@ struct BLRk4 : BLBase {
         A[1] = th + w * (sum[1] + k[1]);
         A[2] = pr + w * (sum[2] + k[2]);
         A[3] = pth + w * (sum[3] + k[3]);
-        slot = 3;
         return false;
       }
       case 5: {
@@ -290,10 +300,9 @@ struct BLRk4 : BLBase {
         B1[2] = ph + w * (sum[4] + k[4]);
         B1[3] = pr + w * (sum[2] + k[2]);
         B1[4] = pth + w * (sum[3] + k[3]);
-        slot = 6;
         return false;
       }
-      case 9: {
+      default: {  // 9: path B2 done -> error control
         const double w = (0.5 * h) / 6.0;
         const double Br = B1[0] + w * (sum[0] + k[0]);
         const double Bth = B1[1] + w * (sum[1] + k[1]);
@@ -316,7 +325,8 @@ struct BLRk4 : BLBase {
           ph = Bph;
           pr = Bpr;
           pth = Bpth;
-          slot = 10;
+          need_k1 = true;
+          pending = true;
           return false;
         }
         int st;
@@ -324,22 +334,18 @@ struct BLRk4 : BLBase {
           stop_here(st, (uint32_t)it, o);
           return true;
         }
-        slot = 0;
         return false;
-      }
-      default: {  // 10: k = f(s_new)
-        for (int i = 0; i < 5; ++i) k1[i] = k[i];
-        if (events(f, A[0], A[1], sp_ph, kp[0], kp[1], o)) return true;
-        return next_step(f, o);
       }
     }
   }
 };
 
-// DOPRI5 (Dormand-Prince 5(4), FSAL).  Slots: -1 -> k1 = f(s) of a new ray;
-// 0..4 -> k2..k6; 5 -> k7 = f(y5), then error control.  Phi is not advanced
-// (the reference's `advance` updates r, theta, p_r, p_theta only).
+// DOPRI5 (dopri5_adaptive, geodesic.hpp:284-414), kSlots = 6: slots 0..4
+// -> k2..k6, slot 5 -> k7 = f(y5) then error control.  FSAL: after an
+// accepted step k1 = k7, so only a new ray needs slot -1.  Phi is not
+// advanced (the reference's `advance` updates r, theta, p_r, p_theta only).
 struct BLDopri5 : BLBase {
+  static constexpr int kSlots = 6;
   double kk[7][4];
 
   KT_HD void init(const Frame& f, const Geo& s) { init_state(f, s); }
@@ -358,7 +364,7 @@ struct BLDopri5 : BLBase {
     }
   }
 
-  KT_HD void input(double y[4]) const {
+  KT_HD void input(int slot, double y[4]) const {
     const double a2[1] = {1.0 / 5.0};
     const double a3[2] = {3.0 / 40.0, 9.0 / 40.0};
     const double a4[3] = {44.0 / 45.0, -56.0 / 15.0, 32.0 / 9.0};
@@ -378,22 +384,18 @@ struct BLDopri5 : BLBase {
     }
   }
 
-  KT_HD bool consume(const Frame& f, const double k[5], RayResult* o) {
-    if (slot < 0) {
-      for (int i = 0; i < 4; ++i) kk[0][i] = k[i];
-      slot = 0;
-      return false;
-    }
-    if (slot < 5) {
-      switch (slot) {  // constant indices keep kk in registers
-        case 0: for (int i = 0; i < 4; ++i) kk[1][i] = k[i]; break;
-        case 1: for (int i = 0; i < 4; ++i) kk[2][i] = k[i]; break;
-        case 2: for (int i = 0; i < 4; ++i) kk[3][i] = k[i]; break;
-        case 3: for (int i = 0; i < 4; ++i) kk[4][i] = k[i]; break;
-        default: for (int i = 0; i < 4; ++i) kk[5][i] = k[i]; break;
-      }
-      ++slot;
-      return false;
+  KT_HD bool consume(const Frame& f, int slot, const double k[5], RayResult* o) {
+    switch (slot) {  // constant indices keep kk in registers
+      case -1:
+        for (int i = 0; i < 4; ++i) kk[0][i] = k[i];
+        need_k1 = false;
+        return false;
+      case 0: for (int i = 0; i < 4; ++i) kk[1][i] = k[i]; return false;
+      case 1: for (int i = 0; i < 4; ++i) kk[2][i] = k[i]; return false;
+      case 2: for (int i = 0; i < 4; ++i) kk[3][i] = k[i]; return false;
+      case 3: for (int i = 0; i < 4; ++i) kk[4][i] = k[i]; return false;
+      case 4: for (int i = 0; i < 4; ++i) kk[5][i] = k[i]; return false;
+      default: break;
     }
     for (int i = 0; i < 4; ++i) kk[6][i] = k[i];
     const double b5[6] = {35.0 / 384.0, 0.0, 500.0 / 1113.0, 125.0 / 192.0, -2187.0 / 6784.0,
@@ -412,7 +414,6 @@ struct BLDopri5 : BLBase {
     const double err = sqrt(err2 / 4.0);
     step_used = h;
     ++attempts;
-    slot = 0;
     if (!finite(err)) {
       h = (finite(h) && h > 1e-10) ? h * 0.5 : 1e-6;
       if (h < 1e-10) h = 1e-10;
@@ -449,8 +450,10 @@ struct BLDopri5 : BLBase {
 };
 
 // ------------------------------------------------------------- KS chart
-// trace_single_ks (main.cpp:1530-1660), RK4 step doubling in (X,Y,Z,p).
+// trace_single_ks (main.cpp:1530-1660), RK4 step doubling in (X,Y,Z,p),
+// kSlots = 10 as BLRk4.
 struct KSRk4 {
+  static constexpr int kSlots = 10;
   double s[6];   // X, Y, Z, pX, pY, pZ
   double pT;
   double h;
@@ -460,8 +463,9 @@ struct KSRk4 {
   double B1[6];
   double step_used;
   double prev_r;  // r_KS at the start of the step
-  int slot, it, rejects;
+  int it, rejects;
   uint32_t attempts;
+  bool need_k1, pending;
 
   // Returns false when init_ks_state fails: the reference then traces the
   // ray in the BL chart (main.cpp:1537-1538).
@@ -473,15 +477,18 @@ struct KSRk4 {
     h = f.dlam0;
     step_used = h;
     prev_r = r_ks(f.g, s[0], s[1], s[2]);
-    slot = -1;
     it = 0;
     rejects = 0;
     attempts = 0;
+    need_k1 = true;
+    pending = false;
     return true;
   }
 
-  KT_HD void input(double y[6]) const {
-    if (slot == -1 || slot == 10) {
+  KT_HD bool needs_k1() const { return need_k1; }
+
+  KT_HD void input(int slot, double y[6]) const {
+    if (slot < 0) {
       for (int i = 0; i < 6; ++i) y[i] = s[i];
       return;
     }
@@ -489,13 +496,9 @@ struct KSRk4 {
       for (int i = 0; i < 6; ++i) y[i] = B1[i];
       return;
     }
-    const double hb = 0.5 * h;
+    const double c = doubling_coeff(slot, h);
     const bool on_s = slot < 6;
-    const int j = (slot < 3) ? slot : (slot < 6) ? slot - 3 : slot - 6;
-    const double hs = (slot < 3) ? h : hb;
-    // stage 4 of a path takes the full step, stages 2-3 half of it
-    const double c = (on_s ? (j == 2) : (slot == 9)) ? hs : 0.5 * hs;
-    const bool use_k1 = on_s && j == 0;
+    const bool use_k1 = (slot == 0 || slot == 3);
 #pragma unroll
     for (int i = 0; i < 6; ++i) y[i] = (on_s ? s[i] : B1[i]) + c * (use_k1 ? k1[i] : kp[i]);
   }
@@ -509,19 +512,81 @@ struct KSRk4 {
     set_result(o, kOutEscaped, status, rr, 1.0, 1.0, tt, pp, 0.0);
   }
 
-  KT_HD bool consume(const Frame& f, const double k[6], RayResult* o) {
+  // Events of an accepted step (main.cpp:1570-1657); A = s_prev, kp = f(s_prev).
+  KT_HD bool events(const Frame& f, RayResult* o) {
+    const double* sp = A;
+    const double* d0 = kp;
+    const double r_now = r_ks(f.g, s[0], s[1], s[2]);
+    double best_alpha = 2.0;
+    int ev = kEvNone;
+    double disk_r = 0.0, disk_red = 1.0, disk_phi = 0.0;
+    if (sign_change(sp[2], s[2]) || (dmin(fabs(sp[2]), fabs(s[2])) < 0.35)) {
+      double alpha = 0.0;
+      bool hit = first_event(sp[2], s[2], d0[2], k1[2], step_used, 0.0, &alpha);
+      if (!hit && sign_change(sp[2], s[2])) {
+        const double denom = sp[2] - s[2];
+        alpha = (fabs(denom) > 1e-12) ? (sp[2] / denom) : 0.5;
+        alpha = dclamp(alpha, 0.0, 1.0);
+        hit = true;
+      }
+      if (hit) {
+        double xh[6];
+        for (int i = 0; i < 6; ++i) xh[i] = hermite(sp[i], s[i], d0[i], k1[i], step_used, alpha);
+        double r_hit, th_hit, ph_hit;
+        ks_to_bl(f.g, xh[0], xh[1], xh[2], &r_hit, &th_hit, &ph_hit);
+        if (r_hit >= f.r_in && r_hit <= f.r_out) {
+          const double pphi_bl = ks_pphi_bl(r_hit, th_hit, ph_hit, f.g.a, xh[3], xh[4], xh[5]);
+          disk_r = r_hit;
+          disk_red = dclamp(disk_redshift(f.g, f.eq, r_hit, pT, pphi_bl), 0.0, 20.0);
+          disk_phi = ph_hit;
+          best_alpha = alpha;
+          ev = kEvDisk;
+        }
+      }
+    }
+    horizon_escape(prev_r, r_now, f.rh_cut, f.r_esc, &best_alpha, &ev);
+    if (ev != kEvNone) {
+      o->steps = (uint32_t)it + 1;
+      o->attempts = attempts;
+      if (ev == kEvDisk) {
+        set_result(o, kOutDisk, kStEvent, disk_r, disk_red, 1.0, disk_phi, 0.0, 0.0);
+      } else if (ev == kEvHorizon) {
+        set_result(o, kOutHorizon, kStEvent, prev_r + best_alpha * (r_now - prev_r), 0.0, 1.0, 0.0,
+                   0.0, 0.0);
+      } else {
+        double xe[3];
+        for (int i = 0; i < 3; ++i) xe[i] = sp[i] + best_alpha * (s[i] - sp[i]);
+        double re, te, pe;
+        ks_to_bl(f.g, xe[0], xe[1], xe[2], &re, &te, &pe);
+        set_result(o, kOutEscaped, kStEvent, re, 1.0, 1.0, te, pe, 0.0);
+      }
+      return true;
+    }
+    prev_r = r_now;
+    ++it;
+    rejects = 0;
+    if (it >= f.max_steps) {
+      stop_at(f, s, kStStepCap, (uint32_t)it, o);
+      return true;
+    }
+    return false;
+  }
+
+  KT_HD bool consume(const Frame& f, int slot, const double k[6], RayResult* o) {
+    if (slot < 0) {
+      for (int i = 0; i < 6; ++i) k1[i] = k[i];
+      need_k1 = false;
+      if (!pending) return false;
+      pending = false;
+      return events(f, o);
+    }
     switch (slot) {
-      case -1:
-        for (int i = 0; i < 6; ++i) k1[i] = k[i];
-        slot = 0;
-        return false;
       case 0:
       case 3:
         for (int i = 0; i < 6; ++i) {
           sum[i] = k1[i] + 2.0 * k[i];
           kp[i] = k[i];
         }
-        ++slot;
         return false;
       case 1:
       case 4:
@@ -531,114 +596,47 @@ struct KSRk4 {
           sum[i] = sum[i] + 2.0 * k[i];
           kp[i] = k[i];
         }
-        ++slot;
         return false;
       case 6:
         for (int i = 0; i < 6; ++i) {
           sum[i] = k[i];
           kp[i] = k[i];
         }
-        slot = 7;
         return false;
       case 2: {
         const double w = h / 6.0;
         for (int i = 0; i < 6; ++i) A[i] = s[i] + w * (sum[i] + k[i]);
-        slot = 3;
         return false;
       }
       case 5: {
         const double w = (0.5 * h) / 6.0;
         for (int i = 0; i < 6; ++i) B1[i] = s[i] + w * (sum[i] + k[i]);
-        slot = 6;
         return false;
       }
-      case 9: {
+      default: {  // 9
         const double w = (0.5 * h) / 6.0;
         double B[6];
         for (int i = 0; i < 6; ++i) B[i] = B1[i] + w * (sum[i] + k[i]);
-        double e2 = 0.0;
-        {
-          const double e0 = A[0] - B[0], e1 = A[1] - B[1], ez = A[2] - B[2];
-          const double e3 = A[3] - B[3], e4 = A[4] - B[4], e5 = A[5] - B[5];
-          e2 = ((((e0 * e0 + e1 * e1) + ez * ez) + e3 * e3) + e4 * e4) + e5 * e5;
-        }
-        const double err = sqrt(e2) / 15.0;
+        const double e0 = A[0] - B[0], e1 = A[1] - B[1], ez = A[2] - B[2];
+        const double e3 = A[3] - B[3], e4 = A[4] - B[4], e5 = A[5] - B[5];
+        const double err =
+            sqrt(((((e0 * e0 + e1 * e1) + ez * ez) + e3 * e3) + e4 * e4) + e5 * e5) / 15.0;
         step_used = h;
         ++attempts;
         const int acc = doubling_update(err, f.tol, &h);
         if (acc == 1) {
           for (int i = 0; i < 6; ++i) {
-            A[i] = s[i];   // s_prev
+            A[i] = s[i];    // s_prev
             kp[i] = k1[i];  // f(s_prev)
             s[i] = B[i];
           }
-          slot = 10;
+          need_k1 = true;
+          pending = true;
           return false;
         }
         int st;
         if (reject_cap(h, &rejects, &st)) {
           stop_at(f, s, st, (uint32_t)it, o);
-          return true;
-        }
-        slot = 0;
-        return false;
-      }
-      default: {  // 10: k = f(s_new); events (main.cpp:1570-1657)
-        for (int i = 0; i < 6; ++i) k1[i] = k[i];
-        const double* sp = A;
-        const double* d0 = kp;
-        const double r_now = r_ks(f.g, s[0], s[1], s[2]);
-        double best_alpha = 2.0;
-        int ev = kEvNone;
-        double disk_r = 0.0, disk_red = 1.0, disk_phi = 0.0;
-        if (sign_change(sp[2], s[2]) || (dmin(fabs(sp[2]), fabs(s[2])) < 0.35)) {
-          double alpha = 0.0;
-          bool hit = first_event(sp[2], s[2], d0[2], k1[2], step_used, 0.0, &alpha);
-          if (!hit && sign_change(sp[2], s[2])) {
-            const double denom = sp[2] - s[2];
-            alpha = (fabs(denom) > 1e-12) ? (sp[2] / denom) : 0.5;
-            alpha = dclamp(alpha, 0.0, 1.0);
-            hit = true;
-          }
-          if (hit) {
-            double xh[6];
-            for (int i = 0; i < 6; ++i) xh[i] = hermite(sp[i], s[i], d0[i], k1[i], step_used, alpha);
-            double r_hit, th_hit, ph_hit;
-            ks_to_bl(f.g, xh[0], xh[1], xh[2], &r_hit, &th_hit, &ph_hit);
-            if (r_hit >= f.r_in && r_hit <= f.r_out) {
-              const double pphi_bl = ks_pphi_bl(r_hit, th_hit, ph_hit, f.g.a, xh[3], xh[4], xh[5]);
-              disk_r = r_hit;
-              disk_red = dclamp(disk_redshift(f.g, f.eq, r_hit, pT, pphi_bl), 0.0, 20.0);
-              disk_phi = ph_hit;
-              best_alpha = alpha;
-              ev = kEvDisk;
-            }
-          }
-        }
-        horizon_escape(prev_r, r_now, f.rh_cut, f.r_esc, &best_alpha, &ev);
-        if (ev != kEvNone) {
-          o->steps = (uint32_t)it + 1;
-          o->attempts = attempts;
-          if (ev == kEvDisk) {
-            set_result(o, kOutDisk, kStEvent, disk_r, disk_red, 1.0, disk_phi, 0.0, 0.0);
-          } else if (ev == kEvHorizon) {
-            set_result(o, kOutHorizon, kStEvent, prev_r + best_alpha * (r_now - prev_r), 0.0, 1.0,
-                       0.0, 0.0, 0.0);
-          } else {
-            double xe[3];
-            for (int i = 0; i < 3; ++i) xe[i] = sp[i] + best_alpha * (s[i] - sp[i]);
-            double re, te, pe;
-            ks_to_bl(f.g, xe[0], xe[1], xe[2], &re, &te, &pe);
-            set_result(o, kOutEscaped, kStEvent, re, 1.0, 1.0, te, pe, 0.0);
-          }
-          return true;
-        }
-        prev_r = r_now;
-        ++it;
-        rejects = 0;
-        slot = 0;
-        if (it >= f.max_steps) {
-          stop_at(f, s, kStStepCap, (uint32_t)it, o);
           return true;
         }
         return false;
@@ -651,17 +649,19 @@ struct KSRk4 {
 // trace_bundle (ray_bundle.hpp:301-436): RK4 step doubling of the geodesic
 // and the 4x2 deviation matrix W; error control on the geodesic only.
 struct Bundle {
+  static constexpr int kSlots = 10;
   double r, th, ph, pr, pth, pt, pphi;
   double W[8];
   double h;
   double k1[5], kW1[8];  // f(s, W)
   double sum[5], sumW[8], kp[4], kpW[8];
-  double A[4];            // path A geodesic; after acceptance: s_prev (r, th, ph)
+  double A[4];            // path A geodesic; after acceptance: s_prev (r, th)
   double B1[5], B1W[8];
   double Wprev[8];
   double step_used, sp_ph;
-  int slot, it, rejects;
+  int it, rejects;
   uint32_t attempts;
+  bool need_k1, pending;
 
   KT_HD void init(const Frame& f, int px, int py) {
     double al, be;
@@ -684,15 +684,18 @@ struct Bundle {
     W[7] = (bp.pth - bm.pth) / (2.0 * eps);
     h = f.dlam0;
     step_used = h;
-    slot = -1;
     it = 0;
     rejects = 0;
     attempts = 0;
+    need_k1 = true;
+    pending = false;
   }
 
-  // point (geodesic y[4] and W yW[8]) of the next bundle RHS
-  KT_HD void input(double y[4], double yW[8]) const {
-    if (slot == -1 || slot == 10) {
+  KT_HD bool needs_k1() const { return need_k1; }
+
+  // point (geodesic y[4] and W yW[8]) of the slot's bundle RHS
+  KT_HD void input(int slot, double y[4], double yW[8]) const {
+    if (slot < 0) {
       y[0] = r; y[1] = th; y[2] = pr; y[3] = pth;
 #pragma unroll
       for (int i = 0; i < 8; ++i) yW[i] = W[i];
@@ -704,13 +707,9 @@ struct Bundle {
       for (int i = 0; i < 8; ++i) yW[i] = B1W[i];
       return;
     }
-    const double hb = 0.5 * h;
+    const double c = doubling_coeff(slot, h);
     const bool on_s = slot < 6;
-    const int j = (slot < 3) ? slot : (slot < 6) ? slot - 3 : slot - 6;
-    const double hs = (slot < 3) ? h : hb;
-    // stage 4 of a path takes the full step, stages 2-3 half of it
-    const double c = (on_s ? (j == 2) : (slot == 9)) ? hs : 0.5 * hs;
-    const bool use_k1 = on_s && j == 0;
+    const bool use_k1 = (slot == 0 || slot == 3);
     y[0] = (on_s ? r : B1[0]) + c * (use_k1 ? k1[0] : kp[0]);
     y[1] = (on_s ? th : B1[1]) + c * (use_k1 ? k1[1] : kp[1]);
     y[2] = (on_s ? pr : B1[3]) + c * (use_k1 ? k1[2] : kp[2]);
@@ -719,20 +718,83 @@ struct Bundle {
     for (int i = 0; i < 8; ++i) yW[i] = (on_s ? W[i] : B1W[i]) + c * (use_k1 ? kW1[i] : kpW[i]);
   }
 
-  KT_HD bool consume(const Frame& f, const double k[5], const double kW[8], RayResult* o) {
+  // Events of an accepted bundle step (ray_bundle.hpp:337-434).
+  KT_HD bool events(const Frame& f, RayResult* o) {
+    const double sp_r = A[0], sp_th = A[1];
+    double best_alpha = 2.0;
+    int ev = kEvNone;
+    double disk_r = 0.0, disk_red = 1.0, disk_det = 1.0, disk_phi = 0.0;
+    bool skip = false;
+    const double q0 = sp_th - kHalfPi;
+    const double q1 = th - kHalfPi;
+    if (sign_change(q0, q1) || (dmin(fabs(q0), fabs(q1)) < 0.35)) {
+      double alpha = 0.0;
+      if (!first_event(sp_th, th, kp[1], k1[1], step_used, kHalfPi, &alpha)) {
+        skip = true;  // ray_bundle.hpp:352-356 `continue`: no horizon/escape test this step
+      } else {
+        const double r_hit = hermite(sp_r, r, kp[0], k1[0], step_used, alpha);
+        if (r_hit >= f.r_in && r_hit <= f.r_out) {
+          const double J00 = Wprev[0] + alpha * (W[0] - Wprev[0]);
+          const double J01 = Wprev[1] + alpha * (W[1] - Wprev[1]);
+          const double J10 = Wprev[2] + alpha * (W[2] - Wprev[2]);
+          const double J11 = Wprev[3] + alpha * (W[3] - Wprev[3]);
+          double det = fabs(J00 * J11 - J01 * J10);
+          det = det < 1e-12 ? 1e-12 : det;
+          disk_r = r_hit;
+          disk_red = bundle_redshift(f.g, f.eq, r_hit, pt, pphi);
+          disk_det = det;
+          disk_phi = sp_ph + alpha * (ph - sp_ph);
+          best_alpha = alpha;
+          ev = kEvDisk;
+        }
+      }
+    }
+    if (!skip) {
+      horizon_escape(sp_r, r, f.rh_cut, f.r_esc, &best_alpha, &ev);
+      if (ev != kEvNone) {
+        o->steps = (uint32_t)it + 1;
+        o->attempts = attempts;
+        if (ev == kEvDisk) {
+          set_result(o, kOutDisk, kStEvent, disk_r, disk_red, disk_det, disk_phi, 0.0, 0.0);
+        } else if (ev == kEvHorizon) {
+          // BundleResult{}: the pixel reads as escaped toward (0, 0)
+          set_result(o, kOutEscaped, kStEvent, 0.0, 1.0, 1.0, 0.0, 0.0, 0.0);
+        } else {
+          const double th_esc = sp_th + best_alpha * (th - sp_th);
+          const double ph_esc = sp_ph + best_alpha * (ph - sp_ph);
+          set_result(o, kOutEscaped, kStEvent, 0.0, 1.0, 1.0, 0.0, th_esc, ph_esc);
+        }
+        return true;
+      }
+    }
+    ++it;
+    rejects = 0;
+    if (it >= f.max_steps) {
+      o->steps = (uint32_t)it;
+      o->attempts = attempts;
+      set_result(o, kOutEscaped, kStStepCap, 0.0, 1.0, 1.0, 0.0, 0.0, 0.0);
+      return true;
+    }
+    return false;
+  }
+
+  KT_HD bool consume(const Frame& f, int slot, const double k[5], const double kW[8],
+                     RayResult* o) {
+    if (slot < 0) {
+      for (int i = 0; i < 5; ++i) k1[i] = k[i];
+      for (int i = 0; i < 8; ++i) kW1[i] = kW[i];
+      need_k1 = false;
+      if (!pending) return false;
+      pending = false;
+      return events(f, o);
+    }
     switch (slot) {
-      case -1:
-        for (int i = 0; i < 5; ++i) k1[i] = k[i];
-        for (int i = 0; i < 8; ++i) kW1[i] = kW[i];
-        slot = 0;
-        return false;
       case 0:
       case 3:
         for (int i = 0; i < 5; ++i) sum[i] = k1[i] + 2.0 * k[i];
         for (int i = 0; i < 8; ++i) sumW[i] = kW1[i] + 2.0 * kW[i];
         for (int i = 0; i < 4; ++i) kp[i] = k[i];
         for (int i = 0; i < 8; ++i) kpW[i] = kW[i];
-        ++slot;
         return false;
       case 1:
       case 4:
@@ -742,14 +804,12 @@ struct Bundle {
         for (int i = 0; i < 8; ++i) sumW[i] = sumW[i] + 2.0 * kW[i];
         for (int i = 0; i < 4; ++i) kp[i] = k[i];
         for (int i = 0; i < 8; ++i) kpW[i] = kW[i];
-        ++slot;
         return false;
       case 6:
         for (int i = 0; i < 5; ++i) sum[i] = k[i];
         for (int i = 0; i < 8; ++i) sumW[i] = kW[i];
         for (int i = 0; i < 4; ++i) kp[i] = k[i];
         for (int i = 0; i < 8; ++i) kpW[i] = kW[i];
-        slot = 7;
         return false;
       case 2: {
         const double w = h / 6.0;
@@ -757,7 +817,6 @@ struct Bundle {
         A[1] = th + w * (sum[1] + k[1]);
         A[2] = pr + w * (sum[2] + k[2]);
         A[3] = pth + w * (sum[3] + k[3]);
-        slot = 3;
         return false;
       }
       case 5: {
@@ -768,10 +827,9 @@ struct Bundle {
         B1[3] = pr + w * (sum[2] + k[2]);
         B1[4] = pth + w * (sum[3] + k[3]);
         for (int i = 0; i < 8; ++i) B1W[i] = W[i] + w * (sumW[i] + kW[i]);
-        slot = 6;
         return false;
       }
-      case 9: {
+      default: {  // 9
         const double w = (0.5 * h) / 6.0;
         const double Br = B1[0] + w * (sum[0] + k[0]);
         const double Bth = B1[1] + w * (sum[1] + k[1]);
@@ -798,7 +856,8 @@ struct Bundle {
           ph = Bph;
           pr = Bpr;
           pth = Bpth;
-          slot = 10;
+          need_k1 = true;
+          pending = true;
           return false;
         }
         int st;
@@ -807,68 +866,6 @@ struct Bundle {
           o->steps = (uint32_t)it;
           o->attempts = attempts;
           set_result(o, kOutEscaped, st, 0.0, 1.0, 1.0, 0.0, 0.0, 0.0);
-          return true;
-        }
-        slot = 0;
-        return false;
-      }
-      default: {  // 10
-        for (int i = 0; i < 5; ++i) k1[i] = k[i];
-        for (int i = 0; i < 8; ++i) kW1[i] = kW[i];
-        const double sp_r = A[0], sp_th = A[1];
-        double best_alpha = 2.0;
-        int ev = kEvNone;
-        double disk_r = 0.0, disk_red = 1.0, disk_det = 1.0, disk_phi = 0.0;
-        bool skip = false;
-        const double q0 = sp_th - kHalfPi;
-        const double q1 = th - kHalfPi;
-        if (sign_change(q0, q1) || (dmin(fabs(q0), fabs(q1)) < 0.35)) {
-          double alpha = 0.0;
-          if (!first_event(sp_th, th, kp[1], k1[1], step_used, kHalfPi, &alpha)) {
-            skip = true;  // ray_bundle.hpp:352-356 `continue`
-          } else {
-            const double r_hit = hermite(sp_r, r, kp[0], k1[0], step_used, alpha);
-            if (r_hit >= f.r_in && r_hit <= f.r_out) {
-              const double J00 = Wprev[0] + alpha * (W[0] - Wprev[0]);
-              const double J01 = Wprev[1] + alpha * (W[1] - Wprev[1]);
-              const double J10 = Wprev[2] + alpha * (W[2] - Wprev[2]);
-              const double J11 = Wprev[3] + alpha * (W[3] - Wprev[3]);
-              double det = fabs(J00 * J11 - J01 * J10);
-              det = det < 1e-12 ? 1e-12 : det;
-              disk_r = r_hit;
-              disk_red = bundle_redshift(f.g, f.eq, r_hit, pt, pphi);
-              disk_det = det;
-              disk_phi = sp_ph + alpha * (ph - sp_ph);
-              best_alpha = alpha;
-              ev = kEvDisk;
-            }
-          }
-        }
-        if (!skip) {
-          horizon_escape(sp_r, r, f.rh_cut, f.r_esc, &best_alpha, &ev);
-          if (ev != kEvNone) {
-            o->steps = (uint32_t)it + 1;
-            o->attempts = attempts;
-            if (ev == kEvDisk) {
-              set_result(o, kOutDisk, kStEvent, disk_r, disk_red, disk_det, disk_phi, 0.0, 0.0);
-            } else if (ev == kEvHorizon) {
-              // BundleResult{}: the pixel reads as escaped toward (0, 0)
-              set_result(o, kOutEscaped, kStEvent, 0.0, 1.0, 1.0, 0.0, 0.0, 0.0);
-            } else {
-              const double th_esc = sp_th + best_alpha * (th - sp_th);
-              const double ph_esc = sp_ph + best_alpha * (ph - sp_ph);
-              set_result(o, kOutEscaped, kStEvent, 0.0, 1.0, 1.0, 0.0, th_esc, ph_esc);
-            }
-            return true;
-          }
-        }
-        ++it;
-        rejects = 0;
-        slot = 0;
-        if (it >= f.max_steps) {
-          o->steps = (uint32_t)it;
-          o->attempts = attempts;
-          set_result(o, kOutEscaped, kStStepCap, 0.0, 1.0, 1.0, 0.0, 0.0, 0.0);
           return true;
         }
         return false;

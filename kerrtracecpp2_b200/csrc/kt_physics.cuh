@@ -25,6 +25,14 @@
 #define KT_HD inline
 #endif
 
+// Keep a loop rolled in device code: the loop body is the bulk of the
+// kernel, and one copy of it fits the instruction cache.
+#if defined(__CUDA_ARCH__)
+#define KT_ROLLED _Pragma("unroll 1")
+#else
+#define KT_ROLLED
+#endif
+
 namespace kt {
 
 constexpr double kPi = 3.14159265358979323846;  // M_PI
@@ -142,20 +150,45 @@ KT_HD Cov bl_cov(const Metric& g, double r, const Ang& A) {
 // dphi/dlambda (dphi_vel, geodesic.hpp:40-45): the reference evaluates
 // dphi_vel at the same (r, theta) as the RHS, so it is the same g^{mu nu}.
 // k = {dr, dtheta, dp_r, dp_theta, dphi}.
+// The three angles (theta, theta +- 1e-6) and the five inverse metrics
+// (centre, r +- eps_r, theta +- eps_th) are evaluated in rolled loops, so
+// the kernel holds one copy of each; the values are those of the reference.
 KT_HD void bl_rhs(const Metric& g, double r, double th, double pr, double pth, double pt,
                   double pphi, double k[5]) {
-  const Ang A0 = bl_ang(g, th);
-  const Inv U0 = bl_inv(g, r, A0);
-  k[0] = U0.rr * pr;
-  k[1] = U0.hh * pth;
-  k[4] = U0.tp * pt + U0.pp * pphi;
   const double eps_r = 1e-5 * dmax(fabs(r), 0.01);
   const double eps_th = 1e-6;
-  const double hp = bl_ham(bl_inv(g, r + eps_r, A0), pr, pth, pt, pphi);
-  const double hm = bl_ham(bl_inv(g, r - eps_r, A0), pr, pth, pt, pphi);
+  Ang A0, Ap, Am;
+  KT_ROLLED
+  for (int j = 0; j < 3; ++j) {
+    const double x = (j == 0) ? th : (j == 1) ? th + eps_th : th - eps_th;
+    const Ang a = bl_ang(g, x);
+    if (j == 0) A0 = a;
+    else if (j == 1) Ap = a;
+    else Am = a;
+  }
+  double hp = 0.0, hm = 0.0, tp = 0.0, tm = 0.0;
+  KT_ROLLED
+  for (int i = 0; i < 5; ++i) {
+    const double ri = (i == 1) ? r + eps_r : (i == 2) ? r - eps_r : r;
+    Ang A;
+    A.ct = 0.0;
+    A.st2 = (i == 3) ? Ap.st2 : (i == 4) ? Am.st2 : A0.st2;
+    A.Ath = (i == 3) ? Ap.Ath : (i == 4) ? Am.Ath : A0.Ath;
+    A.dth = (i == 3) ? Ap.dth : (i == 4) ? Am.dth : A0.dth;
+    const Inv U = bl_inv(g, ri, A);
+    if (i == 0) {
+      k[0] = U.rr * pr;
+      k[1] = U.hh * pth;
+      k[4] = U.tp * pt + U.pp * pphi;
+    } else {
+      const double h = bl_ham(U, pr, pth, pt, pphi);
+      hp = (i == 1) ? h : hp;
+      hm = (i == 2) ? h : hm;
+      tp = (i == 3) ? h : tp;
+      tm = (i == 4) ? h : tm;
+    }
+  }
   k[2] = -(hp - hm) / (2.0 * eps_r);
-  const double tp = bl_ham(bl_inv(g, r, bl_ang(g, th + eps_th)), pr, pth, pt, pphi);
-  const double tm = bl_ham(bl_inv(g, r, bl_ang(g, th - eps_th)), pr, pth, pt, pphi);
   k[3] = -(tp - tm) / (2.0 * eps_th);
 }
 
@@ -412,27 +445,38 @@ struct KSState {
 };
 
 // geodesic_rhs_ks, main.cpp:1432-1454.  k = {dX, dY, dZ, dpX, dpY, dpZ}.
+// The centre and the six finite-difference points share one rolled loop.
 KT_HD void ks_rhs(const Metric& g, double X, double Y, double Z, double pX, double pY, double pZ,
                   double pT, double k[6]) {
-  double G[16];
-  ks_inv(g, X, Y, Z, G);
-  k[0] = ((G[4] * pT + G[5] * pX) + G[6] * pY) + G[7] * pZ;
-  k[1] = ((G[8] * pT + G[9] * pX) + G[10] * pY) + G[11] * pZ;
-  k[2] = ((G[12] * pT + G[13] * pX) + G[14] * pY) + G[15] * pZ;
   const double p[4] = {pT, pX, pY, pZ};
   const double eX = 1e-5 * (fabs(X) + 0.1);
   const double eY = 1e-5 * (fabs(Y) + 0.1);
   const double eZ = 1e-5 * (fabs(Z) + 0.1);
-  double Gp[16], Gm[16];
-  ks_inv(g, X + eX, Y, Z, Gp);
-  ks_inv(g, X - eX, Y, Z, Gm);
-  k[3] = -(ks_ham(Gp, p) - ks_ham(Gm, p)) / (2.0 * eX);
-  ks_inv(g, X, Y + eY, Z, Gp);
-  ks_inv(g, X, Y - eY, Z, Gm);
-  k[4] = -(ks_ham(Gp, p) - ks_ham(Gm, p)) / (2.0 * eY);
-  ks_inv(g, X, Y, Z + eZ, Gp);
-  ks_inv(g, X, Y, Z - eZ, Gm);
-  k[5] = -(ks_ham(Gp, p) - ks_ham(Gm, p)) / (2.0 * eZ);
+  double h1 = 0.0, h2 = 0.0, h3 = 0.0, h4 = 0.0, h5 = 0.0, h6 = 0.0;
+  KT_ROLLED
+  for (int i = 0; i < 7; ++i) {
+    const double x = (i == 1) ? X + eX : (i == 2) ? X - eX : X;
+    const double y = (i == 3) ? Y + eY : (i == 4) ? Y - eY : Y;
+    const double z = (i == 5) ? Z + eZ : (i == 6) ? Z - eZ : Z;
+    double G[16];
+    ks_inv(g, x, y, z, G);
+    if (i == 0) {
+      k[0] = ((G[4] * pT + G[5] * pX) + G[6] * pY) + G[7] * pZ;
+      k[1] = ((G[8] * pT + G[9] * pX) + G[10] * pY) + G[11] * pZ;
+      k[2] = ((G[12] * pT + G[13] * pX) + G[14] * pY) + G[15] * pZ;
+    } else {
+      const double h = ks_ham(G, p);
+      h1 = (i == 1) ? h : h1;
+      h2 = (i == 2) ? h : h2;
+      h3 = (i == 3) ? h : h3;
+      h4 = (i == 4) ? h : h4;
+      h5 = (i == 5) ? h : h5;
+      h6 = (i == 6) ? h : h6;
+    }
+  }
+  k[3] = -(h1 - h2) / (2.0 * eX);
+  k[4] = -(h3 - h4) / (2.0 * eY);
+  k[5] = -(h5 - h6) / (2.0 * eZ);
 }
 
 // BL_to_KS_spatial (knds_metric.hpp:368-387) from precomputed sin/cos.

@@ -25,16 +25,20 @@ Geo camera_ray(const Frame& f, uint32_t pix) {
   return angle_ray(f.cam, al, be);
 }
 
+// One lane of the kernel: the slot sequence of k_trace for a single ray.
 template <class M>
 RayResult run_bl(const Frame& f, const Geo& s) {
   M m;
   m.init(f, s);
   RayResult res;
   for (;;) {
-    double y[4], k[5];
-    m.input(y);
-    bl_rhs(f.g, y[0], y[1], y[2], y[3], m.pt, m.pphi, k);
-    if (m.consume(f, k, &res)) return res;
+    for (int slot = -1; slot < M::kSlots; ++slot) {
+      if (slot < 0 && !m.needs_k1()) continue;
+      double y[4], k[5];
+      m.input(slot, y);
+      bl_rhs(f.g, y[0], y[1], y[2], y[3], m.pt, m.pphi, k);
+      if (m.consume(f, slot, k, &res)) return res;
+    }
   }
 }
 
@@ -44,10 +48,13 @@ RayResult run_ray(const Frame& f, uint32_t pix) {
     m.init(f, (int)(pix % (uint32_t)f.cam.W), (int)(pix / (uint32_t)f.cam.W));
     RayResult res;
     for (;;) {
-      double y[4], yW[8], k[5], kW[8];
-      m.input(y, yW);
-      bundle_rhs(f.g, y[0], y[1], y[2], y[3], m.pt, m.pphi, yW, k, kW);
-      if (m.consume(f, k, kW, &res)) return res;
+      for (int slot = -1; slot < Bundle::kSlots; ++slot) {
+        if (slot < 0 && !m.needs_k1()) continue;
+        double y[4], yW[8], k[5], kW[8];
+        m.input(slot, y, yW);
+        bundle_rhs(f.g, y[0], y[1], y[2], y[3], m.pt, m.pphi, yW, k, kW);
+        if (m.consume(f, slot, k, kW, &res)) return res;
+      }
     }
   }
   const Geo s = camera_ray(f, pix);
@@ -56,10 +63,13 @@ RayResult run_ray(const Frame& f, uint32_t pix) {
     if (m.init(f, s)) {
       RayResult res;
       for (;;) {
-        double y[6], k[6];
-        m.input(y);
-        ks_rhs(f.g, y[0], y[1], y[2], y[3], y[4], y[5], m.pT, k);
-        if (m.consume(f, k, &res)) return res;
+        for (int slot = -1; slot < KSRk4::kSlots; ++slot) {
+          if (slot < 0 && !m.needs_k1()) continue;
+          double y[6], k[6];
+          m.input(slot, y);
+          ks_rhs(f.g, y[0], y[1], y[2], y[3], y[4], y[5], m.pT, k);
+          if (m.consume(f, slot, k, &res)) return res;
+        }
       }
     }
   }
