@@ -18,7 +18,6 @@
 namespace kt {
 
 constexpr unsigned kFull = 0xffffffffu;
-constexpr int kBlock = 128;
 
 __device__ __forceinline__ void write_result(const OutSoA& o, uint32_t s, const RayResult& r) {
   o.outcome[s] = (uint8_t)r.outcome;
@@ -132,6 +131,15 @@ constexpr size_t smem_bytes(int block) {
   return sizeof(SmemRecord<typename ModeT::Machine>) * (size_t)block;
 }
 
+// Launch shape per mode, measured on B200 (720p KNdS frame, BL chart; 512^2
+// Kerr-Newman frame, KS chart; 480x270 bundle frame): the BL single-ray
+// kernels run best as 64-thread blocks capped at 113 registers (9 blocks =
+// 18 warps per SM, limited by the 46 KB of ray machines per 128 threads);
+// the KS and bundle kernels spill under that cap and keep 128 threads.
+template <class ModeT> struct Shape { static constexpr int kBlock = 128, kMinBlocks = 1; };
+template <> struct Shape<struct ModeBLRk4> { static constexpr int kBlock = 64, kMinBlocks = 9; };
+template <> struct Shape<struct ModeBLDopri5> { static constexpr int kBlock = 64, kMinBlocks = 9; };
+
 // ---- the persistent loop ---------------------------------------------------
 // One iteration of the outer loop is one adaptive attempt for every ray of
 // the warp.  At its start, idle lanes take new rays from the queue (one
@@ -142,7 +150,7 @@ constexpr size_t smem_bytes(int block) {
 // the end of the attempt.
 
 template <class ModeT>
-__global__ void __launch_bounds__(kBlock) k_trace(const Frame f, const OutSoA out, const RayList rl,
+__global__ void __launch_bounds__(Shape<ModeT>::kBlock, Shape<ModeT>::kMinBlocks) k_trace(const Frame f, const OutSoA out, const RayList rl,
                                                   uint32_t* __restrict__ queue, const Fallback fb) {
   extern __shared__ __align__(16) unsigned char smem[];
   using Rec = SmemRecord<typename ModeT::Machine>;
@@ -197,13 +205,14 @@ static cudaError_t shape_for(int device, LaunchShape* shape) {
   int sms = 0, per_sm = 0;
   cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   if (e != cudaSuccess) return e;
-  const size_t smem = smem_bytes<ModeT>(kBlock);
+  const int block = Shape<ModeT>::kBlock;
+  const size_t smem = smem_bytes<ModeT>(block);
   e = cudaFuncSetAttribute(k_trace<ModeT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace<ModeT>, kBlock, smem);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace<ModeT>, block, smem);
   if (e != cudaSuccess) return e;
   if (per_sm < 1) per_sm = 1;
-  shape->block = kBlock;
+  shape->block = block;
   shape->grid = sms * per_sm;
   shape->smem = smem;
   return cudaSuccess;

@@ -150,13 +150,41 @@ KT_HD Cov bl_cov(const Metric& g, double r, const Ang& A) {
 // dphi/dlambda (dphi_vel, geodesic.hpp:40-45): the reference evaluates
 // dphi_vel at the same (r, theta) as the RHS, so it is the same g^{mu nu}.
 // k = {dr, dtheta, dp_r, dp_theta, dphi}.
-// The three angles (theta, theta +- 1e-6) and the five inverse metrics
-// (centre, r +- eps_r, theta +- eps_th) are evaluated in rolled loops, so
-// the kernel holds one copy of each; the values are those of the reference.
+//
+// Three code shapes with identical arithmetic (KT_RHS_VARIANT):
+//   0  the three angles (theta, theta +- 1e-6) and the five inverse metrics
+//      (centre, r +- eps_r, theta +- eps_th) in rolled loops: one copy each;
+//   1  angles rolled; the four finite-difference metrics as two pairs in a
+//      rolled loop (two independent chains per iteration);
+//   2  everything unrolled.
+#ifndef KT_RHS_VARIANT
+#define KT_RHS_VARIANT 1
+#endif
+
+KT_HD Ang ang_select(int i, const Ang& A0, const Ang& Ap, const Ang& Am) {
+  Ang A;
+  A.ct = 0.0;
+  A.st2 = (i == 1) ? Ap.st2 : (i == 2) ? Am.st2 : A0.st2;
+  A.Ath = (i == 1) ? Ap.Ath : (i == 2) ? Am.Ath : A0.Ath;
+  A.dth = (i == 1) ? Ap.dth : (i == 2) ? Am.dth : A0.dth;
+  return A;
+}
+
 KT_HD void bl_rhs(const Metric& g, double r, double th, double pr, double pth, double pt,
                   double pphi, double k[5]) {
   const double eps_r = 1e-5 * dmax(fabs(r), 0.01);
   const double eps_th = 1e-6;
+#if KT_RHS_VARIANT == 2
+  const Ang A0 = bl_ang(g, th);
+  const Inv U0 = bl_inv(g, r, A0);
+  k[0] = U0.rr * pr;
+  k[1] = U0.hh * pth;
+  k[4] = U0.tp * pt + U0.pp * pphi;
+  const double hp = bl_ham(bl_inv(g, r + eps_r, A0), pr, pth, pt, pphi);
+  const double hm = bl_ham(bl_inv(g, r - eps_r, A0), pr, pth, pt, pphi);
+  const double tp = bl_ham(bl_inv(g, r, bl_ang(g, th + eps_th)), pr, pth, pt, pphi);
+  const double tm = bl_ham(bl_inv(g, r, bl_ang(g, th - eps_th)), pr, pth, pt, pphi);
+#else
   Ang A0, Ap, Am;
   KT_ROLLED
   for (int j = 0; j < 3; ++j) {
@@ -167,15 +195,32 @@ KT_HD void bl_rhs(const Metric& g, double r, double th, double pr, double pth, d
     else Am = a;
   }
   double hp = 0.0, hm = 0.0, tp = 0.0, tm = 0.0;
+#if KT_RHS_VARIANT == 1
+  {
+    const Inv U0 = bl_inv(g, r, A0);
+    k[0] = U0.rr * pr;
+    k[1] = U0.hh * pth;
+    k[4] = U0.tp * pt + U0.pp * pphi;
+  }
+  KT_ROLLED
+  for (int j = 0; j < 2; ++j) {
+    // j = 0: (r + eps_r, theta), (r - eps_r, theta); j = 1: (r, theta +- eps_th)
+    const double ra = (j == 0) ? r + eps_r : r;
+    const double rb = (j == 0) ? r - eps_r : r;
+    const Inv Ua = bl_inv(g, ra, ang_select(j == 0 ? 0 : 1, A0, Ap, Am));
+    const Inv Ub = bl_inv(g, rb, ang_select(j == 0 ? 0 : 2, A0, Ap, Am));
+    const double ha = bl_ham(Ua, pr, pth, pt, pphi);
+    const double hb = bl_ham(Ub, pr, pth, pt, pphi);
+    hp = (j == 0) ? ha : hp;
+    hm = (j == 0) ? hb : hm;
+    tp = (j == 1) ? ha : tp;
+    tm = (j == 1) ? hb : tm;
+  }
+#else
   KT_ROLLED
   for (int i = 0; i < 5; ++i) {
     const double ri = (i == 1) ? r + eps_r : (i == 2) ? r - eps_r : r;
-    Ang A;
-    A.ct = 0.0;
-    A.st2 = (i == 3) ? Ap.st2 : (i == 4) ? Am.st2 : A0.st2;
-    A.Ath = (i == 3) ? Ap.Ath : (i == 4) ? Am.Ath : A0.Ath;
-    A.dth = (i == 3) ? Ap.dth : (i == 4) ? Am.dth : A0.dth;
-    const Inv U = bl_inv(g, ri, A);
+    const Inv U = bl_inv(g, ri, ang_select(i == 3 ? 1 : i == 4 ? 2 : 0, A0, Ap, Am));
     if (i == 0) {
       k[0] = U.rr * pr;
       k[1] = U.hh * pth;
@@ -188,6 +233,8 @@ KT_HD void bl_rhs(const Metric& g, double r, double th, double pr, double pth, d
       tm = (i == 4) ? h : tm;
     }
   }
+#endif
+#endif
   k[2] = -(hp - hm) / (2.0 * eps_r);
   k[3] = -(tp - tm) / (2.0 * eps_th);
 }
