@@ -152,6 +152,21 @@ kt_status kt_trace_pixels(kt_context* ctx, const kt_frame_desc* desc,
                           const uint32_t* pix_dev, int64_t n,
                           const kt_geo_soa* out, void* stream);
 
+/* kt_trace for callers that may not allocate device memory (no counterpart
+ * in the reference renderer).  A host that owns all device memory, or a
+ * frame loop that cannot afford cudaMalloc/cudaFree (they can synchronize
+ * the device), passes only its own output buffers: no context, nothing
+ * allocated.  The trace kernels' scratch (ray-queue counters, KS fallback
+ * list) is a fixed device array inside the library, sized for frames of at
+ * most KT_NOALLOC_MAX_PIXELS pixels (8 MiB per GPU, held until the process
+ * exits); larger frames return KT_ERR_INVALID_ARGUMENT.  Runs on the
+ * current device, asynchronously on `stream`.  All calls share that array:
+ * calls ordered on the device are independent, calls that overlap on the
+ * device race.  The first call on a device resolves the array's address for
+ * it; make that call before any stream capture on the device. */
+#define KT_NOALLOC_MAX_PIXELS (1u << 20)
+kt_status kt_trace_noalloc(const kt_frame_desc* desc, const kt_geo_soa* out, void* stream);
+
 /* Same as kt_trace but with host buffers: copies in and out inside the
  * call and returns after the results are on the host. */
 kt_status kt_trace_host(kt_context* ctx, const kt_frame_desc* desc,

@@ -67,6 +67,8 @@ def load_library():
     L.kt_trace.restype = ctypes.c_int
     L.kt_trace_pixels.argtypes = [P, PD, P, ctypes.c_int64, ctypes.POINTER(GeoSoA), P]
     L.kt_trace_pixels.restype = ctypes.c_int
+    L.kt_trace_noalloc.argtypes = [PD, ctypes.POINTER(GeoSoA), P]
+    L.kt_trace_noalloc.restype = ctypes.c_int
     L.kt_trace_host.argtypes = [P, PD, ctypes.POINTER(GeoSoA)]
     L.kt_trace_host.restype = ctypes.c_int
     L.kt_colorize.argtypes = [P, PD, ctypes.POINTER(GeoSoA), ctypes.POINTER(ColorParams), P, I32,

@@ -29,7 +29,7 @@ NVCC_FLAGS = ARCH + ["-O3", "-std=c++17", "--fmad=false", "-lineinfo", "-Xptxas"
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", "-Wextra",
              "-I", os.path.join(CUDA_HOME, "include")]
 
-CU_SOURCES = ["kt_kernels.cu"]
+CU_SOURCES = ["kt_kernels.cu", "kt_noalloc.cu"]
 CXX_SOURCES = ["kt_frame.cpp", "kt_api.cpp", "kt_io.cpp", "kt_compat.cpp"]
 HEADERS = ["ktmath.h", "ktmath_consts.h", "kt_physics.cuh", "kt_machines.cuh", "kt_internal.h",
            "kt_frame.h"]
