@@ -159,6 +159,7 @@ def main():
     ap.add_argument("--workload", default="knds_bl_dopri5_720p", choices=sorted(WORKLOADS))
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
     args = ap.parse_args()
     sys.path.insert(0, os.path.join(ROOT, "tests"))
 
@@ -258,6 +259,46 @@ def main():
     total_ms, kernel_ms = float(t[0]), float(t[1])
     value = world * args.steps * n / (total_ms * 1e-3) / 1e6
 
+    # Mixed precision (KT_PREC_MIXED), timed the same way; its error is taken
+    # against this run's FP64 frame, which is bit-identical to the reference.
+    mixed = None
+    if not args.no_mixed and not desc.bundles:
+        mdesc = abi.frame_desc(**dict(wl, precision=abi.KT_PREC_MIXED))
+        mout = R.alloc(n, counters=True)
+        for _ in range(max(args.warmup, 1)):
+            flush.fill_(1)
+            R.trace(mdesc, mout, stream)
+        torch.cuda.synchronize(device)
+        if dist:
+            dist.barrier()
+        mev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        mev[0].record(stream)
+        for _ in range(args.steps):
+            flush.fill_(1)
+            R.trace(mdesc, mout, stream)
+        mev[1].record(stream)
+        torch.cuda.synchronize(device)
+        mt = torch.tensor([mev[0].elapsed_time(mev[1])], dtype=torch.float64, device=device)
+        if dist:
+            dist.all_reduce(mt, op=dist.ReduceOp.MAX)
+        mval = world * args.steps * n / (float(mt[0]) * 1e-3) / 1e6
+        ref_o, got_o = out["outcome"], mout["outcome"]
+        same = ref_o == got_o
+        disk = same & (ref_o == 1)
+        eg = ((mout["redshift"] - out["redshift"]).abs() / out["redshift"].abs())[disk]
+        er = ((mout["r"] - out["r"]).abs() / out["r"].abs())[disk]
+        q = lambda x, p: float(torch.quantile(x.float(), p)) if x.numel() else None
+        mixed = {"value": mval, "unit": "Mrays/s", "speedup_vs_fp64": mval / value,
+                 "ms_per_step": float(mt[0]) / args.steps,
+                 "error_vs_fp64_oracle": {
+                     "pixels": n, "class_mismatch_frac": float(1.0 - same.double().mean()),
+                     "g_rel_p50": q(eg, 0.5), "g_rel_p90": q(eg, 0.9), "g_rel_p99": q(eg, 0.99),
+                     "g_rel_max": float(eg.max()) if eg.numel() else None,
+                     "r_hit_rel_p50": q(er, 0.5), "r_hit_rel_p99": q(er, 0.99)},
+                 "fp32_rhs": "used beyond r_fp32" if kt.frame_derive(mdesc).r_fp32 != float("inf")
+                 else "off at this tolerance (analytic FP64 gradient)"}
+        del mout
+
     steps_sum = float(out["steps"].to(torch.int64).sum())
     att_sum = float(out["attempts"].to(torch.int64).sum())
     flops = ray_flops(desc, steps_sum, att_sum)
@@ -317,11 +358,12 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (procedural camera frame; no dataset)", "config": base_cfg,
             "mode": "plain FP64, bit-identical to the reference CPU path",
-            "roofline": roofline, "cpu_baseline": cpu,
+            "roofline": roofline, "cpu_baseline": cpu, "mixed_precision": mixed,
             "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": ctypes.sizeof(desc),
                     "d2h_bytes_per_step": d2h, "call": "kt_trace_host"},
             "clocks": clocks, "gpu_launches": args.steps * (2 if desc.chart == 0 and not desc.bundles
-                                                            and abs(desc.Lambda) <= 1e-15 else 1)}
+                                                            and abs(desc.Lambda) <= 1e-15 else 1)
+            * (2 if mixed is not None else 1)}
     if rank == 0:
         print(json.dumps(line), flush=True)
     R.close()

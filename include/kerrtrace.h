@@ -59,7 +59,10 @@ enum { KT_CHART_KS = 0, KT_CHART_BL = 1 };
 enum { KT_RK4_DOUBLING = 0, KT_DOPRI5 = 1 };
 /* Ray solver (RaySolverMode, main.cpp:176); only STANDARD runs here. */
 enum { KT_SOLVER_STANDARD = 0, KT_SOLVER_SEMI_ANALYTIC = 1, KT_SOLVER_ELLIPTIC_CLOSED = 2 };
-/* Arithmetic of the trace. */
+/* Arithmetic of the trace.  FP64: the reference's arithmetic bit for bit.
+ * MIXED: analytic Hamiltonian gradient, FP32 right-hand side in the far
+ * field when tol >= 1e-8, FP64 state, error control and events; agrees with
+ * FP64 to about the reference's own finite-difference noise. */
 enum { KT_PREC_FP64 = 0, KT_PREC_MIXED = 1 };
 /* kt_frame_desc.flags: theta_deg, phi_deg and fov_deg hold radians (the
  * reference's CameraParams_CUDA carries radians, gpu/cuda/tracer.cuh:16-20). */
@@ -100,6 +103,8 @@ typedef struct kt_frame_derived {
   int32_t reserved0;
   double tol;
   double bundle_eps;  /* fov_h / width * 0.5 (ray_bundle.hpp:282) */
+  double r_fp32;      /* KT_PREC_MIXED: FP32 right-hand side beyond this
+                         radius (infinity: FP32 not used at this tolerance) */
 } kt_frame_derived;
 
 /* Per-pixel results, struct of arrays, width*height entries, row-major

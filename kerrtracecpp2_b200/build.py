@@ -29,10 +29,14 @@ NVCC_FLAGS = ARCH + ["-O3", "-std=c++17", "--fmad=false", "-lineinfo", "-Xptxas"
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", "-Wextra",
              "-I", os.path.join(CUDA_HOME, "include")]
 
-CU_SOURCES = ["kt_kernels.cu", "kt_noalloc.cu"]
+CU_SOURCES = ["kt_kernels.cu", "kt_noalloc.cu", "kt_mixed.cu"]
 CXX_SOURCES = ["kt_frame.cpp", "kt_api.cpp", "kt_io.cpp", "kt_compat.cpp"]
 HEADERS = ["ktmath.h", "ktmath_consts.h", "kt_physics.cuh", "kt_machines.cuh", "kt_internal.h",
-           "kt_frame.h"]
+           "kt_frame.h", "kt_trace_kernel.cuh"]
+# Per-file compile flags: the exact kernels keep every multiply and add of
+# the reference's arithmetic separate; the mixed-precision kernels are not
+# compared bit for bit and use FMA contraction.
+CU_FLAGS = {"kt_mixed.cu": ["--fmad=true"]}
 
 
 def run(cmd, verbose):
@@ -64,7 +68,9 @@ def build(force=False, verbose=False):
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src + ".o")
         if force or newer(o, [s] + hdrs):
-            ptxas_log.append(run([NVCC] + NVCC_FLAGS + ["-c", s, "-o", o], verbose))
+            flags = [f for f in NVCC_FLAGS if not (src in CU_FLAGS and f == "--fmad=false")]
+            ptxas_log.append(run([NVCC] + flags + CU_FLAGS.get(src, []) + ["-c", s, "-o", o],
+                                 verbose))
         objs.append(o)
     for src in CXX_SOURCES:
         s = os.path.join(CSRC, src)

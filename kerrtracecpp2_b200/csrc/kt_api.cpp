@@ -28,7 +28,7 @@ struct kt_context {
   size_t bg_cap = 0;
   cudaStream_t stream = nullptr;
   kt::LaunchShape shapes[kt::kNumModes];
-  bool shape_ok[kt::kNumModes] = {false, false, false, false};
+  bool shape_ok[kt::kNumModes] = {};
 };
 
 namespace {
@@ -78,12 +78,6 @@ kt_status ensure(kt_context* ctx, void** buf, size_t* cap, size_t need, const ch
   return KT_OK;
 }
 
-kt::Mode mode_of(const kt::Frame& f) {
-  if (f.bundles) return kt::kModeBundle;
-  if (f.chart == KT_CHART_KS) return kt::kModeKSRk4;
-  return f.intg == KT_DOPRI5 ? kt::kModeBLDopri5 : kt::kModeBLRk4;
-}
-
 kt_status shape(kt_context* ctx, kt::Mode m, kt::LaunchShape* s) {
   if (!ctx->shape_ok[m]) {
     KT_CUDA(ctx, kt::launch_shape(m, ctx->device, &ctx->shapes[m]), "occupancy query");
@@ -117,21 +111,21 @@ bool out_complete(const kt_geo_soa* o) {
 // whose KS initialisation failed, main.cpp:1537-1538).
 kt_status run_trace(kt_context* ctx, const kt::Frame& f, const kt::OutSoA& out,
                     const kt::RayList& rl, uint64_t n_max, cudaStream_t st) {
-  const kt::Mode m = mode_of(f);
+  const kt::Mode m = kt::frame_mode(f);
   kt::LaunchShape s;
   kt_status r = shape(ctx, m, &s);
   if (r != KT_OK) return r;
   KT_CUDA(ctx, cudaMemsetAsync(ctx->d_counters, 0, 4 * sizeof(uint32_t), st), "reset queue");
   kt::Fallback fb = {nullptr, nullptr, ctx->d_counters + 2};
-  if (m == kt::kModeKSRk4) {
+  if (kt::is_ks_mode(m)) {
     r = ensure(ctx, (void**)&ctx->d_fb, &ctx->fb_cap, 2 * n_max * sizeof(uint32_t), "fallback list");
     if (r != KT_OK) return r;
     fb.pix = ctx->d_fb;
     fb.slot = ctx->d_fb + n_max;
   }
   KT_CUDA(ctx, kt::launch_trace(m, f, out, rl, ctx->d_counters, fb, s, st), "trace kernel launch");
-  if (m == kt::kModeKSRk4) {
-    const kt::Mode bm = f.intg == KT_DOPRI5 ? kt::kModeBLDopri5 : kt::kModeBLRk4;
+  if (kt::is_ks_mode(m)) {
+    const kt::Mode bm = kt::fallback_mode(f);
     kt::LaunchShape bs;
     r = shape(ctx, bm, &bs);
     if (r != KT_OK) return r;

@@ -166,8 +166,12 @@ kt_status prepare_frame(const kt_frame_desc* d, Frame* f, kt_frame_derived* dv, 
     *err = "only --solver-mode standard runs on this backend";
     return KT_ERR_UNSUPPORTED;
   }
-  if (d->precision != KT_PREC_FP64) {
-    *err = "only KT_PREC_FP64 is implemented";
+  if (d->precision != KT_PREC_FP64 && d->precision != KT_PREC_MIXED) {
+    *err = "precision must be KT_PREC_FP64 or KT_PREC_MIXED";
+    return KT_ERR_INVALID_ARGUMENT;
+  }
+  if (d->precision == KT_PREC_MIXED && d->bundles) {
+    *err = "the mixed-precision tracer has no ray-bundle mode";
     return KT_ERR_UNSUPPORTED;
   }
   if ((d->flags & ~(uint32_t)KT_FLAG_ANGLES_RADIANS) != 0) {
@@ -215,6 +219,13 @@ kt_status prepare_frame(const kt_frame_desc* d, Frame* f, kt_frame_derived* dv, 
   fr.r_out = d->disk_out;
   fr.r_esc = d->r_obs * 1.05;
   fr.bundle_eps = (fov / (double)d->width) * 0.5;
+  // Mixed precision: the FP32 RHS carries ~1e-7 relative rounding noise, which
+  // the step controller sees as error; it is used only when the tolerance is
+  // looser than 1e-8, beyond max(4M, 2 r_+), away from turning points.
+  fr.precision = d->precision;
+  fr.r_fp32 = (d->precision == KT_PREC_MIXED && fr.tol >= 1e-8) ? dmax(4.0 * d->M, 2.0 * rh)
+                                                                  : ktm_inf();
+  fr.turn_frac = 0.05;
   *f = fr;
   if (dv) {
     memset(dv, 0, sizeof *dv);
@@ -234,6 +245,7 @@ kt_status prepare_frame(const kt_frame_desc* d, Frame* f, kt_frame_derived* dv, 
     dv->max_steps = fr.max_steps;
     dv->tol = fr.tol;
     dv->bundle_eps = fr.bundle_eps;
+    dv->r_fp32 = fr.r_fp32;
   }
   return KT_OK;
 }

@@ -39,7 +39,32 @@ struct Fallback {
   uint32_t* count;
 };
 
-enum Mode : int { kModeBLRk4 = 0, kModeBLDopri5 = 1, kModeKSRk4 = 2, kModeBundle = 3, kNumModes = 4 };
+enum Mode : int {
+  kModeBLRk4 = 0,
+  kModeBLDopri5 = 1,
+  kModeKSRk4 = 2,
+  kModeBundle = 3,
+  kModeBLRk4Mixed = 4,
+  kModeBLDopri5Mixed = 5,
+  kModeKSRk4Mixed = 6,
+  kNumModes = 7
+};
+
+// Kernel mode of a prepared frame (and, for the KS chart, of its BL
+// fallback pass).
+inline Mode frame_mode(const Frame& f) {
+  if (f.bundles) return kModeBundle;
+  const bool mixed = f.precision == 1;
+  if (f.chart == 0) return mixed ? kModeKSRk4Mixed : kModeKSRk4;
+  if (f.intg == 1) return mixed ? kModeBLDopri5Mixed : kModeBLDopri5;
+  return mixed ? kModeBLRk4Mixed : kModeBLRk4;
+}
+inline Mode fallback_mode(const Frame& f) {
+  const bool mixed = f.precision == 1;
+  if (f.intg == 1) return mixed ? kModeBLDopri5Mixed : kModeBLDopri5;
+  return mixed ? kModeBLRk4Mixed : kModeBLRk4;
+}
+inline bool is_ks_mode(Mode m) { return m == kModeKSRk4 || m == kModeKSRk4Mixed; }
 
 struct LaunchShape {
   int block;    // threads per block
@@ -60,6 +85,12 @@ cudaError_t launch_colorize(const ColourConst& cc, int64_t n, const uint8_t* out
                             const double* r, const double* red, const double* magnif,
                             const double* th_esc, const double* ph_esc, const uint8_t* bg,
                             int bg_w, int bg_h, uint8_t* rgb, cudaStream_t stream);
+
+// Mixed-precision kernels (kt_mixed.cu).
+cudaError_t launch_shape_mixed(Mode mode, int device, LaunchShape* shape);
+cudaError_t launch_trace_mixed(Mode mode, const Frame& f, const OutSoA& out, const RayList& rl,
+                               uint32_t* queue, const Fallback& fb, const LaunchShape& shape,
+                               cudaStream_t stream);
 
 // FP64 throughput probe: n_iter dependent FMA chains per thread.
 cudaError_t launch_fp64_probe(double* out, int n_iter, int grid, int block, cudaStream_t stream);

@@ -38,8 +38,12 @@ struct Frame {
   double r_in, r_out, r_esc, rh_cut;
   double dlam0, tol;
   double bundle_eps;
+  double r_fp32;     // mixed precision: FP32 RHS beyond this radius (inf: never)
+  double turn_frac;  // mixed precision: FP64 when |p_r| or |p_th|/r < turn_frac |p_t|
   int max_steps;
   int chart, intg, bundles;
+  int precision;     // KT_PREC_FP64 / KT_PREC_MIXED
+  int pad0;
 };
 
 struct RayResult {

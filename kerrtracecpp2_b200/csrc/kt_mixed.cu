@@ -1,0 +1,122 @@
+// kt_mixed.cu -- mixed-precision trace kernels (KT_PREC_MIXED).
+//
+// Same persistent loop and the same FP64 integrators as the exact kernels
+// (state, stage sums, embedded error estimate, step-size controller, event
+// location and the disk-crossing root all stay FP64), with a different
+// right-hand side: the Hamiltonian gradient is evaluated analytically
+// (bl_rhs_analytic / ks_rhs_analytic: one inverse metric with four
+// reciprocals instead of five metrics with 26 correctly rounded divisions),
+// in FP32 where the tolerance and the geometry allow it, else in FP64.
+// FP32 is used for a warp's RHS only when every active lane of the warp is
+// beyond r_fp32 and away from a radial or polar turning point, so lanes never
+// diverge between the two paths.  This file is compiled with FMA
+// contraction on; its results are not bit-identical to the reference and
+// are compared with the FP64 oracle statistically.
+#include "kt_trace_kernel.cuh"
+
+namespace kt {
+
+__device__ __forceinline__ bool warp_all(bool p) { return __all_sync(__activemask(), p); }
+
+// BL: FP32 beyond r_fp32 unless p_r or p_theta/r is small against |p_t|.
+__device__ __forceinline__ void bl_rhs_mixed(const Frame& f, const double y[4], double pt,
+                                             double pphi, double k[5]) {
+  const double lim = f.turn_frac * fabs(pt);
+  const bool far = y[0] > f.r_fp32 && fabs(y[2]) > lim && fabs(y[3]) > lim * y[0];
+  if (warp_all(far))
+    bl_rhs_analytic<float>(f.g, y[0], y[1], y[2], y[3], pt, pphi, k);
+  else
+    bl_rhs_analytic<double>(f.g, y[0], y[1], y[2], y[3], pt, pphi, k);
+}
+
+struct ModeBLRk4Mixed {
+  using Machine = BLRk4;
+  static constexpr int kSlots = BLRk4::kSlots;
+  BLRk4* m;
+  __device__ __forceinline__ bool needs_k1() const { return m->needs_k1(); }
+  __device__ __forceinline__ bool start(const Frame& f, uint32_t pix, uint32_t, const Fallback&) {
+    m->init(f, camera_ray(f, pix));
+    return true;
+  }
+  __device__ __forceinline__ bool slot(const Frame& f, int s, RayResult* res) {
+    double y[4], k[5];
+    m->input(s, y);
+    bl_rhs_mixed(f, y, m->pt, m->pphi, k);
+    return m->consume(f, s, k, res);
+  }
+};
+
+struct ModeBLDopri5Mixed {
+  using Machine = BLDopri5;
+  static constexpr int kSlots = BLDopri5::kSlots;
+  BLDopri5* m;
+  __device__ __forceinline__ bool needs_k1() const { return m->needs_k1(); }
+  __device__ __forceinline__ bool start(const Frame& f, uint32_t pix, uint32_t, const Fallback&) {
+    m->init(f, camera_ray(f, pix));
+    return true;
+  }
+  __device__ __forceinline__ bool slot(const Frame& f, int s, RayResult* res) {
+    double y[4], k[5];
+    m->input(s, y);
+    bl_rhs_mixed(f, y, m->pt, m->pphi, k);
+    return m->consume(f, s, k, res);
+  }
+};
+
+// KS: FP32 beyond r_fp32 unless the radial momentum x.p/|x| is small.
+struct ModeKSRk4Mixed {
+  using Machine = KSRk4;
+  static constexpr int kSlots = KSRk4::kSlots;
+  KSRk4* m;
+  __device__ __forceinline__ bool needs_k1() const { return m->needs_k1(); }
+  __device__ __forceinline__ bool start(const Frame& f, uint32_t pix, uint32_t out_slot,
+                                        const Fallback& fb) {
+    if (m->init(f, camera_ray(f, pix))) return true;
+    const uint32_t i = atomicAdd(fb.count, 1u);
+    fb.pix[i] = pix;
+    fb.slot[i] = out_slot;
+    return false;
+  }
+  __device__ __forceinline__ bool slot(const Frame& f, int s, RayResult* res) {
+    double y[6], k[6];
+    m->input(s, y);
+    const double rr = sqrt(y[0] * y[0] + y[1] * y[1] + y[2] * y[2]);
+    const double prad = (y[0] * y[3] + y[1] * y[4] + y[2] * y[5]) / rr;
+    const bool far = rr > f.r_fp32 && fabs(prad) > f.turn_frac * fabs(m->pT);
+    if (warp_all(far))
+      ks_rhs_analytic<float>(f.g, y[0], y[1], y[2], y[3], y[4], y[5], m->pT, k);
+    else
+      ks_rhs_analytic<double>(f.g, y[0], y[1], y[2], y[3], y[4], y[5], m->pT, k);
+    return m->consume(f, s, k, res);
+  }
+};
+
+template <class ModeT>
+static cudaError_t launch_one(const Frame& f, const OutSoA& out, const RayList& rl,
+                              uint32_t* queue, const Fallback& fb, const LaunchShape& s,
+                              cudaStream_t stream) {
+  k_trace<ModeT><<<s.grid, s.block, s.smem, stream>>>(f, out, rl, queue, fb);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_shape_mixed(Mode mode, int device, LaunchShape* shape) {
+  switch (mode) {
+    case kModeBLRk4Mixed: return shape_for<ModeBLRk4Mixed>(device, shape);
+    case kModeBLDopri5Mixed: return shape_for<ModeBLDopri5Mixed>(device, shape);
+    case kModeKSRk4Mixed: return shape_for<ModeKSRk4Mixed>(device, shape);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_trace_mixed(Mode mode, const Frame& f, const OutSoA& out, const RayList& rl,
+                               uint32_t* queue, const Fallback& fb, const LaunchShape& s,
+                               cudaStream_t stream) {
+  switch (mode) {
+    case kModeBLRk4Mixed: return launch_one<ModeBLRk4Mixed>(f, out, rl, queue, fb, s, stream);
+    case kModeBLDopri5Mixed: return launch_one<ModeBLDopri5Mixed>(f, out, rl, queue, fb, s, stream);
+    case kModeKSRk4Mixed: return launch_one<ModeKSRk4Mixed>(f, out, rl, queue, fb, s, stream);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace kt

@@ -239,6 +239,145 @@ KT_HD void bl_rhs(const Metric& g, double r, double th, double pr, double pth, d
   k[3] = -(tp - tm) / (2.0 * eps_th);
 }
 
+// Analytic Hamiltonian gradient for the mixed-precision tracer (no
+// counterpart in the reference, which differentiates H by central
+// differences).  With S = Sigma, R = Delta_r, T = Delta_theta, A = r^2+a^2,
+// s2 = sin^2, c = cos, xi2 = Xi^2, the inverse metric is
+//   g^tt = -xi2/S (A^2/R - a^2 s2/T)      g^tphi = a xi2/S (1/T - A/R)
+//   g^rr = R/S     g^thth = T/S           g^phiphi = xi2/S (1/(T s2) - a^2/R)
+// and dH/dr, dH/dtheta follow by the quotient rule from dS/dr = 2r,
+// dR/dr = 2r(1 - L r^2/3) - (2L r/3) A - 2M, dS/dth = -2a^2 s c,
+// dT/dth = -(2 L a^2/3) s c, d(s2)/dth = 2 s c.  One evaluation, four
+// reciprocals; T is float (far field) or double.  k as bl_rhs.
+template <class T>
+KT_HD void bl_rhs_analytic(const Metric& g, double r_, double th_, double pr_, double pth_,
+                           double pt_, double pphi_, double k[5]) {
+  const T r = (T)r_, pr = (T)pr_, pth = (T)pth_, pt = (T)pt_, pphi = (T)pphi_;
+  const T a = (T)g.a, a2 = (T)g.a2, L = (T)g.L, M = (T)g.M, Q2 = (T)g.Q2, xi2 = (T)g.xi2;
+  T sn, c;
+  if (sizeof(T) == sizeof(float)) {
+    float sf, cf;
+    sincosf((float)th_, &sf, &cf);
+    sn = (T)sf;
+    c = (T)cf;
+  } else {
+    double sd, cd;
+    ktm_sincos(th_, &sd, &cd);
+    sn = (T)sd;
+    c = (T)cd;
+  }
+  const T s2 = sn * sn, sc = sn * c;
+  const T r2 = r * r;
+  const T A = r2 + a2;
+  const T S = r2 + a2 * c * c;
+  const T Lr2_3 = L * r2 / (T)3;
+  const T R = A * ((T)1 - Lr2_3) - (T)2 * M * r + Q2;
+  const T Tt = (T)1 + L * a2 * c * c / (T)3;
+  const T iS = (T)1 / S, iR = (T)1 / R, iT = (T)1 / Tt;
+  const bool pole = !(s2 > (T)1e-14);
+  const T is2 = pole ? (T)0 : (T)1 / s2;
+  // g^{mu nu}
+  const T X_tt = A * A * iR - a2 * s2 * iT;
+  const T X_tp = iT - A * iR;
+  const T X_pp = pole ? (T)0 : (iT * is2 - a2 * iR);
+  const T U_tp = a * xi2 * iS * X_tp;
+  const T U_rr = R * iS, U_hh = Tt * iS;
+  const T U_pp = xi2 * iS * X_pp;
+  // d/dr
+  const T dS_r = (T)2 * r;
+  const T dR_r = (T)2 * r * ((T)1 - Lr2_3) - ((T)2 * L * r / (T)3) * A - (T)2 * M;
+  const T diS_r = -dS_r * iS * iS, diR_r = -dR_r * iR * iR;
+  const T dX_tt_r = (T)2 * A * dS_r * iR + A * A * diR_r;  // dA/dr = dS/dr = 2r
+  const T dX_tp_r = -(dS_r * iR + A * diR_r);
+  const T dX_pp_r = pole ? (T)0 : -a2 * diR_r;
+  const T dU_tt_r = -xi2 * (diS_r * X_tt + iS * dX_tt_r);
+  const T dU_tp_r = a * xi2 * (diS_r * X_tp + iS * dX_tp_r);
+  const T dU_rr_r = dR_r * iS + R * diS_r;
+  const T dU_hh_r = Tt * diS_r;
+  const T dU_pp_r = xi2 * (diS_r * X_pp + iS * dX_pp_r);
+  // d/dtheta
+  const T dS_t = -(T)2 * a2 * sc;
+  const T dT_t = -((T)2 * L * a2 / (T)3) * sc;
+  const T diS_t = -dS_t * iS * iS, diT_t = -dT_t * iT * iT;
+  const T dis2_t = pole ? (T)0 : -(T)2 * sc * is2 * is2;
+  const T dX_tt_t = -a2 * ((T)2 * sc * iT + s2 * diT_t);
+  const T dX_pp_t = pole ? (T)0 : (diT_t * is2 + iT * dis2_t);
+  const T dU_tt_t = -xi2 * (diS_t * X_tt + iS * dX_tt_t);
+  const T dU_tp_t = a * xi2 * (diS_t * X_tp + iS * diT_t);
+  const T dU_rr_t = R * diS_t;
+  const T dU_hh_t = dT_t * iS + Tt * diS_t;
+  const T dU_pp_t = xi2 * (diS_t * X_pp + iS * dX_pp_t);
+  const T ptpt = pt * pt, ptpp = (T)2 * pt * pphi, prpr = pr * pr, phph = pth * pth,
+          pppp = pphi * pphi;
+  k[0] = (double)(U_rr * pr);
+  k[1] = (double)(U_hh * pth);
+  k[4] = (double)(U_tp * pt + U_pp * pphi);
+  k[2] = (double)(-(T)0.5 * (dU_tt_r * ptpt + dU_tp_r * ptpp + dU_rr_r * prpr + dU_hh_r * phph +
+                            dU_pp_r * pppp));
+  k[3] = (double)(-(T)0.5 * (dU_tt_t * ptpt + dU_tp_t * ptpp + dU_rr_t * prpr + dU_hh_t * phph +
+                            dU_pp_t * pppp));
+}
+
+// Reciprocal in T: correctly rounded on host and device alike.
+template <class T>
+KT_HD T kt_rcp(T x) {
+#if defined(__CUDA_ARCH__)
+  if (sizeof(T) == sizeof(float)) return (T)__frcp_rn((float)x);
+  return (T)__drcp_rn((double)x);
+#else
+  return (T)1 / x;
+#endif
+}
+
+// Analytic KS gradient for the mixed-precision tracer.  With
+// g^ab = eta^ab - H l^a l^b (ingoing, knds_metric.hpp:202-218) the
+// Hamiltonian is H_ham = (eta^ab p_a p_b)/2 - H ell^2/2 with
+// ell = l^a p_a = -p_T + u/D + Z p_Z/r, u = (rX + aY) p_X + (rY - aX) p_Y,
+// D = r^2 + a^2, H = (2Mr - Q^2)/rho2, rho2 = r^2 + a^2 Z^2/r^2, and r(X,Y,Z)
+// the root of r^4 - (R^2 - a^2) r^2 - a^2 Z^2 = 0, whose gradient is
+// dr/dX = X r/E, dr/dY = Y r/E, dr/dZ = Z (r^2+a^2)/(r E), E = 2r^2-(R^2-a^2).
+// dx/dlam = p - H ell l, dp/dlam = -grad H_ham = (grad H) ell^2/2 + H ell grad ell.
+template <class T>
+KT_HD void ks_rhs_analytic(const Metric& g, double X_, double Y_, double Z_, double pX_,
+                           double pY_, double pZ_, double pT_, double k[6]) {
+  const T X = (T)X_, Y = (T)Y_, Z = (T)Z_, pX = (T)pX_, pY = (T)pY_, pZ = (T)pZ_, pT = (T)pT_;
+  const T a = (T)g.a, a2 = (T)g.a2, M = (T)g.M, Q2 = (T)g.Q2;
+  const T R2 = X * X + Y * Y + Z * Z;
+  const T b = R2 - a2;
+  const T r = sqrt((T)0.5 * (b + sqrt(b * b + (T)4 * a2 * Z * Z)));
+  const T r2 = r * r;
+  const T ir = kt_rcp(r);
+  const T D = r2 + a2;
+  const T iD = kt_rcp(D);
+  const T iE = kt_rcp((T)2 * r2 - b);
+  const T drX = X * r * iE, drY = Y * r * iE, drZ = Z * D * ir * iE;
+  const T rho2 = r2 + a2 * Z * Z * ir * ir;
+  const T irho2 = kt_rcp(rho2);
+  const T N = (T)2 * M * r - Q2;
+  const T H = N * irho2;
+  const T l1 = (r * X + a * Y) * iD, l2 = (r * Y - a * X) * iD, l3 = Z * ir;
+  const T u = (r * X + a * Y) * pX + (r * Y - a * X) * pY;
+  const T ell = -pT + u * iD + Z * pZ * ir;
+  const T w = X * pX + Y * pY;
+  // d(rho2), dH, d(ell) for x_i = X, Y, Z
+  const T dr[3] = {drX, drY, drZ};
+  const T du[3] = {drX * w + r * pX - a * pY, drY * w + a * pX + r * pY, drZ * w};
+  const T Hl = H * ell;
+  k[0] = (double)(pX - Hl * l1);
+  k[1] = (double)(pY - Hl * l2);
+  k[2] = (double)(pZ - Hl * l3);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const T drho2 = (T)2 * r * dr[i] + a2 * ((i == 2 ? (T)2 * Z : (T)0) * ir * ir -
+                                              (T)2 * Z * Z * ir * ir * ir * dr[i]);
+    const T dH = ((T)2 * M * dr[i] - H * drho2) * irho2;
+    const T dD = (T)2 * r * dr[i];
+    const T dell = (du[i] - u * iD * dD) * iD +
+                   pZ * ((i == 2 ? r : (T)0) - Z * dr[i]) * ir * ir;
+    k[3 + i] = (double)((T)0.5 * dH * ell * ell + Hl * dell);
+  }
+}
+
 // keplerian_omega, knds_metric.hpp:354-363
 KT_HD double kepler_omega(const Metric& g, double r) {
   const double s = (g.a < 0.0) ? 1.0 : -1.0;

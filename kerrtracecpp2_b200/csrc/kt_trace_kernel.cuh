@@ -1,0 +1,145 @@
+// kt_trace_kernel.cuh -- the persistent trace loop, shared by the exact
+// (kt_kernels.cu) and the mixed-precision (kt_mixed.cu) kernels.
+//
+// One CUDA thread carries one ray at a time through a per-ray machine
+// (kt_machines.cuh); the 32 rays of a warp advance through the slots of an
+// adaptive attempt in lockstep, one Hamiltonian right-hand side per slot.
+// At every attempt boundary the lanes whose rays finished take new rays from
+// a device queue (one atomicAdd per warp for all its idle lanes).  Rays
+// differ in length by 3-50x, so refilling keeps the FP64 pipes busy until
+// the queue runs dry; the grid is sized to the resident capacity of the GPU
+// (persistent kernel).  Ray machines live in shared memory; results go out
+// as SoA.
+//
+// The kernels do no waiting on other threads: the only inter-thread
+// operation is the warp-synchronous refill and the queue atomic.  Every ray
+// stops after at most max_steps accepted steps with at most 65 rejected
+// attempts each (the reference's limits), so every loop ends.
+#pragma once
+
+#include "kt_internal.h"
+
+namespace kt {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ void write_result(const OutSoA& o, uint32_t s, const RayResult& r) {
+  o.outcome[s] = (uint8_t)r.outcome;
+  o.r[s] = r.r;
+  o.red[s] = r.red;
+  o.magnif[s] = r.magnif;
+  o.phi_disk[s] = r.phi_disk;
+  o.th_esc[s] = r.th_esc;
+  o.ph_esc[s] = r.ph_esc;
+  if (o.status) o.status[s] = (uint8_t)r.status;
+  if (o.steps) o.steps[s] = r.steps;
+  if (o.attempts) o.attempts[s] = r.attempts;
+}
+
+// ---- per-mode start (new ray) and one slot (one RHS) ---------------------
+
+__device__ __forceinline__ Geo camera_ray(const Frame& f, uint32_t pix) {
+  const int px = (int)(pix % (uint32_t)f.cam.W);
+  const int py = (int)(pix / (uint32_t)f.cam.W);
+  double al, be;
+  pixel_angles(f.cam, px, py, &al, &be);
+  return angle_ray(f.cam, al, be);
+}
+
+// Each mode keeps its ray machine in shared memory (one record per thread,
+// record size an odd number of 8-byte words so a warp's accesses spread over
+// the banks): the machine is touched only between RHS evaluations, so the
+// registers are left to the RHS working set and more warps fit per SM.
+template <class M>
+struct alignas(8) SmemRecord {
+  M m;
+  double pad[((sizeof(M) + 7) / 8) % 2 == 0 ? 1 : 2];
+};
+
+template <class ModeT>
+constexpr size_t smem_bytes(int block) {
+  return sizeof(SmemRecord<typename ModeT::Machine>) * (size_t)block;
+}
+
+// Launch shape per mode: 128-thread blocks by default; a mode may
+// specialise this (see kt_kernels.cu, kt_mixed.cu).
+template <class ModeT> struct Shape { static constexpr int kBlock = 128, kMinBlocks = 1; };
+// ---- the persistent loop ---------------------------------------------------
+// One iteration of the outer loop is one adaptive attempt for every ray of
+// the warp.  At its start, idle lanes take new rays from the queue (one
+// atomicAdd per warp).  Slot -1 runs only if some lane needs it (new rays,
+// f at the end of an accepted step); slots 0..kSlots-1 run for every active
+// lane.  All lanes of the warp see the same slot index, so the bookkeeping
+// after each RHS runs converged; a lane whose ray ends mid-attempt idles to
+// the end of the attempt.
+
+template <class ModeT>
+__global__ void __launch_bounds__(Shape<ModeT>::kBlock, Shape<ModeT>::kMinBlocks) k_trace(const Frame f, const OutSoA out, const RayList rl,
+                                                  uint32_t* __restrict__ queue, const Fallback fb) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  using Rec = SmemRecord<typename ModeT::Machine>;
+  ModeT mode;
+  mode.m = &reinterpret_cast<Rec*>(smem)[threadIdx.x].m;
+  bool active = false;
+  uint32_t out_slot = 0;
+  const uint32_t n = rl.n_dev ? *rl.n_dev : rl.n;
+  const unsigned lane = threadIdx.x & 31u;
+  bool exhausted = false;
+  for (;;) {
+    if (!exhausted) {
+      const unsigned need = __ballot_sync(kFull, !active);
+      if (need) {
+        const int leader = __ffs(need) - 1;
+        const unsigned cnt = (unsigned)__popc(need);
+        unsigned base = 0;
+        if ((int)lane == leader) base = atomicAdd(queue, cnt);
+        base = __shfl_sync(kFull, base, leader);
+        if (base + cnt >= n) exhausted = true;
+        if (!active) {
+          const unsigned idx = base + (unsigned)__popc(need & ((1u << lane) - 1u));
+          if (idx < n) {
+            const uint32_t pix = rl.pix ? rl.pix[idx] : idx;
+            out_slot = rl.slot ? rl.slot[idx] : idx;
+            active = mode.start(f, pix, out_slot, fb);
+          }
+        }
+      }
+    }
+    if (!__any_sync(kFull, active)) {
+      if (exhausted) break;
+      continue;
+    }
+    KT_ROLLED
+    for (int s = -1; s < ModeT::kSlots; ++s) {
+      const bool part = active && (s >= 0 || mode.needs_k1());
+      if (s < 0 && !__any_sync(kFull, part)) continue;
+      if (part) {
+        RayResult res;
+        if (mode.slot(f, s, &res)) {
+          write_result(out, out_slot, res);
+          active = false;
+        }
+      }
+    }
+  }
+}
+
+template <class ModeT>
+static cudaError_t shape_for(int device, LaunchShape* shape) {
+  int sms = 0, per_sm = 0;
+  cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  if (e != cudaSuccess) return e;
+  const int block = Shape<ModeT>::kBlock;
+  const size_t smem = smem_bytes<ModeT>(block);
+  e = cudaFuncSetAttribute(k_trace<ModeT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace<ModeT>, block, smem);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) per_sm = 1;
+  shape->block = block;
+  shape->grid = sms * per_sm;
+  shape->smem = smem;
+  return cudaSuccess;
+}
+
+}  // namespace kt

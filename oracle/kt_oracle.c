@@ -1277,6 +1277,8 @@ int orc_frame_derive(const kt_frame_desc* d, kt_frame_derived* out) {
   out->max_steps = f.max_steps;
   out->tol = f.tol;
   out->bundle_eps = (f.cam.fov_h / (double)f.cam.W) * 0.5;
+  out->r_fp32 = (d->precision == KT_PREC_MIXED && f.tol >= 1e-8)
+                    ? omax(4.0 * d->M, 2.0 * f.rh) : ktm_inf(); /* renderer's mixed mode */
   return 0;
 }
 

@@ -25,6 +25,25 @@ Geo camera_ray(const Frame& f, uint32_t pix) {
   return angle_ray(f.cam, al, be);
 }
 
+// The mixed-precision right-hand sides of kt_mixed.cu for one lane (the
+// kernel decides FP32 per warp; a single lane decides for itself).
+void bl_rhs_mixed_host(const Frame& f, const double y[4], double pt, double pphi, double k[5]) {
+  const double lim = f.turn_frac * fabs(pt);
+  if (y[0] > f.r_fp32 && fabs(y[2]) > lim && fabs(y[3]) > lim * y[0])
+    bl_rhs_analytic<float>(f.g, y[0], y[1], y[2], y[3], pt, pphi, k);
+  else
+    bl_rhs_analytic<double>(f.g, y[0], y[1], y[2], y[3], pt, pphi, k);
+}
+
+void ks_rhs_mixed_host(const Frame& f, const double y[6], double pT, double k[6]) {
+  const double rr = sqrt(y[0] * y[0] + y[1] * y[1] + y[2] * y[2]);
+  const double prad = (y[0] * y[3] + y[1] * y[4] + y[2] * y[5]) / rr;
+  if (rr > f.r_fp32 && fabs(prad) > f.turn_frac * fabs(pT))
+    ks_rhs_analytic<float>(f.g, y[0], y[1], y[2], y[3], y[4], y[5], pT, k);
+  else
+    ks_rhs_analytic<double>(f.g, y[0], y[1], y[2], y[3], y[4], y[5], pT, k);
+}
+
 // One lane of the kernel: the slot sequence of k_trace for a single ray.
 template <class M>
 RayResult run_bl(const Frame& f, const Geo& s) {
@@ -36,7 +55,10 @@ RayResult run_bl(const Frame& f, const Geo& s) {
       if (slot < 0 && !m.needs_k1()) continue;
       double y[4], k[5];
       m.input(slot, y);
-      bl_rhs(f.g, y[0], y[1], y[2], y[3], m.pt, m.pphi, k);
+      if (f.precision == KT_PREC_MIXED)
+        bl_rhs_mixed_host(f, y, m.pt, m.pphi, k);
+      else
+        bl_rhs(f.g, y[0], y[1], y[2], y[3], m.pt, m.pphi, k);
       if (m.consume(f, slot, k, &res)) return res;
     }
   }
@@ -67,7 +89,10 @@ RayResult run_ray(const Frame& f, uint32_t pix) {
           if (slot < 0 && !m.needs_k1()) continue;
           double y[6], k[6];
           m.input(slot, y);
-          ks_rhs(f.g, y[0], y[1], y[2], y[3], y[4], y[5], m.pT, k);
+          if (f.precision == KT_PREC_MIXED)
+            ks_rhs_mixed_host(f, y, m.pT, k);
+          else
+            ks_rhs(f.g, y[0], y[1], y[2], y[3], y[4], y[5], m.pT, k);
           if (m.consume(f, slot, k, &res)) return res;
         }
       }

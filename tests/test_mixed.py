@@ -1,0 +1,54 @@
+"""Mixed-precision tracer (KT_PREC_MIXED) on the CPU (its per-ray code
+compiled for the host): analytic Hamiltonian gradient, FP32 right-hand side
+in the far field when the tolerance allows, FP64 integrator.  Its results
+differ from the FP64 oracle by about the oracle's own finite-difference
+noise; the bars below are the ones the GPU tests use."""
+import numpy as np
+import pytest
+
+import golden_lib as G
+import oracle_lib as O
+from test_hostcheck import hc, run  # noqa: F401  (fixture + runner)
+from kerrtracecpp2_b200 import abi
+
+
+def errors(got, want):
+    same = got["outcome"] == want["outcome"]
+    disk = same & (want["outcome"] == 1)
+    eg = np.abs(got["redshift"][disk] - want["redshift"][disk]) / np.abs(want["redshift"][disk])
+    er = np.abs(got["r"][disk] - want["r"][disk]) / np.abs(want["r"][disk])
+    return 1.0 - same.mean(), eg, er
+
+
+CASES = {
+    "cfg2_bl_dopri5": dict(width=48, height=27),
+    "cfg2_bl_rk4": dict(width=48, height=27),
+    "cfg1_ks_rk4": dict(width=64, height=36),
+    "cfg5_ks": dict(width=48, height=48),
+    "kn_charged": dict(),
+    "retrograde": dict(),
+}
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_mixed_close_to_fp64_oracle(hc, name):  # noqa: F811
+    kw = dict(G.cases()[name])
+    kw["precision"] = abi.KT_PREC_MIXED
+    d = abi.frame_desc(**kw)
+    got = run(hc, d)
+    mism, eg, er = errors(got, G.result(name))
+    n = d.width * d.height
+    assert mism * n <= max(1, 1e-3 * n)
+    assert np.median(eg) < 1e-5 and np.percentile(eg, 99) < 1e-3
+    assert np.median(er) < 1e-4
+
+
+def test_mixed_uses_fp32_only_for_loose_tolerance():
+    import kerrtracecpp2_b200 as kt
+
+    strict = kt.frame_derive(abi.frame_desc(precision=abi.KT_PREC_MIXED, tol=1e-10, width=4, height=4))
+    loose = kt.frame_derive(abi.frame_desc(precision=abi.KT_PREC_MIXED, tol=1e-7, width=4, height=4))
+    assert strict.r_fp32 == float("inf")
+    assert loose.r_fp32 == max(4.0, 2.0 * loose.r_horizon)
+    with pytest.raises(kt.KerrTraceError):
+        kt.frame_derive(abi.frame_desc(precision=abi.KT_PREC_MIXED, bundles=1, width=4, height=4))
