@@ -41,7 +41,13 @@ WORKLOADS = {
     "bundles_bl_1080p": dict(chart=1, bundles=1, a=0.998, theta_deg=60.0, width=1920, height=1080),
     "kn_ks_rk4_512": dict(chart=0, a=0.7, Q=0.1, theta_deg=70.0, r_obs=50.0, disk_out=15.0,
                           width=512, height=512),
+    # 64 seeded parameter sets (kerrtracecpp2_b200.random_parameter_sets, seed
+    # 1) at 256^2..1024^2, KS chart requested, RK4 step doubling; one batch.
+    "batch64_ks_rk4_seed1": dict(batch=64, seed=1, width=0, height=0, chart=0),
 }
+# Frames of the batched 720p leg: the headline frame seen from this many
+# camera azimuths, traced as one batch.
+BATCH_720P_FRAMES = 8
 
 # Algorithmic FP64 operations (+, -, *, / and sqrt = 1, fma = 2), counted
 # from the reference's arithmetic as kt_physics.cuh evaluates it:
@@ -150,6 +156,194 @@ def cpu_reference_sample(desc, seconds, flavour="ieee"):
     return len(pix) / dt, pix, threads, kind, sample, res
 
 
+def cpu_reference_batch(descs, seconds, flavour="ieee"):
+    """The reference's CPU path on the same strided fraction of every frame
+    of a batch.  Returns (rays_per_s, threads, kind, sample)."""
+    import oracle_lib as O  # noqa: E402  (tests/oracle_lib.py)
+
+    threads = os.cpu_count() or 1
+    use_ref = O.ref_available(flavour)
+    kind = "reference" if use_ref else "port"
+
+    def run(stride):
+        t0 = time.perf_counter()
+        rays = 0
+        for d in descs:
+            pix = np.arange(0, d.width * d.height, stride, dtype=np.uint32)
+            if use_ref:
+                O.trace_ref(d, flavour, pix=pix, nthreads=threads)
+            else:
+                O.trace_port(d, pix=pix, nthreads=threads)
+            rays += len(pix)
+        return rays, time.perf_counter() - t0
+
+    total = sum(d.width * d.height for d in descs)
+    stride = max(1, total // (len(descs) * max(64, threads * 4)))
+    rays, dt = run(stride)
+    rate = rays / max(dt, 1e-6)
+    stride = max(1, int(total / max(rays, rate * seconds)))
+    rays, dt = run(stride)
+    sample = (f"{rays} of {total} rays: every {stride}th pixel (row-major) of each of the "
+              f"{len(descs)} frames")
+    return rays / dt, threads, kind, sample
+
+
+def bench_batch(args, wl, base_cfg, rank, world, local_rank):
+    """Config 4: 64 seeded parameter sets at uneven resolutions, one CUDA
+    graph launch per step (kt_batch_launch), launch variants and regroup
+    thresholds chosen by the autotuner.  The per-frame kt_trace loop over
+    the same frames is timed beside it."""
+    import kerrtracecpp2_b200 as kt
+    from kerrtracecpp2_b200 import abi
+
+    descs = kt.random_parameter_sets(wl["batch"], seed=wl["seed"])
+    if world > 1:
+        for d in descs:
+            d.phi_deg = 360.0 * rank / world
+    n_rays = sum(d.width * d.height for d in descs)
+    common = {"metric": METRIC, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+              "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+              "vs_baseline": None, "dtype": "f64",
+              "data": "synthetic (seeded random parameter sets; no dataset)", "config": base_cfg}
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        per_step = max(2.0, 120.0 / max(1, args.steps + args.warmup))
+        for _ in range(args.warmup):
+            cpu_reference_batch(descs, per_step)
+        rates, info = [], None
+        for _ in range(args.steps):
+            rate, threads, kind, sample = cpu_reference_batch(descs, per_step)
+            rates.append(rate)
+            info = (threads, kind, sample)
+        v = float(np.mean(rates)) / 1e6
+        line = dict(common, impl="reference", value=v, ms_per_step=1e3 * n_rays / (v * 1e6),
+                    cpu_baseline={"value": v, "unit": "Mrays/s", "cores": info[0], "kind": info[1],
+                                  "sample": info[2]},
+                    e2e={"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0,
+                         "d2h_bytes_per_step": 0})
+        print(json.dumps(line), flush=True)
+        return 0
+
+    import torch
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist  # noqa: F811
+        from datetime import timedelta
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    device = torch.device("cuda", local_rank)
+    torch.cuda.set_device(device)
+    R = kt.Renderer(local_rank)
+    stream = torch.cuda.current_stream(device)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=device)
+    t0 = time.perf_counter()
+    b = R.batch(descs, options=abi.batch_options(autotune=True))
+    tune_s = time.perf_counter() - t0
+    groups = b.groups()
+    for _ in range(max(args.warmup, 1)):
+        flush.fill_(1)
+        b.launch(stream)
+    torch.cuda.synchronize(device)
+
+    def timed(fn):
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize(device)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record(stream)
+        for _ in range(args.steps):
+            flush.fill_(1)
+            fn()
+        ev[1].record(stream)
+        torch.cuda.synchronize(device)
+        t = torch.tensor([ev[0].elapsed_time(ev[1])], dtype=torch.float64, device=device)
+        if dist:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t[0])
+
+    clk_path = os.path.join(tempfile.gettempdir(), f"kt_clocks_{os.getpid()}.csv")
+    proc, fh = start_clock_sampler(clk_path)
+    time.sleep(0.3)
+    total_ms = timed(lambda: b.launch(stream))
+    clocks = stop_clock_sampler(proc, fh, clk_path, local_rank)
+    value = world * args.steps * n_rays / (total_ms * 1e-3) / 1e6
+
+    # The same frames, one kt_trace per frame (the reference's one frame per
+    # render call), into the same outputs.
+    def per_frame():
+        for d, o in zip(descs, b.outs):
+            R.trace(d, o, stream)
+
+    seq_ms = timed(per_frame)
+    seq_value = world * args.steps * n_rays / (seq_ms * 1e-3) / 1e6
+
+    # Algorithmic flops of the BL frames (the FP64 roofline counts cover the
+    # BL integrators); the KS frames' share of the time is not attributed.
+    flops_bl, rays_bl = 0.0, 0
+    for d, o in zip(descs, b.outs):
+        f = ray_flops(d, float(o["steps"].to(torch.int64).sum()),
+                      float(o["attempts"].to(torch.int64).sum()))
+        if f is not None:
+            flops_bl += f
+            rays_bl += d.width * d.height
+
+    # End to end: launch + copy every frame's results to pinned host memory.
+    host = [{k: torch.empty(d.width * d.height, dtype=o[k].dtype, pin_memory=True)
+             for k in ("outcome", "r", "redshift", "magnif", "phi_disk", "theta_esc", "phi_esc")}
+            for d, o in zip(descs, b.outs)]
+    d2h = sum(t.numel() * t.element_size() for h in host for t in h.values())
+    e2e_ms = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize(device)
+        t1 = time.perf_counter()
+        b.launch(stream)
+        for h, o in zip(host, b.outs):
+            for k, t in h.items():
+                t.copy_(o[k], non_blocking=True)
+        torch.cuda.synchronize(device)
+        e2e_ms.append(1e3 * (time.perf_counter() - t1))
+    et = torch.tensor([sum(e2e_ms)], dtype=torch.float64, device=device)
+    if dist:
+        dist.all_reduce(et, op=dist.ReduceOp.MAX)
+    e2e_value = world * args.steps * n_rays / (float(et[0]) * 1e-3) / 1e6
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        rate, threads, kind, sample = cpu_reference_batch(descs, args.cpu_seconds)
+        cpu = {"value": rate / 1e6, "unit": "Mrays/s", "cores": threads, "kind": kind,
+               "sample": sample + ("; reference built -O3 without -ffast-math, glibc libm"
+                                   if kind == "reference" else "")}
+
+    launches = sum(1 + (1 if g["kernel_name"].startswith("ks_rk4") else 0) for g in groups)
+    line = dict(common, value=value, ms_per_step=total_ms / args.steps,
+                mode="plain FP64, bit-identical to the reference CPU path",
+                batch={"frames": len(descs), "rays": n_rays, "graph_launches_per_step": 1,
+                       "autotune_s": tune_s, "groups": groups,
+                       "per_frame_kt_trace": {"value": seq_value, "unit": "Mrays/s",
+                                              "ms_per_step": seq_ms / args.steps},
+                       "speedup_vs_per_frame": value / seq_value},
+                roofline=None, roofline_note=(
+                    f"BL frames: {rays_bl} rays, {flops_bl:.4g} algorithmic FP64 flops per step; "
+                    "KS RHS flops are not counted, so no whole-batch roofline"),
+                cpu_baseline=cpu,
+                e2e={"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": 0,
+                     "d2h_bytes_per_step": d2h,
+                     "call": "kt_batch_launch + copies of every frame's results to pinned host"},
+                clocks=clocks, gpu_launches=args.steps * launches)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    b.close()
+    R.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -160,6 +354,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
     args = ap.parse_args()
     sys.path.insert(0, os.path.join(ROOT, "tests"))
 
@@ -169,6 +364,13 @@ def main():
     from kerrtracecpp2_b200 import abi
 
     wl = dict(WORKLOADS[args.workload])
+    if wl.get("batch"):
+        base_cfg = {"workload": args.workload, "frames": wl["batch"], "seed": wl["seed"],
+                    "sizes": "square, side ~ U{256..1024} step 16", "chart": "KS requested "
+                    "(Lambda != 0 frames run in BL, as the reference does)",
+                    "integrator": "RK4-doubling", "tol": 1e-7,
+                    "parallelism": f"frames{args.gpus}", "l2": "256 MB flush between steps"}
+        return bench_batch(args, wl, base_cfg, rank, world, local_rank)
     base_cfg = {"workload": args.workload, "width": wl["width"], "height": wl["height"],
                 "chart": "BL" if wl.get("chart", 0) == 1 else "KS",
                 "integrator": "DOPRI5" if wl.get("integrator", 0) == 1 else "RK4-doubling",
@@ -299,6 +501,49 @@ def main():
                  else "off at this tolerance (analytic FP64 gradient)"}
         del mout
 
+    # Mixed precision, batched: BATCH_720P_FRAMES frames of this workload (the
+    # camera at azimuths 360*k/F deg) as one autotuned kt_batch, one graph
+    # launch per step.
+    mixed_batched = None
+    if mixed is not None and not args.no_batch:
+        descs = [abi.frame_desc(**dict(wl, precision=abi.KT_PREC_MIXED,
+                                       phi_deg=wl.get("phi_deg", 0.0) + 360.0 * k / BATCH_720P_FRAMES))
+                 for k in range(BATCH_720P_FRAMES)]
+        b = R.batch(descs, options=abi.batch_options(autotune=True))
+        for _ in range(max(args.warmup, 1)):
+            flush.fill_(1)
+            b.launch(stream)
+        torch.cuda.synchronize(device)
+        if dist:
+            dist.barrier()
+        bev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        bev[0].record(stream)
+        for _ in range(args.steps):
+            flush.fill_(1)
+            b.launch(stream)
+        bev[1].record(stream)
+        torch.cuda.synchronize(device)
+        bt = torch.tensor([bev[0].elapsed_time(bev[1])], dtype=torch.float64, device=device)
+        if dist:
+            dist.all_reduce(bt, op=dist.ReduceOp.MAX)
+        bval = world * args.steps * n * BATCH_720P_FRAMES / (float(bt[0]) * 1e-3) / 1e6
+        f0 = b.outs[0]
+        same = f0["outcome"] == out["outcome"]
+        disk = same & (out["outcome"] == 1)
+        eg = ((f0["redshift"] - out["redshift"]).abs() / out["redshift"].abs())[disk]
+        mixed_batched = {"value": bval, "unit": "Mrays/s", "frames": BATCH_720P_FRAMES,
+                         "speedup_vs_fp64": bval / value,
+                         "ms_per_step": float(bt[0]) / args.steps,
+                         "groups": [{k: g[k] for k in ("kernel_name", "variant", "block", "min_blocks",
+                                                        "grid", "refill_min", "best_ms", "default_ms")}
+                                    for g in b.groups()],
+                         "error_vs_fp64_oracle_frame0": {
+                             "class_mismatch_frac": float(1.0 - same.double().mean()),
+                             "g_rel_p50": float(torch.quantile(eg.float(), 0.5)) if eg.numel() else None,
+                             "g_rel_p99": float(torch.quantile(eg.float(), 0.99)) if eg.numel() else None}}
+        b.close()
+        del b
+
     steps_sum = float(out["steps"].to(torch.int64).sum())
     att_sum = float(out["attempts"].to(torch.int64).sum())
     flops = ray_flops(desc, steps_sum, att_sum)
@@ -359,11 +604,13 @@ def main():
             "data": "synthetic (procedural camera frame; no dataset)", "config": base_cfg,
             "mode": "plain FP64, bit-identical to the reference CPU path",
             "roofline": roofline, "cpu_baseline": cpu, "mixed_precision": mixed,
+            "mixed_batched": mixed_batched,
             "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": ctypes.sizeof(desc),
                     "d2h_bytes_per_step": d2h, "call": "kt_trace_host"},
             "clocks": clocks, "gpu_launches": args.steps * (2 if desc.chart == 0 and not desc.bundles
                                                             and abs(desc.Lambda) <= 1e-15 else 1)
-            * (2 if mixed is not None else 1)}
+            * (2 if mixed is not None else 1)
+            + (args.steps * len(mixed_batched["groups"]) if mixed_batched else 0)}
     if rank == 0:
         print(json.dumps(line), flush=True)
     R.close()

@@ -133,8 +133,9 @@ typedef struct kt_context kt_context;
 
 int kt_abi_version(void);
 const char* kt_status_string(kt_status s);
-/* sizeof of kt_frame_desc, kt_frame_derived, kt_geo_soa, kt_color_params
- * (lets bindings check their struct layout); returns the count written. */
+/* sizeof of kt_frame_desc, kt_frame_derived, kt_geo_soa, kt_color_params,
+ * kt_batch_options, kt_batch_group_info (lets bindings check their struct
+ * layout); writes min(n, 6) sizes and returns the count written. */
 int kt_abi_struct_sizes(size_t* sizes, int n);
 
 kt_status kt_create(kt_context** ctx, int device);
@@ -196,6 +197,76 @@ kt_status kt_colorize_host(kt_context* ctx, const kt_geo_soa* geo_host, int32_t 
 kt_status kt_render_host(kt_context* ctx, const kt_frame_desc* desc,
                          const kt_color_params* cp, const uint8_t* bg_rgb_host,
                          int32_t bg_w, int32_t bg_h, uint8_t* rgb_out_host);
+
+/* ---- batches: many frames in one CUDA graph launch ----------------------
+ * No counterpart in the reference renderer, which traces one frame per
+ * render_image call (main.cpp:2209-2478) and loops over frames in its
+ * animation driver.  A batch holds n_frames frames of any sizes, charts,
+ * integrators and precisions, each with its own caller-owned device result
+ * arrays.  kt_batch_create groups the frames by kernel (KS RK4, BL RK4, BL
+ * DOPRI5, bundles; FP64 or mixed), prepares one persistent launch per group
+ * over the group's rays (all its frames in one device ray queue), and
+ * captures the launches into one CUDA graph; kt_batch_launch replays that
+ * graph with a single cudaGraphLaunch.  Results are bit-identical to
+ * kt_trace of each frame.
+ *
+ * Tuning: each group's launch has a block size and register cap (one of
+ * KT_BATCH_VARIANTS compiled variants), a persistent grid, and a regroup
+ * threshold (idle lanes of a warp take new rays only when at least that many
+ * are idle).  Rays per warp is 32: one ray per lane.  With KT_BATCH_AUTOTUNE,
+ * kt_batch_create times every variant x threshold on a sample of the group's
+ * rays (tune_fraction of them, in runs of 256 neighbouring pixels) and keeps
+ * the fastest; the sample's results are written to the outputs.  Otherwise
+ * the variant and threshold are the options' (or the single-frame defaults).
+ *
+ * The graph reads the frames' parameters and output pointers from device
+ * memory owned by the batch: the outputs stay bound to the batch.  Launches
+ * of one batch must not overlap on the device (they share its queues);
+ * different batches are independent. */
+typedef struct kt_batch kt_batch;
+
+#define KT_BATCH_VARIANTS 3
+#define KT_BATCH_AUTOTUNE 1u
+
+typedef struct kt_batch_options {
+  uint32_t flags;          /* KT_BATCH_AUTOTUNE */
+  int32_t variant;         /* -1: per-mode default; else 0..KT_BATCH_VARIANTS-1 */
+  int32_t refill_min;      /* 0: 1 (refill as soon as one lane is idle); 1..32 */
+  int32_t tune_reps;       /* timed repetitions per candidate (>= 1) */
+  double tune_fraction;    /* share of a group's rays in the tuning sample, (0, 1] */
+} kt_batch_options;
+
+typedef struct kt_batch_group_info {
+  int32_t kernel;          /* 0 BL RK4, 1 BL DOPRI5, 2 KS RK4, 3 bundles, 4-6 mixed BL RK4 / BL DOPRI5 / KS RK4 */
+  int32_t n_frames;
+  uint64_t n_rays;
+  int32_t variant;
+  int32_t block;           /* threads per block */
+  int32_t min_blocks;      /* blocks per SM the register cap is set for */
+  int32_t grid;            /* persistent blocks */
+  int32_t refill_min;
+  int32_t rays_per_warp;
+  int32_t tuned;           /* 1: chosen by measurement */
+  int32_t candidates;      /* candidates timed */
+  double sample_rays;      /* rays in the tuning sample */
+  double best_ms;          /* tuning sample time of the chosen candidate */
+  double default_ms;       /* tuning sample time of the default candidate */
+} kt_batch_group_info;
+
+void kt_batch_options_defaults(kt_batch_options* opt);
+/* Creates the batch on the context's device.  descs[i] and outs[i] (device
+ * pointers, as for kt_trace) describe frame i.  opt may be NULL (defaults).
+ * Tuning, when asked for, runs synchronously on the context's stream. */
+kt_status kt_batch_create(kt_context* ctx, const kt_frame_desc* descs,
+                          const kt_geo_soa* outs, int32_t n_frames,
+                          const kt_batch_options* opt, kt_batch** batch);
+/* Traces every frame of the batch: one cudaGraphLaunch on `stream`. */
+kt_status kt_batch_launch(kt_batch* batch, void* stream);
+int32_t kt_batch_group_count(const kt_batch* batch);
+kt_status kt_batch_group(const kt_batch* batch, int32_t i, kt_batch_group_info* info);
+/* Total rays of the batch (sum of width*height). */
+uint64_t kt_batch_rays(const kt_batch* batch);
+void kt_batch_destroy(kt_batch* batch);
 
 /* Measured FP64 FMA throughput of the context's device (GFLOP/s, 2 flops
  * per FMA): the non-tensor FP64 peak the trace kernels are bounded by. */

@@ -23,7 +23,8 @@ from .abi import (ColorParams, FrameDerived, FrameDesc, GeoSoA, color_params, fr
 
 __all__ = ["FrameParams", "IntegratorControls", "Renderer", "load_library", "trace_geodesics",
            "colorize_buffer", "render_image", "frame_derive", "starfield", "KerrTraceError",
-           "frame_desc", "color_params", "FrameDesc", "ColorParams"]
+           "frame_desc", "color_params", "FrameDesc", "ColorParams", "Batch",
+           "random_parameter_sets"]
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_PKG, "libkerrtrace.so")
@@ -87,6 +88,21 @@ def load_library():
     L.kt_kgeo_read_header.restype = ctypes.c_int
     L.kt_kgeo_read.argtypes = [ctypes.c_char_p, ctypes.POINTER(GeoSoA), ctypes.c_int64]
     L.kt_kgeo_read.restype = ctypes.c_int
+    PB = ctypes.POINTER(abi.BatchOptions)
+    L.kt_batch_options_defaults.argtypes = [PB]
+    L.kt_batch_options_defaults.restype = None
+    L.kt_batch_create.argtypes = [P, PD, ctypes.POINTER(GeoSoA), I32, PB, ctypes.POINTER(P)]
+    L.kt_batch_create.restype = ctypes.c_int
+    L.kt_batch_launch.argtypes = [P, P]
+    L.kt_batch_launch.restype = ctypes.c_int
+    L.kt_batch_group_count.argtypes = [P]
+    L.kt_batch_group_count.restype = I32
+    L.kt_batch_group.argtypes = [P, I32, ctypes.POINTER(abi.BatchGroupInfo)]
+    L.kt_batch_group.restype = ctypes.c_int
+    L.kt_batch_rays.argtypes = [P]
+    L.kt_batch_rays.restype = ctypes.c_uint64
+    L.kt_batch_destroy.argtypes = [P]
+    L.kt_batch_destroy.restype = None
     if L.kt_abi_version() != abi.KT_ABI_VERSION:
         raise ImportError("libkerrtrace.so ABI version mismatch")
     _lib = L
@@ -256,6 +272,13 @@ class Renderer:
         _check(self.L.kt_measure_fp64_peak(self.ctx, ctypes.byref(v)), "kt_measure_fp64_peak", self.ctx)
         return v.value
 
+    def batch(self, descs, outs=None, options=None):
+        """kt_batch_create over frames `descs` (a list of kt_frame_desc) with
+        device outputs `outs` (one dict of tensors per frame; allocated when
+        None).  Returns a Batch; Batch.launch() traces every frame with one
+        CUDA graph launch."""
+        return Batch(self, descs, outs, options)
+
     # -- host-buffer entry points --------------------------------------------
     def trace_host(self, desc, counters=True):
         out = _np_soa(desc.width * desc.height, counters)
@@ -272,6 +295,75 @@ class Renderer:
                                      _np_ptr(bgc) if bgc is not None else None, bw, bh, _np_ptr(rgb)),
                "kt_render_host", self.ctx)
         return rgb
+
+
+class Batch:
+    """A kt_batch: frames traced together by one CUDA graph launch."""
+
+    def __init__(self, renderer, descs, outs=None, options=None):
+        self.r = renderer
+        self.L = renderer.L
+        self.descs = list(descs)
+        n = len(self.descs)
+        self.outs = outs if outs is not None else [renderer.alloc(d.width * d.height)
+                                                   for d in self.descs]
+        arr_d = (FrameDesc * n)(*self.descs)
+        arr_o = (GeoSoA * n)(*[_soa_struct(o, _torch_ptr) for o in self.outs])
+        self.handle = ctypes.c_void_p()
+        opt = options if options is not None else abi.batch_options()
+        _check(self.L.kt_batch_create(renderer.ctx, arr_d, arr_o, n, ctypes.byref(opt),
+                                      ctypes.byref(self.handle)), "kt_batch_create", renderer.ctx)
+
+    @property
+    def n_rays(self):
+        return int(self.L.kt_batch_rays(self.handle))
+
+    def groups(self):
+        out = []
+        for i in range(self.L.kt_batch_group_count(self.handle)):
+            gi = abi.BatchGroupInfo()
+            _check(self.L.kt_batch_group(self.handle, i, ctypes.byref(gi)), "kt_batch_group")
+            d = gi.as_dict()
+            d["kernel_name"] = abi.BATCH_KERNELS[gi.kernel]
+            out.append(d)
+        return out
+
+    def launch(self, stream=None):
+        _check(self.L.kt_batch_launch(self.handle, Renderer._stream(stream)), "kt_batch_launch",
+               self.r.ctx)
+
+    def close(self):
+        if self.handle:
+            self.L.kt_batch_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def random_parameter_sets(n=64, seed=1, side_min=256, side_max=1024, lambdas=(0.0, 1e-4)):
+    """Seeded random frames for batch rendering: a ~ U[0, 0.998], Q ~ U[0, 0.4]
+    redrawn until a^2 + Q^2 < 1, Lambda drawn from `lambdas`, theta_obs ~
+    U[5, 89] degrees, r_obs ~ U[20, 200], square frames of side ~ U{side_min
+    .. side_max} (multiples of 16); KS chart, RK4 step doubling and the CLI's
+    other defaults.  Returns a list of kt_frame_desc."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        a = rng.uniform(0.0, 0.998)
+        q = rng.uniform(0.0, 0.4)
+        while a * a + q * q >= 1.0:
+            q = rng.uniform(0.0, 0.4)
+        lam = float(lambdas[int(rng.integers(len(lambdas)))])
+        th = rng.uniform(5.0, 89.0)
+        r_obs = rng.uniform(20.0, 200.0)
+        side = int(rng.integers(side_min // 16, side_max // 16 + 1)) * 16
+        out.append(frame_desc(a=a, Q=q, Lambda=lam, theta_deg=th, r_obs=r_obs, width=side,
+                              height=side, chart=KT_CHART_KS, integrator=KT_RK4_DOUBLING))
+    return out
 
 
 _default = {}

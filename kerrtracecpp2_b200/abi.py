@@ -84,6 +84,49 @@ class ColorParams(ctypes.Structure):
     ]
 
 
+KT_BATCH_VARIANTS = 3
+KT_BATCH_AUTOTUNE = 1
+
+
+class BatchOptions(ctypes.Structure):
+    _fields_ = [
+        ("flags", ctypes.c_uint32), ("variant", ctypes.c_int32), ("refill_min", ctypes.c_int32),
+        ("tune_reps", ctypes.c_int32), ("tune_fraction", ctypes.c_double),
+    ]
+
+
+class BatchGroupInfo(ctypes.Structure):
+    _fields_ = [
+        ("kernel", ctypes.c_int32), ("n_frames", ctypes.c_int32), ("n_rays", ctypes.c_uint64),
+        ("variant", ctypes.c_int32), ("block", ctypes.c_int32), ("min_blocks", ctypes.c_int32),
+        ("grid", ctypes.c_int32), ("refill_min", ctypes.c_int32), ("rays_per_warp", ctypes.c_int32),
+        ("tuned", ctypes.c_int32), ("candidates", ctypes.c_int32),
+        ("sample_rays", ctypes.c_double), ("best_ms", ctypes.c_double),
+        ("default_ms", ctypes.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+# Kernel of a batch group (kt_batch_group_info.kernel).
+BATCH_KERNELS = ["bl_rk4", "bl_dopri5", "ks_rk4", "bundles", "bl_rk4_mixed", "bl_dopri5_mixed",
+                 "ks_rk4_mixed"]
+
+
+def batch_options(autotune=False, **kw):
+    """kt_batch_options with the library's defaults (per-mode variant,
+    refill as soon as one lane is idle, 2 timed repetitions, 1/16 sample)."""
+    o = BatchOptions()
+    o.flags = KT_BATCH_AUTOTUNE if autotune else 0
+    o.variant, o.refill_min, o.tune_reps, o.tune_fraction = -1, 0, 2, 1.0 / 16.0
+    for k, v in kw.items():
+        if not hasattr(o, k):
+            raise KeyError(f"kt_batch_options has no field {k!r}")
+        setattr(o, k, v)
+    return o
+
+
 # Result arrays of one frame: name -> numpy dtype, in kt_geo_soa order.
 GEO_FIELDS = [
     ("outcome", "u1"), ("r", "f8"), ("redshift", "f8"), ("magnif", "f8"), ("phi_disk", "f8"),

@@ -10,6 +10,7 @@ reference has a separate multiply and add).
 Usage: python kerrtracecpp2_b200/build.py [--force] [--verbose]
 """
 import argparse
+import concurrent.futures
 import os
 import subprocess
 import sys
@@ -30,9 +31,9 @@ CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", "-Wextr
              "-I", os.path.join(CUDA_HOME, "include")]
 
 CU_SOURCES = ["kt_kernels.cu", "kt_noalloc.cu", "kt_mixed.cu"]
-CXX_SOURCES = ["kt_frame.cpp", "kt_api.cpp", "kt_io.cpp", "kt_compat.cpp"]
+CXX_SOURCES = ["kt_frame.cpp", "kt_api.cpp", "kt_batch.cpp", "kt_io.cpp", "kt_compat.cpp"]
 HEADERS = ["ktmath.h", "ktmath_consts.h", "kt_physics.cuh", "kt_machines.cuh", "kt_internal.h",
-           "kt_frame.h", "kt_trace_kernel.cuh"]
+           "kt_frame.h", "kt_context.h", "kt_trace_kernel.cuh"]
 # Per-file compile flags: the exact kernels keep every multiply and add of
 # the reference's arithmetic separate; the mixed-precision kernels are not
 # compared bit for bit and use FMA contraction.
@@ -63,21 +64,24 @@ def build(force=False, verbose=False):
         os.path.join(ROOT, "include", "kerrtrace.h"),
         os.path.join(ROOT, "include", "kerrtrace_cuda_render.h")]
     objs = []
-    ptxas_log = []
+    jobs = []  # (command, is_nvcc)
     for src in CU_SOURCES:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src + ".o")
         if force or newer(o, [s] + hdrs):
             flags = [f for f in NVCC_FLAGS if not (src in CU_FLAGS and f == "--fmad=false")]
-            ptxas_log.append(run([NVCC] + flags + CU_FLAGS.get(src, []) + ["-c", s, "-o", o],
-                                 verbose))
+            jobs.append(([NVCC] + flags + CU_FLAGS.get(src, []) + ["-c", s, "-o", o], True))
         objs.append(o)
     for src in CXX_SOURCES:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src + ".o")
         if force or newer(o, [s] + hdrs):
-            run(["g++"] + CXX_FLAGS + ["-c", s, "-o", o], verbose)
+            jobs.append((["g++"] + CXX_FLAGS + ["-c", s, "-o", o], False))
         objs.append(o)
+    # Translation units compile independently: run them in parallel.
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        outs = list(ex.map(lambda j: run(j[0], verbose), jobs))
+    ptxas_log = [o for o, (_, is_nvcc) in zip(outs, jobs) if is_nvcc]
     if force or newer(LIB, objs):
         run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs, verbose)
     cli_src = os.path.join(PKG, "cli", "kerr_tracer.cpp")

@@ -92,6 +92,41 @@ cudaError_t launch_trace_mixed(Mode mode, const Frame& f, const OutSoA& out, con
                                uint32_t* queue, const Fallback& fb, const LaunchShape& shape,
                                cudaStream_t stream);
 
+// ---- batches of frames (k_trace_batch, kt_trace_kernel.cuh) ---------------
+// Ray g of a batch is pixel g - offsets[k] of frame k, where offsets[k] <= g
+// < offsets[k+1]; frames[k] and outs[k] are that frame's constants and
+// result arrays.  Rays traced: list[0..n) (batch ray indices) or 0..n-1 when
+// list is NULL; the count is *n_dev when n_dev is set.  Idle lanes of a warp
+// take new rays only when at least `refill_min` lanes are idle (or the warp
+// is empty), so more lanes share the new rays' first RHS evaluations.
+struct BatchRays {
+  const Frame* frames;
+  const OutSoA* outs;
+  const uint64_t* offsets;
+  int n_frames;
+  int refill_min;
+  const uint32_t* list;
+  const uint32_t* n_dev;
+  uint64_t n;
+};
+
+// Launch-shape variants the batch autotuner chooses from: (threads per
+// block, minimum resident blocks per SM).  The second number sets the
+// register cap: 65536 / (threads x blocks) per thread, rounded down to the
+// allocation granule (112 for 64 x 9, 80 for 64 x 12, none for 128 x 1).
+constexpr int kBatchVariants = 3;
+constexpr int kBatchBlock[kBatchVariants] = {64, 128, 64};
+constexpr int kBatchMinBlocks[kBatchVariants] = {9, 1, 12};
+
+// Shape (grid at full occupancy) and launch of variant `variant` of `mode`.
+// The KS fallback list receives batch ray indices.
+cudaError_t batch_shape(Mode mode, int variant, int device, LaunchShape* shape);
+cudaError_t launch_batch(Mode mode, int variant, const BatchRays& br, uint32_t* queue,
+                         const Fallback& fb, const LaunchShape& s, cudaStream_t st);
+cudaError_t batch_shape_mixed(Mode mode, int variant, int device, LaunchShape* shape);
+cudaError_t launch_batch_mixed(Mode mode, int variant, const BatchRays& br, uint32_t* queue,
+                               const Fallback& fb, const LaunchShape& s, cudaStream_t st);
+
 // FP64 throughput probe: n_iter dependent FMA chains per thread.
 cudaError_t launch_fp64_probe(double* out, int n_iter, int grid, int block, cudaStream_t stream);
 

@@ -11,7 +11,7 @@ struct ModeBLRk4 {
   static constexpr int kSlots = BLRk4::kSlots;
   BLRk4* m;
   __device__ __forceinline__ bool needs_k1() const { return m->needs_k1(); }
-  __device__ __forceinline__ bool start(const Frame& f, uint32_t pix, uint32_t, const Fallback&) {
+  __device__ __forceinline__ bool start(const Frame& f, uint32_t pix, uint32_t, uint32_t, const Fallback&) {
     m->init(f, camera_ray(f, pix));
     return true;
   }
@@ -28,7 +28,7 @@ struct ModeBLDopri5 {
   static constexpr int kSlots = BLDopri5::kSlots;
   BLDopri5* m;
   __device__ __forceinline__ bool needs_k1() const { return m->needs_k1(); }
-  __device__ __forceinline__ bool start(const Frame& f, uint32_t pix, uint32_t, const Fallback&) {
+  __device__ __forceinline__ bool start(const Frame& f, uint32_t pix, uint32_t, uint32_t, const Fallback&) {
     m->init(f, camera_ray(f, pix));
     return true;
   }
@@ -46,13 +46,13 @@ struct ModeKSRk4 {
   KSRk4* m;
   __device__ __forceinline__ bool needs_k1() const { return m->needs_k1(); }
   __device__ __forceinline__ bool start(const Frame& f, uint32_t pix, uint32_t out_slot,
-                                        const Fallback& fb) {
+                                        uint32_t fb_key, const Fallback& fb) {
     if (m->init(f, camera_ray(f, pix))) return true;
     // init_ks_state failed: the ray is traced in the BL chart by a second
     // launch over the fallback list.
     const uint32_t i = atomicAdd(fb.count, 1u);
-    fb.pix[i] = pix;
-    fb.slot[i] = out_slot;
+    fb.pix[i] = fb_key;
+    if (fb.slot) fb.slot[i] = out_slot;
     return false;
   }
   __device__ __forceinline__ bool slot(const Frame& f, int s, RayResult* res) {
@@ -68,7 +68,7 @@ struct ModeBundle {
   static constexpr int kSlots = Bundle::kSlots;
   Bundle* m;
   __device__ __forceinline__ bool needs_k1() const { return m->needs_k1(); }
-  __device__ __forceinline__ bool start(const Frame& f, uint32_t pix, uint32_t, const Fallback&) {
+  __device__ __forceinline__ bool start(const Frame& f, uint32_t pix, uint32_t, uint32_t, const Fallback&) {
     m->init(f, (int)(pix % (uint32_t)f.cam.W), (int)(pix / (uint32_t)f.cam.W));
     return true;
   }
@@ -111,6 +111,27 @@ cudaError_t launch_trace(Mode mode, const Frame& f, const OutSoA& out, const Ray
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
+}
+
+cudaError_t batch_shape(Mode mode, int variant, int device, LaunchShape* shape) {
+  switch (mode) {
+    case kModeBLRk4: return batch_shape<ModeBLRk4>(variant, device, shape);
+    case kModeBLDopri5: return batch_shape<ModeBLDopri5>(variant, device, shape);
+    case kModeKSRk4: return batch_shape<ModeKSRk4>(variant, device, shape);
+    case kModeBundle: return batch_shape<ModeBundle>(variant, device, shape);
+    default: return batch_shape_mixed(mode, variant, device, shape);
+  }
+}
+
+cudaError_t launch_batch(Mode mode, int variant, const BatchRays& br, uint32_t* queue,
+                         const Fallback& fb, const LaunchShape& s, cudaStream_t st) {
+  switch (mode) {
+    case kModeBLRk4: return batch_launch<ModeBLRk4>(variant, br, queue, fb, s, st);
+    case kModeBLDopri5: return batch_launch<ModeBLDopri5>(variant, br, queue, fb, s, st);
+    case kModeKSRk4: return batch_launch<ModeKSRk4>(variant, br, queue, fb, s, st);
+    case kModeBundle: return batch_launch<ModeBundle>(variant, br, queue, fb, s, st);
+    default: return launch_batch_mixed(mode, variant, br, queue, fb, s, st);
+  }
 }
 
 // ---- colour ------------------------------------------------------------------

@@ -34,7 +34,7 @@ struct ModeBLRk4Mixed {
   static constexpr int kSlots = BLRk4::kSlots;
   BLRk4* m;
   __device__ __forceinline__ bool needs_k1() const { return m->needs_k1(); }
-  __device__ __forceinline__ bool start(const Frame& f, uint32_t pix, uint32_t, const Fallback&) {
+  __device__ __forceinline__ bool start(const Frame& f, uint32_t pix, uint32_t, uint32_t, const Fallback&) {
     m->init(f, camera_ray(f, pix));
     return true;
   }
@@ -51,7 +51,7 @@ struct ModeBLDopri5Mixed {
   static constexpr int kSlots = BLDopri5::kSlots;
   BLDopri5* m;
   __device__ __forceinline__ bool needs_k1() const { return m->needs_k1(); }
-  __device__ __forceinline__ bool start(const Frame& f, uint32_t pix, uint32_t, const Fallback&) {
+  __device__ __forceinline__ bool start(const Frame& f, uint32_t pix, uint32_t, uint32_t, const Fallback&) {
     m->init(f, camera_ray(f, pix));
     return true;
   }
@@ -70,11 +70,11 @@ struct ModeKSRk4Mixed {
   KSRk4* m;
   __device__ __forceinline__ bool needs_k1() const { return m->needs_k1(); }
   __device__ __forceinline__ bool start(const Frame& f, uint32_t pix, uint32_t out_slot,
-                                        const Fallback& fb) {
+                                        uint32_t fb_key, const Fallback& fb) {
     if (m->init(f, camera_ray(f, pix))) return true;
     const uint32_t i = atomicAdd(fb.count, 1u);
-    fb.pix[i] = pix;
-    fb.slot[i] = out_slot;
+    fb.pix[i] = fb_key;
+    if (fb.slot) fb.slot[i] = out_slot;
     return false;
   }
   __device__ __forceinline__ bool slot(const Frame& f, int s, RayResult* res) {
@@ -115,6 +115,25 @@ cudaError_t launch_trace_mixed(Mode mode, const Frame& f, const OutSoA& out, con
     case kModeBLRk4Mixed: return launch_one<ModeBLRk4Mixed>(f, out, rl, queue, fb, s, stream);
     case kModeBLDopri5Mixed: return launch_one<ModeBLDopri5Mixed>(f, out, rl, queue, fb, s, stream);
     case kModeKSRk4Mixed: return launch_one<ModeKSRk4Mixed>(f, out, rl, queue, fb, s, stream);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t batch_shape_mixed(Mode mode, int variant, int device, LaunchShape* shape) {
+  switch (mode) {
+    case kModeBLRk4Mixed: return batch_shape<ModeBLRk4Mixed>(variant, device, shape);
+    case kModeBLDopri5Mixed: return batch_shape<ModeBLDopri5Mixed>(variant, device, shape);
+    case kModeKSRk4Mixed: return batch_shape<ModeKSRk4Mixed>(variant, device, shape);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_batch_mixed(Mode mode, int variant, const BatchRays& br, uint32_t* queue,
+                               const Fallback& fb, const LaunchShape& s, cudaStream_t st) {
+  switch (mode) {
+    case kModeBLRk4Mixed: return batch_launch<ModeBLRk4Mixed>(variant, br, queue, fb, s, st);
+    case kModeBLDopri5Mixed: return batch_launch<ModeBLDopri5Mixed>(variant, br, queue, fb, s, st);
+    case kModeKSRk4Mixed: return batch_launch<ModeKSRk4Mixed>(variant, br, queue, fb, s, st);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -100,7 +100,7 @@ __global__ void __launch_bounds__(Shape<ModeT>::kBlock, Shape<ModeT>::kMinBlocks
           if (idx < n) {
             const uint32_t pix = rl.pix ? rl.pix[idx] : idx;
             out_slot = rl.slot ? rl.slot[idx] : idx;
-            active = mode.start(f, pix, out_slot, fb);
+            active = mode.start(f, pix, out_slot, pix, fb);
           }
         }
       }
@@ -140,6 +140,122 @@ static cudaError_t shape_for(int device, LaunchShape* shape) {
   shape->grid = sms * per_sm;
   shape->smem = smem;
   return cudaSuccess;
+}
+
+// ---- batches of frames -----------------------------------------------------
+// Many frames (parameter sets, resolutions) in one persistent launch
+// (BatchRays, kt_internal.h).  Each lane carries its own frame index; the
+// frame constants are read from global memory through L1.  The loop is
+// k_trace's, with a refill threshold and a binary search for a new ray's
+// frame.
+
+// Frame of batch ray g: the last k with offsets[k] <= g.
+__device__ __forceinline__ int batch_frame_of(const BatchRays& br, uint64_t g) {
+  int lo = 0, hi = br.n_frames - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (br.offsets[mid] <= g)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+template <class ModeT, int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB)
+    k_trace_batch(const BatchRays br, uint32_t* __restrict__ queue, const Fallback fb) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  using Rec = SmemRecord<typename ModeT::Machine>;
+  ModeT mode;
+  mode.m = &reinterpret_cast<Rec*>(smem)[threadIdx.x].m;
+  bool active = false;
+  int fi = 0;
+  uint32_t pix = 0;
+  const uint64_t n = br.n_dev ? (uint64_t)*br.n_dev : br.n;
+  const unsigned lane = threadIdx.x & 31u;
+  bool exhausted = false;
+  for (;;) {
+    if (!exhausted) {
+      const unsigned need = __ballot_sync(kFull, !active);
+      const int idle = __popc(need);
+      if (need && (idle >= br.refill_min || need == kFull)) {
+        const int leader = __ffs(need) - 1;
+        unsigned base = 0;
+        if ((int)lane == leader) base = atomicAdd(queue, (unsigned)idle);
+        base = __shfl_sync(kFull, base, leader);
+        if ((uint64_t)base + (uint64_t)idle >= n) exhausted = true;
+        if (!active) {
+          const uint64_t idx = (uint64_t)base + (unsigned)__popc(need & ((1u << lane) - 1u));
+          if (idx < n) {
+            const uint32_t g = br.list ? br.list[idx] : (uint32_t)idx;
+            fi = batch_frame_of(br, g);
+            pix = (uint32_t)(g - br.offsets[fi]);
+            active = mode.start(br.frames[fi], pix, pix, g, fb);
+          }
+        }
+      }
+    }
+    if (!__any_sync(kFull, active)) {
+      if (exhausted) break;
+      continue;
+    }
+    const Frame& f = br.frames[fi];
+    KT_ROLLED
+    for (int s = -1; s < ModeT::kSlots; ++s) {
+      const bool part = active && (s >= 0 || mode.needs_k1());
+      if (s < 0 && !__any_sync(kFull, part)) continue;
+      if (part) {
+        RayResult res;
+        if (mode.slot(f, s, &res)) {
+          write_result(br.outs[fi], pix, res);
+          active = false;
+        }
+      }
+    }
+  }
+}
+
+template <class ModeT, int BLOCK, int MINB>
+static cudaError_t batch_shape_for(int device, LaunchShape* shape) {
+  int sms = 0, per_sm = 0;
+  cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  if (e != cudaSuccess) return e;
+  const size_t smem = smem_bytes<ModeT>(BLOCK);
+  e = cudaFuncSetAttribute(k_trace_batch<ModeT, BLOCK, MINB>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace_batch<ModeT, BLOCK, MINB>,
+                                                    BLOCK, smem);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) per_sm = 1;
+  shape->block = BLOCK;
+  shape->grid = sms * per_sm;
+  shape->smem = smem;
+  return cudaSuccess;
+}
+
+// One case per entry of kBatchBlock / kBatchMinBlocks (kt_internal.h).
+template <class ModeT>
+static cudaError_t batch_shape(int variant, int device, LaunchShape* s) {
+  switch (variant) {
+    case 0: return batch_shape_for<ModeT, 64, 9>(device, s);
+    case 1: return batch_shape_for<ModeT, 128, 1>(device, s);
+    case 2: return batch_shape_for<ModeT, 64, 12>(device, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <class ModeT>
+static cudaError_t batch_launch(int variant, const BatchRays& br, uint32_t* queue,
+                                const Fallback& fb, const LaunchShape& s, cudaStream_t st) {
+  switch (variant) {
+    case 0: k_trace_batch<ModeT, 64, 9><<<s.grid, s.block, s.smem, st>>>(br, queue, fb); break;
+    case 1: k_trace_batch<ModeT, 128, 1><<<s.grid, s.block, s.smem, st>>>(br, queue, fb); break;
+    case 2: k_trace_batch<ModeT, 64, 12><<<s.grid, s.block, s.smem, st>>>(br, queue, fb); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
 }
 
 }  // namespace kt

@@ -40,10 +40,42 @@ def test_exports_every_declared_symbol():
 
 
 def test_struct_layout(L):
-    sizes = (ctypes.c_size_t * 4)()
-    assert L.kt_abi_struct_sizes(sizes, 4) == 4
+    sizes = (ctypes.c_size_t * 6)()
+    assert L.kt_abi_struct_sizes(sizes, 6) == 6
     assert list(sizes) == [ctypes.sizeof(abi.FrameDesc), ctypes.sizeof(abi.FrameDerived),
-                           ctypes.sizeof(abi.GeoSoA), ctypes.sizeof(abi.ColorParams)]
+                           ctypes.sizeof(abi.GeoSoA), ctypes.sizeof(abi.ColorParams),
+                           ctypes.sizeof(abi.BatchOptions), ctypes.sizeof(abi.BatchGroupInfo)]
+
+
+def test_batch_options_defaults(L):
+    o = abi.BatchOptions()
+    L.kt_batch_options_defaults(ctypes.byref(o))
+    ref = abi.batch_options()
+    assert [getattr(o, f) for f, _ in o._fields_] == [getattr(ref, f) for f, _ in ref._fields_]
+
+
+def test_batch_entry_points_reject_null(L):
+    d = abi.frame_desc(width=4, height=4)
+    h = ctypes.c_void_p()
+    assert L.kt_batch_create(None, ctypes.byref(d), None, 1, None, ctypes.byref(h)) == \
+        abi.KT_ERR_INVALID_ARGUMENT
+    assert L.kt_batch_launch(None, None) == abi.KT_ERR_INVALID_ARGUMENT
+    assert L.kt_batch_group_count(None) == 0 and L.kt_batch_rays(None) == 0
+    gi = abi.BatchGroupInfo()
+    assert L.kt_batch_group(None, 0, ctypes.byref(gi)) == abi.KT_ERR_INVALID_ARGUMENT
+    L.kt_batch_destroy(None)
+
+
+def test_random_parameter_sets():
+    a = kt.random_parameter_sets(64, seed=1)
+    b = kt.random_parameter_sets(64, seed=1)
+    assert [bytes(x) for x in a] == [bytes(x) for x in b]
+    assert len(a) == 64
+    for d in a:
+        assert 0 <= d.a <= 0.998 and 0 <= d.Q <= 0.4 and d.a ** 2 + d.Q ** 2 < 1
+        assert d.Lambda in (0.0, 1e-4) and 5 <= d.theta_deg <= 89 and 20 <= d.r_obs <= 200
+        assert d.width == d.height and 256 <= d.width <= 1024 and d.width % 16 == 0
+        assert d.chart == abi.KT_CHART_KS and d.integrator == abi.KT_RK4_DOUBLING
 
 
 def test_defaults_match_reference_cli(L):
