@@ -62,8 +62,12 @@ enum { KT_SOLVER_STANDARD = 0, KT_SOLVER_SEMI_ANALYTIC = 1, KT_SOLVER_ELLIPTIC_C
 /* Arithmetic of the trace.  FP64: the reference's arithmetic bit for bit.
  * MIXED: analytic Hamiltonian gradient, FP32 right-hand side in the far
  * field when tol >= 1e-8, FP64 state, error control and events; agrees with
- * FP64 to about the reference's own finite-difference noise. */
-enum { KT_PREC_FP64 = 0, KT_PREC_MIXED = 1 };
+ * FP64 to about the reference's own finite-difference noise.
+ * SMOOTH: the differentiable tracer (kt_vjp, kt_l2_grad): FP64, analytic
+ * Hamiltonian gradient, analytic BL->KS Jacobian, disk crossing solved to
+ * convergence, RK4 step doubling only; its outputs are smooth functions of
+ * the frame parameters between changes of the accept/reject pattern. */
+enum { KT_PREC_FP64 = 0, KT_PREC_MIXED = 1, KT_PREC_SMOOTH = 2 };
 /* kt_frame_desc.flags: theta_deg, phi_deg and fov_deg hold radians (the
  * reference's CameraParams_CUDA carries radians, gpu/cuda/tracer.cuh:16-20). */
 #define KT_FLAG_ANGLES_RADIANS 1u
@@ -134,8 +138,8 @@ typedef struct kt_context kt_context;
 int kt_abi_version(void);
 const char* kt_status_string(kt_status s);
 /* sizeof of kt_frame_desc, kt_frame_derived, kt_geo_soa, kt_color_params,
- * kt_batch_options, kt_batch_group_info (lets bindings check their struct
- * layout); writes min(n, 6) sizes and returns the count written. */
+ * kt_batch_options, kt_batch_group_info, kt_grad_stats (lets bindings check
+ * their struct layout); writes min(n, 7) sizes and returns the count written. */
 int kt_abi_struct_sizes(size_t* sizes, int n);
 
 kt_status kt_create(kt_context** ctx, int device);
@@ -267,6 +271,50 @@ kt_status kt_batch_group(const kt_batch* batch, int32_t i, kt_batch_group_info* 
 /* Total rays of the batch (sum of width*height). */
 uint64_t kt_batch_rays(const kt_batch* batch);
 void kt_batch_destroy(kt_batch* batch);
+
+/* ---- gradients: the discrete adjoint of the smooth tracer ---------------
+ * No counterpart in the reference renderer.  The gradient is that of the
+ * KT_PREC_SMOOTH tracer (whatever desc->precision says) with respect to the
+ * frame parameters, in this order (units of kt_frame_desc): */
+enum {
+  KT_GRAD_A = 0, KT_GRAD_Q = 1, KT_GRAD_LAMBDA = 2, KT_GRAD_THETA = 3, KT_GRAD_R_OBS = 4,
+  KT_GRAD_DISK_OUT = 5, KT_GRAD_COUNT = 6
+};
+/* Point-sampled pixels: g and r_hit of a disk pixel do not depend on the
+ * disk's outer radius (it only decides which rays hit), so the
+ * KT_GRAD_DISK_OUT entry is 0.  In the KS chart (Lambda = 0 only; any other
+ * Lambda sends the frame to the BL chart, main.cpp:2033-2040) the Lambda
+ * entry is the derivative of the BL-chart trace of the same frame, which
+ * is what the tracer computes for Lambda != 0; it takes a second pass
+ * unless KT_GRAD_SKIP_LAMBDA is given (the entry is then 0). */
+#define KT_GRAD_SKIP_LAMBDA 1u
+
+typedef struct kt_grad_stats {
+  double loss;           /* kt_l2_grad: the loss; kt_vjp: 0 */
+  int64_t grad_pixels;   /* disk pixels whose reverse sweep ran */
+  int64_t bl_pixels;     /* pixels traced in the BL chart (first pass) */
+  int64_t unrecorded;    /* disk pixels with a cotangent but > 131072 steps: no gradient */
+  float ms_main;         /* device time of the gradient pass */
+  float ms_lambda;       /* device time of the BL pass for Lambda (0 if none) */
+} kt_grad_stats;
+
+/* Vector-Jacobian product: grad[k] = sum over pixels p of
+ * cot_redshift[p] dg_p/dtheta_k + cot_r[p] d r_hit,p/dtheta_k over the disk
+ * pixels (device arrays of width*height doubles; either may be NULL).
+ * `out` (device SoA, optional) receives the smooth forward results.  grad
+ * and stats are host memory; the call returns when they are written. */
+kt_status kt_vjp(kt_context* ctx, const kt_frame_desc* desc, const double* cot_redshift,
+                 const double* cot_r, const kt_geo_soa* out, uint32_t flags,
+                 double grad[KT_GRAD_COUNT], kt_grad_stats* stats, void* stream);
+
+/* L2 image loss against a target frame (device SoA of a smooth trace with
+ * other parameters): L = sum over pixels that are disk hits in both frames
+ * of w_g (g - g_t)^2 + w_r (r_hit - r_t)^2, and its gradient, in one fused
+ * forward + reverse pass per pixel. */
+kt_status kt_l2_grad(kt_context* ctx, const kt_frame_desc* desc, const kt_geo_soa* target,
+                     double w_g, double w_r, const kt_geo_soa* out, uint32_t flags,
+                     double* loss, double grad[KT_GRAD_COUNT], kt_grad_stats* stats,
+                     void* stream);
 
 /* Measured FP64 FMA throughput of the context's device (GFLOP/s, 2 flops
  * per FMA): the non-tensor FP64 peak the trace kernels are bounded by. */

@@ -25,6 +25,7 @@ KT_SOLVER_SEMI_ANALYTIC = 1
 KT_SOLVER_ELLIPTIC_CLOSED = 2
 KT_PREC_FP64 = 0
 KT_PREC_MIXED = 1
+KT_PREC_SMOOTH = 2
 KT_OUT_ESCAPED = 0
 KT_OUT_DISK = 1
 KT_OUT_HORIZON = 2
@@ -125,6 +126,22 @@ def batch_options(autotune=False, **kw):
             raise KeyError(f"kt_batch_options has no field {k!r}")
         setattr(o, k, v)
     return o
+
+
+# Gradient entries (kt_vjp / kt_l2_grad), in kt_frame_desc units.
+GRAD_NAMES = ["a", "Q", "Lambda", "theta_deg", "r_obs", "disk_out"]
+KT_GRAD_COUNT = 6
+KT_GRAD_SKIP_LAMBDA = 1
+
+
+class GradStats(ctypes.Structure):
+    _fields_ = [
+        ("loss", ctypes.c_double), ("grad_pixels", ctypes.c_int64), ("bl_pixels", ctypes.c_int64),
+        ("unrecorded", ctypes.c_int64), ("ms_main", ctypes.c_float), ("ms_lambda", ctypes.c_float),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 # Result arrays of one frame: name -> numpy dtype, in kt_geo_soa order.

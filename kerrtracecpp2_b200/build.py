@@ -30,10 +30,12 @@ NVCC_FLAGS = ARCH + ["-O3", "-std=c++17", "--fmad=false", "-lineinfo", "-Xptxas"
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", "-Wextra",
              "-I", os.path.join(CUDA_HOME, "include")]
 
-CU_SOURCES = ["kt_kernels.cu", "kt_noalloc.cu", "kt_mixed.cu"]
-CXX_SOURCES = ["kt_frame.cpp", "kt_api.cpp", "kt_batch.cpp", "kt_io.cpp", "kt_compat.cpp"]
+CU_SOURCES = ["kt_kernels.cu", "kt_noalloc.cu", "kt_mixed.cu", "kt_adjoint.cu"]
+CXX_SOURCES = ["kt_frame.cpp", "kt_api.cpp", "kt_batch.cpp", "kt_grad.cpp", "kt_io.cpp",
+               "kt_compat.cpp"]
 HEADERS = ["ktmath.h", "ktmath_consts.h", "kt_physics.cuh", "kt_machines.cuh", "kt_internal.h",
-           "kt_frame.h", "kt_context.h", "kt_trace_kernel.cuh"]
+           "kt_frame.h", "kt_context.h", "kt_trace_kernel.cuh", "kt_dual.cuh", "kt_smooth.cuh",
+           "kt_smray.cuh", "kt_adjoint.h"]
 # Per-file compile flags: the exact kernels keep every multiply and add of
 # the reference's arithmetic separate; the mixed-precision kernels are not
 # compared bit for bit and use FMA contraction.

@@ -1,0 +1,24 @@
+// kt_adjoint.h -- launchers of the smooth tracer and of its adjoint
+// (kt_adjoint.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "kt_internal.h"
+#include "kt_smray.cuh"
+
+namespace kt {
+
+// Smooth trace of pixels 0..n-1 into `out` (outcome NULL: no outputs); with
+// `job`, the reverse sweeps and the per-ray contributions too.  `queue` must
+// be zero on entry.
+cudaError_t launch_smooth(const Frame& f, const OutSoA& out, uint32_t n, const SmJob* job,
+                          uint32_t* queue, int device, cudaStream_t st);
+
+// out[kGSlots] = fixed-order sums over the rays of contrib[kGSlots][n];
+// `partial` holds grad_sum_scratch_doubles() - kGSlots doubles.
+cudaError_t launch_grad_sum(const double* contrib, uint32_t n, double* partial, double* out,
+                            cudaStream_t st);
+size_t grad_sum_scratch_doubles();
+
+}  // namespace kt

@@ -12,6 +12,7 @@
 #include <string>
 
 #include "../../include/kerrtrace.h"
+#include "kt_adjoint.h"
 #include "kt_context.h"
 #include "kt_frame.h"
 #include "kt_internal.h"
@@ -33,6 +34,14 @@ kt_status shape(kt_context* ctx, kt::Mode m, kt::LaunchShape* s) {
 // whose KS initialisation failed, main.cpp:1537-1538).
 kt_status run_trace(kt_context* ctx, const kt::Frame& f, const kt::OutSoA& out,
                     const kt::RayList& rl, uint64_t n_max, cudaStream_t st) {
+  if (f.precision == KT_PREC_SMOOTH) {
+    if (rl.pix || rl.slot || rl.n_dev)
+      return fail(ctx, KT_ERR_UNSUPPORTED, "the smooth tracer traces whole frames only");
+    KT_CUDA(ctx, cudaMemsetAsync(ctx->d_counters, 0, 4 * sizeof(uint32_t), st), "reset queue");
+    KT_CUDA(ctx, kt::launch_smooth(f, out, rl.n, nullptr, ctx->d_counters, ctx->device, st),
+            "smooth kernel launch");
+    return KT_OK;
+  }
   const kt::Mode m = kt::frame_mode(f);
   kt::LaunchShape s;
   kt_status r = shape(ctx, m, &s);
@@ -79,11 +88,12 @@ const char* kt_status_string(kt_status s) {
 }
 
 int kt_abi_struct_sizes(size_t* sizes, int n) {
-  const size_t v[6] = {sizeof(kt_frame_desc),    sizeof(kt_frame_derived),
+  const size_t v[7] = {sizeof(kt_frame_desc),    sizeof(kt_frame_derived),
                        sizeof(kt_geo_soa),       sizeof(kt_color_params),
-                       sizeof(kt_batch_options), sizeof(kt_batch_group_info)};
+                       sizeof(kt_batch_options), sizeof(kt_batch_group_info),
+                       sizeof(kt_grad_stats)};
   int k = 0;
-  for (; k < n && k < 6; ++k) sizes[k] = v[k];
+  for (; k < n && k < 7; ++k) sizes[k] = v[k];
   return k;
 }
 
@@ -162,6 +172,8 @@ void kt_destroy(kt_context* ctx) {
   cudaFree(ctx->d_fb);
   cudaFree(ctx->d_stage);
   cudaFree(ctx->d_bg);
+  cudaFree(ctx->d_grad);
+  cudaFree(ctx->d_gsum);
   delete ctx;
 }
 

@@ -268,6 +268,9 @@ kt_status kt_batch_create(kt_context* ctx, const kt_frame_desc* descs, const kt_
       ctx->err = "frame " + std::to_string(i) + ": " + ctx->err;
       return r;
     }
+    if (frames[i].precision == KT_PREC_SMOOTH)
+      return fail(ctx, KT_ERR_UNSUPPORTED,
+                  "frame " + std::to_string(i) + ": the smooth tracer does not run in batches");
     if (!out_complete(&outs[i]))
       return fail(ctx, KT_ERR_INVALID_ARGUMENT,
                   "frame " + std::to_string(i) + ": output pointer is NULL");

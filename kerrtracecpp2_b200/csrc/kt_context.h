@@ -21,6 +21,11 @@ struct kt_context {
   size_t stage_cap = 0;
   unsigned char* d_bg = nullptr;
   size_t bg_cap = 0;
+  // gradients: per-ray contributions [kGSlots][n], sums, host copy
+  double* d_grad = nullptr;
+  size_t grad_cap = 0;
+  double* d_gsum = nullptr;
+  size_t gsum_cap = 0;
   cudaStream_t stream = nullptr;
   kt::LaunchShape shapes[kt::kNumModes];
   bool shape_ok[kt::kNumModes] = {};

@@ -166,12 +166,18 @@ kt_status prepare_frame(const kt_frame_desc* d, Frame* f, kt_frame_derived* dv, 
     *err = "only --solver-mode standard runs on this backend";
     return KT_ERR_UNSUPPORTED;
   }
-  if (d->precision != KT_PREC_FP64 && d->precision != KT_PREC_MIXED) {
-    *err = "precision must be KT_PREC_FP64 or KT_PREC_MIXED";
+  if (d->precision != KT_PREC_FP64 && d->precision != KT_PREC_MIXED &&
+      d->precision != KT_PREC_SMOOTH) {
+    *err = "precision must be KT_PREC_FP64, KT_PREC_MIXED or KT_PREC_SMOOTH";
     return KT_ERR_INVALID_ARGUMENT;
   }
-  if (d->precision == KT_PREC_MIXED && d->bundles) {
-    *err = "the mixed-precision tracer has no ray-bundle mode";
+  if (d->precision != KT_PREC_FP64 && d->bundles) {
+    *err = "the mixed-precision and smooth tracers have no ray-bundle mode";
+    return KT_ERR_UNSUPPORTED;
+  }
+  if (d->precision == KT_PREC_SMOOTH && d->integrator == KT_DOPRI5 &&
+      (d->chart == KT_CHART_BL || fabs(d->Lambda) > 1e-15)) {
+    *err = "the smooth tracer integrates with RK4 step doubling only";
     return KT_ERR_UNSUPPORTED;
   }
   if ((d->flags & ~(uint32_t)KT_FLAG_ANGLES_RADIANS) != 0) {

@@ -1,0 +1,145 @@
+// kt_grad.cpp -- kt_vjp and kt_l2_grad: the discrete adjoint of the smooth
+// tracer behind the C ABI (kernels in kt_adjoint.cu).
+#include <cuda_runtime.h>
+#include <string.h>
+
+#include <string>
+
+#include "../../include/kerrtrace.h"
+#include "kt_adjoint.h"
+#include "kt_context.h"
+#include "kt_frame.h"
+
+using namespace ktc;
+
+namespace {
+
+constexpr double kDeg = 3.141592653589793 / 180.0;
+
+struct EventPair {
+  cudaEvent_t a = nullptr, b = nullptr;
+  ~EventPair() {
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+  }
+};
+
+// One gradient pass: launch, reduce, copy the kGSlots sums to `sums`.
+kt_status grad_pass(kt_context* ctx, const kt::Frame& f, const kt::OutSoA& out, uint32_t n,
+                    const kt::SmCot& cot, bool force_bl, cudaStream_t st, double* sums, float* ms) {
+  kt::SmJob job;
+  job.cot = cot;
+  job.force_bl = force_bl ? 1 : 0;
+  job.contrib = ctx->d_grad;
+  EventPair ev;
+  KT_CUDA(ctx, cudaEventCreate(&ev.a), "event");
+  KT_CUDA(ctx, cudaEventCreate(&ev.b), "event");
+  KT_CUDA(ctx, cudaMemsetAsync(ctx->d_counters, 0, 4 * sizeof(uint32_t), st), "reset queue");
+  KT_CUDA(ctx, cudaEventRecord(ev.a, st), "event");
+  KT_CUDA(ctx, kt::launch_smooth(f, out, n, &job, ctx->d_counters, ctx->device, st), "adjoint kernel launch");
+  KT_CUDA(ctx, kt::launch_grad_sum(ctx->d_grad, n, ctx->d_gsum + kt::kGSlots, ctx->d_gsum, st),
+          "gradient sum");
+  KT_CUDA(ctx, cudaEventRecord(ev.b, st), "event");
+  KT_CUDA(ctx, cudaMemcpyAsync(sums, ctx->d_gsum, kt::kGSlots * sizeof(double), cudaMemcpyDeviceToHost, st),
+          "copy gradient");
+  KT_CUDA(ctx, cudaStreamSynchronize(st), "gradient pass");
+  KT_CUDA(ctx, cudaEventElapsedTime(ms, ev.a, ev.b), "event time");
+  return KT_OK;
+}
+
+kt_status grad_run(kt_context* ctx, const kt_frame_desc* desc_in, const kt::SmCot& cot,
+                   const kt_geo_soa* out_soa, uint32_t flags, double* grad, kt_grad_stats* stats,
+                   cudaStream_t st, const char* who) {
+  if (!ctx) return KT_ERR_INVALID_ARGUMENT;
+  if (!desc_in || !grad) return fail(ctx, KT_ERR_INVALID_ARGUMENT, std::string(who) + ": NULL pointer");
+  if (flags & ~KT_GRAD_SKIP_LAMBDA) return fail(ctx, KT_ERR_INVALID_ARGUMENT, std::string(who) + ": unknown flags");
+  if (out_soa && !out_complete(out_soa))
+    return fail(ctx, KT_ERR_INVALID_ARGUMENT, std::string(who) + ": incomplete output SoA");
+  kt_frame_desc desc = *desc_in;
+  desc.precision = KT_PREC_SMOOTH;
+  kt::Frame f;
+  kt_status r = kt::prepare_frame(&desc, &f, nullptr, &ctx->err);
+  if (r != KT_OK) return r;
+  DeviceGuard g(ctx->device);
+  const uint64_t n = (uint64_t)desc.width * (uint64_t)desc.height;
+  r = ensure(ctx, (void**)&ctx->d_grad, &ctx->grad_cap, n * kt::kGSlots * sizeof(double), "gradient buffer");
+  if (r != KT_OK) return r;
+  r = ensure(ctx, (void**)&ctx->d_gsum, &ctx->gsum_cap, kt::grad_sum_scratch_doubles() * sizeof(double),
+             "gradient sums");
+  if (r != KT_OK) return r;
+  kt::OutSoA out;
+  memset(&out, 0, sizeof out);
+  if (out_soa) out = to_out(out_soa);
+  double s[kt::kGSlots], sl[kt::kGSlots];
+  float ms = 0.f, ms_l = 0.f;
+  r = grad_pass(ctx, f, out, (uint32_t)n, cot, false, st, s, &ms);
+  if (r != KT_OK) return r;
+  double lambda = s[kt::kGLambda];
+  if (f.chart == KT_CHART_KS) {
+    lambda = 0.0;
+    if (!(flags & KT_GRAD_SKIP_LAMBDA)) {
+      kt::OutSoA none;
+      memset(&none, 0, sizeof none);
+      r = grad_pass(ctx, f, none, (uint32_t)n, cot, true, st, sl, &ms_l);
+      if (r != KT_OK) return r;
+      lambda = sl[kt::kGLambda];
+    }
+  }
+  const double th_scale = (desc.flags & KT_FLAG_ANGLES_RADIANS) ? 1.0 : kDeg;
+  grad[KT_GRAD_A] = s[kt::kGA];
+  grad[KT_GRAD_Q] = s[kt::kGQ];
+  grad[KT_GRAD_LAMBDA] = lambda;
+  grad[KT_GRAD_THETA] = s[kt::kGTheta] * th_scale;
+  grad[KT_GRAD_R_OBS] = s[kt::kGRobs];
+  grad[KT_GRAD_DISK_OUT] = 0.0;
+  if (stats) {
+    memset(stats, 0, sizeof *stats);
+    stats->loss = s[kt::kGLoss];
+    stats->grad_pixels = (int64_t)s[kt::kGNumGrad];
+    stats->bl_pixels = (int64_t)s[kt::kGNumBL];
+    stats->unrecorded = (int64_t)s[kt::kGNumUnrecorded];
+    stats->ms_main = ms;
+    stats->ms_lambda = ms_l;
+  }
+  return KT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+kt_status kt_vjp(kt_context* ctx, const kt_frame_desc* desc, const double* cot_redshift,
+                 const double* cot_r, const kt_geo_soa* out, uint32_t flags, double* grad,
+                 kt_grad_stats* stats, void* stream) {
+  kt::SmCot cot;
+  memset(&cot, 0, sizeof cot);
+  cot.mode = 1;
+  cot.g = cot_redshift;
+  cot.r = cot_r;
+  return grad_run(ctx, desc, cot, out, flags, grad, stats, (cudaStream_t)stream, "kt_vjp");
+}
+
+kt_status kt_l2_grad(kt_context* ctx, const kt_frame_desc* desc, const kt_geo_soa* target, double w_g,
+                     double w_r, const kt_geo_soa* out, uint32_t flags, double* loss, double* grad,
+                     kt_grad_stats* stats, void* stream) {
+  if (!ctx) return KT_ERR_INVALID_ARGUMENT;
+  if (!target || !target->outcome || !target->redshift || !target->r || !loss)
+    return fail(ctx, KT_ERR_INVALID_ARGUMENT, "kt_l2_grad: NULL pointer");
+  if (!kt::finite(w_g) || !kt::finite(w_r))
+    return fail(ctx, KT_ERR_INVALID_ARGUMENT, "kt_l2_grad: non-finite weight");
+  kt::SmCot cot;
+  memset(&cot, 0, sizeof cot);
+  cot.mode = 2;
+  cot.t_out = target->outcome;
+  cot.t_g = target->redshift;
+  cot.t_r = target->r;
+  cot.w_g = w_g;
+  cot.w_r = w_r;
+  kt_grad_stats st_local;
+  kt_grad_stats* sp = stats ? stats : &st_local;
+  const kt_status r = grad_run(ctx, desc, cot, out, flags, grad, sp, (cudaStream_t)stream, "kt_l2_grad");
+  if (r == KT_OK) *loss = sp->loss;
+  return r;
+}
+
+}  // extern "C"

@@ -617,14 +617,22 @@ struct SmCot {
   double w_g, w_r;
 };
 
-// Gradient slots of one pixel (and of the frame after the sum).
-enum : int {
-  kGA = 0, kGQ = 1, kGLambda = 2, kGTheta = 3, kGRobs = 4, kGDiskOut = 5, kGLoss = 6, kGFlags = 7,
-  kGSlots = 8
+// A launch of the smooth kernel with gradients: cotangent source, chart
+// override (trace every ray in the BL chart) and the [kGSlots][n] output.
+struct SmJob {
+  SmCot cot;
+  int force_bl;
+  double* contrib;
 };
-// kGFlags bits
-constexpr double kGFlagBL = 1.0;          // traced in the BL chart
-constexpr double kGFlagNoRecord = 2.0;    // disk hit after > 131072 steps: no gradient
+
+// Gradient slots of one pixel (and of the frame after the sum): dL/d(a, Q,
+// Lambda, theta_obs [rad], r_obs), the loss, and counts: pixels whose
+// reverse sweep ran, pixels traced in the BL chart, disk hits with a
+// cotangent but more than 131072 steps (no gradient).
+enum : int {
+  kGA = 0, kGQ = 1, kGLambda = 2, kGTheta = 3, kGRobs = 4, kGLoss = 5, kGNumGrad = 6, kGNumBL = 7,
+  kGNumUnrecorded = 8, kGSlots = 9
+};
 
 // One pixel of the smooth tracer: outputs into *o; with a cotangent source,
 // the pixel's loss and gradient into g[kGSlots] (theta in radians).
@@ -648,7 +656,7 @@ KT_HD void sm_pixel(const Frame& f, uint32_t pix, bool force_bl, const SmCot& co
                    : sm_trace<ChartBL>(f, P, ybl, cbl, f.cam.phi_obs, o, &ev, ck, &k1, &nck);
   if (!kGrad) return;
   for (int q = 0; q < kGSlots; ++q) g[q] = 0.0;
-  g[kGFlags] = ks ? 0.0 : kGFlagBL;
+  g[kGNumBL] = ks ? 0.0 : 1.0;
   if (o->outcome != kOutDisk) return;
   double gbar = 0.0, rbar = 0.0;
   if (cot.mode == 1) {
@@ -663,9 +671,10 @@ KT_HD void sm_pixel(const Frame& f, uint32_t pix, bool force_bl, const SmCot& co
   }
   if (gbar == 0.0 && rbar == 0.0) return;
   if (N == 0) {
-    g[kGFlags] = g[kGFlags] + kGFlagNoRecord;
+    g[kGNumUnrecorded] = 1.0;
     return;
   }
+  g[kGNumGrad] = 1.0;
   double ybar[kSmMaxN], cbar[2], pbar[kSmPrm];
   typedef Dual<5> D5;
   SmPrm<D5> Pd;

@@ -126,3 +126,57 @@ extern "C" int hc_trace_pixels(const kt_frame_desc* d, int64_t n, const uint32_t
   }
   return 0;
 }
+
+// The smooth tracer and its adjoint on the host (kt_smray.cuh compiled by
+// g++ with the kernels' floating-point flags): pixels pix[0..n) of the
+// frame; cotangent mode 0 (forward only), 1 (arrays over the frame's pixels)
+// or 2 (L2 against target arrays); contrib[kGSlots][n] per listed pixel.
+#include "../kerrtracecpp2_b200/csrc/kt_smray.cuh"
+
+extern "C" int hc_smooth_pixels(const kt_frame_desc* d, int64_t n, const uint32_t* pix, int mode,
+                                int force_bl, const double* cot_g, const double* cot_r,
+                                const uint8_t* t_out, const double* t_g, const double* t_r,
+                                double w_g, double w_r, uint8_t* outcome, double* r, double* red,
+                                double* phi_disk, double* th_esc, double* ph_esc, uint32_t* steps,
+                                uint32_t* attempts, double* contrib) {
+  kt_frame_desc dd = *d;
+  dd.precision = KT_PREC_SMOOTH;
+  Frame f;
+  std::string err;
+  if (prepare_frame(&dd, &f, nullptr, &err) != KT_OK) return 1;
+  SmCot cot;
+  memset(&cot, 0, sizeof cot);
+  cot.mode = mode;
+  cot.g = cot_g;
+  cot.r = cot_r;
+  cot.t_out = t_out;
+  cot.t_g = t_g;
+  cot.t_r = t_r;
+  cot.w_g = w_g;
+  cot.w_r = w_r;
+#pragma omp parallel
+  {
+    SmScratch* sc = new SmScratch;
+#pragma omp for schedule(dynamic, 2)
+    for (int64_t i = 0; i < n; ++i) {
+      RayResult o;
+      double g[kGSlots];
+      if (mode == 0)
+        sm_pixel<false>(f, pix[i], force_bl != 0, cot, &o, g, nullptr);
+      else
+        sm_pixel<true>(f, pix[i], force_bl != 0, cot, &o, g, sc);
+      outcome[i] = (uint8_t)o.outcome;
+      r[i] = o.r;
+      red[i] = o.red;
+      phi_disk[i] = o.phi_disk;
+      th_esc[i] = o.th_esc;
+      ph_esc[i] = o.ph_esc;
+      steps[i] = o.steps;
+      attempts[i] = o.attempts;
+      if (mode != 0 && contrib)
+        for (int q = 0; q < kGSlots; ++q) contrib[q * n + i] = g[q];
+    }
+    delete sc;
+  }
+  return 0;
+}

@@ -1,0 +1,127 @@
+"""The smooth tracer and its adjoint on the GPU (kt_trace with
+KT_PREC_SMOOTH, kt_vjp, kt_l2_grad): bit-identical to the host build of the
+same code (smooth_lib), and on config 5 (512x512 KS, a=0.7, Q=0.1,
+theta=70, r_obs=50, disk ISCO-15, L2 loss against the same tracer at a=0.72,
+theta=71) the gradient against central differences with h = 1e-6 of the
+loss restricted to the pixels on which every stencil is smooth (see
+test_smooth.py)."""
+import numpy as np
+import pytest
+
+import smooth_lib as S
+from kerrtracecpp2_b200 import abi
+
+pytestmark = pytest.mark.gpu
+
+CFG5 = dict(chart=0, a=0.7, Q=0.1, Lambda=0.0, theta_deg=70.0, r_obs=50.0, disk_out=15.0)
+KNDS = dict(chart=1, a=0.9, Q=0.3, Lambda=1e-4, r_obs=60.0, theta_deg=85.0, disk_out=20.0)
+FIELDS = ["outcome", "r", "redshift", "phi_disk", "theta_esc", "phi_esc", "steps", "attempts"]
+
+
+def to_np(out):
+    import torch
+
+    torch.cuda.synchronize()
+    got = {k: (v.cpu().numpy() if v is not None else None) for k, v in out.items()}
+    got["steps"] = got["steps"].view(np.uint32)
+    got["attempts"] = got["attempts"].view(np.uint32)
+    return got
+
+
+def smooth_gpu(renderer, kw):
+    return to_np(renderer.trace(abi.frame_desc(precision=abi.KT_PREC_SMOOTH, **kw)))
+
+
+@pytest.mark.parametrize("kw", [dict(CFG5, width=96, height=96), dict(KNDS, width=96, height=54),
+                                dict(CFG5, width=77, height=31, tol=1e-10)],
+                         ids=["cfg5_ks", "knds_bl", "cfg5_tight"])
+def test_smooth_trace_gpu_equals_host(renderer, kw):
+    got = smooth_gpu(renderer, kw)
+    want, _ = S.smooth(abi.frame_desc(**kw))
+    for f in FIELDS:
+        assert np.array_equal(got[f], want[f]), f
+
+
+@pytest.mark.parametrize("kw", [dict(CFG5, width=64, height=64), dict(KNDS, width=64, height=36)],
+                         ids=["ks", "bl"])
+def test_vjp_gpu_equals_host(renderer, kw):
+    import torch
+
+    d = abi.frame_desc(**kw)
+    n = d.width * d.height
+    rng = np.random.default_rng(7)
+    cg, cr = rng.normal(size=n), rng.normal(size=n)
+    out = renderer.alloc(n)
+    grad, st = renderer.vjp(d, torch.from_numpy(cg).cuda(), torch.from_numpy(cr).cuda(), out=out)
+    fwd, c = S.smooth(d, mode=1, cot_g=cg, cot_r=cr)
+    got = to_np(out)
+    for f in FIELDS:
+        assert np.array_equal(got[f], fwd[f]), f
+    h = c.sum(axis=1)
+    want = [h[0], h[1], h[2], h[3] * np.pi / 180, h[4], 0.0]
+    if kw["chart"] == 0:
+        _, cl = S.smooth(d, mode=1, cot_g=cg, cot_r=cr, force_bl=True)
+        want[2] = cl.sum(axis=1)[2]
+    np.testing.assert_allclose(grad, want, rtol=1e-11, atol=1e-12 * np.abs(want).max())
+    assert st["grad_pixels"] == int(h[6]) and st["unrecorded"] == 0
+    assert st["bl_pixels"] == (0 if kw["chart"] == 0 else n)
+
+
+def test_config5_l2_gradient_against_central_differences(renderer):
+    """512x512, tol 1e-7: kt_l2_grad's loss equals the loss of its own
+    forward, and the VJP with the loss's cotangents on the smooth pixels
+    agrees with central differences (h = 1e-6; theta in radians) of that
+    loss to 1e-4 relative; the measured agreement is printed."""
+    import torch
+
+    base = dict(CFG5, width=512, height=512)
+    n = 512 * 512
+    wg, wr = 1.0, 0.01
+    tgt_t = renderer.trace(abi.frame_desc(precision=abi.KT_PREC_SMOOTH, **dict(base, a=0.72, theta_deg=71.0)))
+    tgt = to_np(tgt_t)
+    out = renderer.alloc(n)
+    loss, grad_l2, st = renderer.l2_grad(abi.frame_desc(**base), tgt_t, wg, wr, out=out)
+    b0 = to_np(out)
+    m_all = (b0["outcome"] == 1) & (tgt["outcome"] == 1)
+    want_loss = np.sum(wg * (b0["redshift"][m_all] - tgt["redshift"][m_all]) ** 2 +
+                       wr * (b0["r"][m_all] - tgt["r"][m_all]) ** 2)
+    assert loss == pytest.approx(want_loss, rel=1e-12)
+    assert st["grad_pixels"] == m_all.sum()
+
+    h = 1e-6
+    steps = {"a": h, "Q": h, "Lambda": 1e-7, "theta_deg": np.degrees(h), "r_obs": h}
+    bl0 = smooth_gpu(renderer, dict(base, chart=1))
+    ok = m_all.copy()
+    renders = {}
+    for k, hk in steps.items():
+        o0 = bl0 if k == "Lambda" else b0
+        op = smooth_gpu(renderer, dict(base, **{k: base[k] + hk}))
+        om = smooth_gpu(renderer, dict(base, **{k: base[k] - hk}))
+        renders[k] = (op, om, hk)
+        ok &= (o0["outcome"] == 1) & (op["outcome"] == 1) & (om["outcome"] == 1)
+        for f in ("steps", "attempts"):
+            ok &= (op[f] == o0[f]) & (om[f] == o0[f])
+        for f in ("redshift", "r"):
+            ok &= np.abs(op[f] - 2 * o0[f] + om[f]) <= 1e-8 + 0.01 * np.abs(op[f] - om[f])
+
+    def loss_on(o):
+        return np.sum(wg * (o["redshift"][ok] - tgt["redshift"][ok]) ** 2 +
+                      wr * (o["r"][ok] - tgt["r"][ok]) ** 2)
+
+    def cot(o):
+        return (torch.from_numpy(np.where(ok, 2 * wg * (o["redshift"] - tgt["redshift"]), 0.0)).cuda(),
+                torch.from_numpy(np.where(ok, 2 * wr * (o["r"] - tgt["r"]), 0.0)).cuda())
+
+    d = abi.frame_desc(**base)
+    g, _ = renderer.vjp(d, *cot(b0), flags=abi.KT_GRAD_SKIP_LAMBDA)
+    gl, _ = renderer.vjp(abi.frame_desc(**dict(base, chart=1)), *cot(bl0))
+    adj = {"a": g[0], "Q": g[1], "Lambda": gl[2], "theta_deg": g[3], "r_obs": g[4]}
+    worst = 0.0
+    for k, (op, om, hk) in renders.items():
+        fd = (loss_on(op) - loss_on(om)) / (2 * hk)
+        rel = abs(adj[k] - fd) / abs(fd)
+        worst = max(worst, rel)
+        print(f"{k}: adjoint {adj[k]:.10g} central difference {fd:.10g} rel {rel:.2e}")
+    print(f"smooth pixels {ok.sum()} of {m_all.sum()} disk pixels; worst rel {worst:.2e}")
+    assert worst <= 1e-4
+    assert grad_l2[abi.GRAD_NAMES.index("disk_out")] == 0.0

@@ -1,0 +1,190 @@
+"""The smooth tracer (KT_PREC_SMOOTH) and its discrete adjoint, compiled for
+the host (smooth_lib): close to the reference's own path (the oracle),
+per-ray derivatives against central differences, the L2 image-loss
+gradient against central differences of the loss, and the VJP's algebraic
+properties.  The GPU kernels are checked against this host build bit for
+bit in test_gpu_grad.py.
+
+Finite differences of a point-sampled image are only meaningful where the
+stencil stays on one smooth piece of the renderer: a pixel that changes
+class, changes which disk crossing it takes, or changes its accept/reject
+pattern between the stencil's renders is a discontinuity, and is left out
+of the FD reference (`smooth_pixels`)."""
+import numpy as np
+import pytest
+
+import oracle_lib as O
+import smooth_lib as S
+from kerrtracecpp2_b200 import abi
+
+CFG5 = dict(chart=0, a=0.7, Q=0.1, theta_deg=70.0, r_obs=50.0, disk_out=15.0)
+KNDS = dict(chart=1, a=0.9, Q=0.3, Lambda=1e-4, r_obs=60.0, theta_deg=85.0, disk_out=20.0)
+PARAMS = ["a", "Q", "Lambda", "theta_deg", "r_obs"]
+
+
+@pytest.mark.parametrize("kw", [dict(CFG5, width=96, height=96), dict(KNDS, width=96, height=54),
+                                dict(chart=0, a=0.5, fov_deg=45.0, width=160, height=90)],
+                         ids=["cfg5_ks", "knds_bl", "cfg1_ks"])
+def test_smooth_tracer_close_to_reference_path(kw):
+    """The smooth tracer changes three numerical details of the reference's
+    algorithm; the images agree to the reference's own discretisation
+    noise (its 8-bisection crossing moves r_hit by up to ~2e-5)."""
+    d = abi.frame_desc(**kw)
+    sm, _ = S.smooth(d)
+    ex = O.trace_port(d)
+    same = sm["outcome"] == ex["outcome"]
+    assert same.mean() >= 0.999
+    disk = same & (ex["outcome"] == 1)
+    eg = np.abs(sm["redshift"][disk] - ex["redshift"][disk]) / ex["redshift"][disk]
+    er = np.abs(sm["r"][disk] - ex["r"][disk]) / ex["r"][disk]
+    assert np.median(eg) < 1e-5 and np.percentile(eg, 99) < 1e-4
+    assert np.median(er) < 2e-5 and er.max() < 1e-4
+
+
+def _step(name, h):
+    """Central-difference step of a parameter: theta in radians; Lambda at
+    most 1e-7 (its natural scale is 1/r^2 ~ 1e-3 of the others')."""
+    if name == "theta_deg":
+        return np.degrees(h)
+    return min(h, 1e-7) if name == "Lambda" else h
+
+
+def smooth_pixels(base, names, h, pix=None):
+    """Renders of the central-difference stencil of each parameter and the
+    pixels on which every stencil stays on one smooth piece."""
+    b0, _ = S.smooth(abi.frame_desc(**base), pix=pix)
+    bl0 = None
+    ok = b0["outcome"] == 1
+    renders = {}
+    for k in names:
+        o0 = b0
+        if k == "Lambda" and base.get("chart", 0) == 0 and base.get("Lambda", 0.0) == 0.0:
+            if bl0 is None:  # Lambda != 0 sends a KS frame to the BL chart
+                bl0, _ = S.smooth(abi.frame_desc(**dict(base, chart=1)), pix=pix)
+            o0 = bl0
+        ok &= o0["outcome"] == 1
+        hk = _step(k, h)
+        op, _ = S.smooth(abi.frame_desc(**dict(base, **{k: base.get(k, 0.0) + hk})), pix=pix)
+        om, _ = S.smooth(abi.frame_desc(**dict(base, **{k: base.get(k, 0.0) - hk})), pix=pix)
+        renders[k] = (op, om, o0, hk)
+        ok &= (op["outcome"] == 1) & (om["outcome"] == 1)
+        for f in ("steps", "attempts"):
+            ok &= (op[f] == o0[f]) & (om[f] == o0[f])
+        for f in ("redshift", "r"):
+            ok &= np.abs(op[f] - 2 * o0[f] + om[f]) <= 1e-8 + 0.01 * np.abs(op[f] - om[f])
+    return b0, bl0, renders, ok
+
+
+@pytest.mark.parametrize("frame,names", [
+    (dict(CFG5, width=64, height=64, tol=1e-10), ["a", "Q", "theta_deg", "r_obs"]),
+    (dict(KNDS, width=64, height=36, tol=1e-10), PARAMS),
+], ids=["ks", "bl_lambda"])
+def test_per_ray_gradients_match_central_differences(frame, names):
+    """d g / d theta and d r_hit / d theta of single rays from the adjoint
+    (unit cotangents) against central differences with h = 1e-4."""
+    n = frame["width"] * frame["height"]
+    pix = np.arange(0, n, 7, dtype=np.uint32)
+    b0, _, renders, ok = smooth_pixels(frame, names, 1e-4, pix)
+    d = abi.frame_desc(**frame)
+    ones, zeros = np.ones(n), np.zeros(n)
+    _, cg = S.smooth(d, pix=pix, mode=1, cot_g=ones, cot_r=zeros)
+    _, cr = S.smooth(d, pix=pix, mode=1, cot_g=zeros, cot_r=ones)
+    assert ok.sum() >= 40
+    slot = {"a": 0, "Q": 1, "Lambda": 2, "theta_deg": 3, "r_obs": 4}
+    for k in names:
+        op, om, _, hk = renders[k]
+        scale = np.pi / 180 if k == "theta_deg" else 1.0
+        for f, c in (("redshift", cg), ("r", cr)):
+            fd = ((op[f] - om[f]) / (2 * hk))[ok]
+            adj = c[slot[k]][ok] * scale
+            tol = 2e-4 * np.abs(fd) + 1e-5 * (np.abs(fd).max() + 1e-12)
+            bad = np.abs(adj - fd) > tol
+            assert not bad.any(), (k, f, np.flatnonzero(ok)[bad][:5], adj[bad][:5], fd[bad][:5])
+
+
+def l2_setup(width, tol):
+    base = dict(CFG5, Lambda=0.0, width=width, height=width, tol=tol)
+    tgt, _ = S.smooth(abi.frame_desc(**dict(base, a=0.72, theta_deg=71.0)))
+    return base, tgt
+
+
+@pytest.mark.parametrize("h", [1e-6, 1e-5])
+def test_l2_loss_gradient_matches_central_differences(h):
+    """Config-5 geometry at 128x128, tol 1e-7: the gradient of the L2 loss
+    of (g, r_hit) against a target frame, restricted to the pixels on which
+    every stencil is smooth, against central differences of that loss.
+    Lambda's entry is the BL chart's (cotangents from the BL trace)."""
+    base, tgt = l2_setup(128, 1e-7)
+    wg, wr = 1.0, 0.01
+    names = PARAMS if h == 1e-6 else ["a", "Q", "theta_deg", "r_obs"]
+    b0, bl0, renders, ok = smooth_pixels(base, names, h)
+    mask = ok & (tgt["outcome"] == 1)
+    assert mask.sum() > 3000
+
+    def loss(o):
+        return np.sum(wg * (o["redshift"][mask] - tgt["redshift"][mask]) ** 2 +
+                      wr * (o["r"][mask] - tgt["r"][mask]) ** 2)
+
+    def cot(o):
+        return (np.where(mask, 2 * wg * (o["redshift"] - tgt["redshift"]), 0.0),
+                np.where(mask, 2 * wr * (o["r"] - tgt["r"]), 0.0))
+
+    d = abi.frame_desc(**base)
+    _, c = S.smooth(d, mode=1, cot_g=cot(b0)[0], cot_r=cot(b0)[1])
+    grad = c.sum(axis=1)
+    adj = {"a": grad[0], "Q": grad[1], "theta_deg": grad[3] * np.pi / 180, "r_obs": grad[4]}
+    if "Lambda" in names:
+        cgl, crl = cot(bl0)
+        _, cl = S.smooth(d, mode=1, cot_g=cgl, cot_r=crl, force_bl=True)
+        adj["Lambda"] = cl.sum(axis=1)[2]
+    for k in names:
+        op, om, _, hk = renders[k]
+        fd = (loss(op) - loss(om)) / (2 * hk)
+        assert abs(adj[k] - fd) <= 5e-4 * abs(fd), (k, adj[k], fd)
+
+
+def test_fused_l2_equals_vjp_with_l2_cotangents():
+    """kt_l2_grad's fused cotangents are exactly 2 w (x - x_target) on the
+    pixels that are disk hits in both frames."""
+    base, tgt = l2_setup(48, 1e-7)
+    d = abi.frame_desc(**base)
+    o, cf = S.smooth(d, mode=2, target=tgt, w_g=1.0, w_r=0.25)
+    m = (o["outcome"] == 1) & (tgt["outcome"] == 1)
+    cg = np.where(m, 2.0 * (o["redshift"] - tgt["redshift"]), 0.0)
+    cr = np.where(m, 2.0 * 0.25 * (o["r"] - tgt["r"]), 0.0)
+    _, cv = S.smooth(d, mode=1, cot_g=cg, cot_r=cr)
+    assert np.array_equal(cf[:5], cv[:5])
+    loss = np.sum((o["redshift"][m] - tgt["redshift"][m]) ** 2 + 0.25 * (o["r"][m] - tgt["r"][m]) ** 2)
+    assert cf[5].sum() == pytest.approx(loss, rel=1e-14)
+
+
+def test_vjp_is_linear_and_deterministic():
+    d = abi.frame_desc(**dict(KNDS, width=32, height=18))
+    n = d.width * d.height
+    rng = np.random.default_rng(3)
+    cg, cr = rng.normal(size=n), rng.normal(size=n)
+    _, c1 = S.smooth(d, mode=1, cot_g=cg, cot_r=cr)
+    _, c2 = S.smooth(d, mode=1, cot_g=2 * cg, cot_r=2 * cr)
+    _, c3 = S.smooth(d, mode=1, cot_g=cg, cot_r=cr)
+    assert np.array_equal(2 * c1[:5], c2[:5])
+    assert np.array_equal(c1, c3)
+    _, c0 = S.smooth(d, mode=1, cot_g=np.zeros(n), cot_r=np.zeros(n))
+    assert not c0[:6].any()
+    assert c1[6].sum() == np.sum(c1[6] > 0) and c1[6].sum() > 0  # rays with a reverse sweep
+
+
+def test_smooth_frames_rejected_where_unsupported(L=None):
+    import ctypes
+
+    import kerrtracecpp2_b200 as kt
+
+    lib = kt.load_library()
+    out = abi.FrameDerived()
+    for kw, st in [(dict(bundles=1), abi.KT_ERR_UNSUPPORTED),
+                   (dict(chart=1, integrator=1), abi.KT_ERR_UNSUPPORTED),
+                   (dict(precision=3), abi.KT_ERR_INVALID_ARGUMENT)]:
+        d = abi.frame_desc(width=4, height=4, **dict(dict(precision=abi.KT_PREC_SMOOTH), **kw))
+        assert lib.kt_frame_derive(ctypes.byref(d), ctypes.byref(out)) == st
+    # the KS chart ignores --dopri5, as the reference does
+    d = abi.frame_desc(width=4, height=4, chart=0, integrator=1, precision=abi.KT_PREC_SMOOTH)
+    assert lib.kt_frame_derive(ctypes.byref(d), ctypes.byref(out)) == abi.KT_OK

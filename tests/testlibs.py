@@ -2,7 +2,8 @@
 
   libktmath_shim.so   ktmath.h with C linkage (libm accuracy tests)
   libkt_hostcheck.so  the kernels' per-ray code compiled for the host
-                      (op-order checks against the oracle without a GPU)
+                      (op-order checks against the oracle without a GPU;
+                      the smooth tracer and its adjoint)
 
 and makes sure the oracle port exists.  Called by conftest.py and
 __graft_entry__.build().
@@ -37,7 +38,8 @@ def _run(cmd):
 def build_all(force=False):
     os.makedirs(BUILD, exist_ok=True)
     heads = [os.path.join(CSRC, h) for h in ("ktmath.h", "ktmath_consts.h", "kt_physics.cuh",
-                                             "kt_machines.cuh", "kt_frame.h")]
+                                             "kt_machines.cuh", "kt_frame.h", "kt_dual.cuh",
+                                             "kt_smooth.cuh", "kt_smray.cuh")]
     heads.append(os.path.join(ROOT, "include", "kerrtrace.h"))
     src = os.path.join(TESTS, "ktmath_shim.c")
     if force or _newer(SHIM, [src] + heads):
