@@ -44,6 +44,8 @@ WORKLOADS = {
     # 64 seeded parameter sets (kerrtracecpp2_b200.random_parameter_sets, seed
     # 1) at 256^2..1024^2, KS chart requested, RK4 step doubling; one batch.
     "batch64_ks_rk4_seed1": dict(batch=64, seed=1, width=0, height=0, chart=0),
+    # Config 5 gradient alone (adjoint_leg): value = adjoint ms per frame.
+    "adjoint_ks_512": dict(adjoint=True, width=512, height=512, chart=0),
 }
 # Frames of the batched 720p leg: the headline frame seen from this many
 # camera azimuths, traced as one batch.
@@ -154,6 +156,94 @@ def cpu_reference_sample(desc, seconds, flavour="ieee"):
     dt = time.perf_counter() - t0
     sample = f"{len(pix)} of {n} pixels (every {stride}th, row-major) of the same frame"
     return len(pix) / dt, pix, threads, kind, sample, res
+
+
+ADJOINT_FRAME = dict(chart=0, a=0.7, Q=0.1, Lambda=0.0, theta_deg=70.0, r_obs=50.0, disk_out=15.0,
+                     width=512, height=512)
+
+
+def adjoint_leg(R, steps, warmup, stream, flush):
+    """Config 5: 512x512 KS frame, L2 loss of (g, r_hit) against the smooth
+    tracer at a=0.72, theta=71; kt_l2_grad (fused forward + reverse per ray)
+    timed on the device against kt_trace of the same frame (plain FP64, the
+    reference's arithmetic) and the smooth forward alone."""
+    import torch
+    from kerrtracecpp2_b200 import abi
+
+    n = ADJOINT_FRAME["width"] * ADJOINT_FRAME["height"]
+    d = abi.frame_desc(**ADJOINT_FRAME)
+    ds = abi.frame_desc(precision=abi.KT_PREC_SMOOTH, **ADJOINT_FRAME)
+    tgt = R.trace(abi.frame_desc(precision=abi.KT_PREC_SMOOTH,
+                                 **dict(ADJOINT_FRAME, a=0.72, theta_deg=71.0)))
+    out = R.alloc(n)
+
+    def timed(fn):
+        for _ in range(max(warmup, 1)):
+            flush.fill_(1)
+            fn()
+        torch.cuda.synchronize()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * steps)]
+        for i in range(steps):
+            flush.fill_(1)
+            ev[2 * i].record(stream)
+            fn()
+            ev[2 * i + 1].record(stream)
+        torch.cuda.synchronize()
+        return float(np.mean([ev[2 * i].elapsed_time(ev[2 * i + 1]) for i in range(steps)]))
+
+    fwd_ms = timed(lambda: R.trace(d, out, stream))
+    smooth_ms = timed(lambda: R.trace(ds, out, stream))
+    res = {}
+
+    def grad():
+        res["r"] = R.l2_grad(d, tgt, 1.0, 0.01, out=out, stream=stream)
+
+    grad_ms = timed(grad)
+    loss, g, st = res["r"]
+    return {"frame": "512x512 KS, a=0.7, Q=0.1, theta=70, r_obs=50, disk ISCO-15, tol 1e-7",
+            "loss": "sum over pixels that are disk hits in both frames of (g-g_t)^2 + 0.01 (r-r_t)^2, "
+                    "target: the same tracer at a=0.72, theta=71",
+            "ms_per_frame": grad_ms, "ms_main_pass": st["ms_main"], "ms_lambda_pass": st["ms_lambda"],
+            "forward_fp64_ms": fwd_ms, "forward_smooth_ms": smooth_ms,
+            "ratio_vs_forward_fp64": grad_ms / fwd_ms,
+            "ratio_vs_forward_fp64_without_lambda_pass": st["ms_main"] / fwd_ms,
+            "grad": dict(zip(abi.GRAD_NAMES, [float(x) for x in g])), "loss_value": loss,
+            "grad_pixels": st["grad_pixels"], "unrecorded": st["unrecorded"],
+            "checkpoint_interval_steps": 32,
+            "fd_check": "tests/test_gpu_grad.py (central differences, h=1e-6)"}
+
+
+def bench_adjoint(args, rank, world, local_rank):
+    """The config-5 gradient as its own line: value = adjoint ms per frame
+    (kt_l2_grad, both passes), one frame per GPU; the reference has no
+    gradient, so its arm is unavailable for this workload."""
+    cfg = {"workload": args.workload, "width": 512, "height": 512, "chart": "KS", "a": 0.7, "Q": 0.1,
+           "theta": 70.0, "r_obs": 50.0, "tol": 1e-7, "parallelism": f"frames{args.gpus}",
+           "l2": "256 MB flush between steps"}
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "the reference renderer has no "
+                              "gradient (no adjoint or VJP entry)"}), flush=True)
+        return 0
+    import torch
+
+    import kerrtracecpp2_b200 as kt
+
+    device = torch.device("cuda", local_rank)
+    torch.cuda.set_device(device)
+    R = kt.Renderer(local_rank)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=device)
+    stream = torch.cuda.current_stream(device)
+    adj = adjoint_leg(R, args.steps, args.warmup, stream, flush)
+    line = {"metric": METRIC, "value": adj["ms_per_frame"], "unit": "ms/frame (adjoint)",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": adj["ms_per_frame"], "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (procedural camera frame; no dataset)",
+            "config": cfg, "adjoint": adj, "gpu_launches": args.steps * 9}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    R.close()
+    return 0
 
 
 def cpu_reference_batch(descs, seconds, flavour="ieee"):
@@ -355,6 +445,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     args = ap.parse_args()
     sys.path.insert(0, os.path.join(ROOT, "tests"))
 
@@ -364,6 +455,8 @@ def main():
     from kerrtracecpp2_b200 import abi
 
     wl = dict(WORKLOADS[args.workload])
+    if wl.get("adjoint"):
+        return bench_adjoint(args, rank, world, local_rank)
     if wl.get("batch"):
         base_cfg = {"workload": args.workload, "frames": wl["batch"], "seed": wl["seed"],
                     "sizes": "square, side ~ U{256..1024} step 16", "chart": "KS requested "
@@ -544,6 +637,10 @@ def main():
         b.close()
         del b
 
+    adjoint = None
+    if not args.no_adjoint:
+        adjoint = adjoint_leg(R, args.steps, args.warmup, stream, flush)
+
     steps_sum = float(out["steps"].to(torch.int64).sum())
     att_sum = float(out["attempts"].to(torch.int64).sum())
     flops = ray_flops(desc, steps_sum, att_sum)
@@ -604,13 +701,14 @@ def main():
             "data": "synthetic (procedural camera frame; no dataset)", "config": base_cfg,
             "mode": "plain FP64, bit-identical to the reference CPU path",
             "roofline": roofline, "cpu_baseline": cpu, "mixed_precision": mixed,
-            "mixed_batched": mixed_batched,
+            "mixed_batched": mixed_batched, "adjoint": adjoint,
             "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": ctypes.sizeof(desc),
                     "d2h_bytes_per_step": d2h, "call": "kt_trace_host"},
             "clocks": clocks, "gpu_launches": args.steps * (2 if desc.chart == 0 and not desc.bundles
                                                             and abs(desc.Lambda) <= 1e-15 else 1)
             * (2 if mixed is not None else 1)
-            + (args.steps * len(mixed_batched["groups"]) if mixed_batched else 0)}
+            + (args.steps * len(mixed_batched["groups"]) if mixed_batched else 0)
+            + (args.steps * 9 if adjoint else 0)}
     if rank == 0:
         print(json.dumps(line), flush=True)
     R.close()

@@ -1,9 +1,11 @@
 // kt_adjoint.cu -- kernels of the smooth tracer (KT_PREC_SMOOTH) and of its
 // discrete adjoint (kt_vjp, kt_l2_grad).
 //
-// One thread per ray, rays from a device queue (persistent grid).  The
+// One thread per ray, rays from a device queue (persistent grid), one kernel
+// per chart (a kernel with both charts' code overflowed the instruction
+// cache: most issue slots went to instruction-fetch stalls).  The
 // gradient kernel traces its ray with checkpoints in local memory
-// (SmScratch, ~9 KB per thread), and for a disk hit with a non-zero
+// (SmScratch, ~12 KB per thread), and for a disk hit with a non-zero
 // cotangent runs the reverse sweep right away; it writes the ray's loss and
 // gradient contributions to a [kGSlots][n] array, which k_sum_* reduce in a
 // fixed order (the sum does not depend on the schedule).
@@ -20,17 +22,28 @@ constexpr int kSmBlock = 64;
 constexpr int kSumBlocks = 296;
 constexpr int kSumThreads = 256;
 
-template <bool kGrad>
+// Rays: pixels 0..n-1 or list[0..*n_dev).  The KS kernel appends the rays
+// whose KS initialisation fails to fb_pix (count *fb_n) for the BL kernel.
+template <class C, bool kGrad>
 __global__ void __launch_bounds__(kSmBlock) k_smooth(const Frame f, const OutSoA out, const SmJob job,
-                                                     uint32_t n, uint32_t* __restrict__ queue) {
+                                                     uint32_t n, const uint32_t* __restrict__ list,
+                                                     const uint32_t* __restrict__ n_dev,
+                                                     uint32_t* __restrict__ queue,
+                                                     uint32_t* __restrict__ fb_pix,
+                                                     uint32_t* __restrict__ fb_n) {
   SmScratch sc;
+  const uint32_t count = n_dev ? *n_dev : n;
   KT_ROLLED
   for (;;) {
-    const uint32_t pix = atomicAdd(queue, 1u);
-    if (pix >= n) break;
+    const uint32_t i = atomicAdd(queue, 1u);
+    if (i >= count) break;
+    const uint32_t pix = list ? list[i] : i;
     RayResult o;
     double g[kGSlots];
-    sm_pixel<kGrad>(f, pix, job.force_bl != 0, job.cot, &o, g, kGrad ? &sc : nullptr);
+    if (!sm_pixel<C, kGrad>(f, pix, job.cot, &o, g, kGrad ? &sc : nullptr)) {
+      fb_pix[atomicAdd(fb_n, 1u)] = pix;
+      continue;
+    }
     if (out.outcome) write_result(out, pix, o);
     if (kGrad)
       for (int q = 0; q < kGSlots; ++q) job.contrib[(size_t)q * n + pix] = g[q];
@@ -76,30 +89,42 @@ __global__ void __launch_bounds__(kSumThreads) k_sum_final(const double* __restr
   }
 }
 
-template <bool kGrad>
-static cudaError_t smooth_grid(int device, int* grid) {
+template <class C, bool kGrad>
+static cudaError_t smooth_launch(const Frame& f, const OutSoA& out, uint32_t n, const SmJob& job,
+                                 const uint32_t* list, const uint32_t* n_dev, uint32_t* queue,
+                                 uint32_t* fb_pix, uint32_t* fb_n, int device, cudaStream_t st) {
   int sms = 0, per_sm = 0;
   cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   if (e != cudaSuccess) return e;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_smooth<kGrad>, kSmBlock, 0);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_smooth<C, kGrad>, kSmBlock, 0);
   if (e != cudaSuccess) return e;
-  *grid = sms * (per_sm < 1 ? 1 : per_sm);
-  return cudaSuccess;
+  const int grid = sms * (per_sm < 1 ? 1 : per_sm);
+  k_smooth<C, kGrad><<<grid, kSmBlock, 0, st>>>(f, out, job, n, list, n_dev, queue, fb_pix, fb_n);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_smooth(const Frame& f, const OutSoA& out, uint32_t n, const SmJob* job,
-                          uint32_t* queue, int device, cudaStream_t st) {
-  int grid = 0;
-  cudaError_t e = job ? smooth_grid<true>(device, &grid) : smooth_grid<false>(device, &grid);
-  if (e != cudaSuccess) return e;
-  if (job) {
-    k_smooth<true><<<grid, kSmBlock, 0, st>>>(f, out, *job, n, queue);
-  } else {
-    SmJob none;
-    memset(&none, 0, sizeof none);
-    k_smooth<false><<<grid, kSmBlock, 0, st>>>(f, out, none, n, queue);
+                          uint32_t* counters, uint32_t* fb_pix, int device, cudaStream_t st) {
+  SmJob none;
+  memset(&none, 0, sizeof none);
+  const SmJob& jb = job ? *job : none;
+  const bool grad = job != nullptr;
+  if (f.chart == 0 && !(job && job->force_bl)) {
+    // KS pass over all pixels, then BL over the rays whose KS init failed
+    cudaError_t e = grad ? smooth_launch<ChartKS, true>(f, out, n, jb, nullptr, nullptr, counters,
+                                                        fb_pix, counters + 2, device, st)
+                         : smooth_launch<ChartKS, false>(f, out, n, jb, nullptr, nullptr, counters,
+                                                         fb_pix, counters + 2, device, st);
+    if (e != cudaSuccess) return e;
+    return grad ? smooth_launch<ChartBL, true>(f, out, n, jb, fb_pix, counters + 2, counters + 1,
+                                               nullptr, nullptr, device, st)
+                : smooth_launch<ChartBL, false>(f, out, n, jb, fb_pix, counters + 2, counters + 1,
+                                                nullptr, nullptr, device, st);
   }
-  return cudaGetLastError();
+  return grad ? smooth_launch<ChartBL, true>(f, out, n, jb, nullptr, nullptr, counters, nullptr,
+                                             nullptr, device, st)
+              : smooth_launch<ChartBL, false>(f, out, n, jb, nullptr, nullptr, counters, nullptr,
+                                              nullptr, device, st);
 }
 
 cudaError_t launch_grad_sum(const double* contrib, uint32_t n, double* partial, double* out,

@@ -37,8 +37,10 @@ kt_status run_trace(kt_context* ctx, const kt::Frame& f, const kt::OutSoA& out,
   if (f.precision == KT_PREC_SMOOTH) {
     if (rl.pix || rl.slot || rl.n_dev)
       return fail(ctx, KT_ERR_UNSUPPORTED, "the smooth tracer traces whole frames only");
+    kt_status r = ensure(ctx, (void**)&ctx->d_fb, &ctx->fb_cap, 2 * n_max * sizeof(uint32_t), "fallback list");
+    if (r != KT_OK) return r;
     KT_CUDA(ctx, cudaMemsetAsync(ctx->d_counters, 0, 4 * sizeof(uint32_t), st), "reset queue");
-    KT_CUDA(ctx, kt::launch_smooth(f, out, rl.n, nullptr, ctx->d_counters, ctx->device, st),
+    KT_CUDA(ctx, kt::launch_smooth(f, out, rl.n, nullptr, ctx->d_counters, ctx->d_fb, ctx->device, st),
             "smooth kernel launch");
     return KT_OK;
   }

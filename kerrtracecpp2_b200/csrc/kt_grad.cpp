@@ -36,7 +36,8 @@ kt_status grad_pass(kt_context* ctx, const kt::Frame& f, const kt::OutSoA& out, 
   KT_CUDA(ctx, cudaEventCreate(&ev.b), "event");
   KT_CUDA(ctx, cudaMemsetAsync(ctx->d_counters, 0, 4 * sizeof(uint32_t), st), "reset queue");
   KT_CUDA(ctx, cudaEventRecord(ev.a, st), "event");
-  KT_CUDA(ctx, kt::launch_smooth(f, out, n, &job, ctx->d_counters, ctx->device, st), "adjoint kernel launch");
+  KT_CUDA(ctx, kt::launch_smooth(f, out, n, &job, ctx->d_counters, ctx->d_fb, ctx->device, st),
+          "adjoint kernel launch");
   KT_CUDA(ctx, kt::launch_grad_sum(ctx->d_grad, n, ctx->d_gsum + kt::kGSlots, ctx->d_gsum, st),
           "gradient sum");
   KT_CUDA(ctx, cudaEventRecord(ev.b, st), "event");
@@ -66,6 +67,8 @@ kt_status grad_run(kt_context* ctx, const kt_frame_desc* desc_in, const kt::SmCo
   if (r != KT_OK) return r;
   r = ensure(ctx, (void**)&ctx->d_gsum, &ctx->gsum_cap, kt::grad_sum_scratch_doubles() * sizeof(double),
              "gradient sums");
+  if (r != KT_OK) return r;
+  r = ensure(ctx, (void**)&ctx->d_fb, &ctx->fb_cap, 2 * n * sizeof(uint32_t), "fallback list");
   if (r != KT_OK) return r;
   kt::OutSoA out;
   memset(&out, 0, sizeof out);

@@ -24,6 +24,17 @@
 #include "kt_dual.cuh"
 #include "kt_machines.cuh"
 
+// Functions called from many places in the smooth kernels are real calls on
+// the device (one copy of the body each): the kernels are otherwise too big
+// for the instruction cache.
+#if defined(__CUDA_ARCH__)
+#define KT_HD_CALL __host__ __device__ __noinline__
+#elif defined(__CUDACC__)
+#define KT_HD_CALL __host__ __device__ inline
+#else
+#define KT_HD_CALL inline
+#endif
+
 namespace kt {
 
 constexpr int kSmPrm = 3;  // (a, Q, Lambda)
@@ -177,9 +188,13 @@ struct ChartKS {
 
 // ------------------------------------------------------------- BL chart
 // state y = (r, theta, p_r, p_theta), constants (p_t, p_phi), passenger phi
-// (dphi/dlam = dH/dp_phi).  H = (g^tt p_t^2 + 2 g^tphi p_t p_phi + g^rr p_r^2
-// + g^thth p_theta^2 + g^phiphi p_phi^2)/2 with the metric of sm_bl_metric;
-// its derivatives in (r, theta, a, Q, Lambda) by the quotient rule.
+// (dphi/dlam = dH/dp_phi).  With the metric of sm_bl_metric, the Hamiltonian
+// (knds_metric.hpp:122-132) is, collected over the metric's denominators,
+//   H = K / (2 S),  K = R p_r^2 + Tt p_theta^2 + xi^2 (W iT - P^2 iR),
+//   P = A p_t + a p_phi,  W = a^2 s2 p_t^2 + 2 a p_t p_phi + p_phi^2 / s2
+// (1/s2 -> 0 within 1e-14 of the axis, the reference's guard on g^phiphi),
+// iR = 1/R, iT = 1/Tt.  Its derivatives in (r, theta, a, Q, Lambda) follow
+// from those of A, S, R, Tt, s2, xi^2 and a.
 struct ChartBL {
   static constexpr int kX = 2;
   static constexpr int kN = 4;
@@ -192,9 +207,9 @@ struct ChartBL {
     const T &r = y[0], &th = y[1], &pr = y[2], &pth = y[3], &pt = c[0], &pph = c[1];
     const T a = P.a, L = P.L;
     const T a2 = a * a;
-    T s, co;
-    sm_sincos(th, &s, &co);
-    const T s2 = s * s, c2 = co * co, sc = s * co;
+    T sn, co;
+    sm_sincos(th, &sn, &co);
+    const T s2 = sn * sn, c2 = co * co, sc = sn * co;
     const T r2 = r * r;
     const T A = r2 + a2;
     const T S = r2 + a2 * c2;
@@ -206,19 +221,19 @@ struct ChartBL {
     const T iS = 1.0 / S, iR = 1.0 / R, iT = 1.0 / Tt;
     const bool pole = !(s2 > 1e-14);
     const T is2 = pole ? T(0.0) : 1.0 / s2;
-    const T Xtt = A * A * iR - a2 * s2 * iT;
-    const T Xtp = iT - A * iR;
-    const T Xpp = pole ? T(0.0) : iT * is2 - a2 * iR;
-    const T Utt = -xi2 * iS * Xtt, Utp = a * xi2 * iS * Xtp, Urr = R * iS, Uhh = Tt * iS,
-            Upp = xi2 * iS * Xpp;
-    gy[2] = Urr * pr;
-    gy[3] = Uhh * pth;
-    gc[0] = Utt * pt + Utp * pph;
-    gc[1] = Utp * pt + Upp * pph;
-    const T ptpt = pt * pt, ptpp = 2.0 * pt * pph, prpr = pr * pr, hh = pth * pth, pppp = pph * pph;
-    // variables: 0 r, 1 theta, 2 a, 3 Q, 4 Lambda
+    const T Pp = A * pt + a * pph;
+    const T W = a2 * s2 * pt * pt + 2.0 * a * pt * pph + pph * pph * is2;
+    const T K = R * pr * pr + Tt * pth * pth + xi2 * (W * iT - Pp * Pp * iR);
+    const T H = 0.5 * K * iS;
+    gy[2] = R * pr * iS;
+    gy[3] = Tt * pth * iS;
+    gc[0] = xi2 * ((a2 * s2 * pt + a * pph) * iT - Pp * A * iR) * iS;
+    gc[1] = xi2 * ((a * pt + pph * is2) * iT - Pp * a * iR) * iS;
+    const T prpr = pr * pr, hh = pth * pth, ptpt = pt * pt;
+    const T WiT_P2iR = W * iT - Pp * Pp * iR;
+    // dH/dv = (dK/dv - 2 H dS/dv) / (2 S) for v = r, theta, a, Q, Lambda
+    const T zero(0.0);
     for (int v = 0; v < 5; ++v) {
-      const T zero(0.0);
       const T dA = v == 0 ? 2.0 * r : v == 2 ? 2.0 * a : zero;
       const T dS = v == 0 ? 2.0 * r : v == 1 ? -2.0 * a2 * sc : v == 2 ? 2.0 * a * c2 : zero;
       const T dR = v == 0 ? 2.0 * r * (1.0 - Lr2_3) - (2.0 * L * r / 3.0) * A - 2.0 * M
@@ -232,19 +247,13 @@ struct ChartBL {
                             : zero;
       const T ds2 = v == 1 ? 2.0 * sc : zero;
       const T dxi2 = v == 2 ? 2.0 * xi * (2.0 * L * a / 3.0) : v == 4 ? 2.0 * xi * (a2 / 3.0) : zero;
-      const T da2 = v == 2 ? 2.0 * a : zero;
-      const T da = v == 2 ? T(1.0) : zero;
-      const T diS = -dS * iS * iS, diR = -dR * iR * iR, diT = -dT * iT * iT;
-      const T dis2 = pole ? zero : -ds2 * is2 * is2;
-      const T dXtt = 2.0 * A * dA * iR + A * A * diR - (da2 * s2 * iT + a2 * ds2 * iT + a2 * s2 * diT);
-      const T dXtp = diT - (dA * iR + A * diR);
-      const T dXpp = pole ? zero : diT * is2 + iT * dis2 - (da2 * iR + a2 * diR);
-      const T dUtt = -(dxi2 * iS * Xtt + xi2 * diS * Xtt + xi2 * iS * dXtt);
-      const T dUtp = da * xi2 * iS * Xtp + a * (dxi2 * iS * Xtp + xi2 * diS * Xtp + xi2 * iS * dXtp);
-      const T dUrr = dR * iS + R * diS;
-      const T dUhh = dT * iS + Tt * diS;
-      const T dUpp = dxi2 * iS * Xpp + xi2 * diS * Xpp + xi2 * iS * dXpp;
-      const T dH = 0.5 * (dUtt * ptpt + dUtp * ptpp + dUrr * prpr + dUhh * hh + dUpp * pppp);
+      const double da = v == 2 ? 1.0 : 0.0;
+      const T dP = dA * pt + da * pph;
+      const T dW = (v == 2 ? 2.0 * a * s2 * ptpt + 2.0 * pt * pph : zero) + a2 * ds2 * ptpt -
+                   (pole ? zero : pph * pph * ds2 * is2 * is2);
+      const T dK = dR * prpr + dT * hh + dxi2 * WiT_P2iR +
+                   xi2 * (dW * iT - W * dT * iT * iT - 2.0 * Pp * dP * iR + Pp * Pp * dR * iR * iR);
+      const T dH = (0.5 * dK - H * dS) * iS;
       if (v < 2)
         gy[v] = dH;
       else
@@ -254,12 +263,19 @@ struct ChartBL {
 
   template <class T>
   KT_HD static T ham(double M, const SmPrm<T>& P, const T* y, const T* c) {
-    T s, co;
-    sm_sincos(y[1], &s, &co);
-    SmBL<T> U;
-    sm_bl_metric<T>(M, P, y[0], s, co, (SmBL<T>*)nullptr, &U);
-    return 0.5 * (U.tt * c[0] * c[0] + 2.0 * U.tp * c[0] * c[1] + U.rr * y[2] * y[2] +
-                  U.hh * y[3] * y[3] + U.pp * c[1] * c[1]);
+    T sn, co;
+    sm_sincos(y[1], &sn, &co);
+    const T a = P.a, a2 = a * a, r2 = y[0] * y[0];
+    const T s2 = sn * sn, c2 = co * co;
+    const T A = r2 + a2, S = r2 + a2 * c2;
+    const T R = A * (1.0 - P.L * r2 / 3.0) - 2.0 * M * y[0] + P.Q * P.Q;
+    const T Tt = 1.0 + P.L * a2 * c2 / 3.0;
+    const T xi = 1.0 + P.L * a2 / 3.0;
+    const T is2 = (s2 > 1e-14) ? 1.0 / s2 : T(0.0);
+    const T Pp = A * c[0] + a * c[1];
+    const T W = a2 * s2 * c[0] * c[0] + 2.0 * a * c[0] * c[1] + c[1] * c[1] * is2;
+    const T K = R * y[2] * y[2] + Tt * y[3] * y[3] + xi * xi * (W / Tt - Pp * Pp / R);
+    return 0.5 * K / S;
   }
 
   template <class T, class A>
@@ -268,7 +284,7 @@ struct ChartBL {
 
 // f = (dH/dp, -dH/dx) and the passenger rate (BL: dphi = dH/dp_phi).
 template <class C, class T>
-KT_HD void sm_rhs(double M, const SmPrm<T>& P, const T* y, const T* c, T* f, T* fpas) {
+KT_HD_CALL void sm_rhs(double M, const SmPrm<T>& P, const T* y, const T* c, T* f, T* fpas) {
   T gy[C::kN], gc[C::kC], gp[kSmPrm];
   C::grad(M, P, y, c, gy, gc, gp);
   for (int i = 0; i < C::kX; ++i) {

@@ -11,8 +11,9 @@
 //   * the event: the crossing parameter alpha* solves
 //     q(alpha) = Hermite(y_{N-1}, y_N, f_{N-1}, f_N; h, alpha)[eq] - target = 0,
 //     so d alpha* = -dq / q'(alpha*) (implicit function theorem).  The hit
-//     outputs are evaluated in Dual<2n + c + 3> over (y_{N-1}, y_N, constants,
-//     a, Q, Lambda) with alpha* carrying that derivative;
+//     outputs are differentiated in Dual over the hit state, the constants
+//     and (a, Q, Lambda); alpha*'s share goes back through q, and f_{N-1},
+//     f_N pass theirs on through VJPs of the RHS;
 //   * the accepted steps, last to first.  Step n starts from (y_n, H_n),
 //     H_n the controller's dlam; its attempts j = 0..R have sizes h_0 = H_n,
 //     h_{j+1} = rho(h_j, e_j) after a rejection, and the accepted one gives
@@ -27,7 +28,8 @@
 //   * states come back from the checkpoints: a segment of k steps is replayed
 //     from its checkpoint (same controller, same rejections, so the same
 //     accepted steps); segments longer than 32 steps are replayed once into
-//     inner checkpoints every 32 steps.
+//     inner checkpoints every 32 steps.  The last 32 step starts are kept
+//     by the forward itself, so the final sub-segment needs no replay.
 // VJP of the RHS f = J grad_y H (J = [[0, I], [-I, 0]]): v^T df/dy =
 // H_yy (J^T v) and v^T df/dc = d/dc (grad_y H) . (J^T v) = the derivative of
 // dH/dc along J^T v, so one Dual<1> evaluation of the full gradient of H along
@@ -48,9 +50,10 @@ struct SmCk {  // state at the start of an accepted step and dlam before its att
   double h;
 };
 
-struct SmSt {  // state at the start of an accepted step and dlam before its attempts
+struct SmSt {  // state at the start of an accepted step, dlam before its attempts, attempts
   double y[kSmMaxN];
   double H;
+  int na;
 };
 
 // Data of the final (event) step kept for the adjoint.
@@ -63,47 +66,97 @@ struct SmEvent {
   int deriv;           // 1: redshift has a derivative (not a constant or clamped)
 };
 
-// Primal RK4 step of size h from y with k1 = f(y); the passenger (BL phi)
-// rides along.  Stage inputs y + h/2 k1, y + h/2 k2, y + h k3; result
-// y + h/6 (k1 + 2 k2 + 2 k3 + k4) (rk4_step_ks, main.cpp:1456-1486).
-template <class C>
-KT_HD void sm_rk4(double M, const SmPrm<double>& P, const double* c, const double* y, double pas,
-                  const double* k1, double k1p, double h, double* yo, double* paso) {
-  double u[C::kN], k[C::kN], sum[C::kN], kp, sump = k1p;
-  for (int i = 0; i < C::kN; ++i) {
-    sum[i] = k1[i];
-    u[i] = y[i] + 0.5 * h * k1[i];
-  }
-  sm_rhs<C>(M, P, u, c, k, &kp);
-  for (int i = 0; i < C::kN; ++i) {
-    sum[i] = sum[i] + 2.0 * k[i];
-    u[i] = y[i] + 0.5 * h * k[i];
-  }
-  sump = sump + 2.0 * kp;
-  sm_rhs<C>(M, P, u, c, k, &kp);
-  for (int i = 0; i < C::kN; ++i) {
-    sum[i] = sum[i] + 2.0 * k[i];
-    u[i] = y[i] + h * k[i];
-  }
-  sump = sump + 2.0 * kp;
-  sm_rhs<C>(M, P, u, c, k, &kp);
-  for (int i = 0; i < C::kN; ++i) yo[i] = y[i] + h / 6.0 * (sum[i] + k[i]);
-  *paso = pas + h / 6.0 * (sump + kp);
+// Stages of one adaptive attempt from y with step h, t = 0..9: path A =
+// RK4 stages 2-4 of one step h (t = 0-2), path B1 = stages 2-4 of a step h/2
+// (t = 3-5), path B2 = stages 1-4 of a step h/2 from B1's result (t = 6-9);
+// stage 1 of A and B1 is k1 = f(y), given.  Stage inputs base + h/2 k1,
+// base + h/2 k2, base + h k3; result base + h/6 (k1 + 2 k2 + 2 k3 + k4)
+// (rk4_step_ks, main.cpp:1456-1486).  One rolled loop, one RHS call site: the
+// kernel's code stays small enough for the instruction cache.
+struct SmStages {
+  double u[10][kSmMaxN];  // stage inputs
+  double k[10][kSmMaxN];  // f(u)
+};
+
+KT_HD void sm_stage_of(int t, int* sub, int* s) {
+  *sub = t < 3 ? 0 : (t < 6 ? 1 : 2);
+  *s = *sub == 0 ? t + 1 : (*sub == 1 ? t - 2 : t - 6);
 }
 
-// One adaptive attempt from (y, pas) with k1 = f(y) and step *h: path A one
-// step h, path B two steps h/2 (mid point ym), err = |A - B| / 15.  Returns
-// doubling_update's result; on acceptance (yo, paso) = B.
+// Paths A and B of an attempt (results yA, yB and B's passenger); with
+// `rec`, the stage inputs and slopes are kept.
+template <class C>
+KT_HD_CALL void sm_paths(double M, const SmPrm<double>& P, const double* c, const double* y, double pas,
+                         const double* k1, double k1p, double hh, double* yA, double* yB, double* pB,
+                         SmStages* rec) {
+  constexpr int n = C::kN;
+  double base[n], kp[n], sum[n], yB1[n], u[n], k[n];
+  double pbase = pas, sump = k1p, pB1 = pas, kk;
+  KT_ROLLED
+  for (int t = 0; t < 10; ++t) {
+    int sub, s;
+    sm_stage_of(t, &sub, &s);
+    const double hs = sub == 0 ? hh : 0.5 * hh;
+    if (s == 1 && sub < 2) {
+      for (int i = 0; i < n; ++i) {
+        base[i] = y[i];
+        kp[i] = k1[i];
+        sum[i] = k1[i];
+      }
+      pbase = pas;
+      sump = k1p;
+    }
+    if (s == 0) {
+      for (int i = 0; i < n; ++i) {
+        base[i] = yB1[i];
+        u[i] = yB1[i];
+      }
+      pbase = pB1;
+    } else {
+      const double cs = (s == 3) ? hs : 0.5 * hs;
+      for (int i = 0; i < n; ++i) u[i] = base[i] + cs * kp[i];
+    }
+    sm_rhs<C>(M, P, u, c, k, &kk);
+    if (rec)
+      for (int i = 0; i < n; ++i) {
+        rec->u[t][i] = u[i];
+        rec->k[t][i] = k[i];
+      }
+    if (s == 0) {
+      for (int i = 0; i < n; ++i) {
+        kp[i] = k[i];
+        sum[i] = k[i];
+      }
+      sump = kk;
+      continue;
+    }
+    const double w = (s == 3) ? 1.0 : 2.0;
+    for (int i = 0; i < n; ++i) {
+      sum[i] = sum[i] + w * k[i];
+      kp[i] = k[i];
+    }
+    sump = sump + w * kk;
+    if (s == 3) {
+      for (int i = 0; i < n; ++i) {
+        const double r = base[i] + hs / 6.0 * sum[i];
+        yA[i] = sub == 0 ? r : yA[i];
+        yB1[i] = sub == 1 ? r : yB1[i];
+        yB[i] = sub == 2 ? r : yB[i];
+      }
+      const double pr = pbase + hs / 6.0 * sump;
+      pB1 = sub == 1 ? pr : pB1;
+      *pB = sub == 2 ? pr : *pB;
+    }
+  }
+}
+
+// One adaptive attempt from (y, pas) with k1 = f(y) and step *h:
+// err = |A - B| / 15, doubling_update; on acceptance (yo, paso) = B.
 template <class C>
 KT_HD int sm_attempt(double M, const SmPrm<double>& P, double tol, const double* c, const double* y,
-                     double pas, const double* k1, double k1p, double* h, double* yo, double* paso,
-                     double* ym) {
-  double yA[C::kN], yB1[C::kN], yB[C::kN], kb[C::kN], pA, pB1, pB, kbp;
-  const double hh = *h;
-  sm_rk4<C>(M, P, c, y, pas, k1, k1p, hh, yA, &pA);
-  sm_rk4<C>(M, P, c, y, pas, k1, k1p, 0.5 * hh, yB1, &pB1);
-  sm_rhs<C>(M, P, yB1, c, kb, &kbp);
-  sm_rk4<C>(M, P, c, yB1, pB1, kb, kbp, 0.5 * hh, yB, &pB);
+                     double pas, const double* k1, double k1p, double* h, double* yo, double* paso) {
+  double yA[C::kN], yB[C::kN], pB = 0.0;
+  sm_paths<C>(M, P, c, y, pas, k1, k1p, *h, yA, yB, &pB, nullptr);
   double e2 = 0.0;
   for (int i = 0; i < C::kN; ++i) {
     const double d = yA[i] - yB[i];
@@ -111,10 +164,7 @@ KT_HD int sm_attempt(double M, const SmPrm<double>& P, double tol, const double*
   }
   const int res = doubling_update(sqrt(e2) / 15.0, tol, h);
   if (res == 1) {
-    for (int i = 0; i < C::kN; ++i) {
-      yo[i] = yB[i];
-      if (ym) ym[i] = yB1[i];
-    }
+    for (int i = 0; i < C::kN; ++i) yo[i] = yB[i];
     *paso = pB;
   }
   return res;
@@ -138,12 +188,14 @@ KT_HD void sm_stop(const Frame& f, const double* y, double pas, int status, uint
 }
 
 // Trace one ray from (y, c, pas).  With ck != NULL, checkpoints are recorded
-// (*ck_k = final interval, *ck_n = count).  On a disk hit `ev` receives the
+// (*ck_k = final interval, *ck_n = count); with ring != NULL, step m's start
+// (y, dlam, attempts) is kept in ring[m % 32] (the last 32 steps).  On a disk hit `ev` receives the
 // final step; returns the number of accepted steps N (0 if the ray ended
 // otherwise or more than 131072 steps were taken with recording on).
 template <class C>
 KT_HD int sm_trace(const Frame& f, const SmPrm<double>& P, const double* y_in, const double* c,
-                   double pas_in, RayResult* o, SmEvent* ev, SmCk* ck, int* ck_k, int* ck_n) {
+                   double pas_in, RayResult* o, SmEvent* ev, SmCk* ck, int* ck_k, int* ck_n,
+                   SmSt* ring) {
   const double M = f.g.M;
   double y[C::kN], yp[C::kN], k1[C::kN], kprev[C::kN];
   double pas = pas_in, pasp, k1p, kprevp;
@@ -180,19 +232,25 @@ KT_HD int sm_trace(const Frame& f, const SmPrm<double>& P, const double* y_in, c
     pasp = pas;
     kprevp = k1p;
     const double H_start = h;
+    const uint32_t att0 = attempts;
+    if (ring) {
+      for (int i = 0; i < C::kN; ++i) ring[it % kSmCkSteps].y[i] = y[i];
+      ring[it % kSmCkSteps].H = h;
+    }
     double step_used = h;
     int rejects = 0;
     KT_ROLLED
     for (;;) {
       step_used = h;
       ++attempts;
-      if (sm_attempt<C>(M, P, f.tol, c, yp, pasp, kprev, kprevp, &h, y, &pas, nullptr) == 1) break;
+      if (sm_attempt<C>(M, P, f.tol, c, yp, pasp, kprev, kprevp, &h, y, &pas) == 1) break;
       int status;
       if (reject_cap(h, &rejects, &status)) {
         sm_stop<C>(f, yp, pasp, status, (uint32_t)it, attempts, o);
         return 0;
       }
     }
+    if (ring) ring[it % kSmCkSteps].na = (int)(attempts - att0);
     sm_rhs<C>(M, P, y, c, k1, &k1p);
     // events (main.cpp:1570-1657, 364-433)
     const double r_now = C::radius(f.g.a, y);
@@ -275,8 +333,8 @@ KT_HD int sm_trace(const Frame& f, const SmPrm<double>& P, const double* y_in, c
 }
 
 // Replay `n` accepted steps from checkpoint `ck0` (the controller from its
-// dlam, rejections included).  Stores each step's start (y_n, H_n) into
-// st[0..n) and/or a checkpoint every k2 steps into ck2.
+// dlam, rejections included).  Stores each step's start (y_n, H_n) and its
+// number of attempts into st[0..n) and/or a checkpoint every k2 steps into ck2.
 template <class C>
 KT_HD void sm_replay(const Frame& f, const SmPrm<double>& P, const double* c, const SmCk& ck0, int n,
                      SmSt* st, SmCk* ck2, int k2) {
@@ -295,13 +353,15 @@ KT_HD void sm_replay(const Frame& f, const SmPrm<double>& P, const double* c, co
       st[m].H = h;
     }
     sm_rhs<C>(M, P, y, c, k1, &k1p);
-    int rejects = 0;
+    int rejects = 0, na = 0;
     KT_ROLLED
     for (;;) {
-      if (sm_attempt<C>(M, P, f.tol, c, y, pas, k1, k1p, &h, y1, &pas1, nullptr) == 1) break;
+      ++na;
+      if (sm_attempt<C>(M, P, f.tol, c, y, pas, k1, k1p, &h, y1, &pas1) == 1) break;
       int status;
       if (reject_cap(h, &rejects, &status)) break;  // not reached: the forward accepted
     }
+    if (st) st[m].na = na;
     for (int i = 0; i < C::kN; ++i) y[i] = y1[i];
     pas = pas1;
   }
@@ -346,8 +406,8 @@ KT_HD void sm_ctl_partials(double err, double tol, double h, double* dh, double*
 
 // v^T df/d(y, c, prm) at u: ybar = .., cbar += .., pbar += ..
 template <class C>
-KT_HD void sm_vjp_f(double M, const SmPrm<double>& P, const double* u, const double* c, const double* v,
-                    double* ubar, double* cbar, double* pbar) {
+KT_HD_CALL void sm_vjp_f(double M, const SmPrm<double>& P, const double* u, const double* c,
+                         const double* v, double* ubar, double* cbar, double* pbar) {
   Dual<1> yd[C::kN], cd[C::kC], gy[C::kN], gc[C::kC], gp[kSmPrm];
   for (int i = 0; i < C::kX; ++i) {
     yd[i] = Dual<1>(u[i]);
@@ -366,191 +426,221 @@ KT_HD void sm_vjp_f(double M, const SmPrm<double>& P, const double* u, const dou
   for (int q = 0; q < kSmPrm; ++q) pbar[q] = pbar[q] + gp[q].d[0];
 }
 
-// Reverse of one RK4 step of size h from y (sm_rk4's arithmetic).  In:
-// ybar = cotangent of the result.  Out: ybar = cotangent of y, hbar += the
-// step size's, cbar/pbar += the constants' and parameters'.  Optionally
-// returns the result of the step in yo.
+// Reverse of one attempt from y with size hh.  gout: cotangent of the dlam
+// the controller sets after it (H_{n+1} after the accepted attempt, the next
+// attempt's size after a rejection); yb_out: cotangent of path B's result
+// (y_{n+1}; NULL for a rejected attempt); hbar_extra: a further cotangent of
+// hh (the event's, on the last step).  ybar/cbar/pbar += ..; returns the
+// cotangent of hh.
+//
+// The forward pass records the 10 stages; the reverse walks them back
+// (q = 0-3: B2 stages 4..1, q = 4-6: B1 stages 4..2, q = 7-9: A stages 4..2,
+// q = 10: the shared k1 = f(y)) with one VJP call site.  For a stage s of a
+// sub-step with size hs and result cotangent Y: kbar_s = hs/6 w_s Y +
+// beta_{s+1} hs ubar_{s+1}, ubar_s = VJP_f(u_s, kbar_s), the sub-step's base
+// gets Y + sum ubar_s, and its size gets sum w_s/6 Y.k_s + beta_s ubar_s.k_{s-1}.
 template <class C>
-KT_HD void sm_rk4_bwd(double M, const SmPrm<double>& P, const double* c, const double* y, double h,
-                      double* ybar, double* hbar, double* cbar, double* pbar, double* yo) {
-  double u[4][C::kN], k[4][C::kN], kp;
-  for (int i = 0; i < C::kN; ++i) u[0][i] = y[i];
-  sm_rhs<C>(M, P, u[0], c, k[0], &kp);
-  for (int i = 0; i < C::kN; ++i) u[1][i] = y[i] + 0.5 * h * k[0][i];
-  sm_rhs<C>(M, P, u[1], c, k[1], &kp);
-  for (int i = 0; i < C::kN; ++i) u[2][i] = y[i] + 0.5 * h * k[1][i];
-  sm_rhs<C>(M, P, u[2], c, k[2], &kp);
-  for (int i = 0; i < C::kN; ++i) u[3][i] = y[i] + h * k[2][i];
-  sm_rhs<C>(M, P, u[3], c, k[3], &kp);
-  if (yo)
-    for (int i = 0; i < C::kN; ++i)
-      yo[i] = y[i] + h / 6.0 * (k[0][i] + 2.0 * k[1][i] + 2.0 * k[2][i] + k[3][i]);
-  double kb[4][C::kN], ub[C::kN];
-  const double w[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
-  const double beta[4] = {0.0, 0.5, 0.5, 1.0};  // u_s = y + beta_s h k_{s-1}
-  double hb = 0.0;
-  for (int s = 0; s < 4; ++s) {
-    double dot = 0.0;
-    for (int i = 0; i < C::kN; ++i) {
-      kb[s][i] = w[s] * h * ybar[i];
-      dot = dot + ybar[i] * k[s][i];
-    }
-    hb = hb + w[s] * dot;
-  }
-  KT_ROLLED
-  for (int s = 3; s >= 0; --s) {
-    sm_vjp_f<C>(M, P, u[s], c, kb[s], ub, cbar, pbar);
-    double dot = 0.0;
-    for (int i = 0; i < C::kN; ++i) {
-      ybar[i] = ybar[i] + ub[i];
-      if (s > 0) {
-        kb[s - 1][i] = kb[s - 1][i] + beta[s] * h * ub[i];
-        dot = dot + ub[i] * k[s - 1][i];
-      }
-    }
-    if (s > 0) hb = hb + beta[s] * dot;
-  }
-  *hbar = *hbar + hb;
-}
-
-// Reverse of one attempt from y with size h: cotangents Abar (of path A's
-// result) and Bbar (of path B's).  ybar += .., returns the size's cotangent.
-template <class C>
-KT_HD double sm_attempt_bwd(double M, const SmPrm<double>& P, const double* c, const double* y, double h,
-                            const double* Abar, const double* Bbar, double* ybar, double* cbar,
-                            double* pbar) {
-  double yb1[C::kN], k1[C::kN], k1p, pas1, t[C::kN], hb_half = 0.0, hb_full = 0.0;
+KT_HD double sm_attempt_bwd(const Frame& f, const SmPrm<double>& P, const double* c, const double* y,
+                            double hh, double gout, const double* yb_out, double hbar_extra,
+                            double* ybar, double* cbar, double* pbar, SmStages* st) {
+  constexpr int n = C::kN;
+  const double M = f.g.M;
+  double k1[n], k1p, yA[n], yB[n], pB = 0.0;
   sm_rhs<C>(M, P, y, c, k1, &k1p);
-  sm_rk4<C>(M, P, c, y, 0.0, k1, k1p, 0.5 * h, yb1, &pas1);
-  for (int i = 0; i < C::kN; ++i) t[i] = Bbar[i];
-  sm_rk4_bwd<C>(M, P, c, yb1, 0.5 * h, t, &hb_half, cbar, pbar, nullptr);  // second half step
-  sm_rk4_bwd<C>(M, P, c, y, 0.5 * h, t, &hb_half, cbar, pbar, nullptr);    // first half step
-  for (int i = 0; i < C::kN; ++i) ybar[i] = ybar[i] + t[i];
-  for (int i = 0; i < C::kN; ++i) t[i] = Abar[i];
-  sm_rk4_bwd<C>(M, P, c, y, h, t, &hb_full, cbar, pbar, nullptr);
-  for (int i = 0; i < C::kN; ++i) ybar[i] = ybar[i] + t[i];
-  return 0.5 * hb_half + hb_full;
-}
-
-// Paths A and B of an attempt and its error (sm_attempt's arithmetic).
-template <class C>
-KT_HD double sm_attempt_err(double M, const SmPrm<double>& P, const double* c, const double* y, double h,
-                            double* d) {
-  double yA[C::kN], yB1[C::kN], yB[C::kN], k1[C::kN], kb[C::kN], k1p, kbp, pa;
-  sm_rhs<C>(M, P, y, c, k1, &k1p);
-  sm_rk4<C>(M, P, c, y, 0.0, k1, k1p, h, yA, &pa);
-  sm_rk4<C>(M, P, c, y, 0.0, k1, k1p, 0.5 * h, yB1, &pa);
-  sm_rhs<C>(M, P, yB1, c, kb, &kbp);
-  sm_rk4<C>(M, P, c, yB1, 0.0, kb, kbp, 0.5 * h, yB, &pa);
-  double e2 = 0.0;
-  for (int i = 0; i < C::kN; ++i) {
+  sm_paths<C>(M, P, c, y, 0.0, k1, k1p, hh, yA, yB, &pB, st);
+  double d[n], e2 = 0.0;
+  for (int i = 0; i < n; ++i) {
     d[i] = yA[i] - yB[i];
     e2 = e2 + d[i] * d[i];
   }
-  return sqrt(e2) / 15.0;
+  const double e = sqrt(e2) / 15.0;
+  double dh, de;
+  sm_ctl_partials(e, f.tol, hh, &dh, &de);
+  const double eb = gout * de;
+  const double kap = (e > 0.0 && finite(e)) ? eb / (225.0 * e) : 0.0;
+  double hb = gout * dh + hbar_extra;
+  const double wst[4] = {1.0 / 6.0, 2.0 / 6.0, 2.0 / 6.0, 1.0 / 6.0};
+  double Y[n], bacc[n], kbn[n], k0s[n], uc[n], vc[n], ub[n];
+  double hs = 0.5 * hh, hsub = 0.0;
+  for (int i = 0; i < n; ++i) {
+    Y[i] = (yb_out ? yb_out[i] : 0.0) - kap * d[i];
+    bacc[i] = Y[i];
+    kbn[i] = hs * wst[3] * Y[i];
+    k0s[i] = 0.0;
+  }
+  KT_ROLLED
+  for (int q = 0; q <= 10; ++q) {
+    if (q == 4 || q == 7) {
+      // finish B2 (-> cotangent of B1's result) or B1; start B1 or A
+      hb = hb + 0.5 * hsub;
+      hsub = 0.0;
+      hs = (q == 4) ? 0.5 * hh : hh;
+      for (int i = 0; i < n; ++i) {
+        if (q == 7) ybar[i] = ybar[i] + bacc[i];
+        Y[i] = (q == 4) ? bacc[i] : kap * d[i];
+        bacc[i] = Y[i];
+        kbn[i] = hs * wst[3] * Y[i];
+      }
+    }
+    if (q == 10) {
+      hb = hb + hsub;
+      for (int i = 0; i < n; ++i) ybar[i] = ybar[i] + bacc[i];
+    }
+    const int t = q < 10 ? 9 - q : 0;
+    int sub, s;
+    sm_stage_of(t, &sub, &s);
+    for (int i = 0; i < n; ++i) {
+      uc[i] = (q == 10) ? y[i] : st->u[t][i];
+      vc[i] = (q == 10) ? k0s[i] : kbn[i];
+    }
+    sm_vjp_f<C>(M, P, uc, c, vc, ub, cbar, pbar);
+    if (q == 10) {
+      for (int i = 0; i < n; ++i) ybar[i] = ybar[i] + ub[i];
+      break;
+    }
+    // direct size term of stage s and the base's cotangent
+    double dk = 0.0;
+    for (int i = 0; i < n; ++i) {
+      dk = dk + Y[i] * st->k[t][i];
+      bacc[i] = bacc[i] + ub[i];
+    }
+    hsub = hsub + wst[s] * dk;
+    if (s >= 1) {
+      // stage s's input was base + beta_s hs k_{s-1}
+      const double beta = (s == 3) ? 1.0 : 0.5;
+      double dkm = 0.0;
+      for (int i = 0; i < n; ++i) {
+        const double km = (s == 1 && sub < 2) ? k1[i] : st->k[t - 1][i];
+        dkm = dkm + ub[i] * km;
+        const double nk = hs * wst[s - 1] * Y[i] + beta * hs * ub[i];
+        if (s == 1 && sub < 2) {
+          k0s[i] = k0s[i] + nk;
+        } else {
+          kbn[i] = nk;
+        }
+      }
+      hsub = hsub + beta * dkm;
+      if (s == 1 && sub < 2) {
+        // the shared k1's direct size term (w_1 / 6 Y . k1)
+        double d1 = 0.0;
+        for (int i = 0; i < n; ++i) d1 = d1 + Y[i] * k1[i];
+        hsub = hsub + wst[0] * d1;
+      }
+    }
+  }
+  return hb;
 }
 
 constexpr int kSmMaxAttempts = 66;  // reject cap 64 + the accepted attempt
 
-// Reverse of accepted step n from (y_n, H_n).  In: ybar = cotangent of
-// y_{n+1}, *Hbar = cotangent of H_{n+1}, hbar_acc = extra cotangent of the
-// accepted size (the event's).  Out: ybar = cotangent of y_n, *Hbar = of H_n.
+// Reverse of accepted step n from (y_n, H_n, attempts).  In: ybar =
+// cotangent of y_{n+1}, *Hbar = cotangent of H_{n+1}, hbar_acc = extra
+// cotangent of the accepted size (the event's).  Out: ybar = cotangent of
+// y_n, *Hbar = of H_n.
 template <class C>
 KT_HD void sm_step_bwd(const Frame& f, const SmPrm<double>& P, const double* c, const SmSt& st,
-                       double hbar_acc, double* ybar, double* Hbar, double* cbar, double* pbar) {
+                       double hbar_acc, double* ybar, double* Hbar, double* cbar, double* pbar,
+                       SmStages* stg) {
   const double M = f.g.M;
-  double hs[kSmMaxAttempts], es[kSmMaxAttempts], d[C::kN];
-  // replay the attempts: sizes and errors
-  int na = 0;
-  double h = st.H;
-  KT_ROLLED
-  for (;;) {
-    hs[na] = h;
-    es[na] = sm_attempt_err<C>(M, P, c, st.y, h, d);
-    const double e = es[na];
-    ++na;
-    const int res = doubling_update(e, f.tol, &h);
-    if (res == 1 || na == kSmMaxAttempts) break;
+  double hs[kSmMaxAttempts];
+  const int na = st.na < kSmMaxAttempts ? st.na : kSmMaxAttempts;
+  hs[0] = st.H;
+  if (na > 1) {
+    // sizes of the attempts: the controller after each rejection
+    double k1[C::kN], k1p, yo[C::kN], po;
+    sm_rhs<C>(M, P, st.y, c, k1, &k1p);
+    double h = st.H;
+    KT_ROLLED
+    for (int j = 0; j + 1 < na; ++j) {
+      sm_attempt<C>(M, P, f.tol, c, st.y, 0.0, k1, k1p, &h, yo, &po);
+      hs[j + 1] = h;
+    }
   }
-  double yb_out[C::kN], Abar[C::kN], Bbar[C::kN];
+  double yb_out[C::kN];
   for (int i = 0; i < C::kN; ++i) {
     yb_out[i] = ybar[i];
     ybar[i] = 0.0;
   }
-  // accepted attempt: H_{n+1} = sigma(h_R, e_R), y_{n+1} = B(y_n, h_R)
-  double dh, de;
-  sm_ctl_partials(es[na - 1], f.tol, hs[na - 1], &dh, &de);
-  double hb = *Hbar * dh + hbar_acc;
-  double eb = *Hbar * de;
+  double gout = *Hbar;
   KT_ROLLED
   for (int j = na - 1; j >= 0; --j) {
-    // cotangent of e_j -> paths A and B through d = A - B
-    const double e = es[j];
-    sm_attempt_err<C>(M, P, c, st.y, hs[j], d);
-    const double kap = (e > 0.0 && finite(e)) ? eb / (225.0 * e) : 0.0;
-    for (int i = 0; i < C::kN; ++i) {
-      Abar[i] = kap * d[i];
-      Bbar[i] = (j == na - 1 ? yb_out[i] : 0.0) - kap * d[i];
-    }
-    hb = hb + sm_attempt_bwd<C>(M, P, c, st.y, hs[j], Abar, Bbar, ybar, cbar, pbar);
-    if (j > 0) {
-      // h_j = rho(h_{j-1}, e_{j-1}) (a rejection)
-      sm_ctl_partials(es[j - 1], f.tol, hs[j - 1], &dh, &de);
-      eb = hb * de;
-      hb = hb * dh;
-    }
+    const bool acc = (j == na - 1);
+    gout = sm_attempt_bwd<C>(f, P, c, st.y, hs[j], gout, acc ? yb_out : nullptr, acc ? hbar_acc : 0.0,
+                             ybar, cbar, pbar, stg);
   }
-  *Hbar = hb;
+  *Hbar = gout;
 }
 
-// Cotangents of the event step's inputs from (gbar, rbar):
-// (y_{N-1}, y_N, constants, prm, h) -> ybar_prev, ybar_N, cbar, pbar, hbar.
+// Cotangents of the event step's inputs from (gbar, rbar): the hit state
+// yh = Hermite(y_{N-1}, y_N, f_{N-1}, f_N; h, alpha*) feeds the outputs
+// (r_hit; g through the disk redshift), differentiated in Dual over (yh,
+// constants, a, Q, Lambda); alpha* moves with the inputs as
+// d alpha* = -dq / q'(alpha*) (q the equator coordinate's interpolant minus
+// its target), so the inputs also get lambda dq/dx with lambda = -alphabar/q';
+// f_{N-1}, f_N pass their cotangents on through VJPs of the RHS.
 template <class C>
-KT_HD void sm_event_bwd(double M, const SmPrm<double>& P, const double* c, const SmEvent& ev,
+KT_HD void sm_event_bwd(const Frame& f, const SmPrm<double>& P, const double* c, const SmEvent& ev,
                         double gbar, double rbar, double* ybp, double* ybN, double* cbar,
                         double* pbar, double* hbar) {
-  constexpr int NE = 2 * C::kN + C::kC + kSmPrm + 1;
-  typedef Dual<NE> D;
-  D yp[C::kN], y[C::kN], cd[C::kC], fp[C::kN], fN[C::kN], fpp, fNp;
-  for (int i = 0; i < C::kN; ++i) {
-    yp[i] = D::var(ev.yp[i], i);
-    y[i] = D::var(ev.y[i], C::kN + i);
-  }
-  for (int j = 0; j < C::kC; ++j) cd[j] = D::var(c[j], 2 * C::kN + j);
+  constexpr int n = C::kN;
+  constexpr int ND = n + C::kC + kSmPrm;
+  typedef Dual<ND> D;
+  const double M = f.g.M;
+  double fe[2][n], pp;
+  KT_ROLLED
+  for (int w = 0; w < 2; ++w) sm_rhs<C>(M, P, w == 0 ? ev.yp : ev.y, c, fe[w], &pp);
+  const double h = ev.h, al = ev.alpha;
+  const double a2 = al * al, a3 = a2 * al;
+  const double b00 = 2.0 * a3 - 3.0 * a2 + 1.0, b10 = a3 - 2.0 * a2 + al, b01 = 3.0 * a2 - 2.0 * a3,
+               b11 = a3 - a2;
+  const double d00 = 6.0 * a2 - 6.0 * al, d10 = 3.0 * a2 - 4.0 * al + 1.0, d01 = 6.0 * al - 6.0 * a2,
+               d11 = 3.0 * a2 - 2.0 * al;
+  D yh[n], cd[C::kC];
+  for (int i = 0; i < n; ++i)
+    yh[i] = D::var(b00 * ev.yp[i] + b10 * (h * fe[0][i]) + b01 * ev.y[i] + b11 * (h * fe[1][i]), i);
+  for (int j = 0; j < C::kC; ++j) cd[j] = D::var(c[j], n + j);
   SmPrm<D> Pd;
-  Pd.a = D::var(P.a, 2 * C::kN + C::kC);
-  Pd.Q = D::var(P.Q, 2 * C::kN + C::kC + 1);
-  Pd.L = D::var(P.L, 2 * C::kN + C::kC + 2);
-  const D hd = D::var(ev.h, NE - 1);
-  sm_rhs<C>(M, Pd, yp, cd, fp, &fpp);
-  sm_rhs<C>(M, Pd, y, cd, fN, &fNp);
-  const int e = C::kEq;
-  // implicit crossing parameter
-  D q = sm_hermite_h(yp[e], y[e], fp[e], fN[e], hd, D(ev.alpha)) - C::kEqTarget;
-  const double dqda = sm_hermite_da(yp[e].v, y[e].v, fp[e].v, fN[e].v, ev.h, ev.alpha);
-  D al(ev.alpha);
-  for (int k = 0; k < NE; ++k) al.d[k] = -q.d[k] / dqda;
-  D r, pph;
-  if (C::kN == 6) {
-    D yh[C::kN];
-    for (int i = 0; i < C::kN; ++i) yh[i] = sm_hermite_h(yp[i], y[i], fp[i], fN[i], hd, al);
-    r = C::radius(Pd.a, yh);
-    pph = yh[0] * yh[4] - yh[1] * yh[3];
-  } else {
-    r = sm_hermite_h(yp[0], y[0], fp[0], fN[0], hd, al);
-    pph = cd[C::kC - 1];
-  }
+  Pd.a = D::var(P.a, n + C::kC);
+  Pd.Q = D::var(P.Q, n + C::kC + 1);
+  Pd.L = D::var(P.L, n + C::kC + 2);
+  const D r = C::radius(Pd.a, yh);
+  const D pph = (n == 6) ? yh[0] * yh[4] - yh[1] * yh[3] : cd[C::kC - 1];
   D red;
   const bool has = sm_redshift<D>(M, Pd, r, cd[0], pph, &red) && ev.deriv;
-  double s[NE];
-  for (int k = 0; k < NE; ++k) s[k] = rbar * r.d[k] + (has ? gbar * red.d[k] : 0.0);
-  for (int i = 0; i < C::kN; ++i) {
-    ybp[i] = s[i];
-    ybN[i] = s[C::kN + i];
+  double yhb[n];
+  for (int i = 0; i < n; ++i) yhb[i] = rbar * r.d[i] + (has ? gbar * red.d[i] : 0.0);
+  for (int j = 0; j < C::kC; ++j) cbar[j] = cbar[j] + rbar * r.d[n + j] + (has ? gbar * red.d[n + j] : 0.0);
+  for (int q = 0; q < kSmPrm; ++q)
+    pbar[q] = pbar[q] + rbar * r.d[n + C::kC + q] + (has ? gbar * red.d[n + C::kC + q] : 0.0);
+  // alpha
+  double alb = 0.0;
+  for (int i = 0; i < n; ++i)
+    alb = alb + yhb[i] * (d00 * ev.yp[i] + d10 * (h * fe[0][i]) + d01 * ev.y[i] + d11 * (h * fe[1][i]));
+  const int e = C::kEq;
+  const double dqda = d00 * ev.yp[e] + d10 * (h * fe[0][e]) + d01 * ev.y[e] + d11 * (h * fe[1][e]);
+  const double lam = -alb / dqda;
+  double fb[2][n];
+  double hb = 0.0;
+  for (int i = 0; i < n; ++i) {
+    const double g = yhb[i] + (i == e ? lam : 0.0);
+    ybp[i] = b00 * g;
+    ybN[i] = b01 * g;
+    fb[0][i] = b10 * h * g;
+    fb[1][i] = b11 * h * g;
+    hb = hb + (b10 * fe[0][i] + b11 * fe[1][i]) * g;
   }
-  for (int j = 0; j < C::kC; ++j) cbar[j] = cbar[j] + s[2 * C::kN + j];
-  for (int q2 = 0; q2 < kSmPrm; ++q2) pbar[q2] = pbar[q2] + s[2 * C::kN + C::kC + q2];
-  *hbar = s[NE - 1];
+  double ub[n];
+  KT_ROLLED
+  for (int w = 0; w < 2; ++w) {
+    sm_vjp_f<C>(M, P, w == 0 ? ev.yp : ev.y, c, fb[w], ub, cbar, pbar);
+    for (int i = 0; i < n; ++i) {
+      if (w == 0)
+        ybp[i] = ybp[i] + ub[i];
+      else
+        ybN[i] = ybN[i] + ub[i];
+    }
+  }
+  *hbar = hb;
 }
 
 // Scratch of one ray's adjoint (per thread, local memory).
@@ -558,6 +648,7 @@ struct SmScratch {
   SmCk ck1[kSmCkCap];
   SmCk ck2[kSmCkCap];
   SmSt st[kSmCkSteps];
+  SmStages stages;
 };
 
 // Reverse sweep of a ray traced with recording (N accepted steps, the last
@@ -568,11 +659,10 @@ template <class C>
 KT_HD void sm_adjoint(const Frame& f, const SmPrm<double>& P, const double* c, const SmEvent& ev,
                       int N, int k1, double gbar, double rbar, SmScratch* sc, double* ybar,
                       double* cbar, double* pbar) {
-  const double M = f.g.M;
   double ybN[C::kN], yb_direct[C::kN], hbar_ev = 0.0;
   for (int j = 0; j < C::kC; ++j) cbar[j] = 0.0;
   for (int q = 0; q < kSmPrm; ++q) pbar[q] = 0.0;
-  sm_event_bwd<C>(M, P, c, ev, gbar, rbar, yb_direct, ybN, cbar, pbar, &hbar_ev);
+  sm_event_bwd<C>(f, P, c, ev, gbar, rbar, yb_direct, ybN, cbar, pbar, &hbar_ev);
   // The walk starts at step N-1 with the cotangent of y_N (H_N unused); the
   // direct seed of y_{N-1} joins after that step.
   for (int i = 0; i < C::kN; ++i) ybar[i] = ybN[i];
@@ -589,10 +679,14 @@ KT_HD void sm_adjoint(const Frame& f, const SmPrm<double>& P, const double* c, c
     for (int sub = nsub - 1; sub >= 0; --sub) {
       const int t0 = sub * kSmCkSteps;
       const int tl = (len - t0 < kSmCkSteps) ? len - t0 : kSmCkSteps;
-      sm_replay<C>(f, P, c, nsub > 1 ? sc->ck2[sub] : sc->ck1[sgi], tl, sc->st, nullptr, 0);
+      // the last sub-segment (steps from a multiple of 32 up to N-1) is still
+      // in the forward's ring of step starts
+      if (!(sgi == nseg - 1 && sub == nsub - 1))
+        sm_replay<C>(f, P, c, nsub > 1 ? sc->ck2[sub] : sc->ck1[sgi], tl, sc->st, nullptr, 0);
       KT_ROLLED
       for (int m = tl - 1; m >= 0; --m) {
-        sm_step_bwd<C>(f, P, c, sc->st[m], last ? hbar_ev : 0.0, ybar, &Hbar, cbar, pbar);
+        sm_step_bwd<C>(f, P, c, sc->st[m], last ? hbar_ev : 0.0, ybar, &Hbar, cbar, pbar,
+                       &sc->stages);
         if (last) {
           for (int i = 0; i < C::kN; ++i) ybar[i] = ybar[i] + yb_direct[i];
           last = false;
@@ -634,80 +728,84 @@ enum : int {
   kGNumUnrecorded = 8, kGSlots = 9
 };
 
-// One pixel of the smooth tracer: outputs into *o; with a cotangent source,
-// the pixel's loss and gradient into g[kGSlots] (theta in radians).
-template <bool kGrad>
-KT_HD void sm_pixel(const Frame& f, uint32_t pix, bool force_bl, const SmCot& cot, RayResult* o,
-                    double* g, SmScratch* sc) {
+// One pixel of the smooth tracer in chart C: outputs into *o; with a
+// cotangent source, the pixel's loss, gradient (theta in radians) and counts
+// into g[kGSlots].  In the KS chart a ray whose KS initialisation fails
+// (init_ks_state, main.cpp:1533-1538) is not traced: returns false, and the
+// caller hands it to the BL chart.
+template <class C, bool kGrad>
+KT_HD bool sm_pixel(const Frame& f, uint32_t pix, const SmCot& cot, RayResult* o, double* g,
+                    SmScratch* sc) {
+  constexpr bool kKS = C::kN == 6;
   const int px = (int)(pix % (uint32_t)f.cam.W), py = (int)(pix / (uint32_t)f.cam.W);
   double al, be;
   pixel_angles(f.cam, px, py, &al, &be);
   const double M = f.g.M;
   const SmPrm<double> P = sm_prm<double>(f.g);
-  double ybl[4], cbl[2];
+  double ybl[4], cbl[2], y0[C::kN], c0[C::kC];
   sm_camera<double>(M, P, f.cam.r_obs, f.cam.theta_obs, al, be, ybl, cbl);
-  bool ks = (f.chart == 0) && !force_bl;
-  double yks[6], cks[1];
-  if (ks) ks = sm_bl_to_ks<double>(M, P, ybl, cbl, f.cam.phi_obs, yks, cks);
+  if (kKS) {
+    double yk[6], ck[1];
+    if (!sm_bl_to_ks<double>(M, P, ybl, cbl, f.cam.phi_obs, yk, ck)) return false;
+    for (int i = 0; i < C::kN; ++i) y0[i] = yk[i];
+    c0[0] = ck[0];
+  } else {
+    for (int i = 0; i < C::kN; ++i) y0[i] = ybl[i];
+    for (int j = 0; j < C::kC; ++j) c0[j] = cbl[j];
+  }
   SmEvent ev;
   int k1 = 0, nck = 0;
   SmCk* ck = kGrad ? sc->ck1 : nullptr;
-  const int N = ks ? sm_trace<ChartKS>(f, P, yks, cks, 0.0, o, &ev, ck, &k1, &nck)
-                   : sm_trace<ChartBL>(f, P, ybl, cbl, f.cam.phi_obs, o, &ev, ck, &k1, &nck);
-  if (!kGrad) return;
+  const int N = sm_trace<C>(f, P, y0, c0, kKS ? 0.0 : f.cam.phi_obs, o, &ev, ck, &k1, &nck,
+                            kGrad ? sc->st : nullptr);
+  if (!kGrad) return true;
   for (int q = 0; q < kGSlots; ++q) g[q] = 0.0;
-  g[kGNumBL] = ks ? 0.0 : 1.0;
-  if (o->outcome != kOutDisk) return;
+  g[kGNumBL] = kKS ? 0.0 : 1.0;
+  if (o->outcome != kOutDisk) return true;
   double gbar = 0.0, rbar = 0.0;
   if (cot.mode == 1) {
     gbar = cot.g ? cot.g[pix] : 0.0;
     rbar = cot.r ? cot.r[pix] : 0.0;
   } else if (cot.mode == 2) {
-    if (cot.t_out[pix] != kOutDisk) return;
+    if (cot.t_out[pix] != kOutDisk) return true;
     const double dg = o->red - cot.t_g[pix], dr = o->r - cot.t_r[pix];
     g[kGLoss] = cot.w_g * dg * dg + cot.w_r * dr * dr;
     gbar = 2.0 * cot.w_g * dg;
     rbar = 2.0 * cot.w_r * dr;
   }
-  if (gbar == 0.0 && rbar == 0.0) return;
+  if (gbar == 0.0 && rbar == 0.0) return true;
   if (N == 0) {
     g[kGNumUnrecorded] = 1.0;
-    return;
+    return true;
   }
   g[kGNumGrad] = 1.0;
-  double ybar[kSmMaxN], cbar[2], pbar[kSmPrm];
+  double ybar[C::kN], cbar[C::kC], pbar[kSmPrm];
+  sm_adjoint<C>(f, P, c0, ev, N, k1, gbar, rbar, sc, ybar, cbar, pbar);
+  // chain through the camera ray: Dual over (a, Q, Lambda, theta_obs, r_obs)
   typedef Dual<5> D5;
   SmPrm<D5> Pd;
   Pd.a = D5::var(P.a, 0);
   Pd.Q = D5::var(P.Q, 1);
   Pd.L = D5::var(P.L, 2);
   const D5 thd = D5::var(f.cam.theta_obs, 3), rd = D5::var(f.cam.r_obs, 4);
-  D5 yb5[4], cb5[2];
+  D5 yb5[4], cb5[2], y5[C::kN], c5[C::kC];
   sm_camera<D5>(M, Pd, rd, thd, al, be, yb5, cb5);
-  double gi[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-  if (ks) {
-    sm_adjoint<ChartKS>(f, P, cks, ev, N, k1, gbar, rbar, sc, ybar, cbar, pbar);
-    D5 y5[6], c5[1];
-    sm_bl_to_ks<D5>(M, Pd, yb5, cb5, f.cam.phi_obs, y5, c5);
-    for (int k = 0; k < 5; ++k) {
-      double s = cbar[0] * c5[0].d[k];
-      for (int i = 0; i < 6; ++i) s = s + ybar[i] * y5[i].d[k];
-      gi[k] = s;
-    }
+  if (kKS) {
+    D5 yk[6], ck5[1];
+    sm_bl_to_ks<D5>(M, Pd, yb5, cb5, f.cam.phi_obs, yk, ck5);
+    for (int i = 0; i < C::kN; ++i) y5[i] = yk[i];
+    c5[0] = ck5[0];
   } else {
-    sm_adjoint<ChartBL>(f, P, cbl, ev, N, k1, gbar, rbar, sc, ybar, cbar, pbar);
-    for (int k = 0; k < 5; ++k) {
-      double s = cbar[0] * cb5[0].d[k] + cbar[1] * cb5[1].d[k];
-      for (int i = 0; i < 4; ++i) s = s + ybar[i] * yb5[i].d[k];
-      gi[k] = s;
-    }
+    for (int i = 0; i < C::kN; ++i) y5[i] = yb5[i];
+    for (int j = 0; j < C::kC; ++j) c5[j] = cb5[j];
   }
-  for (int q = 0; q < kSmPrm; ++q) gi[q] = gi[q] + pbar[q];
-  g[kGA] = gi[0];
-  g[kGQ] = gi[1];
-  g[kGLambda] = gi[2];
-  g[kGTheta] = gi[3];
-  g[kGRobs] = gi[4];
+  for (int k = 0; k < 5; ++k) {
+    double acc = k < kSmPrm ? pbar[k] : 0.0;
+    for (int j = 0; j < C::kC; ++j) acc = acc + cbar[j] * c5[j].d[k];
+    for (int i = 0; i < C::kN; ++i) acc = acc + ybar[i] * y5[i].d[k];
+    g[k] = acc;
+  }
+  return true;
 }
 
 }  // namespace kt

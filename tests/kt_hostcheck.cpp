@@ -161,10 +161,17 @@ extern "C" int hc_smooth_pixels(const kt_frame_desc* d, int64_t n, const uint32_
     for (int64_t i = 0; i < n; ++i) {
       RayResult o;
       double g[kGSlots];
-      if (mode == 0)
-        sm_pixel<false>(f, pix[i], force_bl != 0, cot, &o, g, nullptr);
-      else
-        sm_pixel<true>(f, pix[i], force_bl != 0, cot, &o, g, sc);
+      const bool ks = f.chart == KT_CHART_KS && !force_bl;
+      bool done = false;
+      if (ks)
+        done = mode == 0 ? sm_pixel<ChartKS, false>(f, pix[i], cot, &o, g, nullptr)
+                         : sm_pixel<ChartKS, true>(f, pix[i], cot, &o, g, sc);
+      if (!done) {
+        if (mode == 0)
+          sm_pixel<ChartBL, false>(f, pix[i], cot, &o, g, nullptr);
+        else
+          sm_pixel<ChartBL, true>(f, pix[i], cot, &o, g, sc);
+      }
       outcome[i] = (uint8_t)o.outcome;
       r[i] = o.r;
       red[i] = o.red;
