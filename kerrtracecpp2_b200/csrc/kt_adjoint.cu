@@ -8,7 +8,8 @@
 // (SmScratch, ~12 KB per thread), and for a disk hit with a non-zero
 // cotangent runs the reverse sweep right away; it writes the ray's loss and
 // gradient contributions to a [kGSlots][n] array, which k_sum_* reduce in a
-// fixed order (the sum does not depend on the schedule).
+// fixed order (the sum does not depend on the schedule).  The tangent kernel
+// gives one parameter's entry by forward mode (no recording).
 //
 // Compiled with --fmad=false: the recorded forward and every replay of it
 // must round identically, which contraction choices made per inlining site
@@ -47,6 +48,32 @@ __global__ void __launch_bounds__(kSmBlock) k_smooth(const Frame f, const OutSoA
     if (out.outcome) write_result(out, pix, o);
     if (kGrad)
       for (int q = 0; q < kGSlots; ++q) job.contrib[(size_t)q * n + pix] = g[q];
+  }
+}
+
+// The same over the forward-mode tangent along job.tangent_dir.
+template <class C>
+__global__ void __launch_bounds__(kSmBlock) k_smooth_tangent(const Frame f, const OutSoA out,
+                                                             const SmJob job, uint32_t n,
+                                                             const uint32_t* __restrict__ list,
+                                                             const uint32_t* __restrict__ n_dev,
+                                                             uint32_t* __restrict__ queue,
+                                                             uint32_t* __restrict__ fb_pix,
+                                                             uint32_t* __restrict__ fb_n) {
+  const uint32_t count = n_dev ? *n_dev : n;
+  KT_ROLLED
+  for (;;) {
+    const uint32_t i = atomicAdd(queue, 1u);
+    if (i >= count) break;
+    const uint32_t pix = list ? list[i] : i;
+    RayResult o;
+    double g[kGSlots];
+    if (!sm_pixel_tangent<C>(f, pix, job.tangent_dir, job.cot, &o, g)) {
+      fb_pix[atomicAdd(fb_n, 1u)] = pix;
+      continue;
+    }
+    if (out.outcome) write_result(out, pix, o);
+    for (int q = 0; q < kGSlots; ++q) job.contrib[(size_t)q * n + pix] = g[q];
   }
 }
 
@@ -89,6 +116,20 @@ __global__ void __launch_bounds__(kSumThreads) k_sum_final(const double* __restr
   }
 }
 
+template <class C>
+static cudaError_t tangent_launch(const Frame& f, const OutSoA& out, uint32_t n, const SmJob& job,
+                                  const uint32_t* list, const uint32_t* n_dev, uint32_t* queue,
+                                  uint32_t* fb_pix, uint32_t* fb_n, int device, cudaStream_t st) {
+  int sms = 0, per_sm = 0;
+  cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  if (e != cudaSuccess) return e;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_smooth_tangent<C>, kSmBlock, 0);
+  if (e != cudaSuccess) return e;
+  const int grid = sms * (per_sm < 1 ? 1 : per_sm);
+  k_smooth_tangent<C><<<grid, kSmBlock, 0, st>>>(f, out, job, n, list, n_dev, queue, fb_pix, fb_n);
+  return cudaGetLastError();
+}
+
 template <class C, bool kGrad>
 static cudaError_t smooth_launch(const Frame& f, const OutSoA& out, uint32_t n, const SmJob& job,
                                  const uint32_t* list, const uint32_t* n_dev, uint32_t* queue,
@@ -109,6 +150,17 @@ cudaError_t launch_smooth(const Frame& f, const OutSoA& out, uint32_t n, const S
   memset(&none, 0, sizeof none);
   const SmJob& jb = job ? *job : none;
   const bool grad = job != nullptr;
+  if (grad && job->tangent_dir >= 0) {
+    if (f.chart == 0 && !job->force_bl) {
+      cudaError_t e = tangent_launch<ChartKS>(f, out, n, jb, nullptr, nullptr, counters, fb_pix,
+                                              counters + 2, device, st);
+      if (e != cudaSuccess) return e;
+      return tangent_launch<ChartBL>(f, out, n, jb, fb_pix, counters + 2, counters + 1, nullptr,
+                                     nullptr, device, st);
+    }
+    return tangent_launch<ChartBL>(f, out, n, jb, nullptr, nullptr, counters, nullptr, nullptr,
+                                   device, st);
+  }
   if (f.chart == 0 && !(job && job->force_bl)) {
     // KS pass over all pixels, then BL over the rays whose KS init failed
     cudaError_t e = grad ? smooth_launch<ChartKS, true>(f, out, n, jb, nullptr, nullptr, counters,

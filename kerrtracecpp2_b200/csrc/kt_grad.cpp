@@ -25,11 +25,15 @@ struct EventPair {
 };
 
 // One gradient pass: launch, reduce, copy the kGSlots sums to `sums`.
+// force_bl: trace every ray in the BL chart; tangent_dir >= 0: forward-mode
+// tangent along that parameter instead of the reverse sweep.
 kt_status grad_pass(kt_context* ctx, const kt::Frame& f, const kt::OutSoA& out, uint32_t n,
-                    const kt::SmCot& cot, bool force_bl, cudaStream_t st, double* sums, float* ms) {
+                    const kt::SmCot& cot, bool force_bl, int tangent_dir, cudaStream_t st,
+                    double* sums, float* ms) {
   kt::SmJob job;
   job.cot = cot;
   job.force_bl = force_bl ? 1 : 0;
+  job.tangent_dir = tangent_dir;
   job.contrib = ctx->d_grad;
   EventPair ev;
   KT_CUDA(ctx, cudaEventCreate(&ev.a), "event");
@@ -75,7 +79,7 @@ kt_status grad_run(kt_context* ctx, const kt_frame_desc* desc_in, const kt::SmCo
   if (out_soa) out = to_out(out_soa);
   double s[kt::kGSlots], sl[kt::kGSlots];
   float ms = 0.f, ms_l = 0.f;
-  r = grad_pass(ctx, f, out, (uint32_t)n, cot, false, st, s, &ms);
+  r = grad_pass(ctx, f, out, (uint32_t)n, cot, false, -1, st, s, &ms);
   if (r != KT_OK) return r;
   double lambda = s[kt::kGLambda];
   if (f.chart == KT_CHART_KS) {
@@ -83,7 +87,8 @@ kt_status grad_run(kt_context* ctx, const kt_frame_desc* desc_in, const kt::SmCo
     if (!(flags & KT_GRAD_SKIP_LAMBDA)) {
       kt::OutSoA none;
       memset(&none, 0, sizeof none);
-      r = grad_pass(ctx, f, none, (uint32_t)n, cot, true, st, sl, &ms_l);
+      // one derivative in the BL chart: forward-mode tangent along Lambda
+      r = grad_pass(ctx, f, none, (uint32_t)n, cot, true, kt::kGLambda, st, sl, &ms_l);
       if (r != KT_OK) return r;
       lambda = sl[kt::kGLambda];
     }

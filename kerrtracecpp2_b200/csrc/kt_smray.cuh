@@ -712,10 +712,13 @@ struct SmCot {
 };
 
 // A launch of the smooth kernel with gradients: cotangent source, chart
-// override (trace every ray in the BL chart) and the [kGSlots][n] output.
+// override (trace every ray in the BL chart), reverse sweep (tangent_dir < 0)
+// or forward-mode tangent along one parameter (tangent_dir = kGA..kGRobs),
+// and the [kGSlots][n] output.
 struct SmJob {
   SmCot cot;
   int force_bl;
+  int tangent_dir;
   double* contrib;
 };
 
@@ -805,6 +808,305 @@ KT_HD bool sm_pixel(const Frame& f, uint32_t pix, const SmCot& cot, RayResult* o
     for (int i = 0; i < C::kN; ++i) acc = acc + ybar[i] * y5[i].d[k];
     g[k] = acc;
   }
+  return true;
+}
+
+// ---- forward-mode tangent along one parameter -----------------------------
+// The same tracer with every quantity a Dual<1>: the values are computed by
+// the same operations in the same order as sm_trace's, so the trace (steps,
+// events, outputs) is the smooth forward's bit for bit, and the tangents are
+// the derivative of the discrete map along one parameter, the controller
+// included (the derivative the reverse sweep gives for that parameter).
+// Cost: one pass, no checkpoints; used where a single derivative is needed
+// (a KS frame's Lambda entry, which lives in the BL chart).
+typedef Dual<1> T1;
+
+template <class C>
+KT_HD_CALL void sm_paths_t(double M, const SmPrm<T1>& P, const T1* c, const T1* y, double pas,
+                           const T1* k1, double k1p, const T1& hh, T1* yA, T1* yB, double* pB) {
+  constexpr int n = C::kN;
+  T1 base[n], kp[n], sum[n], yB1[n], u[n], k[n], kk;
+  double pbase = pas, sump = k1p, pB1 = pas;
+  KT_ROLLED
+  for (int t = 0; t < 10; ++t) {
+    int sub, s;
+    sm_stage_of(t, &sub, &s);
+    const T1 hs = sub == 0 ? hh : 0.5 * hh;
+    if (s == 1 && sub < 2) {
+      for (int i = 0; i < n; ++i) {
+        base[i] = y[i];
+        kp[i] = k1[i];
+        sum[i] = k1[i];
+      }
+      pbase = pas;
+      sump = k1p;
+    }
+    if (s == 0) {
+      for (int i = 0; i < n; ++i) {
+        base[i] = yB1[i];
+        u[i] = yB1[i];
+      }
+      pbase = pB1;
+    } else {
+      const T1 cs = (s == 3) ? hs : 0.5 * hs;
+      for (int i = 0; i < n; ++i) u[i] = base[i] + cs * kp[i];
+    }
+    sm_rhs<C>(M, P, u, c, k, &kk);
+    if (s == 0) {
+      for (int i = 0; i < n; ++i) {
+        kp[i] = k[i];
+        sum[i] = k[i];
+      }
+      sump = kk.v;
+      continue;
+    }
+    const double w = (s == 3) ? 1.0 : 2.0;
+    for (int i = 0; i < n; ++i) {
+      sum[i] = sum[i] + w * k[i];
+      kp[i] = k[i];
+    }
+    sump = sump + w * kk.v;
+    if (s == 3) {
+      for (int i = 0; i < n; ++i) {
+        const T1 r = base[i] + hs / 6.0 * sum[i];
+        if (sub == 0) yA[i] = r;
+        if (sub == 1) yB1[i] = r;
+        if (sub == 2) yB[i] = r;
+      }
+      const double pr = pbase + hs.v / 6.0 * sump;
+      pB1 = sub == 1 ? pr : pB1;
+      *pB = sub == 2 ? pr : *pB;
+    }
+  }
+}
+
+// doubling_update on Dual<1>: the same branches on the values; the new dlam's
+// tangent from the step size's and the error's.
+KT_HD int sm_update_t(const T1& err, double tol, T1* h) {
+  if (!finite(err.v)) {
+    const bool big = finite(h->v) && h->v > 1e-10;
+    *h = big ? (*h) * 0.5 : T1(1e-6);
+    if (h->v < 1e-10) *h = T1(1e-10);
+    return -1;
+  }
+  const bool accepted = (err.v < tol || h->v < 1e-10);
+  if (accepted) {
+    T1 scale(4.0);
+    if (err.v > 1e-14) {
+      scale.v = 0.9 * ktm_pow(tol / err.v, 0.2);
+      scale.d[0] = -0.2 * scale.v / err.v * err.d[0];
+    }
+    T1 hn = (*h) * scale;
+    if (!finite(hn.v)) hn = *h;
+    *h = hn;
+    if (h->v > 100.0) *h = T1(100.0);
+    if (h->v < 1e-10) *h = T1(1e-10);
+  } else {
+    const T1 half = (*h) * 0.5;
+    const T1 h09 = (*h) * 0.9;
+    const double pw = ktm_pow(tol / err.v, 0.25);
+    T1 hn;
+    hn.v = h09.v * pw;
+    hn.d[0] = h09.d[0] * pw + h09.v * (-0.25 * pw / err.v * err.d[0]);
+    if (!finite(hn.v)) hn = half;
+    *h = hn;
+    if (h->v > half.v) *h = half;
+    if (h->v < 1e-10) *h = T1(1e-10);
+  }
+  return accepted ? 1 : 0;
+}
+
+template <class C>
+KT_HD int sm_attempt_t(double M, const SmPrm<T1>& P, double tol, const T1* c, const T1* y, double pas,
+                       const T1* k1, double k1p, T1* h, T1* yo, double* paso) {
+  T1 yA[C::kN], yB[C::kN];
+  double pB = 0.0;
+  sm_paths_t<C>(M, P, c, y, pas, k1, k1p, *h, yA, yB, &pB);
+  T1 e2(0.0);
+  for (int i = 0; i < C::kN; ++i) {
+    const T1 d = yA[i] - yB[i];
+    e2 = e2 + d * d;
+  }
+  T1 err(sqrt(e2.v) / 15.0);
+  if (e2.v > 0.0) err = sm_sqrt(e2) / 15.0;
+  const int res = sm_update_t(err, tol, h);
+  if (res == 1) {
+    for (int i = 0; i < C::kN; ++i) yo[i] = yB[i];
+    *paso = pB;
+  }
+  return res;
+}
+
+// sm_trace on Dual<1> (no recording).  On a disk hit: returns true with the
+// hit radius and redshift carrying their tangents (*deriv = 0 where the
+// redshift is a constant or clamped).
+template <class C>
+KT_HD bool sm_trace_t(const Frame& f, const SmPrm<T1>& P, const T1* y_in, const T1* c, double pas_in,
+                      RayResult* o, T1* r_out, T1* g_out, int* deriv_out) {
+  const double M = f.g.M;
+  T1 y[C::kN], yp[C::kN], k1[C::kN], kprev[C::kN], kpT;
+  double pas = pas_in, pasp, k1p, kprevp;
+  for (int i = 0; i < C::kN; ++i) y[i] = y_in[i];
+  T1 h(f.dlam0);
+  uint32_t attempts = 0;
+  sm_rhs<C>(M, P, y, c, k1, &kpT);
+  k1p = kpT.v;
+  double prev_r = C::radius(f.g.a, y).v;
+  KT_ROLLED
+  for (int it = 0;; ++it) {
+    for (int i = 0; i < C::kN; ++i) {
+      yp[i] = y[i];
+      kprev[i] = k1[i];
+    }
+    pasp = pas;
+    kprevp = k1p;
+    T1 step_used = h;
+    int rejects = 0;
+    KT_ROLLED
+    for (;;) {
+      step_used = h;
+      ++attempts;
+      if (sm_attempt_t<C>(M, P, f.tol, c, yp, pasp, kprev, kprevp, &h, y, &pas) == 1) break;
+      int status;
+      if (reject_cap(h.v, &rejects, &status)) {
+        double yv[C::kN];
+        for (int i = 0; i < C::kN; ++i) yv[i] = yp[i].v;
+        sm_stop<C>(f, yv, pasp, status, (uint32_t)it, attempts, o);
+        return false;
+      }
+    }
+    sm_rhs<C>(M, P, y, c, k1, &kpT);
+    k1p = kpT.v;
+    double yv[C::kN], ypv[C::kN];
+    for (int i = 0; i < C::kN; ++i) {
+      yv[i] = y[i].v;
+      ypv[i] = yp[i].v;
+    }
+    const double r_now = C::radius(f.g.a, yv);
+    double best_alpha = 2.0;
+    int evt = kEvNone;
+    T1 disk_r(0.0), disk_red(1.0);
+    double disk_phi = 0.0;
+    int deriv = 0;
+    const int e = C::kEq;
+    const double q0 = ypv[e] - C::kEqTarget, q1 = yv[e] - C::kEqTarget;
+    if (sign_change(q0, q1) || dmin(fabs(q0), fabs(q1)) < 0.35) {
+      double alpha = 0.0;
+      if (sm_first_crossing(ypv[e], yv[e], kprev[e].v, k1[e].v, step_used.v, C::kEqTarget, &alpha)) {
+        // alpha* moves with the parameter: d alpha = -dq / q'(alpha)
+        const T1 q = sm_hermite_h(yp[e], y[e], kprev[e], k1[e], step_used, T1(alpha)) - C::kEqTarget;
+        const double dqda = sm_hermite_da(ypv[e], yv[e], kprev[e].v, k1[e].v, step_used.v, alpha);
+        T1 al(alpha);
+        al.d[0] = -q.d[0] / dqda;
+        T1 yh[C::kN];
+        for (int i = 0; i < C::kN; ++i) yh[i] = sm_hermite_h(yp[i], y[i], kprev[i], k1[i], step_used, al);
+        const T1 r_hit = C::radius(P.a, yh);
+        if (r_hit.v >= f.r_in && r_hit.v <= f.r_out) {
+          const T1 pph = (C::kN == 6) ? yh[0] * yh[4] - yh[1] * yh[3] : c[C::kC - 1];
+          T1 red;
+          deriv = sm_redshift<T1>(M, P, r_hit, c[0], pph, &red) ? 1 : 0;
+          if (!(red.v > 0.0 && red.v < 20.0)) deriv = 0;
+          disk_r = r_hit;
+          disk_red = red;
+          if (C::kN == 6) {
+            double rr, tt;
+            ks_to_bl(f.g, yh[0].v, yh[1].v, yh[2].v, &rr, &tt, &disk_phi);
+          } else {
+            disk_phi = pasp + alpha * (pas - pasp);
+          }
+          best_alpha = alpha;
+          evt = kEvDisk;
+        }
+      }
+    }
+    horizon_escape(prev_r, r_now, f.rh_cut, f.r_esc, &best_alpha, &evt);
+    if (evt != kEvNone) {
+      o->steps = (uint32_t)it + 1;
+      o->attempts = attempts;
+      if (evt == kEvDisk) {
+        set_result(o, kOutDisk, kStEvent, disk_r.v, dclamp(disk_red.v, 0.0, 20.0), 1.0, disk_phi, 0.0,
+                   0.0);
+        *r_out = disk_r;
+        *g_out = disk_red;
+        *deriv_out = deriv;
+        return true;
+      }
+      if (evt == kEvHorizon) {
+        set_result(o, kOutHorizon, kStEvent, prev_r + best_alpha * (r_now - prev_r), 0.0, 1.0, 0.0,
+                   0.0, 0.0);
+      } else if (C::kN == 6) {
+        double xe[3];
+        for (int i = 0; i < 3; ++i) xe[i] = ypv[i] + best_alpha * (yv[i] - ypv[i]);
+        double re, te, pe;
+        ks_to_bl(f.g, xe[0], xe[1], xe[2], &re, &te, &pe);
+        set_result(o, kOutEscaped, kStEvent, re, 1.0, 1.0, te, pe, 0.0);
+      } else {
+        const double te = ypv[1] + best_alpha * (yv[1] - ypv[1]);
+        const double pe = pasp + best_alpha * (pas - pasp);
+        set_result(o, kOutEscaped, kStEvent, f.r_esc, 1.0, 1.0, te, pe, 0.0);
+      }
+      return false;
+    }
+    prev_r = r_now;
+    if (it + 1 >= f.max_steps) {
+      sm_stop<C>(f, yv, pas, kStStepCap, (uint32_t)(it + 1), attempts, o);
+      return false;
+    }
+  }
+}
+
+// One pixel with the tangent along parameter `dir` (kGA..kGRobs): outputs
+// into *o, g[kGSlots] as sm_pixel's with only g[dir] set among the
+// derivatives.  Returns false where the KS initialisation fails (KS chart).
+template <class C>
+KT_HD bool sm_pixel_tangent(const Frame& f, uint32_t pix, int dir, const SmCot& cot, RayResult* o,
+                            double* g) {
+  constexpr bool kKS = C::kN == 6;
+  const int px = (int)(pix % (uint32_t)f.cam.W), py = (int)(pix / (uint32_t)f.cam.W);
+  double al, be;
+  pixel_angles(f.cam, px, py, &al, &be);
+  const double M = f.g.M;
+  SmPrm<T1> Pd;
+  Pd.a = T1(f.g.a);
+  Pd.Q = T1(f.g.Q);
+  Pd.L = T1(f.g.L);
+  T1 th(f.cam.theta_obs), ro(f.cam.r_obs);
+  if (dir == kGA) Pd.a.d[0] = 1.0;
+  if (dir == kGQ) Pd.Q.d[0] = 1.0;
+  if (dir == kGLambda) Pd.L.d[0] = 1.0;
+  if (dir == kGTheta) th.d[0] = 1.0;
+  if (dir == kGRobs) ro.d[0] = 1.0;
+  T1 ybl[4], cbl[2], y0[C::kN], c0[C::kC];
+  sm_camera<T1>(M, Pd, ro, th, al, be, ybl, cbl);
+  if (kKS) {
+    T1 yk[6], ck[1];
+    if (!sm_bl_to_ks<T1>(M, Pd, ybl, cbl, f.cam.phi_obs, yk, ck)) return false;
+    for (int i = 0; i < C::kN; ++i) y0[i] = yk[i];
+    c0[0] = ck[0];
+  } else {
+    for (int i = 0; i < C::kN; ++i) y0[i] = ybl[i];
+    for (int j = 0; j < C::kC; ++j) c0[j] = cbl[j];
+  }
+  T1 r_hit, g_hit;
+  int deriv = 0;
+  const bool disk = sm_trace_t<C>(f, Pd, y0, c0, kKS ? 0.0 : f.cam.phi_obs, o, &r_hit, &g_hit, &deriv);
+  for (int q = 0; q < kGSlots; ++q) g[q] = 0.0;
+  g[kGNumBL] = kKS ? 0.0 : 1.0;
+  if (!disk) return true;
+  double gbar = 0.0, rbar = 0.0;
+  if (cot.mode == 1) {
+    gbar = cot.g ? cot.g[pix] : 0.0;
+    rbar = cot.r ? cot.r[pix] : 0.0;
+  } else if (cot.mode == 2) {
+    if (cot.t_out[pix] != kOutDisk) return true;
+    const double dg = o->red - cot.t_g[pix], dr = o->r - cot.t_r[pix];
+    g[kGLoss] = cot.w_g * dg * dg + cot.w_r * dr * dr;
+    gbar = 2.0 * cot.w_g * dg;
+    rbar = 2.0 * cot.w_r * dr;
+  }
+  if (gbar == 0.0 && rbar == 0.0) return true;
+  g[kGNumGrad] = 1.0;
+  g[dir] = rbar * r_hit.d[0] + (deriv ? gbar * g_hit.d[0] : 0.0);
   return true;
 }
 

@@ -134,7 +134,7 @@ extern "C" int hc_trace_pixels(const kt_frame_desc* d, int64_t n, const uint32_t
 #include "../kerrtracecpp2_b200/csrc/kt_smray.cuh"
 
 extern "C" int hc_smooth_pixels(const kt_frame_desc* d, int64_t n, const uint32_t* pix, int mode,
-                                int force_bl, const double* cot_g, const double* cot_r,
+                                int force_bl, int tangent_dir, const double* cot_g, const double* cot_r,
                                 const uint8_t* t_out, const double* t_g, const double* t_r,
                                 double w_g, double w_r, uint8_t* outcome, double* r, double* red,
                                 double* phi_disk, double* th_esc, double* ph_esc, uint32_t* steps,
@@ -163,7 +163,11 @@ extern "C" int hc_smooth_pixels(const kt_frame_desc* d, int64_t n, const uint32_
       double g[kGSlots];
       const bool ks = f.chart == KT_CHART_KS && !force_bl;
       bool done = false;
-      if (ks)
+      if (mode != 0 && tangent_dir >= 0) {
+        if (ks) done = sm_pixel_tangent<ChartKS>(f, pix[i], tangent_dir, cot, &o, g);
+        if (!done) sm_pixel_tangent<ChartBL>(f, pix[i], tangent_dir, cot, &o, g);
+        done = true;
+      } else if (ks)
         done = mode == 0 ? sm_pixel<ChartKS, false>(f, pix[i], cot, &o, g, nullptr)
                          : sm_pixel<ChartKS, true>(f, pix[i], cot, &o, g, sc);
       if (!done) {

@@ -20,7 +20,7 @@ def lib():
         L = ctypes.CDLL(testlibs.HOSTCHECK)
         P = ctypes.c_void_p
         L.hc_smooth_pixels.argtypes = ([ctypes.POINTER(FrameDesc), ctypes.c_int64, P, ctypes.c_int,
-                                        ctypes.c_int] + [P] * 5 + [ctypes.c_double] * 2 + [P] * 9)
+                                        ctypes.c_int, ctypes.c_int] + [P] * 5 + [ctypes.c_double] * 2 + [P] * 9)
         L.hc_smooth_pixels.restype = ctypes.c_int
         _lib = L
     return _lib
@@ -31,10 +31,12 @@ def _p(a):
 
 
 def smooth(desc, pix=None, mode=0, cot_g=None, cot_r=None, target=None, w_g=1.0, w_r=0.0,
-           force_bl=False):
+           force_bl=False, tangent=-1):
     """Trace pixels `pix` (default: all) with the smooth tracer; mode 1/2
     also runs the adjoint (cotangent arrays over the whole frame, or the L2
-    loss against `target`, a dict with outcome/redshift/r over the frame).
+    loss against `target`, a dict with outcome/redshift/r over the frame);
+    with tangent = k (0 a, 1 Q, 2 Lambda, 3 theta, 4 r_obs) the derivative
+    along that parameter comes from the forward-mode tangent instead.
     Returns (outputs dict, contrib[N_SLOTS][len(pix)] or None)."""
     n_frame = desc.width * desc.height
     pix = np.arange(n_frame, dtype=np.uint32) if pix is None else np.ascontiguousarray(pix, np.uint32)
@@ -47,7 +49,7 @@ def smooth(desc, pix=None, mode=0, cot_g=None, cot_r=None, target=None, w_g=1.0,
     arr = lambda a, dt: None if a is None else np.ascontiguousarray(a, dt)  # noqa: E731
     keep = [arr(cot_g, np.float64), arr(cot_r, np.float64), arr(t.get("outcome"), np.uint8),
             arr(t.get("redshift"), np.float64), arr(t.get("r"), np.float64)]
-    rc = lib().hc_smooth_pixels(ctypes.byref(desc), n, _p(pix), mode, int(force_bl),
+    rc = lib().hc_smooth_pixels(ctypes.byref(desc), n, _p(pix), mode, int(force_bl), int(tangent),
                                 *[_p(k) for k in keep], w_g, w_r,
                                 *[_p(out[k]) for k in ("outcome", "r", "redshift", "phi_disk",
                                                        "theta_esc", "phi_esc", "steps",

@@ -60,7 +60,7 @@ def test_vjp_gpu_equals_host(renderer, kw):
     h = c.sum(axis=1)
     want = [h[0], h[1], h[2], h[3] * np.pi / 180, h[4], 0.0]
     if kw["chart"] == 0:
-        _, cl = S.smooth(d, mode=1, cot_g=cg, cot_r=cr, force_bl=True)
+        _, cl = S.smooth(d, mode=1, cot_g=cg, cot_r=cr, force_bl=True, tangent=2)
         want[2] = cl.sum(axis=1)[2]
     np.testing.assert_allclose(grad, want, rtol=1e-11, atol=1e-12 * np.abs(want).max())
     assert st["grad_pixels"] == int(h[6]) and st["unrecorded"] == 0

@@ -113,7 +113,8 @@ def test_l2_loss_gradient_matches_central_differences(h):
     """Config-5 geometry at 128x128, tol 1e-7: the gradient of the L2 loss
     of (g, r_hit) against a target frame, restricted to the pixels on which
     every stencil is smooth, against central differences of that loss.
-    Lambda's entry is the BL chart's (cotangents from the BL trace)."""
+    Lambda's entry is the BL chart's (cotangents from the BL trace), by the
+    forward-mode tangent as kt_l2_grad computes it."""
     base, tgt = l2_setup(128, 1e-7)
     wg, wr = 1.0, 0.01
     names = PARAMS if h == 1e-6 else ["a", "Q", "theta_deg", "r_obs"]
@@ -135,7 +136,7 @@ def test_l2_loss_gradient_matches_central_differences(h):
     adj = {"a": grad[0], "Q": grad[1], "theta_deg": grad[3] * np.pi / 180, "r_obs": grad[4]}
     if "Lambda" in names:
         cgl, crl = cot(bl0)
-        _, cl = S.smooth(d, mode=1, cot_g=cgl, cot_r=crl, force_bl=True)
+        _, cl = S.smooth(d, mode=1, cot_g=cgl, cot_r=crl, force_bl=True, tangent=2)
         adj["Lambda"] = cl.sum(axis=1)[2]
     for k in names:
         op, om, _, hk = renders[k]
@@ -188,3 +189,26 @@ def test_smooth_frames_rejected_where_unsupported(L=None):
     # the KS chart ignores --dopri5, as the reference does
     d = abi.frame_desc(width=4, height=4, chart=0, integrator=1, precision=abi.KT_PREC_SMOOTH)
     assert lib.kt_frame_derive(ctypes.byref(d), ctypes.byref(out)) == abi.KT_OK
+
+
+@pytest.mark.parametrize("frame,dirs", [(dict(KNDS, width=48, height=27), [0, 1, 2, 3, 4]),
+                                        (dict(CFG5, width=48, height=48), [0, 1, 3, 4])],
+                         ids=["bl", "ks"])
+def test_tangent_equals_adjoint(frame, dirs):
+    """The forward-mode tangent (used for a KS frame's Lambda entry) traces
+    the same rays as the smooth forward, bit for bit, and gives each pixel's
+    derivative along one parameter equal to the reverse sweep's."""
+    d = abi.frame_desc(**frame)
+    n = d.width * d.height
+    rng = np.random.default_rng(11)
+    cg, cr = rng.normal(size=n), rng.normal(size=n)
+    fwd, ca = S.smooth(d, mode=1, cot_g=cg, cot_r=cr)
+    for k in dirs:
+        ft, ct = S.smooth(d, mode=1, cot_g=cg, cot_r=cr, tangent=k)
+        for f in ("outcome", "r", "redshift", "steps", "attempts"):
+            assert np.array_equal(ft[f], fwd[f]), f
+        scale = np.abs(ca[k]).max()
+        np.testing.assert_allclose(ct[k], ca[k], rtol=1e-7, atol=1e-11 * scale)
+        others = [q for q in range(5) if q != k]
+        assert not ct[others].any()
+        assert np.array_equal(ct[6], ca[6])  # the same pixels get a derivative
