@@ -316,6 +316,20 @@ kt_status kt_l2_grad(kt_context* ctx, const kt_frame_desc* desc, const kt_geo_so
                      double* loss, double grad[KT_GRAD_COUNT], kt_grad_stats* stats,
                      void* stream);
 
+/* The same over the pixels pix_dev[0..n_pix) only (device indices
+ * py*width+px; outputs and cotangents still indexed over the whole frame):
+ * the per-GPU share of a frame split across GPUs, whose partial gradients
+ * add up (one all-reduce of KT_GRAD_COUNT doubles).  Indices outside the
+ * frame are skipped. */
+kt_status kt_vjp_pixels(kt_context* ctx, const kt_frame_desc* desc, const uint32_t* pix_dev,
+                        int64_t n_pix, const double* cot_redshift, const double* cot_r,
+                        const kt_geo_soa* out, uint32_t flags, double grad[KT_GRAD_COUNT],
+                        kt_grad_stats* stats, void* stream);
+kt_status kt_l2_grad_pixels(kt_context* ctx, const kt_frame_desc* desc, const uint32_t* pix_dev,
+                            int64_t n_pix, const kt_geo_soa* target, double w_g, double w_r,
+                            const kt_geo_soa* out, uint32_t flags, double* loss,
+                            double grad[KT_GRAD_COUNT], kt_grad_stats* stats, void* stream);
+
 /* Measured FP64 FMA throughput of the context's device (GFLOP/s, 2 flops
  * per FMA): the non-tensor FP64 peak the trace kernels are bounded by. */
 kt_status kt_measure_fp64_peak(kt_context* ctx, double* gflops);

@@ -23,22 +23,25 @@ constexpr int kSmBlock = 64;
 constexpr int kSumBlocks = 296;
 constexpr int kSumThreads = 256;
 
-// Rays: pixels 0..n-1 or list[0..*n_dev).  The KS kernel appends the rays
+// Rays: pixels 0..n-1, or list[0..*n_dev) (a count on the device) or
+// list[0..n_list) (on the host).  The KS kernel appends the rays
 // whose KS initialisation fails to fb_pix (count *fb_n) for the BL kernel.
 template <class C, bool kGrad>
 __global__ void __launch_bounds__(kSmBlock) k_smooth(const Frame f, const OutSoA out, const SmJob job,
                                                      uint32_t n, const uint32_t* __restrict__ list,
+                                                     uint32_t n_list,
                                                      const uint32_t* __restrict__ n_dev,
                                                      uint32_t* __restrict__ queue,
                                                      uint32_t* __restrict__ fb_pix,
                                                      uint32_t* __restrict__ fb_n) {
   SmScratch sc;
-  const uint32_t count = n_dev ? *n_dev : n;
+  const uint32_t count = n_dev ? *n_dev : (list ? n_list : n);
   KT_ROLLED
   for (;;) {
     const uint32_t i = atomicAdd(queue, 1u);
     if (i >= count) break;
     const uint32_t pix = list ? list[i] : i;
+    if (pix >= n) continue;  // a caller's list with an index outside the frame
     RayResult o;
     double g[kGSlots];
     if (!sm_pixel<C, kGrad>(f, pix, job.cot, &o, g, kGrad ? &sc : nullptr)) {
@@ -56,16 +59,18 @@ template <class C>
 __global__ void __launch_bounds__(kSmBlock) k_smooth_tangent(const Frame f, const OutSoA out,
                                                              const SmJob job, uint32_t n,
                                                              const uint32_t* __restrict__ list,
+                                                             uint32_t n_list,
                                                              const uint32_t* __restrict__ n_dev,
                                                              uint32_t* __restrict__ queue,
                                                              uint32_t* __restrict__ fb_pix,
                                                              uint32_t* __restrict__ fb_n) {
-  const uint32_t count = n_dev ? *n_dev : n;
+  const uint32_t count = n_dev ? *n_dev : (list ? n_list : n);
   KT_ROLLED
   for (;;) {
     const uint32_t i = atomicAdd(queue, 1u);
     if (i >= count) break;
     const uint32_t pix = list ? list[i] : i;
+    if (pix >= n) continue;  // a caller's list with an index outside the frame
     RayResult o;
     double g[kGSlots];
     if (!sm_pixel_tangent<C>(f, pix, job.tangent_dir, job.cot, &o, g)) {
@@ -118,7 +123,8 @@ __global__ void __launch_bounds__(kSumThreads) k_sum_final(const double* __restr
 
 template <class C>
 static cudaError_t tangent_launch(const Frame& f, const OutSoA& out, uint32_t n, const SmJob& job,
-                                  const uint32_t* list, const uint32_t* n_dev, uint32_t* queue,
+                                  const uint32_t* list, uint32_t n_list, const uint32_t* n_dev,
+                                  uint32_t* queue,
                                   uint32_t* fb_pix, uint32_t* fb_n, int device, cudaStream_t st) {
   int sms = 0, per_sm = 0;
   cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -126,13 +132,15 @@ static cudaError_t tangent_launch(const Frame& f, const OutSoA& out, uint32_t n,
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_smooth_tangent<C>, kSmBlock, 0);
   if (e != cudaSuccess) return e;
   const int grid = sms * (per_sm < 1 ? 1 : per_sm);
-  k_smooth_tangent<C><<<grid, kSmBlock, 0, st>>>(f, out, job, n, list, n_dev, queue, fb_pix, fb_n);
+  k_smooth_tangent<C><<<grid, kSmBlock, 0, st>>>(f, out, job, n, list, n_list, n_dev, queue, fb_pix,
+                                                  fb_n);
   return cudaGetLastError();
 }
 
 template <class C, bool kGrad>
 static cudaError_t smooth_launch(const Frame& f, const OutSoA& out, uint32_t n, const SmJob& job,
-                                 const uint32_t* list, const uint32_t* n_dev, uint32_t* queue,
+                                 const uint32_t* list, uint32_t n_list, const uint32_t* n_dev,
+                                 uint32_t* queue,
                                  uint32_t* fb_pix, uint32_t* fb_n, int device, cudaStream_t st) {
   int sms = 0, per_sm = 0;
   cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -140,7 +148,8 @@ static cudaError_t smooth_launch(const Frame& f, const OutSoA& out, uint32_t n, 
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_smooth<C, kGrad>, kSmBlock, 0);
   if (e != cudaSuccess) return e;
   const int grid = sms * (per_sm < 1 ? 1 : per_sm);
-  k_smooth<C, kGrad><<<grid, kSmBlock, 0, st>>>(f, out, job, n, list, n_dev, queue, fb_pix, fb_n);
+  k_smooth<C, kGrad><<<grid, kSmBlock, 0, st>>>(f, out, job, n, list, n_list, n_dev, queue, fb_pix,
+                                                 fb_n);
   return cudaGetLastError();
 }
 
@@ -152,30 +161,30 @@ cudaError_t launch_smooth(const Frame& f, const OutSoA& out, uint32_t n, const S
   const bool grad = job != nullptr;
   if (grad && job->tangent_dir >= 0) {
     if (f.chart == 0 && !job->force_bl) {
-      cudaError_t e = tangent_launch<ChartKS>(f, out, n, jb, nullptr, nullptr, counters, fb_pix,
+      cudaError_t e = tangent_launch<ChartKS>(f, out, n, jb, jb.pix, jb.n_pix, nullptr, counters, fb_pix,
                                               counters + 2, device, st);
       if (e != cudaSuccess) return e;
-      return tangent_launch<ChartBL>(f, out, n, jb, fb_pix, counters + 2, counters + 1, nullptr,
+      return tangent_launch<ChartBL>(f, out, n, jb, fb_pix, 0, counters + 2, counters + 1, nullptr,
                                      nullptr, device, st);
     }
-    return tangent_launch<ChartBL>(f, out, n, jb, nullptr, nullptr, counters, nullptr, nullptr,
+    return tangent_launch<ChartBL>(f, out, n, jb, jb.pix, jb.n_pix, nullptr, counters, nullptr, nullptr,
                                    device, st);
   }
   if (f.chart == 0 && !(job && job->force_bl)) {
     // KS pass over all pixels, then BL over the rays whose KS init failed
-    cudaError_t e = grad ? smooth_launch<ChartKS, true>(f, out, n, jb, nullptr, nullptr, counters,
+    cudaError_t e = grad ? smooth_launch<ChartKS, true>(f, out, n, jb, jb.pix, jb.n_pix, nullptr, counters,
                                                         fb_pix, counters + 2, device, st)
-                         : smooth_launch<ChartKS, false>(f, out, n, jb, nullptr, nullptr, counters,
+                         : smooth_launch<ChartKS, false>(f, out, n, jb, jb.pix, jb.n_pix, nullptr, counters,
                                                          fb_pix, counters + 2, device, st);
     if (e != cudaSuccess) return e;
-    return grad ? smooth_launch<ChartBL, true>(f, out, n, jb, fb_pix, counters + 2, counters + 1,
+    return grad ? smooth_launch<ChartBL, true>(f, out, n, jb, fb_pix, 0, counters + 2, counters + 1,
                                                nullptr, nullptr, device, st)
-                : smooth_launch<ChartBL, false>(f, out, n, jb, fb_pix, counters + 2, counters + 1,
+                : smooth_launch<ChartBL, false>(f, out, n, jb, fb_pix, 0, counters + 2, counters + 1,
                                                 nullptr, nullptr, device, st);
   }
-  return grad ? smooth_launch<ChartBL, true>(f, out, n, jb, nullptr, nullptr, counters, nullptr,
+  return grad ? smooth_launch<ChartBL, true>(f, out, n, jb, jb.pix, jb.n_pix, nullptr, counters, nullptr,
                                              nullptr, device, st)
-              : smooth_launch<ChartBL, false>(f, out, n, jb, nullptr, nullptr, counters, nullptr,
+              : smooth_launch<ChartBL, false>(f, out, n, jb, jb.pix, jb.n_pix, nullptr, counters, nullptr,
                                               nullptr, device, st);
 }
 

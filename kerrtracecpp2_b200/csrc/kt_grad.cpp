@@ -28,18 +28,24 @@ struct EventPair {
 // force_bl: trace every ray in the BL chart; tangent_dir >= 0: forward-mode
 // tangent along that parameter instead of the reverse sweep.
 kt_status grad_pass(kt_context* ctx, const kt::Frame& f, const kt::OutSoA& out, uint32_t n,
-                    const kt::SmCot& cot, bool force_bl, int tangent_dir, cudaStream_t st,
-                    double* sums, float* ms) {
+                    const uint32_t* pix, uint32_t n_pix, const kt::SmCot& cot, bool force_bl,
+                    int tangent_dir, cudaStream_t st, double* sums, float* ms) {
   kt::SmJob job;
   job.cot = cot;
   job.force_bl = force_bl ? 1 : 0;
   job.tangent_dir = tangent_dir;
   job.contrib = ctx->d_grad;
+  job.pix = pix;
+  job.n_pix = n_pix;
   EventPair ev;
   KT_CUDA(ctx, cudaEventCreate(&ev.a), "event");
   KT_CUDA(ctx, cudaEventCreate(&ev.b), "event");
   KT_CUDA(ctx, cudaMemsetAsync(ctx->d_counters, 0, 4 * sizeof(uint32_t), st), "reset queue");
   KT_CUDA(ctx, cudaEventRecord(ev.a, st), "event");
+  // with a pixel list only the listed pixels' contributions are written
+  if (pix)
+    KT_CUDA(ctx, cudaMemsetAsync(ctx->d_grad, 0, (size_t)n * kt::kGSlots * sizeof(double), st),
+            "clear contributions");
   KT_CUDA(ctx, kt::launch_smooth(f, out, n, &job, ctx->d_counters, ctx->d_fb, ctx->device, st),
           "adjoint kernel launch");
   KT_CUDA(ctx, kt::launch_grad_sum(ctx->d_grad, n, ctx->d_gsum + kt::kGSlots, ctx->d_gsum, st),
@@ -52,11 +58,14 @@ kt_status grad_pass(kt_context* ctx, const kt::Frame& f, const kt::OutSoA& out, 
   return KT_OK;
 }
 
-kt_status grad_run(kt_context* ctx, const kt_frame_desc* desc_in, const kt::SmCot& cot,
-                   const kt_geo_soa* out_soa, uint32_t flags, double* grad, kt_grad_stats* stats,
-                   cudaStream_t st, const char* who) {
+kt_status grad_run(kt_context* ctx, const kt_frame_desc* desc_in, const uint32_t* pix, int64_t n_pix,
+                   const kt::SmCot& cot, const kt_geo_soa* out_soa, uint32_t flags, double* grad,
+                   kt_grad_stats* stats, cudaStream_t st, const char* who) {
   if (!ctx) return KT_ERR_INVALID_ARGUMENT;
   if (!desc_in || !grad) return fail(ctx, KT_ERR_INVALID_ARGUMENT, std::string(who) + ": NULL pointer");
+  if (n_pix < 0 || (n_pix > 0 && !pix) ||
+      n_pix > (int64_t)desc_in->width * (int64_t)desc_in->height)
+    return fail(ctx, KT_ERR_INVALID_ARGUMENT, std::string(who) + ": bad pixel list");
   if (flags & ~KT_GRAD_SKIP_LAMBDA) return fail(ctx, KT_ERR_INVALID_ARGUMENT, std::string(who) + ": unknown flags");
   if (out_soa && !out_complete(out_soa))
     return fail(ctx, KT_ERR_INVALID_ARGUMENT, std::string(who) + ": incomplete output SoA");
@@ -79,7 +88,7 @@ kt_status grad_run(kt_context* ctx, const kt_frame_desc* desc_in, const kt::SmCo
   if (out_soa) out = to_out(out_soa);
   double s[kt::kGSlots], sl[kt::kGSlots];
   float ms = 0.f, ms_l = 0.f;
-  r = grad_pass(ctx, f, out, (uint32_t)n, cot, false, -1, st, s, &ms);
+  r = grad_pass(ctx, f, out, (uint32_t)n, pix, (uint32_t)n_pix, cot, false, -1, st, s, &ms);
   if (r != KT_OK) return r;
   double lambda = s[kt::kGLambda];
   if (f.chart == KT_CHART_KS) {
@@ -88,7 +97,8 @@ kt_status grad_run(kt_context* ctx, const kt_frame_desc* desc_in, const kt::SmCo
       kt::OutSoA none;
       memset(&none, 0, sizeof none);
       // one derivative in the BL chart: forward-mode tangent along Lambda
-      r = grad_pass(ctx, f, none, (uint32_t)n, cot, true, kt::kGLambda, st, sl, &ms_l);
+      r = grad_pass(ctx, f, none, (uint32_t)n, pix, (uint32_t)n_pix, cot, true, kt::kGLambda, st,
+                    sl, &ms_l);
       if (r != KT_OK) return r;
       lambda = sl[kt::kGLambda];
     }
@@ -116,20 +126,36 @@ kt_status grad_run(kt_context* ctx, const kt_frame_desc* desc_in, const kt::SmCo
 
 extern "C" {
 
-kt_status kt_vjp(kt_context* ctx, const kt_frame_desc* desc, const double* cot_redshift,
-                 const double* cot_r, const kt_geo_soa* out, uint32_t flags, double* grad,
-                 kt_grad_stats* stats, void* stream) {
+kt_status kt_vjp_pixels(kt_context* ctx, const kt_frame_desc* desc, const uint32_t* pix_dev,
+                        int64_t n_pix, const double* cot_redshift, const double* cot_r,
+                        const kt_geo_soa* out, uint32_t flags, double* grad, kt_grad_stats* stats,
+                        void* stream) {
   kt::SmCot cot;
   memset(&cot, 0, sizeof cot);
   cot.mode = 1;
   cot.g = cot_redshift;
   cot.r = cot_r;
-  return grad_run(ctx, desc, cot, out, flags, grad, stats, (cudaStream_t)stream, "kt_vjp");
+  return grad_run(ctx, desc, pix_dev, n_pix, cot, out, flags, grad, stats, (cudaStream_t)stream,
+                  "kt_vjp");
+}
+
+kt_status kt_vjp(kt_context* ctx, const kt_frame_desc* desc, const double* cot_redshift,
+                 const double* cot_r, const kt_geo_soa* out, uint32_t flags, double* grad,
+                 kt_grad_stats* stats, void* stream) {
+  return kt_vjp_pixels(ctx, desc, nullptr, 0, cot_redshift, cot_r, out, flags, grad, stats, stream);
 }
 
 kt_status kt_l2_grad(kt_context* ctx, const kt_frame_desc* desc, const kt_geo_soa* target, double w_g,
                      double w_r, const kt_geo_soa* out, uint32_t flags, double* loss, double* grad,
                      kt_grad_stats* stats, void* stream) {
+  return kt_l2_grad_pixels(ctx, desc, nullptr, 0, target, w_g, w_r, out, flags, loss, grad, stats,
+                           stream);
+}
+
+kt_status kt_l2_grad_pixels(kt_context* ctx, const kt_frame_desc* desc, const uint32_t* pix_dev,
+                            int64_t n_pix, const kt_geo_soa* target, double w_g, double w_r,
+                            const kt_geo_soa* out, uint32_t flags, double* loss, double* grad,
+                            kt_grad_stats* stats, void* stream) {
   if (!ctx) return KT_ERR_INVALID_ARGUMENT;
   if (!target || !target->outcome || !target->redshift || !target->r || !loss)
     return fail(ctx, KT_ERR_INVALID_ARGUMENT, "kt_l2_grad: NULL pointer");
@@ -145,7 +171,8 @@ kt_status kt_l2_grad(kt_context* ctx, const kt_frame_desc* desc, const kt_geo_so
   cot.w_r = w_r;
   kt_grad_stats st_local;
   kt_grad_stats* sp = stats ? stats : &st_local;
-  const kt_status r = grad_run(ctx, desc, cot, out, flags, grad, sp, (cudaStream_t)stream, "kt_l2_grad");
+  const kt_status r = grad_run(ctx, desc, pix_dev, n_pix, cot, out, flags, grad, sp, (cudaStream_t)stream,
+                               "kt_l2_grad");
   if (r == KT_OK) *loss = sp->loss;
   return r;
 }

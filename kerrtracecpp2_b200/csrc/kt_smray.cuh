@@ -714,12 +714,14 @@ struct SmCot {
 // A launch of the smooth kernel with gradients: cotangent source, chart
 // override (trace every ray in the BL chart), reverse sweep (tangent_dir < 0)
 // or forward-mode tangent along one parameter (tangent_dir = kGA..kGRobs),
-// and the [kGSlots][n] output.
+// the [kGSlots][n] output (indexed by pixel) and an optional pixel list.
 struct SmJob {
   SmCot cot;
   int force_bl;
   int tangent_dir;
   double* contrib;
+  const uint32_t* pix;  // trace only these pixels (n_pix of them), or all when NULL
+  uint32_t n_pix;
 };
 
 // Gradient slots of one pixel (and of the frame after the sum): dL/d(a, Q,

@@ -125,3 +125,29 @@ def test_config5_l2_gradient_against_central_differences(renderer):
     print(f"smooth pixels {ok.sum()} of {m_all.sum()} disk pixels; worst rel {worst:.2e}")
     assert worst <= 1e-4
     assert grad_l2[abi.GRAD_NAMES.index("disk_out")] == 0.0
+
+
+def test_pixel_list_gradients_add_up(renderer):
+    """A frame's gradient split into the tiles of three ranks
+    (kerrtracecpp2_b200.shard.frame_tiles, kt_l2_grad_pixels on each share)
+    sums to the whole frame's: the per-pixel work is the same, only the
+    summation order differs.  KS frame, so the Lambda tangent pass is split
+    too."""
+    import torch
+
+    from kerrtracecpp2_b200 import shard
+
+    base = dict(CFG5, width=128, height=96)
+    tgt = renderer.trace(abi.frame_desc(precision=abi.KT_PREC_SMOOTH, **dict(base, a=0.72, theta_deg=71.0)))
+    d = abi.frame_desc(**base)
+    loss, grad, st = renderer.l2_grad(d, tgt, 1.0, 0.01)
+    tot_loss, tot_grad, tot_pix = 0.0, np.zeros(abi.KT_GRAD_COUNT), 0
+    for rank in range(3):
+        pix = torch.from_numpy(shard.frame_tiles(d.width, d.height, 3, rank, 16).astype(np.int32)).cuda()
+        l_r, g_r, s_r = renderer.l2_grad(d, tgt, 1.0, 0.01, pix=pix)
+        tot_loss += l_r
+        tot_grad += g_r
+        tot_pix += s_r["grad_pixels"]
+    assert tot_pix == st["grad_pixels"]
+    assert tot_loss == pytest.approx(loss, rel=1e-12)
+    np.testing.assert_allclose(tot_grad, grad, rtol=1e-10, atol=1e-12 * np.abs(grad).max())
