@@ -39,6 +39,8 @@ WORKLOADS = {
     "kerr_ks_rk4_320x180": dict(chart=0, a=0.5, r_obs=40.0, theta_deg=80.0, phi_deg=0.0,
                                 fov_deg=45.0, disk_out=12.0, width=320, height=180),
     "bundles_bl_1080p": dict(chart=1, bundles=1, a=0.998, theta_deg=60.0, width=1920, height=1080),
+    # config 3's geometry at a quarter of the resolution (profiling size)
+    "bundles_bl_480x270": dict(chart=1, bundles=1, a=0.998, theta_deg=60.0, width=480, height=270),
     "kn_ks_rk4_512": dict(chart=0, a=0.7, Q=0.1, theta_deg=70.0, r_obs=50.0, disk_out=15.0,
                           width=512, height=512),
     # 64 seeded parameter sets (kerrtracecpp2_b200.random_parameter_sets, seed
@@ -557,7 +559,7 @@ def main():
     # Mixed precision (KT_PREC_MIXED), timed the same way; its error is taken
     # against this run's FP64 frame, which is bit-identical to the reference.
     mixed = None
-    if not args.no_mixed and not desc.bundles:
+    if not args.no_mixed:
         mdesc = abi.frame_desc(**dict(wl, precision=abi.KT_PREC_MIXED))
         mout = R.alloc(n, counters=True)
         for _ in range(max(args.warmup, 1)):
@@ -598,7 +600,7 @@ def main():
     # camera at azimuths 360*k/F deg) as one autotuned kt_batch, one graph
     # launch per step.
     mixed_batched = None
-    if mixed is not None and not args.no_batch:
+    if mixed is not None and not args.no_batch and args.workload == "knds_bl_dopri5_720p":
         descs = [abi.frame_desc(**dict(wl, precision=abi.KT_PREC_MIXED,
                                        phi_deg=wl.get("phi_deg", 0.0) + 360.0 * k / BATCH_720P_FRAMES))
                  for k in range(BATCH_720P_FRAMES)]

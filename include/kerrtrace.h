@@ -62,7 +62,9 @@ enum { KT_SOLVER_STANDARD = 0, KT_SOLVER_SEMI_ANALYTIC = 1, KT_SOLVER_ELLIPTIC_C
 /* Arithmetic of the trace.  FP64: the reference's arithmetic bit for bit.
  * MIXED: analytic Hamiltonian gradient, FP32 right-hand side in the far
  * field when tol >= 1e-8, FP64 state, error control and events; agrees with
- * FP64 to about the reference's own finite-difference noise.
+ * FP64 to about the reference's own finite-difference noise.  With
+ * bundles: Hess(H) W by one dual-number evaluation of the analytic gradient
+ * (FP64; the Jacobi map and its determinant FP64).
  * SMOOTH: the differentiable tracer (kt_vjp, kt_l2_grad): FP64, analytic
  * Hamiltonian gradient, analytic BL->KS Jacobian, disk crossing solved to
  * convergence, RK4 step doubling only; its outputs are smooth functions of
@@ -241,7 +243,7 @@ typedef struct kt_batch_options {
 } kt_batch_options;
 
 typedef struct kt_batch_group_info {
-  int32_t kernel;          /* 0 BL RK4, 1 BL DOPRI5, 2 KS RK4, 3 bundles, 4-6 mixed BL RK4 / BL DOPRI5 / KS RK4 */
+  int32_t kernel;          /* 0 BL RK4, 1 BL DOPRI5, 2 KS RK4, 3 bundles, 4-7 mixed BL RK4 / BL DOPRI5 / KS RK4 / bundles */
   int32_t n_frames;
   uint64_t n_rays;
   int32_t variant;

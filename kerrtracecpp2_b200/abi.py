@@ -112,7 +112,7 @@ class BatchGroupInfo(ctypes.Structure):
 
 # Kernel of a batch group (kt_batch_group_info.kernel).
 BATCH_KERNELS = ["bl_rk4", "bl_dopri5", "ks_rk4", "bundles", "bl_rk4_mixed", "bl_dopri5_mixed",
-                 "ks_rk4_mixed"]
+                 "ks_rk4_mixed", "bundles_mixed"]
 
 
 def batch_options(autotune=False, **kw):

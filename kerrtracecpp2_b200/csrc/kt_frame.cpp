@@ -171,8 +171,8 @@ kt_status prepare_frame(const kt_frame_desc* d, Frame* f, kt_frame_derived* dv, 
     *err = "precision must be KT_PREC_FP64, KT_PREC_MIXED or KT_PREC_SMOOTH";
     return KT_ERR_INVALID_ARGUMENT;
   }
-  if (d->precision != KT_PREC_FP64 && d->bundles) {
-    *err = "the mixed-precision and smooth tracers have no ray-bundle mode";
+  if (d->precision == KT_PREC_SMOOTH && d->bundles) {
+    *err = "the smooth tracer has no ray-bundle mode";
     return KT_ERR_UNSUPPORTED;
   }
   if (d->precision == KT_PREC_SMOOTH && d->integrator == KT_DOPRI5 &&

@@ -47,14 +47,15 @@ enum Mode : int {
   kModeBLRk4Mixed = 4,
   kModeBLDopri5Mixed = 5,
   kModeKSRk4Mixed = 6,
-  kNumModes = 7
+  kModeBundleMixed = 7,
+  kNumModes = 8
 };
 
 // Kernel mode of a prepared frame (and, for the KS chart, of its BL
 // fallback pass).
 inline Mode frame_mode(const Frame& f) {
-  if (f.bundles) return kModeBundle;
   const bool mixed = f.precision == 1;
+  if (f.bundles) return mixed ? kModeBundleMixed : kModeBundle;
   if (f.chart == 0) return mixed ? kModeKSRk4Mixed : kModeKSRk4;
   if (f.intg == 1) return mixed ? kModeBLDopri5Mixed : kModeBLDopri5;
   return mixed ? kModeBLRk4Mixed : kModeBLRk4;

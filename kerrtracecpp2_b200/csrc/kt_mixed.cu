@@ -2,8 +2,9 @@
 //
 // Same persistent loop and the same FP64 integrators as the exact kernels
 // (state, stage sums, embedded error estimate, step-size controller, event
-// location and the disk-crossing root all stay FP64), with a different
-// right-hand side: the Hamiltonian gradient is evaluated analytically
+// location and the disk-crossing root all stay FP64; in bundle mode the
+// Jacobi map W and its determinant too), with a different right-hand side:
+// the Hamiltonian gradient is evaluated analytically
 // (bl_rhs_analytic / ks_rhs_analytic: one inverse metric with four
 // reciprocals instead of five metrics with 26 correctly rounded divisions),
 // in FP32 where the tolerance and the geometry allow it, else in FP64.
@@ -12,6 +13,7 @@
 // diverge between the two paths.  This file is compiled with FMA
 // contraction on; its results are not bit-identical to the reference and
 // are compared with the FP64 oracle statistically.
+#include "kt_smooth.cuh"
 #include "kt_trace_kernel.cuh"
 
 namespace kt {
@@ -91,6 +93,23 @@ struct ModeKSRk4Mixed {
   }
 };
 
+struct ModeBundleMixed {
+  using Machine = Bundle;
+  static constexpr int kSlots = Bundle::kSlots;
+  Bundle* m;
+  __device__ __forceinline__ bool needs_k1() const { return m->needs_k1(); }
+  __device__ __forceinline__ bool start(const Frame& f, uint32_t pix, uint32_t, uint32_t, const Fallback&) {
+    m->init(f, (int)(pix % (uint32_t)f.cam.W), (int)(pix / (uint32_t)f.cam.W));
+    return true;
+  }
+  __device__ __forceinline__ bool slot(const Frame& f, int s, RayResult* res) {
+    double y[4], yW[8], k[5], kW[8];
+    m->input(s, y, yW);
+    bundle_rhs_analytic(f.g, y, m->pt, m->pphi, yW, k, kW);
+    return m->consume(f, s, k, kW, res);
+  }
+};
+
 template <class ModeT>
 static cudaError_t launch_one(const Frame& f, const OutSoA& out, const RayList& rl,
                               uint32_t* queue, const Fallback& fb, const LaunchShape& s,
@@ -104,6 +123,7 @@ cudaError_t launch_shape_mixed(Mode mode, int device, LaunchShape* shape) {
     case kModeBLRk4Mixed: return shape_for<ModeBLRk4Mixed>(device, shape);
     case kModeBLDopri5Mixed: return shape_for<ModeBLDopri5Mixed>(device, shape);
     case kModeKSRk4Mixed: return shape_for<ModeKSRk4Mixed>(device, shape);
+    case kModeBundleMixed: return shape_for<ModeBundleMixed>(device, shape);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -115,6 +135,7 @@ cudaError_t launch_trace_mixed(Mode mode, const Frame& f, const OutSoA& out, con
     case kModeBLRk4Mixed: return launch_one<ModeBLRk4Mixed>(f, out, rl, queue, fb, s, stream);
     case kModeBLDopri5Mixed: return launch_one<ModeBLDopri5Mixed>(f, out, rl, queue, fb, s, stream);
     case kModeKSRk4Mixed: return launch_one<ModeKSRk4Mixed>(f, out, rl, queue, fb, s, stream);
+    case kModeBundleMixed: return launch_one<ModeBundleMixed>(f, out, rl, queue, fb, s, stream);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -124,6 +145,7 @@ cudaError_t batch_shape_mixed(Mode mode, int variant, int device, LaunchShape* s
     case kModeBLRk4Mixed: return batch_shape<ModeBLRk4Mixed>(variant, device, shape);
     case kModeBLDopri5Mixed: return batch_shape<ModeBLDopri5Mixed>(variant, device, shape);
     case kModeKSRk4Mixed: return batch_shape<ModeKSRk4Mixed>(variant, device, shape);
+    case kModeBundleMixed: return batch_shape<ModeBundleMixed>(variant, device, shape);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -134,6 +156,7 @@ cudaError_t launch_batch_mixed(Mode mode, int variant, const BatchRays& br, uint
     case kModeBLRk4Mixed: return batch_launch<ModeBLRk4Mixed>(variant, br, queue, fb, s, st);
     case kModeBLDopri5Mixed: return batch_launch<ModeBLDopri5Mixed>(variant, br, queue, fb, s, st);
     case kModeKSRk4Mixed: return batch_launch<ModeKSRk4Mixed>(variant, br, queue, fb, s, st);
+    case kModeBundleMixed: return batch_launch<ModeBundleMixed>(variant, br, queue, fb, s, st);
     default: return cudaErrorInvalidValue;
   }
 }

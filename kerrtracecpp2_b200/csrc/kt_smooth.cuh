@@ -113,8 +113,9 @@ struct ChartKS {
   static constexpr int kEq = 2;  // state index of the equator coordinate (Z)
   static constexpr double kEqTarget = 0.0;
 
-  // gy = dH/dy (X, Y, Z, pX, pY, pZ), gc = dH/dp_T, gp = dH/d(a, Q, Lambda).
-  template <class T>
+  // gy = dH/dy (X, Y, Z, pX, pY, pZ), gc = dH/dp_T, gp = dH/d(a, Q, Lambda)
+  // (only with kPrm: the right-hand side needs gy and gc alone).
+  template <class T, bool kPrm = true>
   KT_HD static void grad(double M, const SmPrm<T>& P, const T* y, const T* c, T* gy, T* gc, T* gp) {
     const T &X = y[0], &Y = y[1], &Z = y[2], &pX = y[3], &pY = y[4], &pZ = y[5], &pT = c[0];
     const T a = P.a, a2 = P.a * P.a;
@@ -143,7 +144,8 @@ struct ChartKS {
     // d/dX, d/dY, d/dZ, d/da
     const T rv[4] = {X * r * iE, Y * r * iE, Z * D * ir * iE, a * (Z2 - r2) * ir * iE};
     const T ir3 = ir * ir * ir;
-    for (int v = 0; v < 4; ++v) {
+#pragma unroll
+    for (int v = 0; v < (kPrm ? 4 : 3); ++v) {
       const T rr = rv[v];
       T drho2 = 2.0 * r * rr - 2.0 * a2 * Z2 * ir3 * rr;
       if (v == 2) drho2 = drho2 + 2.0 * a2 * Z * ir * ir;
@@ -164,8 +166,10 @@ struct ChartKS {
       else
         gp[0] = dH;
     }
-    gp[1] = P.Q * ell * ell * irho2;  // dF/dQ = -2Q/rho2
-    gp[2] = T(0.0);                   // the KS chart carries no Lambda
+    if (kPrm) {
+      gp[1] = P.Q * ell * ell * irho2;  // dF/dQ = -2Q/rho2
+      gp[2] = T(0.0);                   // the KS chart carries no Lambda
+    }
   }
 
   template <class T>
@@ -202,7 +206,7 @@ struct ChartBL {
   static constexpr int kEq = 1;  // theta
   static constexpr double kEqTarget = 1.57079632679489661923;  // M_PI/2 as the reference
 
-  template <class T>
+  template <class T, bool kPrm = true>
   KT_HD static void grad(double M, const SmPrm<T>& P, const T* y, const T* c, T* gy, T* gc, T* gp) {
     const T &r = y[0], &th = y[1], &pr = y[2], &pth = y[3], &pt = c[0], &pph = c[1];
     const T a = P.a, L = P.L;
@@ -233,7 +237,8 @@ struct ChartBL {
     const T WiT_P2iR = W * iT - Pp * Pp * iR;
     // dH/dv = (dK/dv - 2 H dS/dv) / (2 S) for v = r, theta, a, Q, Lambda
     const T zero(0.0);
-    for (int v = 0; v < 5; ++v) {
+#pragma unroll
+    for (int v = 0; v < (kPrm ? 5 : 2); ++v) {
       const T dA = v == 0 ? 2.0 * r : v == 2 ? 2.0 * a : zero;
       const T dS = v == 0 ? 2.0 * r : v == 1 ? -2.0 * a2 * sc : v == 2 ? 2.0 * a * c2 : zero;
       const T dR = v == 0 ? 2.0 * r * (1.0 - Lr2_3) - (2.0 * L * r / 3.0) * A - 2.0 * M
@@ -286,12 +291,48 @@ struct ChartBL {
 template <class C, class T>
 KT_HD_CALL void sm_rhs(double M, const SmPrm<T>& P, const T* y, const T* c, T* f, T* fpas) {
   T gy[C::kN], gc[C::kC], gp[kSmPrm];
-  C::grad(M, P, y, c, gy, gc, gp);
+  C::template grad<T, false>(M, P, y, c, gy, gc, gp);
   for (int i = 0; i < C::kX; ++i) {
     f[i] = gy[C::kX + i];
     f[C::kX + i] = -gy[i];
   }
   if (fpas) *fpas = (C::kC > 1) ? gc[C::kC - 1] : T(0.0);
+}
+
+// Bundle RHS (bundle_rhs, ray_bundle.hpp:130-156) from one evaluation of
+// the analytic BL gradient of H in Dual<2>, the tangents being W's two
+// columns: the values are the geodesic RHS (dr = dH/dp_r, dtheta = dH/dp_theta,
+// dp = -dH/dx, dphi = dH/dp_phi), the tangents the Hessian-vector products
+// Hess(H) W, so dW = J_s Hess(H) W needs no finite-difference Hessian (the
+// reference evaluates 33 Hamiltonians at 9 metric points for it).  FP64;
+// the mixed-precision bundle tracer's RHS.
+KT_HD void bundle_rhs_analytic(const Metric& g, const double y[4], double pt, double pphi,
+                               const double W[8], double k[5], double dW[8]) {
+  typedef Dual<2> D;
+  SmPrm<D> P;
+  P.a = D(g.a);
+  P.Q = D(g.Q);
+  P.L = D(g.L);
+  D yd[4], cd[2], gy[4], gc[2], gp[3];
+  for (int i = 0; i < 4; ++i) {
+    yd[i] = D(y[i]);
+    yd[i].d[0] = W[2 * i];
+    yd[i].d[1] = W[2 * i + 1];
+  }
+  cd[0] = D(pt);
+  cd[1] = D(pphi);
+  ChartBL::grad<D, false>(g.M, P, yd, cd, gy, gc, gp);
+  k[0] = gy[2].v;
+  k[1] = gy[3].v;
+  k[2] = -gy[0].v;
+  k[3] = -gy[1].v;
+  k[4] = gc[1].v;
+  for (int c = 0; c < 2; ++c) {
+    dW[c] = gy[2].d[c];
+    dW[2 + c] = gy[3].d[c];
+    dW[4 + c] = -gy[0].d[c];
+    dW[6 + c] = -gy[1].d[c];
+  }
 }
 
 // --------------------------------------------------------------- camera

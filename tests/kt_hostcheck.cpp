@@ -12,6 +12,7 @@
 
 #include "../include/kerrtrace.h"
 #include "../kerrtracecpp2_b200/csrc/kt_frame.h"
+#include "../kerrtracecpp2_b200/csrc/kt_smray.cuh"
 
 using namespace kt;
 
@@ -74,7 +75,10 @@ RayResult run_ray(const Frame& f, uint32_t pix) {
         if (slot < 0 && !m.needs_k1()) continue;
         double y[4], yW[8], k[5], kW[8];
         m.input(slot, y, yW);
-        bundle_rhs(f.g, y[0], y[1], y[2], y[3], m.pt, m.pphi, yW, k, kW);
+        if (f.precision == KT_PREC_MIXED)
+          bundle_rhs_analytic(f.g, y, m.pt, m.pphi, yW, k, kW);
+        else
+          bundle_rhs(f.g, y[0], y[1], y[2], y[3], m.pt, m.pphi, yW, k, kW);
         if (m.consume(f, slot, k, kW, &res)) return res;
       }
     }
@@ -131,8 +135,6 @@ extern "C" int hc_trace_pixels(const kt_frame_desc* d, int64_t n, const uint32_t
 // g++ with the kernels' floating-point flags): pixels pix[0..n) of the
 // frame; cotangent mode 0 (forward only), 1 (arrays over the frame's pixels)
 // or 2 (L2 against target arrays); contrib[kGSlots][n] per listed pixel.
-#include "../kerrtracecpp2_b200/csrc/kt_smray.cuh"
-
 extern "C" int hc_smooth_pixels(const kt_frame_desc* d, int64_t n, const uint32_t* pix, int mode,
                                 int force_bl, int tangent_dir, const double* cot_g, const double* cot_r,
                                 const uint8_t* t_out, const double* t_g, const double* t_r,

@@ -41,3 +41,20 @@ def test_mixed_against_fp64(renderer, name):
           f"p99 {np.percentile(eg, 99):.2e}, r rel err p50 {np.median(er):.2e}")
     assert 1 - same.mean() < 1e-4
     assert np.median(eg) < 5e-6 and np.median(er) < 5e-5
+
+
+def test_mixed_bundles_against_fp64(renderer):
+    """Bundle mode (config 3 geometry at 1/100 of the pixels): the analytic
+    Hessian-vector products against the reference's finite-difference
+    Hessian; magnification compared on the disk pixels."""
+    kw = dict(chart=1, bundles=1, a=0.998, theta_deg=60.0, width=192, height=108)
+    ref = trace(renderer, abi.frame_desc(**kw))
+    got = trace(renderer, abi.frame_desc(precision=abi.KT_PREC_MIXED, **kw))
+    same = got["outcome"] == ref["outcome"]
+    disk = same & (ref["outcome"] == 1)
+    eg = np.abs(got["redshift"][disk] - ref["redshift"][disk]) / np.abs(ref["redshift"][disk])
+    em = np.abs(got["magnif"][disk] - ref["magnif"][disk]) / np.abs(ref["magnif"][disk])
+    print(f"bundles: class mismatch {1 - same.mean():.2e}, g rel p50 {np.median(eg):.2e}, "
+          f"magnif rel p50 {np.median(em):.2e} p99 {np.percentile(em, 99):.2e}")
+    assert 1 - same.mean() < 1e-3
+    assert np.median(eg) < 5e-6 and np.median(em) < 1e-4

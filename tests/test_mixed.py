@@ -50,5 +50,23 @@ def test_mixed_uses_fp32_only_for_loose_tolerance():
     loose = kt.frame_derive(abi.frame_desc(precision=abi.KT_PREC_MIXED, tol=1e-7, width=4, height=4))
     assert strict.r_fp32 == float("inf")
     assert loose.r_fp32 == max(4.0, 2.0 * loose.r_horizon)
-    with pytest.raises(kt.KerrTraceError):
-        kt.frame_derive(abi.frame_desc(precision=abi.KT_PREC_MIXED, bundles=1, width=4, height=4))
+
+
+@pytest.mark.parametrize("name", ["cfg3_bundles", "bundle_step_cap"])
+def test_mixed_bundles_close_to_fp64_oracle(hc, name):  # noqa: F811
+    """Bundle mode with the analytic Hessian-vector products (one Dual<2>
+    gradient per RHS): class, g and the Jacobi magnification against the
+    reference's finite-difference Hessian."""
+    kw = dict(G.cases()[name])
+    kw["precision"] = abi.KT_PREC_MIXED
+    d = abi.frame_desc(**kw)
+    got = run(hc, d)
+    want = G.result(name)
+    mism, eg, er = errors(got, want)
+    n = d.width * d.height
+    assert mism * n <= max(1, 1e-3 * n)
+    disk = (got["outcome"] == want["outcome"]) & (want["outcome"] == 1)
+    if disk.any():
+        assert np.median(eg) < 1e-5 and np.median(er) < 1e-4
+        em = np.abs(got["magnif"][disk] - want["magnif"][disk]) / np.abs(want["magnif"][disk])
+        assert np.median(em) < 1e-4
