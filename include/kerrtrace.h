@@ -128,11 +128,16 @@ typedef struct kt_geo_soa {
   uint32_t* attempts; /* optional (NULL): adaptive attempts (accepted+rejected) */
 } kt_geo_soa;
 
-/* ColorParams (main.cpp:72-81), blackbody palette. */
+/* ColorParams (main.cpp:72-81). */
 typedef struct kt_color_params {
   double exposure, gamma, temp_scale;
-  int32_t palette; /* 0 = blackbody; 1 = interstellar (not implemented) */
+  int32_t palette; /* 0 = blackbody (disk_colour); 1 = interstellar
+                      (disk_colour_interstellar, main.cpp:1719-1797) */
   int32_t reserved0;
+  /* interstellar palette: rings x sectors of hashed warm colours,
+   * Gaussian-blended with width disk_sigma (cell units), hue offset */
+  int32_t disk_rings, disk_sectors;
+  double disk_sigma, disk_hue_offset;
 } kt_color_params;
 
 typedef struct kt_context kt_context;
@@ -192,17 +197,36 @@ kt_status kt_colorize(kt_context* ctx, const kt_frame_desc* desc,
                       uint8_t* rgb_out, void* stream);
 
 /* colorize_buffer (main.cpp:1817) on host buffers: the per-pixel records of
- * a width x height frame (e.g. read from a .kgeo file), black-hole mass M and
- * the ISCO radius recorded with them; RGB8 out (width*height*3 bytes). */
+ * a width x height frame (e.g. read from a .kgeo file), black-hole mass M,
+ * the ISCO radius and the disk's inner and outer radii recorded with them
+ * (KGeoMeta, main.cpp:101-106); RGB8 out (width*height*3 bytes). */
 kt_status kt_colorize_host(kt_context* ctx, const kt_geo_soa* geo_host, int32_t width,
-                           int32_t height, double M, double r_isco,
-                           const kt_color_params* cp, const uint8_t* bg_rgb_host,
-                           int32_t bg_w, int32_t bg_h, uint8_t* rgb_out_host);
+                           int32_t height, double M, double r_isco, double r_disk_in,
+                           double r_disk_out, const kt_color_params* cp,
+                           const uint8_t* bg_rgb_host, int32_t bg_w, int32_t bg_h,
+                           uint8_t* rgb_out_host);
 
 /* render_image equivalent: trace + colorize, host buffers in and out. */
 kt_status kt_render_host(kt_context* ctx, const kt_frame_desc* desc,
                          const kt_color_params* cp, const uint8_t* bg_rgb_host,
                          int32_t bg_w, int32_t bg_h, uint8_t* rgb_out_host);
+
+/* render_image with its camera_spp argument (main.cpp:2232-2322, the CLI's
+ * --camera-spp / --spp, main.cpp:2557): camera_spp passes, each a full
+ * trace + colorize at the frame's pixel offset plus the pass's jitter
+ * (kt_camera_spp_offsets), averaged in linear light
+ * (pow(c / 255, gamma), mean, pow(., 1 / gamma), lround) on the device.
+ * camera_spp <= 1 is kt_render_host.  KT_ERR_INVALID_ARGUMENT above
+ * KT_MAX_CAMERA_SPP. */
+#define KT_MAX_CAMERA_SPP 256
+kt_status kt_render_spp_host(kt_context* ctx, const kt_frame_desc* desc,
+                             const kt_color_params* cp, int32_t camera_spp,
+                             const uint8_t* bg_rgb_host, int32_t bg_w, int32_t bg_h,
+                             uint8_t* rgb_out_host);
+
+/* The camera_spp jitter offsets in pixels (main.cpp:2238-2279):
+ * xy[2 s], xy[2 s + 1] for pass s < max(camera_spp, 1). */
+kt_status kt_camera_spp_offsets(int32_t camera_spp, double* xy);
 
 /* ---- batches: many frames in one CUDA graph launch ----------------------
  * No counterpart in the reference renderer, which traces one frame per

@@ -77,6 +77,10 @@ def load_library():
     L.kt_colorize.restype = ctypes.c_int
     L.kt_render_host.argtypes = [P, PD, ctypes.POINTER(ColorParams), P, I32, I32, P]
     L.kt_render_host.restype = ctypes.c_int
+    L.kt_render_spp_host.argtypes = [P, PD, ctypes.POINTER(ColorParams), I32, P, I32, I32, P]
+    L.kt_render_spp_host.restype = ctypes.c_int
+    L.kt_camera_spp_offsets.argtypes = [I32, P]
+    L.kt_camera_spp_offsets.restype = ctypes.c_int
     L.kt_measure_fp64_peak.argtypes = [P, ctypes.POINTER(D)]
     L.kt_measure_fp64_peak.restype = ctypes.c_int
     L.kt_starfield.argtypes = [ctypes.c_uint64, I32, I32, P]
@@ -333,14 +337,16 @@ class Renderer:
                "kt_trace_host", self.ctx)
         return out
 
-    def render_host(self, desc, cp=None, bg=None):
+    def render_host(self, desc, cp=None, bg=None, camera_spp=1):
+        """render_image: trace + colorize into an (H, W, 3) uint8 image;
+        camera_spp > 1 averages that many jittered passes in linear light."""
         cp = cp or color_params()
         rgb = np.zeros((desc.height, desc.width, 3), np.uint8)
         bgc = np.ascontiguousarray(bg) if bg is not None else None
         bw, bh = (bg.shape[1], bg.shape[0]) if bg is not None else (0, 0)
-        _check(self.L.kt_render_host(self.ctx, ctypes.byref(desc), ctypes.byref(cp),
-                                     _np_ptr(bgc) if bgc is not None else None, bw, bh, _np_ptr(rgb)),
-               "kt_render_host", self.ctx)
+        _check(self.L.kt_render_spp_host(self.ctx, ctypes.byref(desc), ctypes.byref(cp), int(camera_spp),
+                                         _np_ptr(bgc) if bgc is not None else None, bw, bh, _np_ptr(rgb)),
+               "kt_render_spp_host", self.ctx)
         return rgb
 
 
@@ -432,11 +438,22 @@ def trace_geodesics(W, H, fp, use_bundles=False, chart=KT_CHART_KS, intg=KT_RK4_
 
 def render_image(W, H, fp, bg=None, use_bundles=False, chart=KT_CHART_KS, intg=KT_RK4_DOUBLING,
                  ctl=None, M_bh=1.0, Q_bh=0.0, Lam=0.0, cp=None, pixel_offset_x=0.0,
-                 pixel_offset_y=0.0, device=0):
-    """render_image (main.cpp:2209): trace + colorize; (H, W, 3) uint8."""
+                 pixel_offset_y=0.0, device=0, camera_spp=1):
+    """render_image (main.cpp:2209): trace + colorize; (H, W, 3) uint8.
+    camera_spp > 1 renders that many jittered passes and averages them in
+    linear light (main.cpp:2232-2322)."""
     desc = make_desc(W, H, fp, use_bundles, chart, intg, ctl, pixel_offset_x, pixel_offset_y, M_bh,
                      Q_bh, Lam)
-    return _renderer(device).render_host(desc, cp, bg)
+    return _renderer(device).render_host(desc, cp, bg, camera_spp)
+
+
+def camera_spp_offsets(camera_spp):
+    """kt_camera_spp_offsets: the (spp, 2) pixel jitter of each pass."""
+    L = load_library()
+    n = max(int(camera_spp), 1)
+    xy = np.zeros((n, 2), np.float64)
+    _check(L.kt_camera_spp_offsets(int(camera_spp), _np_ptr(xy)), "kt_camera_spp_offsets")
+    return xy
 
 
 def colorize_buffer(geo, desc, cp=None, bg=None, device=0):

@@ -26,6 +26,9 @@ KT_SOLVER_ELLIPTIC_CLOSED = 2
 KT_PREC_FP64 = 0
 KT_PREC_MIXED = 1
 KT_PREC_SMOOTH = 2
+KT_PALETTE_BLACKBODY = 0
+KT_PALETTE_INTERSTELLAR = 1
+KT_MAX_CAMERA_SPP = 256
 KT_OUT_ESCAPED = 0
 KT_OUT_DISK = 1
 KT_OUT_HORIZON = 2
@@ -81,7 +84,9 @@ class ColorParams(ctypes.Structure):
     _fields_ = [
         ("exposure", ctypes.c_double), ("gamma", ctypes.c_double),
         ("temp_scale", ctypes.c_double), ("palette", ctypes.c_int32),
-        ("reserved0", ctypes.c_int32),
+        ("reserved0", ctypes.c_int32), ("disk_rings", ctypes.c_int32),
+        ("disk_sectors", ctypes.c_int32), ("disk_sigma", ctypes.c_double),
+        ("disk_hue_offset", ctypes.c_double),
     ]
 
 
@@ -174,9 +179,12 @@ def frame_desc(**kw):
 
 
 def color_params(**kw):
-    """ColorParams defaults (main.cpp:72-81): exposure 1, gamma 2.2, temp_scale 1."""
+    """ColorParams defaults (main.cpp:72-81): exposure 1, gamma 2.2, temp_scale 1,
+    blackbody palette; interstellar palette 7 rings x 14 sectors, sigma 0.5,
+    hue offset 0."""
     c = ColorParams()
     c.exposure, c.gamma, c.temp_scale, c.palette = 1.0, 2.2, 1.0, 0
+    c.disk_rings, c.disk_sectors, c.disk_sigma, c.disk_hue_offset = 7, 14, 0.5, 0.0
     for k, v in kw.items():
         setattr(c, k, v)
     return c

@@ -214,6 +214,10 @@ int main(int argc, char** argv) {
     else if (a == "--temp-scale") cp.temp_scale = atof(next());
     else if (a == "--disk-interstellar") cp.palette = 1;
     else if (a == "--disk-blackbody") cp.palette = 0;
+    else if (a == "--disk-rings") cp.disk_rings = atoi(next());
+    else if (a == "--disk-sectors") cp.disk_sectors = atoi(next());
+    else if (a == "--disk-sigma") cp.disk_sigma = atof(next());
+    else if (a == "--disk-hue-offset") cp.disk_hue_offset = atof(next());
     else if (a == "--geo-only") geo_only = true;
     else if (a == "--geo-file") geo_file = next();
     else if (a == "--color-only") {
@@ -243,14 +247,16 @@ int main(int argc, char** argv) {
            "\"width\": %d, \"height\": %d, \"chart\": %d, \"integrator\": %d, \"bundles\": %d, "
            "\"solver_mode\": %d, \"max_steps\": %d, \"step_init\": %.17g, \"tol\": %.17g, "
            "\"camera_spp\": %d, \"exposure\": %.17g, \"gamma\": %.17g, \"temp_scale\": %.17g, "
-           "\"palette\": %d}\n",
+           "\"palette\": %d, \"disk_rings\": %d, \"disk_sectors\": %d, \"disk_sigma\": %.17g, "
+           "\"disk_hue_offset\": %.17g}\n",
            d.M, d.a, d.Q, d.Lambda, d.theta_deg, d.phi_deg, d.r_obs, d.disk_out, d.fov_deg, d.width,
            d.height, d.chart, d.integrator, d.bundles, d.solver_mode, d.max_steps, d.step_init, d.tol,
-           camera_spp, cp.exposure, cp.gamma, cp.temp_scale, cp.palette);
+           camera_spp, cp.exposure, cp.gamma, cp.temp_scale, cp.palette, cp.disk_rings,
+           cp.disk_sectors, cp.disk_sigma, cp.disk_hue_offset);
     return 0;
   }
-  if (camera_spp > 1) {
-    fprintf(stderr, "Error: --camera-spp > 1 is not implemented by this backend yet\n");
+  if (camera_spp > KT_MAX_CAMERA_SPP) {
+    fprintf(stderr, "Error: --camera-spp above %d is not supported\n", KT_MAX_CAMERA_SPP);
     return 2;
   }
 
@@ -280,8 +286,8 @@ int main(int argc, char** argv) {
     if (st != KT_OK) return die("cannot read .kgeo", ctx, st);
     printf("Loaded: %s  %dx%d  a=%g  r_isco=%g\n", geo_file.c_str(), W, H, meta[1], meta[4]);
     std::vector<uint8_t> rgb(3 * n);
-    st = kt_colorize_host(ctx, &g, W, H, meta[0], meta[4], &cp, bg.empty() ? nullptr : bg.data(), bw,
-                          bh, rgb.data());
+    st = kt_colorize_host(ctx, &g, W, H, meta[0], meta[4], meta[5], meta[6], &cp,
+                          bg.empty() ? nullptr : bg.data(), bw, bh, rgb.data());
     if (st != KT_OK) return die("colorize", ctx, st);
     std::string base = geo_file;
     if (base.size() > 5 && base.substr(base.size() - 5) == ".kgeo") base = base.substr(0, base.size() - 5);
@@ -302,32 +308,52 @@ int main(int argc, char** argv) {
          dv.integrator == KT_DOPRI5 ? "DOPRI5" : "RK4-doubling", d.tol, d.max_steps, d.width,
          d.height);
   const size_t n = (size_t)d.width * d.height;
+  const std::string spp_tag = camera_spp > 1 ? "_spp" + std::to_string(camera_spp) : "";
   const std::string tag = std::string(d.bundles ? "bundles" : "trace") + "_" +
                           std::to_string(d.width) + "x" + std::to_string(d.height) + "_" +
-                          (dv.chart == KT_CHART_KS ? "ks" : "bl") + "_gpu-b200_" + timestamp();
+                          (dv.chart == KT_CHART_KS ? "ks" : "bl") + "_gpu-b200" + spp_tag + "_" +
+                          timestamp();
   const double t0 = now_s();
-  if (geo_only) {
-    std::vector<uint8_t> oc(n);
-    std::vector<double> f6(6 * n);
-    kt_geo_soa g = {oc.data(), &f6[0], &f6[n], &f6[2 * n], &f6[3 * n], &f6[4 * n], &f6[5 * n],
-                    nullptr, nullptr, nullptr};
+  // main.cpp:2897-2945: --geo-only traces and saves the .kgeo (camera_spp
+  // plays no part); a full render with --geo-file also saves the frame's
+  // .kgeo beside the PNG, except with camera_spp > 1 (main.cpp:2232-2236).
+  const bool save_geo = geo_only || (!geo_file.empty() && camera_spp <= 1);
+  if (!geo_only && !geo_file.empty() && camera_spp > 1)
+    fprintf(stderr, "Info: camera-spp>1 uses jittered multi-pass sampling and disables .kgeo export "
+                    "for this frame.\n");
+  std::vector<uint8_t> oc, rgb;
+  std::vector<double> f6;
+  kt_geo_soa g = {};
+  if (save_geo) {
+    oc.resize(n);
+    f6.resize(6 * n);
+    g = {oc.data(), &f6[0], &f6[n], &f6[2 * n], &f6[3 * n], &f6[4 * n], &f6[5 * n], nullptr, nullptr,
+         nullptr};
     st = kt_trace_host(ctx, &d, &g);
     if (st != KT_OK) return die("trace", ctx, st);
-    const double el = now_s() - t0;
-    printf("Trace: %gs  (%.1f kpix/s)\n", el, n / el / 1e3);
+  }
+  if (!geo_only) {
+    rgb.resize(3 * n);
+    if (save_geo)
+      st = kt_colorize_host(ctx, &g, d.width, d.height, d.M, dv.r_isco, dv.r_disk_in, dv.r_disk_out,
+                            &cp, bg.empty() ? nullptr : bg.data(), bw, bh, rgb.data());
+    else
+      st = kt_render_spp_host(ctx, &d, &cp, camera_spp, bg.empty() ? nullptr : bg.data(), bw, bh,
+                              rgb.data());
+    if (st != KT_OK) return die("render", ctx, st);
+  }
+  const double el = now_s() - t0;
+  printf("%s: %gs  (%.1f kpix/s)\n", geo_only ? "Trace" : "Time", el, n / el / 1e3);
+  if (!geo_only) {
+    const std::string png = out_path.empty() ? out_dir + "/" + tag + ".png" : out_path;
+    if (!write_png(png.c_str(), rgb.data(), d.width, d.height)) return die("cannot write PNG", ctx, KT_ERR_IO);
+    printf("Saved: %s\n", png.c_str());
+  }
+  if (save_geo) {
     const std::string path = geo_file.empty() ? out_dir + "/" + tag + ".kgeo" : geo_file;
     st = kt_kgeo_write(path.c_str(), &d, &g);
     if (st != KT_OK) return die("cannot write .kgeo", ctx, st);
     printf("Geo saved: %s\n", path.c_str());
-  } else {
-    std::vector<uint8_t> rgb(3 * n);
-    st = kt_render_host(ctx, &d, &cp, bg.empty() ? nullptr : bg.data(), bw, bh, rgb.data());
-    if (st != KT_OK) return die("render", ctx, st);
-    const double el = now_s() - t0;
-    printf("Time: %gs  (%.1f kpix/s)\n", el, n / el / 1e3);
-    const std::string png = out_path.empty() ? out_dir + "/" + tag + ".png" : out_path;
-    if (!write_png(png.c_str(), rgb.data(), d.width, d.height)) return die("cannot write PNG", ctx, KT_ERR_IO);
-    printf("Saved: %s\n", png.c_str());
   }
   kt_destroy(ctx);
   return 0;

@@ -69,6 +69,48 @@ kt_status run_trace(kt_context* ctx, const kt::Frame& f, const kt::OutSoA& out,
   return KT_OK;
 }
 
+// The jitter offsets of render_image's camera_spp branch (main.cpp:2238-2279):
+// spp = 2 splits horizontally; otherwise the centre for odd spp, then +/-
+// pairs from a fixed table, then +/- pairs on a golden-angle spiral of
+// radius 0.49 sqrt((m + 1) / (spp + 1)).
+void spp_offsets(int spp, double* xy) {
+  if (spp <= 1) {
+    xy[0] = xy[1] = 0.0;
+    return;
+  }
+  if (spp == 2) {
+    xy[0] = -0.35; xy[1] = 0.0;
+    xy[2] = 0.35; xy[3] = 0.0;
+    return;
+  }
+  static const double kPairs[7][2] = {{0.35, 0.00}, {0.00, 0.35}, {0.25, 0.25}, {0.45, 0.20},
+                                      {0.20, 0.45}, {0.40, 0.00}, {0.00, 0.40}};
+  int k = 0;
+  if (spp % 2 == 1) {
+    xy[0] = xy[1] = 0.0;
+    k = 1;
+  }
+  for (int j = 0; j < 7 && k + 2 <= spp; ++j, k += 2) {
+    xy[2 * k] = kPairs[j][0];
+    xy[2 * k + 1] = kPairs[j][1];
+    xy[2 * k + 2] = -kPairs[j][0];
+    xy[2 * k + 3] = -kPairs[j][1];
+  }
+  const double golden = 2.39996322972865332;
+  for (int m = 1; k < spp; ++m) {
+    const double rad = 0.49 * sqrt((double)m / (double)(spp + 1));
+    const double ang = golden * (double)m;
+    const double x = rad * ktm_cos(ang), y = rad * ktm_sin(ang);
+    xy[2 * k] = x;
+    xy[2 * k + 1] = y;
+    if (++k < spp) {
+      xy[2 * k] = -x;
+      xy[2 * k + 1] = -y;
+      ++k;
+    }
+  }
+}
+
 }  // namespace
 
 extern "C" {
@@ -124,6 +166,11 @@ void kt_color_params_defaults(kt_color_params* cp) {
   cp->exposure = 1.0;
   cp->gamma = 2.2;
   cp->temp_scale = 1.0;
+  // ColorParams' defaults (main.cpp:76-80)
+  cp->disk_rings = 7;
+  cp->disk_sectors = 14;
+  cp->disk_sigma = 0.5;
+  cp->disk_hue_offset = 0.0;
 }
 
 kt_status kt_frame_derive(const kt_frame_desc* desc, kt_frame_derived* out) {
@@ -262,7 +309,10 @@ kt_status kt_colorize(kt_context* ctx, const kt_frame_desc* desc, const kt_geo_s
     return fail(ctx, KT_ERR_INVALID_ARGUMENT, "kt_colorize: NULL pointer");
   if (bg_rgb && (bg_w < 1 || bg_h < 1))
     return fail(ctx, KT_ERR_INVALID_ARGUMENT, "kt_colorize: background size must be >= 1");
-  if (cp->palette != 0) return fail(ctx, KT_ERR_UNSUPPORTED, "only the blackbody palette is implemented");
+  if (cp->palette != 0 && cp->palette != 1)
+    return fail(ctx, KT_ERR_INVALID_ARGUMENT, "kt_colorize: palette must be 0 (blackbody) or 1 (interstellar)");
+  if (cp->palette == 1 && !geo->phi_disk)
+    return fail(ctx, KT_ERR_INVALID_ARGUMENT, "kt_colorize: the interstellar palette needs phi_disk");
   kt::Frame f;
   kt_status r = kt::prepare_frame(desc, &f, nullptr, &ctx->err);
   if (r != KT_OK) return r;
@@ -270,7 +320,8 @@ kt_status kt_colorize(kt_context* ctx, const kt_frame_desc* desc, const kt_geo_s
   const kt::ColourConst cc = kt::make_colour(f, *cp);
   const int64_t n = (int64_t)desc->width * desc->height;
   KT_CUDA(ctx, kt::launch_colorize(cc, n, geo->outcome, geo->r, geo->redshift, geo->magnif,
-                                   geo->theta_esc, geo->phi_esc, bg_rgb, bg_w, bg_h, rgb_out,
+                                   geo->phi_disk, geo->theta_esc, geo->phi_esc, bg_rgb, bg_w, bg_h,
+                                   rgb_out,
                                    (cudaStream_t)stream),
           "colorize kernel launch");
   return KT_OK;
@@ -279,16 +330,29 @@ kt_status kt_colorize(kt_context* ctx, const kt_frame_desc* desc, const kt_geo_s
 kt_status kt_render_host(kt_context* ctx, const kt_frame_desc* desc, const kt_color_params* cp,
                          const uint8_t* bg_rgb_host, int32_t bg_w, int32_t bg_h,
                          uint8_t* rgb_out_host) {
+  return kt_render_spp_host(ctx, desc, cp, 1, bg_rgb_host, bg_w, bg_h, rgb_out_host);
+}
+
+kt_status kt_render_spp_host(kt_context* ctx, const kt_frame_desc* desc, const kt_color_params* cp,
+                             int32_t camera_spp, const uint8_t* bg_rgb_host, int32_t bg_w,
+                             int32_t bg_h, uint8_t* rgb_out_host) {
   if (!ctx) return KT_ERR_INVALID_ARGUMENT;
-  if (!cp || !rgb_out_host) return fail(ctx, KT_ERR_INVALID_ARGUMENT, "kt_render_host: NULL pointer");
+  if (!desc || !cp || !rgb_out_host) return fail(ctx, KT_ERR_INVALID_ARGUMENT, "kt_render_host: NULL pointer");
   if (bg_rgb_host && (bg_w < 1 || bg_h < 1))
     return fail(ctx, KT_ERR_INVALID_ARGUMENT, "kt_render_host: background size must be >= 1");
+  if (cp->palette != 0 && cp->palette != 1)
+    return fail(ctx, KT_ERR_INVALID_ARGUMENT, "kt_render_host: palette must be 0 or 1");
+  const int spp = camera_spp < 1 ? 1 : camera_spp;
+  if (spp > KT_MAX_CAMERA_SPP)
+    return fail(ctx, KT_ERR_INVALID_ARGUMENT, "kt_render_spp_host: camera_spp above KT_MAX_CAMERA_SPP");
   kt::Frame f;
   kt_status r = kt::prepare_frame(desc, &f, nullptr, &ctx->err);
   if (r != KT_OK) return r;
   DeviceGuard g(ctx->device);
   const size_t n = (size_t)desc->width * (size_t)desc->height;
-  const size_t need = n * (6 * 8 + 1 + 3) + 256;
+  // six float64 fields, the linear-light sum (spp > 1), outcome, one RGB pass
+  const size_t acc_bytes = spp > 1 ? 24 * n : 0;
+  const size_t need = n * (6 * 8 + 1 + 3) + acc_bytes + 256;
   r = ensure(ctx, (void**)&ctx->d_stage, &ctx->stage_cap, need, "staging buffer");
   if (r != KT_OK) return r;
   unsigned char* p = ctx->d_stage;
@@ -300,6 +364,7 @@ kt_status kt_render_host(kt_context* ctx, const kt_frame_desc* desc, const kt_co
   d.phi_disk = (double*)p; p += 8 * n;
   d.theta_esc = (double*)p; p += 8 * n;
   d.phi_esc = (double*)p; p += 8 * n;
+  double* d_acc = (double*)p; p += acc_bytes;
   d.outcome = p; p += n;
   uint8_t* d_rgb = p;
   const uint8_t* d_bg = nullptr;
@@ -311,24 +376,52 @@ kt_status kt_render_host(kt_context* ctx, const kt_frame_desc* desc, const kt_co
             "copy background");
     d_bg = ctx->d_bg;
   }
+  // render_image (main.cpp:2232-2322): with camera_spp > 1 every pass is a
+  // full render at the frame's pixel offset plus the pass's jitter.
+  double offs[2 * KT_MAX_CAMERA_SPP];
+  spp_offsets(spp, offs);
+  const double gamma_eff = cp->gamma < 1e-6 ? 1e-6 : cp->gamma;
   kt::RayList rl = {nullptr, nullptr, nullptr, (uint32_t)n};
-  r = run_trace(ctx, f, to_out(&d), rl, n, ctx->stream);
-  if (r != KT_OK) return r;
-  const kt::ColourConst cc = kt::make_colour(f, *cp);
-  if (cp->palette != 0) return fail(ctx, KT_ERR_UNSUPPORTED, "only the blackbody palette is implemented");
-  KT_CUDA(ctx, kt::launch_colorize(cc, (int64_t)n, d.outcome, d.r, d.redshift, d.magnif, d.theta_esc,
-                                   d.phi_esc, d_bg, bg_w, bg_h, d_rgb, ctx->stream),
-          "colorize kernel launch");
+  for (int s = 0; s < spp; ++s) {
+    kt::Frame fs;
+    if (spp == 1) {
+      fs = f;
+    } else {
+      kt_frame_desc ds = *desc;
+      ds.pixel_offset_x = desc->pixel_offset_x + offs[2 * s];
+      ds.pixel_offset_y = desc->pixel_offset_y + offs[2 * s + 1];
+      r = kt::prepare_frame(&ds, &fs, nullptr, &ctx->err);
+      if (r != KT_OK) return r;
+    }
+    r = run_trace(ctx, fs, to_out(&d), rl, n, ctx->stream);
+    if (r != KT_OK) return r;
+    const kt::ColourConst cc = kt::make_colour(fs, *cp);
+    KT_CUDA(ctx, kt::launch_colorize(cc, (int64_t)n, d.outcome, d.r, d.redshift, d.magnif, d.phi_disk,
+                                     d.theta_esc, d.phi_esc, d_bg, bg_w, bg_h, d_rgb, ctx->stream),
+            "colorize kernel launch");
+    if (spp > 1)
+      KT_CUDA(ctx, kt::launch_spp_accumulate((int64_t)(3 * n), d_rgb, d_acc, gamma_eff, s == 0, ctx->stream),
+              "supersample accumulate launch");
+  }
+  if (spp > 1)
+    KT_CUDA(ctx, kt::launch_spp_finish((int64_t)(3 * n), d_acc, 1.0 / (double)spp, gamma_eff, d_rgb, ctx->stream),
+            "supersample finish launch");
   KT_CUDA(ctx, cudaMemcpyAsync(rgb_out_host, d_rgb, 3 * n, cudaMemcpyDeviceToHost, ctx->stream),
           "copy image to host");
   KT_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "render");
   return KT_OK;
 }
 
+kt_status kt_camera_spp_offsets(int32_t camera_spp, double* xy) {
+  if (!xy || camera_spp > KT_MAX_CAMERA_SPP) return KT_ERR_INVALID_ARGUMENT;
+  spp_offsets(camera_spp < 1 ? 1 : camera_spp, xy);
+  return KT_OK;
+}
+
 kt_status kt_colorize_host(kt_context* ctx, const kt_geo_soa* g, int32_t width, int32_t height,
-                           double M, double r_isco, const kt_color_params* cp,
-                           const uint8_t* bg_rgb_host, int32_t bg_w, int32_t bg_h,
-                           uint8_t* rgb_out_host) {
+                           double M, double r_isco, double r_disk_in, double r_disk_out,
+                           const kt_color_params* cp, const uint8_t* bg_rgb_host, int32_t bg_w,
+                           int32_t bg_h, uint8_t* rgb_out_host) {
   if (!ctx) return KT_ERR_INVALID_ARGUMENT;
   if (!g || !g->outcome || !g->r || !g->redshift || !g->magnif || !g->theta_esc || !g->phi_esc ||
       !cp || !rgb_out_host)
@@ -337,10 +430,13 @@ kt_status kt_colorize_host(kt_context* ctx, const kt_geo_soa* g, int32_t width, 
     return fail(ctx, KT_ERR_INVALID_ARGUMENT, "kt_colorize_host: bad frame size");
   if (bg_rgb_host && (bg_w < 1 || bg_h < 1))
     return fail(ctx, KT_ERR_INVALID_ARGUMENT, "kt_colorize_host: background size must be >= 1");
-  if (cp->palette != 0) return fail(ctx, KT_ERR_UNSUPPORTED, "only the blackbody palette is implemented");
+  if (cp->palette != 0 && cp->palette != 1)
+    return fail(ctx, KT_ERR_INVALID_ARGUMENT, "kt_colorize_host: palette must be 0 or 1");
+  if (cp->palette == 1 && !g->phi_disk)
+    return fail(ctx, KT_ERR_INVALID_ARGUMENT, "kt_colorize_host: the interstellar palette needs phi_disk");
   DeviceGuard guard(ctx->device);
   const size_t n = (size_t)width * (size_t)height;
-  const size_t need = n * (5 * 8 + 1 + 3) + 256;
+  const size_t need = n * (6 * 8 + 1 + 3) + 256;
   kt_status r = ensure(ctx, (void**)&ctx->d_stage, &ctx->stage_cap, need, "staging buffer");
   if (r != KT_OK) return r;
   unsigned char* p = ctx->d_stage;
@@ -349,13 +445,17 @@ kt_status kt_colorize_host(kt_context* ctx, const kt_geo_soa* g, int32_t width, 
   double* d_mag = (double*)p; p += 8 * n;
   double* d_th = (double*)p; p += 8 * n;
   double* d_ph = (double*)p; p += 8 * n;
+  double* d_pd = (double*)p; p += 8 * n;
   uint8_t* d_out = p; p += n;
   uint8_t* d_rgb = p;
   const struct { void* dst; const void* src; size_t bytes; } cps[] = {
       {d_r, g->r, 8 * n}, {d_red, g->redshift, 8 * n}, {d_mag, g->magnif, 8 * n},
-      {d_th, g->theta_esc, 8 * n}, {d_ph, g->phi_esc, 8 * n}, {d_out, g->outcome, n}};
+      {d_th, g->theta_esc, 8 * n}, {d_ph, g->phi_esc, 8 * n}, {d_out, g->outcome, n},
+      {d_pd, g->phi_disk, 8 * n}};
   for (const auto& c : cps)
-    KT_CUDA(ctx, cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyHostToDevice, ctx->stream), "copy in");
+    if (c.src)
+      KT_CUDA(ctx, cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyHostToDevice, ctx->stream),
+              "copy in");
   const uint8_t* d_bg = nullptr;
   if (bg_rgb_host) {
     const size_t bb = (size_t)bg_w * (size_t)bg_h * 3;
@@ -373,8 +473,16 @@ kt_status kt_colorize_host(kt_context* ctx, const kt_geo_soa* g, int32_t width, 
   cc.temp_scale = cp->temp_scale;
   cc.log10_50 = ktm_log10(4e4 / 800.0);
   cc.pt_peak = kt::page_thorne(3.0 * r_isco, r_isco);
-  KT_CUDA(ctx, kt::launch_colorize(cc, (int64_t)n, d_out, d_r, d_red, d_mag, d_th, d_ph, d_bg, bg_w,
-                                   bg_h, d_rgb, ctx->stream),
+  cc.palette = cp->palette;
+  cc.rings = cp->disk_rings;
+  cc.sectors = cp->disk_sectors;
+  cc.pad0 = 0;
+  cc.sigma = cp->disk_sigma;
+  cc.hue_offset = cp->disk_hue_offset;
+  cc.r_in = r_disk_in;
+  cc.r_out = r_disk_out;
+  KT_CUDA(ctx, kt::launch_colorize(cc, (int64_t)n, d_out, d_r, d_red, d_mag, d_pd, d_th, d_ph, d_bg,
+                                   bg_w, bg_h, d_rgb, ctx->stream),
           "colorize kernel launch");
   KT_CUDA(ctx, cudaMemcpyAsync(rgb_out_host, d_rgb, 3 * n, cudaMemcpyDeviceToHost, ctx->stream),
           "copy image to host");

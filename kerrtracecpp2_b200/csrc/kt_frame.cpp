@@ -265,6 +265,14 @@ ColourConst make_colour(const Frame& f, const kt_color_params& cp) {
   cc.temp_scale = cp.temp_scale;
   cc.log10_50 = ktm_log10(4e4 / 800.0);  // blackbody's log10(4e4/800.0), main.cpp:1665
   cc.pt_peak = page_thorne(3.0 * f.r_in, f.r_in);
+  cc.palette = cp.palette;
+  cc.rings = cp.disk_rings;
+  cc.sectors = cp.disk_sectors;
+  cc.pad0 = 0;
+  cc.sigma = cp.disk_sigma;
+  cc.hue_offset = cp.disk_hue_offset;
+  cc.r_in = f.r_in;
+  cc.r_out = f.r_out;
   return cc;
 }
 

@@ -84,8 +84,16 @@ cudaError_t launch_trace(Mode mode, const Frame& f, const OutSoA& out, const Ray
 // Colour pass: SoA -> RGB8.
 cudaError_t launch_colorize(const ColourConst& cc, int64_t n, const uint8_t* outcome,
                             const double* r, const double* red, const double* magnif,
-                            const double* th_esc, const double* ph_esc, const uint8_t* bg,
+                            const double* phi_disk, const double* th_esc, const double* ph_esc,
+                            const uint8_t* bg,
                             int bg_w, int bg_h, uint8_t* rgb, cudaStream_t stream);
+
+// Camera supersampling over n3 = 3 x pixels channel values: linear-light sum
+// of the passes (first != 0 starts it) and the mean back to 8 bits.
+cudaError_t launch_spp_accumulate(int64_t n3, const uint8_t* rgb, double* acc, double gamma, int first,
+                                  cudaStream_t stream);
+cudaError_t launch_spp_finish(int64_t n3, const double* acc, double inv_n, double gamma, uint8_t* rgb,
+                              cudaStream_t stream);
 
 // Mixed-precision kernels (kt_mixed.cu).
 cudaError_t launch_shape_mixed(Mode mode, int device, LaunchShape* shape);

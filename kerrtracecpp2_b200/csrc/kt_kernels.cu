@@ -140,14 +140,18 @@ cudaError_t launch_batch(Mode mode, int variant, const BatchRays& br, uint32_t* 
 // colours from float32 GeoPixel fields; the same rounding is applied here.
 __global__ void k_colorize(const ColourConst cc, int64_t n, const uint8_t* __restrict__ outcome,
                            const double* __restrict__ r, const double* __restrict__ red,
-                           const double* __restrict__ magnif, const double* __restrict__ th_esc,
+                           const double* __restrict__ magnif, const double* __restrict__ phi_disk,
+                           const double* __restrict__ th_esc,
                            const double* __restrict__ ph_esc, const uint8_t* __restrict__ bg,
                            int bg_w, int bg_h, uint8_t* __restrict__ rgb) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     uint8_t c[3] = {0, 0, 0};
     const int oc = outcome[i];
-    if (oc == kOutDisk) {
+    if (oc == kOutDisk && cc.palette == 1) {
+      disk_colour_interstellar(cc, (double)(float)r[i], (double)(float)phi_disk[i],
+                               (double)(float)red[i], (double)(float)magnif[i], c);
+    } else if (oc == kOutDisk) {
       disk_colour(cc, (double)(float)r[i], (double)(float)red[i], (double)(float)magnif[i], c);
     } else if (oc == kOutEscaped && bg != nullptr) {
       bg_sample(bg, bg_w, bg_h, (double)(float)th_esc[i], (double)(float)ph_esc[i], c);
@@ -160,14 +164,61 @@ __global__ void k_colorize(const ColourConst cc, int64_t n, const uint8_t* __res
 
 cudaError_t launch_colorize(const ColourConst& cc, int64_t n, const uint8_t* outcome,
                             const double* r, const double* red, const double* magnif,
-                            const double* th_esc, const double* ph_esc, const uint8_t* bg,
+                            const double* phi_disk, const double* th_esc, const double* ph_esc,
+                            const uint8_t* bg,
                             int bg_w, int bg_h, uint8_t* rgb, cudaStream_t stream) {
   if (n <= 0) return cudaSuccess;
   const int block = 256;
   int64_t grid = (n + block - 1) / block;
   if (grid > 148 * 32) grid = 148 * 32;
-  k_colorize<<<(int)grid, block, 0, stream>>>(cc, n, outcome, r, red, magnif, th_esc, ph_esc, bg,
-                                              bg_w, bg_h, rgb);
+  k_colorize<<<(int)grid, block, 0, stream>>>(cc, n, outcome, r, red, magnif, phi_disk, th_esc,
+                                              ph_esc, bg, bg_w, bg_h, rgb);
+  return cudaGetLastError();
+}
+
+// ---- camera supersampling ------------------------------------------------------
+
+// render_image's camera_spp > 1 branch (main.cpp:2280-2321): each pass's
+// 8-bit image is taken to linear light, pow(clamp(c/255, 0, 1), gamma), and
+// summed in pass order; the sum of the first pass is the value itself.
+__global__ void k_spp_accumulate(int64_t n3, const uint8_t* __restrict__ rgb, double* __restrict__ acc,
+                                 double gamma, int first) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n3;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double lin = ktm_pow(dclamp((double)rgb[i] / 255.0, 0.0, 1.0), gamma);
+    acc[i] = first ? lin : acc[i] + lin;
+  }
+}
+
+// The mean back to display values: lround(255 pow(clamp(acc / n, 0, 1), 1 / gamma)),
+// lround's half-away-from-zero rounding written out for a non-negative value.
+__global__ void k_spp_finish(int64_t n3, const double* __restrict__ acc, double inv_n, double gamma,
+                             uint8_t* __restrict__ rgb) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n3;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double x = 255.0 * ktm_pow(dclamp(acc[i] * inv_n, 0.0, 1.0), 1.0 / gamma);
+    const double t = trunc(x);
+    rgb[i] = (uint8_t)(int)((x - t >= 0.5) ? t + 1.0 : t);
+  }
+}
+
+static int elementwise_grid(int64_t n, int block) {
+  int64_t grid = (n + block - 1) / block;
+  if (grid > 148 * 32) grid = 148 * 32;
+  return (int)grid;
+}
+
+cudaError_t launch_spp_accumulate(int64_t n3, const uint8_t* rgb, double* acc, double gamma, int first,
+                                  cudaStream_t stream) {
+  if (n3 <= 0) return cudaSuccess;
+  k_spp_accumulate<<<elementwise_grid(n3, 256), 256, 0, stream>>>(n3, rgb, acc, gamma, first);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_spp_finish(int64_t n3, const double* acc, double inv_n, double gamma, uint8_t* rgb,
+                              cudaStream_t stream) {
+  if (n3 <= 0) return cudaSuccess;
+  k_spp_finish<<<elementwise_grid(n3, 256), 256, 0, stream>>>(n3, acc, inv_n, gamma, rgb);
   return cudaGetLastError();
 }
 

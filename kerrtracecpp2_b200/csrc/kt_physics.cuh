@@ -934,6 +934,9 @@ struct ColourConst {
   double M, r_isco, exposure, gamma, temp_scale;
   double log10_50;  // log10(4e4/800.0), a per-frame constant
   double pt_peak;   // page_thorne(3 r_isco, r_isco)
+  // interstellar palette (ColorParams, main.cpp:72-81) and the disk edges
+  int palette, rings, sectors, pad0;
+  double sigma, hue_offset, r_in, r_out;
 };
 
 KT_HD void disk_colour(const ColourConst& cc, double r, double red, double magnif, uint8_t out[3]) {
@@ -948,6 +951,99 @@ KT_HD void disk_colour(const ColourConst& cc, double r, double red, double magni
   blackbody(T, cc.log10_50, c);
 #pragma unroll
   for (int k = 0; k < 3; ++k) out[k] = to_u8(tonemap((c[k] / 255.0) * I, cc.exposure, cc.gamma) * 255);
+}
+
+// hsv_to_rgb (main.cpp:1689-1707).
+KT_HD void hsv_to_rgb(double h, double s, double v, double out[3]) {
+  h = h - floor(h);
+  const double hh = h * 6.0;
+  const int hi = (int)hh;
+  const double f = hh - (double)hi;
+  const double p = v * (1.0 - s);
+  const double q = v * (1.0 - s * f);
+  const double t = v * (1.0 - s * (1.0 - f));
+  double rr, gg, bb;
+  switch (hi % 6) {
+    case 0: rr = v; gg = t; bb = p; break;
+    case 1: rr = q; gg = v; bb = p; break;
+    case 2: rr = p; gg = v; bb = t; break;
+    case 3: rr = p; gg = q; bb = v; break;
+    case 4: rr = t; gg = p; bb = v; break;
+    default: rr = v; gg = p; bb = q; break;
+  }
+  // the reference returns uint8 (x*255 + 0.5 truncated) and blends those
+  out[0] = (double)to_u8(rr * 255.0 + 0.5);
+  out[1] = (double)to_u8(gg * 255.0 + 0.5);
+  out[2] = (double)to_u8(bb * 255.0 + 0.5);
+}
+
+// cell_hash (main.cpp:1710-1713): fractional part of a scrambled sine.
+KT_HD double cell_hash(int cell_id, double salt_a, double salt_b) {
+  const double v = ktm_sin((double)cell_id * salt_a + salt_b) * 43758.5453;
+  return v - floor(v);
+}
+
+// disk_colour_interstellar (main.cpp:1719-1797): rings x sectors of hashed
+// warm colours, Gaussian-blended across cell edges (about 30% of the cells
+// are gaps), then the blackbody path's physical intensity.  fmod(x, 1.0) of
+// the hue is x - trunc(x), which is exact.
+KT_HD void disk_colour_interstellar(const ColourConst& cc, double r, double phi, double red,
+                                    double magnif, uint8_t out[3]) {
+  const int NR = cc.rings > 0 ? cc.rings : 1;
+  const int NS = cc.sectors > 0 ? cc.sectors : 1;
+  const double sigma = cc.sigma > 0 ? cc.sigma : 0.5;
+  const double two_pi = 2.0 * 3.14159265358979323846;
+  const double r_norm = dclamp((r - cc.r_in) / (cc.r_out - cc.r_in), 0.0, 1.0);
+  const double phi_norm = (phi - floor(phi / two_pi) * two_pi) / two_pi;
+  const double ring_pos = r_norm * (double)NR;
+  const double sec_pos = phi_norm * (double)NS;
+  double acc_r = 0.0, acc_g = 0.0, acc_b = 0.0, w_total = 0.0;
+  const double inv2sig2 = 1.0 / ((2.0 * sigma) * sigma);
+  const int SEARCH = (int)ceil(3.0 * sigma) + 1;
+  KT_ROLLED
+  for (int ri = -SEARCH; ri <= NR + SEARCH; ++ri) {
+    const double dr = ring_pos - (double)ri;
+    if ((dr * dr) * inv2sig2 > 16.0) continue;
+    const int ri_clamped = ri < 0 ? 0 : ri >= NR ? NR - 1 : ri;
+    KT_ROLLED
+    for (int si_raw = -SEARCH; si_raw <= NS + SEARCH; ++si_raw) {
+      double ds = sec_pos - (double)si_raw;
+      ds = ds - floor((ds + (double)NS * 0.5) / (double)NS) * (double)NS;
+      const double dist2 = dr * dr + ds * ds;
+      const double w = ktm_exp(-dist2 * inv2sig2);
+      if (w < 1e-4) continue;
+      const int si_clamped = ((si_raw % NS) + NS) % NS;
+      const int cell_id = ri_clamped * NS + si_clamped;
+      const double h1 = cell_hash(cell_id, 127.1, 311.7);
+      const double h2 = cell_hash(cell_id, 269.5, 183.3);
+      const double h3 = cell_hash(cell_id, 419.2, 371.9);
+      if (h3 < 0.30) continue;
+      const double hx = h1 * 0.14 + cc.hue_offset;
+      const double hue = hx - trunc(hx);
+      const double sat = 0.70 + h2 * 0.30;
+      const double val = 0.50 + h1 * 0.50;
+      double c[3];
+      hsv_to_rgb(hue, sat, val, c);
+      acc_r += w * c[0];
+      acc_g += w * c[1];
+      acc_b += w * c[2];
+      w_total += w;
+    }
+  }
+  if (w_total < 1e-6) {
+    out[0] = out[1] = out[2] = 0;
+    return;
+  }
+  const double pt_norm = page_thorne(r, cc.r_isco);
+  double I = (cc.pt_peak > 0.0) ? pt_norm / cc.pt_peak : 0.0;
+  const double red_c = dclamp(red, 0.1, 10.0);
+  const double lift = 1.0 + 0.85 * dclamp(1.0 - red_c, 0.0, 1.0);
+  I *= ktm_pow(red_c, 4.0) * lift;
+  I *= dclamp(1.0 / magnif, 0.05, 5.0);
+  const double norm = w_total * 255.0;
+  out[0] = to_u8(tonemap(acc_r / norm * I, cc.exposure, cc.gamma) * 255);
+  out[1] = to_u8(tonemap(acc_g / norm * I, cc.exposure, cc.gamma) * 255);
+  out[2] = to_u8(tonemap(acc_b / norm * I, cc.exposure, cc.gamma) * 255);
 }
 
 KT_HD int iclamp(int v, int lo, int hi) { return v < lo ? lo : v > hi ? hi : v; }

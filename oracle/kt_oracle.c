@@ -1382,6 +1382,96 @@ static void disk_colour(double r, double red, double magnif, double M, double r_
   for (int k = 0; k < 3; ++k) out[k] = to_u8(tonemap((c[k] / 255.0) * I, exposure, gamma) * 255);
 }
 
+/* hsv_to_rgb (main.cpp:1689-1707); the uint8 channels as doubles. */
+static void hsv_to_rgb(double h, double s, double v, double out[3]) {
+  h = h - floor(h);
+  const double hh = h * 6.0;
+  const int hi = (int)hh;
+  const double f = hh - (double)hi;
+  const double p = v * (1.0 - s);
+  const double q = v * (1.0 - s * f);
+  const double t = v * (1.0 - s * (1.0 - f));
+  double rr, gg, bb;
+  switch (hi % 6) {
+    case 0: rr = v; gg = t; bb = p; break;
+    case 1: rr = q; gg = v; bb = p; break;
+    case 2: rr = p; gg = v; bb = t; break;
+    case 3: rr = p; gg = q; bb = v; break;
+    case 4: rr = t; gg = p; bb = v; break;
+    default: rr = v; gg = p; bb = q; break;
+  }
+  out[0] = (double)to_u8(rr * 255 + 0.5);
+  out[1] = (double)to_u8(gg * 255 + 0.5);
+  out[2] = (double)to_u8(bb * 255 + 0.5);
+}
+
+/* cell_hash (main.cpp:1710-1713) */
+static double cell_hash(int cell_id, double a, double b) {
+  const double v = ktm_sin((double)cell_id * a + b) * 43758.5453;
+  return v - floor(v);
+}
+
+/* disk_colour_interstellar (main.cpp:1719-1797); fmod(x, 1.0) is exact and
+ * equals x - trunc(x). */
+static void disk_colour_interstellar(double r, double phi, double red, double magnif, double r_in,
+                                     double r_out, double r_isco, const kt_color_params* cp,
+                                     uint8_t out[3]) {
+  const int NR = cp->disk_rings > 0 ? cp->disk_rings : 1;
+  const int NS = cp->disk_sectors > 0 ? cp->disk_sectors : 1;
+  const double sigma = cp->disk_sigma > 0 ? cp->disk_sigma : 0.5;
+  const double r_norm = oclamp((r - r_in) / (r_out - r_in), 0.0, 1.0);
+  const double phi_norm = (phi - floor(phi / (2.0 * ORC_PI)) * (2.0 * ORC_PI)) / (2.0 * ORC_PI);
+  const double ring_pos = r_norm * NR;
+  const double sec_pos = phi_norm * NS;
+  double acc_r = 0.0, acc_g = 0.0, acc_b = 0.0, w_total = 0.0;
+  const double inv2sig2 = 1.0 / (2.0 * sigma * sigma);
+  const int SEARCH = (int)ceil(3.0 * sigma) + 1;
+  for (int ri = -SEARCH; ri <= NR + SEARCH; ++ri) {
+    const double dr = ring_pos - (double)ri;
+    if (dr * dr * inv2sig2 > 16.0) continue;
+    const int ri_clamped = ri < 0 ? 0 : ri >= NR ? NR - 1 : ri;
+    for (int si_raw = -SEARCH; si_raw <= NS + SEARCH; ++si_raw) {
+      double ds = sec_pos - (double)si_raw;
+      ds = ds - floor((ds + NS * 0.5) / NS) * NS;
+      const double dist2 = dr * dr + ds * ds;
+      const double w = ktm_exp(-dist2 * inv2sig2);
+      if (w < 1e-4) continue;
+      const int si_clamped = ((si_raw % NS) + NS) % NS;
+      const int cell_id = ri_clamped * NS + si_clamped;
+      const double h1 = cell_hash(cell_id, 127.1, 311.7);
+      const double h2 = cell_hash(cell_id, 269.5, 183.3);
+      const double h3 = cell_hash(cell_id, 419.2, 371.9);
+      if (h3 < 0.30) continue;
+      const double hx = h1 * 0.14 + cp->disk_hue_offset;
+      const double hue = hx - trunc(hx);
+      const double sat = 0.70 + h2 * 0.30;
+      const double val = 0.50 + h1 * 0.50;
+      double c[3];
+      hsv_to_rgb(hue, sat, val, c);
+      acc_r += w * c[0];
+      acc_g += w * c[1];
+      acc_b += w * c[2];
+      w_total += w;
+    }
+  }
+  if (w_total < 1e-6) {
+    out[0] = out[1] = out[2] = 0;
+    return;
+  }
+  const double pt_norm = page_thorne(r, r_isco);
+  const double r_peak = 3.0 * r_isco;
+  const double pt_peak = page_thorne(r_peak, r_isco);
+  double I = (pt_peak > 0.0) ? pt_norm / pt_peak : 0.0;
+  const double red_c = oclamp(red, 0.1, 10.0);
+  const double lift = 1.0 + 0.85 * oclamp(1.0 - red_c, 0.0, 1.0);
+  I *= ktm_pow(red_c, 4.0) * lift;
+  I *= oclamp(1.0 / magnif, 0.05, 5.0);
+  const double norm = w_total * 255.0;
+  out[0] = to_u8(tonemap(acc_r / norm * I, cp->exposure, cp->gamma) * 255);
+  out[1] = to_u8(tonemap(acc_g / norm * I, cp->exposure, cp->gamma) * 255);
+  out[2] = to_u8(tonemap(acc_b / norm * I, cp->exposure, cp->gamma) * 255);
+}
+
 static int iclamp(int v, int lo, int hi) { return v < lo ? lo : v > hi ? hi : v; }
 
 static void bg_sample(const uint8_t* px, int w, int h, double theta, double phi, uint8_t out[3]) {
@@ -1421,6 +1511,81 @@ void orc_colorize(const kt_frame_desc* d, int64_t n, const uint8_t* outcome, con
     rgb[3 * i + 0] = c[0];
     rgb[3 * i + 1] = c[1];
     rgb[3 * i + 2] = c[2];
+  }
+}
+
+void orc_colorize_cp(const kt_frame_desc* d, int64_t n, const uint8_t* outcome, const double* r,
+                     const double* redshift, const double* magnif, const double* phi_disk,
+                     const double* theta_esc, const double* phi_esc, const kt_color_params* cp,
+                     const uint8_t* bg, int bg_w, int bg_h, uint8_t* rgb) {
+  Frame f;
+  setup_frame(d, &f);
+  for (int64_t i = 0; i < n; ++i) {
+    uint8_t c[3] = {0, 0, 0};
+    if (outcome[i] == KT_OUT_DISK && cp->palette == 1) {
+      disk_colour_interstellar((double)(float)r[i], (double)(float)phi_disk[i],
+                               (double)(float)redshift[i], (double)(float)magnif[i], f.r_in,
+                               d->disk_out, f.r_in, cp, c);
+    } else if (outcome[i] == KT_OUT_DISK) {
+      disk_colour((double)(float)r[i], (double)(float)redshift[i], (double)(float)magnif[i], d->M,
+                  f.r_in, cp->exposure, cp->gamma, cp->temp_scale, c);
+    } else if (outcome[i] == KT_OUT_ESCAPED && bg && bg_w > 0 && bg_h > 0) {
+      bg_sample(bg, bg_w, bg_h, (double)(float)theta_esc[i], (double)(float)phi_esc[i], c);
+    }
+    rgb[3 * i + 0] = c[0];
+    rgb[3 * i + 1] = c[1];
+    rgb[3 * i + 2] = c[2];
+  }
+}
+
+/* --camera-spp (main.cpp:2232-2322): the jitter offsets, and the average
+ * of the passes' images in linear light. */
+void orc_spp_offsets(int spp, double* xy) {
+  int k = 0;
+  if (spp <= 1) {
+    xy[0] = xy[1] = 0.0;
+    return;
+  }
+  if (spp == 2) {
+    xy[0] = -0.35; xy[1] = 0.0; xy[2] = 0.35; xy[3] = 0.0;
+    return;
+  }
+  if ((spp % 2) == 1) {
+    xy[0] = xy[1] = 0.0;
+    k = 1;
+  }
+  static const double seed[7][2] = {{0.35, 0.00}, {0.00, 0.35}, {0.25, 0.25}, {0.45, 0.20},
+                                    {0.20, 0.45}, {0.40, 0.00}, {0.00, 0.40}};
+  for (int j = 0; j < 7; ++j) {
+    if (k + 2 > spp) break;
+    xy[2 * k] = seed[j][0]; xy[2 * k + 1] = seed[j][1]; ++k;
+    xy[2 * k] = -seed[j][0]; xy[2 * k + 1] = -seed[j][1]; ++k;
+  }
+  const double golden = 2.39996322972865332;
+  for (int m = 0; k < spp; ++m) {
+    const double rr = 0.49 * sqrt((double)(m + 1) / (double)(spp + 1));
+    const double a = golden * (double)(m + 1);
+    const double x = rr * ktm_cos(a), y = rr * ktm_sin(a);
+    xy[2 * k] = x; xy[2 * k + 1] = y; ++k;
+    if (k < spp) {
+      xy[2 * k] = -x; xy[2 * k + 1] = -y; ++k;
+    }
+  }
+}
+
+static double spp_lround(double x) { /* std::lround for x >= 0 */
+  const double t = trunc(x);
+  return (x - t >= 0.5) ? t + 1.0 : t;
+}
+
+void orc_spp_combine(int64_t n, int spp, const uint8_t* passes, double gamma, uint8_t* rgb) {
+  const double g = gamma < 1e-6 ? 1e-6 : gamma;
+  const double inv_n = 1.0 / (double)spp;
+  for (int64_t i = 0; i < 3 * n; ++i) {
+    double acc = 0.0;
+    for (int s = 0; s < spp; ++s) acc += ktm_pow(oclamp((double)passes[(int64_t)s * 3 * n + i] / 255.0, 0.0, 1.0), g);
+    const double disp = ktm_pow(oclamp(acc * inv_n, 0.0, 1.0), 1.0 / g);
+    rgb[i] = (uint8_t)(int64_t)spp_lround(255.0 * disp);
   }
 }
 

@@ -39,6 +39,18 @@ void orc_colorize(const kt_frame_desc* d, int64_t n, const uint8_t* outcome, con
                   const double* phi_esc, double exposure, double gamma, double temp_scale,
                   const uint8_t* bg, int bg_w, int bg_h, uint8_t* rgb);
 
+/* colorize_buffer with every ColorParams field (blackbody or interstellar
+ * palette, main.cpp:1719-1866); disk edges r_isco and disk_out. */
+void orc_colorize_cp(const kt_frame_desc* d, int64_t n, const uint8_t* outcome, const double* r,
+                     const double* redshift, const double* magnif, const double* phi_disk,
+                     const double* theta_esc, const double* phi_esc, const kt_color_params* cp,
+                     const uint8_t* bg, int bg_w, int bg_h, uint8_t* rgb);
+
+/* --camera-spp: jitter offsets (2*spp doubles) and the linear-light average
+ * of spp RGB8 passes (spp*n*3 bytes, pass after pass). */
+void orc_spp_offsets(int spp, double* xy);
+void orc_spp_combine(int64_t n, int spp, const uint8_t* passes, double gamma, uint8_t* rgb);
+
 /* Known-answer helpers (tests/core_tests.cpp of the reference). */
 void orc_metric_bl(double M, double a, double Q, double L, double r, double th, double* cov16,
                    double* con16);

@@ -167,6 +167,65 @@ void ref_colorize(const void* geopixels, int W, int H, double exposure, double g
   std::memcpy(rgb, out.data(), out.size() * 3);
 }
 
+static ColorParams to_cp(const kt_color_params* c) {
+  ColorParams cp;
+  cp.exposure = c->exposure;
+  cp.gamma = c->gamma;
+  cp.temp_scale = c->temp_scale;
+  cp.palette = c->palette == 1 ? DiskPalette::INTERSTELLAR : DiskPalette::BLACKBODY;
+  cp.disk_rings = c->disk_rings;
+  cp.disk_sectors = c->disk_sectors;
+  cp.disk_sigma = c->disk_sigma;
+  cp.disk_hue_offset = c->disk_hue_offset;
+  return cp;
+}
+
+static BackgroundImage to_bg(const uint8_t* bg, int bg_w, int bg_h) {
+  BackgroundImage img;
+  if (bg && bg_w > 0 && bg_h > 0) {
+    img.w = bg_w;
+    img.h = bg_h;
+    img.px.assign(bg, bg + (size_t)bg_w * bg_h * 3);
+  }
+  return img;
+}
+
+// colorize_buffer with every ColorParams field (both palettes).
+void ref_colorize_cp(const void* geopixels, int W, int H, const kt_color_params* c,
+                     const uint8_t* bg, int bg_w, int bg_h, double M_bh, double r_isco,
+                     double r_disk_in, double r_disk_out, uint8_t* rgb) {
+  std::vector<GeoPixel> geo((size_t)W * H);
+  std::memcpy(geo.data(), geopixels, geo.size() * sizeof(GeoPixel));
+  auto out = colorize_buffer(geo, W, H, to_cp(c), to_bg(bg, bg_w, bg_h), M_bh, r_isco, r_disk_in,
+                             r_disk_out);
+  std::memcpy(rgb, out.data(), out.size() * 3);
+}
+
+// render_image (main.cpp:2209-2478, CPU branch) with camera_spp passes.
+void ref_render_image(const kt_frame_desc* d, const kt_color_params* c, const uint8_t* bg, int bg_w,
+                      int bg_h, int camera_spp, int nthreads, uint8_t* rgb) {
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+  FrameParams fp;
+  fp.a = d->a;
+  fp.theta = d->theta_deg;
+  fp.phi = d->phi_deg;
+  fp.r_obs = d->r_obs;
+  fp.disk_out = d->disk_out;
+  fp.fov = d->fov_deg;
+  IntegratorControls ctl;
+  ctl.max_steps = std::max(1, (int)d->max_steps);
+  ctl.step_init = std::max(1e-10, d->step_init);
+  ctl.tol = std::max(1e-10, d->tol);
+  auto out = render_image(d->width, d->height, fp, to_bg(bg, bg_w, bg_h), d->bundles != 0,
+                          RaySolverMode::STANDARD,
+                          d->chart == KT_CHART_KS ? CoordinateChart::KS : CoordinateChart::BL,
+                          d->integrator == KT_DOPRI5 ? Integrator::DOPRI5 : Integrator::RK4_DOUBLING,
+                          ctl, camera_spp, d->M, d->Q, d->Lambda, IntersectionMode::HERMITE, 0, false,
+                          false, false, to_cp(c), nullptr, false, d->pixel_offset_x,
+                          d->pixel_offset_y);
+  std::memcpy(rgb, out.data(), out.size() * 3);
+}
+
 // Per-frame scalars as the reference computes them.
 double ref_r_horizon(double M, double a, double Q, double L) { return KNdSMetric(M, a, Q, L).r_horizon(); }
 double ref_r_isco(double M, double a, double Q, double L) { return KNdSMetric(M, a, Q, L).r_isco(); }

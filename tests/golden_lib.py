@@ -41,3 +41,20 @@ def mismatches(got, want, fields=FIELDS):
     """Per-field count of entries whose bits differ."""
     return {k: int(np.sum(bits(np.asarray(got[k], dtype=want[k].dtype)) != bits(want[k])))
             for k in fields}
+
+
+COLOUR_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "colour.npz")
+_zc = None
+
+
+def colour():
+    """tests/golden/colour.npz (make_colour_golden.py): interstellar palette
+    images and camera_spp renders from the reference."""
+    global _zc
+    if _zc is None:
+        _zc = dict(np.load(COLOUR_PATH))
+    return _zc
+
+
+def colour_meta():
+    return json.loads(bytes(colour()["meta_json"]).decode())

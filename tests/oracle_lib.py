@@ -15,7 +15,7 @@ import os
 
 import numpy as np
 
-from kerrtracecpp2_b200.abi import FrameDerived, FrameDesc
+from kerrtracecpp2_b200.abi import ColorParams, FrameDerived, FrameDesc
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 PORT_PATH = os.path.join(ROOT, "oracle", "_build", "liboracle_port.so")
@@ -44,6 +44,13 @@ def port():
         L.orc_frame_derive.argtypes = [ctypes.POINTER(FrameDesc), ctypes.POINTER(FrameDerived)]
         L.orc_colorize.argtypes = [ctypes.POINTER(FrameDesc), ctypes.c_int64] + [_P] * 6 + [_D] * 3 + [_P, ctypes.c_int, ctypes.c_int, _P]
         L.orc_colorize.restype = None
+        PC = ctypes.POINTER(ColorParams)
+        L.orc_colorize_cp.argtypes = [ctypes.POINTER(FrameDesc), ctypes.c_int64] + [_P] * 7 + [PC, _P, ctypes.c_int, ctypes.c_int, _P]
+        L.orc_colorize_cp.restype = None
+        L.orc_spp_offsets.argtypes = [ctypes.c_int, _P]
+        L.orc_spp_offsets.restype = None
+        L.orc_spp_combine.argtypes = [ctypes.c_int64, ctypes.c_int, _P, _D, _P]
+        L.orc_spp_combine.restype = None
         for f in ("orc_r_horizon", "orc_r_isco"):
             getattr(L, f).argtypes = [_D] * 4
             getattr(L, f).restype = _D
@@ -67,6 +74,11 @@ def ref(flavour="strict"):
         L.ref_trace_geodesics.argtypes = [ctypes.POINTER(FrameDesc), _P, ctypes.c_int]
         L.ref_colorize.argtypes = [_P, ctypes.c_int, ctypes.c_int, _D, _D, _D, _P, ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, _P]
         L.ref_colorize.restype = None
+        PC = ctypes.POINTER(ColorParams)
+        L.ref_colorize_cp.argtypes = [_P, ctypes.c_int, ctypes.c_int, PC, _P, ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, _P]
+        L.ref_colorize_cp.restype = None
+        L.ref_render_image.argtypes = [ctypes.POINTER(FrameDesc), PC, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P]
+        L.ref_render_image.restype = None
         for f in ("ref_r_horizon", "ref_r_isco"):
             getattr(L, f).argtypes = [_D] * 4
             getattr(L, f).restype = _D
@@ -156,6 +168,54 @@ def colorize_ref(desc, geopixels, r_isco, bg=None, exposure=1.0, gamma=2.2, temp
     bgc = np.ascontiguousarray(bg) if bg is not None else None
     ref(flavour).ref_colorize(_ptr(geopixels), desc.width, desc.height, exposure, gamma, temp_scale,
                               _ptr(bgc), bw, bh, desc.M, r_isco, r_isco, desc.disk_out, _ptr(rgb))
+    return rgb
+
+
+def colorize_port_cp(desc, geo, cp, bg=None):
+    """orc_colorize_cp: both palettes (cp a kt_color_params)."""
+    n = len(geo["outcome"])
+    rgb = np.zeros((n, 3), np.uint8)
+    bw, bh = (bg.shape[1], bg.shape[0]) if bg is not None else (0, 0)
+    bgc = np.ascontiguousarray(bg) if bg is not None else None
+    port().orc_colorize_cp(ctypes.byref(desc), n, *[_ptr(np.ascontiguousarray(geo[k])) for k in
+                           ("outcome", "r", "redshift", "magnif", "phi_disk", "theta_esc", "phi_esc")],
+                           ctypes.byref(cp), _ptr(bgc), bw, bh, _ptr(rgb))
+    return rgb
+
+
+def colorize_ref_cp(desc, geopixels, r_isco, cp, bg=None, flavour="strict"):
+    """The reference's colorize_buffer with every ColorParams field."""
+    n = desc.width * desc.height
+    rgb = np.zeros((n, 3), np.uint8)
+    bw, bh = (bg.shape[1], bg.shape[0]) if bg is not None else (0, 0)
+    bgc = np.ascontiguousarray(bg) if bg is not None else None
+    ref(flavour).ref_colorize_cp(_ptr(geopixels), desc.width, desc.height, ctypes.byref(cp), _ptr(bgc),
+                                 bw, bh, desc.M, r_isco, r_isco, desc.disk_out, _ptr(rgb))
+    return rgb
+
+
+def render_ref(desc, cp, spp, bg=None, flavour="strict", nthreads=0):
+    """The reference's render_image (CPU branch) with camera_spp passes."""
+    n = desc.width * desc.height
+    rgb = np.zeros((n, 3), np.uint8)
+    bw, bh = (bg.shape[1], bg.shape[0]) if bg is not None else (0, 0)
+    bgc = np.ascontiguousarray(bg) if bg is not None else None
+    ref(flavour).ref_render_image(ctypes.byref(desc), ctypes.byref(cp), _ptr(bgc), bw, bh, spp,
+                                  nthreads, _ptr(rgb))
+    return rgb
+
+
+def spp_offsets_port(spp):
+    xy = np.zeros(2 * max(spp, 1))
+    port().orc_spp_offsets(spp, _ptr(xy))
+    return xy.reshape(-1, 2)
+
+
+def spp_combine_port(passes, gamma):
+    """passes: (spp, n, 3) uint8 -> (n, 3) uint8, the reference's average."""
+    spp, n = passes.shape[0], passes.shape[1]
+    rgb = np.zeros((n, 3), np.uint8)
+    port().orc_spp_combine(n, spp, _ptr(np.ascontiguousarray(passes)), gamma, _ptr(rgb))
     return rgb
 
 
