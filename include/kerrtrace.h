@@ -57,7 +57,11 @@ typedef enum kt_status {
 enum { KT_CHART_KS = 0, KT_CHART_BL = 1 };
 /* Integrator (Integrator, geodesic.hpp:417). */
 enum { KT_RK4_DOUBLING = 0, KT_DOPRI5 = 1 };
-/* Ray solver (RaySolverMode, main.cpp:176); only STANDARD runs here. */
+/* Ray solver (RaySolverMode, main.cpp:176).  STANDARD and SEMI_ANALYTIC
+ * (the separable Kerr tracer, main.cpp:436-703; FP64 precision) run here;
+ * ELLIPTIC_CLOSED returns KT_ERR_UNSUPPORTED.  A solver the frame cannot use
+ * falls back to STANDARD as in the reference: bundles; SEMI_ANALYTIC in the
+ * KS chart; either with Q or Lambda != 0. */
 enum { KT_SOLVER_STANDARD = 0, KT_SOLVER_SEMI_ANALYTIC = 1, KT_SOLVER_ELLIPTIC_CLOSED = 2 };
 /* Arithmetic of the trace.  FP64: the reference's arithmetic bit for bit.
  * MIXED: analytic Hamiltonian gradient, FP32 right-hand side in the far
@@ -106,7 +110,7 @@ typedef struct kt_frame_derived {
   double r_obs, theta_obs, phi_obs, fov_h; /* radians */
   double dlam0;       /* max(step_init, 1e-10) */
   int32_t max_steps;  /* max(1, max_steps) */
-  int32_t reserved0;
+  int32_t solver;     /* effective solver (select_solver_mode, main.cpp:235-276) */
   double tol;
   double bundle_eps;  /* fov_h / width * 0.5 (ray_bundle.hpp:282) */
   double r_fp32;      /* KT_PREC_MIXED: FP32 right-hand side beyond this

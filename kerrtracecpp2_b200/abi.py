@@ -64,7 +64,7 @@ class FrameDerived(ctypes.Structure):
         ("r_escape", ctypes.c_double),
         ("r_obs", ctypes.c_double), ("theta_obs", ctypes.c_double), ("phi_obs", ctypes.c_double),
         ("fov_h", ctypes.c_double),
-        ("dlam0", ctypes.c_double), ("max_steps", ctypes.c_int32), ("reserved0", ctypes.c_int32),
+        ("dlam0", ctypes.c_double), ("max_steps", ctypes.c_int32), ("solver", ctypes.c_int32),
         ("tol", ctypes.c_double), ("bundle_eps", ctypes.c_double), ("r_fp32", ctypes.c_double),
     ]
 

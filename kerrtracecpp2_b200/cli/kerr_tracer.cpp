@@ -303,10 +303,16 @@ int main(int argc, char** argv) {
   if (st != KT_OK) return die("invalid frame", ctx, st);
   printf("KNdS  M=%g a=%g Q=%g Lambda=%g\n  r+=%.10g  r_ISCO=%.10g\n", d.M, d.a, d.Q, d.Lambda,
          dv.r_horizon, dv.r_isco);
-  printf("Mode: %s  chart=%s  %s  standard  backend=gpu-b200  tol=%g  max-steps=%d  %dx%d\n",
+  static const char* const kSolverName[] = {"standard", "semi-analytic", "elliptic-closed"};
+  if (dv.solver != d.solver_mode)  // select_solver_mode's fallback (main.cpp:2051-2060)
+    fprintf(stderr, "Info: requested solver '%s' not available here; using standard integrator.\n",
+            kSolverName[d.solver_mode]);
+  printf("Mode: %s  chart=%s  %s  %s  backend=gpu-b200  tol=%g  max-steps=%d  %dx%d\n",
          d.bundles ? "ray bundles" : "single ray", dv.chart == KT_CHART_KS ? "KS" : "BL",
-         dv.integrator == KT_DOPRI5 ? "DOPRI5" : "RK4-doubling", d.tol, d.max_steps, d.width,
-         d.height);
+         dv.solver == KT_SOLVER_SEMI_ANALYTIC ? "RK4-doubling"
+         : dv.integrator == KT_DOPRI5         ? "DOPRI5"
+                                              : "RK4-doubling",
+         kSolverName[dv.solver], d.tol, d.max_steps, d.width, d.height);
   const size_t n = (size_t)d.width * d.height;
   const std::string spp_tag = camera_spp > 1 ? "_spp" + std::to_string(camera_spp) : "";
   const std::string tag = std::string(d.bundles ? "bundles" : "trace") + "_" +

@@ -50,14 +50,14 @@ kt_status run_trace(kt_context* ctx, const kt::Frame& f, const kt::OutSoA& out,
   if (r != KT_OK) return r;
   KT_CUDA(ctx, cudaMemsetAsync(ctx->d_counters, 0, 4 * sizeof(uint32_t), st), "reset queue");
   kt::Fallback fb = {nullptr, nullptr, ctx->d_counters + 2};
-  if (kt::is_ks_mode(m)) {
+  if (kt::has_fallback(m)) {
     r = ensure(ctx, (void**)&ctx->d_fb, &ctx->fb_cap, 2 * n_max * sizeof(uint32_t), "fallback list");
     if (r != KT_OK) return r;
     fb.pix = ctx->d_fb;
     fb.slot = ctx->d_fb + n_max;
   }
   KT_CUDA(ctx, kt::launch_trace(m, f, out, rl, ctx->d_counters, fb, s, st), "trace kernel launch");
-  if (kt::is_ks_mode(m)) {
+  if (kt::has_fallback(m)) {
     const kt::Mode bm = kt::fallback_mode(f);
     kt::LaunchShape bs;
     r = shape(ctx, bm, &bs);

@@ -4,11 +4,12 @@
 //
 // Device memory of a batch (one allocation, 256-byte aligned sections):
 //   per group: Frame[n_g], OutSoA[n_g], uint64 offsets[n_g + 1], and for the
-//   KS groups the fallback list uint32[n_rays_g]; then 4 uint32 counters per
+//   KS and separable-Kerr groups the fallback list uint32[n_rays_g]; then 4 uint32 counters per
 //   group ([0] ray queue, [1] fallback queue, [2] fallback count).
 // The graph: memset(counters) -> one branch per group, each branch the
 // group's persistent launch (KS groups: then the BL launch over the rays
-// whose KS initialisation failed, main.cpp:1537-1538) -> join.
+// whose KS initialisation failed, main.cpp:1537-1538; separable-Kerr
+// groups: the BL RK4 launch over the rays that gave up) -> join.
 #include <cuda_runtime.h>
 #include <string.h>
 
@@ -33,12 +34,13 @@ static_assert(KT_BATCH_VARIANTS == kt::kBatchVariants, "variant count of the ABI
 
 struct Group {
   kt::Mode mode;
+  kt::Mode fb_mode = kt::kModeBLRk4;  // BL launch over the fallback list
   std::vector<int> frames;  // batch frame indices
   uint64_t n_rays = 0;
   kt::Frame* d_frames = nullptr;
   kt::OutSoA* d_outs = nullptr;
   uint64_t* d_offsets = nullptr;
-  uint32_t* d_fb = nullptr;      // KS groups only
+  uint32_t* d_fb = nullptr;      // groups with a fallback pass only
   uint32_t* d_counters = nullptr;
   int variant = 0;
   int refill_min = 1;
@@ -84,16 +86,15 @@ kt::BatchRays group_rays(const Group& g, const uint32_t* list, const uint32_t* n
 }
 
 // Enqueue one group's trace: the persistent launch over `list` (or all its
-// rays) and, for KS groups, the BL launch over the fallback list.  The
+// rays) and, for groups with a fallback pass, the BL launch over the fallback list.  The
 // group's counters must be zero.
 cudaError_t enqueue_group(const Group& g, int variant, const kt::LaunchShape& s, int refill_min,
                           const uint32_t* list, uint64_t n, cudaStream_t st) {
   kt::Fallback fb = {g.d_fb, nullptr, g.d_counters + 2};
   cudaError_t e = kt::launch_batch(g.mode, variant, group_rays(g, list, nullptr, n, refill_min),
                                    g.d_counters, fb, s, st);
-  if (e != cudaSuccess || !kt::is_ks_mode(g.mode)) return e;
-  const kt::Mode bm = g.mode == kt::kModeKSRk4Mixed ? kt::kModeBLRk4Mixed : kt::kModeBLRk4;
-  return kt::launch_batch(bm, g.fb_variant, group_rays(g, g.d_fb, g.d_counters + 2, 0, 1),
+  if (e != cudaSuccess || !kt::has_fallback(g.mode)) return e;
+  return kt::launch_batch(g.fb_mode, g.fb_variant, group_rays(g, g.d_fb, g.d_counters + 2, 0, 1),
                           g.d_counters + 1, fb, g.fb_shape, st);
 }
 
@@ -252,7 +253,9 @@ kt_status kt_batch_create(kt_context* ctx, const kt_frame_desc* descs, const kt_
     return fail(ctx, KT_ERR_INVALID_ARGUMENT, "kt_batch_create: bad options");
   // Frames -> groups by kernel mode.
   std::vector<kt::Frame> frames((size_t)n_frames);
-  std::vector<int> group_of_mode(kt::kNumModes, -1);
+  // key: kernel mode x mode of its fallback pass (a KS frame's BL pass
+  // integrates with the frame's integrator, main.cpp:1537-1538)
+  std::vector<int> group_of_key(kt::kNumModes * kt::kNumModes, -1);
   kt_batch* b = new (std::nothrow) kt_batch();
   if (!b) return fail(ctx, KT_ERR_OUT_OF_MEMORY, "kt_batch_create: host allocation");
   b->ctx = ctx;
@@ -275,12 +278,15 @@ kt_status kt_batch_create(kt_context* ctx, const kt_frame_desc* descs, const kt_
       return fail(ctx, KT_ERR_INVALID_ARGUMENT,
                   "frame " + std::to_string(i) + ": output pointer is NULL");
     const kt::Mode m = kt::frame_mode(frames[i]);
-    if (group_of_mode[m] < 0) {
-      group_of_mode[m] = (int)b->groups.size();
+    const kt::Mode fm = kt::has_fallback(m) ? kt::fallback_mode(frames[i]) : kt::kModeBLRk4;
+    const int key = m * kt::kNumModes + fm;
+    if (group_of_key[key] < 0) {
+      group_of_key[key] = (int)b->groups.size();
       b->groups.emplace_back();
       b->groups.back().mode = m;
+      b->groups.back().fb_mode = fm;
     }
-    Group& g = b->groups[group_of_mode[m]];
+    Group& g = b->groups[group_of_key[key]];
     g.frames.push_back(i);
     g.n_rays += (uint64_t)descs[i].width * (uint64_t)descs[i].height;
     b->n_rays += (uint64_t)descs[i].width * (uint64_t)descs[i].height;
@@ -301,7 +307,7 @@ kt_status kt_batch_create(kt_context* ctx, const kt_frame_desc* descs, const kt_
     off_offsets.push_back(bytes);
     bytes = align256(bytes + (nf + 1) * sizeof(uint64_t));
     off_fb.push_back(bytes);
-    if (kt::is_ks_mode(g.mode)) bytes = align256(bytes + g.n_rays * sizeof(uint32_t));
+    if (kt::has_fallback(g.mode)) bytes = align256(bytes + g.n_rays * sizeof(uint32_t));
   }
   const size_t off_counters = bytes;
   const size_t counters_bytes = b->groups.size() * 4 * sizeof(uint32_t);
@@ -314,7 +320,7 @@ kt_status kt_batch_create(kt_context* ctx, const kt_frame_desc* descs, const kt_
     g.d_frames = (kt::Frame*)(b->d_mem + off_frames[gi]);
     g.d_outs = (kt::OutSoA*)(b->d_mem + off_outs[gi]);
     g.d_offsets = (uint64_t*)(b->d_mem + off_offsets[gi]);
-    g.d_fb = kt::is_ks_mode(g.mode) ? (uint32_t*)(b->d_mem + off_fb[gi]) : nullptr;
+    g.d_fb = kt::has_fallback(g.mode) ? (uint32_t*)(b->d_mem + off_fb[gi]) : nullptr;
     g.d_counters = d_counters + 4 * gi;
     std::vector<kt::Frame> hf(nf);
     std::vector<kt::OutSoA> ho(nf);
@@ -331,10 +337,9 @@ kt_status kt_batch_create(kt_context* ctx, const kt_frame_desc* descs, const kt_
             "batch outputs");
     KT_CUDA(ctx, cudaMemcpy(g.d_offsets, hoff.data(), (nf + 1) * sizeof(uint64_t),
                             cudaMemcpyHostToDevice), "batch offsets");
-    if (kt::is_ks_mode(g.mode)) {
-      const kt::Mode bm = g.mode == kt::kModeKSRk4Mixed ? kt::kModeBLRk4Mixed : kt::kModeBLRk4;
-      g.fb_variant = default_variant(bm);
-      KT_CUDA(ctx, kt::batch_shape(bm, g.fb_variant, ctx->device, &g.fb_shape), "occupancy query");
+    if (kt::has_fallback(g.mode)) {
+      g.fb_variant = default_variant(g.fb_mode);
+      KT_CUDA(ctx, kt::batch_shape(g.fb_mode, g.fb_variant, ctx->device, &g.fb_shape), "occupancy query");
     }
     g.variant = opt.variant >= 0 ? opt.variant : default_variant(g.mode);
     g.refill_min = opt.refill_min > 0 ? opt.refill_min : 1;

@@ -162,9 +162,10 @@ kt_status prepare_frame(const kt_frame_desc* d, Frame* f, kt_frame_derived* dv, 
     *err = "bundles must be 0 or 1";
     return KT_ERR_INVALID_ARGUMENT;
   }
-  if (d->solver_mode != KT_SOLVER_STANDARD) {
-    *err = "only --solver-mode standard runs on this backend";
-    return KT_ERR_UNSUPPORTED;
+  if (d->solver_mode != KT_SOLVER_STANDARD && d->solver_mode != KT_SOLVER_SEMI_ANALYTIC &&
+      d->solver_mode != KT_SOLVER_ELLIPTIC_CLOSED) {
+    *err = "solver_mode must be KT_SOLVER_STANDARD, _SEMI_ANALYTIC or _ELLIPTIC_CLOSED";
+    return KT_ERR_INVALID_ARGUMENT;
   }
   if (d->precision != KT_PREC_FP64 && d->precision != KT_PREC_MIXED &&
       d->precision != KT_PREC_SMOOTH) {
@@ -199,6 +200,23 @@ kt_status prepare_frame(const kt_frame_desc* d, Frame* f, kt_frame_derived* dv, 
   fr.chart = chart;
   fr.intg = d->integrator;
   fr.bundles = d->bundles;
+  // select_solver_mode (main.cpp:235-276) on the effective chart: bundles,
+  // and the KS chart for the semi-analytic solver, take the standard
+  // tracers; both other solvers need Kerr (Q = Lambda = 0).
+  int solver = d->solver_mode;
+  const bool kerr = fabs(d->Q) <= 1e-15 && fabs(d->Lambda) <= 1e-15;
+  if (d->bundles && solver != KT_SOLVER_STANDARD) solver = KT_SOLVER_STANDARD;
+  if (solver == KT_SOLVER_SEMI_ANALYTIC && (chart != KT_CHART_BL || !kerr)) solver = KT_SOLVER_STANDARD;
+  if (solver == KT_SOLVER_ELLIPTIC_CLOSED && !kerr) solver = KT_SOLVER_STANDARD;
+  if (solver == KT_SOLVER_ELLIPTIC_CLOSED) {
+    *err = "the elliptic-closed solver does not run on this backend";
+    return KT_ERR_UNSUPPORTED;
+  }
+  if (solver == KT_SOLVER_SEMI_ANALYTIC && d->precision != KT_PREC_FP64) {
+    *err = "the semi-analytic solver runs in FP64 only";
+    return KT_ERR_UNSUPPORTED;
+  }
+  fr.solver = solver;
   // Camera (camera.hpp:32-35): degrees -> radians as theta_deg * M_PI / 180.
   double th, ph, fov;
   if (d->flags & KT_FLAG_ANGLES_RADIANS) {
@@ -249,6 +267,7 @@ kt_status prepare_frame(const kt_frame_desc* d, Frame* f, kt_frame_derived* dv, 
     dv->fov_h = fov;
     dv->dlam0 = fr.dlam0;
     dv->max_steps = fr.max_steps;
+    dv->solver = fr.solver;
     dv->tol = fr.tol;
     dv->bundle_eps = fr.bundle_eps;
     dv->r_fp32 = fr.r_fp32;

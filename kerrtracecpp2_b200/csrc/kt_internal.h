@@ -48,13 +48,16 @@ enum Mode : int {
   kModeBLDopri5Mixed = 5,
   kModeKSRk4Mixed = 6,
   kModeBundleMixed = 7,
-  kNumModes = 8
+  kModeSepRk4 = 8,
+  kNumModes = 9
 };
 
-// Kernel mode of a prepared frame (and, for the KS chart, of its BL
-// fallback pass).
+// Kernel mode of a prepared frame (and of the BL pass over the rays its
+// kernel hands back: KS rays whose initialisation failed, separable-Kerr
+// rays that gave up).
 inline Mode frame_mode(const Frame& f) {
   const bool mixed = f.precision == 1;
+  if (f.solver == 1) return kModeSepRk4;
   if (f.bundles) return mixed ? kModeBundleMixed : kModeBundle;
   if (f.chart == 0) return mixed ? kModeKSRk4Mixed : kModeKSRk4;
   if (f.intg == 1) return mixed ? kModeBLDopri5Mixed : kModeBLDopri5;
@@ -62,10 +65,16 @@ inline Mode frame_mode(const Frame& f) {
 }
 inline Mode fallback_mode(const Frame& f) {
   const bool mixed = f.precision == 1;
+  // trace_single_separable_kerr falls back to RK4 step doubling whatever the
+  // integrator (main.cpp:582-583, 612, 646)
+  if (f.solver == 1) return kModeBLRk4;
   if (f.intg == 1) return mixed ? kModeBLDopri5Mixed : kModeBLDopri5;
   return mixed ? kModeBLRk4Mixed : kModeBLRk4;
 }
 inline bool is_ks_mode(Mode m) { return m == kModeKSRk4 || m == kModeKSRk4Mixed; }
+inline bool is_mixed_mode(Mode m) { return m >= kModeBLRk4Mixed && m <= kModeBundleMixed; }
+// Modes whose kernel may hand rays to a second, BL launch (fallback list).
+inline bool has_fallback(Mode m) { return is_ks_mode(m) || m == kModeSepRk4; }
 
 struct LaunchShape {
   int block;    // threads per block

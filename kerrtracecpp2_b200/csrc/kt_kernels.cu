@@ -80,6 +80,39 @@ struct ModeBundle {
   }
 };
 
+// Separable Kerr (semi-analytic solver): rays that give up are appended to
+// the fallback list for the BL RK4 launch and write no result here.
+struct ModeSepRk4 {
+  using Machine = SepRk4;
+  static constexpr int kSlots = SepRk4::kSlots;
+  SepRk4* m;
+  Fallback fb;
+  __device__ __forceinline__ bool needs_k1() const { return m->needs_k1(); }
+  __device__ __forceinline__ void hand_back(uint32_t key, uint32_t out_slot) const {
+    const uint32_t i = atomicAdd(fb.count, 1u);
+    fb.pix[i] = key;
+    if (fb.slot) fb.slot[i] = out_slot;
+  }
+  __device__ __forceinline__ bool start(const Frame& f, uint32_t pix, uint32_t out_slot,
+                                        uint32_t fb_key, const Fallback& fbl) {
+    fb = fbl;
+    if (m->init(f, camera_ray(f, pix), fb_key, out_slot)) return true;
+    hand_back(fb_key, out_slot);
+    return false;
+  }
+  __device__ __forceinline__ bool slot(const Frame& f, int s, RayResult* res) {
+    double y[2], k[3];
+    m->input(s, y);
+    const bool ok = sep_rhs(m->c, y[0], y[1], m->sr, m->sth, k);
+    if (!m->consume(f, s, k, ok, res)) return false;
+    if (m->fallback) {
+      hand_back(m->fb_key, m->out_slot);
+      res->outcome = -1;
+    }
+    return true;
+  }
+};
+
 // Launch shape per mode, measured on B200 (720p KNdS frame, BL chart; 512^2
 // Kerr-Newman frame, KS chart; 480x270 bundle frame): the BL single-ray
 // kernels run best as 64-thread blocks capped at 113 registers (9 blocks =
@@ -89,12 +122,13 @@ template <> struct Shape<struct ModeBLRk4> { static constexpr int kBlock = 64, k
 template <> struct Shape<struct ModeBLDopri5> { static constexpr int kBlock = 64, kMinBlocks = 9; };
 
 cudaError_t launch_shape(Mode mode, int device, LaunchShape* shape) {
-  if (mode >= kModeBLRk4Mixed) return launch_shape_mixed(mode, device, shape);
+  if (is_mixed_mode(mode)) return launch_shape_mixed(mode, device, shape);
   switch (mode) {
     case kModeBLRk4: return shape_for<ModeBLRk4>(device, shape);
     case kModeBLDopri5: return shape_for<ModeBLDopri5>(device, shape);
     case kModeKSRk4: return shape_for<ModeKSRk4>(device, shape);
     case kModeBundle: return shape_for<ModeBundle>(device, shape);
+    case kModeSepRk4: return shape_for<ModeSepRk4>(device, shape);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -102,12 +136,13 @@ cudaError_t launch_shape(Mode mode, int device, LaunchShape* shape) {
 cudaError_t launch_trace(Mode mode, const Frame& f, const OutSoA& out, const RayList& rl,
                          uint32_t* queue, const Fallback& fb, const LaunchShape& s,
                          cudaStream_t stream) {
-  if (mode >= kModeBLRk4Mixed) return launch_trace_mixed(mode, f, out, rl, queue, fb, s, stream);
+  if (is_mixed_mode(mode)) return launch_trace_mixed(mode, f, out, rl, queue, fb, s, stream);
   switch (mode) {
     case kModeBLRk4: k_trace<ModeBLRk4><<<s.grid, s.block, s.smem, stream>>>(f, out, rl, queue, fb); break;
     case kModeBLDopri5: k_trace<ModeBLDopri5><<<s.grid, s.block, s.smem, stream>>>(f, out, rl, queue, fb); break;
     case kModeKSRk4: k_trace<ModeKSRk4><<<s.grid, s.block, s.smem, stream>>>(f, out, rl, queue, fb); break;
     case kModeBundle: k_trace<ModeBundle><<<s.grid, s.block, s.smem, stream>>>(f, out, rl, queue, fb); break;
+    case kModeSepRk4: k_trace<ModeSepRk4><<<s.grid, s.block, s.smem, stream>>>(f, out, rl, queue, fb); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
@@ -119,6 +154,7 @@ cudaError_t batch_shape(Mode mode, int variant, int device, LaunchShape* shape) 
     case kModeBLDopri5: return batch_shape<ModeBLDopri5>(variant, device, shape);
     case kModeKSRk4: return batch_shape<ModeKSRk4>(variant, device, shape);
     case kModeBundle: return batch_shape<ModeBundle>(variant, device, shape);
+    case kModeSepRk4: return batch_shape<ModeSepRk4>(variant, device, shape);
     default: return batch_shape_mixed(mode, variant, device, shape);
   }
 }
@@ -130,6 +166,7 @@ cudaError_t launch_batch(Mode mode, int variant, const BatchRays& br, uint32_t* 
     case kModeBLDopri5: return batch_launch<ModeBLDopri5>(variant, br, queue, fb, s, st);
     case kModeKSRk4: return batch_launch<ModeKSRk4>(variant, br, queue, fb, s, st);
     case kModeBundle: return batch_launch<ModeBundle>(variant, br, queue, fb, s, st);
+    case kModeSepRk4: return batch_launch<ModeSepRk4>(variant, br, queue, fb, s, st);
     default: return launch_batch_mixed(mode, variant, br, queue, fb, s, st);
   }
 }

@@ -43,7 +43,7 @@ struct Frame {
   int max_steps;
   int chart, intg, bundles;
   int precision;     // KT_PREC_FP64 / KT_PREC_MIXED
-  int pad0;
+  int solver;        // effective KT_SOLVER_STANDARD / KT_SOLVER_SEMI_ANALYTIC
 };
 
 struct RayResult {
@@ -872,6 +872,244 @@ struct Bundle {
           set_result(o, kOutEscaped, st, 0.0, 1.0, 1.0, 0.0, 0.0, 0.0);
           return true;
         }
+        return false;
+      }
+    }
+  }
+};
+
+// -------------------------------------------------- separable Kerr (BL)
+// The semi-analytic solver, trace_single_separable_kerr with
+// rk4_adaptive_separable_kerr and rk4_step_separable_kerr (main.cpp:506-703):
+// RK4 step doubling on (r, theta, phi) with the separated right-hand side
+// (sep_rhs), kSlots = 10 as in BLRk4 (f(s) shared by both paths, f at the
+// end of an accepted step shared by the events and the next attempt).  A
+// stage whose right-hand side or end state is not finite fails the attempt
+// (h halved).  The ray gives up -- and is traced again from the camera by
+// the standard BL tracer with RK4 step doubling -- when the constants of
+// motion cannot be formed, after 65 rejected attempts of one step, on a
+// non-finite step size, or when f at the end of a step near the equator
+// is not finite; `fallback` is then set.
+struct SepRk4 {
+  static constexpr int kSlots = 10;
+  SepConst c;
+  double pt, pphi;   // camera covector (disk redshift)
+  double r, th, ph;  // SeparableState
+  double h, step_used;
+  double k1[3];      // f(s) = {dr, dth, dph}
+  double kp[3];      // previous stage; after acceptance f(s_prev) (dr, dth)
+  double sum[3];
+  double A[3];       // path A result; after acceptance s_prev
+  double B1[3];
+  double prevR, prevT;  // R, Theta at the start of the step
+  double Rn, Tn;        // ... at its end
+  int sr, sth;
+  int it, rejects;
+  uint32_t attempts;
+  uint32_t fb_key, out_slot;
+  bool need_k1, pending, k1_ok, fail, fallback;
+
+  KT_HD bool needs_k1() const { return need_k1; }
+
+  // false: the constants cannot be formed (init_separable_consts).
+  KT_HD bool init(const Frame& f, const Geo& s, uint32_t key, uint32_t slot) {
+    fb_key = key;
+    out_slot = slot;
+    fallback = false;
+    if (!sep_init(f.g, s.th, s.pth, s.pt, s.pphi, &c)) return false;
+    // branch signs from the BL velocities dr = g^rr p_r, dth = g^thth p_th
+    const Inv U = bl_inv(f.g, s.r, bl_ang(f.g, s.th));
+    sr = (U.rr * s.pr >= 0.0) ? 1 : -1;
+    sth = (U.hh * s.pth >= 0.0) ? 1 : -1;
+    pt = s.pt;
+    pphi = s.pphi;
+    r = s.r;
+    th = s.th;
+    ph = s.ph;
+    h = f.dlam0;
+    step_used = h;
+    prevR = sep_R(c, r);
+    prevT = sep_Theta(c, th);
+    it = 0;
+    rejects = 0;
+    attempts = 0;
+    need_k1 = true;
+    pending = false;
+    return true;
+  }
+
+  KT_HD void input(int slot, double y[2]) const {
+    if (slot < 0) {
+      y[0] = r; y[1] = th;
+      return;
+    }
+    if (slot == 6) {
+      y[0] = B1[0]; y[1] = B1[1];
+      return;
+    }
+    const double cf = doubling_coeff(slot, h);
+    const bool on_s = slot < 6;
+    const bool use_k1 = (slot == 0 || slot == 3);
+    y[0] = (on_s ? r : B1[0]) + cf * (use_k1 ? k1[0] : kp[0]);
+    y[1] = (on_s ? th : B1[1]) + cf * (use_k1 ? k1[1] : kp[1]);
+  }
+
+  KT_HD bool give_up(RayResult* o) {
+    fallback = true;
+    o->steps = (uint32_t)it;
+    o->attempts = attempts;
+    set_result(o, kOutEscaped, kStEvent, 0.0, 1.0, 1.0, 0.0, 0.0, 0.0);
+    return true;
+  }
+
+  // Events of the accepted step s_prev = A -> (r, th, ph) (main.cpp:633-699).
+  KT_HD bool events(const Frame& f, RayResult* o) {
+    double best_alpha = 2.0;
+    int ev = kEvNone;
+    double disk_r = 0.0, disk_red = 1.0, disk_phi = 0.0;
+    const double q0 = A[1] - kHalfPi;
+    const double q1 = th - kHalfPi;
+    if (sign_change(q0, q1) || (dmin(fabs(q0), fabs(q1)) < 0.35)) {
+      if (!k1_ok) return give_up(o);  // f(s_prev) was finite: the attempt used it
+      double alpha = 0.0;
+      if (first_event(A[1], th, kp[1], k1[1], step_used, kHalfPi, &alpha)) {
+        const double r_hit = hermite(A[0], r, kp[0], k1[0], step_used, alpha);
+        if (r_hit >= f.r_in && r_hit <= f.r_out) {
+          disk_r = r_hit;
+          disk_red = dclamp(disk_redshift(f.g, f.eq, r_hit, pt, pphi), 0.0, 20.0);
+          disk_phi = A[2] + alpha * (ph - A[2]);
+          best_alpha = alpha;
+          ev = kEvDisk;
+        }
+      }
+    }
+    horizon_escape(A[0], r, f.rh_cut, f.r_esc, &best_alpha, &ev);
+    if (ev == kEvNone) return false;
+    o->steps = (uint32_t)it + 1;
+    o->attempts = attempts;
+    if (ev == kEvDisk) {
+      set_result(o, kOutDisk, kStEvent, disk_r, disk_red, 1.0, disk_phi, 0.0, 0.0);
+    } else if (ev == kEvHorizon) {
+      set_result(o, kOutHorizon, kStEvent, A[0] + best_alpha * (r - A[0]), 0.0, 1.0, 0.0, 0.0, 0.0);
+    } else {
+      const double th_esc = A[1] + best_alpha * (th - A[1]);
+      const double ph_esc = A[2] + best_alpha * (ph - A[2]);
+      // {ESCAPED, r_escape, 1.0, th_esc, ph_esc}: the phi_disk and theta_esc slots
+      set_result(o, kOutEscaped, kStEvent, f.r_esc, 1.0, 1.0, th_esc, ph_esc, 0.0);
+    }
+    return true;
+  }
+
+  // k: f at the slot's input; ok: sep_rhs found it finite.  Returns true
+  // when the ray is finished (o filled; fallback set if it gave up).
+  KT_HD bool consume(const Frame& f, int slot, const double k[3], bool ok, RayResult* o) {
+    if (slot < 0) {
+      for (int i = 0; i < 3; ++i) k1[i] = k[i];
+      k1_ok = ok;
+      need_k1 = false;
+      if (!pending) return false;
+      pending = false;
+      if (events(f, o)) return true;
+      prevR = Rn;
+      prevT = Tn;
+      ++it;
+      rejects = 0;
+      if (it >= f.max_steps) {
+        o->steps = (uint32_t)it;
+        o->attempts = attempts;
+        set_result(o, kOutEscaped, kStStepCap, r, 1.0, 1.0, th, ph, 0.0);
+        return true;
+      }
+      return false;
+    }
+    switch (slot) {
+      case 0:
+      case 3:
+        if (slot == 0) fail = !k1_ok;
+        fail = fail || !ok;
+        for (int i = 0; i < 3; ++i) sum[i] = k1[i] + 2.0 * k[i];
+        for (int i = 0; i < 2; ++i) kp[i] = k[i];
+        return false;
+      case 1:
+      case 4:
+      case 7:
+      case 8:
+        fail = fail || !ok;
+        for (int i = 0; i < 3; ++i) sum[i] = sum[i] + 2.0 * k[i];
+        for (int i = 0; i < 2; ++i) kp[i] = k[i];
+        return false;
+      case 6:
+        fail = fail || !ok;
+        for (int i = 0; i < 3; ++i) sum[i] = k[i];
+        for (int i = 0; i < 2; ++i) kp[i] = k[i];
+        return false;
+      case 2: {
+        const double w = h / 6.0;
+        A[0] = r + w * (sum[0] + k[0]);
+        A[1] = th + w * (sum[1] + k[1]);
+        A[2] = ph + w * (sum[2] + k[2]);
+        fail = fail || !ok || !(finite(A[0]) && finite(A[1]) && finite(A[2]));
+        return false;
+      }
+      case 5: {
+        const double w = (0.5 * h) / 6.0;
+        B1[0] = r + w * (sum[0] + k[0]);
+        B1[1] = th + w * (sum[1] + k[1]);
+        B1[2] = ph + w * (sum[2] + k[2]);
+        fail = fail || !ok || !(finite(B1[0]) && finite(B1[1]) && finite(B1[2]));
+        return false;
+      }
+      default: {  // 9: path B2 done -> error control
+        const double w = (0.5 * h) / 6.0;
+        const double Br = B1[0] + w * (sum[0] + k[0]);
+        const double Bth = B1[1] + w * (sum[1] + k[1]);
+        const double Bph = B1[2] + w * (sum[2] + k[2]);
+        fail = fail || !ok || !(finite(Br) && finite(Bth) && finite(Bph));
+        step_used = h;
+        ++attempts;
+        bool accepted = false;
+        if (fail) {
+          h = dmax(h * 0.5, 1e-10);
+        } else {
+          const double e0 = A[0] - Br, e1 = A[1] - Bth, e2 = A[2] - Bph;
+          const double err = sqrt((e0 * e0 + e1 * e1) + e2 * e2) / 15.0;
+          if (!finite(err)) {
+            h = dmax(h * 0.5, 1e-10);
+          } else if (err < f.tol || h < 1e-10) {
+            const double sc = (err > 1e-14) ? 0.9 * ktm_pow(f.tol / err, 0.2) : 4.0;
+            h = dclamp(h * sc, 1e-10, 100.0);
+            accepted = true;
+          } else {
+            h = dmax((h * 0.9) * ktm_pow(f.tol / err, 0.25), 1e-10);
+          }
+        }
+        if (!accepted) {
+          if (!finite(h) || ++rejects > 64) return give_up(o);
+          return false;
+        }
+        A[0] = r;  // s_prev
+        A[1] = th;
+        A[2] = ph;
+        kp[0] = k1[0];  // f(s_prev): dr, dth
+        kp[1] = k1[1];
+        r = Br;
+        th = Bth;
+        ph = Bph;
+        // theta kept in [0, pi], then the turning points of R and Theta flip
+        // the branch signs (main.cpp:615-628)
+        if (th < 0.0) {
+          th = -th;
+          sth = -sth;
+        } else if (th > kPi) {
+          th = 2.0 * kPi - th;
+          sth = -sth;
+        }
+        Rn = sep_R(c, r);
+        Tn = sep_Theta(c, th);
+        if (Rn <= 1e-9 && prevR > 1e-9) sr = -sr;
+        if (Tn <= 1e-11 && prevT > 1e-11) sth = -sth;
+        need_k1 = true;
+        pending = true;
         return false;
       }
     }

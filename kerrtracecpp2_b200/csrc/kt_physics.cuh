@@ -413,6 +413,68 @@ KT_HD double bundle_redshift(const Metric& g, const Ang& eq, double r, double pt
   return red;
 }
 
+// ---------------------------------------------- separable Kerr (Q = Lambda = 0)
+// The semi-analytic solver's first integrals and potentials
+// (main.cpp:440-504): E = -p_t, L_z = p_phi, Carter's Q_c; R(r) and
+// Theta(theta); dr, dtheta carry the branch signs, dphi is sign-free.
+
+struct SepConst {
+  double M, a, E, Lz, Qc;
+};
+
+// Delta = r^2 - 2 M r + a^2 (main.cpp:470-472)
+KT_HD double sep_delta(const SepConst& c, double r) { return (r * r - (2.0 * c.M) * r) + c.a * c.a; }
+
+// R(r) = P^2 - Delta (Q_c + (L_z - a E)^2), P = E (r^2 + a^2) - a L_z (main.cpp:474-479)
+KT_HD double sep_R(const SepConst& c, double r) {
+  const double P = c.E * (r * r + c.a * c.a) - c.a * c.Lz;
+  const double u = c.Lz - c.a * c.E;
+  return P * P - sep_delta(c, r) * (c.Qc + u * u);
+}
+
+// Theta(theta) = Q_c - cos^2 (L_z^2 / max(sin^2, 1e-14) - a^2 E^2) (main.cpp:481-486)
+KT_HD double sep_Theta_sc(const SepConst& c, double st, double ct) {
+  const double st2 = dmax(st * st, 1e-14);
+  return c.Qc - (ct * ct) * ((c.Lz * c.Lz) / st2 - ((c.a * c.a) * c.E) * c.E);
+}
+KT_HD double sep_Theta(const SepConst& c, double th) {
+  double st, ct;
+  ktm_sincos(th, &st, &ct);
+  return sep_Theta_sc(c, st, ct);
+}
+
+// init_separable_consts (main.cpp:454-468) for a Kerr frame: false when
+// E = -p_t is not a positive finite number or Q_c is not finite.
+KT_HD bool sep_init(const Metric& g, double th, double pth, double pt, double pphi, SepConst* c) {
+  c->M = g.M;
+  c->a = g.a;
+  c->E = -pt;
+  c->Lz = pphi;
+  if (!(finite(c->E) && finite(c->Lz) && c->E > 0.0)) return false;
+  double st, ct;
+  ktm_sincos(th, &st, &ct);
+  const double st2 = dmax(st * st, 1e-14);
+  c->Qc = pth * pth + (ct * ct) * ((c->Lz * c->Lz) / st2 - ((c->a * c->a) * c->E) * c->E);
+  return finite(c->Qc);
+}
+
+// kerr_sep_rhs (main.cpp:488-504): k = {dr, dtheta, dphi}; false when any
+// of them is not finite.  sr, sth: branch signs (>= 0 counts as +).
+KT_HD bool sep_rhs(const SepConst& c, double r, double th, int sr, int sth, double k[3]) {
+  double st, ct;
+  ktm_sincos(th, &st, &ct);
+  const double st2 = dmax(st * st, 1e-14);
+  const double sig = dmax(r * r + ((c.a * c.a) * ct) * ct, 1e-14);
+  const double del = sep_delta(c, r);
+  const double P = c.E * (r * r + c.a * c.a) - c.a * c.Lz;
+  const double R = sep_R(c, r);
+  const double T = sep_Theta_sc(c, st, ct);
+  k[0] = ((sr >= 0) ? 1.0 : -1.0) * sqrt(dmax(R, 0.0)) / sig;
+  k[1] = ((sth >= 0) ? 1.0 : -1.0) * sqrt(dmax(T, 0.0)) / sig;
+  k[2] = (c.Lz / st2 + c.a * (P / dmax(del, 1e-14) - c.E)) / sig;
+  return finite(k[0]) && finite(k[1]) && finite(k[2]);
+}
+
 // ------------------------------------------------------------------ events
 // geodesic.hpp:49-140
 

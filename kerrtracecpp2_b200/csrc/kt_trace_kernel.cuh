@@ -116,7 +116,7 @@ __global__ void __launch_bounds__(Shape<ModeT>::kBlock, Shape<ModeT>::kMinBlocks
       if (part) {
         RayResult res;
         if (mode.slot(f, s, &res)) {
-          write_result(out, out_slot, res);
+          if (res.outcome >= 0) write_result(out, out_slot, res);  // < 0: handed to the BL pass
           active = false;
         }
       }
@@ -208,7 +208,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
       if (part) {
         RayResult res;
         if (mode.slot(f, s, &res)) {
-          write_result(br.outs[fi], pix, res);
+          if (res.outcome >= 0) write_result(br.outs[fi], pix, res);
           active = false;
         }
       }

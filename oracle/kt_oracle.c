@@ -624,6 +624,7 @@ typedef struct {
   Metric g;
   Cam cam;
   int chart, intg, bundles;
+  int solver; /* effective RaySolverMode: KT_SOLVER_STANDARD or KT_SOLVER_SEMI_ANALYTIC */
   int max_steps;
   double step_init, tol;
   double r_in, r_out, r_esc, rh;
@@ -707,6 +708,208 @@ static Ray trace_single(const Frame* f, Geo s) {
       const double ph_esc = sp.ph + best_alpha * (s.ph - sp.ph);
       o = ray_result(KT_OUT_ESCAPED, f->r_esc, 1.0, th_esc, ph_esc, 0.0);
     } else {
+      continue;
+    }
+    o.steps = (uint32_t)it + 1;
+    o.attempts = att;
+    return o;
+  }
+  Ray o = ray_result(KT_OUT_ESCAPED, s.r, 1.0, s.th, s.ph, 0.0);
+  o.steps = (uint32_t)max_steps;
+  o.attempts = att;
+  return o;
+}
+
+/* --------------------------------------------- separable Kerr tracer
+ * The semi-analytic solver (main.cpp:436-703): Kerr only (Q = Lambda = 0),
+ * BL chart.  The first integrals E = -p_t, L_z = p_phi and Carter's Q_c
+ * reduce the ray to (r, theta, phi) with the radial and polar potentials
+ * R(r), Theta(theta) and the branch signs of dr and dtheta; RK4 step
+ * doubling on those three.  Any failure restarts the ray on the standard
+ * BL tracer with RK4 step doubling. */
+typedef struct { double M, a, E, Lz, Qc; } SepC;           /* SeparableKerrConsts */
+typedef struct { double r, th, ph; int sr, sth; } SepS;     /* SeparableState */
+
+/* init_separable_consts, main.cpp:454-468 */
+static int sep_init(const Geo* s, const Metric* g, SepC* c) {
+  if (fabs(g->Q) > 1e-15 || fabs(g->L) > 1e-15) return 0;
+  c->M = g->M;
+  c->a = g->a;
+  c->E = -s->pt;
+  c->Lz = s->pphi;
+  if (!(oisfinite(c->E) && oisfinite(c->Lz) && c->E > 0.0)) return 0;
+  const double st = ktm_sin(s->th), ct = ktm_cos(s->th);
+  const double st2 = omax(st * st, 1e-14);
+  c->Qc = s->pth * s->pth + (ct * ct) * ((c->Lz * c->Lz) / st2 - ((c->a * c->a) * c->E) * c->E);
+  return oisfinite(c->Qc);
+}
+
+/* kerr_sep_delta, kerr_sep_R, kerr_sep_Theta (main.cpp:470-486) */
+static double sep_delta(const SepC* c, double r) { return (r * r - (2.0 * c->M) * r) + c->a * c->a; }
+
+static double sep_R(const SepC* c, double r) {
+  const double P = c->E * (r * r + c->a * c->a) - c->a * c->Lz;
+  const double u = c->Lz - c->a * c->E;
+  const double K = c->Qc + u * u;
+  return P * P - sep_delta(c, r) * K;
+}
+
+static double sep_Theta(const SepC* c, double th) {
+  const double st = ktm_sin(th), ct = ktm_cos(th);
+  const double st2 = omax(st * st, 1e-14);
+  return c->Qc - (ct * ct) * ((c->Lz * c->Lz) / st2 - ((c->a * c->a) * c->E) * c->E);
+}
+
+/* kerr_sep_rhs, main.cpp:488-504 */
+static int sep_rhs(const SepC* c, const SepS* s, double* dr, double* dth, double* dph) {
+  const double st = ktm_sin(s->th), ct = ktm_cos(s->th);
+  const double st2 = omax(st * st, 1e-14);
+  const double sig = omax(s->r * s->r + ((c->a * c->a) * ct) * ct, 1e-14);
+  const double del = sep_delta(c, s->r);
+  const double P = c->E * (s->r * s->r + c->a * c->a) - c->a * c->Lz;
+  const double R = sep_R(c, s->r);
+  const double T = sep_Theta(c, s->th);
+  *dr = ((s->sr >= 0) ? 1.0 : -1.0) * sqrt(omax(R, 0.0)) / sig;
+  *dth = ((s->sth >= 0) ? 1.0 : -1.0) * sqrt(omax(T, 0.0)) / sig;
+  *dph = (c->Lz / st2 + c->a * (P / omax(del, 1e-14) - c->E)) / sig;
+  return oisfinite(*dr) && oisfinite(*dth) && oisfinite(*dph);
+}
+
+/* rk4_step_separable_kerr, main.cpp:506-537 */
+static int sep_rk4(const SepC* c, SepS* s, double h) {
+  double r1, t1, p1, r2, t2, p2, r3, t3, p3, r4, t4, p4;
+  const SepS s0 = *s;
+  SepS q = s0;
+  if (!sep_rhs(c, &s0, &r1, &t1, &p1)) return 0;
+  q.r = s0.r + (0.5 * h) * r1;
+  q.th = s0.th + (0.5 * h) * t1;
+  q.ph = s0.ph + (0.5 * h) * p1;
+  if (!sep_rhs(c, &q, &r2, &t2, &p2)) return 0;
+  q.r = s0.r + (0.5 * h) * r2;
+  q.th = s0.th + (0.5 * h) * t2;
+  q.ph = s0.ph + (0.5 * h) * p2;
+  if (!sep_rhs(c, &q, &r3, &t3, &p3)) return 0;
+  q.r = s0.r + h * r3;
+  q.th = s0.th + h * t3;
+  q.ph = s0.ph + h * p3;
+  if (!sep_rhs(c, &q, &r4, &t4, &p4)) return 0;
+  const double w = h / 6.0;
+  s->r += w * (((r1 + 2.0 * r2) + 2.0 * r3) + r4);
+  s->th += w * (((t1 + 2.0 * t2) + 2.0 * t3) + t4);
+  s->ph += w * (((p1 + 2.0 * p2) + 2.0 * p3) + p4);
+  return oisfinite(s->r) && oisfinite(s->th) && oisfinite(s->ph);
+}
+
+/* rk4_adaptive_separable_kerr, main.cpp:539-576: 1 accepted, 0 rejected */
+static int sep_adaptive(const SepC* c, SepS* s, double* h, double tol) {
+  SepS A = *s, B = *s;
+  if (!sep_rk4(c, &A, *h) || !sep_rk4(c, &B, 0.5 * *h) || !sep_rk4(c, &B, 0.5 * *h)) {
+    *h = omax(*h * 0.5, 1e-10);
+    return 0;
+  }
+  const double e0 = A.r - B.r, e1 = A.th - B.th, e2 = A.ph - B.ph;
+  const double err = sqrt((e0 * e0 + e1 * e1) + e2 * e2) / 15.0;
+  if (!oisfinite(err)) {
+    *h = omax(*h * 0.5, 1e-10);
+    return 0;
+  }
+  if (err < tol || *h < 1e-10) {
+    *s = B;
+    const double sc = (err > 1e-14) ? 0.9 * ktm_pow(tol / err, 0.2) : 4.0;
+    *h = oclamp(*h * sc, 1e-10, 100.0);
+    return 1;
+  }
+  *h = omax((*h * 0.9) * ktm_pow(tol / err, 0.25), 1e-10);
+  return 0;
+}
+
+/* trace_single_separable_kerr, main.cpp:578-703.  The standard tracer it
+ * falls back to always integrates with RK4 step doubling. */
+static Ray trace_separable(const Frame* f, const Geo* sbl) {
+  Frame fb = *f;
+  fb.intg = KT_RK4_DOUBLING;
+  SepC c;
+  if (!sep_init(sbl, &f->g, &c)) return trace_single(&fb, *sbl);
+  double dr0, dth0, dpr0, dpth0;
+  geo_rhs(&f->g, sbl->r, sbl->th, sbl->pr, sbl->pth, sbl->pt, sbl->pphi, &dr0, &dth0, &dpr0, &dpth0);
+  SepS s = {sbl->r, sbl->th, sbl->ph, dr0 >= 0.0 ? 1 : -1, dth0 >= 0.0 ? 1 : -1};
+  const double rh_cut = f->rh * 1.03;
+  double h = omax(f->step_init, 1e-10);
+  double prevR = sep_R(&c, s.r), prevT = sep_Theta(&c, s.th);
+  const int max_steps = f->max_steps < 1 ? 1 : f->max_steps;
+  uint32_t att = 0;
+  for (int it = 0; it < max_steps; ++it) {
+    const SepS sp = s;
+    double step_used = h;
+    int rejects = 0;
+    for (;;) {
+      step_used = h;
+      ++att;
+      if (sep_adaptive(&c, &s, &h, f->tol)) break;
+      if (!oisfinite(h) || ++rejects > 64) return trace_single(&fb, *sbl);
+    }
+    if (s.th < 0.0) {
+      s.th = -s.th;
+      s.sth = -s.sth;
+    } else if (s.th > ORC_PI) {
+      s.th = 2.0 * ORC_PI - s.th;
+      s.sth = -s.sth;
+    }
+    const double Rn = sep_R(&c, s.r), Tn = sep_Theta(&c, s.th);
+    if (Rn <= 1e-9 && prevR > 1e-9) s.sr = -s.sr;
+    if (Tn <= 1e-11 && prevT > 1e-11) s.sth = -s.sth;
+
+    double best_alpha = 2.0;
+    int ev = EV_NONE;
+    double disk_r = 0.0, disk_red = 1.0, disk_phi = 0.0;
+    const double q0 = sp.th - ORC_PI / 2.0;
+    const double q1 = s.th - ORC_PI / 2.0;
+    if (sign_change(q0, q1) || (omin(fabs(q0), fabs(q1)) < 0.35)) {
+      double a0, b0, c0, a1, b1, c1;
+      if (!sep_rhs(&c, &sp, &a0, &b0, &c0) || !sep_rhs(&c, &s, &a1, &b1, &c1))
+        return trace_single(&fb, *sbl);
+      double alpha = 0.0;
+      if (first_event(sp.th, s.th, b0, b1, step_used, ORC_PI / 2.0, &alpha)) {
+        const double r_hit = hermite(sp.r, s.r, a0, a1, step_used, alpha);
+        if (r_hit >= f->r_in && r_hit <= f->r_out) {
+          disk_r = r_hit;
+          disk_red = oclamp(disk_redshift(&f->g, r_hit, sbl->pt, sbl->pphi), 0.0, 20.0);
+          disk_phi = sp.ph + alpha * (s.ph - sp.ph);
+          best_alpha = alpha;
+          ev = EV_DISK;
+        }
+      }
+    }
+    if (s.r <= rh_cut) {
+      const double denom_h = sp.r - s.r;
+      double alpha_h = (fabs(denom_h) > 1e-12) ? ((sp.r - rh_cut) / denom_h) : 0.0;
+      alpha_h = oclamp(alpha_h, 0.0, 1.0);
+      if (alpha_h < best_alpha) {
+        best_alpha = alpha_h;
+        ev = EV_HORIZON;
+      }
+    }
+    if (s.r >= f->r_esc) {
+      const double denom_e = s.r - sp.r;
+      double alpha_e = (fabs(denom_e) > 1e-12) ? ((f->r_esc - sp.r) / denom_e) : 1.0;
+      alpha_e = oclamp(alpha_e, 0.0, 1.0);
+      if (alpha_e < best_alpha) {
+        best_alpha = alpha_e;
+        ev = EV_ESCAPE;
+      }
+    }
+    Ray o;
+    if (ev == EV_DISK) {
+      o = ray_result(KT_OUT_DISK, disk_r, disk_red, disk_phi, 0.0, 0.0);
+    } else if (ev == EV_HORIZON) {
+      o = ray_result(KT_OUT_HORIZON, sp.r + best_alpha * (s.r - sp.r), 0.0, 0.0, 0.0, 0.0);
+    } else if (ev == EV_ESCAPE) {
+      const double th_esc = sp.th + best_alpha * (s.th - sp.th);
+      const double ph_esc = sp.ph + best_alpha * (s.ph - sp.ph);
+      o = ray_result(KT_OUT_ESCAPED, f->r_esc, 1.0, th_esc, ph_esc, 0.0);
+    } else {
+      prevR = Rn;
+      prevT = Tn;
       continue;
     }
     o.steps = (uint32_t)it + 1;
@@ -1246,6 +1449,14 @@ static void setup_frame(const kt_frame_desc* d, Frame* f) {
   f->chart = chart;
   f->intg = d->integrator;
   f->bundles = d->bundles != 0;
+  /* select_solver_mode (main.cpp:235-276) on the effective chart */
+  f->solver = d->solver_mode;
+  if (f->bundles && f->solver != KT_SOLVER_STANDARD) f->solver = KT_SOLVER_STANDARD;
+  if (f->solver == KT_SOLVER_SEMI_ANALYTIC &&
+      (chart != KT_CHART_BL || fabs(d->Q) > 1e-15 || fabs(d->Lambda) > 1e-15))
+    f->solver = KT_SOLVER_STANDARD;
+  if (f->solver == KT_SOLVER_ELLIPTIC_CLOSED && (fabs(d->Q) > 1e-15 || fabs(d->Lambda) > 1e-15))
+    f->solver = KT_SOLVER_STANDARD;
   f->max_steps = d->max_steps < 1 ? 1 : d->max_steps;
   f->step_init = omax(1e-10, d->step_init);
   f->tol = omax(1e-10, d->tol);
@@ -1275,6 +1486,7 @@ int orc_frame_derive(const kt_frame_desc* d, kt_frame_derived* out) {
   out->fov_h = f.cam.fov_h;
   out->dlam0 = omax(f.step_init, 1e-10);
   out->max_steps = f.max_steps;
+  out->solver = f.solver;
   out->tol = f.tol;
   out->bundle_eps = (f.cam.fov_h / (double)f.cam.W) * 0.5;
   out->r_fp32 = (d->precision == KT_PREC_MIXED && f.tol >= 1e-8)
@@ -1304,7 +1516,9 @@ void orc_trace_pixels(const kt_frame_desc* d, int64_t n, const uint32_t* pix, ui
       double al, be;
       cam_pixel_angles(&f.cam, px, py, f.offx, f.offy, &al, &be);
       const Geo s = cam_angle_ray(&f.cam, al, be, &f.g);
-      o = (f.chart == KT_CHART_KS) ? trace_single_ks(&f, &s) : trace_single(&f, s);
+      o = (f.chart == KT_CHART_KS) ? trace_single_ks(&f, &s)
+          : (f.solver == KT_SOLVER_SEMI_ANALYTIC) ? trace_separable(&f, &s)
+                                                  : trace_single(&f, s);
     }
     outcome[i] = o.outcome;
     r[i] = o.r;

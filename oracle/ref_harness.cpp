@@ -32,10 +32,17 @@ struct RayOut {
   double r, redshift, magnif, phi_disk, theta_esc, phi_esc;
 };
 
+RaySolverMode solver_of(const kt_frame_desc* d) {
+  return d->solver_mode == KT_SOLVER_SEMI_ANALYTIC ? RaySolverMode::SEMI_ANALYTIC
+         : d->solver_mode == KT_SOLVER_ELLIPTIC_CLOSED ? RaySolverMode::ELLIPTIC_CLOSED
+                                                      : RaySolverMode::STANDARD;
+}
+
 struct FrameSetup {
   KNdSMetric g;
   Camera cam;
   CoordinateChart eff_chart;
+  RaySolverMode solver;  // after select_solver_mode
   Integrator intg;
   IntegratorControls ctl;
   bool bundles;
@@ -56,7 +63,9 @@ FrameSetup setup_frame(const kt_frame_desc* d) {
   ctl.step_init = std::max(1e-10, d->step_init);
   ctl.tol = std::max(1e-10, d->tol);
   const double r_isco = g.r_isco();
-  return FrameSetup{g, cam, chart,
+  const RaySolverMode solver =
+      select_solver_mode(solver_of(d), d->bundles != 0, chart, d->Q, d->Lambda).effective;
+  return FrameSetup{g, cam, chart, solver,
                     d->integrator == KT_DOPRI5 ? Integrator::DOPRI5 : Integrator::RK4_DOUBLING,
                     ctl, d->bundles != 0, r_isco, d->disk_out, cam.r_obs * 1.05,
                     d->pixel_offset_x, d->pixel_offset_y};
@@ -78,8 +87,14 @@ RayOut trace_one(const FrameSetup& f, int px, int py) {
   }
   auto s = f.cam.pixel_ray(px, py, f.g, f.offx, f.offy);
   TraceResult res{};
-  if (f.eff_chart == CoordinateChart::KS)
+  if (f.solver == RaySolverMode::ELLIPTIC_CLOSED) {
+    EllipticFallbackReason why = EllipticFallbackReason::NONE;
+    res = trace_single_elliptic_closed(s, f.g, f.r_disk_in, f.r_disk_out, f.r_escape, &why,
+                                       f.eff_chart, f.intg, f.ctl);
+  } else if (f.eff_chart == CoordinateChart::KS)
     res = trace_single_ks(s, f.g, f.r_disk_in, f.r_disk_out, f.r_escape, f.intg, f.ctl);
+  else if (f.solver == RaySolverMode::SEMI_ANALYTIC)
+    res = trace_single_separable_kerr(s, f.g, f.r_disk_in, f.r_disk_out, f.r_escape, f.ctl);
   else
     res = trace_single(s, f.g, f.r_disk_in, f.r_disk_out, f.r_escape, f.intg, f.ctl);
   o.outcome = (res.out == Outcome::DISK_HIT) ? 1 : (res.out == Outcome::HORIZON) ? 2
@@ -139,7 +154,7 @@ void ref_trace_geodesics(const kt_frame_desc* d, void* geopixels, int nthreads) 
   ctl.max_steps = std::max(1, (int)d->max_steps);
   ctl.step_init = std::max(1e-10, d->step_init);
   ctl.tol = std::max(1e-10, d->tol);
-  auto geo = trace_geodesics(d->width, d->height, fp, d->bundles != 0, RaySolverMode::STANDARD,
+  auto geo = trace_geodesics(d->width, d->height, fp, d->bundles != 0, solver_of(d),
                              d->chart == KT_CHART_KS ? CoordinateChart::KS : CoordinateChart::BL,
                              d->integrator == KT_DOPRI5 ? Integrator::DOPRI5 : Integrator::RK4_DOUBLING,
                              ctl, d->pixel_offset_x, d->pixel_offset_y, d->M, d->Q, d->Lambda);
@@ -217,7 +232,7 @@ void ref_render_image(const kt_frame_desc* d, const kt_color_params* c, const ui
   ctl.step_init = std::max(1e-10, d->step_init);
   ctl.tol = std::max(1e-10, d->tol);
   auto out = render_image(d->width, d->height, fp, to_bg(bg, bg_w, bg_h), d->bundles != 0,
-                          RaySolverMode::STANDARD,
+                          solver_of(d),
                           d->chart == KT_CHART_KS ? CoordinateChart::KS : CoordinateChart::BL,
                           d->integrator == KT_DOPRI5 ? Integrator::DOPRI5 : Integrator::RK4_DOUBLING,
                           ctl, camera_spp, d->M, d->Q, d->Lambda, IntersectionMode::HERMITE, 0, false,

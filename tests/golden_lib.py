@@ -58,3 +58,28 @@ def colour():
 
 def colour_meta():
     return json.loads(bytes(colour()["meta_json"]).decode())
+
+
+SEMI_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "semi.npz")
+_zs = None
+
+
+def semi():
+    """tests/golden/semi.npz (make_semi_golden.py): the semi-analytic solver."""
+    global _zs
+    if _zs is None:
+        _zs = dict(np.load(SEMI_PATH))
+    return _zs
+
+
+def semi_cases():
+    return json.loads(bytes(semi()["meta_json"]).decode())
+
+
+def semi_desc(name):
+    return abi.frame_desc(**semi_cases()[name])
+
+
+def semi_result(name):
+    z = semi()
+    return {k: z[f"{name}/{k}"] for k in FIELDS}

@@ -84,6 +84,27 @@ RayResult run_ray(const Frame& f, uint32_t pix) {
     }
   }
   const Geo s = camera_ray(f, pix);
+  if (f.solver == KT_SOLVER_SEMI_ANALYTIC) {
+    SepRk4 m;
+    if (m.init(f, s, pix, pix)) {
+      RayResult res;
+      for (;;) {
+        bool done = false;
+        for (int slot = -1; slot < SepRk4::kSlots && !done; ++slot) {
+          if (slot < 0 && !m.needs_k1()) continue;
+          double y[2], k[3];
+          m.input(slot, y);
+          const bool ok = sep_rhs(m.c, y[0], y[1], m.sr, m.sth, k);
+          done = m.consume(f, slot, k, ok, &res);
+        }
+        if (done) {
+          if (!m.fallback) return res;
+          break;
+        }
+      }
+    }
+    return run_bl<BLRk4>(f, s);  // the separable tracer gave up: standard BL, RK4
+  }
   if (f.chart == KT_CHART_KS) {
     KSRk4 m;
     if (m.init(f, s)) {
