@@ -48,6 +48,12 @@ WORKLOADS = {
     "batch64_ks_rk4_seed1": dict(batch=64, seed=1, width=0, height=0, chart=0),
     # Config 5 gradient alone (adjoint_leg): value = adjoint ms per frame.
     "adjoint_ks_512": dict(adjoint=True, width=512, height=512, chart=0),
+    # The semi-analytic solver (--bl --semi-analytic) at the CLI's default
+    # Kerr frame, 720p, default step cap 500000: every ray with a radial
+    # turning point parks there and runs to the cap, ~1 s of CPU per ray.
+    "semi_bl_kerr_720p": dict(chart=1, solver_mode=1, a=0.998, r_obs=40.0, theta_deg=80.0,
+                              fov_deg=30.0, disk_out=12.0, width=1280, height=720,
+                              cpu_calib_pixels=64),
 }
 # Frames of the batched 720p leg: the headline frame seen from this many
 # camera azimuths, traced as one batch.
@@ -118,8 +124,8 @@ def stop_clock_sampler(proc, f, path, gpu_index):
 
 def ray_flops(desc, steps, attempts):
     """Algorithmic FP64 flops of one traced frame from the kernel's counters."""
-    if desc.bundles or desc.chart == 0 and abs(desc.Lambda) <= 1e-15:
-        return None  # counted only for the BL single-ray integrators
+    if desc.bundles or desc.chart == 0 and abs(desc.Lambda) <= 1e-15 or desc.solver_mode != 0:
+        return None  # counted only for the standard BL single-ray integrators
     n = desc.width * desc.height
     if desc.integrator == 1:
         rhs = n + 6.0 * attempts
@@ -128,8 +134,9 @@ def ray_flops(desc, steps, attempts):
     return rhs * FLOPS_BL_RHS + attempts * FLOPS_RK4_ATTEMPT
 
 
-def cpu_reference_sample(desc, seconds, flavour="ieee"):
-    """Time the reference's CPU path on a strided sample of the frame.
+def cpu_reference_sample(desc, seconds, flavour="ieee", calib_pixels=None):
+    """Time the reference's CPU path on a strided sample of the frame
+    (calibrated on calib_pixels pixels, by default 512 or 16 per thread).
 
     Returns (rays_per_s, n_pixels, threads, kind, sample, results)."""
     import oracle_lib as O  # noqa: E402  (tests/oracle_lib.py)
@@ -145,7 +152,7 @@ def cpu_reference_sample(desc, seconds, flavour="ieee"):
         return O.trace_port(desc, pix=pix, nthreads=threads)
 
     # calibrate on ~0.2% of the frame, then size the sample to `seconds`
-    stride = max(1, n // max(512, threads * 16))
+    stride = max(1, n // (calib_pixels or max(512, threads * 16)))
     pix = np.arange(0, n, stride, dtype=np.uint32)
     t0 = time.perf_counter()
     trace(pix)
@@ -457,6 +464,10 @@ def main():
     from kerrtracecpp2_b200 import abi
 
     wl = dict(WORKLOADS[args.workload])
+    calib = wl.pop("cpu_calib_pixels", None)
+    if wl.get("solver_mode", 0) != 0:
+        # the semi-analytic solver runs in FP64 only; no gradient leg
+        args.no_mixed = args.no_adjoint = True
     if wl.get("adjoint"):
         return bench_adjoint(args, rank, world, local_rank)
     if wl.get("batch"):
@@ -471,6 +482,7 @@ def main():
                 "integrator": "DOPRI5" if wl.get("integrator", 0) == 1 else "RK4-doubling",
                 "tol": wl.get("tol", 1e-7), "a": wl.get("a"), "Q": wl.get("Q", 0.0),
                 "Lambda": wl.get("Lambda", 0.0), "bundles": bool(wl.get("bundles", 0)),
+                "solver": "semi-analytic" if wl.get("solver_mode", 0) == 1 else "standard",
                 "parallelism": f"frames{args.gpus}", "l2": "256 MB flush between steps"}
 
     if args.impl == "reference":
@@ -479,11 +491,11 @@ def main():
         desc = abi.frame_desc(**wl)
         per_step = max(2.0, 120.0 / max(1, args.steps + args.warmup))
         for _ in range(args.warmup):
-            cpu_reference_sample(desc, per_step)
+            cpu_reference_sample(desc, per_step, calib_pixels=calib)
         rates = []
         info = None
         for _ in range(args.steps):
-            rate, pix, threads, kind, sample, _ = cpu_reference_sample(desc, per_step)
+            rate, pix, threads, kind, sample, _ = cpu_reference_sample(desc, per_step, calib_pixels=calib)
             rates.append(rate)
             info = (threads, kind, sample)
         v = float(np.mean(rates)) / 1e6
@@ -686,7 +698,8 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, pix, threads, kind, sample, res = cpu_reference_sample(desc, args.cpu_seconds)
+        rate, pix, threads, kind, sample, res = cpu_reference_sample(desc, args.cpu_seconds,
+                                                                     calib_pixels=calib)
         got_out = out["outcome"].cpu().numpy()[pix]
         got_g = out["redshift"].cpu().numpy()[pix]
         disk = (got_out == 1) & (res["outcome"] == 1)

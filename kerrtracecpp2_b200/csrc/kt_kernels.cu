@@ -103,7 +103,7 @@ struct ModeSepRk4 {
   __device__ __forceinline__ bool slot(const Frame& f, int s, RayResult* res) {
     double y[2], k[3];
     m->input(s, y);
-    const bool ok = sep_rhs(m->c, y[0], y[1], m->sr, m->sth, k);
+    const bool ok = m->rhs(s, y, k);
     if (!m->consume(f, s, k, ok, res)) return false;
     if (m->fallback) {
       hand_back(m->fb_key, m->out_slot);
@@ -112,6 +112,8 @@ struct ModeSepRk4 {
     return true;
   }
 };
+
+template <> struct Defers<ModeSepRk4> { static constexpr bool value = true; };
 
 // Launch shape per mode, measured on B200 (720p KNdS frame, BL chart; 512^2
 // Kerr-Newman frame, KS chart; 480x270 bundle frame): the BL single-ray

@@ -903,6 +903,8 @@ struct SepRk4 {
   double B1[3];
   double prevR, prevT;  // R, Theta at the start of the step
   double Rn, Tn;        // ... at its end
+  double kin[2];        // (r, theta) at which k1 was evaluated
+  int kin_sr, kin_sth;  // ... and the branch signs
   int sr, sth;
   int it, rejects;
   uint32_t attempts;
@@ -930,6 +932,8 @@ struct SepRk4 {
     step_used = h;
     prevR = sep_R(c, r);
     prevT = sep_Theta(c, th);
+    kin[0] = kin[1] = ktm_nan();
+    kin_sr = kin_sth = 0;
     it = 0;
     rejects = 0;
     attempts = 0;
@@ -952,6 +956,138 @@ struct SepRk4 {
     const bool use_k1 = (slot == 0 || slot == 3);
     y[0] = (on_s ? r : B1[0]) + cf * (use_k1 ? k1[0] : kp[0]);
     y[1] = (on_s ? th : B1[1]) + cf * (use_k1 ? k1[1] : kp[1]);
+  }
+
+  // The right-hand side at the slot's input y (sep_rhs, a function of
+  // (r, theta, sr, sth) alone).  When y and the signs are those of k1 it is
+  // k1: a ray whose radial and polar velocities are both zero stays at that
+  // point, every stage of its attempts has the same input, and only phi
+  // advances -- the solver's rays with a radial turning point end that way
+  // and run to the step cap.  (-0 == +0 here: sep_rhs gives the same
+  // values for either zero.)
+  KT_HD bool rhs(int slot, const double y[2], double k[3]) {
+    if (y[0] == kin[0] && y[1] == kin[1] && sr == kin_sr && sth == kin_sth) {
+      k[0] = k1[0];
+      k[1] = k1[1];
+      k[2] = k1[2];
+      return k1_ok;
+    }
+    const bool ok = sep_rhs(c, y[0], y[1], sr, sth, k);
+    if (slot < 0) {
+      kin[0] = y[0];
+      kin[1] = y[1];
+      kin_sr = sr;
+      kin_sth = sth;
+    }
+    return ok;
+  }
+
+  // After an accepted step without event: the next step or the step cap.
+  KT_HD bool end_step(const Frame& f, RayResult* o) {
+    ++it;
+    rejects = 0;
+    if (it >= f.max_steps) {
+      o->steps = (uint32_t)it;
+      o->attempts = attempts;
+      set_result(o, kOutEscaped, kStStepCap, r, 1.0, 1.0, th, ph, 0.0);
+      return true;
+    }
+    return false;
+  }
+
+  // At an attempt boundary: f(s) is finite with dr = dth = 0 (k1 belongs to
+  // the current point, kin).  r + c * (+-0) = r and th + c * (+-0) = th for
+  // r, th != 0, so every stage input of every later attempt is this point,
+  // every right-hand side is k1, and only phi moves.
+  KT_HD bool parked() const {
+    return k1_ok && k1[0] == 0.0 && k1[1] == 0.0 && r != 0.0 && th != 0.0;
+  }
+
+  // Up to kParkedBudget attempts of a parked ray, each with the arithmetic
+  // of slots 0..9 and -1 written out for stages that all return k1: the
+  // stage sums of r and theta are +-0 (A, B1, B2 keep r and theta), those
+  // of phi are ((c + 2c) + 2c) + c with c = k1[2]; the step ends where it
+  // started, so R and Theta equal prevR and prevT (no branch flip) and
+  // f(s_new) is k1.  Two shortcuts, both exact:
+  //  - with r, theta fixed and dr = dth = 0 the event tests see the same
+  //    numbers at every step (the Hermite terms in h * dy vanish), so once
+  //    they find nothing they are not repeated;
+  //  - at h = 100 (the cap) with err <= tol / 2 the new step is the cap
+  //    again: sc = 0.9 (tol / err)^0.2 >= 0.9 * 2^0.2 > 1.03 (4 for
+  //    err <= 1e-14), so pow is not needed.
+  static constexpr int kParkedBudget = 256;
+  KT_HD_CALL bool parked_steps(const Frame& f, RayResult* o) {
+    const double cph = k1[2];
+    const double t = ((cph + 2.0 * cph) + 2.0 * cph) + cph;
+    const double tol = f.tol;
+    double hh = h, p = ph;
+    int n_it = it, rej = rejects;
+    uint32_t n_att = attempts;
+    bool quiet = false;
+    for (int n = 0; n < kParkedBudget; ++n) {
+      const double w = hh / 6.0;
+      const double wb = (0.5 * hh) / 6.0;
+      const double Aph = p + w * t;
+      const double B1ph = p + wb * t;
+      const double Bph = B1ph + wb * t;
+      const double used = hh;
+      ++n_att;
+      bool accepted = false;
+      if (!(finite(Aph) && finite(B1ph) && finite(Bph))) {
+        hh = dmax(hh * 0.5, 1e-10);
+      } else {
+        const double e2 = Aph - Bph;
+        const double err = sqrt(e2 * e2) / 15.0;  // (0*0 + 0*0) + e2*e2 = e2*e2
+        if (!finite(err)) {
+          hh = dmax(hh * 0.5, 1e-10);
+        } else if (err < tol || hh < 1e-10) {
+          accepted = true;
+          if (!(hh == 100.0 && (err <= 1e-14 || err <= 0.5 * tol))) {
+            const double sc = (err > 1e-14) ? 0.9 * ktm_pow(tol / err, 0.2) : 4.0;
+            hh = dclamp(hh * sc, 1e-10, 100.0);
+          }
+        } else {
+          hh = dmax((hh * 0.9) * ktm_pow(tol / err, 0.25), 1e-10);
+        }
+      }
+      if (!accepted) {
+        if (!finite(hh) || ++rej > 64) {
+          it = n_it;
+          attempts = n_att;
+          return give_up(o);
+        }
+        continue;
+      }
+      const double p_prev = p;
+      p = Bph;
+      if (!quiet) {
+        A[0] = r;
+        A[1] = th;
+        A[2] = p_prev;
+        kp[0] = k1[0];
+        kp[1] = k1[1];
+        step_used = used;
+        ph = p;
+        it = n_it;
+        attempts = n_att;
+        if (events(f, o)) return true;
+        quiet = true;
+      }
+      ++n_it;
+      rej = 0;
+      if (n_it >= f.max_steps) {
+        o->steps = (uint32_t)n_it;
+        o->attempts = n_att;
+        set_result(o, kOutEscaped, kStStepCap, r, 1.0, 1.0, th, p, 0.0);
+        return true;
+      }
+    }
+    h = hh;
+    ph = p;
+    it = n_it;
+    rejects = rej;
+    attempts = n_att;
+    return false;
   }
 
   KT_HD bool give_up(RayResult* o) {
@@ -1012,14 +1148,8 @@ struct SepRk4 {
       if (events(f, o)) return true;
       prevR = Rn;
       prevT = Tn;
-      ++it;
-      rejects = 0;
-      if (it >= f.max_steps) {
-        o->steps = (uint32_t)it;
-        o->attempts = attempts;
-        set_result(o, kOutEscaped, kStStepCap, r, 1.0, 1.0, th, ph, 0.0);
-        return true;
-      }
+      if (end_step(f, o)) return true;
+      if (parked()) return parked_steps(f, o);
       return false;
     }
     switch (slot) {

@@ -25,6 +25,16 @@
 #define KT_HD inline
 #endif
 
+// A real call on the device (one copy of the body, its registers apart from
+// the caller's); inline on the host.
+#if defined(__CUDA_ARCH__)
+#define KT_HD_CALL __host__ __device__ __noinline__
+#elif defined(__CUDACC__)
+#define KT_HD_CALL __host__ __device__ inline
+#else
+#define KT_HD_CALL inline
+#endif
+
 // Keep a loop rolled in device code: the loop body is the bulk of the
 // kernel, and one copy of it fits the instruction cache.
 #if defined(__CUDA_ARCH__)

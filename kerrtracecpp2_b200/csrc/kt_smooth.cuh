@@ -25,15 +25,8 @@
 #include "kt_machines.cuh"
 
 // Functions called from many places in the smooth kernels are real calls on
-// the device (one copy of the body each): the kernels are otherwise too big
+// the device (KT_HD_CALL, kt_physics.cuh): the kernels are otherwise too big
 // for the instruction cache.
-#if defined(__CUDA_ARCH__)
-#define KT_HD_CALL __host__ __device__ __noinline__
-#elif defined(__CUDACC__)
-#define KT_HD_CALL __host__ __device__ inline
-#else
-#define KT_HD_CALL inline
-#endif
 
 namespace kt {
 

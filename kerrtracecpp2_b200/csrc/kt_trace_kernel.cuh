@@ -61,6 +61,10 @@ constexpr size_t smem_bytes(int block) {
   return sizeof(SmemRecord<typename ModeT::Machine>) * (size_t)block;
 }
 
+// Modes whose slot() may finish a ray without a result (handed to the
+// fallback list: RayResult::outcome < 0); specialised where that happens.
+template <class ModeT> struct Defers { static constexpr bool value = false; };
+
 // Launch shape per mode: 128-thread blocks by default; a mode may
 // specialise this (see kt_kernels.cu, kt_mixed.cu).
 template <class ModeT> struct Shape { static constexpr int kBlock = 128, kMinBlocks = 1; };
@@ -74,7 +78,7 @@ template <class ModeT> struct Shape { static constexpr int kBlock = 128, kMinBlo
 // the end of the attempt.
 
 template <class ModeT>
-__global__ void __launch_bounds__(Shape<ModeT>::kBlock, Shape<ModeT>::kMinBlocks) k_trace(const Frame f, const OutSoA out, const RayList rl,
+__global__ void __launch_bounds__(Shape<ModeT>::kBlock, Shape<ModeT>::kMinBlocks) k_trace(const __grid_constant__ Frame f, const OutSoA out, const RayList rl,
                                                   uint32_t* __restrict__ queue, const Fallback fb) {
   extern __shared__ __align__(16) unsigned char smem[];
   using Rec = SmemRecord<typename ModeT::Machine>;
@@ -116,7 +120,7 @@ __global__ void __launch_bounds__(Shape<ModeT>::kBlock, Shape<ModeT>::kMinBlocks
       if (part) {
         RayResult res;
         if (mode.slot(f, s, &res)) {
-          if (res.outcome >= 0) write_result(out, out_slot, res);  // < 0: handed to the BL pass
+          if (!Defers<ModeT>::value || res.outcome >= 0) write_result(out, out_slot, res);
           active = false;
         }
       }
@@ -208,7 +212,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
       if (part) {
         RayResult res;
         if (mode.slot(f, s, &res)) {
-          if (res.outcome >= 0) write_result(br.outs[fi], pix, res);
+          if (!Defers<ModeT>::value || res.outcome >= 0) write_result(br.outs[fi], pix, res);
           active = false;
         }
       }

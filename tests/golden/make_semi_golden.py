@@ -8,7 +8,7 @@ Kerr frames in the BL chart, most with a reduced step cap: in this solver a
 ray whose radial potential reaches zero stops moving in r (dr is
 sqrt(max(R, 0)) and the branch sign flips only on a sampled crossing of
 R = 1e-9), so every ray with a radial turning point runs to the step cap.
-One case keeps the default cap of 500000 steps.  Also the frames the solver
+Two cases keep the default cap of 500000 steps.  Also the frames the solver
 hands to the standard tracers (KS chart, charge, Lambda, bundles).
 
 Stored per case: the frame descriptor, the float64 per-pixel results
@@ -36,6 +36,10 @@ SEMI = dict(chart=abi.KT_CHART_BL, solver_mode=abi.KT_SOLVER_SEMI_ANALYTIC)
 CASES = {
     "semi_kerr": dict(SEMI, a=0.5, width=32, height=18, fov_deg=40.0, max_steps=4000),
     "semi_default_cap": dict(SEMI, a=0.9, width=8, height=5, fov_deg=40.0),
+    # tol 1e-10 at the default cap: phi of a parked ray grows until the
+    # step-doubling error of its rounding reaches tol; the controller then
+    # shrinks and regrows the step
+    "semi_tight_default_cap": dict(SEMI, a=0.9, tol=1e-10, width=8, height=5, fov_deg=40.0),
     "semi_fast_spin": dict(SEMI, a=0.998, theta_deg=60.0, width=24, height=14, max_steps=3000),
     "semi_tight_tol": dict(SEMI, a=0.9, theta_deg=85.0, r_obs=60.0, fov_deg=30.0, disk_out=20.0,
                            tol=1e-10, width=24, height=14, max_steps=3000),

@@ -94,7 +94,7 @@ RayResult run_ray(const Frame& f, uint32_t pix) {
           if (slot < 0 && !m.needs_k1()) continue;
           double y[2], k[3];
           m.input(slot, y);
-          const bool ok = sep_rhs(m.c, y[0], y[1], m.sr, m.sth, k);
+          const bool ok = m.rhs(slot, y, k);
           done = m.consume(f, slot, k, ok, &res);
         }
         if (done) {
