@@ -1024,9 +1024,13 @@ struct SepRk4 {
     int n_it = it, rej = rejects;
     uint32_t n_att = attempts;
     bool quiet = false;
+    double wh = hh, w = hh / 6.0, wb = (0.5 * hh) / 6.0;  // stage weights of step wh
     for (int n = 0; n < kParkedBudget; ++n) {
-      const double w = hh / 6.0;
-      const double wb = (0.5 * hh) / 6.0;
+      if (hh != wh) {
+        wh = hh;
+        w = hh / 6.0;
+        wb = (0.5 * hh) / 6.0;
+      }
       const double Aph = p + w * t;
       const double B1ph = p + wb * t;
       const double Bph = B1ph + wb * t;
