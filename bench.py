@@ -71,6 +71,11 @@ BATCH_720P_FRAMES = 8
 FLOPS_BL_RHS = 453.0
 FLOPS_DOPRI5_ATTEMPT = 447.0
 FLOPS_RK4_ATTEMPT = 335.0
+# DRAM bytes read + written by one k_trace<ModeBLDopri5> launch on the
+# default 720p frame, from one ncu capture of that launch
+# (dram__bytes_read.sum 1.263 MB + dram__bytes_write.sum 4.794 MB): the
+# frame's 52.5 MB of outputs stay in L2 during the launch.
+TRAFFIC_DOPRI5_720P = 6.057472e6
 
 
 def env_int(name, default):
@@ -664,7 +669,8 @@ def main():
         achieved = flops / (kernel_ms * 1e-3) / 1e12
         peak = peak_gflops / 1e3
         roofline = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                    "frac": achieved / peak, "traffic": None,
+                    "frac": achieved / peak,
+                    "traffic": TRAFFIC_DOPRI5_720P if args.workload == "knds_bl_dopri5_720p" else None,
                     "peak_source": "measured in this run: kt_measure_fp64_peak (dependent FMA chains, all SMs)",
                     "flops_per_frame": flops, "rhs_per_ray": (n + 6.0 * att_sum) / n
                     if desc.integrator == 1 else (n + 10.0 * att_sum + steps_sum) / n,
