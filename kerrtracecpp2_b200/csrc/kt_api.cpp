@@ -10,6 +10,7 @@
 
 #include <new>
 #include <string>
+#include <vector>
 
 #include "../../include/kerrtrace.h"
 #include "kt_adjoint.h"
@@ -350,23 +351,6 @@ kt_status kt_render_spp_host(kt_context* ctx, const kt_frame_desc* desc, const k
   if (r != KT_OK) return r;
   DeviceGuard g(ctx->device);
   const size_t n = (size_t)desc->width * (size_t)desc->height;
-  // six float64 fields, the linear-light sum (spp > 1), outcome, one RGB pass
-  const size_t acc_bytes = spp > 1 ? 24 * n : 0;
-  const size_t need = n * (6 * 8 + 1 + 3) + acc_bytes + 256;
-  r = ensure(ctx, (void**)&ctx->d_stage, &ctx->stage_cap, need, "staging buffer");
-  if (r != KT_OK) return r;
-  unsigned char* p = ctx->d_stage;
-  kt_geo_soa d;
-  memset(&d, 0, sizeof d);
-  d.r = (double*)p; p += 8 * n;
-  d.redshift = (double*)p; p += 8 * n;
-  d.magnif = (double*)p; p += 8 * n;
-  d.phi_disk = (double*)p; p += 8 * n;
-  d.theta_esc = (double*)p; p += 8 * n;
-  d.phi_esc = (double*)p; p += 8 * n;
-  double* d_acc = (double*)p; p += acc_bytes;
-  d.outcome = p; p += n;
-  uint8_t* d_rgb = p;
   const uint8_t* d_bg = nullptr;
   if (bg_rgb_host) {
     const size_t bb = (size_t)bg_w * (size_t)bg_h * 3;
@@ -376,36 +360,120 @@ kt_status kt_render_spp_host(kt_context* ctx, const kt_frame_desc* desc, const k
             "copy background");
     d_bg = ctx->d_bg;
   }
-  // render_image (main.cpp:2232-2322): with camera_spp > 1 every pass is a
-  // full render at the frame's pixel offset plus the pass's jitter.
-  double offs[2 * KT_MAX_CAMERA_SPP];
-  spp_offsets(spp, offs);
-  const double gamma_eff = cp->gamma < 1e-6 ? 1e-6 : cp->gamma;
-  kt::RayList rl = {nullptr, nullptr, nullptr, (uint32_t)n};
-  for (int s = 0; s < spp; ++s) {
-    kt::Frame fs;
-    if (spp == 1) {
-      fs = f;
-    } else {
-      kt_frame_desc ds = *desc;
-      ds.pixel_offset_x = desc->pixel_offset_x + offs[2 * s];
-      ds.pixel_offset_y = desc->pixel_offset_y + offs[2 * s + 1];
-      r = kt::prepare_frame(&ds, &fs, nullptr, &ctx->err);
-      if (r != KT_OK) return r;
-    }
-    r = run_trace(ctx, fs, to_out(&d), rl, n, ctx->stream);
+  const kt::ColourConst cc = kt::make_colour(f, *cp);
+  if (spp == 1) {
+    // render_image (main.cpp:2209-2478): trace + colorize
+    const size_t need = n * (6 * 8 + 1 + 3) + 256;
+    r = ensure(ctx, (void**)&ctx->d_stage, &ctx->stage_cap, need, "staging buffer");
     if (r != KT_OK) return r;
-    const kt::ColourConst cc = kt::make_colour(fs, *cp);
+    unsigned char* p = ctx->d_stage;
+    kt_geo_soa d;
+    memset(&d, 0, sizeof d);
+    d.r = (double*)p; p += 8 * n;
+    d.redshift = (double*)p; p += 8 * n;
+    d.magnif = (double*)p; p += 8 * n;
+    d.phi_disk = (double*)p; p += 8 * n;
+    d.theta_esc = (double*)p; p += 8 * n;
+    d.phi_esc = (double*)p; p += 8 * n;
+    d.outcome = p; p += n;
+    uint8_t* d_rgb = p;
+    kt::RayList rl = {nullptr, nullptr, nullptr, (uint32_t)n};
+    r = run_trace(ctx, f, to_out(&d), rl, n, ctx->stream);
+    if (r != KT_OK) return r;
     KT_CUDA(ctx, kt::launch_colorize(cc, (int64_t)n, d.outcome, d.r, d.redshift, d.magnif, d.phi_disk,
                                      d.theta_esc, d.phi_esc, d_bg, bg_w, bg_h, d_rgb, ctx->stream),
             "colorize kernel launch");
-    if (spp > 1)
-      KT_CUDA(ctx, kt::launch_spp_accumulate((int64_t)(3 * n), d_rgb, d_acc, gamma_eff, s == 0, ctx->stream),
-              "supersample accumulate launch");
+    KT_CUDA(ctx, cudaMemcpyAsync(rgb_out_host, d_rgb, 3 * n, cudaMemcpyDeviceToHost, ctx->stream),
+            "copy image to host");
+    KT_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "render");
+    return KT_OK;
   }
-  if (spp > 1)
-    KT_CUDA(ctx, kt::launch_spp_finish((int64_t)(3 * n), d_acc, 1.0 / (double)spp, gamma_eff, d_rgb, ctx->stream),
-            "supersample finish launch");
+  // camera_spp > 1 (main.cpp:2232-2322): every pass is a full render at the
+  // frame's pixel offset plus the pass's jitter.  The passes differ only in
+  // their camera, so they share one kernel mode: one batch launch traces all
+  // of them (lanes refill across pass boundaries), one kernel colours them
+  // and averages in linear light.
+  if (f.precision == KT_PREC_SMOOTH)
+    return fail(ctx, KT_ERR_UNSUPPORTED, "kt_render_spp_host: the smooth tracer renders one pass");
+  if ((uint64_t)n * (uint64_t)spp > 0x7fffffffULL)
+    return fail(ctx, KT_ERR_INVALID_ARGUMENT, "kt_render_spp_host: more than 2^31 rays");
+  double offs[2 * KT_MAX_CAMERA_SPP];
+  spp_offsets(spp, offs);
+  std::vector<kt::Frame> frames((size_t)spp);
+  for (int s = 0; s < spp; ++s) {
+    kt_frame_desc ds = *desc;
+    ds.pixel_offset_x = desc->pixel_offset_x + offs[2 * s];
+    ds.pixel_offset_y = desc->pixel_offset_y + offs[2 * s + 1];
+    r = kt::prepare_frame(&ds, &frames[(size_t)s], nullptr, &ctx->err);
+    if (r != KT_OK) return r;
+  }
+  const kt::Mode m = kt::frame_mode(f);
+  // staging: Frame[spp] | OutSoA[spp] | offsets[spp + 1] | 6 f64 fields
+  // [spp][n] | outcome [spp][n] | rgb [3n]
+  auto a256 = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  const size_t nt = n * (size_t)spp;
+  const size_t off_outs = a256(spp * sizeof(kt::Frame));
+  const size_t off_offs = off_outs + a256(spp * sizeof(kt::OutSoA));
+  const size_t off_f64 = off_offs + a256((spp + 1) * sizeof(uint64_t));
+  const size_t off_oc = off_f64 + a256(6 * 8 * nt);
+  const size_t off_rgb = off_oc + a256(nt);
+  r = ensure(ctx, (void**)&ctx->d_stage, &ctx->stage_cap, off_rgb + 3 * n + 256, "staging buffer");
+  if (r != KT_OK) return r;
+  if (kt::has_fallback(m)) {
+    r = ensure(ctx, (void**)&ctx->d_fb, &ctx->fb_cap, nt * sizeof(uint32_t), "fallback list");
+    if (r != KT_OK) return r;
+  }
+  unsigned char* base = ctx->d_stage;
+  double* f64 = (double*)(base + off_f64);
+  uint8_t* oc = base + off_oc;
+  uint8_t* d_rgb = base + off_rgb;
+  kt::SppPasses P = {oc, f64, f64 + nt, f64 + 2 * nt, f64 + 3 * nt, f64 + 4 * nt, f64 + 5 * nt};
+  std::vector<kt::OutSoA> outs((size_t)spp);
+  std::vector<uint64_t> offsets((size_t)spp + 1);
+  for (int s = 0; s < spp; ++s) {
+    const size_t o = (size_t)s * n;
+    outs[(size_t)s] = kt::OutSoA{oc + o, f64 + o, f64 + nt + o, f64 + 2 * nt + o, f64 + 3 * nt + o,
+                                 f64 + 4 * nt + o, f64 + 5 * nt + o, nullptr, nullptr, nullptr};
+    offsets[(size_t)s] = o;
+  }
+  offsets[(size_t)spp] = nt;
+  KT_CUDA(ctx, cudaMemcpyAsync(base, frames.data(), spp * sizeof(kt::Frame), cudaMemcpyHostToDevice,
+                               ctx->stream), "pass frames");
+  KT_CUDA(ctx, cudaMemcpyAsync(base + off_outs, outs.data(), spp * sizeof(kt::OutSoA),
+                               cudaMemcpyHostToDevice, ctx->stream), "pass outputs");
+  KT_CUDA(ctx, cudaMemcpyAsync(base + off_offs, offsets.data(), (spp + 1) * sizeof(uint64_t),
+                               cudaMemcpyHostToDevice, ctx->stream), "pass offsets");
+  kt::BatchRays br;
+  br.frames = (const kt::Frame*)base;
+  br.outs = (const kt::OutSoA*)(base + off_outs);
+  br.offsets = (const uint64_t*)(base + off_offs);
+  br.n_frames = spp;
+  br.refill_min = 1;
+  br.list = nullptr;
+  br.n_dev = nullptr;
+  br.n = nt;
+  // the single-frame launch shapes: 64 x 9 for the exact BL kernels, 128 x 1 otherwise
+  auto variant = [](kt::Mode md) { return (md == kt::kModeBLRk4 || md == kt::kModeBLDopri5) ? 0 : 1; };
+  kt::LaunchShape ls;
+  KT_CUDA(ctx, kt::batch_shape(m, variant(m), ctx->device, &ls), "occupancy query");
+  KT_CUDA(ctx, cudaMemsetAsync(ctx->d_counters, 0, 4 * sizeof(uint32_t), ctx->stream), "reset queue");
+  const kt::Fallback fb = {kt::has_fallback(m) ? ctx->d_fb : nullptr, nullptr, ctx->d_counters + 2};
+  KT_CUDA(ctx, kt::launch_batch(m, variant(m), br, ctx->d_counters, fb, ls, ctx->stream),
+          "trace kernel launch");
+  if (kt::has_fallback(m)) {
+    const kt::Mode bm = kt::fallback_mode(f);
+    kt::LaunchShape bs;
+    KT_CUDA(ctx, kt::batch_shape(bm, variant(bm), ctx->device, &bs), "occupancy query");
+    kt::BatchRays fl = br;
+    fl.list = ctx->d_fb;
+    fl.n_dev = ctx->d_counters + 2;
+    fl.n = 0;
+    KT_CUDA(ctx, kt::launch_batch(bm, variant(bm), fl, ctx->d_counters + 1, fb, bs, ctx->stream),
+            "fallback kernel launch");
+  }
+  const double gamma_eff = cp->gamma < 1e-6 ? 1e-6 : cp->gamma;
+  KT_CUDA(ctx, kt::launch_spp_colorize(cc, (int64_t)n, spp, P, d_bg, bg_w, bg_h, gamma_eff, d_rgb,
+                                       ctx->stream), "supersample colour launch");
   KT_CUDA(ctx, cudaMemcpyAsync(rgb_out_host, d_rgb, 3 * n, cudaMemcpyDeviceToHost, ctx->stream),
           "copy image to host");
   KT_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "render");

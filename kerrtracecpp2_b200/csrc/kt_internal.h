@@ -97,12 +97,15 @@ cudaError_t launch_colorize(const ColourConst& cc, int64_t n, const uint8_t* out
                             const uint8_t* bg,
                             int bg_w, int bg_h, uint8_t* rgb, cudaStream_t stream);
 
-// Camera supersampling over n3 = 3 x pixels channel values: linear-light sum
-// of the passes (first != 0 starts it) and the mean back to 8 bits.
-cudaError_t launch_spp_accumulate(int64_t n3, const uint8_t* rgb, double* acc, double gamma, int first,
-                                  cudaStream_t stream);
-cudaError_t launch_spp_finish(int64_t n3, const double* acc, double inv_n, double gamma, uint8_t* rgb,
-                              cudaStream_t stream);
+// Camera supersampling: the traced passes as [spp][n] arrays, coloured and
+// averaged in linear light into rgb (3 n bytes) by one kernel.
+struct SppPasses {
+  const uint8_t* outcome;
+  const double *r, *red, *magnif, *phi_disk, *th_esc, *ph_esc;
+};
+cudaError_t launch_spp_colorize(const ColourConst& cc, int64_t n, int spp, const SppPasses& P,
+                                const uint8_t* bg, int bg_w, int bg_h, double gamma, uint8_t* rgb,
+                                cudaStream_t stream);
 
 // Mixed-precision kernels (kt_mixed.cu).
 cudaError_t launch_shape_mixed(Mode mode, int device, LaunchShape* shape);

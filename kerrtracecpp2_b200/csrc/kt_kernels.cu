@@ -175,8 +175,24 @@ cudaError_t launch_batch(Mode mode, int variant, const BatchRays& br, uint32_t* 
 
 // ---- colour ------------------------------------------------------------------
 
-// colorize_buffer (main.cpp:1817-1866), blackbody palette.  The reference
-// colours from float32 GeoPixel fields; the same rounding is applied here.
+// One pixel of colorize_buffer (main.cpp:1817-1866), both palettes.  The
+// reference colours from float32 GeoPixel fields; the same rounding is
+// applied here.
+__device__ __forceinline__ void pixel_colour(const ColourConst& cc, int oc, double r, double red,
+                                             double magnif, double phi_disk, double th_esc,
+                                             double ph_esc, const uint8_t* __restrict__ bg, int bg_w,
+                                             int bg_h, uint8_t c[3]) {
+  c[0] = c[1] = c[2] = 0;
+  if (oc == kOutDisk && cc.palette == 1) {
+    disk_colour_interstellar(cc, (double)(float)r, (double)(float)phi_disk, (double)(float)red,
+                             (double)(float)magnif, c);
+  } else if (oc == kOutDisk) {
+    disk_colour(cc, (double)(float)r, (double)(float)red, (double)(float)magnif, c);
+  } else if (oc == kOutEscaped && bg != nullptr) {
+    bg_sample(bg, bg_w, bg_h, (double)(float)th_esc, (double)(float)ph_esc, c);
+  }
+}
+
 __global__ void k_colorize(const ColourConst cc, int64_t n, const uint8_t* __restrict__ outcome,
                            const double* __restrict__ r, const double* __restrict__ red,
                            const double* __restrict__ magnif, const double* __restrict__ phi_disk,
@@ -185,16 +201,9 @@ __global__ void k_colorize(const ColourConst cc, int64_t n, const uint8_t* __res
                            int bg_w, int bg_h, uint8_t* __restrict__ rgb) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
-    uint8_t c[3] = {0, 0, 0};
-    const int oc = outcome[i];
-    if (oc == kOutDisk && cc.palette == 1) {
-      disk_colour_interstellar(cc, (double)(float)r[i], (double)(float)phi_disk[i],
-                               (double)(float)red[i], (double)(float)magnif[i], c);
-    } else if (oc == kOutDisk) {
-      disk_colour(cc, (double)(float)r[i], (double)(float)red[i], (double)(float)magnif[i], c);
-    } else if (oc == kOutEscaped && bg != nullptr) {
-      bg_sample(bg, bg_w, bg_h, (double)(float)th_esc[i], (double)(float)ph_esc[i], c);
-    }
+    uint8_t c[3];
+    pixel_colour(cc, outcome[i], r[i], red[i], magnif[i], phi_disk[i], th_esc[i], ph_esc[i], bg,
+                 bg_w, bg_h, c);
     rgb[3 * i + 0] = c[0];
     rgb[3 * i + 1] = c[1];
     rgb[3 * i + 2] = c[2];
@@ -217,47 +226,48 @@ cudaError_t launch_colorize(const ColourConst& cc, int64_t n, const uint8_t* out
 
 // ---- camera supersampling ------------------------------------------------------
 
-// render_image's camera_spp > 1 branch (main.cpp:2280-2321): each pass's
-// 8-bit image is taken to linear light, pow(clamp(c/255, 0, 1), gamma), and
-// summed in pass order; the sum of the first pass is the value itself.
-__global__ void k_spp_accumulate(int64_t n3, const uint8_t* __restrict__ rgb, double* __restrict__ acc,
-                                 double gamma, int first) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n3;
+// render_image's camera_spp > 1 branch (main.cpp:2280-2321) after all passes
+// are traced: per pixel, the colour of every pass, taken to linear light
+// pow(clamp(c/255, 0, 1), gamma) and summed in pass order (the sum of the
+// first pass is the value itself), then lround(255 pow(clamp(sum/n, 0, 1),
+// 1/gamma)), lround's half-away-from-zero rounding written out for a
+// non-negative value.  The 256 linear values of the 8-bit levels are
+// computed once per block.
+__global__ void k_spp_colorize(const ColourConst cc, int64_t n, int spp, const SppPasses P,
+                               const uint8_t* __restrict__ bg, int bg_w, int bg_h, double gamma,
+                               uint8_t* __restrict__ rgb) {
+  __shared__ double lin[256];
+  for (int c = threadIdx.x; c < 256; c += blockDim.x)
+    lin[c] = ktm_pow(dclamp((double)c / 255.0, 0.0, 1.0), gamma);
+  __syncthreads();
+  const double inv_n = 1.0 / (double)spp;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
-    const double lin = ktm_pow(dclamp((double)rgb[i] / 255.0, 0.0, 1.0), gamma);
-    acc[i] = first ? lin : acc[i] + lin;
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int s = 0; s < spp; ++s) {
+      const int64_t j = (int64_t)s * n + i;
+      uint8_t c[3];
+      pixel_colour(cc, P.outcome[j], P.r[j], P.red[j], P.magnif[j], P.phi_disk[j], P.th_esc[j],
+                   P.ph_esc[j], bg, bg_w, bg_h, c);
+#pragma unroll
+      for (int ch = 0; ch < 3; ++ch) acc[ch] = (s == 0) ? lin[c[ch]] : acc[ch] + lin[c[ch]];
+    }
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch) {
+      const double x = 255.0 * ktm_pow(dclamp(acc[ch] * inv_n, 0.0, 1.0), 1.0 / gamma);
+      const double t = trunc(x);
+      rgb[3 * i + ch] = (uint8_t)(int)((x - t >= 0.5) ? t + 1.0 : t);
+    }
   }
 }
 
-// The mean back to display values: lround(255 pow(clamp(acc / n, 0, 1), 1 / gamma)),
-// lround's half-away-from-zero rounding written out for a non-negative value.
-__global__ void k_spp_finish(int64_t n3, const double* __restrict__ acc, double inv_n, double gamma,
-                             uint8_t* __restrict__ rgb) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n3;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const double x = 255.0 * ktm_pow(dclamp(acc[i] * inv_n, 0.0, 1.0), 1.0 / gamma);
-    const double t = trunc(x);
-    rgb[i] = (uint8_t)(int)((x - t >= 0.5) ? t + 1.0 : t);
-  }
-}
-
-static int elementwise_grid(int64_t n, int block) {
-  int64_t grid = (n + block - 1) / block;
-  if (grid > 148 * 32) grid = 148 * 32;
-  return (int)grid;
-}
-
-cudaError_t launch_spp_accumulate(int64_t n3, const uint8_t* rgb, double* acc, double gamma, int first,
-                                  cudaStream_t stream) {
-  if (n3 <= 0) return cudaSuccess;
-  k_spp_accumulate<<<elementwise_grid(n3, 256), 256, 0, stream>>>(n3, rgb, acc, gamma, first);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_spp_finish(int64_t n3, const double* acc, double inv_n, double gamma, uint8_t* rgb,
-                              cudaStream_t stream) {
-  if (n3 <= 0) return cudaSuccess;
-  k_spp_finish<<<elementwise_grid(n3, 256), 256, 0, stream>>>(n3, acc, inv_n, gamma, rgb);
+cudaError_t launch_spp_colorize(const ColourConst& cc, int64_t n, int spp, const SppPasses& P,
+                                const uint8_t* bg, int bg_w, int bg_h, double gamma, uint8_t* rgb,
+                                cudaStream_t stream) {
+  if (n <= 0) return cudaSuccess;
+  int64_t grid = (n + 255) / 256;
+  if (grid > 148 * 16) grid = 148 * 16;
+  k_spp_colorize<<<(int)grid, 256, 0, stream>>>(cc, n, spp, P, bg, bg_w, bg_h, gamma, rgb);
   return cudaGetLastError();
 }
 
