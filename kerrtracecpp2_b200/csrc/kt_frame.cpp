@@ -20,15 +20,11 @@ namespace kt {
 
 static double delta_r(const Metric& g, double r) { return bl_delta_r(g, r, r * r + g.a2); }
 
-// r_horizon (knds_metric.hpp:237-315): closed form for Lambda = 0, else a
-// 20000-point logarithmic scan of Delta_r with 160-step bisection; for
-// Lambda > 0 the largest root is cosmological and the next one is taken.
-double host_r_horizon(const Metric& g) {
+// The roots of Delta_r for Lambda != 0 as r_horizon finds them
+// (knds_metric.hpp:244-314): a 20000-point logarithmic scan with 160-step
+// bisection; sorted, at most 16.
+static int knds_roots(const Metric& g, double roots[16]) {
   const double M = g.M, a = g.a, Q = g.Q, L = g.L;
-  if (fabs(L) < 1e-15) {
-    const double disc = (M * M - a * a) - Q * Q;
-    return M + sqrt(dmax(disc, 0.0));
-  }
   const double scale = dmax(fabs(M), 1.0);
   const double rmin = dmax(1e-6 * scale, 1e-9);
   double rmax;
@@ -56,7 +52,6 @@ double host_r_horizon(const Metric& g) {
     (void)fhi;
     return 0.5 * (lo + hi);
   };
-  double roots[16];
   int nroots = 0;
   auto push_root = [&](double rr) {
     if (!finite(rr) || rr <= 0.0) return;
@@ -84,13 +79,35 @@ double host_r_horizon(const Metric& g) {
     prev_r = r;
     prev_f = f;
   }
+  std::sort(roots, roots + nroots);
+  return nroots;
+}
+
+// r_horizon (knds_metric.hpp:237-315): closed form for Lambda = 0, else the
+// largest root of Delta_r, or for Lambda > 0 (the largest is cosmological)
+// the next one.
+double host_r_horizon(const Metric& g) {
+  const double M = g.M, a = g.a, Q = g.Q, L = g.L;
+  if (fabs(L) < 1e-15) {
+    const double disc = (M * M - a * a) - Q * Q;
+    return M + sqrt(dmax(disc, 0.0));
+  }
+  double roots[16];
+  const int nroots = knds_roots(g, roots);
   if (nroots == 0) {
     const double disc = (M * M - a * a) - Q * Q;
     return M + sqrt(dmax(disc, 0.0));
   }
-  std::sort(roots, roots + nroots);
   if (L > 0.0 && nroots >= 2) return roots[nroots - 2];
   return roots[nroots - 1];
+}
+
+// The cosmological horizon for Lambda > 0 (the largest root), else +inf.
+double host_r_cosmo(const Metric& g) {
+  if (!(g.L > 0.0) || fabs(g.L) < 1e-15) return ktm_inf();
+  double roots[16];
+  const int nroots = knds_roots(g, roots);
+  return nroots >= 2 ? roots[nroots - 1] : ktm_inf();
 }
 
 // r_isco (knds_metric.hpp:318-349): Bardeen-Press-Teukolsky closed form for
@@ -250,6 +267,14 @@ kt_status prepare_frame(const kt_frame_desc* d, Frame* f, kt_frame_derived* dv, 
   fr.r_fp32 = (d->precision == KT_PREC_MIXED && fr.tol >= 1e-8) ? dmax(4.0 * d->M, 2.0 * rh)
                                                                   : ktm_inf();
   fr.turn_frac = 0.05;
+  // Mixed-precision bundles: rays whose step skipped the horizon and escape
+  // tests (near the equator, no crossing found) and that creep onto a
+  // horizon in BL coordinates -- ingoing within 1e-4 r_+ of r_+, or
+  // outgoing within 1e-4 r_c of the cosmological horizon -- end as a horizon
+  // hit, the record the controller's eventual failure gives them.
+  const bool doom = d->precision == KT_PREC_MIXED && d->bundles;
+  fr.r_doom = doom ? rh * (1.0 + 1e-4) : -ktm_inf();
+  fr.r_cdoom = doom ? host_r_cosmo(fr.g) * (1.0 - 1e-4) : ktm_inf();
   *f = fr;
   if (dv) {
     memset(dv, 0, sizeof *dv);

@@ -9,6 +9,7 @@
 namespace kt {
 
 double host_r_horizon(const Metric& g);
+double host_r_cosmo(const Metric& g);
 double host_r_isco(const Metric& g);
 
 // Validate `d`, apply the reference's fallback rules and clamps, fill the

@@ -40,6 +40,8 @@ struct Frame {
   double bundle_eps;
   double r_fp32;     // mixed precision: FP32 RHS beyond this radius (inf: never)
   double turn_frac;  // mixed precision: FP64 when |p_r| or |p_th|/r < turn_frac |p_t|
+  double r_doom;     // mixed-precision bundles: a ray ingoing below r_doom or
+  double r_cdoom;    // outgoing beyond r_cdoom ends as a horizon hit (+-inf: never)
   int max_steps;
   int chart, intg, bundles;
   int precision;     // KT_PREC_FP64 / KT_PREC_MIXED
@@ -752,6 +754,19 @@ struct Bundle {
           ev = kEvDisk;
         }
       }
+    }
+    if (skip && ((r <= f.r_doom && k1[0] < 0.0) || (r >= f.r_cdoom && k1[0] > 0.0))) {
+      // Mixed precision only (r_doom = -inf, r_cdoom = +inf otherwise): the
+      // step near the equator skipped the horizon and escape tests, and the
+      // ray is ingoing within 1e-4 r_+ of the outer horizon (inside every
+      // photon orbit) or outgoing within 1e-4 r_c of the cosmological one:
+      // it can only creep onto that horizon in BL coordinates, theta frozen,
+      // until the controller gives up, which ends it with the same record
+      // as a horizon hit.
+      o->steps = (uint32_t)it + 1;
+      o->attempts = attempts;
+      set_result(o, kOutEscaped, kStEvent, 0.0, 1.0, 1.0, 0.0, 0.0, 0.0);
+      return true;
     }
     if (!skip) {
       horizon_escape(sp_r, r, f.rh_cut, f.r_esc, &best_alpha, &ev);
