@@ -890,61 +890,40 @@ KT_HD void bundle_hessian(const Metric& g, double r, double th, double pr, doubl
   const double rp = r + e0, rm = r + (-e0);
   const double prp = pr + e2, prm = pr + (-e2);
   const double pthp = pth + e3, pthm = pth + (-e3);
-  // The nine metric points (r + {0,+,-}e0, theta + {0,+,-}e1), one g^{mu nu}
-  // each, in an order in which every entry's terms arrive in the
-  // reference's association order: diagonal (vp - 2 H0) + vm, cross
-  // ((pp - pm) - mp) + mm.  One rolled loop, one bl_inv call site.
-  double H0 = 0.0, d0 = 0.0, d1 = 0.0, d2 = 0.0, d3 = 0.0;
-  double c01 = 0.0, c02 = 0.0, c03 = 0.0, c12 = 0.0, c13 = 0.0, c23 = 0.0;
-  KT_ROLLED
-  for (int q = 0; q < 9; ++q) {
-    // q: 0 (0,0) 1 (+,0) 2 (-,0) 3 (0,+) 4 (0,-) 5 (+,+) 6 (+,-) 7 (-,+) 8 (-,-)
-    const double rr = (q == 1 || q == 5 || q == 6) ? rp : (q == 2 || q == 7 || q == 8) ? rm : r;
-    const int ja = (q == 3 || q == 5 || q == 7) ? 1 : (q == 4 || q == 6 || q == 8) ? 2 : 0;
-    const Ang A = ang_select(ja, A0, Ap, Am);
-    const Inv U = bl_inv(g, rr, A);
-    if (q == 0) {
-      H0 = bl_ham(U, pr, pth, pt, pphi);
-      d2 = (bl_ham(U, prp, pth, pt, pphi) - 2.0 * H0) + bl_ham(U, prm, pth, pt, pphi);
-      d3 = (bl_ham(U, pr, pthp, pt, pphi) - 2.0 * H0) + bl_ham(U, pr, pthm, pt, pphi);
-      c23 = (((bl_ham(U, prp, pthp, pt, pphi) - bl_ham(U, prp, pthm, pt, pphi)) -
-              bl_ham(U, prm, pthp, pt, pphi)) + bl_ham(U, prm, pthm, pt, pphi));
-    } else if (q <= 4) {
-      const double v = bl_ham(U, pr, pth, pt, pphi);
-      const double a2 = bl_ham(U, prp, pth, pt, pphi), b2 = bl_ham(U, prm, pth, pt, pphi);
-      const double a3 = bl_ham(U, pr, pthp, pt, pphi), b3 = bl_ham(U, pr, pthm, pt, pphi);
-      if (q == 1) {
-        d0 = v - 2.0 * H0;
-        c02 = a2 - b2;
-        c03 = a3 - b3;
-      } else if (q == 2) {
-        d0 = d0 + v;
-        c02 = (c02 - a2) + b2;
-        c03 = (c03 - a3) + b3;
-      } else if (q == 3) {
-        d1 = v - 2.0 * H0;
-        c12 = a2 - b2;
-        c13 = a3 - b3;
-      } else {
-        d1 = d1 + v;
-        c12 = (c12 - a2) + b2;
-        c13 = (c13 - a3) + b3;
-      }
-    } else {
-      const double v = bl_ham(U, pr, pth, pt, pphi);
-      c01 = (q == 5) ? v : (q == 8) ? c01 + v : c01 - v;
-    }
-  }
-  Hs[0][0] = d0 / (e0 * e0);
-  Hs[1][1] = d1 / (e1 * e1);
-  Hs[2][2] = d2 / (e2 * e2);
-  Hs[3][3] = d3 / (e3 * e3);
-  Hs[0][1] = Hs[1][0] = c01 / ((4.0 * e0) * e1);
-  Hs[0][2] = Hs[2][0] = c02 / ((4.0 * e0) * e2);
-  Hs[0][3] = Hs[3][0] = c03 / ((4.0 * e0) * e3);
-  Hs[1][2] = Hs[2][1] = c12 / ((4.0 * e1) * e2);
-  Hs[1][3] = Hs[3][1] = c13 / ((4.0 * e1) * e3);
-  Hs[2][3] = Hs[3][2] = c23 / ((4.0 * e2) * e3);
+  // g^{mu nu} at (r + {0,+,-}e0, theta + {0,+,-}e1)
+  const Inv U00 = bl_inv(g, r, A0), Up0 = bl_inv(g, rp, A0), Um0 = bl_inv(g, rm, A0);
+  const Inv U0p = bl_inv(g, r, Ap), U0m = bl_inv(g, r, Am);
+  const Inv Upp = bl_inv(g, rp, Ap), Upm = bl_inv(g, rp, Am);
+  const Inv Ump = bl_inv(g, rm, Ap), Umm = bl_inv(g, rm, Am);
+  const double H0 = bl_ham(U00, pr, pth, pt, pphi);
+  const double e[4] = {e0, e1, e2, e3};
+  double vp[4], vm[4];
+  vp[0] = bl_ham(Up0, pr, pth, pt, pphi);
+  vm[0] = bl_ham(Um0, pr, pth, pt, pphi);
+  vp[1] = bl_ham(U0p, pr, pth, pt, pphi);
+  vm[1] = bl_ham(U0m, pr, pth, pt, pphi);
+  vp[2] = bl_ham(U00, prp, pth, pt, pphi);
+  vm[2] = bl_ham(U00, prm, pth, pt, pphi);
+  vp[3] = bl_ham(U00, pr, pthp, pt, pphi);
+  vm[3] = bl_ham(U00, pr, pthm, pt, pphi);
+#pragma unroll
+  for (int a = 0; a < 4; ++a) Hs[a][a] = ((vp[a] - 2.0 * H0) + vm[a]) / (e[a] * e[a]);
+  // cross(a,b) = (pp - pm - mp + mm) / (4 e_a e_b)
+#define KT_CROSS(a, b, pp, pm, mp, mm) \
+  Hs[a][b] = Hs[b][a] = ((((pp) - (pm)) - (mp)) + (mm)) / ((4.0 * e[a]) * e[b])
+  KT_CROSS(0, 1, bl_ham(Upp, pr, pth, pt, pphi), bl_ham(Upm, pr, pth, pt, pphi),
+           bl_ham(Ump, pr, pth, pt, pphi), bl_ham(Umm, pr, pth, pt, pphi));
+  KT_CROSS(0, 2, bl_ham(Up0, prp, pth, pt, pphi), bl_ham(Up0, prm, pth, pt, pphi),
+           bl_ham(Um0, prp, pth, pt, pphi), bl_ham(Um0, prm, pth, pt, pphi));
+  KT_CROSS(0, 3, bl_ham(Up0, pr, pthp, pt, pphi), bl_ham(Up0, pr, pthm, pt, pphi),
+           bl_ham(Um0, pr, pthp, pt, pphi), bl_ham(Um0, pr, pthm, pt, pphi));
+  KT_CROSS(1, 2, bl_ham(U0p, prp, pth, pt, pphi), bl_ham(U0p, prm, pth, pt, pphi),
+           bl_ham(U0m, prp, pth, pt, pphi), bl_ham(U0m, prm, pth, pt, pphi));
+  KT_CROSS(1, 3, bl_ham(U0p, pr, pthp, pt, pphi), bl_ham(U0p, pr, pthm, pt, pphi),
+           bl_ham(U0m, pr, pthp, pt, pphi), bl_ham(U0m, pr, pthm, pt, pphi));
+  KT_CROSS(2, 3, bl_ham(U00, prp, pthp, pt, pphi), bl_ham(U00, prp, pthm, pt, pphi),
+           bl_ham(U00, prm, pthp, pt, pphi), bl_ham(U00, prm, pthm, pt, pphi));
+#undef KT_CROSS
 }
 
 // bundle_rhs (ray_bundle.hpp:130-156): geodesic RHS (k[0..4] as bl_rhs) and
