@@ -265,13 +265,15 @@ typedef struct kt_batch kt_batch;
 typedef struct kt_batch_options {
   uint32_t flags;          /* KT_BATCH_AUTOTUNE */
   int32_t variant;         /* -1: per-mode default; else 0..KT_BATCH_VARIANTS-1 */
-  int32_t refill_min;      /* 0: 1 (refill as soon as one lane is idle); 1..32 */
+  int32_t refill_min;      /* 0: per-mode default (the single-frame kernels' threshold:
+                              16 for bundles, 1 for the separable tracer, 32 otherwise);
+                              1..32: idle lanes of a warp take new rays once this many are idle */
   int32_t tune_reps;       /* timed repetitions per candidate (>= 1) */
   double tune_fraction;    /* share of a group's rays in the tuning sample, (0, 1] */
 } kt_batch_options;
 
 typedef struct kt_batch_group_info {
-  int32_t kernel;          /* 0 BL RK4, 1 BL DOPRI5, 2 KS RK4, 3 bundles, 4-7 mixed BL RK4 / BL DOPRI5 / KS RK4 / bundles */
+  int32_t kernel;          /* 0 BL RK4, 1 BL DOPRI5, 2 KS RK4, 3 bundles, 4-7 mixed BL RK4 / BL DOPRI5 / KS RK4 / bundles, 8 separable Kerr */
   int32_t n_frames;
   uint64_t n_rays;
   int32_t variant;

@@ -117,7 +117,7 @@ class BatchGroupInfo(ctypes.Structure):
 
 # Kernel of a batch group (kt_batch_group_info.kernel).
 BATCH_KERNELS = ["bl_rk4", "bl_dopri5", "ks_rk4", "bundles", "bl_rk4_mixed", "bl_dopri5_mixed",
-                 "ks_rk4_mixed", "bundles_mixed"]
+                 "ks_rk4_mixed", "bundles_mixed", "separable_kerr"]
 
 
 def batch_options(autotune=False, **kw):

@@ -28,7 +28,7 @@ using namespace ktc;
 namespace {
 
 constexpr uint32_t kSampleRun = 256;     // neighbouring rays per tuning run
-constexpr int kRefillCandidates[] = {1, 8, 16, 24};
+constexpr int kRefillCandidates[] = {1, 16, 24, 32};
 constexpr uint64_t kMaxGroupRays = 1ull << 31;
 static_assert(KT_BATCH_VARIANTS == kt::kBatchVariants, "variant count of the ABI");
 
@@ -51,9 +51,14 @@ struct Group {
 };
 
 int default_variant(kt::Mode m) {
-  // The single-frame launch shapes: 64 x 9 for the exact BL kernels, 128 x 1
-  // for the others.
-  return (m == kt::kModeBLRk4 || m == kt::kModeBLDopri5) ? 0 : 1;
+  // The single-frame launch shapes (kt_kernels.cu, kt_mixed.cu): 128 x 1
+  // for the bundle and separable-Kerr kernels, 64 x 9 for the others.
+  return (m == kt::kModeBundle || m == kt::kModeBundleMixed || m == kt::kModeSepRk4) ? 1 : 0;
+}
+
+int default_refill(kt::Mode m) {
+  // ... and their refill thresholds
+  return m == kt::kModeBundle ? 16 : m == kt::kModeSepRk4 ? 1 : 32;
 }
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -342,7 +347,7 @@ kt_status kt_batch_create(kt_context* ctx, const kt_frame_desc* descs, const kt_
       KT_CUDA(ctx, kt::batch_shape(g.fb_mode, g.fb_variant, ctx->device, &g.fb_shape), "occupancy query");
     }
     g.variant = opt.variant >= 0 ? opt.variant : default_variant(g.mode);
-    g.refill_min = opt.refill_min > 0 ? opt.refill_min : 1;
+    g.refill_min = opt.refill_min > 0 ? opt.refill_min : default_refill(g.mode);
     if (opt.flags & KT_BATCH_AUTOTUNE) {
       kt_status r = tune_group(ctx, g, opt);
       if (r != KT_OK) return r;

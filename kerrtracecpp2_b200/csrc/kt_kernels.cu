@@ -115,13 +115,19 @@ struct ModeSepRk4 {
 
 template <> struct Defers<ModeSepRk4> { static constexpr bool value = true; };
 
-// Launch shape per mode, measured on B200 (720p KNdS frame, BL chart; 512^2
-// Kerr-Newman frame, KS chart; 480x270 bundle frame): the BL single-ray
-// kernels run best as 64-thread blocks capped at 113 registers (9 blocks =
-// 18 warps per SM, limited by the 46 KB of ray machines per 128 threads);
-// the KS and bundle kernels spill under that cap and keep 128 threads.
-template <> struct Shape<struct ModeBLRk4> { static constexpr int kBlock = 64, kMinBlocks = 9; };
-template <> struct Shape<struct ModeBLDopri5> { static constexpr int kBlock = 64, kMinBlocks = 9; };
+// Launch shape per mode, measured on B200 (720p config-2 frame, BL chart
+// DOPRI5 and RK4; 720p Kerr KS frame; 1080p config-3 bundles): the BL and KS
+// single-ray kernels run best as 64-thread blocks capped at 113 registers
+// (9 blocks per SM), the bundle kernel as 128-thread blocks.  Refilling a
+// warp only once all its lanes are idle (kRefill 32) keeps the 32 rays of a
+// warp neighbouring pixels that start together: the camera set-up and the
+// first slots run converged and the rays' step sequences stay alike, which
+// outweighs the lanes idling at the end of each group of 32 (KS: 62 against
+// 73 ms, BL RK4: 66 against 68, DOPRI5: equal; bundles best at 16).
+template <> struct Shape<struct ModeBLRk4> { static constexpr int kBlock = 64, kMinBlocks = 9, kRefill = 32; };
+template <> struct Shape<struct ModeBLDopri5> { static constexpr int kBlock = 64, kMinBlocks = 9, kRefill = 32; };
+template <> struct Shape<struct ModeKSRk4> { static constexpr int kBlock = 64, kMinBlocks = 9, kRefill = 32; };
+template <> struct Shape<struct ModeBundle> { static constexpr int kBlock = 128, kMinBlocks = 1, kRefill = 16; };
 
 cudaError_t launch_shape(Mode mode, int device, LaunchShape* shape) {
   if (is_mixed_mode(mode)) return launch_shape_mixed(mode, device, shape);

@@ -136,7 +136,6 @@ KT_HD void horizon_escape(double r_prev, double r_now, double rh_cut, double r_e
 struct BLBase {
   double r, th, ph, pr, pth, pt, pphi;  // GeodesicState
   double h;                             // dlam
-  double k1[5];                         // f(s) = {dr, dth, dpr, dpth, dphi}
   double step_used;
   int it, rejects;
   uint32_t attempts;
@@ -161,10 +160,10 @@ struct BLBase {
   KT_HD bool needs_k1() const { return need_k1; }
 
   // Events of trace_single (main.cpp:364-433) for the accepted step
-  // (sp_*) -> (current state), with f at both ends.  Returns true when the
-  // ray stops.
+  // (sp_*) -> (current state), with f at both ends (k0_*, k1_*: dr and
+  // dtheta).  Returns true when the ray stops.
   KT_HD bool events(const Frame& f, double sp_r, double sp_th, double sp_ph, double k0_r,
-                    double k0_th, RayResult* o) {
+                    double k0_th, double k1_r, double k1_th, RayResult* o) {
     double best_alpha = 2.0;
     int ev = kEvNone;
     double disk_r = 0.0, disk_red = 1.0, disk_phi = 0.0;
@@ -172,8 +171,8 @@ struct BLBase {
     const double q1 = th - kHalfPi;
     if (sign_change(q0, q1) || (dmin(fabs(q0), fabs(q1)) < 0.35)) {
       double alpha = 0.0;
-      if (first_event(sp_th, th, k0_th, k1[1], step_used, kHalfPi, &alpha)) {
-        const double r_hit = hermite(sp_r, r, k0_r, k1[0], step_used, alpha);
+      if (first_event(sp_th, th, k0_th, k1_th, step_used, kHalfPi, &alpha)) {
+        const double r_hit = hermite(sp_r, r, k0_r, k1_r, step_used, alpha);
         if (r_hit >= f.r_in && r_hit <= f.r_out) {
           disk_r = r_hit;
           disk_red = dclamp(disk_redshift(f.g, f.eq, r_hit, pt, pphi), 0.0, 20.0);
@@ -234,6 +233,7 @@ KT_HD double doubling_coeff(int slot, double h) {
 // RK4 step doubling (rk4_adaptive, geodesic.hpp:204-257), kSlots = 10.
 struct BLRk4 : BLBase {
   static constexpr int kSlots = 10;
+  double k1[5];  // f(s) = {dr, dth, dpr, dpth, dphi}
   double sum[5];
   double kp[4];
   double A[4];   // path A result (r, th, pr, pth); after acceptance: s_prev
@@ -271,7 +271,7 @@ struct BLRk4 : BLBase {
       need_k1 = false;
       if (!pending) return false;
       pending = false;
-      if (events(f, A[0], A[1], sp_ph, kp[0], kp[1], o)) return true;
+      if (events(f, A[0], A[1], sp_ph, kp[0], kp[1], k1[0], k1[1], o)) return true;
       return next_step(f, o);
     }
     switch (slot) {
@@ -437,9 +437,7 @@ struct BLDopri5 : BLBase {
       pr = y5[2];
       pth = y5[3];
       for (int i = 0; i < 4; ++i) kk[0][i] = kk[6][i];  // FSAL
-      k1[0] = kk[0][0];
-      k1[1] = kk[0][1];
-      if (events(f, sp_r, sp_th, ph, k0_r, k0_th, o)) return true;
+      if (events(f, sp_r, sp_th, ph, k0_r, k0_th, kk[0][0], kk[0][1], o)) return true;
       return next_step(f, o);
     } else {
       double hnew = (h * 0.9) * ktm_pow(1.0 / err, 0.25);

@@ -110,6 +110,17 @@ struct ModeBundleMixed {
   }
 };
 
+// Launch shapes, measured on B200 as for the exact kernels: refilling a
+// warp only when all 32 lanes are idle matters more here, since the FP32/FP64
+// choice is made per warp and a warp of neighbouring rays that started
+// together makes it alike (720p config 2 DOPRI5: 24.3 against 31.9 ms; BL
+// RK4: 25.2 against 41.1; KS RK4: 22.3 against 52.1; 1080p bundles: 224
+// against 243).
+template <> struct Shape<ModeBLRk4Mixed> { static constexpr int kBlock = 64, kMinBlocks = 9, kRefill = 32; };
+template <> struct Shape<ModeBLDopri5Mixed> { static constexpr int kBlock = 64, kMinBlocks = 9, kRefill = 32; };
+template <> struct Shape<ModeKSRk4Mixed> { static constexpr int kBlock = 64, kMinBlocks = 9, kRefill = 32; };
+template <> struct Shape<ModeBundleMixed> { static constexpr int kBlock = 128, kMinBlocks = 1, kRefill = 32; };
+
 template <class ModeT>
 static cudaError_t launch_one(const Frame& f, const OutSoA& out, const RayList& rl,
                               uint32_t* queue, const Fallback& fb, const LaunchShape& s,

@@ -65,9 +65,12 @@ constexpr size_t smem_bytes(int block) {
 // fallback list: RayResult::outcome < 0); specialised where that happens.
 template <class ModeT> struct Defers { static constexpr bool value = false; };
 
-// Launch shape per mode: 128-thread blocks by default; a mode may
+// Launch shape per mode: threads per block, minimum resident blocks (the
+// register cap) and the refill threshold -- idle lanes of a warp take new
+// rays only when at least kRefill lanes are idle (or the warp is empty).
+// 128-thread blocks and refill at every idle lane by default; a mode may
 // specialise this (see kt_kernels.cu, kt_mixed.cu).
-template <class ModeT> struct Shape { static constexpr int kBlock = 128, kMinBlocks = 1; };
+template <class ModeT> struct Shape { static constexpr int kBlock = 128, kMinBlocks = 1, kRefill = 1; };
 // ---- the persistent loop ---------------------------------------------------
 // One iteration of the outer loop is one adaptive attempt for every ray of
 // the warp.  At its start, idle lanes take new rays from the queue (one
@@ -92,7 +95,8 @@ __global__ void __launch_bounds__(Shape<ModeT>::kBlock, Shape<ModeT>::kMinBlocks
   for (;;) {
     if (!exhausted) {
       const unsigned need = __ballot_sync(kFull, !active);
-      if (need) {
+      if (need && (Shape<ModeT>::kRefill <= 1 || need == kFull ||
+                   __popc(need) >= Shape<ModeT>::kRefill)) {
         const int leader = __ffs(need) - 1;
         const unsigned cnt = (unsigned)__popc(need);
         unsigned base = 0;
