@@ -1,8 +1,11 @@
 // kt_adjoint.cu -- kernels of the smooth tracer (KT_PREC_SMOOTH) and of its
 // discrete adjoint (kt_vjp, kt_l2_grad).
 //
-// One thread per ray, rays from a device queue (persistent grid), one kernel
-// per chart (a kernel with both charts' code overflowed the instruction
+// One thread per ray, rays from a device queue (persistent grid) in groups
+// of 32 consecutive rays per warp (a warp takes the next group once all its
+// lanes are done: neighbouring rays follow alike paths, so the warp's lanes
+// stay converged far longer than with rays taken one lane at a time), one
+// kernel per chart (a kernel with both charts' code overflowed the instruction
 // cache: most issue slots went to instruction-fetch stalls).  The
 // gradient kernel traces its ray with checkpoints in local memory
 // (SmScratch, ~12 KB per thread), and for a disk hit with a non-zero
@@ -36,21 +39,27 @@ __global__ void __launch_bounds__(kSmBlock) k_smooth(const Frame f, const OutSoA
                                                      uint32_t* __restrict__ fb_n) {
   SmScratch sc;
   const uint32_t count = n_dev ? *n_dev : (list ? n_list : n);
+  const unsigned lane = threadIdx.x & 31u;
   KT_ROLLED
   for (;;) {
-    const uint32_t i = atomicAdd(queue, 1u);
-    if (i >= count) break;
-    const uint32_t pix = list ? list[i] : i;
-    if (pix >= n) continue;  // a caller's list with an index outside the frame
-    RayResult o;
-    double g[kGSlots];
-    if (!sm_pixel<C, kGrad>(f, pix, job.cot, &o, g, kGrad ? &sc : nullptr)) {
-      fb_pix[atomicAdd(fb_n, 1u)] = pix;
-      continue;
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(queue, 32u);
+    base = __shfl_sync(kFull, base, 0);
+    if (base >= count) break;
+    const uint32_t i = base + lane;
+    const uint32_t pix = i < count ? (list ? list[i] : i) : n;
+    if (pix < n) {  // else past the end, or a caller's list index outside the frame
+      RayResult o;
+      double g[kGSlots];
+      if (!sm_pixel<C, kGrad>(f, pix, job.cot, &o, g, kGrad ? &sc : nullptr)) {
+        fb_pix[atomicAdd(fb_n, 1u)] = pix;
+      } else {
+        if (out.outcome) write_result(out, pix, o);
+        if (kGrad)
+          for (int q = 0; q < kGSlots; ++q) job.contrib[(size_t)q * n + pix] = g[q];
+      }
     }
-    if (out.outcome) write_result(out, pix, o);
-    if (kGrad)
-      for (int q = 0; q < kGSlots; ++q) job.contrib[(size_t)q * n + pix] = g[q];
+    __syncwarp();
   }
 }
 
@@ -65,20 +74,26 @@ __global__ void __launch_bounds__(kSmBlock) k_smooth_tangent(const Frame f, cons
                                                              uint32_t* __restrict__ fb_pix,
                                                              uint32_t* __restrict__ fb_n) {
   const uint32_t count = n_dev ? *n_dev : (list ? n_list : n);
+  const unsigned lane = threadIdx.x & 31u;
   KT_ROLLED
   for (;;) {
-    const uint32_t i = atomicAdd(queue, 1u);
-    if (i >= count) break;
-    const uint32_t pix = list ? list[i] : i;
-    if (pix >= n) continue;  // a caller's list with an index outside the frame
-    RayResult o;
-    double g[kGSlots];
-    if (!sm_pixel_tangent<C>(f, pix, job.tangent_dir, job.cot, &o, g)) {
-      fb_pix[atomicAdd(fb_n, 1u)] = pix;
-      continue;
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(queue, 32u);
+    base = __shfl_sync(kFull, base, 0);
+    if (base >= count) break;
+    const uint32_t i = base + lane;
+    const uint32_t pix = i < count ? (list ? list[i] : i) : n;
+    if (pix < n) {
+      RayResult o;
+      double g[kGSlots];
+      if (!sm_pixel_tangent<C>(f, pix, job.tangent_dir, job.cot, &o, g)) {
+        fb_pix[atomicAdd(fb_n, 1u)] = pix;
+      } else {
+        if (out.outcome) write_result(out, pix, o);
+        for (int q = 0; q < kGSlots; ++q) job.contrib[(size_t)q * n + pix] = g[q];
+      }
     }
-    if (out.outcome) write_result(out, pix, o);
-    for (int q = 0; q < kGSlots; ++q) job.contrib[(size_t)q * n + pix] = g[q];
+    __syncwarp();
   }
 }
 
