@@ -2,8 +2,8 @@
 KT_PREC_SMOOTH, kt_vjp, kt_l2_grad): bit-identical to the host build of the
 same code (smooth_lib), and on config 5 (512x512 KS, a=0.7, Q=0.1,
 theta=70, r_obs=50, disk ISCO-15, L2 loss against the same tracer at a=0.72,
-theta=71) the gradient against central differences with h = 1e-6 of the
-loss restricted to the pixels on which every stencil is smooth (see
+theta=71) the gradient against five-point central differences of the loss
+restricted to the pixels on which every stencil is smooth (see
 test_smooth.py)."""
 import numpy as np
 import pytest
@@ -70,8 +70,14 @@ def test_vjp_gpu_equals_host(renderer, kw):
 def test_config5_l2_gradient_against_central_differences(renderer):
     """512x512, tol 1e-7: kt_l2_grad's loss equals the loss of its own
     forward, and the VJP with the loss's cotangents on the smooth pixels
-    agrees with central differences (h = 1e-6; theta in radians) of that
-    loss to 1e-4 relative; the measured agreement is printed."""
+    agrees with central differences of that loss to 1e-5 relative.  The
+    differences use the five-point stencil with h = 1e-4 (theta in radians;
+    Lambda: 1e-6), where the stencil's rounding noise (~1e-10 in r_hit over
+    2h) is far below the derivative; a pixel counts as smooth when every
+    stencil render keeps its class, step and attempt counts, its g and r_hit
+    have small second differences and their central differences over h and
+    2h agree (no kink in the first derivative).  The two-point differences
+    at the same h are printed beside them."""
     import torch
 
     base = dict(CFG5, width=512, height=512)
@@ -88,21 +94,27 @@ def test_config5_l2_gradient_against_central_differences(renderer):
     assert loss == pytest.approx(want_loss, rel=1e-12)
     assert st["grad_pixels"] == m_all.sum()
 
-    h = 1e-6
-    steps = {"a": h, "Q": h, "Lambda": 1e-7, "theta_deg": np.degrees(h), "r_obs": h}
+    h = 1e-4
+    steps = {"a": h, "Q": h, "Lambda": 1e-6, "theta_deg": np.degrees(h), "r_obs": h}
     bl0 = smooth_gpu(renderer, dict(base, chart=1))
     ok = m_all.copy()
     renders = {}
     for k, hk in steps.items():
         o0 = bl0 if k == "Lambda" else b0
-        op = smooth_gpu(renderer, dict(base, **{k: base[k] + hk}))
-        om = smooth_gpu(renderer, dict(base, **{k: base[k] - hk}))
-        renders[k] = (op, om, hk)
-        ok &= (o0["outcome"] == 1) & (op["outcome"] == 1) & (om["outcome"] == 1)
-        for f in ("steps", "attempts"):
-            ok &= (op[f] == o0[f]) & (om[f] == o0[f])
+        rs = {j: smooth_gpu(renderer, dict(base, **{k: base[k] + j * hk})) for j in (-2, -1, 1, 2)}
+        renders[k] = (rs, hk)
+        for o in rs.values():
+            ok &= (o0["outcome"] == 1) & (o["outcome"] == 1)
+            for f in ("steps", "attempts"):
+                ok &= o[f] == o0[f]
         for f in ("redshift", "r"):
-            ok &= np.abs(op[f] - 2 * o0[f] + om[f]) <= 1e-8 + 0.01 * np.abs(op[f] - om[f])
+            for j in (1, 2):
+                op, om = rs[j][f], rs[-j][f]
+                ok &= np.abs(op - 2 * o0[f] + om) <= 1e-8 + 0.01 * np.abs(op - om)
+            # the first derivative itself smooth on [-2h, 2h]: the two
+            # central differences agree to O(h^2)
+            d1, d2 = rs[1][f] - rs[-1][f], rs[2][f] - rs[-2][f]
+            ok &= np.abs(d2 - 2 * d1) <= 1e-12 + 1e-4 * np.abs(d1)
 
     def loss_on(o):
         return np.sum(wg * (o["redshift"][ok] - tgt["redshift"][ok]) ** 2 +
@@ -117,13 +129,16 @@ def test_config5_l2_gradient_against_central_differences(renderer):
     gl, _ = renderer.vjp(abi.frame_desc(**dict(base, chart=1)), *cot(bl0))
     adj = {"a": g[0], "Q": g[1], "Lambda": gl[2], "theta_deg": g[3], "r_obs": g[4]}
     worst = 0.0
-    for k, (op, om, hk) in renders.items():
-        fd = (loss_on(op) - loss_on(om)) / (2 * hk)
-        rel = abs(adj[k] - fd) / abs(fd)
+    for k, (rs, hk) in renders.items():
+        L = {j: loss_on(o) for j, o in rs.items()}
+        fd2 = (L[1] - L[-1]) / (2 * hk)
+        fd4 = (L[-2] - 8 * L[-1] + 8 * L[1] - L[2]) / (12 * hk)
+        rel = abs(adj[k] - fd4) / abs(fd4)
         worst = max(worst, rel)
-        print(f"{k}: adjoint {adj[k]:.10g} central difference {fd:.10g} rel {rel:.2e}")
+        print(f"{k}: adjoint {adj[k]:.10g} five-point {fd4:.10g} rel {rel:.2e} "
+              f"(two-point rel {abs(adj[k] - fd2) / abs(fd2):.2e})")
     print(f"smooth pixels {ok.sum()} of {m_all.sum()} disk pixels; worst rel {worst:.2e}")
-    assert worst <= 1e-4
+    assert worst <= 1e-5
     assert grad_l2[abi.GRAD_NAMES.index("disk_out")] == 0.0
 
 
