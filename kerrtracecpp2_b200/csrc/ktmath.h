@@ -452,4 +452,40 @@ KTM_FN double ktm_acos(double x) {
   return 2.0 * ktm_atan2(sqrt(1.0 - x), sqrt(1.0 + x));
 }
 
+/* atan(x) = atan2(x, 1): |x| <= 1 reduces to atan01(|x|) exactly. */
+KTM_FN double ktm_atan(double x) { return ktm_atan2(x, 1.0); }
+
+/* asin(x) = atan2(x, sqrt((1 - x)(1 + x))); 1 - x is exact for x >= 1/2. */
+KTM_FN double ktm_asin(double x) {
+  if (ktm_isnan(x)) return x;
+  if (fabs(x) > 1.0) return ktm_nan();
+  return ktm_atan2(x, sqrt((1.0 - x) * (1.0 + x)));
+}
+
+/* hypot(x, y) = sqrt(x^2 + y^2) without overflow or underflow: both scaled
+ * by a power of two that brings the larger into [1, 2), the sum of squares
+ * in double-double, one Newton correction of its square root. */
+KTM_FN double ktm_hypot(double x, double y) {
+  double a = fabs(x), b = fabs(y);
+  if (ktm_isinf(a) || ktm_isinf(b)) return ktm_inf();
+  if (ktm_isnan(a) || ktm_isnan(b)) return a + b;
+  if (a < b) {
+    const double t = a;
+    a = b;
+    b = t;
+  }
+  if (b == 0.0) return a;
+  const int e = (int)((ktm_bits(a) >> 52) & 0x7ff) - 1023;
+  const int k = e < -1000 ? -1000 : e;  /* subnormal a: a moderate scale is enough */
+  a = ktm_scale(a, -k);
+  b = ktm_scale(b, -k);
+  const double h = a * a, hl = fma(a, a, -h);
+  const double q = b * b, ql = fma(b, b, -q);
+  const double s = h + q;
+  const double sl = ((h - s) + q) + (hl + ql);
+  double r = sqrt(s);
+  r = r + (fma(-r, r, s) + sl) / (2.0 * r);
+  return ktm_scale(r, k);
+}
+
 #endif /* KTMATH_H */

@@ -12,3 +12,6 @@ double kts_pow(double x, double y) { return ktm_pow(x, y); }
 double kts_cbrt(double x) { return ktm_cbrt(x); }
 double kts_atan2(double y, double x) { return ktm_atan2(y, x); }
 double kts_acos(double x) { return ktm_acos(x); }
+double kts_atan(double x) { return ktm_atan(x); }
+double kts_asin(double x) { return ktm_asin(x); }
+double kts_hypot(double x, double y) { return ktm_hypot(x, y); }

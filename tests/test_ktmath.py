@@ -15,10 +15,10 @@ mpmath.mp.prec = 120
 @pytest.fixture(scope="module")
 def L():
     lib = ctypes.CDLL(testlibs.SHIM)
-    for n in ("sin", "cos", "exp", "log", "log10", "cbrt", "acos"):
+    for n in ("sin", "cos", "exp", "log", "log10", "cbrt", "acos", "atan", "asin"):
         f = getattr(lib, "kts_" + n)
         f.restype, f.argtypes = ctypes.c_double, [ctypes.c_double]
-    for n in ("pow", "atan2"):
+    for n in ("pow", "atan2", "hypot"):
         f = getattr(lib, "kts_" + n)
         f.restype, f.argtypes = ctypes.c_double, [ctypes.c_double] * 2
     return lib
@@ -29,7 +29,7 @@ def ulp_err(got, exact):
     if exact == 0:
         return 0.0 if got == 0 else float("inf")
     e = math.frexp(float(exact))[1]
-    return float(abs(mpmath.mpf(got) - exact) / mpmath.mpf(2) ** (e - 53))
+    return float(abs(mpmath.mpf(got) - exact) / mpmath.mpf(2) ** max(e - 53, -1074))  # subnormal spacing
 
 
 CASES = [
@@ -43,6 +43,13 @@ CASES = [
     ("cbrt", mpmath.cbrt, lambda r: (math.exp(r.uniform(-50, 50)),), 0.6),
     ("atan2", mpmath.atan2, lambda r: (r.uniform(-10, 10), r.uniform(-10, 10)), 2.0),
     ("acos", mpmath.acos, lambda r: (r.uniform(-1, 1),), 2.0),
+    ("atan", mpmath.atan, lambda r: (r.uniform(-50, 50),), 2.0),
+    ("atan", mpmath.atan, lambda r: (r.uniform(-1, 1),), 2.0),
+    ("asin", mpmath.asin, lambda r: (r.uniform(-1, 1),), 2.0),
+    ("asin", mpmath.asin, lambda r: (1.0 - math.exp(r.uniform(-30, -1)),), 2.0),
+    ("hypot", lambda x, y: mpmath.sqrt(x * x + y * y), lambda r: (r.uniform(-10, 10), r.uniform(-10, 10)), 1.0),
+    ("hypot", lambda x, y: mpmath.sqrt(x * x + y * y),
+     lambda r: (math.ldexp(r.uniform(1, 2), r.randint(-1070, 1020)), math.ldexp(r.uniform(1, 2), r.randint(-1070, 1020))), 1.0),
 ]
 
 
@@ -73,6 +80,13 @@ def test_special_values(L):
     assert L.kts_cbrt(-27.0) == -3.0
     assert L.kts_acos(1.0) == 0.0
     assert math.isnan(L.kts_acos(1.5))
+    assert L.kts_asin(1.0) == math.pi / 2 and L.kts_asin(-0.0) == 0.0
+    assert math.isnan(L.kts_asin(1.5))
+    assert L.kts_atan(math.inf) == math.pi / 2 and L.kts_atan(0.0) == 0.0
+    assert L.kts_hypot(3.0, 4.0) == 5.0 and L.kts_hypot(-0.0, 2.5) == 2.5
+    assert L.kts_hypot(math.inf, math.nan) == math.inf
+    assert L.kts_hypot(1e308, 1e308) == pytest.approx(math.sqrt(2) * 1e308, rel=1e-15)
+    assert L.kts_hypot(3e-320, 4e-320) == pytest.approx(5e-320, rel=1e-3)
 
 
 def test_exact_points(L):
