@@ -35,7 +35,7 @@ CXX_SOURCES = ["kt_frame.cpp", "kt_api.cpp", "kt_batch.cpp", "kt_grad.cpp", "kt_
                "kt_compat.cpp"]
 HEADERS = ["ktmath.h", "ktmath_consts.h", "kt_physics.cuh", "kt_machines.cuh", "kt_internal.h",
            "kt_frame.h", "kt_context.h", "kt_trace_kernel.cuh", "kt_dual.cuh", "kt_smooth.cuh",
-           "kt_smray.cuh", "kt_adjoint.h"]
+           "kt_smray.cuh", "kt_adjoint.h", "kt_elliptic.cuh"]
 # Per-file compile flags: the exact kernels keep every multiply and add of
 # the reference's arithmetic separate; the mixed-precision kernels are not
 # compared bit for bit and use FMA contraction.

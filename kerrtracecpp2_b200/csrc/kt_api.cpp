@@ -67,6 +67,8 @@ kt_status run_trace(kt_context* ctx, const kt::Frame& f, const kt::OutSoA& out,
     KT_CUDA(ctx, kt::launch_trace(bm, f, out, fl, ctx->d_counters + 1, fb, bs, st),
             "fallback kernel launch");
   }
+  if (f.solver == KT_SOLVER_ELLIPTIC_CLOSED)
+    KT_CUDA(ctx, kt::launch_elliptic(f, out, rl, st), "elliptic kernel launch");
   return KT_OK;
 }
 
@@ -470,6 +472,12 @@ kt_status kt_render_spp_host(kt_context* ctx, const kt_frame_desc* desc, const k
     fl.n = 0;
     KT_CUDA(ctx, kt::launch_batch(bm, variant(bm), fl, ctx->d_counters + 1, fb, bs, ctx->stream),
             "fallback kernel launch");
+  }
+  if (f.solver == KT_SOLVER_ELLIPTIC_CLOSED) {
+    const kt::RayList all = {nullptr, nullptr, nullptr, (uint32_t)n};
+    for (int s = 0; s < spp; ++s)
+      KT_CUDA(ctx, kt::launch_elliptic(frames[(size_t)s], outs[(size_t)s], all, ctx->stream),
+              "elliptic kernel launch");
   }
   const double gamma_eff = cp->gamma < 1e-6 ? 1e-6 : cp->gamma;
   KT_CUDA(ctx, kt::launch_spp_colorize(cc, (int64_t)n, spp, P, d_bg, bg_w, bg_h, gamma_eff, d_rgb,

@@ -276,6 +276,9 @@ kt_status kt_batch_create(kt_context* ctx, const kt_frame_desc* descs, const kt_
       ctx->err = "frame " + std::to_string(i) + ": " + ctx->err;
       return r;
     }
+    if (frames[i].solver == KT_SOLVER_ELLIPTIC_CLOSED)
+      return fail(ctx, KT_ERR_UNSUPPORTED,
+                  "frame " + std::to_string(i) + ": the elliptic-closed solver does not run in batches");
     if (frames[i].precision == KT_PREC_SMOOTH)
       return fail(ctx, KT_ERR_UNSUPPORTED,
                   "frame " + std::to_string(i) + ": the smooth tracer does not run in batches");

@@ -225,12 +225,8 @@ kt_status prepare_frame(const kt_frame_desc* d, Frame* f, kt_frame_derived* dv, 
   if (d->bundles && solver != KT_SOLVER_STANDARD) solver = KT_SOLVER_STANDARD;
   if (solver == KT_SOLVER_SEMI_ANALYTIC && (chart != KT_CHART_BL || !kerr)) solver = KT_SOLVER_STANDARD;
   if (solver == KT_SOLVER_ELLIPTIC_CLOSED && !kerr) solver = KT_SOLVER_STANDARD;
-  if (solver == KT_SOLVER_ELLIPTIC_CLOSED) {
-    *err = "the elliptic-closed solver does not run on this backend";
-    return KT_ERR_UNSUPPORTED;
-  }
-  if (solver == KT_SOLVER_SEMI_ANALYTIC && d->precision != KT_PREC_FP64) {
-    *err = "the semi-analytic solver runs in FP64 only";
+  if (solver != KT_SOLVER_STANDARD && d->precision != KT_PREC_FP64) {
+    *err = "the semi-analytic and elliptic-closed solvers run in FP64 only";
     return KT_ERR_UNSUPPORTED;
   }
   fr.solver = solver;

@@ -90,6 +90,11 @@ cudaError_t launch_trace(Mode mode, const Frame& f, const OutSoA& out, const Ray
                          uint32_t* queue, const Fallback& fb, const LaunchShape& shape,
                          cudaStream_t stream);
 
+// Elliptic-closed solver: after the standard trace of rl into out, the
+// closed-form disk hits replace the rays the standard tracer did not end at
+// the horizon.
+cudaError_t launch_elliptic(const Frame& f, const OutSoA& out, const RayList& rl, cudaStream_t stream);
+
 // Colour pass: SoA -> RGB8.
 cudaError_t launch_colorize(const ColourConst& cc, int64_t n, const uint8_t* outcome,
                             const double* r, const double* red, const double* magnif,

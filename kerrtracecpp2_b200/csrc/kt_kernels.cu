@@ -2,6 +2,7 @@
 //
 // Compiled with --fmad=false: every multiply and add of the reference's
 // arithmetic is rounded separately, as in the reference's CPU build.
+#include "kt_elliptic.cuh"
 #include "kt_trace_kernel.cuh"
 
 namespace kt {
@@ -177,6 +178,42 @@ cudaError_t launch_batch(Mode mode, int variant, const BatchRays& br, uint32_t* 
     case kModeSepRk4: return batch_launch<ModeSepRk4>(variant, br, queue, fb, s, st);
     default: return launch_batch_mixed(mode, variant, br, queue, fb, s, st);
   }
+}
+
+// ---- elliptic-closed solver -------------------------------------------------
+
+// After the standard trace of the same rays (the reference's fallback and its
+// horizon-precedence check, main.cpp:1227-1295): a ray whose closed-form
+// equator crossing lies in the disk, and which the standard tracer did not
+// end at the horizon, becomes that disk hit.  One thread per ray.
+__global__ void __launch_bounds__(128) k_elliptic(const __grid_constant__ Frame f, const OutSoA out,
+                                                  const RayList rl) {
+  const uint32_t n = rl.n_dev ? *rl.n_dev : rl.n;
+  for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
+    const uint32_t pix = rl.pix ? rl.pix[idx] : idx;
+    const uint32_t slot = rl.slot ? rl.slot[idx] : idx;
+    if (out.outcome[slot] == kOutHorizon) continue;
+    double r, g;
+    int why;
+    if (!elliptic_closed_form(f, camera_ray(f, pix), &r, &g, &why)) continue;
+    // TraceResult{DISK_HIT, r, g}: phi_disk and the escape angles stay 0
+    out.outcome[slot] = (uint8_t)kOutDisk;
+    out.r[slot] = r;
+    out.red[slot] = g;
+    out.magnif[slot] = 1.0;
+    out.phi_disk[slot] = 0.0;
+    out.th_esc[slot] = 0.0;
+    out.ph_esc[slot] = 0.0;
+  }
+}
+
+cudaError_t launch_elliptic(const Frame& f, const OutSoA& out, const RayList& rl, cudaStream_t stream) {
+  const uint64_t n = rl.n_dev ? (uint64_t)0xffffffffu : rl.n;
+  if (n == 0) return cudaSuccess;
+  uint64_t grid = (n + 127) / 128;
+  if (grid > 148 * 8) grid = 148 * 8;
+  k_elliptic<<<(int)grid, 128, 0, stream>>>(f, out, rl);
+  return cudaGetLastError();
 }
 
 // ---- colour ------------------------------------------------------------------

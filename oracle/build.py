@@ -5,7 +5,10 @@ Produces:
   oracle/_ref/libktref_strict.so    the reference renderer compiled from its
   oracle/_ref/libktref_stock.so     own sources (only where the reference tree
   oracle/_ref/libktref_ieee.so      exists, i.e. in the build container):
-    strict: -O2 -ffp-contract=off, the renderer's libm interposed (parity);
+    strict: -O2 -ffp-contract=off, the renderer's libm interposed (parity),
+            complex products and quotients by the textbook formulas
+            (-fcx-limited-range, as the reference's own -ffast-math build
+            evaluates them; only the elliptic-closed solver uses them);
     stock : the reference's own -O3 -ffast-math, glibc libm (as shipped);
     ieee  : -O3 without -ffast-math, glibc libm.  The timed CPU baseline:
             under -ffast-math (-ffinite-math-only) the reference's DOPRI5
@@ -99,8 +102,8 @@ def build_reference(reference, force=False):
         obj = os.path.join(REF_OUT, "interpose.o")
         run(["gcc", "-std=c11", "-O2", "-ffp-contract=off", MARCH, "-fPIC", "-c",
              "-o", obj, interpose])
-        run(["g++"] + common + ["-O2", "-ffp-contract=off", "-fno-builtin", MARCH, "-shared",
-                                "-o", strict, harness, obj, "-lm"])
+        run(["g++"] + common + ["-O2", "-ffp-contract=off", "-fno-builtin", "-fcx-limited-range",
+                                MARCH, "-shared", "-o", strict, harness, obj, "-lm"])
     stock = os.path.join(REF_OUT, "libktref_stock.so")
     if force or newer(stock, deps):
         run(["g++"] + common + ["-O3", "-ffast-math", MARCH, "-shared", "-o", stock, harness,

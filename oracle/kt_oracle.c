@@ -1185,6 +1185,480 @@ static Ray trace_single_ks(const Frame* f, const Geo* sbl) {
   return o;
 }
 
+/* ------------------------------------------------------ elliptic-closed
+ * trace_single_elliptic_closed (main.cpp:705-1295): for a Kerr ray, the
+ * Mino time of its first equator crossing (closed form, Jacobi cn) and its
+ * radius there from the roots of the radial quartic (Jacobi inversion in
+ * one of three root configurations), Carlson R_F for the elliptic
+ * integrals.  Only a crossing inside the disk is used, and only when the
+ * standard tracer of the frame's chart does not end the ray at the horizon;
+ * every other ray is the standard tracer's.  Complex products and quotients
+ * by the textbook formulas (the reference's -ffast-math arithmetic), |z| by
+ * hypot. */
+typedef struct { double re, im; } Cx;
+static Cx cx(double re, double im) { Cx z = {re, im}; return z; }
+static Cx cx_add(Cx a, Cx b) { return cx(a.re + b.re, a.im + b.im); }
+static Cx cx_sub(Cx a, Cx b) { return cx(a.re - b.re, a.im - b.im); }
+static Cx cx_mul(Cx a, Cx b) { return cx(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re); }
+static Cx cx_div(Cx a, Cx b) {
+  const double t = b.re * b.re + b.im * b.im;
+  return cx((a.re * b.re + a.im * b.im) / t, (a.im * b.re - a.re * b.im) / t);
+}
+static double cx_abs(Cx a) { return ktm_hypot(a.re, a.im); }
+
+/* carlson_rf, main.cpp:706-742 */
+static double carlson_rf(double x, double y, double z) {
+  if (!(x >= 0.0 && y >= 0.0 && z >= 0.0)) return ktm_nan();
+  if (!oisfinite(x) || !oisfinite(y) || !oisfinite(z)) return ktm_nan();
+  double xn = x, yn = y, zn = z;
+  for (int it = 0; it < 64; ++it) {
+    const double mu = ((xn + yn) + zn) / 3.0;
+    if (!(mu > 0.0) || !oisfinite(mu)) return ktm_nan();
+    const double X = 1.0 - xn / mu, Y = 1.0 - yn / mu, Z = 1.0 - zn / mu;
+    const double eps = omax(omax(fabs(X), fabs(Y)), fabs(Z));
+    if (eps < 1e-10) {
+      const double E2 = X * Y - Z * Z;
+      const double E3 = (X * Y) * Z;
+      const double corr = (((1.0 - E2 / 10.0) + E3 / 14.0) + (E2 * E2) / 24.0) - ((3.0 * E2) * E3) / 44.0;
+      return corr / sqrt(mu);
+    }
+    const double sx = sqrt(xn), sy = sqrt(yn), sz = sqrt(zn);
+    const double lam = (sx * sy + sx * sz) + sy * sz;
+    xn = 0.25 * (xn + lam);
+    yn = 0.25 * (yn + lam);
+    zn = 0.25 * (zn + lam);
+  }
+  return ktm_nan();
+}
+
+/* ellint_F_incomplete, ellint_K_complete (main.cpp:744-757) */
+static double ell_F(double phi, double m) {
+  const double sn = ktm_sin(phi), cs = ktm_cos(phi);
+  const double x = cs * cs;
+  const double y = 1.0 - (m * sn) * sn;
+  if (y <= 0.0) return ktm_nan();
+  return sn * carlson_rf(x, y, 1.0);
+}
+
+static double ell_K(double m) {
+  if (!(m >= 0.0 && m < 1.0)) return ktm_nan();
+  return carlson_rf(0.0, 1.0 - m, 1.0);
+}
+
+/* jacobi_sn2_from_u, main.cpp:759-777 */
+static double jac_sn2(double u, double m, double Kc) {
+  if (!(m >= 0.0 && m < 1.0) || !(Kc > 0.0) || !oisfinite(u)) return ktm_nan();
+  double ur = fmod(u, 2.0 * Kc);
+  if (ur < 0.0) ur += 2.0 * Kc;
+  if (ur > Kc) ur = 2.0 * Kc - ur;
+  double lo = 0.0, hi = 0.5 * ORC_PI;
+  for (int it = 0; it < 64; ++it) {
+    const double mid = 0.5 * (lo + hi);
+    const double Fm = ell_F(mid, m);
+    if (!oisfinite(Fm)) return ktm_nan();
+    if (Fm < ur)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  const double sn = ktm_sin(0.5 * (lo + hi));
+  return sn * sn;
+}
+
+/* quartic_roots_monic_complex (main.cpp:779-812): Durand-Kerner from four
+ * points on the circle of radius 1 + max |b_i|. */
+static void quartic_roots(const double b[4], Cx z[4]) {
+  double rad = fabs(b[0]);
+  for (int i = 1; i < 4; ++i) rad = omax(rad, fabs(b[i]));
+  rad = 1.0 + rad;
+  const double PI_ = 3.141592653589793238462643383279502884;
+  for (int i = 0; i < 4; ++i) {
+    const double a = (0.5 * (double)i) * PI_;
+    z[i] = cx(rad * ktm_cos(a), rad * ktm_sin(a));
+  }
+  for (int it = 0; it < 160; ++it) {
+    double max_delta = 0.0;
+    Cx zn[4];
+    for (int i = 0; i < 4; ++i) {
+      Cx den = cx(1.0, 0.0);
+      for (int j = 0; j < 4; ++j)
+        if (i != j) den = cx_mul(den, cx_sub(z[i], z[j]));
+      if (cx_abs(den) < 1e-20) den = cx(1e-20, 0.0);
+      /* (((z + b0) z + b1) z + b2) z + b3 */
+      Cx p = cx_add(z[i], cx(b[0], 0.0));
+      p = cx_add(cx_mul(p, z[i]), cx(b[1], 0.0));
+      p = cx_add(cx_mul(p, z[i]), cx(b[2], 0.0));
+      p = cx_add(cx_mul(p, z[i]), cx(b[3], 0.0));
+      const Cx delta = cx_div(p, den);
+      zn[i] = cx_sub(z[i], delta);
+      max_delta = omax(max_delta, cx_abs(delta));
+    }
+    for (int i = 0; i < 4; ++i) z[i] = zn[i];
+    if (max_delta < 1e-13) break;
+  }
+}
+
+/* jacobi_sn_cn_from_u, main.cpp:834-876 */
+static int jac_sn_cn(double u, double m, double Kc, double* sn, double* cn) {
+  *sn = *cn = ktm_nan();
+  if (!(m >= 0.0 && m < 1.0) || !(Kc > 0.0) || !oisfinite(u)) return 0;
+  const double twoK = 2.0 * Kc;
+  long long n = (long long)floor(u / twoK);
+  double ur = u - (double)n * twoK;
+  if (ur < 0.0) {
+    ur += twoK;
+    --n;
+  }
+  const int second = ur > Kc;
+  const double target = second ? (twoK - ur) : ur;
+  double lo = 0.0, hi = 0.5 * ORC_PI;
+  for (int it = 0; it < 72; ++it) {
+    const double mid = 0.5 * (lo + hi);
+    const double Fm = ell_F(mid, m);
+    if (!oisfinite(Fm)) return 0;
+    if (Fm < target)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  const double amp = 0.5 * (lo + hi);
+  double s_ = ktm_sin(amp), c_ = ktm_cos(amp);
+  if (second) c_ = -c_;
+  if ((n & 1LL) != 0) {
+    s_ = -s_;
+    c_ = -c_;
+  }
+  *sn = s_;
+  *cn = c_;
+  return oisfinite(s_) && oisfinite(c_);
+}
+
+/* jacobi_sc_from_u, main.cpp:878-885 */
+static int jac_sc(double u, double m, double Kc, double* sc) {
+  double sn, cn;
+  *sc = ktm_nan();
+  if (!jac_sn_cn(u, m, Kc, &sn, &cn)) return 0;
+  if (fabs(cn) < 1e-14) return 0;
+  *sc = sn / cn;
+  return oisfinite(*sc);
+}
+
+enum { RAD_REAL4 = 0, RAD_REAL2 = 1, RAD_COMPLEX4 = 2 };
+typedef struct {
+  int kind;
+  double r1, r2, r3, r4;
+  double m, Kc, omega, X0;
+  int phase_sign, tau_sign;
+  double A, B, r_lo, r_hi;
+  double a2, b1, g0;
+} RadMap; /* EllipticRadialMap, main.cpp:893-916 */
+
+/* elliptic_radial_r_from_phase, main.cpp:918-956 */
+static double rad_r(const RadMap* mp, double X) {
+  if (mp->kind == RAD_REAL4) {
+    const double sn2 = jac_sn2(X, mp->m, mp->Kc);
+    if (!oisfinite(sn2)) return ktm_nan();
+    const double r24 = mp->r2 - mp->r4, r14 = mp->r1 - mp->r4;
+    const double den = r24 - r14 * sn2;
+    if (fabs(den) < 1e-14) return ktm_nan();
+    return (mp->r1 * r24 - (mp->r2 * r14) * sn2) / den;
+  }
+  if (mp->kind == RAD_REAL2) {
+    double sn, cn;
+    if (!jac_sn_cn(X, mp->m, mp->Kc, &sn, &cn)) return ktm_nan();
+    const double num = (mp->B * mp->r_hi - mp->A * mp->r_lo) + (mp->B * mp->r_hi + mp->A * mp->r_lo) * cn;
+    const double den = (mp->B - mp->A) + (mp->B + mp->A) * cn;
+    if (fabs(den) < 1e-14) return ktm_nan();
+    return num / den;
+  }
+  double sc;
+  if (!jac_sc(X, mp->m, mp->Kc, &sc)) return ktm_nan();
+  const double den = 1.0 + mp->g0 * sc;
+  if (fabs(den) < 1e-14) return ktm_nan();
+  return -mp->a2 * ((mp->g0 - sc) / den) - mp->b1;
+}
+
+/* align_initial_radial_sign (main.cpp:981-1000) */
+static void rad_align(RadMap* mp, double dr0, int flip_phase, int flip_tau) {
+  if (fabs(dr0) < 1e-14) return;
+  const double probe = 1e-6;
+  const double Xp = (double)mp->phase_sign * mp->X0 + ((double)mp->tau_sign * mp->omega) * probe;
+  const double Xm = (double)mp->phase_sign * mp->X0 - ((double)mp->tau_sign * mp->omega) * probe;
+  const double rp = rad_r(mp, Xp), rm = rad_r(mp, Xm);
+  if (!oisfinite(rp) || !oisfinite(rm)) return;
+  if ((dr0 >= 0.0) == (rp >= rm)) return;
+  if (flip_phase) mp->phase_sign = -mp->phase_sign;
+  if (flip_tau) mp->tau_sign = -mp->tau_sign;
+}
+
+static void sort_desc(double* v, int n) {
+  for (int i = 1; i < n; ++i)
+    for (int j = i; j > 0 && v[j] > v[j - 1]; --j) {
+      const double t = v[j];
+      v[j] = v[j - 1];
+      v[j - 1] = t;
+    }
+}
+
+/* init_elliptic_radial_map, main.cpp:958-1168 */
+static int rad_init(const SepC* c, double r0, double dr0, RadMap* out) {
+  const double u = c->Lz - c->a * c->E;
+  const double Kpot = c->Qc + u * u;
+  const double A0 = (c->E * c->a) * c->a - c->a * c->Lz;
+  const double c4 = c->E * c->E;
+  if (!(c4 > 1e-18)) return 0;
+  const double c2 = (2.0 * c->E) * A0 - Kpot;
+  const double c1 = (2.0 * c->M) * Kpot;
+  const double c0 = A0 * A0 - (c->a * c->a) * Kpot;
+  const double b[4] = {0.0, c2 / c4, c1 / c4, c0 / c4};
+  Cx z[4];
+  quartic_roots(b, z);
+  double rr[4];
+  Cx cr[4];
+  int nr = 0, nc = 0;
+  for (int i = 0; i < 4; ++i) {
+    if (!oisfinite(z[i].re) || !oisfinite(z[i].im)) return 0;
+    const double tol = 1e-7 * omax(1.0, fabs(z[i].re));
+    if (fabs(z[i].im) <= tol)
+      rr[nr++] = z[i].re;
+    else
+      cr[nc++] = z[i];
+  }
+  memset(out, 0, sizeof *out);
+  out->phase_sign = out->tau_sign = 1;
+  if (nr == 4) {
+    sort_desc(rr, 4);
+    out->kind = RAD_REAL4;
+    out->r1 = rr[0];
+    out->r2 = rr[1];
+    out->r3 = rr[2];
+    out->r4 = rr[3];
+    const double den_omega = (out->r1 - out->r3) * (out->r2 - out->r4);
+    if (!(den_omega > 0.0)) return 0;
+    out->omega = 0.5 * sqrt(den_omega);
+    const double k_num = (out->r2 - out->r3) * (out->r1 - out->r4);
+    const double k_den = (out->r2 - out->r4) * (out->r1 - out->r3);
+    if (!(k_den > 0.0)) return 0;
+    out->m = k_num / k_den;
+    if (!(out->m >= 0.0 && out->m < 1.0)) return 0;
+    out->Kc = ell_K(out->m);
+    if (!oisfinite(out->Kc) || !(out->Kc > 0.0)) return 0;
+    const double den_obs = r0 - out->r2, den_root = out->r1 - out->r4;
+    if (fabs(den_obs) < 1e-14 || fabs(den_root) < 1e-14) return 0;
+    const double u0_raw = ((r0 - out->r1) / den_obs) * ((out->r2 - out->r4) / den_root);
+    if (!oisfinite(u0_raw)) return 0;
+    if (u0_raw < -1e-6 || u0_raw > 1.0 + 1e-6) return 0;
+    const double u0 = oclamp(u0_raw, 0.0, 1.0);
+    out->X0 = ell_F(ktm_asin(sqrt(u0)), out->m);
+    if (!oisfinite(out->X0)) return 0;
+    const int case1 = (r0 >= out->r3 && r0 <= out->r2);
+    const int alpha = case1 ? -1 : 1;
+    const int nu_r = (dr0 >= 0.0) ? 1 : -1;
+    out->phase_sign = alpha * nu_r;
+    out->tau_sign = 1;
+    rad_align(out, dr0, 1, 0);
+    return 1;
+  }
+  if (nr == 2 && nc == 2) {
+    const double r1 = omin(rr[0], rr[1]), r2 = omax(rr[0], rr[1]); /* ascending */
+    const double b1 = 0.5 * (cr[0].re + cr[1].re);
+    const double a1 = 0.5 * (fabs(cr[0].im) + fabs(cr[1].im));
+    if (!(a1 > 0.0) || !oisfinite(a1) || !oisfinite(b1)) return 0;
+    const double A = sqrt(a1 * a1 + (b1 - r2) * (b1 - r2));
+    const double B = sqrt(a1 * a1 + (b1 - r1) * (b1 - r1));
+    if (!(A > 0.0 && B > 0.0 && B > A)) return 0;
+    const double r21 = r2 - r1;
+    const double k3 = (((A + B) * (A + B)) - r21 * r21) / ((4.0 * A) * B);
+    if (!(k3 > 0.0 && k3 < 1.0)) return 0;
+    const double K3 = ell_K(k3);
+    if (!oisfinite(K3) || !(K3 > 0.0)) return 0;
+    const double x3 = (A * (r0 - r1) - B * (r0 - r2)) / (A * (r0 - r1) + B * (r0 - r2));
+    if (!oisfinite(x3)) return 0;
+    const double phi0 = ktm_acos(oclamp(x3, -1.0, 1.0));
+    const double F0 = ell_F(phi0, k3);
+    if (!oisfinite(F0)) return 0;
+    out->kind = RAD_REAL2;
+    out->r1 = r2;
+    out->r2 = r1;
+    out->r_lo = r1;
+    out->r_hi = r2;
+    out->A = A;
+    out->B = B;
+    out->m = k3;
+    out->Kc = K3;
+    out->omega = sqrt(A * B);
+    out->X0 = F0;
+    out->phase_sign = (dr0 >= 0.0) ? 1 : -1;
+    out->tau_sign = 1;
+    rad_align(out, dr0, 1, 0);
+    return 1;
+  }
+  if (nr == 0 && nc == 4) {
+    Cx pos[4], neg[4];
+    int np = 0, nn = 0;
+    for (int i = 0; i < 4; ++i) {
+      if (cr[i].im >= 0.0) {
+        if (np < 4) pos[np] = cr[i];
+        ++np;
+      } else {
+        if (nn < 4) neg[nn] = cr[i];
+        ++nn;
+      }
+    }
+    if (np != 2 || nn != 2) return 0;
+    const double d00 = cx_abs(cx_sub(pos[0], cx(neg[0].re, -neg[0].im)));
+    const double d01 = cx_abs(cx_sub(pos[0], cx(neg[1].re, -neg[1].im)));
+    const int j0 = (d00 <= d01) ? 0 : 1;
+    const double bA = 0.5 * (pos[0].re + neg[j0].re);
+    const double aA = 0.5 * (fabs(pos[0].im) + fabs(neg[j0].im));
+    const double bB = 0.5 * (pos[1].re + neg[1 - j0].re);
+    const double aB = 0.5 * (fabs(pos[1].im) + fabs(neg[1 - j0].im));
+    if (!(aA > 0.0 && aB > 0.0)) return 0;
+    double b1 = bA, a1 = aA, b2 = bB, a2 = aB;
+    if (bB > bA) {
+      b1 = bB;
+      a1 = aB;
+      b2 = bA;
+      a2 = aA;
+    }
+    if (!(b1 > b2)) return 0;
+    const double C = sqrt((a1 - a2) * (a1 - a2) + (b1 - b2) * (b1 - b2));
+    const double D = sqrt((a1 + a2) * (a1 + a2) + (b1 - b2) * (b1 - b2));
+    if (!(C > 0.0 && D > 0.0)) return 0;
+    const double k4 = ((4.0 * C) * D) / ((C + D) * (C + D));
+    if (!(k4 > 0.0 && k4 < 1.0)) return 0;
+    const double K4 = ell_K(k4);
+    if (!oisfinite(K4) || !(K4 > 0.0)) return 0;
+    const double g_num = (4.0 * a2) * a2 - (C - D) * (C - D);
+    const double g_den = (C + D) * (C + D) - (4.0 * a2) * a2;
+    if (!(g_num > 0.0 && g_den > 0.0)) return 0;
+    const double g0 = sqrt(g_num / g_den);
+    if (!(g0 > 0.0) || !oisfinite(g0)) return 0;
+    const double x4 = (r0 - b2) / omax(a2, 1e-15);
+    const double phi0 = ktm_atan(x4) + ktm_atan(g0);
+    const double F0 = ell_F(phi0, k4);
+    if (!oisfinite(F0)) return 0;
+    out->kind = RAD_COMPLEX4;
+    out->m = k4;
+    out->Kc = K4;
+    out->omega = 0.5 * (C + D);
+    out->X0 = F0;
+    out->phase_sign = 1;
+    out->tau_sign = (dr0 >= 0.0) ? 1 : -1;
+    out->a2 = a2;
+    out->b1 = b1;
+    out->g0 = g0;
+    rad_align(out, dr0, 0, 1);
+    return 1;
+  }
+  return 0;
+}
+
+/* separable_radial_potential, main.cpp:1170-1176 */
+static double sep_Rpot(const SepC* c, double r) {
+  const double u = c->Lz - c->a * c->E;
+  const double Kpot = c->Qc + u * u;
+  const double A0 = c->E * (r * r + c->a * c->a) - c->a * c->Lz;
+  const double Delta = (r * r - (2.0 * c->M) * r) + c->a * c->a;
+  return A0 * A0 - Delta * Kpot;
+}
+
+/* first_equator_crossing_mino_time, main.cpp:1178-1219 */
+static int eq_crossing(const SepC* c, double th0, double dth0, double* tau_first) {
+  const double A = ((c->a * c->a) * c->E) * c->E;
+  if (!(A > 1e-15)) return 0;
+  const double B = (A - c->Lz * c->Lz) - c->Qc;
+  const double disc = B * B + (4.0 * A) * c->Qc;
+  if (!(disc >= 0.0)) return 0;
+  const double sq = sqrt(disc);
+  const double up = (B + sq) / (2.0 * A), um = (B - sq) / (2.0 * A);
+  if (!(up > 0.0 && um < 0.0)) return 0;
+  const double m = up / (up - um);
+  if (!(m >= 0.0 && m < 1.0)) return 0;
+  const double Kc = ell_K(m);
+  if (!oisfinite(Kc) || !(Kc > 0.0)) return 0;
+  const double omega = sqrt(A * (up - um));
+  if (!(omega > 0.0) || !oisfinite(omega)) return 0;
+  const double mu_plus = sqrt(up);
+  const double mu0 = ktm_cos(th0);
+  const double c0 = oclamp(fabs(mu0) / omax(mu_plus, 1e-15), 0.0, 1.0);
+  const double phi0 = ktm_acos(c0);
+  const double u_base = ell_F(phi0, m);
+  if (!oisfinite(u_base)) return 0;
+  const double tau_period = (4.0 * Kc) / omega;
+  if (!(tau_period > 0.0) || !oisfinite(tau_period)) return 0;
+  const int toward = (ktm_cos(th0) * dth0) > 0.0;
+  const double u0 = toward ? u_base : -u_base;
+  double tf = (Kc - u0) / omega;
+  if (tf < 0.0) tf += tau_period;
+  *tau_first = tf;
+  return oisfinite(tf);
+}
+
+/* EllipticFallbackReason (main.cpp:178-186) */
+enum { EF_NONE = 0, EF_INIT = 1, EF_THETA = 2, EF_RADIAL_INIT = 3, EF_RADIAL_INVALID = 4,
+       EF_OUTSIDE_DISK = 5 };
+
+/* The closed-form part of trace_single_elliptic_closed: 1 with (r, g) of a
+ * disk crossing (to be used unless the standard tracer ends the ray at the
+ * horizon), else 0 with the fallback reason. */
+static int elliptic_closed_form(const Frame* f, const Geo* sbl, double* r_out, double* g_out, int* reason) {
+  SepC c;
+  if (!sep_init(sbl, &f->g, &c)) {
+    *reason = EF_INIT;
+    return 0;
+  }
+  double dr0, dth0, dpr0, dpth0;
+  geo_rhs(&f->g, sbl->r, sbl->th, sbl->pr, sbl->pth, sbl->pt, sbl->pphi, &dr0, &dth0, &dpr0, &dpth0);
+  double tau_first = 0.0;
+  if (!eq_crossing(&c, sbl->th, dth0, &tau_first)) {
+    *reason = EF_THETA;
+    return 0;
+  }
+  RadMap mp;
+  if (!rad_init(&c, sbl->r, dr0, &mp)) {
+    *reason = EF_RADIAL_INIT;
+    return 0;
+  }
+  const double rh_cut = f->rh * 1.03;
+  const double X = (double)mp.phase_sign * mp.X0 + ((double)mp.tau_sign * mp.omega) * tau_first;
+  const double r_now = rad_r(&mp, X);
+  if (!oisfinite(r_now)) {
+    *reason = EF_RADIAL_INVALID;
+    return 0;
+  }
+  const double R = sep_Rpot(&c, r_now);
+  const double R_scale = omax(1.0, fabs(((((c.E * c.E) * r_now) * r_now) * r_now) * r_now));
+  if (R < -1e-8 * R_scale || (mp.kind != RAD_COMPLEX4 && r_now < mp.r1) || r_now < rh_cut) {
+    *reason = EF_RADIAL_INVALID;
+    return 0;
+  }
+  if (r_now > f->r_esc || !(r_now >= f->r_in && r_now <= f->r_out)) {
+    *reason = EF_OUTSIDE_DISK;
+    return 0;
+  }
+  *reason = EF_NONE;
+  *r_out = r_now;
+  *g_out = oclamp(disk_redshift(&f->g, r_now, sbl->pt, sbl->pphi), 0.0, 20.0);
+  return 1;
+}
+
+static Ray trace_standard(const Frame* f, const Geo* sbl) {
+  return (f->chart == KT_CHART_KS) ? trace_single_ks(f, sbl) : trace_single(f, *sbl);
+}
+
+/* trace_single_elliptic_closed, main.cpp:1227-1295 */
+static Ray trace_elliptic(const Frame* f, const Geo* sbl, int* reason) {
+  double r, g;
+  const Ray std_ray = trace_standard(f, sbl);
+  if (!elliptic_closed_form(f, sbl, &r, &g, reason)) return std_ray;
+  if (std_ray.outcome == KT_OUT_HORIZON) return std_ray; /* horizon precedence */
+  Ray o = ray_result(KT_OUT_DISK, r, g, 0.0, 0.0, 0.0);
+  o.steps = std_ray.steps;
+  o.attempts = std_ray.attempts;
+  return o;
+}
+
 /* ------------------------------------------------------------- ray bundles
  * ray_bundle.hpp:56-436 */
 static void hessian_H(const Metric* g, double r, double th, double pr, double pth, double pt,
@@ -1516,7 +1990,9 @@ void orc_trace_pixels(const kt_frame_desc* d, int64_t n, const uint32_t* pix, ui
       double al, be;
       cam_pixel_angles(&f.cam, px, py, f.offx, f.offy, &al, &be);
       const Geo s = cam_angle_ray(&f.cam, al, be, &f.g);
-      o = (f.chart == KT_CHART_KS) ? trace_single_ks(&f, &s)
+      int reason = 0;
+      o = (f.solver == KT_SOLVER_ELLIPTIC_CLOSED) ? trace_elliptic(&f, &s, &reason)
+          : (f.chart == KT_CHART_KS) ? trace_single_ks(&f, &s)
           : (f.solver == KT_SOLVER_SEMI_ANALYTIC) ? trace_separable(&f, &s)
                                                   : trace_single(&f, s);
     }
@@ -1529,6 +2005,24 @@ void orc_trace_pixels(const kt_frame_desc* d, int64_t n, const uint32_t* pix, ui
     phi_esc[i] = o.phi_esc;
     if (steps) steps[i] = o.steps;
     if (attempts) attempts[i] = o.attempts;
+  }
+}
+
+/* The elliptic-closed solver's fallback reason per pixel (0: the closed
+ * form gave a disk crossing), for frames whose effective solver is it. */
+void orc_elliptic_reasons(const kt_frame_desc* d, int64_t n, const uint32_t* pix, uint8_t* reason) {
+  Frame f;
+  setup_frame(d, &f);
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int64_t i = 0; i < n; ++i) {
+    const int px = (int)(pix[i] % (uint32_t)d->width);
+    const int py = (int)(pix[i] / (uint32_t)d->width);
+    double al, be, r, g;
+    cam_pixel_angles(&f.cam, px, py, f.offx, f.offy, &al, &be);
+    const Geo s = cam_angle_ray(&f.cam, al, be, &f.g);
+    int why = 0;
+    elliptic_closed_form(&f, &s, &r, &g, &why);
+    reason[i] = (uint8_t)why;
   }
 }
 

@@ -50,6 +50,7 @@ void orc_colorize_cp(const kt_frame_desc* d, int64_t n, const uint8_t* outcome, 
  * of spp RGB8 passes (spp*n*3 bytes, pass after pass). */
 void orc_spp_offsets(int spp, double* xy);
 void orc_spp_combine(int64_t n, int spp, const uint8_t* passes, double gamma, uint8_t* rgb);
+void orc_elliptic_reasons(const kt_frame_desc* d, int64_t n, const uint32_t* pix, uint8_t* reason);
 
 /* Known-answer helpers (tests/core_tests.cpp of the reference). */
 void orc_metric_bl(double M, double a, double Q, double L, double r, double th, double* cov16,

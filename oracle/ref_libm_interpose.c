@@ -7,6 +7,8 @@
  * binds to the renderer's deterministic libm (ktmath.h) instead of glibc's.
  * The reference source is not modified: this is symbol interposition at link
  * time.  Nothing outside the strict oracle library sees these symbols. */
+#include <complex.h>
+
 #include "../kerrtracecpp2_b200/csrc/ktmath.h"
 
 #define KT_HIDDEN __attribute__((visibility("hidden")))
@@ -20,3 +22,9 @@ KT_HIDDEN double log10(double x) { return ktm_log10(x); }
 KT_HIDDEN double cbrt(double x) { return ktm_cbrt(x); }
 KT_HIDDEN double atan2(double y, double x) { return ktm_atan2(y, x); }
 KT_HIDDEN double acos(double x) { return ktm_acos(x); }
+/* the elliptic-closed solver (main.cpp:705-1301): std::asin, std::atan and
+ * std::abs of a std::complex<double> (cabs) */
+KT_HIDDEN double asin(double x) { return ktm_asin(x); }
+KT_HIDDEN double atan(double x) { return ktm_atan(x); }
+KT_HIDDEN double hypot(double x, double y) { return ktm_hypot(x, y); }
+KT_HIDDEN double cabs(double complex z) { return ktm_hypot(creal(z), cimag(z)); }

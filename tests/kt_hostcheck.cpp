@@ -12,6 +12,7 @@
 
 #include "../include/kerrtrace.h"
 #include "../kerrtracecpp2_b200/csrc/kt_frame.h"
+#include "../kerrtracecpp2_b200/csrc/kt_elliptic.cuh"
 #include "../kerrtracecpp2_b200/csrc/kt_smray.cuh"
 
 using namespace kt;
@@ -65,7 +66,21 @@ RayResult run_bl(const Frame& f, const Geo& s) {
   }
 }
 
+RayResult run_ray_standard(const Frame& f, uint32_t pix);
+
+// The elliptic-closed solver as the kernels run it: the standard trace,
+// then the closed-form disk hit unless the standard trace ends at the horizon.
 RayResult run_ray(const Frame& f, uint32_t pix) {
+  RayResult res = run_ray_standard(f, pix);
+  if (f.solver != KT_SOLVER_ELLIPTIC_CLOSED || res.outcome == kOutHorizon) return res;
+  double r, g;
+  int why;
+  if (elliptic_closed_form(f, camera_ray(f, pix), &r, &g, &why))
+    set_result(&res, kOutDisk, res.status, r, g, 1.0, 0.0, 0.0, 0.0);
+  return res;
+}
+
+RayResult run_ray_standard(const Frame& f, uint32_t pix) {
   if (f.bundles) {
     Bundle m;
     m.init(f, (int)(pix % (uint32_t)f.cam.W), (int)(pix / (uint32_t)f.cam.W));
