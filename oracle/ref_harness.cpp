@@ -117,6 +117,25 @@ extern "C" {
 double ref_libm_probe_cos(double x) { return std::cos(x); }
 double ref_libm_probe_pow(double x, double y) { return std::pow(x, y); }
 
+// The elliptic-closed solver's fallback reason (EllipticFallbackReason,
+// 0 = the closed form was used or checked) per pixel, from the reference's
+// own trace_single_elliptic_closed, for a frame whose effective solver it is.
+void ref_elliptic_reasons(const kt_frame_desc* d, int64_t n, const uint32_t* pix, uint8_t* reason,
+                          int nthreads) {
+  const FrameSetup f = setup_frame(d);
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int64_t i = 0; i < n; ++i) {
+    const int px = (int)(pix[i] % (uint32_t)d->width);
+    const int py = (int)(pix[i] / (uint32_t)d->width);
+    auto s = f.cam.pixel_ray(px, py, f.g, f.offx, f.offy);
+    EllipticFallbackReason why = EllipticFallbackReason::NONE;
+    trace_single_elliptic_closed(s, f.g, f.r_disk_in, f.r_disk_out, f.r_escape, &why, f.eff_chart,
+                                 f.intg, f.ctl);
+    reason[i] = (uint8_t)why;
+  }
+}
+
 // Trace pixels pix[i] (= py*width+px) through the reference's per-ray
 // tracers, with the dispatch of trace_geodesics; float64 SoA out.
 void ref_trace_pixels(const kt_frame_desc* d, int64_t n, const uint32_t* pix,

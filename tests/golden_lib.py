@@ -83,3 +83,28 @@ def semi_desc(name):
 def semi_result(name):
     z = semi()
     return {k: z[f"{name}/{k}"] for k in FIELDS}
+
+
+ELL_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "elliptic.npz")
+_ze = None
+
+
+def ell():
+    """tests/golden/elliptic.npz (make_elliptic_golden.py): the elliptic-closed solver."""
+    global _ze
+    if _ze is None:
+        _ze = dict(np.load(ELL_PATH))
+    return _ze
+
+
+def ell_cases():
+    return json.loads(bytes(ell()["meta_json"]).decode())
+
+
+def ell_desc(name):
+    return abi.frame_desc(**ell_cases()[name])
+
+
+def ell_result(name):
+    z = ell()
+    return {k: z[f"{name}/{k}"] for k in FIELDS}

@@ -51,6 +51,8 @@ def port():
         L.orc_spp_offsets.restype = None
         L.orc_spp_combine.argtypes = [ctypes.c_int64, ctypes.c_int, _P, _D, _P]
         L.orc_spp_combine.restype = None
+        L.orc_elliptic_reasons.argtypes = [ctypes.POINTER(FrameDesc), ctypes.c_int64, _P, _P]
+        L.orc_elliptic_reasons.restype = None
         for f in ("orc_r_horizon", "orc_r_isco"):
             getattr(L, f).argtypes = [_D] * 4
             getattr(L, f).restype = _D
@@ -72,6 +74,8 @@ def ref(flavour="strict"):
         L.ref_trace_pixels.argtypes = [ctypes.POINTER(FrameDesc), ctypes.c_int64, _P] + [_P] * 7 + [ctypes.c_int]
         L.ref_trace_pixels.restype = None
         L.ref_trace_geodesics.argtypes = [ctypes.POINTER(FrameDesc), _P, ctypes.c_int]
+        L.ref_elliptic_reasons.argtypes = [ctypes.POINTER(FrameDesc), ctypes.c_int64, _P, _P, ctypes.c_int]
+        L.ref_elliptic_reasons.restype = None
         L.ref_colorize.argtypes = [_P, ctypes.c_int, ctypes.c_int, _D, _D, _D, _P, ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, _P]
         L.ref_colorize.restype = None
         PC = ctypes.POINTER(ColorParams)
@@ -140,6 +144,22 @@ def trace_ref(desc, flavour="strict", pix=None, nthreads=0):
 GEOPIXEL_DTYPE = np.dtype([("outcome", "u1"), ("pad", "u1", 3), ("r", "<f4"), ("redshift", "<f4"),
                            ("magnif", "<f4"), ("phi_disk", "<f4"), ("theta_esc", "<f4"),
                            ("phi_esc", "<f4")])
+
+
+def elliptic_reasons_ref(desc, flavour="strict", pix=None, nthreads=0):
+    """The reference's elliptic-closed fallback reason per pixel (uint8)."""
+    pix = all_pixels(desc) if pix is None else np.ascontiguousarray(pix, np.uint32)
+    out = np.zeros(len(pix), np.uint8)
+    ref(flavour).ref_elliptic_reasons(ctypes.byref(desc), len(pix), _ptr(pix), _ptr(out), nthreads)
+    return out
+
+
+def elliptic_reasons_port(desc, pix=None):
+    """The oracle's elliptic-closed fallback reason per pixel (uint8)."""
+    pix = all_pixels(desc) if pix is None else np.ascontiguousarray(pix, np.uint32)
+    out = np.zeros(len(pix), np.uint8)
+    port().orc_elliptic_reasons(ctypes.byref(desc), len(pix), _ptr(pix), _ptr(out))
+    return out
 
 
 def trace_geodesics_ref(desc, flavour="strict", nthreads=0):

@@ -115,7 +115,8 @@ def test_fallback_rules():
     (dict(a=float("nan")), abi.KT_ERR_INVALID_ARGUMENT),
     (dict(tol=float("inf")), abi.KT_ERR_INVALID_ARGUMENT),
     (dict(chart=7), abi.KT_ERR_INVALID_ARGUMENT),
-    (dict(solver_mode=abi.KT_SOLVER_ELLIPTIC_CLOSED), abi.KT_ERR_UNSUPPORTED),
+    (dict(solver_mode=abi.KT_SOLVER_ELLIPTIC_CLOSED, precision=abi.KT_PREC_MIXED), abi.KT_ERR_UNSUPPORTED),
+    (dict(solver_mode=9), abi.KT_ERR_INVALID_ARGUMENT),
     (dict(precision=7), abi.KT_ERR_INVALID_ARGUMENT),
     (dict(precision=abi.KT_PREC_SMOOTH, bundles=1), abi.KT_ERR_UNSUPPORTED),
     (dict(r_obs=-1.0), abi.KT_ERR_INVALID_ARGUMENT),

@@ -1,0 +1,65 @@
+"""The elliptic-closed solver on the GPU (the standard trace, then
+k_elliptic): bit-identical to the reference's results in
+tests/golden/elliptic.npz through kt_trace, kt_trace_pixels and a
+supersampled render; rejected in batches."""
+import numpy as np
+import pytest
+
+import golden_lib as G
+from kerrtracecpp2_b200 import abi
+
+pytestmark = pytest.mark.gpu
+NAMES = sorted(G.ell_cases())
+
+
+def to_np(out):
+    import torch
+
+    torch.cuda.synchronize()
+    return {k: (v.cpu().numpy() if v is not None else None) for k, v in out.items()}
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_trace_matches_reference(renderer, name):
+    got = to_np(renderer.trace(G.ell_desc(name)))
+    assert G.mismatches(got, G.ell_result(name)) == {k: 0 for k in G.FIELDS}
+
+
+def test_pixel_list_matches_frame(renderer):
+    import torch
+
+    name = "ell_kerr_ks"
+    d = G.ell_desc(name)
+    n = d.width * d.height
+    perm = np.random.default_rng(5).permutation(n).astype(np.int32)
+    got = to_np(renderer.trace_pixels(d, torch.from_numpy(perm).cuda()))
+    want = G.ell_result(name)
+    assert G.mismatches(got, {k: v[perm] for k, v in want.items()}) == {k: 0 for k in G.FIELDS}
+
+
+def test_supersampled_render_equals_colour_of_passes(renderer):
+    """camera_spp 2 with the elliptic solver: each pass gets the closed form
+    too, so the render equals the average of the two single-pass renders
+    taken at the jitter offsets."""
+    import kerrtracecpp2_b200 as kt
+    import oracle_lib as O
+
+    kw = dict(G.ell_cases()["ell_offsets"])
+    bg = G.data()["bg"]
+    cp = abi.color_params()
+    passes = []
+    for ox, oy in kt.camera_spp_offsets(2):
+        d = abi.frame_desc(**dict(kw, pixel_offset_x=kw["pixel_offset_x"] + ox,
+                                  pixel_offset_y=kw["pixel_offset_y"] + oy))
+        passes.append(renderer.render_host(d, cp, bg).reshape(-1, 3))
+    want = O.spp_combine_port(np.stack(passes), cp.gamma)
+    got = renderer.render_host(abi.frame_desc(**kw), cp, bg, camera_spp=2)
+    assert np.array_equal(got.reshape(-1, 3), want)
+
+
+def test_batch_rejects_elliptic_frames(renderer):
+    import kerrtracecpp2_b200 as kt
+
+    with pytest.raises(kt.KerrTraceError) as e:
+        renderer.batch([G.ell_desc("ell_offsets")])
+    assert e.value.status == abi.KT_ERR_UNSUPPORTED

@@ -127,7 +127,8 @@ def test_errors_are_status_codes(renderer):
     assert e.value.status == abi.KT_ERR_INVALID_ARGUMENT
     with pytest.raises(kt.KerrTraceError) as e:
         renderer.trace(abi.frame_desc(width=8, height=8, chart=abi.KT_CHART_BL,
-                                      solver_mode=abi.KT_SOLVER_ELLIPTIC_CLOSED))
+                                      solver_mode=abi.KT_SOLVER_ELLIPTIC_CLOSED,
+                                      precision=abi.KT_PREC_MIXED))
     assert e.value.status == abi.KT_ERR_UNSUPPORTED
     # the context stays usable after an error
     got = trace(renderer, G.desc("one_pixel"))

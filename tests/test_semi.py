@@ -108,9 +108,6 @@ def test_unsupported_solver_requests():
     import kerrtracecpp2_b200 as kt
 
     with pytest.raises(kt.KerrTraceError) as e:
-        kt.frame_derive(abi.frame_desc(solver_mode=abi.KT_SOLVER_ELLIPTIC_CLOSED, chart=abi.KT_CHART_BL))
-    assert e.value.status == abi.KT_ERR_UNSUPPORTED
-    with pytest.raises(kt.KerrTraceError) as e:
         kt.frame_derive(abi.frame_desc(solver_mode=abi.KT_SOLVER_SEMI_ANALYTIC, chart=abi.KT_CHART_BL,
                                        precision=abi.KT_PREC_MIXED))
     assert e.value.status == abi.KT_ERR_UNSUPPORTED
