@@ -57,11 +57,12 @@ typedef enum kt_status {
 enum { KT_CHART_KS = 0, KT_CHART_BL = 1 };
 /* Integrator (Integrator, geodesic.hpp:417). */
 enum { KT_RK4_DOUBLING = 0, KT_DOPRI5 = 1 };
-/* Ray solver (RaySolverMode, main.cpp:176).  STANDARD and SEMI_ANALYTIC
- * (the separable Kerr tracer, main.cpp:436-703; FP64 precision) run here;
- * ELLIPTIC_CLOSED returns KT_ERR_UNSUPPORTED.  A solver the frame cannot use
- * falls back to STANDARD as in the reference: bundles; SEMI_ANALYTIC in the
- * KS chart; either with Q or Lambda != 0. */
+/* Ray solver (RaySolverMode, main.cpp:176): STANDARD, SEMI_ANALYTIC (the
+ * separable Kerr tracer, main.cpp:436-703) and ELLIPTIC_CLOSED (the closed-
+ * form disk crossing over the standard trace, main.cpp:705-1295), the last
+ * two in FP64 precision only and ELLIPTIC_CLOSED not in batches.  A solver
+ * the frame cannot use falls back to STANDARD as in the reference: bundles;
+ * SEMI_ANALYTIC in the KS chart; either with Q or Lambda != 0. */
 enum { KT_SOLVER_STANDARD = 0, KT_SOLVER_SEMI_ANALYTIC = 1, KT_SOLVER_ELLIPTIC_CLOSED = 2 };
 /* Arithmetic of the trace.  FP64: the reference's arithmetic bit for bit.
  * MIXED: analytic Hamiltonian gradient, FP32 right-hand side in the far
