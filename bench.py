@@ -51,6 +51,10 @@ WORKLOADS = {
     # The semi-analytic solver (--bl --semi-analytic) at the CLI's default
     # Kerr frame, 720p, default step cap 500000: every ray with a radial
     # turning point parks there and runs to the cap, ~1 s of CPU per ray.
+    # The elliptic-closed solver (--elliptic-closed) on config 1's Kerr frame
+    # at 720p: the standard KS trace plus the closed-form disk crossings.
+    "elliptic_ks_kerr_720p": dict(chart=0, solver_mode=2, a=0.5, r_obs=40.0, theta_deg=80.0,
+                                  fov_deg=45.0, disk_out=12.0, width=1280, height=720),
     "semi_bl_kerr_720p": dict(chart=1, solver_mode=1, a=0.998, r_obs=40.0, theta_deg=80.0,
                               fov_deg=30.0, disk_out=12.0, width=1280, height=720,
                               cpu_calib_pixels=64),
@@ -487,7 +491,7 @@ def main():
                 "integrator": "DOPRI5" if wl.get("integrator", 0) == 1 else "RK4-doubling",
                 "tol": wl.get("tol", 1e-7), "a": wl.get("a"), "Q": wl.get("Q", 0.0),
                 "Lambda": wl.get("Lambda", 0.0), "bundles": bool(wl.get("bundles", 0)),
-                "solver": "semi-analytic" if wl.get("solver_mode", 0) == 1 else "standard",
+                "solver": ["standard", "semi-analytic", "elliptic-closed"][wl.get("solver_mode", 0)],
                 "parallelism": f"frames{args.gpus}", "l2": "256 MB flush between steps"}
 
     if args.impl == "reference":
