@@ -143,6 +143,18 @@ def ray_flops(desc, steps, attempts):
     return rhs * FLOPS_BL_RHS + attempts * FLOPS_RK4_ATTEMPT
 
 
+def trace_launches(dv, desc):
+    """Kernel launches of one kt_trace: the persistent trace kernel, the BL
+    launch over the fallback list (KS chart, semi-analytic solver) and the
+    elliptic-closed kernel."""
+    n = 1
+    if not desc.bundles and (dv.chart == 0 or dv.solver == 1):
+        n += 1
+    if dv.solver == 2:
+        n += 1
+    return n
+
+
 def cpu_reference_sample(desc, seconds, flavour="ieee", calib_pixels=None):
     """Time the reference's CPU path on a strided sample of the frame
     (calibrated on calib_pixels pixels, by default 512 or 16 per thread).
@@ -729,8 +741,7 @@ def main():
             "mixed_batched": mixed_batched, "adjoint": adjoint,
             "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": ctypes.sizeof(desc),
                     "d2h_bytes_per_step": d2h, "call": "kt_trace_host"},
-            "clocks": clocks, "gpu_launches": args.steps * (2 if desc.chart == 0 and not desc.bundles
-                                                            and abs(desc.Lambda) <= 1e-15 else 1)
+            "clocks": clocks, "gpu_launches": args.steps * trace_launches(kt.frame_derive(desc), desc)
             * (2 if mixed is not None else 1)
             + (args.steps * len(mixed_batched["groups"]) if mixed_batched else 0)
             + (args.steps * 9 if adjoint else 0)}
