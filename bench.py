@@ -77,9 +77,9 @@ FLOPS_DOPRI5_ATTEMPT = 447.0
 FLOPS_RK4_ATTEMPT = 335.0
 # DRAM bytes read + written by one k_trace<ModeBLDopri5> launch on the
 # default 720p frame, from one ncu capture of that launch
-# (dram__bytes_read.sum 1.263 MB + dram__bytes_write.sum 4.794 MB): the
+# (dram__bytes_read.sum 0.109 MB + dram__bytes_write.sum 5.450 MB): the
 # frame's 52.5 MB of outputs stay in L2 during the launch.
-TRAFFIC_DOPRI5_720P = 6.057472e6
+TRAFFIC_DOPRI5_720P = 5.559552e6
 
 
 def env_int(name, default):
