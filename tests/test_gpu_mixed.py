@@ -58,3 +58,68 @@ def test_mixed_bundles_against_fp64(renderer):
           f"magnif rel p50 {np.median(em):.2e} p99 {np.percentile(em, 99):.2e}")
     assert 1 - same.mean() < 1e-3
     assert np.median(eg) < 5e-6 and np.median(em) < 1e-4
+
+
+def test_mixed_error_table_every_config(renderer):
+    """The error of the mixed-precision path against the FP64 oracle for
+    every benchmark configuration at its full size: pixel class, g and r_hit
+    on the disk pixels of both, and the colour of the pixel (blackbody
+    palette, seed-0 star field).  Config 4 is its 64 parameter sets, traced
+    as one batch in each precision.  The table is printed."""
+    import torch
+
+    import kerrtracecpp2_b200 as kt
+
+    cfgs = {
+        "1 KS RK4 320x180": [FRAMES["cfg1_ks_rk4"]],
+        "2 KNdS BL DOPRI5 720p": [FRAMES["cfg2_720p_dopri5"]],
+        "3 bundles 1080p": [dict(chart=1, bundles=1, a=0.998, theta_deg=60.0, width=1920, height=1080)],
+        "4 64 sets, batch": None,
+        "5 KS RK4 512x512": [FRAMES["cfg5_ks_rk4"]],
+    }
+    bg = torch.from_numpy(np.ascontiguousarray(kt.starfield(0, 2048, 1024))).cuda()
+    rows = []
+    for name, frames in cfgs.items():
+        if frames is None:
+            descs = kt.random_parameter_sets(64, seed=1)
+            outs = []
+            for prec in (abi.KT_PREC_FP64, abi.KT_PREC_MIXED):
+                ds = [abi.frame_desc(**{**{f: getattr(d, f) for f, _ in abi.FrameDesc._fields_},
+                                        "precision": prec}) for d in descs]
+                b = renderer.batch(ds)
+                b.launch()
+                outs.append((ds, b.outs))
+            pairs = [((outs[0][0][i], outs[0][1][i]), (outs[1][0][i], outs[1][1][i]))
+                     for i in range(len(descs))]
+        else:
+            pairs = []
+            for kw in frames:
+                dp = abi.frame_desc(**kw)
+                dm = abi.frame_desc(precision=abi.KT_PREC_MIXED, **kw)
+                pairs.append(((dp, renderer.trace(dp)), (dm, renderer.trace(dm))))
+        n = mism = 0
+        eg_all, er_all, cdiff = [], [], []
+        for (dp, op), (dm, om) in pairs:
+            rp = renderer.colorize(dp, op, bg=bg)
+            rm = renderer.colorize(dm, om, bg=bg)
+            torch.cuda.synchronize()
+            ref = {k: v.cpu().numpy() for k, v in op.items() if v is not None}
+            got = {k: v.cpu().numpy() for k, v in om.items() if v is not None}
+            same = got["outcome"] == ref["outcome"]
+            disk = same & (ref["outcome"] == 1)
+            n += same.size
+            mism += int((~same).sum())
+            eg_all.append(np.abs(got["redshift"][disk] - ref["redshift"][disk]) / np.abs(ref["redshift"][disk]))
+            er_all.append(np.abs(got["r"][disk] - ref["r"][disk]) / np.abs(ref["r"][disk]))
+            d = np.abs(rm.cpu().numpy().astype(int) - rp.cpu().numpy().astype(int)).reshape(-1, 3).max(axis=1)
+            cdiff.append(d)
+        eg, er, cd = np.concatenate(eg_all), np.concatenate(er_all), np.concatenate(cdiff)
+        rows.append((name, n, mism / n, np.median(eg), np.percentile(eg, 99), np.median(er),
+                     np.percentile(er, 99), (cd > 0).mean(), np.percentile(cd, 99.9), cd.max()))
+    print("\nconfig | pixels | class mismatch | g p50 | g p99 | r_hit p50 | r_hit p99 | "
+          "colour: pixels differing | p99.9 diff | max diff")
+    for r in rows:
+        print(f"{r[0]} | {r[1]} | {r[2]:.1e} | {r[3]:.1e} | {r[4]:.1e} | {r[5]:.1e} | {r[6]:.1e} | "
+              f"{r[7]:.2e} | {r[8]:.0f} | {r[9]}")
+    for r in rows:
+        assert r[2] < 1e-3 and r[3] < 5e-6, r
