@@ -212,3 +212,44 @@ def test_tangent_equals_adjoint(frame, dirs):
         others = [q for q in range(5) if q != k]
         assert not ct[others].any()
         assert np.array_equal(ct[6], ca[6])  # the same pixels get a derivative
+
+
+@pytest.mark.skipif(not O.ref_available("strict"), reason="reference tree not built here")
+def test_gradient_against_reference_renderer_differences():
+    """The adjoint of the smooth tracer against the reference renderer
+    itself (strict build): least-squares slopes of the reference's L2 loss
+    (config-5 geometry, 128x128, disk pixels in every render) over 11
+    parameter offsets in +-1e-2.  The reference's disk crossing is the
+    midpoint after 8 bisections, a staircase in the parameters, so its loss
+    is differentiable only at this coarse scale: the agreement is 1e-3 to
+    2e-1 relative, printed; the test asserts the sign and the first digit."""
+    base = dict(CFG5, Lambda=0.0, width=128, height=128)
+    wg, wr, h = 1.0, 0.01, 1e-2
+    tgt, _ = S.smooth(abi.frame_desc(**dict(base, a=0.72, theta_deg=71.0)))
+    ref0 = O.trace_ref(abi.frame_desc(**base), "strict")
+    scale = {"a": 1.0, "Q": 1.0, "theta_deg": np.degrees(1.0), "r_obs": 1.0}
+    offs = np.linspace(-1.0, 1.0, 11)
+    ok = (ref0["outcome"] == 1) & (tgt["outcome"] == 1)
+    renders = {}
+    for k, sc in scale.items():
+        renders[k] = [O.trace_ref(abi.frame_desc(**dict(base, **{k: base[k] + x * h * sc})), "strict")
+                      for x in offs]
+        for o in renders[k]:
+            ok &= o["outcome"] == 1
+
+    def loss(o):
+        return np.sum(wg * (o["redshift"][ok] - tgt["redshift"][ok]) ** 2 +
+                      wr * (o["r"][ok] - tgt["r"][ok]) ** 2)
+
+    _, c = S.smooth(abi.frame_desc(**base), mode=1,
+                    cot_g=np.where(ok, 2 * wg * (ref0["redshift"] - tgt["redshift"]), 0.0),
+                    cot_r=np.where(ok, 2 * wr * (ref0["r"] - tgt["r"]), 0.0))
+    g = c.sum(axis=1)
+    adj = {"a": g[0], "Q": g[1], "theta_deg": g[3] * np.pi / 180, "r_obs": g[4]}
+    for k, sc in scale.items():
+        x = offs * h * sc
+        L = np.array([loss(o) for o in renders[k]])
+        slope = np.linalg.lstsq(np.vstack([x, x * x, np.ones_like(x)]).T, L, rcond=None)[0][0]
+        rel = abs(adj[k] - slope) / abs(slope)
+        print(f"{k}: adjoint {adj[k]:.6g} reference slope {slope:.6g} rel {rel:.1e}")
+        assert rel < 0.5
