@@ -60,7 +60,7 @@ enum { KT_RK4_DOUBLING = 0, KT_DOPRI5 = 1 };
 /* Ray solver (RaySolverMode, main.cpp:176): STANDARD, SEMI_ANALYTIC (the
  * separable Kerr tracer, main.cpp:436-703) and ELLIPTIC_CLOSED (the closed-
  * form disk crossing over the standard trace, main.cpp:705-1295), the last
- * two in FP64 precision only and ELLIPTIC_CLOSED not in batches.  A solver
+ * two in FP64 precision only.  A solver
  * the frame cannot use falls back to STANDARD as in the reference: bundles;
  * SEMI_ANALYTIC in the KS chart; either with Q or Lambda != 0. */
 enum { KT_SOLVER_STANDARD = 0, KT_SOLVER_SEMI_ANALYTIC = 1, KT_SOLVER_ELLIPTIC_CLOSED = 2 };

@@ -47,6 +47,10 @@ struct Group {
   kt::LaunchShape shape{};
   int fb_variant = 0;
   kt::LaunchShape fb_shape{};
+  // frames of the elliptic-closed solver: after the group's trace, the
+  // closed-form disk hits (k_elliptic) over each such frame
+  std::vector<kt::Frame> ell_frames;
+  std::vector<kt::OutSoA> ell_outs;
   kt_batch_group_info info{};
 };
 
@@ -98,9 +102,17 @@ cudaError_t enqueue_group(const Group& g, int variant, const kt::LaunchShape& s,
   kt::Fallback fb = {g.d_fb, nullptr, g.d_counters + 2};
   cudaError_t e = kt::launch_batch(g.mode, variant, group_rays(g, list, nullptr, n, refill_min),
                                    g.d_counters, fb, s, st);
-  if (e != cudaSuccess || !kt::has_fallback(g.mode)) return e;
-  return kt::launch_batch(g.fb_mode, g.fb_variant, group_rays(g, g.d_fb, g.d_counters + 2, 0, 1),
+  if (e != cudaSuccess) return e;
+  if (kt::has_fallback(g.mode))
+    e = kt::launch_batch(g.fb_mode, g.fb_variant, group_rays(g, g.d_fb, g.d_counters + 2, 0, 1),
                           g.d_counters + 1, fb, g.fb_shape, st);
+  if (e != cudaSuccess || list != nullptr) return e;  // a tuning sample: no closed form
+  for (size_t k = 0; k < g.ell_frames.size() && e == cudaSuccess; ++k) {
+    const kt::Frame& f = g.ell_frames[k];
+    const kt::RayList all = {nullptr, nullptr, nullptr, (uint32_t)((uint64_t)f.cam.W * f.cam.H)};
+    e = kt::launch_elliptic(f, g.ell_outs[k], all, st);
+  }
+  return e;
 }
 
 // Time the candidates (variant x regroup threshold) on a sample of the
@@ -276,9 +288,6 @@ kt_status kt_batch_create(kt_context* ctx, const kt_frame_desc* descs, const kt_
       ctx->err = "frame " + std::to_string(i) + ": " + ctx->err;
       return r;
     }
-    if (frames[i].solver == KT_SOLVER_ELLIPTIC_CLOSED)
-      return fail(ctx, KT_ERR_UNSUPPORTED,
-                  "frame " + std::to_string(i) + ": the elliptic-closed solver does not run in batches");
     if (frames[i].precision == KT_PREC_SMOOTH)
       return fail(ctx, KT_ERR_UNSUPPORTED,
                   "frame " + std::to_string(i) + ": the smooth tracer does not run in batches");
@@ -296,6 +305,10 @@ kt_status kt_batch_create(kt_context* ctx, const kt_frame_desc* descs, const kt_
     }
     Group& g = b->groups[group_of_key[key]];
     g.frames.push_back(i);
+    if (frames[i].solver == KT_SOLVER_ELLIPTIC_CLOSED) {
+      g.ell_frames.push_back(frames[i]);
+      g.ell_outs.push_back(to_out(&outs[i]));
+    }
     g.n_rays += (uint64_t)descs[i].width * (uint64_t)descs[i].height;
     b->n_rays += (uint64_t)descs[i].width * (uint64_t)descs[i].height;
   }

@@ -1,7 +1,7 @@
 """The elliptic-closed solver on the GPU (the standard trace, then
 k_elliptic): bit-identical to the reference's results in
 tests/golden/elliptic.npz through kt_trace, kt_trace_pixels and a
-supersampled render; rejected in batches."""
+supersampled render and batches."""
 import numpy as np
 import pytest
 
@@ -57,9 +57,16 @@ def test_supersampled_render_equals_colour_of_passes(renderer):
     assert np.array_equal(got.reshape(-1, 3), want)
 
 
-def test_batch_rejects_elliptic_frames(renderer):
-    import kerrtracecpp2_b200 as kt
-
-    with pytest.raises(kt.KerrTraceError) as e:
-        renderer.batch([G.ell_desc("ell_offsets")])
-    assert e.value.status == abi.KT_ERR_UNSUPPORTED
+def test_elliptic_frames_in_a_batch(renderer):
+    """Elliptic-closed frames share a batch with standard frames of the same
+    kernels (KS RK4, BL DOPRI5): the graph runs the closed form over the
+    elliptic frames only."""
+    names = ["ell_kerr_ks", "ell_edge_on_dopri5", "ell_step_cap"]
+    descs = [G.ell_desc(n) for n in names] + [G.desc("cfg1_ks_rk4"), G.desc("cfg2_bl_dopri5")]
+    wants = [G.ell_result(n) for n in names] + [G.result("cfg1_ks_rk4"), G.result("cfg2_bl_dopri5")]
+    b = renderer.batch(descs)
+    for _ in range(2):
+        b.launch()
+        for o, want in zip(b.outs, wants):
+            assert G.mismatches(to_np(o), want) == {k: 0 for k in G.FIELDS}
+    b.close()
