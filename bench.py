@@ -143,6 +143,25 @@ def ray_flops(desc, steps, attempts):
     return rhs * FLOPS_BL_RHS + attempts * FLOPS_RK4_ATTEMPT
 
 
+def boundary_distance(outcome, pix, radius=8):
+    """For pixels whose class differs between two renders: the largest, over
+    those pixels, of the distance (in pixels) to the nearest pixel of another
+    class in `outcome` (H x W) -- how far from a class boundary (critical
+    curve, disk edge) a disagreement lies.  None without disagreements;
+    radius + 1 when some lies farther than `radius`."""
+    if len(pix) == 0:
+        return None
+    H, W = outcome.shape
+    worst = 0.0
+    for p in np.asarray(pix, np.int64):
+        y, x = divmod(int(p), W)
+        y0, y1, x0, x1 = max(0, y - radius), min(H, y + radius + 1), max(0, x - radius), min(W, x + radius + 1)
+        yy, xx = np.nonzero(outcome[y0:y1, x0:x1] != outcome[y, x])
+        d = float(np.min(np.hypot(yy + y0 - y, xx + x0 - x))) if yy.size else radius + 1.0
+        worst = max(worst, d)
+    return worst
+
+
 def trace_launches(dv, desc):
     """Kernel launches of one kt_trace: the persistent trace kernel, the BL
     launch over the fallback list (KS chart, semi-analytic solver) and the
@@ -730,6 +749,9 @@ def main():
                "sample": sample + ("; reference built -O3 without -ffast-math, glibc libm"
                                    if kind == "reference" else ""),
                "class_mismatch_vs_gpu": int(np.sum(got_out != res["outcome"])),
+               "class_mismatch_boundary_distance_px": boundary_distance(
+                   out["outcome"].cpu().numpy().reshape(desc.height, desc.width),
+                   pix[got_out != res["outcome"]]),
                "g_rel_diff_vs_gpu_median": float(np.median(rel)) if rel.size else None}
 
     line = {"metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world,
