@@ -229,6 +229,19 @@ kt_status kt_render_spp_host(kt_context* ctx, const kt_frame_desc* desc,
                              const uint8_t* bg_rgb_host, int32_t bg_w, int32_t bg_h,
                              uint8_t* rgb_out_host);
 
+/* The elliptic-closed solver's fallback reason per pixel, the reference's
+ * --debug-elliptic tag (EllipticFallbackReason, main.cpp:178-186, stored in
+ * GeoPixel padding at main.cpp:2111-2121 and coloured by colorize_buffer,
+ * main.cpp:1828-1843): 0 the closed form placed the crossing in the disk,
+ * 1 constants of motion, 2 polar crossing, 3 radial map, 4 radial value
+ * invalid, 5 outside the disk.  All 0 where the frame's effective solver is
+ * not ELLIPTIC_CLOSED.  reason: width*height bytes (device / host). */
+#define KT_ELLIPTIC_REASONS 6
+kt_status kt_elliptic_reasons(kt_context* ctx, const kt_frame_desc* desc, uint8_t* reason,
+                              void* stream);
+kt_status kt_elliptic_reasons_host(kt_context* ctx, const kt_frame_desc* desc,
+                                   uint8_t* reason_host);
+
 /* The camera_spp jitter offsets in pixels (main.cpp:2238-2279):
  * xy[2 s], xy[2 s + 1] for pass s < max(camera_spp, 1). */
 kt_status kt_camera_spp_offsets(int32_t camera_spp, double* xy);

@@ -81,6 +81,10 @@ def load_library():
     L.kt_render_spp_host.restype = ctypes.c_int
     L.kt_camera_spp_offsets.argtypes = [I32, P]
     L.kt_camera_spp_offsets.restype = ctypes.c_int
+    L.kt_elliptic_reasons.argtypes = [P, PD, P, P]
+    L.kt_elliptic_reasons.restype = ctypes.c_int
+    L.kt_elliptic_reasons_host.argtypes = [P, PD, P]
+    L.kt_elliptic_reasons_host.restype = ctypes.c_int
     L.kt_measure_fp64_peak.argtypes = [P, ctypes.POINTER(D)]
     L.kt_measure_fp64_peak.restype = ctypes.c_int
     L.kt_starfield.argtypes = [ctypes.c_uint64, I32, I32, P]
@@ -322,6 +326,17 @@ class Renderer:
                                         self._stream(stream)),
                "kt_l2_grad", self.ctx)
         return loss.value, np.array(grad[:]), st.as_dict()
+
+    def elliptic_reasons(self, desc, stream=None):
+        """kt_elliptic_reasons: the elliptic-closed solver's fallback reason
+        per pixel (uint8 tensor, 0 = closed form in the disk)."""
+        import torch
+
+        out = torch.empty(desc.width * desc.height, dtype=torch.uint8,
+                          device=torch.device("cuda", self.device))
+        _check(self.L.kt_elliptic_reasons(self.ctx, ctypes.byref(desc), _torch_ptr(out), self._stream(stream)),
+               "kt_elliptic_reasons", self.ctx)
+        return out
 
     def batch(self, descs, outs=None, options=None):
         """kt_batch_create over frames `descs` (a list of kt_frame_desc) with

@@ -156,6 +156,7 @@ int main(int argc, char** argv) {
   std::string geo_file, bg_spec, out_path, out_dir = "out";
   double arg_r_obs = -1.0;
   int camera_spp = 1;
+  bool debug_elliptic = false;
   for (int i = 1; i < argc; ++i) {
     const std::string a(argv[i]);
     auto next = [&](void) -> const char* {
@@ -214,6 +215,12 @@ int main(int argc, char** argv) {
     else if (a == "--temp-scale") cp.temp_scale = atof(next());
     else if (a == "--disk-interstellar") cp.palette = 1;
     else if (a == "--disk-blackbody") cp.palette = 0;
+    else if (a == "--debug-elliptic") debug_elliptic = true;
+    else if (a == "--anti-fireflies" || a == "--anti_fireflies" || a == "--no-anti-fireflies" ||
+             a == "--no-anti_fireflies" || a == "--elliptic-fallback-black" ||
+             a == "--elliptic-strict-black") {
+      // Metal-backend options: the reference's CPU path ignores them (main.cpp:2327-2328)
+    } else if (a == "--metal-kernel") next();
     else if (a == "--disk-rings") cp.disk_rings = atoi(next());
     else if (a == "--disk-sectors") cp.disk_sectors = atoi(next());
     else if (a == "--disk-sigma") cp.disk_sigma = atof(next());
@@ -340,7 +347,18 @@ int main(int argc, char** argv) {
   }
   if (!geo_only) {
     rgb.resize(3 * n);
-    if (save_geo)
+    if (debug_elliptic) {
+      // colorize_buffer's debug branch (main.cpp:1828-1843): the colour of
+      // the elliptic-closed solver's fallback reason
+      static const uint8_t kTag[KT_ELLIPTIC_REASONS][3] = {
+          {0, 220, 0}, {255, 255, 255}, {0, 220, 220}, {220, 0, 0}, {220, 220, 0}, {60, 60, 220}};
+      std::vector<uint8_t> why(n);
+      if (camera_spp > 1)
+        fprintf(stderr, "Info: --debug-elliptic colours one pass (camera-spp ignored).\n");
+      st = kt_elliptic_reasons_host(ctx, &d, why.data());
+      for (size_t i = 0; st == KT_OK && i < n; ++i)
+        for (int c = 0; c < 3; ++c) rgb[3 * i + c] = why[i] < KT_ELLIPTIC_REASONS ? kTag[why[i]][c] : (c == 1 ? 0 : 128);
+    } else if (save_geo)
       st = kt_colorize_host(ctx, &g, d.width, d.height, d.M, dv.r_isco, dv.r_disk_in, dv.r_disk_out,
                             &cp, bg.empty() ? nullptr : bg.data(), bw, bh, rgb.data());
     else

@@ -488,6 +488,41 @@ kt_status kt_render_spp_host(kt_context* ctx, const kt_frame_desc* desc, const k
   return KT_OK;
 }
 
+kt_status kt_elliptic_reasons(kt_context* ctx, const kt_frame_desc* desc, uint8_t* reason,
+                              void* stream) {
+  if (!ctx) return KT_ERR_INVALID_ARGUMENT;
+  if (!desc || !reason) return fail(ctx, KT_ERR_INVALID_ARGUMENT, "kt_elliptic_reasons: NULL pointer");
+  kt::Frame f;
+  kt_status r = kt::prepare_frame(desc, &f, nullptr, &ctx->err);
+  if (r != KT_OK) return r;
+  DeviceGuard g(ctx->device);
+  const uint32_t n = (uint32_t)((int64_t)desc->width * desc->height);
+  const cudaStream_t st = (cudaStream_t)stream;
+  if (f.solver != KT_SOLVER_ELLIPTIC_CLOSED || f.bundles) {
+    KT_CUDA(ctx, cudaMemsetAsync(reason, 0, n, st), "clear reasons");  // the tag stays 0
+    return KT_OK;
+  }
+  KT_CUDA(ctx, kt::launch_elliptic_reasons(f, n, reason, st), "elliptic reasons launch");
+  return KT_OK;
+}
+
+kt_status kt_elliptic_reasons_host(kt_context* ctx, const kt_frame_desc* desc, uint8_t* reason_host) {
+  if (!ctx) return KT_ERR_INVALID_ARGUMENT;
+  if (!desc || !reason_host) return fail(ctx, KT_ERR_INVALID_ARGUMENT, "kt_elliptic_reasons_host: NULL pointer");
+  if (desc->width < 1 || desc->height < 1)
+    return fail(ctx, KT_ERR_INVALID_ARGUMENT, "kt_elliptic_reasons_host: bad frame size");
+  DeviceGuard g(ctx->device);
+  const size_t n = (size_t)desc->width * (size_t)desc->height;
+  kt_status r = ensure(ctx, (void**)&ctx->d_stage, &ctx->stage_cap, n + 256, "staging buffer");
+  if (r != KT_OK) return r;
+  r = kt_elliptic_reasons(ctx, desc, ctx->d_stage, ctx->stream);
+  if (r != KT_OK) return r;
+  KT_CUDA(ctx, cudaMemcpyAsync(reason_host, ctx->d_stage, n, cudaMemcpyDeviceToHost, ctx->stream),
+          "copy reasons to host");
+  KT_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "elliptic reasons");
+  return KT_OK;
+}
+
 kt_status kt_camera_spp_offsets(int32_t camera_spp, double* xy) {
   if (!xy || camera_spp > KT_MAX_CAMERA_SPP) return KT_ERR_INVALID_ARGUMENT;
   spp_offsets(camera_spp < 1 ? 1 : camera_spp, xy);

@@ -94,6 +94,8 @@ cudaError_t launch_trace(Mode mode, const Frame& f, const OutSoA& out, const Ray
 // closed-form disk hits replace the rays the standard tracer did not end at
 // the horizon.
 cudaError_t launch_elliptic(const Frame& f, const OutSoA& out, const RayList& rl, cudaStream_t stream);
+// Its fallback reason per pixel of the frame (n = width x height).
+cudaError_t launch_elliptic_reasons(const Frame& f, uint32_t n, uint8_t* reason, cudaStream_t stream);
 
 // Colour pass: SoA -> RGB8.
 cudaError_t launch_colorize(const ColourConst& cc, int64_t n, const uint8_t* outcome,

@@ -207,6 +207,27 @@ __global__ void __launch_bounds__(128) k_elliptic(const __grid_constant__ Frame 
   }
 }
 
+// The closed form's fallback reason per pixel (the reference's
+// --debug-elliptic tag, main.cpp:2111-2121): 0 where it places the crossing
+// in the disk, else the EllipticFallbackReason.
+__global__ void __launch_bounds__(128) k_elliptic_reasons(const __grid_constant__ Frame f, uint32_t n,
+                                                          uint8_t* __restrict__ reason) {
+  for (uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x; pix < n; pix += gridDim.x * blockDim.x) {
+    double r, g;
+    int why = kEfNone;
+    elliptic_closed_form(f, camera_ray(f, pix), &r, &g, &why);
+    reason[pix] = (uint8_t)why;
+  }
+}
+
+cudaError_t launch_elliptic_reasons(const Frame& f, uint32_t n, uint8_t* reason, cudaStream_t stream) {
+  if (n == 0) return cudaSuccess;
+  uint64_t grid = ((uint64_t)n + 127) / 128;
+  if (grid > 148 * 8) grid = 148 * 8;
+  k_elliptic_reasons<<<(int)grid, 128, 0, stream>>>(f, n, reason);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_elliptic(const Frame& f, const OutSoA& out, const RayList& rl, cudaStream_t stream) {
   const uint64_t n = rl.n_dev ? (uint64_t)0xffffffffu : rl.n;
   if (n == 0) return cudaSuccess;

@@ -70,3 +70,21 @@ def test_elliptic_frames_in_a_batch(renderer):
         for o, want in zip(b.outs, wants):
             assert G.mismatches(to_np(o), want) == {k: 0 for k in G.FIELDS}
     b.close()
+
+
+@pytest.mark.parametrize("name", [n for n in NAMES if f"{n}/reason" in G.ell()])
+def test_fallback_reasons_match_reference(renderer, name):
+    """kt_elliptic_reasons: the reference's --debug-elliptic tag of every pixel."""
+    import torch
+
+    got = renderer.elliptic_reasons(G.ell_desc(name))
+    torch.cuda.synchronize()
+    assert np.array_equal(got.cpu().numpy(), G.ell()[f"{name}/reason"])
+
+
+def test_fallback_reasons_zero_for_other_solvers(renderer):
+    import torch
+
+    got = renderer.elliptic_reasons(G.desc("cfg1_ks_rk4"))
+    torch.cuda.synchronize()
+    assert not got.cpu().numpy().any()
