@@ -159,13 +159,14 @@ class IntegratorControls:
 
 
 def make_desc(W, H, fp, use_bundles=False, chart=KT_CHART_KS, intg=KT_RK4_DOUBLING, ctl=None,
-              pixel_offset_x=0.0, pixel_offset_y=0.0, M=1.0, Q=0.0, Lam=0.0):
+              pixel_offset_x=0.0, pixel_offset_y=0.0, M=1.0, Q=0.0, Lam=0.0,
+              solver_mode=abi.KT_SOLVER_STANDARD):
     ctl = ctl or IntegratorControls()
     return frame_desc(M=M, a=fp.a, Q=Q, Lambda=Lam, theta_deg=fp.theta, phi_deg=fp.phi,
                       r_obs=fp.r_obs, disk_out=fp.disk_out, fov_deg=fp.fov, width=W, height=H,
                       pixel_offset_x=pixel_offset_x, pixel_offset_y=pixel_offset_y, chart=chart,
                       integrator=intg, bundles=int(bool(use_bundles)), max_steps=ctl.max_steps,
-                      step_init=ctl.step_init, tol=ctl.tol)
+                      step_init=ctl.step_init, tol=ctl.tol, solver_mode=solver_mode)
 
 
 def frame_derive(desc):
@@ -444,21 +445,23 @@ def _renderer(device=0):
 
 
 def trace_geodesics(W, H, fp, use_bundles=False, chart=KT_CHART_KS, intg=KT_RK4_DOUBLING, ctl=None,
-                    pixel_offset_x=0.0, pixel_offset_y=0.0, M_bh=1.0, Q_bh=0.0, Lam=0.0, device=0):
-    """Phase 1 (main.cpp:2014): per-pixel results as float64 numpy arrays."""
+                    pixel_offset_x=0.0, pixel_offset_y=0.0, M_bh=1.0, Q_bh=0.0, Lam=0.0, device=0,
+                    solver_mode=abi.KT_SOLVER_STANDARD):
+    """Phase 1 (main.cpp:2014): per-pixel results as float64 numpy arrays;
+    solver_mode as the reference's RaySolverMode (main.cpp:176)."""
     desc = make_desc(W, H, fp, use_bundles, chart, intg, ctl, pixel_offset_x, pixel_offset_y, M_bh,
-                     Q_bh, Lam)
+                     Q_bh, Lam, solver_mode)
     return _renderer(device).trace_host(desc)
 
 
 def render_image(W, H, fp, bg=None, use_bundles=False, chart=KT_CHART_KS, intg=KT_RK4_DOUBLING,
                  ctl=None, M_bh=1.0, Q_bh=0.0, Lam=0.0, cp=None, pixel_offset_x=0.0,
-                 pixel_offset_y=0.0, device=0, camera_spp=1):
+                 pixel_offset_y=0.0, device=0, camera_spp=1, solver_mode=abi.KT_SOLVER_STANDARD):
     """render_image (main.cpp:2209): trace + colorize; (H, W, 3) uint8.
     camera_spp > 1 renders that many jittered passes and averages them in
     linear light (main.cpp:2232-2322)."""
     desc = make_desc(W, H, fp, use_bundles, chart, intg, ctl, pixel_offset_x, pixel_offset_y, M_bh,
-                     Q_bh, Lam)
+                     Q_bh, Lam, solver_mode)
     return _renderer(device).render_host(desc, cp, bg, camera_spp)
 
 
