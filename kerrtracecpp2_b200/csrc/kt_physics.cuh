@@ -98,13 +98,13 @@ KT_HD Ang bl_ang(const Metric& g, double th) {
   A.ct = ct;
   A.st2 = st * st;
   A.Ath = (g.a2 * ct) * ct;
-  A.dth = 1.0 + ((g.Laa * ct) * ct) / 3.0;
+  A.dth = 1.0 + ktm_div3((g.Laa * ct) * ct);
   return A;
 }
 
 // Delta_r, knds_metric.hpp:51
 KT_HD double bl_delta_r(const Metric& g, double r, double r2a2) {
-  return ((r2a2 * (1.0 - ((g.L * r) * r) / 3.0)) - g.twoM * r) + g.Q2;
+  return ((r2a2 * (1.0 - ktm_div3((g.L * r) * r))) - g.twoM * r) + g.Q2;
 }
 
 // Non-zero entries of g^{mu nu} (contravariant_BL, knds_metric.hpp:99-117).

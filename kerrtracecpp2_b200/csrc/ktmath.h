@@ -190,6 +190,26 @@ KTM_FN double ktm_cos(double x) {
   return c;
 }
 
+/* ------------------------------------------------------------- x / 3 */
+
+/* x / 3.0, the correctly rounded IEEE quotient, in three operations instead
+ * of a division (the metric's Lambda/3 terms divide by 3 five times per
+ * inverse metric).  Method: one correction step of P. Markstein (IBM J. Res.
+ * Dev. 34(1), 1990) applied to q0 = RN(x y), y = RN(1/3) = (2^54 - 1)/(3 2^54):
+ *   |x y - x/3| = (x/3) 2^-54 < ulp(x/3)/2, so |q0 - x/3| < ulp(x/3);
+ *   r = x - 3 q0 is then a small multiple of ulp(q0), exact in one fma;
+ *   q0 + r y = x/3 + (1 - 3y)(q0 - x/3) is within 2^-54 ulp of x/3,
+ * while x/3 in units of its ulp is an integer over 3, at least 1/6 ulp from
+ * any rounding midpoint; so RN(q0 + r y) = RN(x/3).  Zero, subnormal,
+ * near-overflow, Inf and NaN arguments take the division operator. */
+KTM_FN double ktm_div3(double x) {
+  const uint32_t e = (uint32_t)(ktm_bits(x) >> 52) & 0x7ffu;
+  if (e - 64u >= 1936u) return x / 3.0;
+  const double y = 0x1.5555555555555p-2;
+  const double q0 = x * y;
+  return fma(fma(-3.0, q0, x), y, q0);
+}
+
 /* -------------------------------------------------------------------- exp */
 
 /* exp(hi + lo) where |lo| <= ulp(hi). */

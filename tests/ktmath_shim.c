@@ -15,3 +15,6 @@ double kts_acos(double x) { return ktm_acos(x); }
 double kts_atan(double x) { return ktm_atan(x); }
 double kts_asin(double x) { return ktm_asin(x); }
 double kts_hypot(double x, double y) { return ktm_hypot(x, y); }
+void kts_div3_n(const double* x, double* q, long n) {
+  for (long i = 0; i < n; ++i) q[i] = ktm_div3(x[i]);
+}

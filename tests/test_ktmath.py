@@ -96,3 +96,27 @@ def test_exact_points(L):
         assert L.kts_pow(x, 4.0) == x ** 4
     assert abs(L.kts_log10(50.0) - math.log10(50.0)) <= 2.3e-16 * 2
     assert L.kts_cos(math.pi / 2) == pytest.approx(6.123233995736766e-17, rel=1e-15)
+
+
+def test_div3_is_the_ieee_quotient(L):
+    """ktm_div3 (three operations) returns the bits of x / 3.0 for every
+    binade, sign and the special values, and for every pattern of the low 20
+    significand bits at a few exponents."""
+    import numpy as np
+
+    rng = np.random.default_rng(3)
+    bits = rng.integers(0, 2 ** 63, 4_000_000, dtype=np.uint64) | (
+        rng.integers(0, 2, 4_000_000, dtype=np.uint64) << np.uint64(63))
+    low = np.arange(2 ** 20, dtype=np.uint64)
+    patterns = [np.uint64(e) << np.uint64(52) | np.uint64(m) << np.uint64(32) | low
+                for e in (1, 64, 1021, 1023, 1024, 1999, 2045) for m in (0, 0x55555, 0xaaaaa, 0xfffff)]
+    x = np.concatenate([bits] + patterns).view(np.float64)
+    x = np.concatenate([x, np.array([0.0, -0.0, 5e-324, 2.2250738585072014e-308, 1.7976931348623157e308,
+                                     np.inf, -np.inf, np.nan, 3.0, -3.0, 1.0, 0.1])])
+    q = np.empty_like(x)
+    dp = ctypes.POINTER(ctypes.c_double)
+    L.kts_div3_n(x.ctypes.data_as(dp), q.ctypes.data_as(dp), ctypes.c_long(x.size))
+    with np.errstate(all="ignore"):
+        ref = x / 3.0
+    same = (q.view(np.uint64) == ref.view(np.uint64)) | (np.isnan(q) & np.isnan(ref))
+    assert same.all(), x[~same][:5]
