@@ -63,18 +63,27 @@ WORKLOADS = {
 # camera azimuths, traced as one batch.
 BATCH_720P_FRAMES = 8
 
-# Algorithmic FP64 operations (+, -, *, / and sqrt = 1, fma = 2), counted
-# from the reference's arithmetic as kt_physics.cuh evaluates it:
-#   BL RHS (geodesic_rhs + dphi_vel): 3 sincos (70 each incl. reduction),
-#   5 g^{mu nu} evaluations (34 full, 26 at the centre, 24 when only theta
-#   changes), 4 Hamiltonians (16), FD differences -> 453.
-#   DOPRI5 attempt: 6 RHS + stage sums (189) + y5/y4 (117) + error norm (26)
-#   + controller with pow (115) -> 6 RHS + 447.
-#   RK4 doubling attempt: 10 RHS + stage inputs/sums (207) + error (13)
-#   + controller (115) -> 10 RHS + 335; one more RHS per accepted step.
-FLOPS_BL_RHS = 453.0
-FLOPS_DOPRI5_ATTEMPT = 447.0
-FLOPS_RK4_ATTEMPT = 335.0
+# Algorithmic FP64 work, counted from the reference's arithmetic as
+# kt_physics.cuh evaluates it (+, -, * = 1 flop, fma = 2), each division,
+# square root, sincos and pow weighted by its cost measured on the device in
+# the same run (kt_measure_op_costs: the FMA-pipe time of one operation at
+# full throughput, in flops):
+#   BL RHS (geodesic_rhs + dphi_vel): 211 flops of arithmetic (5 g^{mu nu}
+#   evaluations: 28 flops full, 21 at the centre, 19 when only theta changes;
+#   4 Hamiltonians of 16; 18 in the three angle factors; 14 for the offsets,
+#   k and the differences), 26 divisions, 6 divisions by 3 (the Lambda/3
+#   terms), 3 sincos.
+#   DOPRI5 attempt: 6 RHS + 328 flops (stage sums 189, y5/y4 117, error norm
+#   21, controller 1) + 5 divisions + 1 sqrt + 1 pow.
+#   RK4 doubling attempt: 10 RHS + 219 flops (stage inputs/sums 207, error
+#   11, controller 1) + 2 divisions + 1 sqrt + 1 pow; one more RHS per
+#   accepted step.
+# With unit weights (division, x/3 and sqrt 1 flop; sincos 70 and pow 113,
+# the flops of their own arithmetic) the counts give 453, 447 and 335.
+RHS_COUNTS = {"flops": 211.0, "div": 26.0, "div3": 6.0, "sincos": 3.0}
+DOPRI5_ATTEMPT_COUNTS = {"flops": 328.0, "div": 5.0, "sqrt": 1.0, "pow": 1.0}
+RK4_ATTEMPT_COUNTS = {"flops": 219.0, "div": 2.0, "sqrt": 1.0, "pow": 1.0}
+UNIT_WEIGHTS = {"div": 1.0, "div3": 1.0, "sqrt": 1.0, "sincos": 70.0, "pow": 113.0}
 # DRAM bytes read + written by one k_trace<ModeBLDopri5> launch on the
 # default 720p frame, from one ncu capture of that launch
 # (dram__bytes_read.sum 0.109 MB + dram__bytes_write.sum 5.450 MB): the
@@ -131,16 +140,22 @@ def stop_clock_sampler(proc, f, path, gpu_index):
             "reasons": sorted(reasons)}
 
 
-def ray_flops(desc, steps, attempts):
-    """Algorithmic FP64 flops of one traced frame from the kernel's counters."""
+def weighted(counts, w):
+    return counts["flops"] + sum(n * w[k] for k, n in counts.items() if k != "flops")
+
+
+def ray_flops(desc, steps, attempts, w=UNIT_WEIGHTS):
+    """Algorithmic FP64 flops of one traced frame from the kernel's counters,
+    with operation weights w (flops per division, x/3, sqrt, sincos, pow)."""
     if desc.bundles or desc.chart == 0 and abs(desc.Lambda) <= 1e-15 or desc.solver_mode != 0:
         return None  # counted only for the standard BL single-ray integrators
     n = desc.width * desc.height
+    f_rhs = weighted(RHS_COUNTS, w)
     if desc.integrator == 1:
         rhs = n + 6.0 * attempts
-        return rhs * FLOPS_BL_RHS + attempts * FLOPS_DOPRI5_ATTEMPT
+        return rhs * f_rhs + attempts * weighted(DOPRI5_ATTEMPT_COUNTS, w)
     rhs = n + 10.0 * attempts + steps
-    return rhs * FLOPS_BL_RHS + attempts * FLOPS_RK4_ATTEMPT
+    return rhs * f_rhs + attempts * weighted(RK4_ATTEMPT_COUNTS, w)
 
 
 def boundary_distance(outcome, pix, radius=8):
@@ -466,7 +481,7 @@ def bench_batch(args, wl, base_cfg, rank, world, local_rank):
                                               "ms_per_step": seq_ms / args.steps},
                        "speedup_vs_per_frame": value / seq_value},
                 roofline=None, roofline_note=(
-                    f"BL frames: {rays_bl} rays, {flops_bl:.4g} algorithmic FP64 flops per step; "
+                    f"BL frames: {rays_bl} rays, {flops_bl:.4g} algorithmic FP64 flops per step (unit weights); "
                     "KS RHS flops are not counted, so no whole-batch roofline"),
                 cpu_baseline=cpu,
                 e2e={"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": 0,
@@ -697,7 +712,10 @@ def main():
 
     steps_sum = float(out["steps"].to(torch.int64).sum())
     att_sum = float(out["attempts"].to(torch.int64).sum())
-    flops = ray_flops(desc, steps_sum, att_sum)
+    costs = R.op_costs()
+    weights = {k: costs[k] for k in UNIT_WEIGHTS}
+    flops = ray_flops(desc, steps_sum, att_sum, weights)
+    flops_unit = ray_flops(desc, steps_sum, att_sum)
     peak_gflops = R.fp64_peak_gflops()
     roofline = None
     if flops is not None:
@@ -707,7 +725,12 @@ def main():
                     "frac": achieved / peak,
                     "traffic": TRAFFIC_DOPRI5_720P if args.workload == "knds_bl_dopri5_720p" else None,
                     "peak_source": "measured in this run: kt_measure_fp64_peak (dependent FMA chains, all SMs)",
-                    "flops_per_frame": flops, "rhs_per_ray": (n + 6.0 * att_sum) / n
+                    "flops_per_frame": flops,
+                    "op_weights_flops": {k: round(v, 2) for k, v in weights.items()},
+                    "op_weights_source": "measured in this run: kt_measure_op_costs (throughput against FMA)",
+                    "frac_unit_weights": flops_unit / (kernel_ms * 1e-3) / 1e12 / peak,
+                    "flops_per_frame_unit_weights": flops_unit,
+                    "rhs_per_ray": (n + 6.0 * att_sum) / n
                     if desc.integrator == 1 else (n + 10.0 * att_sum + steps_sum) / n,
                     "kernel_ms": kernel_ms}
 

@@ -380,6 +380,20 @@ kt_status kt_l2_grad_pixels(kt_context* ctx, const kt_frame_desc* desc, const ui
  * per FMA): the non-tensor FP64 peak the trace kernels are bounded by. */
 kt_status kt_measure_fp64_peak(kt_context* ctx, double* gflops);
 
+/* Measured cost of the operations that the algorithmic flop count weights,
+ * in flops (2 per FMA, so an operation that takes the time of n FMAs at full
+ * throughput costs 2n): eight independent recurrences per thread on all SMs,
+ * each operation's throughput against the FMA throughput of the same probe. */
+typedef struct kt_op_costs {
+  double fma_gflops; /* FP64 FMA throughput of the probe, GFLOP/s */
+  double div;        /* correctly rounded division */
+  double div3;       /* x / 3, the correctly rounded quotient (three operations) */
+  double sqrt;       /* correctly rounded square root */
+  double sincos;     /* sin and cos of one argument (the renderer's libm) */
+  double pow;        /* pow (the renderer's libm) */
+} kt_op_costs;
+kt_status kt_measure_op_costs(kt_context* ctx, kt_op_costs* out);
+
 /* Deterministic procedural equirectangular star field (RGB8, w*h*3 bytes),
  * the stand-in for the reference's background photographs, which are not in
  * its tree.  Same seed, same image, on any host. */

@@ -87,6 +87,8 @@ def load_library():
     L.kt_elliptic_reasons_host.restype = ctypes.c_int
     L.kt_measure_fp64_peak.argtypes = [P, ctypes.POINTER(D)]
     L.kt_measure_fp64_peak.restype = ctypes.c_int
+    L.kt_measure_op_costs.argtypes = [P, ctypes.POINTER(abi.OpCosts)]
+    L.kt_measure_op_costs.restype = ctypes.c_int
     L.kt_starfield.argtypes = [ctypes.c_uint64, I32, I32, P]
     L.kt_starfield.restype = ctypes.c_int
     L.kt_kgeo_write.argtypes = [ctypes.c_char_p, PD, ctypes.POINTER(GeoSoA)]
@@ -293,6 +295,14 @@ class Renderer:
         v = ctypes.c_double()
         _check(self.L.kt_measure_fp64_peak(self.ctx, ctypes.byref(v)), "kt_measure_fp64_peak", self.ctx)
         return v.value
+
+    def op_costs(self):
+        """kt_measure_op_costs: the measured cost, in flops (2 per FMA), of a
+        division, x/3, sqrt, sincos and pow on this device, and the FMA
+        throughput of the same probe (GFLOP/s)."""
+        v = abi.OpCosts()
+        _check(self.L.kt_measure_op_costs(self.ctx, ctypes.byref(v)), "kt_measure_op_costs", self.ctx)
+        return {f: getattr(v, f) for f, _ in abi.OpCosts._fields_}
 
     def vjp(self, desc, cot_redshift=None, cot_r=None, out=None, flags=0, stream=None, pix=None):
         """kt_vjp: gradient (numpy, kt_frame_desc units, abi.GRAD_NAMES order)

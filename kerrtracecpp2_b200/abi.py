@@ -149,6 +149,14 @@ class GradStats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class OpCosts(ctypes.Structure):
+    """kt_op_costs: measured flops (2 per FMA) of one operation."""
+    _fields_ = [
+        ("fma_gflops", ctypes.c_double), ("div", ctypes.c_double), ("div3", ctypes.c_double),
+        ("sqrt", ctypes.c_double), ("sincos", ctypes.c_double), ("pow", ctypes.c_double),
+    ]
+
+
 # Result arrays of one frame: name -> numpy dtype, in kt_geo_soa order.
 GEO_FIELDS = [
     ("outcome", "u1"), ("r", "f8"), ("redshift", "f8"), ("magnif", "f8"), ("phi_disk", "f8"),

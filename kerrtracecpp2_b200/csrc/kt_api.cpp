@@ -632,4 +632,50 @@ kt_status kt_measure_fp64_peak(kt_context* ctx, double* gflops) {
   return KT_OK;
 }
 
+kt_status kt_measure_op_costs(kt_context* ctx, kt_op_costs* out) {
+  if (!ctx || !out) return KT_ERR_INVALID_ARGUMENT;
+  DeviceGuard g(ctx->device);
+  int sms = 0;
+  KT_CUDA(ctx, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device), "attr");
+  const int block = 256, grid = sms * 8;
+  // iterations per op (about a millisecond each) and the FMA-pipe operations
+  // each recurrence step adds to the measured one
+  const int n_iter[6] = {4096, 512, 512, 512, 64, 32};
+  const double extra[6] = {0.0, 0.0, 1.0, 1.0, 2.0, 1.0};
+  double* d_sink = nullptr;
+  KT_CUDA(ctx, cudaMalloc((void**)&d_sink, grid * sizeof(double)), "probe buffer");
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  double per_iter_ms[6];
+  cudaError_t err = cudaSuccess;
+  for (int op = 0; op < 6 && err == cudaSuccess; ++op) {
+    float best_ms = 1e30f;
+    for (int rep = 0; rep < 4 && err == cudaSuccess; ++rep) {
+      cudaEventRecord(e0, ctx->stream);
+      err = kt::launch_op_probe(op, d_sink, n_iter[op], grid, block, ctx->stream);
+      cudaEventRecord(e1, ctx->stream);
+      if (err == cudaSuccess) err = cudaEventSynchronize(e1);
+      float ms = 0.f;
+      if (err == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess && rep > 0 &&
+          ms < best_ms)
+        best_ms = ms;
+    }
+    per_iter_ms[op] = best_ms / n_iter[op];
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(d_sink);
+  if (err != cudaSuccess) return cuda_fail(ctx, err, "operation-cost probe");
+  double c[6];
+  for (int op = 0; op < 6; ++op) c[op] = 2.0 * (per_iter_ms[op] / per_iter_ms[0] - extra[op]);
+  out->fma_gflops = 2.0 * (double)grid * block * 8.0 / (per_iter_ms[0] * 1e-3) / 1e9;
+  out->div = c[1];
+  out->div3 = c[2];
+  out->sqrt = c[3];
+  out->sincos = c[4];
+  out->pow = c[5];
+  return KT_OK;
+}
+
 }  // extern "C"

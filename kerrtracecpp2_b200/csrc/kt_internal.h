@@ -157,5 +157,8 @@ cudaError_t launch_batch_mixed(Mode mode, int variant, const BatchRays& br, uint
 
 // FP64 throughput probe: n_iter dependent FMA chains per thread.
 cudaError_t launch_fp64_probe(double* out, int n_iter, int grid, int block, cudaStream_t stream);
+// Operation-cost probe (op 0 FMA, 1 division, 2 ktm_div3, 3 sqrt, 4 ktm_sincos,
+// 5 ktm_pow), eight recurrences per thread.
+cudaError_t launch_op_probe(int op, double* out, int n_iter, int grid, int block, cudaStream_t stream);
 
 }  // namespace kt

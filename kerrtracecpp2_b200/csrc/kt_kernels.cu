@@ -356,4 +356,48 @@ cudaError_t launch_fp64_probe(double* out, int n_iter, int grid, int block, cuda
   return cudaGetLastError();
 }
 
+// Throughput of the operations the algorithmic flop count weights (division,
+// x/3, square root, sincos, pow): eight independent recurrences per thread,
+// each step one operation plus `kOpProbeExtra[op]` FMA-pipe operations that
+// keep its argument in range (2.5/x; sqrt(3x); x/3 + 1; 1.2 + 0.3 sin x +
+// 0.001 cos x; 0.3 + 0.5 x^-0.2).  Op 0 is the FMA chain of k_fp64_probe.
+template <int OP>
+__global__ void k_op_probe(double* out, int n_iter) {
+  double v[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) v[j] = 1.0 + (threadIdx.x * 8 + j) * 1e-7;
+  for (int i = 0; i < n_iter; ++i) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      double x = v[j];
+      if (OP == 0) x = fma(x, 0.999999999, 1e-12);
+      if (OP == 1) x = 2.5 / x;
+      if (OP == 2) x = ktm_div3(x) + 1.0;
+      if (OP == 3) x = sqrt(x * 3.0);
+      if (OP == 4) {
+        double sn, cs;
+        ktm_sincos(x, &sn, &cs);
+        x = fma(0.3, sn, fma(1e-3, cs, 1.2));
+      }
+      if (OP == 5) x = fma(0.5, ktm_pow(x, -0.2), 0.3);
+      v[j] = x;
+    }
+  }
+  const double s = ((v[0] + v[1]) + (v[2] + v[3])) + ((v[4] + v[5]) + (v[6] + v[7]));
+  if (s == 12345.678) out[blockIdx.x] = s;  // keeps the recurrences alive
+}
+
+cudaError_t launch_op_probe(int op, double* out, int n_iter, int grid, int block, cudaStream_t stream) {
+  switch (op) {
+    case 0: k_op_probe<0><<<grid, block, 0, stream>>>(out, n_iter); break;
+    case 1: k_op_probe<1><<<grid, block, 0, stream>>>(out, n_iter); break;
+    case 2: k_op_probe<2><<<grid, block, 0, stream>>>(out, n_iter); break;
+    case 3: k_op_probe<3><<<grid, block, 0, stream>>>(out, n_iter); break;
+    case 4: k_op_probe<4><<<grid, block, 0, stream>>>(out, n_iter); break;
+    case 5: k_op_probe<5><<<grid, block, 0, stream>>>(out, n_iter); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
 }  // namespace kt
