@@ -40,6 +40,9 @@ HEADERS = ["ktmath.h", "ktmath_consts.h", "kt_physics.cuh", "kt_machines.cuh", "
 # the reference's arithmetic separate; the mixed-precision kernels are not
 # compared bit for bit and use FMA contraction.
 CU_FLAGS = {"kt_mixed.cu": ["--fmad=true"]}
+# The frame set-up evaluates the independent samples of the horizon scan and
+# the ISCO search on several host threads.
+CXX_FILE_FLAGS = {"kt_frame.cpp": ["-fopenmp"]}
 
 
 def run(cmd, verbose):
@@ -78,14 +81,14 @@ def build(force=False, verbose=False):
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src + ".o")
         if force or newer(o, [s] + hdrs):
-            jobs.append((["g++"] + CXX_FLAGS + ["-c", s, "-o", o], False))
+            jobs.append((["g++"] + CXX_FLAGS + CXX_FILE_FLAGS.get(src, []) + ["-c", s, "-o", o], False))
         objs.append(o)
     # Translation units compile independently: run them in parallel.
     with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
         outs = list(ex.map(lambda j: run(j[0], verbose), jobs))
     ptxas_log = [o for o, (_, is_nvcc) in zip(outs, jobs) if is_nvcc]
     if force or newer(LIB, objs):
-        run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs, verbose)
+        run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lgomp"], verbose)
     cli_src = os.path.join(PKG, "cli", "kerr_tracer.cpp")
     if os.path.exists(cli_src) and (force or newer(CLI, [cli_src, LIB] + hdrs)):
         run(["g++", "-O2", "-std=c++17", "-Wall", "-o", CLI, cli_src, "-L", PKG, "-lkerrtrace",

@@ -13,10 +13,27 @@
 
 #include <algorithm>
 #include <string>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 #include "kt_frame.h"
 
 namespace kt {
+
+// Threads for the independent samples of the horizon scan and the ISCO
+// search (each sample is the same arithmetic as in a serial loop; the pass
+// that reads them is serial).
+static int scan_threads() {
+#ifdef _OPENMP
+  const int n = omp_get_max_threads();
+  return n < 16 ? n : 16;
+#else
+  return 1;
+#endif
+}
 
 static double delta_r(const Metric& g, double r) { return bl_delta_r(g, r, r * r + g.a2); }
 
@@ -65,12 +82,20 @@ static int knds_roots(const Metric& g, double roots[16]) {
   };
   const int samples = 20000;
   const double log_span = ktm_log(rmax / rmin);
-  double prev_r = rmin;
-  double prev_f = delta_r(g, prev_r);
+  std::vector<double> rs(samples + 1), fs(samples + 1);
+  rs[0] = rmin;
+  fs[0] = delta_r(g, rmin);
+#pragma omp parallel for schedule(static) num_threads(scan_threads())
   for (int i = 1; i <= samples; ++i) {
     const double t = (double)i / (double)samples;
-    const double r = rmin * ktm_exp(log_span * t);
-    const double f = delta_r(g, r);
+    rs[i] = rmin * ktm_exp(log_span * t);
+    fs[i] = delta_r(g, rs[i]);
+  }
+  double prev_r = rs[0];
+  double prev_f = fs[0];
+  for (int i = 1; i <= samples; ++i) {
+    const double r = rs[i];
+    const double f = fs[i];
     if (finite(prev_f) && finite(f)) {
       if (prev_f == 0.0) push_root(prev_r);
       if (f == 0.0) push_root(r);
@@ -113,7 +138,7 @@ double host_r_cosmo(const Metric& g) {
 // r_isco (knds_metric.hpp:318-349): Bardeen-Press-Teukolsky closed form for
 // Kerr; otherwise the first radius (1e-4 M steps from 1.05 r_+) where the
 // circular-orbit angular momentum stops decreasing.
-double host_r_isco(const Metric& g) {
+double host_r_isco(const Metric& g, double rh) {
   const double M = g.M, a = g.a;
   if (fabs(g.L) < 1e-15 && fabs(g.Q) < 1e-15) {
     if (fabs(a) < 1e-10) return 6.0 * M;
@@ -131,14 +156,25 @@ double host_r_isco(const Metric& g) {
     const double ut = 1.0 / sqrt(N2);
     return -(G.tp + G.pp * Om) * ut;
   };
-  const double rh = host_r_horizon(g);
+  // The reference's loop: r from 1.05 r_+ in steps of dr (accumulated),
+  // return r at the first step where L(r + dr) < L(r) > 0, else the r that
+  // ends the loop at 30 M.  Here the loop's r values are generated serially
+  // in chunks, L at each r + dr evaluated in parallel, then scanned in order.
   double r = rh * 1.05;
   const double dr = 1e-4 * M;
   double L_prev = L_circ(r);
-  for (; r < 30.0 * M; r += dr) {
-    const double Lc = L_circ(r + dr);
-    if (Lc < L_prev && L_prev > 0.0) return r;
-    L_prev = Lc;
+  const int chunk = 2048;
+  std::vector<double> rv(chunk), Lv(chunk);
+  while (r < 30.0 * M) {
+    int n = 0;
+    for (double x = r; n < chunk && x < 30.0 * M; x += dr) rv[n++] = x;
+#pragma omp parallel for schedule(static) num_threads(scan_threads())
+    for (int j = 0; j < n; ++j) Lv[j] = L_circ(rv[j] + dr);
+    for (int j = 0; j < n; ++j) {
+      if (Lv[j] < L_prev && L_prev > 0.0) return rv[j];
+      L_prev = Lv[j];
+    }
+    r = rv[n - 1] + dr;
   }
   return r;
 }
@@ -250,7 +286,7 @@ kt_status prepare_frame(const kt_frame_desc* d, Frame* f, kt_frame_derived* dv, 
   fr.dlam0 = dmax(dmax(1e-10, d->step_init), 1e-10);
   fr.tol = dmax(1e-10, d->tol);
   const double rh = host_r_horizon(fr.g);
-  const double r_isco = host_r_isco(fr.g);
+  const double r_isco = host_r_isco(fr.g, rh);
   fr.rh_cut = rh * 1.03;
   fr.r_in = r_isco;
   fr.r_out = d->disk_out;

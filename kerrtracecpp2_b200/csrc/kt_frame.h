@@ -10,7 +10,8 @@ namespace kt {
 
 double host_r_horizon(const Metric& g);
 double host_r_cosmo(const Metric& g);
-double host_r_isco(const Metric& g);
+// rh: host_r_horizon(g)
+double host_r_isco(const Metric& g, double rh);
 
 // Validate `d`, apply the reference's fallback rules and clamps, fill the
 // kernel constants `f` and (optionally) the public derived record.

@@ -92,6 +92,24 @@ def test_frame_derive_radii_match_reference():
         assert dv.r_horizon == rh and dv.r_isco == ri
 
 
+def test_frame_derive_radii_match_reference_random_metrics():
+    """Horizon and ISCO of random (M, a, Q, Lambda), both signs of Lambda,
+    against the strict reference build's own r_horizon and r_isco (the
+    scan's samples are evaluated on several threads here)."""
+    if not O.ref_available("strict"):
+        pytest.skip("reference build missing")
+    ref = O.ref("strict")
+    rng = np.random.default_rng(17)
+    for _ in range(40):
+        M = float(rng.uniform(0.5, 2.0))
+        a = float(rng.uniform(-0.99, 0.99)) * M
+        Q = float(rng.uniform(0.0, 0.9)) * M * np.sqrt(max(0.0, 1.0 - (a / M) ** 2))
+        Lam = float(rng.choice([0.0, 1e-4, 3e-3, -2e-4, -1e-3])) / (M * M)
+        dv = kt.frame_derive(abi.frame_desc(M=M, a=a, Q=Q, Lambda=Lam, chart=1, width=4, height=4))
+        assert dv.r_horizon == ref.ref_r_horizon(M, a, Q, Lam), (M, a, Q, Lam)
+        assert dv.r_isco == ref.ref_r_isco(M, a, Q, Lam), (M, a, Q, Lam)
+
+
 @pytest.mark.parametrize("name", sorted(G.cases()))
 def test_frame_derive_matches_oracle(name):
     d = G.desc(name)
