@@ -189,8 +189,11 @@ kt_status kt_trace_pixels(kt_context* ctx, const kt_frame_desc* desc,
 #define KT_NOALLOC_MAX_PIXELS (1u << 20)
 kt_status kt_trace_noalloc(const kt_frame_desc* desc, const kt_geo_soa* out, void* stream);
 
-/* Same as kt_trace but with host buffers: copies in and out inside the
- * call and returns after the results are on the host. */
+/* Same as kt_trace but with host buffers: returns after the results are on
+ * the host.  When every given buffer is page-locked and mapped for the
+ * context's device (cudaHostAlloc, cudaHostRegister), the kernels write the
+ * records into them directly; otherwise they go through a device staging
+ * area and are copied after the trace. */
 kt_status kt_trace_host(kt_context* ctx, const kt_frame_desc* desc,
                         const kt_geo_soa* out_host);
 

@@ -259,6 +259,18 @@ kt_status kt_trace_pixels(kt_context* ctx, const kt_frame_desc* desc, const uint
   return run_trace(ctx, f, to_out(out), rl, (uint64_t)n, (cudaStream_t)stream);
 }
 
+// The device address of a page-locked host buffer mapped into `device`'s
+// address space (cudaHostAlloc, or cudaHostRegister'd memory), else nullptr.
+static void* mapped_host_ptr(void* p, int device) {
+  if (!p) return nullptr;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return (a.type == cudaMemoryTypeHost && a.device == device) ? a.devicePointer : nullptr;
+}
+
 kt_status kt_trace_host(kt_context* ctx, const kt_frame_desc* desc, const kt_geo_soa* out_host) {
   if (!ctx) return KT_ERR_INVALID_ARGUMENT;
   if (!out_complete(out_host)) return fail(ctx, KT_ERR_INVALID_ARGUMENT, "kt_trace_host: NULL output");
@@ -267,6 +279,32 @@ kt_status kt_trace_host(kt_context* ctx, const kt_frame_desc* desc, const kt_geo
   if (r != KT_OK) return r;
   DeviceGuard g(ctx->device);
   const size_t n = (size_t)desc->width * (size_t)desc->height;
+  // Page-locked, mapped host buffers: the kernels write every ray's record
+  // straight into them, so the transfer overlaps the trace.  Otherwise the
+  // records go to a device staging area and are copied after the trace.
+  {
+    kt_geo_soa m = *out_host;
+    void** fields[] = {(void**)&m.outcome, (void**)&m.r, (void**)&m.redshift, (void**)&m.magnif,
+                       (void**)&m.phi_disk, (void**)&m.theta_esc, (void**)&m.phi_esc,
+                       (void**)&m.status, (void**)&m.steps, (void**)&m.attempts};
+    bool direct = true;
+    for (void** fp : fields) {
+      if (!*fp) continue;
+      void* dp = mapped_host_ptr(*fp, ctx->device);
+      if (!dp) {
+        direct = false;
+        break;
+      }
+      *fp = dp;
+    }
+    if (direct) {
+      kt::RayList rl = {nullptr, nullptr, nullptr, (uint32_t)n};
+      r = run_trace(ctx, f, to_out(&m), rl, n, ctx->stream);
+      if (r != KT_OK) return r;
+      KT_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "trace");
+      return KT_OK;
+    }
+  }
   // 6 float64 arrays, attempts, steps, outcome, status
   const size_t need = n * (6 * 8 + 4 + 4 + 1 + 1) + 256;
   r = ensure(ctx, (void**)&ctx->d_stage, &ctx->stage_cap, need, "staging buffer");

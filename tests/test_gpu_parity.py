@@ -91,6 +91,38 @@ def test_trace_host_equals_device(renderer):
     assert G.mismatches(host, dev) == {k: 0 for k in G.FIELDS}
 
 
+@pytest.mark.parametrize("case", ["cfg1_ks_rk4", "cfg2_bl_dopri5", "elliptic", "partly_pinned"])
+def test_trace_host_into_pinned_buffers(renderer, case):
+    """kt_trace_host with page-locked host buffers (the kernels write into
+    them directly) gives the records of the pageable-buffer call (device
+    staging and copies): a KS frame with its BL fallback launch, the DOPRI5
+    frame, an elliptic-solver frame (whose closed-form kernel reads and
+    rewrites the records), and buffers of which only some are page-locked."""
+    import ctypes
+
+    import torch
+
+    import kerrtracecpp2_b200 as kt
+
+    if case == "elliptic":
+        d = abi.frame_desc(chart=abi.KT_CHART_KS, a=0.5, width=96, height=54, fov_deg=45.0,
+                           solver_mode=abi.KT_SOLVER_ELLIPTIC_CLOSED)
+    else:
+        d = G.desc("cfg2_bl_dopri5" if case == "partly_pinned" else case)
+    n = d.width * d.height
+    ref = renderer.trace_host(d)
+    pinned = {k: torch.zeros(n, dtype=getattr(torch, {"u1": "uint8", "u4": "int32", "f8": "float64"}[dt]),
+                             pin_memory=True).numpy() for k, dt in abi.GEO_FIELDS}
+    if case == "partly_pinned":
+        pinned["phi_esc"] = np.zeros(n)
+    st = renderer.L.kt_trace_host(renderer.ctx, ctypes.byref(d),
+                                  ctypes.byref(kt._soa_struct(pinned, kt._np_ptr)))
+    assert st == 0
+    for k, dt in abi.GEO_FIELDS:
+        got = pinned[k].view(np.uint32) if dt == "u4" else pinned[k]
+        assert np.array_equal(G.bits(got), G.bits(ref[k])), k
+
+
 @pytest.mark.parametrize("name", ["cfg1_ks_rk4", "cfg2_bl_dopri5", "cfg3_bundles", "cfg5_ks",
                                   "seven_by_three", "retrograde", "ads_lambda", "offsets"])
 def test_render_matches_reference_colour(renderer, name):
