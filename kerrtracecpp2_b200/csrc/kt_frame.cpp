@@ -17,22 +17,34 @@
 
 #ifdef _OPENMP
 #include <omp.h>
+#include <unistd.h>
 #endif
 
 #include "kt_frame.h"
 
 namespace kt {
 
-// Threads for the independent samples of the horizon scan and the ISCO
-// search (each sample is the same arithmetic as in a serial loop; the pass
-// that reads them is serial).
-static int scan_threads() {
+// f(0) .. f(n-1), independent of one another: the samples of the horizon
+// scan and the ISCO search (each the same arithmetic as in a serial loop;
+// the pass that reads them is serial).  Up to 16 host threads; serial in a
+// process forked from the one whose OpenMP thread pool exists, where that
+// pool is unusable.
+template <class F>
+static void for_each_sample(int n, F&& f) {
+  int threads = 1;
 #ifdef _OPENMP
-  const int n = omp_get_max_threads();
-  return n < 16 ? n : 16;
-#else
-  return 1;
+  static const pid_t owner = getpid();
+  if (getpid() == owner) {
+    threads = omp_get_max_threads();
+    if (threads > 16) threads = 16;
+  }
+  if (threads > 1 && n > 1) {
+#pragma omp parallel for schedule(static) num_threads(threads)
+    for (int i = 0; i < n; ++i) f(i);
+    return;
+  }
 #endif
+  for (int i = 0; i < n; ++i) f(i);
 }
 
 static double delta_r(const Metric& g, double r) { return bl_delta_r(g, r, r * r + g.a2); }
@@ -85,12 +97,12 @@ static int knds_roots(const Metric& g, double roots[16]) {
   std::vector<double> rs(samples + 1), fs(samples + 1);
   rs[0] = rmin;
   fs[0] = delta_r(g, rmin);
-#pragma omp parallel for schedule(static) num_threads(scan_threads())
-  for (int i = 1; i <= samples; ++i) {
+  for_each_sample(samples, [&](int j) {
+    const int i = j + 1;
     const double t = (double)i / (double)samples;
     rs[i] = rmin * ktm_exp(log_span * t);
     fs[i] = delta_r(g, rs[i]);
-  }
+  });
   double prev_r = rs[0];
   double prev_f = fs[0];
   for (int i = 1; i <= samples; ++i) {
@@ -168,8 +180,7 @@ double host_r_isco(const Metric& g, double rh) {
   while (r < 30.0 * M) {
     int n = 0;
     for (double x = r; n < chunk && x < 30.0 * M; x += dr) rv[n++] = x;
-#pragma omp parallel for schedule(static) num_threads(scan_threads())
-    for (int j = 0; j < n; ++j) Lv[j] = L_circ(rv[j] + dr);
+    for_each_sample(n, [&](int j) { Lv[j] = L_circ(rv[j] + dr); });
     for (int j = 0; j < n; ++j) {
       if (Lv[j] < L_prev && L_prev > 0.0) return rv[j];
       L_prev = Lv[j];
