@@ -249,6 +249,38 @@ KT_HD void bl_rhs(const Metric& g, double r, double th, double pr, double pth, d
   k[3] = -(tp - tm) / (2.0 * eps_th);
 }
 
+// Reciprocal and sincos of the mixed-precision right-hand sides, which are
+// not compared bit for bit.  FP64 reciprocal on the device: the hardware seed
+// (rcp.approx.ftz.f64) refined by two Newton-Raphson steps y <- y + y(1 - xy),
+// each of which squares the relative error, to within an ulp of 1/x
+// (arguments outside [1e-300, 1e300] in magnitude take the division); FP32:
+// the correctly rounded __frcp_rn.  sincos on the device: CUDA's double
+// sincos.  On the host both are the renderer's own.
+template <class T>
+KT_HD T mx_rcp(T x) {
+#if defined(__CUDA_ARCH__)
+  if (sizeof(T) == sizeof(float)) return (T)__frcp_rn((float)x);
+  const double xd = (double)x;
+  if (!(fabs(xd) >= 1e-300 && fabs(xd) <= 1e300)) return (T)(1.0 / xd);
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(xd));
+  double e = fma(-xd, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-xd, y, 1.0);
+  return (T)fma(y, e, y);
+#else
+  return (T)1 / x;
+#endif
+}
+
+KT_HD void mx_sincos(double x, double* s, double* c) {
+#if defined(__CUDA_ARCH__)
+  sincos(x, s, c);
+#else
+  ktm_sincos(x, s, c);
+#endif
+}
+
 // Analytic Hamiltonian gradient for the mixed-precision tracer (no
 // counterpart in the reference, which differentiates H by central
 // differences).  With S = Sigma, R = Delta_r, T = Delta_theta, A = r^2+a^2,
@@ -272,20 +304,21 @@ KT_HD void bl_rhs_analytic(const Metric& g, double r_, double th_, double pr_, d
     c = (T)cf;
   } else {
     double sd, cd;
-    ktm_sincos(th_, &sd, &cd);
+    mx_sincos(th_, &sd, &cd);
     sn = (T)sd;
     c = (T)cd;
   }
+  const T third = (T)(1.0 / 3.0);
   const T s2 = sn * sn, sc = sn * c;
   const T r2 = r * r;
   const T A = r2 + a2;
   const T S = r2 + a2 * c * c;
-  const T Lr2_3 = L * r2 / (T)3;
+  const T Lr2_3 = L * r2 * third;
   const T R = A * ((T)1 - Lr2_3) - (T)2 * M * r + Q2;
-  const T Tt = (T)1 + L * a2 * c * c / (T)3;
-  const T iS = (T)1 / S, iR = (T)1 / R, iT = (T)1 / Tt;
+  const T Tt = (T)1 + L * a2 * c * c * third;
+  const T iS = mx_rcp(S), iR = mx_rcp(R), iT = mx_rcp(Tt);
   const bool pole = !(s2 > (T)1e-14);
-  const T is2 = pole ? (T)0 : (T)1 / s2;
+  const T is2 = pole ? (T)0 : mx_rcp(s2);
   // g^{mu nu}
   const T X_tt = A * A * iR - a2 * s2 * iT;
   const T X_tp = iT - A * iR;
@@ -295,7 +328,7 @@ KT_HD void bl_rhs_analytic(const Metric& g, double r_, double th_, double pr_, d
   const T U_pp = xi2 * iS * X_pp;
   // d/dr
   const T dS_r = (T)2 * r;
-  const T dR_r = (T)2 * r * ((T)1 - Lr2_3) - ((T)2 * L * r / (T)3) * A - (T)2 * M;
+  const T dR_r = (T)2 * r * ((T)1 - Lr2_3) - ((T)2 * L * r * third) * A - (T)2 * M;
   const T diS_r = -dS_r * iS * iS, diR_r = -dR_r * iR * iR;
   const T dX_tt_r = (T)2 * A * dS_r * iR + A * A * diR_r;  // dA/dr = dS/dr = 2r
   const T dX_tp_r = -(dS_r * iR + A * diR_r);
@@ -307,7 +340,7 @@ KT_HD void bl_rhs_analytic(const Metric& g, double r_, double th_, double pr_, d
   const T dU_pp_r = xi2 * (diS_r * X_pp + iS * dX_pp_r);
   // d/dtheta
   const T dS_t = -(T)2 * a2 * sc;
-  const T dT_t = -((T)2 * L * a2 / (T)3) * sc;
+  const T dT_t = -((T)2 * L * a2 * third) * sc;
   const T diS_t = -dS_t * iS * iS, diT_t = -dT_t * iT * iT;
   const T dis2_t = pole ? (T)0 : -(T)2 * sc * is2 * is2;
   const T dX_tt_t = -a2 * ((T)2 * sc * iT + s2 * diT_t);
@@ -328,17 +361,6 @@ KT_HD void bl_rhs_analytic(const Metric& g, double r_, double th_, double pr_, d
                             dU_pp_t * pppp));
 }
 
-// Reciprocal in T: correctly rounded on host and device alike.
-template <class T>
-KT_HD T kt_rcp(T x) {
-#if defined(__CUDA_ARCH__)
-  if (sizeof(T) == sizeof(float)) return (T)__frcp_rn((float)x);
-  return (T)__drcp_rn((double)x);
-#else
-  return (T)1 / x;
-#endif
-}
-
 // Analytic KS gradient for the mixed-precision tracer.  With
 // g^ab = eta^ab - H l^a l^b (ingoing, knds_metric.hpp:202-218) the
 // Hamiltonian is H_ham = (eta^ab p_a p_b)/2 - H ell^2/2 with
@@ -356,13 +378,13 @@ KT_HD void ks_rhs_analytic(const Metric& g, double X_, double Y_, double Z_, dou
   const T b = R2 - a2;
   const T r = sqrt((T)0.5 * (b + sqrt(b * b + (T)4 * a2 * Z * Z)));
   const T r2 = r * r;
-  const T ir = kt_rcp(r);
+  const T ir = mx_rcp(r);
   const T D = r2 + a2;
-  const T iD = kt_rcp(D);
-  const T iE = kt_rcp((T)2 * r2 - b);
+  const T iD = mx_rcp(D);
+  const T iE = mx_rcp((T)2 * r2 - b);
   const T drX = X * r * iE, drY = Y * r * iE, drZ = Z * D * ir * iE;
   const T rho2 = r2 + a2 * Z * Z * ir * ir;
-  const T irho2 = kt_rcp(rho2);
+  const T irho2 = mx_rcp(rho2);
   const T N = (T)2 * M * r - Q2;
   const T H = N * irho2;
   const T l1 = (r * X + a * Y) * iD, l2 = (r * Y - a * X) * iD, l3 = Z * ir;

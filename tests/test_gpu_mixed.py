@@ -123,3 +123,27 @@ def test_mixed_error_table_every_config(renderer):
               f"{r[7]:.2e} | {r[8]:.0f} | {r[9]}")
     for r in rows:
         assert r[2] < 1e-3 and r[3] < 5e-6, r
+
+
+def test_mixed_reciprocal_and_sincos():
+    """mx_rcp (hardware seed + two Newton-Raphson steps) is within one ulp
+    of the division on 4 M arguments over the whole exponent range (zero and
+    infinity included), and the device sincos of the mixed path is within
+    4e-16 of the renderer's libm for arguments of order 1."""
+    import os
+    import subprocess
+
+    here = os.path.dirname(os.path.abspath(__file__))
+    root = os.path.dirname(here)
+    exe = os.path.join(here, "_build", "mx_rcp_check")
+    os.makedirs(os.path.dirname(exe), exist_ok=True)
+    nvcc = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "bin", "nvcc")
+    subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17",
+                    "-I", os.path.join(root, "kerrtracecpp2_b200", "csrc"), "-o", exe,
+                    os.path.join(here, "mx_rcp_check.cu")], check=True)
+    out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()
+    vals = dict(zip(out[0::2], out[1::2]))
+    print(vals)
+    assert vals["status"] == "no"  # "no error"
+    assert float(vals["max_rcp_ulp"]) <= 1.0
+    assert float(vals["max_sincos_abs"]) <= 4e-16
