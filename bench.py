@@ -86,9 +86,9 @@ RK4_ATTEMPT_COUNTS = {"flops": 219.0, "div": 2.0, "sqrt": 1.0, "pow": 1.0}
 UNIT_WEIGHTS = {"div": 1.0, "div3": 1.0, "sqrt": 1.0, "sincos": 70.0, "pow": 113.0}
 # DRAM bytes read + written by one k_trace<ModeBLDopri5> launch on the
 # default 720p frame, from one ncu capture of that launch
-# (dram__bytes_read.sum 0.109 MB + dram__bytes_write.sum 5.450 MB): the
+# (dram__bytes_read.sum 0.471 MB + dram__bytes_write.sum 3.600 MB): the
 # frame's 52.5 MB of outputs stay in L2 during the launch.
-TRAFFIC_DOPRI5_720P = 5.559552e6
+TRAFFIC_DOPRI5_720P = 4.070144e6
 
 
 def env_int(name, default):
