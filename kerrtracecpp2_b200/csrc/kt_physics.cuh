@@ -91,6 +91,16 @@ struct Ang {
   double ct, st2, Ath, dth;
 };
 
+// x / 3 as the IEEE quotient, either as ktm_div3's three operations (kD3,
+// the single-ray kernels) or as the division (the bundle kernel, whose
+// unrolled Hessian of nine metric inverses runs faster with it); both give
+// the same bits.
+template <bool kD3>
+KT_HD double third_of(double x) {
+  return kD3 ? ktm_div3(x) : x / 3.0;
+}
+
+template <bool kD3 = true>
 KT_HD Ang bl_ang(const Metric& g, double th) {
   double st, ct;
   ktm_sincos(th, &st, &ct);
@@ -98,13 +108,14 @@ KT_HD Ang bl_ang(const Metric& g, double th) {
   A.ct = ct;
   A.st2 = st * st;
   A.Ath = (g.a2 * ct) * ct;
-  A.dth = 1.0 + ktm_div3((g.Laa * ct) * ct);
+  A.dth = 1.0 + third_of<kD3>((g.Laa * ct) * ct);
   return A;
 }
 
 // Delta_r, knds_metric.hpp:51
+template <bool kD3 = true>
 KT_HD double bl_delta_r(const Metric& g, double r, double r2a2) {
-  return ((r2a2 * (1.0 - ktm_div3((g.L * r) * r))) - g.twoM * r) + g.Q2;
+  return ((r2a2 * (1.0 - third_of<kD3>((g.L * r) * r))) - g.twoM * r) + g.Q2;
 }
 
 // Non-zero entries of g^{mu nu} (contravariant_BL, knds_metric.hpp:99-117).
@@ -112,11 +123,12 @@ struct Inv {
   double tt, tp, rr, hh, pp;  // g^tt, g^tphi, g^rr, g^thth, g^phiphi
 };
 
+template <bool kD3 = true>
 KT_HD Inv bl_inv(const Metric& g, double r, const Ang& A) {
   const double r_sq = r * r;
   const double sig = r_sq + A.Ath;
   const double r2a2 = r_sq + g.a2;
-  const double dr = bl_delta_r(g, r, r2a2);
+  const double dr = bl_delta_r<kD3>(g, r, r2a2);
   const double dth = A.dth;
   const double pre = (sig * dr) * dth;
   Inv U;
@@ -180,26 +192,30 @@ KT_HD Ang ang_select(int i, const Ang& A0, const Ang& Ap, const Ang& Am) {
   return A;
 }
 
-KT_HD void bl_rhs(const Metric& g, double r, double th, double pr, double pth, double pt,
-                  double pphi, double k[5]) {
+// bl_rhs, also handing back the centre's angle factors and g^{mu nu} (the
+// bundle RHS evaluates both again).
+template <bool kD3 = true>
+KT_HD void bl_rhs_centre(const Metric& g, double r, double th, double pr, double pth, double pt,
+                         double pphi, double k[5], Ang* A_c, Inv* U_c) {
   const double eps_r = 1e-5 * dmax(fabs(r), 0.01);
   const double eps_th = 1e-6;
 #if KT_RHS_VARIANT == 2
-  const Ang A0 = bl_ang(g, th);
-  const Inv U0 = bl_inv(g, r, A0);
+  const Ang A0 = bl_ang<kD3>(g, th);
+  const Inv U0 = bl_inv<kD3>(g, r, A0);
   k[0] = U0.rr * pr;
   k[1] = U0.hh * pth;
   k[4] = U0.tp * pt + U0.pp * pphi;
-  const double hp = bl_ham(bl_inv(g, r + eps_r, A0), pr, pth, pt, pphi);
-  const double hm = bl_ham(bl_inv(g, r - eps_r, A0), pr, pth, pt, pphi);
-  const double tp = bl_ham(bl_inv(g, r, bl_ang(g, th + eps_th)), pr, pth, pt, pphi);
-  const double tm = bl_ham(bl_inv(g, r, bl_ang(g, th - eps_th)), pr, pth, pt, pphi);
+  *U_c = U0;
+  const double hp = bl_ham(bl_inv<kD3>(g, r + eps_r, A0), pr, pth, pt, pphi);
+  const double hm = bl_ham(bl_inv<kD3>(g, r - eps_r, A0), pr, pth, pt, pphi);
+  const double tp = bl_ham(bl_inv<kD3>(g, r, bl_ang<kD3>(g, th + eps_th)), pr, pth, pt, pphi);
+  const double tm = bl_ham(bl_inv<kD3>(g, r, bl_ang<kD3>(g, th - eps_th)), pr, pth, pt, pphi);
 #else
   Ang A0, Ap, Am;
   KT_ROLLED
   for (int j = 0; j < 3; ++j) {
     const double x = (j == 0) ? th : (j == 1) ? th + eps_th : th - eps_th;
-    const Ang a = bl_ang(g, x);
+    const Ang a = bl_ang<kD3>(g, x);
     if (j == 0) A0 = a;
     else if (j == 1) Ap = a;
     else Am = a;
@@ -207,18 +223,19 @@ KT_HD void bl_rhs(const Metric& g, double r, double th, double pr, double pth, d
   double hp = 0.0, hm = 0.0, tp = 0.0, tm = 0.0;
 #if KT_RHS_VARIANT == 1
   {
-    const Inv U0 = bl_inv(g, r, A0);
+    const Inv U0 = bl_inv<kD3>(g, r, A0);
     k[0] = U0.rr * pr;
     k[1] = U0.hh * pth;
     k[4] = U0.tp * pt + U0.pp * pphi;
+    *U_c = U0;
   }
   KT_ROLLED
   for (int j = 0; j < 2; ++j) {
     // j = 0: (r + eps_r, theta), (r - eps_r, theta); j = 1: (r, theta +- eps_th)
     const double ra = (j == 0) ? r + eps_r : r;
     const double rb = (j == 0) ? r - eps_r : r;
-    const Inv Ua = bl_inv(g, ra, ang_select(j == 0 ? 0 : 1, A0, Ap, Am));
-    const Inv Ub = bl_inv(g, rb, ang_select(j == 0 ? 0 : 2, A0, Ap, Am));
+    const Inv Ua = bl_inv<kD3>(g, ra, ang_select(j == 0 ? 0 : 1, A0, Ap, Am));
+    const Inv Ub = bl_inv<kD3>(g, rb, ang_select(j == 0 ? 0 : 2, A0, Ap, Am));
     const double ha = bl_ham(Ua, pr, pth, pt, pphi);
     const double hb = bl_ham(Ub, pr, pth, pt, pphi);
     hp = (j == 0) ? ha : hp;
@@ -230,11 +247,12 @@ KT_HD void bl_rhs(const Metric& g, double r, double th, double pr, double pth, d
   KT_ROLLED
   for (int i = 0; i < 5; ++i) {
     const double ri = (i == 1) ? r + eps_r : (i == 2) ? r - eps_r : r;
-    const Inv U = bl_inv(g, ri, ang_select(i == 3 ? 1 : i == 4 ? 2 : 0, A0, Ap, Am));
+    const Inv U = bl_inv<kD3>(g, ri, ang_select(i == 3 ? 1 : i == 4 ? 2 : 0, A0, Ap, Am));
     if (i == 0) {
       k[0] = U.rr * pr;
       k[1] = U.hh * pth;
       k[4] = U.tp * pt + U.pp * pphi;
+      *U_c = U;
     } else {
       const double h = bl_ham(U, pr, pth, pt, pphi);
       hp = (i == 1) ? h : hp;
@@ -247,6 +265,14 @@ KT_HD void bl_rhs(const Metric& g, double r, double th, double pr, double pth, d
 #endif
   k[2] = -(hp - hm) / (2.0 * eps_r);
   k[3] = -(tp - tm) / (2.0 * eps_th);
+  *A_c = A0;
+}
+
+KT_HD void bl_rhs(const Metric& g, double r, double th, double pr, double pth, double pt,
+                  double pphi, double k[5]) {
+  Ang A;
+  Inv U;
+  bl_rhs_centre(g, r, th, pr, pth, pt, pphi, k, &A, &U);
 }
 
 // Reciprocal and sincos of the mixed-precision right-hand sides, which are
@@ -900,23 +926,24 @@ KT_HD double ks_pphi_bl(double r, double th, double ph, double a, double pX, dou
 
 // --------------------------------------------------------------- bundles
 // ray_bundle.hpp:56-214.  Hessian of H by central differences: the 33
-// evaluations fall on 9 distinct (r, theta) points, so 9 g^{mu nu}.
+// evaluations fall on 9 distinct (r, theta) points, so 9 g^{mu nu}; the
+// centre's (U00) and its angle factors come from bl_rhs_centre.
 KT_HD void bundle_hessian(const Metric& g, double r, double th, double pr, double pth, double pt,
-                          double pphi, const Ang& A0, double Hs[4][4]) {
+                          double pphi, const Ang& A0, const Inv& U00, double Hs[4][4]) {
   const double e0 = 1e-5 * (fabs(r) + 0.1);
   const double e1 = 1e-5;
   const double e2 = 1e-5 * (fabs(pr) + 1e-3);
   const double e3 = 1e-5 * (fabs(pth) + 1e-3);
-  const Ang Ap = bl_ang(g, th + e1);
-  const Ang Am = bl_ang(g, th + (-e1));
+  const Ang Ap = bl_ang<false>(g, th + e1);
+  const Ang Am = bl_ang<false>(g, th + (-e1));
   const double rp = r + e0, rm = r + (-e0);
   const double prp = pr + e2, prm = pr + (-e2);
   const double pthp = pth + e3, pthm = pth + (-e3);
   // g^{mu nu} at (r + {0,+,-}e0, theta + {0,+,-}e1)
-  const Inv U00 = bl_inv(g, r, A0), Up0 = bl_inv(g, rp, A0), Um0 = bl_inv(g, rm, A0);
-  const Inv U0p = bl_inv(g, r, Ap), U0m = bl_inv(g, r, Am);
-  const Inv Upp = bl_inv(g, rp, Ap), Upm = bl_inv(g, rp, Am);
-  const Inv Ump = bl_inv(g, rm, Ap), Umm = bl_inv(g, rm, Am);
+  const Inv Up0 = bl_inv<false>(g, rp, A0), Um0 = bl_inv<false>(g, rm, A0);
+  const Inv U0p = bl_inv<false>(g, r, Ap), U0m = bl_inv<false>(g, r, Am);
+  const Inv Upp = bl_inv<false>(g, rp, Ap), Upm = bl_inv<false>(g, rp, Am);
+  const Inv Ump = bl_inv<false>(g, rm, Ap), Umm = bl_inv<false>(g, rm, Am);
   const double H0 = bl_ham(U00, pr, pth, pt, pphi);
   const double e[4] = {e0, e1, e2, e3};
   double vp[4], vm[4];
@@ -952,10 +979,11 @@ KT_HD void bundle_hessian(const Metric& g, double r, double th, double pr, doubl
 // dW = J_s Hess W (dW[i][k], 4x2).
 KT_HD void bundle_rhs(const Metric& g, double r, double th, double pr, double pth, double pt,
                       double pphi, const double W[8], double k[5], double dW[8]) {
-  bl_rhs(g, r, th, pr, pth, pt, pphi, k);
-  const Ang A0 = bl_ang(g, th);
+  Ang A0;
+  Inv U00;
+  bl_rhs_centre<false>(g, r, th, pr, pth, pt, pphi, k, &A0, &U00);
   double Hs[4][4];
-  bundle_hessian(g, r, th, pr, pth, pt, pphi, A0, Hs);
+  bundle_hessian(g, r, th, pr, pth, pt, pphi, A0, U00, Hs);
   double M[4][4];
 #pragma unroll
   for (int j = 0; j < 4; ++j) {

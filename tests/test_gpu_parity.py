@@ -71,6 +71,23 @@ def test_full_720p_frame_properties(renderer):
     assert G.mismatches(sub, want) == {k: 0 for k in G.FIELDS}
 
 
+@pytest.mark.parametrize("kw", [
+    dict(chart=1, bundles=1, a=0.998, theta_deg=60.0, width=1920, height=1080),  # config 3
+    dict(chart=0, a=0.7, Q=0.1, theta_deg=70.0, r_obs=50.0, disk_out=15.0, width=512,
+         height=512),                                                            # config 5
+], ids=["cfg3_1080p", "cfg5_512"])
+def test_full_size_strided_sample(renderer, kw):
+    """Configs 3 and 5 at full size: a strided sample of pixels bit-identical
+    to the oracle, counters included."""
+    d = abi.frame_desc(**kw)
+    a = trace(renderer, d)
+    pix = np.arange(0, d.width * d.height, 1499, dtype=np.uint32)
+    want = O.trace_port(d, pix=pix, counters=True)
+    fields = list(G.FIELDS) + ["steps", "attempts"]
+    sub = {k: a[k][pix] for k in fields}
+    assert G.mismatches(sub, want, fields) == {k: 0 for k in fields}
+
+
 def test_trace_pixels_equals_frame(renderer):
     import torch
 
