@@ -173,7 +173,8 @@ KT_HD Cov bl_cov(const Metric& g, double r, const Ang& A) {
 // dphi_vel at the same (r, theta) as the RHS, so it is the same g^{mu nu}.
 // k = {dr, dtheta, dp_r, dp_theta, dphi}.
 //
-// Three code shapes with identical arithmetic (KT_RHS_VARIANT):
+// Three code shapes with identical arithmetic (KT_RHS_VARIANT, the default of
+// bl_rhs_centre's kVar):
 //   0  the three angles (theta, theta +- 1e-6) and the five inverse metrics
 //      (centre, r +- eps_r, theta +- eps_th) in rolled loops: one copy each;
 //   1  angles rolled; the four finite-difference metrics as two pairs in a
@@ -194,75 +195,76 @@ KT_HD Ang ang_select(int i, const Ang& A0, const Ang& Ap, const Ang& Am) {
 
 // bl_rhs, also handing back the centre's angle factors and g^{mu nu} (the
 // bundle RHS evaluates both again).
-template <bool kD3 = true>
+template <bool kD3 = true, int kVar = KT_RHS_VARIANT>
 KT_HD void bl_rhs_centre(const Metric& g, double r, double th, double pr, double pth, double pt,
                          double pphi, double k[5], Ang* A_c, Inv* U_c) {
   const double eps_r = 1e-5 * dmax(fabs(r), 0.01);
   const double eps_th = 1e-6;
-#if KT_RHS_VARIANT == 2
-  const Ang A0 = bl_ang<kD3>(g, th);
-  const Inv U0 = bl_inv<kD3>(g, r, A0);
-  k[0] = U0.rr * pr;
-  k[1] = U0.hh * pth;
-  k[4] = U0.tp * pt + U0.pp * pphi;
-  *U_c = U0;
-  const double hp = bl_ham(bl_inv<kD3>(g, r + eps_r, A0), pr, pth, pt, pphi);
-  const double hm = bl_ham(bl_inv<kD3>(g, r - eps_r, A0), pr, pth, pt, pphi);
-  const double tp = bl_ham(bl_inv<kD3>(g, r, bl_ang<kD3>(g, th + eps_th)), pr, pth, pt, pphi);
-  const double tm = bl_ham(bl_inv<kD3>(g, r, bl_ang<kD3>(g, th - eps_th)), pr, pth, pt, pphi);
-#else
-  Ang A0, Ap, Am;
-  KT_ROLLED
-  for (int j = 0; j < 3; ++j) {
-    const double x = (j == 0) ? th : (j == 1) ? th + eps_th : th - eps_th;
-    const Ang a = bl_ang<kD3>(g, x);
-    if (j == 0) A0 = a;
-    else if (j == 1) Ap = a;
-    else Am = a;
-  }
+  Ang A0;
   double hp = 0.0, hm = 0.0, tp = 0.0, tm = 0.0;
-#if KT_RHS_VARIANT == 1
-  {
+  if constexpr (kVar == 2) {
+    A0 = bl_ang<kD3>(g, th);
     const Inv U0 = bl_inv<kD3>(g, r, A0);
     k[0] = U0.rr * pr;
     k[1] = U0.hh * pth;
     k[4] = U0.tp * pt + U0.pp * pphi;
     *U_c = U0;
-  }
-  KT_ROLLED
-  for (int j = 0; j < 2; ++j) {
-    // j = 0: (r + eps_r, theta), (r - eps_r, theta); j = 1: (r, theta +- eps_th)
-    const double ra = (j == 0) ? r + eps_r : r;
-    const double rb = (j == 0) ? r - eps_r : r;
-    const Inv Ua = bl_inv<kD3>(g, ra, ang_select(j == 0 ? 0 : 1, A0, Ap, Am));
-    const Inv Ub = bl_inv<kD3>(g, rb, ang_select(j == 0 ? 0 : 2, A0, Ap, Am));
-    const double ha = bl_ham(Ua, pr, pth, pt, pphi);
-    const double hb = bl_ham(Ub, pr, pth, pt, pphi);
-    hp = (j == 0) ? ha : hp;
-    hm = (j == 0) ? hb : hm;
-    tp = (j == 1) ? ha : tp;
-    tm = (j == 1) ? hb : tm;
-  }
-#else
-  KT_ROLLED
-  for (int i = 0; i < 5; ++i) {
-    const double ri = (i == 1) ? r + eps_r : (i == 2) ? r - eps_r : r;
-    const Inv U = bl_inv<kD3>(g, ri, ang_select(i == 3 ? 1 : i == 4 ? 2 : 0, A0, Ap, Am));
-    if (i == 0) {
-      k[0] = U.rr * pr;
-      k[1] = U.hh * pth;
-      k[4] = U.tp * pt + U.pp * pphi;
-      *U_c = U;
+    hp = bl_ham(bl_inv<kD3>(g, r + eps_r, A0), pr, pth, pt, pphi);
+    hm = bl_ham(bl_inv<kD3>(g, r - eps_r, A0), pr, pth, pt, pphi);
+    tp = bl_ham(bl_inv<kD3>(g, r, bl_ang<kD3>(g, th + eps_th)), pr, pth, pt, pphi);
+    tm = bl_ham(bl_inv<kD3>(g, r, bl_ang<kD3>(g, th - eps_th)), pr, pth, pt, pphi);
+  } else {
+    Ang Ap, Am;
+    KT_ROLLED
+    for (int j = 0; j < 3; ++j) {
+      const double x = (j == 0) ? th : (j == 1) ? th + eps_th : th - eps_th;
+      const Ang a = bl_ang<kD3>(g, x);
+      if (j == 0) A0 = a;
+      else if (j == 1) Ap = a;
+      else Am = a;
+    }
+    if constexpr (kVar == 1) {
+      {
+        const Inv U0 = bl_inv<kD3>(g, r, A0);
+        k[0] = U0.rr * pr;
+        k[1] = U0.hh * pth;
+        k[4] = U0.tp * pt + U0.pp * pphi;
+        *U_c = U0;
+      }
+      KT_ROLLED
+      for (int j = 0; j < 2; ++j) {
+        // j = 0: (r + eps_r, theta), (r - eps_r, theta); j = 1: (r, theta +- eps_th)
+        const double ra = (j == 0) ? r + eps_r : r;
+        const double rb = (j == 0) ? r - eps_r : r;
+        const Inv Ua = bl_inv<kD3>(g, ra, ang_select(j == 0 ? 0 : 1, A0, Ap, Am));
+        const Inv Ub = bl_inv<kD3>(g, rb, ang_select(j == 0 ? 0 : 2, A0, Ap, Am));
+        const double ha = bl_ham(Ua, pr, pth, pt, pphi);
+        const double hb = bl_ham(Ub, pr, pth, pt, pphi);
+        hp = (j == 0) ? ha : hp;
+        hm = (j == 0) ? hb : hm;
+        tp = (j == 1) ? ha : tp;
+        tm = (j == 1) ? hb : tm;
+      }
     } else {
-      const double h = bl_ham(U, pr, pth, pt, pphi);
-      hp = (i == 1) ? h : hp;
-      hm = (i == 2) ? h : hm;
-      tp = (i == 3) ? h : tp;
-      tm = (i == 4) ? h : tm;
+      KT_ROLLED
+      for (int i = 0; i < 5; ++i) {
+        const double ri = (i == 1) ? r + eps_r : (i == 2) ? r - eps_r : r;
+        const Inv U = bl_inv<kD3>(g, ri, ang_select(i == 3 ? 1 : i == 4 ? 2 : 0, A0, Ap, Am));
+        if (i == 0) {
+          k[0] = U.rr * pr;
+          k[1] = U.hh * pth;
+          k[4] = U.tp * pt + U.pp * pphi;
+          *U_c = U;
+        } else {
+          const double h = bl_ham(U, pr, pth, pt, pphi);
+          hp = (i == 1) ? h : hp;
+          hm = (i == 2) ? h : hm;
+          tp = (i == 3) ? h : tp;
+          tm = (i == 4) ? h : tm;
+        }
+      }
     }
   }
-#endif
-#endif
   k[2] = -(hp - hm) / (2.0 * eps_r);
   k[3] = -(tp - tm) / (2.0 * eps_th);
   *A_c = A0;
