@@ -136,6 +136,30 @@ KT_HD Dual<N> sm_sqrt(const Dual<N>& x) {
   return r;
 }
 
+// The mixed-precision bundle's variants (not compared bit for bit): the
+// value's reciprocal and sincos from mx_rcp and mx_sincos.
+KT_HD double sm_rcp_fast(double x) { return mx_rcp<double>(x); }
+template <int N>
+KT_HD Dual<N> sm_rcp_fast(const Dual<N>& x) {
+  Dual<N> r;
+  r.v = mx_rcp<double>(x.v);
+  const double s = -r.v * r.v;
+  for (int i = 0; i < N; ++i) r.d[i] = s * x.d[i];
+  return r;
+}
+KT_HD void sm_sincos_fast(double x, double* s, double* c) { mx_sincos(x, s, c); }
+template <int N>
+KT_HD void sm_sincos_fast(const Dual<N>& x, Dual<N>* s, Dual<N>* c) {
+  double sv, cv;
+  mx_sincos(x.v, &sv, &cv);
+  s->v = sv;
+  c->v = cv;
+  for (int i = 0; i < N; ++i) {
+    s->d[i] = cv * x.d[i];
+    c->d[i] = -sv * x.d[i];
+  }
+}
+
 KT_HD void sm_sincos(double x, double* s, double* c) { ktm_sincos(x, s, c); }
 template <int N>
 KT_HD void sm_sincos(const Dual<N>& x, Dual<N>* s, Dual<N>* c) {

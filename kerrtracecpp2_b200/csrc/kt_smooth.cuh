@@ -199,25 +199,37 @@ struct ChartBL {
   static constexpr int kEq = 1;  // theta
   static constexpr double kEqTarget = 1.57079632679489661923;  // M_PI/2 as the reference
 
-  template <class T, bool kPrm = true>
+  // kFast (the mixed-precision bundle): reciprocals and sincos from
+  // mx_rcp / mx_sincos and x/3 as x * (1/3); otherwise the smooth tracer's
+  // arithmetic, identical on host and device.
+  template <class T, bool kPrm = true, bool kFast = false>
   KT_HD static void grad(double M, const SmPrm<T>& P, const T* y, const T* c, T* gy, T* gc, T* gp) {
     const T &r = y[0], &th = y[1], &pr = y[2], &pth = y[3], &pt = c[0], &pph = c[1];
     const T a = P.a, L = P.L;
     const T a2 = a * a;
+    auto third = [](const T& x) -> T {
+      if constexpr (kFast) return x * (1.0 / 3.0);
+      else return x / 3.0;
+    };
+    auto rcp = [](const T& x) -> T {
+      if constexpr (kFast) return sm_rcp_fast(x);
+      else return 1.0 / x;
+    };
     T sn, co;
-    sm_sincos(th, &sn, &co);
+    if constexpr (kFast) sm_sincos_fast(th, &sn, &co);
+    else sm_sincos(th, &sn, &co);
     const T s2 = sn * sn, c2 = co * co, sc = sn * co;
     const T r2 = r * r;
     const T A = r2 + a2;
     const T S = r2 + a2 * c2;
-    const T Lr2_3 = L * r2 / 3.0;
+    const T Lr2_3 = third(L * r2);
     const T R = A * (1.0 - Lr2_3) - 2.0 * M * r + P.Q * P.Q;
-    const T Tt = 1.0 + L * a2 * c2 / 3.0;
-    const T xi = 1.0 + L * a2 / 3.0;
+    const T Tt = 1.0 + third(L * a2 * c2);
+    const T xi = 1.0 + third(L * a2);
     const T xi2 = xi * xi;
-    const T iS = 1.0 / S, iR = 1.0 / R, iT = 1.0 / Tt;
+    const T iS = rcp(S), iR = rcp(R), iT = rcp(Tt);
     const bool pole = !(s2 > 1e-14);
-    const T is2 = pole ? T(0.0) : 1.0 / s2;
+    const T is2 = pole ? T(0.0) : rcp(s2);
     const T Pp = A * pt + a * pph;
     const T W = a2 * s2 * pt * pt + 2.0 * a * pt * pph + pph * pph * is2;
     const T K = R * pr * pr + Tt * pth * pth + xi2 * (W * iT - Pp * Pp * iR);
@@ -234,12 +246,12 @@ struct ChartBL {
     for (int v = 0; v < (kPrm ? 5 : 2); ++v) {
       const T dA = v == 0 ? 2.0 * r : v == 2 ? 2.0 * a : zero;
       const T dS = v == 0 ? 2.0 * r : v == 1 ? -2.0 * a2 * sc : v == 2 ? 2.0 * a * c2 : zero;
-      const T dR = v == 0 ? 2.0 * r * (1.0 - Lr2_3) - (2.0 * L * r / 3.0) * A - 2.0 * M
+      const T dR = v == 0 ? 2.0 * r * (1.0 - Lr2_3) - third(2.0 * L * r) * A - 2.0 * M
                    : v == 2 ? 2.0 * a * (1.0 - Lr2_3)
                    : v == 3 ? 2.0 * P.Q
                    : v == 4 ? -A * r2 / 3.0
                             : zero;
-      const T dT = v == 1 ? -(2.0 * L * a2 / 3.0) * sc
+      const T dT = v == 1 ? -third(2.0 * L * a2) * sc
                    : v == 2 ? 2.0 * L * a * c2 / 3.0
                    : v == 4 ? a2 * c2 / 3.0
                             : zero;
@@ -314,7 +326,7 @@ KT_HD void bundle_rhs_analytic(const Metric& g, const double y[4], double pt, do
   }
   cd[0] = D(pt);
   cd[1] = D(pphi);
-  ChartBL::grad<D, false>(g.M, P, yd, cd, gy, gc, gp);
+  ChartBL::grad<D, false, true>(g.M, P, yd, cd, gy, gc, gp);
   k[0] = gy[2].v;
   k[1] = gy[3].v;
   k[2] = -gy[0].v;
