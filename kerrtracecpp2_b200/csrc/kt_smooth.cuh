@@ -199,18 +199,16 @@ struct ChartBL {
   static constexpr int kEq = 1;  // theta
   static constexpr double kEqTarget = 1.57079632679489661923;  // M_PI/2 as the reference
 
-  // kFast (the mixed-precision bundle): reciprocals and sincos from
-  // mx_rcp / mx_sincos and x/3 as x * (1/3); otherwise the smooth tracer's
+  // x/3 is taken as x * (1/3) (on a Dual, one product per component instead
+  // of a division).  kFast (the mixed-precision bundle): reciprocals and
+  // sincos from mx_rcp / mx_sincos; otherwise the smooth tracer's
   // arithmetic, identical on host and device.
   template <class T, bool kPrm = true, bool kFast = false>
   KT_HD static void grad(double M, const SmPrm<T>& P, const T* y, const T* c, T* gy, T* gc, T* gp) {
     const T &r = y[0], &th = y[1], &pr = y[2], &pth = y[3], &pt = c[0], &pph = c[1];
     const T a = P.a, L = P.L;
     const T a2 = a * a;
-    auto third = [](const T& x) -> T {
-      if constexpr (kFast) return x * (1.0 / 3.0);
-      else return x / 3.0;
-    };
+    auto third = [](const T& x) -> T { return x * (1.0 / 3.0); };
     auto rcp = [](const T& x) -> T {
       if constexpr (kFast) return sm_rcp_fast(x);
       else return 1.0 / x;
@@ -249,14 +247,14 @@ struct ChartBL {
       const T dR = v == 0 ? 2.0 * r * (1.0 - Lr2_3) - third(2.0 * L * r) * A - 2.0 * M
                    : v == 2 ? 2.0 * a * (1.0 - Lr2_3)
                    : v == 3 ? 2.0 * P.Q
-                   : v == 4 ? -A * r2 / 3.0
+                   : v == 4 ? third(-A * r2)
                             : zero;
       const T dT = v == 1 ? -third(2.0 * L * a2) * sc
-                   : v == 2 ? 2.0 * L * a * c2 / 3.0
-                   : v == 4 ? a2 * c2 / 3.0
+                   : v == 2 ? third(2.0 * L * a * c2)
+                   : v == 4 ? third(a2 * c2)
                             : zero;
       const T ds2 = v == 1 ? 2.0 * sc : zero;
-      const T dxi2 = v == 2 ? 2.0 * xi * (2.0 * L * a / 3.0) : v == 4 ? 2.0 * xi * (a2 / 3.0) : zero;
+      const T dxi2 = v == 2 ? 2.0 * xi * third(2.0 * L * a) : v == 4 ? 2.0 * xi * third(a2) : zero;
       const double da = v == 2 ? 1.0 : 0.0;
       const T dP = dA * pt + da * pph;
       const T dW = (v == 2 ? 2.0 * a * s2 * ptpt + 2.0 * pt * pph : zero) + a2 * ds2 * ptpt -
