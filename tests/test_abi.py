@@ -110,6 +110,38 @@ def test_frame_derive_radii_match_reference_random_metrics():
         assert dv.r_isco == ref.ref_r_isco(M, a, Q, Lam), (M, a, Q, Lam)
 
 
+@pytest.mark.filterwarnings("ignore:This process .* is multi-threaded:DeprecationWarning")
+def test_frame_derive_in_forked_child():
+    """The frame set-up's threaded sampling after fork(): a child of a
+    process that has used it derives the same radii (serially) and exits."""
+    import time
+
+    d = abi.frame_desc(chart=1, a=0.9, Q=0.3, Lambda=1e-4, width=4, height=4)
+    want = kt.frame_derive(d)
+    r, w = os.pipe()
+    pid = os.fork()
+    if pid == 0:  # child: no pytest machinery, report through the pipe
+        try:
+            dv = kt.frame_derive(d)
+            os.write(w, f"{dv.r_horizon!r} {dv.r_isco!r}".encode())
+        finally:
+            os._exit(0)
+    os.close(w)
+    deadline = time.time() + 60
+    while time.time() < deadline:
+        done, _ = os.waitpid(pid, os.WNOHANG)
+        if done:
+            break
+        time.sleep(0.05)
+    else:
+        os.kill(pid, 9)
+        os.waitpid(pid, 0)
+        pytest.fail("frame set-up in a forked child did not finish")
+    got = os.read(r, 200).decode().split()
+    os.close(r)
+    assert [float(x) for x in got] == [want.r_horizon, want.r_isco]
+
+
 @pytest.mark.parametrize("name", sorted(G.cases()))
 def test_frame_derive_matches_oracle(name):
     d = G.desc(name)
