@@ -649,6 +649,73 @@ struct KSRk4 {
   }
 };
 
+// ------------------------------------- mixed-precision constraint reprojection
+// Hamiltonian-constraint reprojection (FP64) of the mixed-precision tracer.
+// After an accepted step in the FP32 regime (the new point beyond r_fp32,
+// which is infinite unless the tolerance lets the FP32 right-hand side run),
+// the momenta the integrator evolves are scaled by the lambda that puts the
+// point back on H = 0 -- BL: (p_r, p_theta), with p_t and p_phi constants of
+// motion; KS: (p_X, p_Y, p_Z), with p_T -- when that correction is below
+// 1e-4 (larger ones are not rounding drift).  Returns true when it scaled.
+KT_HD bool bl_reproject(const Frame& f, double r, double th, double* pr, double* pth, double pt,
+                        double pphi) {
+  if (!(r > f.r_fp32)) return false;
+  const Inv U = bl_inv_mx(f.g, r, th);
+  const double kin = U.rr * (*pr) * (*pr) + U.hh * (*pth) * (*pth);
+  const double pot = -((U.tt * pt * pt + 2.0 * U.tp * pt * pphi) + U.pp * pphi * pphi);
+  if (!(kin > 0.0 && pot > 0.0)) return false;
+  const double lam2 = pot / kin;
+  if (!(fabs(lam2 - 1.0) < 2e-4)) return false;
+  const double lam = sqrt(lam2);
+  *pr *= lam;
+  *pth *= lam;
+  return true;
+}
+
+// KS: 2H(lambda) = -p_T^2 + lambda^2 |p|^2 - F (-p_T + lambda m)^2 with
+// m = l_i p_i (the spatial part of l.p), i.e. A lambda^2 + B lambda + C = 0,
+// A = |p|^2 - F m^2, B = 2 F p_T m, C = -p_T^2 (1 + F); the root nearer 1.
+KT_HD bool ks_reproject(const Frame& f, double s[6], double pT) {
+  const Metric& g = f.g;
+  const double X = s[0], Y = s[1], Z = s[2];
+  const double b = ((X * X + Y * Y) + Z * Z) - g.a2;
+  const double r = sqrt(0.5 * (b + sqrt(b * b + 4.0 * g.a2 * Z * Z)));
+  if (!(r > f.r_fp32)) return false;
+  const double ir = mx_rcp(r), iD = mx_rcp(r * r + g.a2);
+  const double rho2 = r * r + g.a2 * Z * Z * ir * ir;
+  const double F = (g.twoM * r - g.Q2) * mx_rcp(rho2);
+  const double m = ((r * X + g.a * Y) * s[3] + (r * Y - g.a * X) * s[4]) * iD + Z * s[5] * ir;
+  const double P2 = (s[3] * s[3] + s[4] * s[4]) + s[5] * s[5];
+  const double A = P2 - F * m * m, B = 2.0 * F * pT * m, C = -pT * pT * (1.0 + F);
+  const double disc = B * B - 4.0 * A * C;
+  if (!(A != 0.0 && disc >= 0.0)) return false;
+  const double q = -0.5 * (B + copysign(sqrt(disc), B));  // roots q/A and C/q
+  const double l1 = q / A, l2 = (q != 0.0) ? C / q : l1;
+  const double lam = (fabs(l1 - 1.0) < fabs(l2 - 1.0)) ? l1 : l2;
+  if (!(fabs(lam - 1.0) < 1e-4)) return false;
+  s[3] *= lam;
+  s[4] *= lam;
+  s[5] *= lam;
+  return true;
+}
+
+// The mixed tracer's step hook: after consume(slot) returned false, with
+// `it0` the step count before it.  RK4 doubling accepts at slot 9 and then
+// evaluates f at the new point (slot -1), which sees the scaled momenta;
+// DOPRI5 accepts at slot 5 and carries f(y5) over (FSAL), so a scaled point
+// has f evaluated again.
+KT_HD void mixed_after_slot(const Frame& f, BLRk4* m, int slot, int) {
+  if (slot == 9 && m->pending) bl_reproject(f, m->r, m->th, &m->pr, &m->pth, m->pt, m->pphi);
+}
+KT_HD void mixed_after_slot(const Frame& f, BLDopri5* m, int slot, int it0) {
+  if (slot == 5 && m->it != it0 &&
+      bl_reproject(f, m->r, m->th, &m->pr, &m->pth, m->pt, m->pphi))
+    m->need_k1 = true;
+}
+KT_HD void mixed_after_slot(const Frame& f, KSRk4* m, int slot, int) {
+  if (slot == 9 && m->pending) ks_reproject(f, m->s, m->pT);
+}
+
 // ---------------------------------------------------- BL Jacobi bundle
 // trace_bundle (ray_bundle.hpp:301-436): RK4 step doubling of the geodesic
 // and the 4x2 deviation matrix W; error control on the geodesic only.

@@ -44,7 +44,10 @@ struct ModeBLRk4Mixed {
     double y[4], k[5];
     m->input(s, y);
     bl_rhs_mixed(f, y, m->pt, m->pphi, k);
-    return m->consume(f, s, k, res);
+    const int it0 = m->it;
+    if (m->consume(f, s, k, res)) return true;
+    mixed_after_slot(f, m, s, it0);
+    return false;
   }
 };
 
@@ -61,7 +64,10 @@ struct ModeBLDopri5Mixed {
     double y[4], k[5];
     m->input(s, y);
     bl_rhs_mixed(f, y, m->pt, m->pphi, k);
-    return m->consume(f, s, k, res);
+    const int it0 = m->it;
+    if (m->consume(f, s, k, res)) return true;
+    mixed_after_slot(f, m, s, it0);
+    return false;
   }
 };
 
@@ -89,7 +95,10 @@ struct ModeKSRk4Mixed {
       ks_rhs_analytic<float>(f.g, y[0], y[1], y[2], y[3], y[4], y[5], m->pT, k);
     else
       ks_rhs_analytic<double>(f.g, y[0], y[1], y[2], y[3], y[4], y[5], m->pT, k);
-    return m->consume(f, s, k, res);
+    const int it0 = m->it;
+    if (m->consume(f, s, k, res)) return true;
+    mixed_after_slot(f, m, s, it0);
+    return false;
   }
 };
 

@@ -309,6 +309,28 @@ KT_HD void mx_sincos(double x, double* s, double* c) {
 #endif
 }
 
+// g^{mu nu} at (r, theta) in FP64 with the mixed path's operations (the
+// mixed tracer's constraint reprojection): the closed forms of
+// bl_rhs_analytic's comment below.
+KT_HD Inv bl_inv_mx(const Metric& g, double r, double th) {
+  double sn, c;
+  mx_sincos(th, &sn, &c);
+  const double third = 1.0 / 3.0;
+  const double s2 = sn * sn, c2 = c * c;
+  const double r2 = r * r, A = r2 + g.a2, S = r2 + g.a2 * c2;
+  const double R = A * (1.0 - g.L * r2 * third) - 2.0 * g.M * r + g.Q2;
+  const double Tt = 1.0 + g.L * g.a2 * c2 * third;
+  const double iS = mx_rcp(S), iR = mx_rcp(R), iT = mx_rcp(Tt);
+  const bool pole = !(s2 > 1e-14);
+  Inv U;
+  U.tt = -g.xi2 * iS * (A * A * iR - g.a2 * s2 * iT);
+  U.tp = g.a * g.xi2 * iS * (iT - A * iR);
+  U.rr = R * iS;
+  U.hh = Tt * iS;
+  U.pp = pole ? 0.0 : g.xi2 * iS * (iT * mx_rcp(s2) - g.a2 * iR);
+  return U;
+}
+
 // Analytic Hamiltonian gradient for the mixed-precision tracer (no
 // counterpart in the reference, which differentiates H by central
 // differences).  With S = Sigma, R = Delta_r, T = Delta_theta, A = r^2+a^2,

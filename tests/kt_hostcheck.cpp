@@ -61,7 +61,9 @@ RayResult run_bl(const Frame& f, const Geo& s) {
         bl_rhs_mixed_host(f, y, m.pt, m.pphi, k);
       else
         bl_rhs(f.g, y[0], y[1], y[2], y[3], m.pt, m.pphi, k);
+      const int it0 = m.it;
       if (m.consume(f, slot, k, &res)) return res;
+      if (f.precision == KT_PREC_MIXED) mixed_after_slot(f, &m, slot, it0);
     }
   }
 }
@@ -133,7 +135,9 @@ RayResult run_ray_standard(const Frame& f, uint32_t pix) {
             ks_rhs_mixed_host(f, y, m.pT, k);
           else
             ks_rhs(f.g, y[0], y[1], y[2], y[3], y[4], y[5], m.pT, k);
+          const int it0 = m.it;
           if (m.consume(f, slot, k, &res)) return res;
+          if (f.precision == KT_PREC_MIXED) mixed_after_slot(f, &m, slot, it0);
         }
       }
     }
