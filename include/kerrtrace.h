@@ -192,8 +192,9 @@ kt_status kt_trace_noalloc(const kt_frame_desc* desc, const kt_geo_soa* out, voi
 /* Same as kt_trace but with host buffers: returns after the results are on
  * the host.  When every given buffer is page-locked and mapped for the
  * context's device (cudaHostAlloc, cudaHostRegister), the kernels write the
- * records into them directly; otherwise they go through a device staging
- * area and are copied after the trace. */
+ * records into them directly (so they must be writable: not registered
+ * with cudaHostRegisterReadOnly); otherwise they go through a device
+ * staging area and are copied after the trace. */
 kt_status kt_trace_host(kt_context* ctx, const kt_frame_desc* desc,
                         const kt_geo_soa* out_host);
 
