@@ -111,7 +111,10 @@ template <int N>
 KT_HD Dual<N> operator/(double a, const Dual<N>& b) {
   Dual<N> r;
   r.v = a / b.v;
-  const double s = -r.v / b.v;
+  // d(a/b) = -(a/b)/b db; for a reciprocal (a = 1) -(1/b)^2 db without a
+  // second division (the value, which the primal branches on, is a / b.v
+  // either way)
+  const double s = (a == 1.0) ? -(r.v * r.v) : -r.v / b.v;
   for (int i = 0; i < N; ++i) r.d[i] = s * b.d[i];
   return r;
 }
