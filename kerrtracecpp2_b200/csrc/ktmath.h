@@ -192,23 +192,24 @@ KTM_FN double ktm_cos(double x) {
 
 /* ------------------------------------------------------------- x / 3 */
 
-/* x / 3.0, the correctly rounded IEEE quotient, in three operations instead
- * of a division (the metric's Lambda/3 terms divide by 3 five times per
- * inverse metric).  Method: one correction step of P. Markstein (IBM J. Res.
- * Dev. 34(1), 1990) applied to q0 = RN(x y), y = RN(1/3) = (2^54 - 1)/(3 2^54):
- *   |x y - x/3| = (x/3) 2^-54 < ulp(x/3)/2, so |q0 - x/3| < ulp(x/3);
- *   r = x - 3 q0 is then a small multiple of ulp(q0), exact in one fma;
- *   q0 + r y = x/3 + (1 - 3y)(q0 - x/3) is within 2^-54 ulp of x/3,
- * while x/3 in units of its ulp is an integer over 3, at least 1/6 ulp from
- * any rounding midpoint; so RN(q0 + r y) = RN(x/3).  Zero, subnormal,
- * near-overflow, Inf and NaN arguments take the division operator. */
-KTM_FN double ktm_div3(double x) {
+/* x / b for a small odd constant b, the correctly rounded IEEE quotient, in
+ * three operations instead of a division (ktm_div3: the metric's Lambda/3
+ * terms).  Method: one correction step of P. Markstein (IBM J. Res. Dev.
+ * 34(1), 1990) applied to q0 = RN(x y), y = RN(1/b), for which
+ * |1 - b y| = 2^-54 (b = 3; it is 2^-56 for b = 15):
+ *   |x y - x/b| = (x/b) |1 - b y| < ulp(x/b)/2, so |q0 - x/b| < ulp(x/b);
+ *   r = x - b q0 is then a small multiple of ulp(q0), exact in one fma;
+ *   q0 + r y = x/b + (1 - b y)(q0 - x/b) is within 2^-54 ulp of x/b,
+ * while x/b in units of its ulp is an integer over the odd b, at least
+ * 1/(2b) ulp from any rounding midpoint; so RN(q0 + r y) = RN(x/b).  Zero,
+ * subnormal, near-overflow, Inf and NaN arguments take the division. */
+KTM_FN double ktm_div_odd(double x, double b, double y) {
   const uint32_t e = (uint32_t)(ktm_bits(x) >> 52) & 0x7ffu;
-  if (e - 64u >= 1936u) return x / 3.0;
-  const double y = 0x1.5555555555555p-2;
+  if (e - 64u >= 1936u) return x / b;
   const double q0 = x * y;
-  return fma(fma(-3.0, q0, x), y, q0);
+  return fma(fma(-b, q0, x), y, q0);
 }
+KTM_FN double ktm_div3(double x) { return ktm_div_odd(x, 3.0, 0x1.5555555555555p-2); }
 
 /* -------------------------------------------------------------------- exp */
 
