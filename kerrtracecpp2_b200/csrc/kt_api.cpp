@@ -4,6 +4,7 @@
 // and records a message readable with kt_last_error().  There is no CPU
 // tracing path: without a CUDA device the trace calls fail with
 // KT_ERR_NO_DEVICE.
+#include <cmath>
 #include <cuda_runtime.h>
 #include <stdio.h>
 #include <string.h>
@@ -492,6 +493,7 @@ kt_status kt_render_spp_host(kt_context* ctx, const kt_frame_desc* desc, const k
   br.list = nullptr;
   br.n_dev = nullptr;
   br.n = nt;
+  br.fp32 = std::isfinite(f.r_fp32);
   // the single-frame launch shapes: 64 x 9 for the exact BL kernels, 128 x 1 otherwise
   auto variant = [](kt::Mode md) { return (md == kt::kModeBLRk4 || md == kt::kModeBLDopri5) ? 0 : 1; };
   kt::LaunchShape ls;

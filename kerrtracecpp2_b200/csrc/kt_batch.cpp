@@ -10,6 +10,7 @@
 // group's persistent launch (KS groups: then the BL launch over the rays
 // whose KS initialisation failed, main.cpp:1537-1538; separable-Kerr
 // groups: the BL RK4 launch over the rays that gave up) -> join.
+#include <cmath>
 #include <cuda_runtime.h>
 #include <string.h>
 
@@ -36,6 +37,7 @@ struct Group {
   kt::Mode mode;
   kt::Mode fb_mode = kt::kModeBLRk4;  // BL launch over the fallback list
   std::vector<int> frames;  // batch frame indices
+  bool fp32 = false;        // some frame may run the mixed FP32 right-hand side
   uint64_t n_rays = 0;
   kt::Frame* d_frames = nullptr;
   kt::OutSoA* d_outs = nullptr;
@@ -91,6 +93,7 @@ kt::BatchRays group_rays(const Group& g, const uint32_t* list, const uint32_t* n
   br.list = list;
   br.n_dev = n_dev;
   br.n = n;
+  br.fp32 = g.fp32;
   return br;
 }
 
@@ -305,6 +308,7 @@ kt_status kt_batch_create(kt_context* ctx, const kt_frame_desc* descs, const kt_
     }
     Group& g = b->groups[group_of_key[key]];
     g.frames.push_back(i);
+    g.fp32 = g.fp32 || std::isfinite(frames[i].r_fp32);
     if (frames[i].solver == KT_SOLVER_ELLIPTIC_CLOSED) {
       g.ell_frames.push_back(frames[i]);
       g.ell_outs.push_back(to_out(&outs[i]));

@@ -136,6 +136,9 @@ struct BatchRays {
   const uint32_t* list;
   const uint32_t* n_dev;
   uint64_t n;
+  // some frame may run the mixed tracer's FP32 right-hand side (a finite
+  // r_fp32): selects the mixed kernels that carry the FP32 branch
+  bool fp32 = true;
 };
 
 // Launch-shape variants the batch autotuner chooses from: (threads per

@@ -657,8 +657,8 @@ struct KSRk4 {
 // point back on H = 0 -- BL: (p_r, p_theta), with p_t and p_phi constants of
 // motion; KS: (p_X, p_Y, p_Z), with p_T -- when that correction is below
 // 1e-4 (larger ones are not rounding drift).  Returns true when it scaled.
-KT_HD bool bl_reproject(const Frame& f, double r, double th, double* pr, double* pth, double pt,
-                        double pphi) {
+KT_HD_CALL bool bl_reproject(const Frame& f, double r, double th, double* pr, double* pth,
+                             double pt, double pphi) {
   if (!(r > f.r_fp32)) return false;
   const Inv U = bl_inv_mx(f.g, r, th);
   const double kin = U.rr * (*pr) * (*pr) + U.hh * (*pth) * (*pth);
@@ -675,7 +675,7 @@ KT_HD bool bl_reproject(const Frame& f, double r, double th, double* pr, double*
 // KS: 2H(lambda) = -p_T^2 + lambda^2 |p|^2 - F (-p_T + lambda m)^2 with
 // m = l_i p_i (the spatial part of l.p), i.e. A lambda^2 + B lambda + C = 0,
 // A = |p|^2 - F m^2, B = 2 F p_T m, C = -p_T^2 (1 + F); the root nearer 1.
-KT_HD bool ks_reproject(const Frame& f, double s[6], double pT) {
+KT_HD_CALL bool ks_reproject(const Frame& f, double s[6], double pT) {
   const Metric& g = f.g;
   const double X = s[0], Y = s[1], Z = s[2];
   const double b = ((X * X + Y * Y) + Z * Z) - g.a2;

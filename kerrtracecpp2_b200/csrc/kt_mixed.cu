@@ -13,6 +13,8 @@
 // diverge between the two paths.  This file is compiled with FMA
 // contraction on; its results are not bit-identical to the reference and
 // are compared with the FP64 oracle statistically.
+#include <cmath>
+
 #include "kt_smooth.cuh"
 #include "kt_trace_kernel.cuh"
 
@@ -31,7 +33,12 @@ __device__ __forceinline__ void bl_rhs_mixed(const Frame& f, const double y[4], 
     bl_rhs_analytic<double>(f.g, y[0], y[1], y[2], y[3], pt, pphi, k);
 }
 
-struct ModeBLRk4Mixed {
+// The single-ray mixed modes come in two instantiations: kFp32 (some frame
+// of the launch has a finite r_fp32) carries the FP32 right-hand side and
+// the constraint reprojection; the other, for tolerances below 1e-8, runs
+// the FP64 analytic RHS alone, without that code in the kernel.
+template <bool kFp32>
+struct ModeBLRk4MixedT {
   using Machine = BLRk4;
   static constexpr int kSlots = BLRk4::kSlots;
   BLRk4* m;
@@ -43,15 +50,21 @@ struct ModeBLRk4Mixed {
   __device__ __forceinline__ bool slot(const Frame& f, int s, RayResult* res) {
     double y[4], k[5];
     m->input(s, y);
-    bl_rhs_mixed(f, y, m->pt, m->pphi, k);
-    const int it0 = m->it;
-    if (m->consume(f, s, k, res)) return true;
-    mixed_after_slot(f, m, s, it0);
-    return false;
+    if constexpr (kFp32) {
+      bl_rhs_mixed(f, y, m->pt, m->pphi, k);
+      const int it0 = m->it;
+      if (m->consume(f, s, k, res)) return true;
+      mixed_after_slot(f, m, s, it0);
+      return false;
+    } else {
+      bl_rhs_analytic<double>(f.g, y[0], y[1], y[2], y[3], m->pt, m->pphi, k);
+      return m->consume(f, s, k, res);
+    }
   }
 };
 
-struct ModeBLDopri5Mixed {
+template <bool kFp32>
+struct ModeBLDopri5MixedT {
   using Machine = BLDopri5;
   static constexpr int kSlots = BLDopri5::kSlots;
   BLDopri5* m;
@@ -63,16 +76,22 @@ struct ModeBLDopri5Mixed {
   __device__ __forceinline__ bool slot(const Frame& f, int s, RayResult* res) {
     double y[4], k[5];
     m->input(s, y);
-    bl_rhs_mixed(f, y, m->pt, m->pphi, k);
-    const int it0 = m->it;
-    if (m->consume(f, s, k, res)) return true;
-    mixed_after_slot(f, m, s, it0);
-    return false;
+    if constexpr (kFp32) {
+      bl_rhs_mixed(f, y, m->pt, m->pphi, k);
+      const int it0 = m->it;
+      if (m->consume(f, s, k, res)) return true;
+      mixed_after_slot(f, m, s, it0);
+      return false;
+    } else {
+      bl_rhs_analytic<double>(f.g, y[0], y[1], y[2], y[3], m->pt, m->pphi, k);
+      return m->consume(f, s, k, res);
+    }
   }
 };
 
 // KS: FP32 beyond r_fp32 unless the radial momentum x.p/|x| is small.
-struct ModeKSRk4Mixed {
+template <bool kFp32>
+struct ModeKSRk4MixedT {
   using Machine = KSRk4;
   static constexpr int kSlots = KSRk4::kSlots;
   KSRk4* m;
@@ -88,17 +107,22 @@ struct ModeKSRk4Mixed {
   __device__ __forceinline__ bool slot(const Frame& f, int s, RayResult* res) {
     double y[6], k[6];
     m->input(s, y);
-    const double rr = sqrt(y[0] * y[0] + y[1] * y[1] + y[2] * y[2]);
-    const double prad = (y[0] * y[3] + y[1] * y[4] + y[2] * y[5]) / rr;
-    const bool far = rr > f.r_fp32 && fabs(prad) > f.turn_frac * fabs(m->pT);
-    if (warp_all(far))
-      ks_rhs_analytic<float>(f.g, y[0], y[1], y[2], y[3], y[4], y[5], m->pT, k);
-    else
+    if constexpr (kFp32) {
+      const double rr = sqrt(y[0] * y[0] + y[1] * y[1] + y[2] * y[2]);
+      const double prad = (y[0] * y[3] + y[1] * y[4] + y[2] * y[5]) / rr;
+      const bool far = rr > f.r_fp32 && fabs(prad) > f.turn_frac * fabs(m->pT);
+      if (warp_all(far))
+        ks_rhs_analytic<float>(f.g, y[0], y[1], y[2], y[3], y[4], y[5], m->pT, k);
+      else
+        ks_rhs_analytic<double>(f.g, y[0], y[1], y[2], y[3], y[4], y[5], m->pT, k);
+      const int it0 = m->it;
+      if (m->consume(f, s, k, res)) return true;
+      mixed_after_slot(f, m, s, it0);
+      return false;
+    } else {
       ks_rhs_analytic<double>(f.g, y[0], y[1], y[2], y[3], y[4], y[5], m->pT, k);
-    const int it0 = m->it;
-    if (m->consume(f, s, k, res)) return true;
-    mixed_after_slot(f, m, s, it0);
-    return false;
+      return m->consume(f, s, k, res);
+    }
   }
 };
 
@@ -125,9 +149,9 @@ struct ModeBundleMixed {
 // together makes it alike (720p config 2 DOPRI5: 24.3 against 31.9 ms; BL
 // RK4: 25.2 against 41.1; KS RK4: 22.3 against 52.1; 1080p bundles: 224
 // against 243).
-template <> struct Shape<ModeBLRk4Mixed> { static constexpr int kBlock = 64, kMinBlocks = 9, kRefill = 32; };
-template <> struct Shape<ModeBLDopri5Mixed> { static constexpr int kBlock = 64, kMinBlocks = 9, kRefill = 32; };
-template <> struct Shape<ModeKSRk4Mixed> { static constexpr int kBlock = 64, kMinBlocks = 9, kRefill = 32; };
+template <bool B> struct Shape<ModeBLRk4MixedT<B>> { static constexpr int kBlock = 64, kMinBlocks = 9, kRefill = 32; };
+template <bool B> struct Shape<ModeBLDopri5MixedT<B>> { static constexpr int kBlock = 64, kMinBlocks = 9, kRefill = 32; };
+template <bool B> struct Shape<ModeKSRk4MixedT<B>> { static constexpr int kBlock = 64, kMinBlocks = 9, kRefill = 32; };
 template <> struct Shape<ModeBundleMixed> { static constexpr int kBlock = 128, kMinBlocks = 1, kRefill = 32; };
 
 template <class ModeT>
@@ -138,11 +162,13 @@ static cudaError_t launch_one(const Frame& f, const OutSoA& out, const RayList& 
   return cudaGetLastError();
 }
 
+// Both instantiations of a mode share its launch bounds, block and shared
+// memory, so one shape (the kFp32 one's) serves either.
 cudaError_t launch_shape_mixed(Mode mode, int device, LaunchShape* shape) {
   switch (mode) {
-    case kModeBLRk4Mixed: return shape_for<ModeBLRk4Mixed>(device, shape);
-    case kModeBLDopri5Mixed: return shape_for<ModeBLDopri5Mixed>(device, shape);
-    case kModeKSRk4Mixed: return shape_for<ModeKSRk4Mixed>(device, shape);
+    case kModeBLRk4Mixed: return shape_for<ModeBLRk4MixedT<true>>(device, shape);
+    case kModeBLDopri5Mixed: return shape_for<ModeBLDopri5MixedT<true>>(device, shape);
+    case kModeKSRk4Mixed: return shape_for<ModeKSRk4MixedT<true>>(device, shape);
     case kModeBundleMixed: return shape_for<ModeBundleMixed>(device, shape);
     default: return cudaErrorInvalidValue;
   }
@@ -151,10 +177,17 @@ cudaError_t launch_shape_mixed(Mode mode, int device, LaunchShape* shape) {
 cudaError_t launch_trace_mixed(Mode mode, const Frame& f, const OutSoA& out, const RayList& rl,
                                uint32_t* queue, const Fallback& fb, const LaunchShape& s,
                                cudaStream_t stream) {
+  const bool fp32 = std::isfinite(f.r_fp32);
   switch (mode) {
-    case kModeBLRk4Mixed: return launch_one<ModeBLRk4Mixed>(f, out, rl, queue, fb, s, stream);
-    case kModeBLDopri5Mixed: return launch_one<ModeBLDopri5Mixed>(f, out, rl, queue, fb, s, stream);
-    case kModeKSRk4Mixed: return launch_one<ModeKSRk4Mixed>(f, out, rl, queue, fb, s, stream);
+    case kModeBLRk4Mixed:
+      return fp32 ? launch_one<ModeBLRk4MixedT<true>>(f, out, rl, queue, fb, s, stream)
+                  : launch_one<ModeBLRk4MixedT<false>>(f, out, rl, queue, fb, s, stream);
+    case kModeBLDopri5Mixed:
+      return fp32 ? launch_one<ModeBLDopri5MixedT<true>>(f, out, rl, queue, fb, s, stream)
+                  : launch_one<ModeBLDopri5MixedT<false>>(f, out, rl, queue, fb, s, stream);
+    case kModeKSRk4Mixed:
+      return fp32 ? launch_one<ModeKSRk4MixedT<true>>(f, out, rl, queue, fb, s, stream)
+                  : launch_one<ModeKSRk4MixedT<false>>(f, out, rl, queue, fb, s, stream);
     case kModeBundleMixed: return launch_one<ModeBundleMixed>(f, out, rl, queue, fb, s, stream);
     default: return cudaErrorInvalidValue;
   }
@@ -162,9 +195,9 @@ cudaError_t launch_trace_mixed(Mode mode, const Frame& f, const OutSoA& out, con
 
 cudaError_t batch_shape_mixed(Mode mode, int variant, int device, LaunchShape* shape) {
   switch (mode) {
-    case kModeBLRk4Mixed: return batch_shape<ModeBLRk4Mixed>(variant, device, shape);
-    case kModeBLDopri5Mixed: return batch_shape<ModeBLDopri5Mixed>(variant, device, shape);
-    case kModeKSRk4Mixed: return batch_shape<ModeKSRk4Mixed>(variant, device, shape);
+    case kModeBLRk4Mixed: return batch_shape<ModeBLRk4MixedT<true>>(variant, device, shape);
+    case kModeBLDopri5Mixed: return batch_shape<ModeBLDopri5MixedT<true>>(variant, device, shape);
+    case kModeKSRk4Mixed: return batch_shape<ModeKSRk4MixedT<true>>(variant, device, shape);
     case kModeBundleMixed: return batch_shape<ModeBundleMixed>(variant, device, shape);
     default: return cudaErrorInvalidValue;
   }
@@ -173,9 +206,15 @@ cudaError_t batch_shape_mixed(Mode mode, int variant, int device, LaunchShape* s
 cudaError_t launch_batch_mixed(Mode mode, int variant, const BatchRays& br, uint32_t* queue,
                                const Fallback& fb, const LaunchShape& s, cudaStream_t st) {
   switch (mode) {
-    case kModeBLRk4Mixed: return batch_launch<ModeBLRk4Mixed>(variant, br, queue, fb, s, st);
-    case kModeBLDopri5Mixed: return batch_launch<ModeBLDopri5Mixed>(variant, br, queue, fb, s, st);
-    case kModeKSRk4Mixed: return batch_launch<ModeKSRk4Mixed>(variant, br, queue, fb, s, st);
+    case kModeBLRk4Mixed:
+      return br.fp32 ? batch_launch<ModeBLRk4MixedT<true>>(variant, br, queue, fb, s, st)
+                     : batch_launch<ModeBLRk4MixedT<false>>(variant, br, queue, fb, s, st);
+    case kModeBLDopri5Mixed:
+      return br.fp32 ? batch_launch<ModeBLDopri5MixedT<true>>(variant, br, queue, fb, s, st)
+                     : batch_launch<ModeBLDopri5MixedT<false>>(variant, br, queue, fb, s, st);
+    case kModeKSRk4Mixed:
+      return br.fp32 ? batch_launch<ModeKSRk4MixedT<true>>(variant, br, queue, fb, s, st)
+                     : batch_launch<ModeKSRk4MixedT<false>>(variant, br, queue, fb, s, st);
     case kModeBundleMixed: return batch_launch<ModeBundleMixed>(variant, br, queue, fb, s, st);
     default: return cudaErrorInvalidValue;
   }
