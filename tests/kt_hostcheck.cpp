@@ -147,6 +147,43 @@ RayResult run_ray_standard(const Frame& f, uint32_t pix) {
 
 }  // namespace
 
+// The mixed tracer's constraint reprojection on one state: the camera ray
+// of pixel `pix` with its evolved momenta scaled by (1 + eps), reprojected;
+// returns 1 when it scaled, and the Hamiltonian (BL: g^{mu nu} of the exact
+// path; KS: the reference's hamiltonian_KS form) before and after, over the
+// scale p_t^2 (BL) or p_T^2 (KS).
+extern "C" int hc_reproject(const kt_frame_desc* d, uint32_t pix, double eps, double* h_before,
+                            double* h_after) {
+  Frame f;
+  std::string err;
+  if (prepare_frame(d, &f, nullptr, &err) != KT_OK) return -1;
+  const Geo s = camera_ray(f, pix);
+  if (f.chart == KT_CHART_BL) {
+    double pr = s.pr * (1.0 + eps), pth = s.pth * (1.0 + eps);
+    auto ham = [&](double a_pr, double a_pth) {
+      const Inv U = bl_inv(f.g, s.r, bl_ang(f.g, s.th));
+      return bl_ham(U, a_pr, a_pth, s.pt, s.pphi) / (s.pt * s.pt);
+    };
+    *h_before = ham(pr, pth);
+    const int done = bl_reproject(f, s.r, s.th, &pr, &pth, s.pt, s.pphi) ? 1 : 0;
+    *h_after = ham(pr, pth);
+    return done;
+  }
+  KSState k;
+  if (!init_ks_state(f.g, s, &k)) return -2;
+  double st[6] = {k.X, k.Y, k.Z, k.pX * (1.0 + eps), k.pY * (1.0 + eps), k.pZ * (1.0 + eps)};
+  auto ham = [&](const double* x) {
+    double G[16];
+    ks_inv(f.g, x[0], x[1], x[2], G);
+    const double p[4] = {k.pT, x[3], x[4], x[5]};
+    return ks_ham(G, p) / (k.pT * k.pT);
+  };
+  *h_before = ham(st);
+  const int done = ks_reproject(f, st, k.pT) ? 1 : 0;
+  *h_after = ham(st);
+  return done;
+}
+
 extern "C" int hc_trace_pixels(const kt_frame_desc* d, int64_t n, const uint32_t* pix,
                                uint8_t* outcome, double* r, double* red, double* magnif,
                                double* phi_disk, double* th_esc, double* ph_esc, uint8_t* status,

@@ -70,3 +70,33 @@ def test_mixed_bundles_close_to_fp64_oracle(hc, name):  # noqa: F811
         assert np.median(eg) < 1e-5 and np.median(er) < 1e-4
         em = np.abs(got["magnif"][disk] - want["magnif"][disk]) / np.abs(want["magnif"][disk])
         assert np.median(em) < 1e-4
+
+
+@pytest.mark.parametrize("chart", [abi.KT_CHART_BL, abi.KT_CHART_KS])
+def test_constraint_reprojection(hc, chart):
+    """The mixed tracer's Hamiltonian-constraint reprojection (host build of
+    bl_reproject / ks_reproject): camera rays whose evolved momenta are
+    scaled by 1 + eps (H = O(eps)) come back onto H = 0 to rounding when
+    the drift is below its 1e-4 bound, and are left alone above it or where
+    the FP32 right-hand side is off (tol below 1e-8)."""
+    import ctypes
+
+    import numpy as np
+
+    hc.hc_reproject.argtypes = [ctypes.POINTER(abi.FrameDesc), ctypes.c_uint32, ctypes.c_double,
+                                ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+    hc.hc_reproject.restype = ctypes.c_int
+    kw = dict(chart=chart, a=0.7, Q=0.2, width=32, height=18, r_obs=50.0, theta_deg=70.0,
+              fov_deg=40.0, precision=abi.KT_PREC_MIXED, tol=1e-7)
+    hb, ha = ctypes.c_double(), ctypes.c_double()
+    rng = np.random.default_rng(5)
+    for pix in rng.integers(0, 32 * 18, 12):
+        for eps in (3e-8, -2e-6, 4e-5):
+            d = abi.frame_desc(**kw)
+            assert hc.hc_reproject(ctypes.byref(d), int(pix), eps, ctypes.byref(hb), ctypes.byref(ha)) == 1
+            assert abs(hb.value) > 1e-9 and abs(ha.value) < 1e-13, (pix, eps, hb.value, ha.value)
+        d = abi.frame_desc(**kw)
+        assert hc.hc_reproject(ctypes.byref(d), int(pix), 1e-3, ctypes.byref(hb), ctypes.byref(ha)) == 0
+        assert ha.value == hb.value
+        d = abi.frame_desc(**dict(kw, tol=1e-9))
+        assert hc.hc_reproject(ctypes.byref(d), int(pix), 1e-5, ctypes.byref(hb), ctypes.byref(ha)) == 0
