@@ -177,11 +177,19 @@ def boundary_distance(outcome, pix, radius=8):
     return worst
 
 
+ORDER_MIN_PIXELS = 1 << 16  # kt_internal.h kOrderMinPixels
+
+
 def trace_launches(dv, desc):
-    """Kernel launches of one kt_trace: the persistent trace kernel, the BL
-    launch over the fallback list (KS chart, semi-analytic solver) and the
-    elliptic-closed kernel."""
+    """Kernel launches of one kt_trace: the centre-out ray order of a whole
+    frame of at least ORDER_MIN_PIXELS pixels (three kernels), the
+    persistent trace kernel, the BL launch over the fallback list (KS chart,
+    semi-analytic solver) and the elliptic-closed kernel."""
+    from kerrtracecpp2_b200 import abi
+
     n = 1
+    if desc.width * desc.height >= ORDER_MIN_PIXELS and desc.precision != abi.KT_PREC_SMOOTH:
+        n += 3
     if not desc.bundles and (dv.chart == 0 or dv.solver == 1):
         n += 1
     if dv.solver == 2:

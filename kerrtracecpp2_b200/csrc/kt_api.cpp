@@ -34,8 +34,31 @@ kt_status shape(kt_context* ctx, kt::Mode m, kt::LaunchShape* s) {
 
 // Launch the trace of rl (and, in the KS chart, the BL pass over the rays
 // whose KS initialisation failed, main.cpp:1537-1538).
+static kt_status run_trace_list(kt_context* ctx, const kt::Frame& f, const kt::OutSoA& out,
+                                const kt::RayList& rl, uint64_t n_max, cudaStream_t st);
+
+// A whole frame of at least kOrderMinPixels pixels (not the smooth tracer)
+// is traced in centre-out order (kt_kernels.cu, launch_ring_order: three
+// small launches on the same stream before the trace), each ray written at
+// its own pixel.  Smaller frames and pixel lists take the row-major order.
 kt_status run_trace(kt_context* ctx, const kt::Frame& f, const kt::OutSoA& out,
                     const kt::RayList& rl, uint64_t n_max, cudaStream_t st) {
+  const int W = f.cam.W, H = f.cam.H;
+  const uint64_t n = (uint64_t)W * (uint64_t)H;
+  if (rl.pix || rl.slot || rl.n_dev || rl.n != n || n < kt::kOrderMinPixels ||
+      f.precision == KT_PREC_SMOOTH)
+    return run_trace_list(ctx, f, out, rl, n_max, st);
+  const size_t words = (size_t)n + kt::ring_scratch_words(n);
+  kt_status r = ensure(ctx, (void**)&ctx->d_order, &ctx->order_cap, words * sizeof(uint32_t),
+                       "ray order");
+  if (r != KT_OK) return r;
+  KT_CUDA(ctx, kt::launch_ring_order(W, H, ctx->d_order + n, ctx->d_order, st), "ray order");
+  const kt::RayList ord = {ctx->d_order, ctx->d_order, nullptr, (uint32_t)n};
+  return run_trace_list(ctx, f, out, ord, n_max, st);
+}
+
+static kt_status run_trace_list(kt_context* ctx, const kt::Frame& f, const kt::OutSoA& out,
+                                const kt::RayList& rl, uint64_t n_max, cudaStream_t st) {
   if (f.precision == KT_PREC_SMOOTH) {
     if (rl.pix || rl.slot || rl.n_dev)
       return fail(ctx, KT_ERR_UNSUPPORTED, "the smooth tracer traces whole frames only");
@@ -224,6 +247,7 @@ void kt_destroy(kt_context* ctx) {
   cudaFree(ctx->d_counters);
   cudaFree(ctx->d_fb);
   cudaFree(ctx->d_stage);
+  cudaFree(ctx->d_order);
   cudaFree(ctx->d_bg);
   cudaFree(ctx->d_grad);
   cudaFree(ctx->d_gsum);

@@ -16,6 +16,9 @@ struct kt_context {
   uint32_t* d_counters = nullptr;  // [0] ray queue, [1] fallback queue, [2] fallback count
   uint32_t* d_fb = nullptr;        // fallback list: pix[cap] then slot[cap]
   size_t fb_cap = 0;
+  // centre-out ray order of a frame (list, then the rings' counts)
+  uint32_t* d_order = nullptr;
+  size_t order_cap = 0;
   // device staging for the host-buffer entry points
   unsigned char* d_stage = nullptr;
   size_t stage_cap = 0;

@@ -237,6 +237,125 @@ cudaError_t launch_elliptic(const Frame& f, const OutSoA& out, const RayList& rl
   return cudaGetLastError();
 }
 
+// ---- centre-out ray order ----------------------------------------------------
+// The camera looks at the black hole, so the image centre holds the shadow
+// and the critical curve, whose rays are the longest, and the edges hold
+// short escaping rays.  A whole frame is traced in rings about the image
+// centre, innermost first, row-major within a ring: the long rays start
+// early and the persistent kernel's tail is short, while a warp's rays stay
+// neighbours (each ring crosses a row in runs of adjacent pixels).  Each
+// ray's arithmetic does not depend on when or beside which rays it runs, so
+// the results are bit for bit those of the row-major trace.  Rings are 4
+// pixels wide, wider where the frame needs more than kOrderClasses of them.
+// The list is a stable counting sort: per-tile ring counts, one exclusive
+// scan in (ring, tile) order, then each tile scattered in pixel order.
+
+struct RingGeom {
+  float cx, cy, inv_w;
+};
+
+__host__ __device__ inline RingGeom ring_geom(int W, int H) {
+  RingGeom g;
+  g.cx = 0.5f * (float)(W - 1);
+  g.cy = 0.5f * (float)(H - 1);
+  const float rmax = sqrtf(g.cx * g.cx + g.cy * g.cy) + 1.0f;
+  const float w = fmaxf(4.0f, rmax / (float)kOrderClasses);
+  g.inv_w = 1.0f / w;
+  return g;
+}
+
+__device__ __forceinline__ int ring_class(const RingGeom& g, int W, uint32_t p) {
+  const int y = (int)(p / (uint32_t)W), x = (int)(p - (uint32_t)y * (uint32_t)W);
+  const float dx = (float)x - g.cx, dy = (float)y - g.cy;
+  return min((int)(sqrtf(dx * dx + dy * dy) * g.inv_w), kOrderClasses - 1);
+}
+
+// counts[c * tiles + t]: pixels of ring c in tile t (tile = `tile` pixels)
+__global__ void k_ring_count(int W, int H, uint32_t tile, uint32_t tiles, uint32_t* __restrict__ counts) {
+  __shared__ uint32_t h[kOrderClasses];
+  for (int i = threadIdx.x; i < kOrderClasses; i += blockDim.x) h[i] = 0;
+  __syncthreads();
+  const RingGeom g = ring_geom(W, H);
+  const uint32_t n = (uint32_t)W * (uint32_t)H;
+  const uint32_t t = blockIdx.x;
+  const uint32_t end = min(n, (t + 1) * tile);
+  for (uint32_t p = t * tile + threadIdx.x; p < end; p += blockDim.x) atomicAdd(&h[ring_class(g, W, p)], 1u);
+  __syncthreads();
+  for (int c = threadIdx.x; c < kOrderClasses; c += blockDim.x) counts[(uint32_t)c * tiles + t] = h[c];
+}
+
+// Exclusive scan of counts[0..m) in place, one block of 1024 threads.
+__global__ void __launch_bounds__(1024) k_ring_scan(uint32_t* __restrict__ a, uint32_t m) {
+  __shared__ uint32_t warp_sum[32];
+  __shared__ uint32_t carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  for (uint32_t base = 0; base < m; base += 1024) {
+    const uint32_t i = base + threadIdx.x;
+    const uint32_t v = (i < m) ? a[i] : 0u;
+    uint32_t x = v;  // inclusive warp scan
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t y = __shfl_up_sync(kFull, x, d);
+      if ((int)lane >= d) x += y;
+    }
+    if (lane == 31) warp_sum[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+      uint32_t s = warp_sum[lane];
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(kFull, s, d);
+        if ((int)lane >= d) s += y;
+      }
+      warp_sum[lane] = s;  // inclusive over warps
+    }
+    __syncthreads();
+    const uint32_t before = carry + (warp ? warp_sum[warp - 1] : 0u) + (x - v);
+    if (i < m) a[i] = before;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += warp_sum[31];
+    __syncthreads();
+  }
+}
+
+// One warp per tile: the tile's pixels in order, each ring's in consecutive
+// places from that ring's offset for the tile.
+__global__ void k_ring_place(int W, int H, uint32_t tile, uint32_t tiles,
+                             const uint32_t* __restrict__ offsets, uint32_t* __restrict__ list) {
+  __shared__ uint32_t next[kOrderClasses];
+  const uint32_t t = blockIdx.x;
+  for (int c = threadIdx.x; c < kOrderClasses; c += 32) next[c] = offsets[(uint32_t)c * tiles + t];
+  __syncwarp();
+  const RingGeom g = ring_geom(W, H);
+  const uint32_t n = (uint32_t)W * (uint32_t)H;
+  const uint32_t end = min(n, (t + 1) * tile);
+  const unsigned lane = threadIdx.x;
+  for (uint32_t p0 = t * tile; p0 < end; p0 += 32) {
+    const uint32_t p = p0 + lane;
+    const int c = (p < end) ? ring_class(g, W, p) : -1;
+    const unsigned same = __match_any_sync(kFull, c);
+    uint32_t at = 0;
+    if (c >= 0) at = next[c] + (uint32_t)__popc(same & ((1u << lane) - 1u));
+    __syncwarp();
+    if (c >= 0) {
+      list[at] = p;
+      if ((int)lane == __ffs(same) - 1) next[c] += (uint32_t)__popc(same);
+    }
+    __syncwarp();
+  }
+}
+
+cudaError_t launch_ring_order(int W, int H, uint32_t* scratch, uint32_t* list, cudaStream_t stream) {
+  const uint64_t n = (uint64_t)W * (uint64_t)H;
+  const uint32_t tile = ring_tile(n), tiles = (uint32_t)((n + tile - 1) / tile);
+  k_ring_count<<<tiles, 256, 0, stream>>>(W, H, tile, tiles, scratch);
+  k_ring_scan<<<1, 1024, 0, stream>>>(scratch, (uint32_t)kOrderClasses * tiles);
+  k_ring_place<<<tiles, 32, 0, stream>>>(W, H, tile, tiles, scratch, list);
+  return cudaGetLastError();
+}
+
 // ---- colour ------------------------------------------------------------------
 
 // One pixel of colorize_buffer (main.cpp:1817-1866), both palettes.  The
