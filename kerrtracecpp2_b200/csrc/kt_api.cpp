@@ -52,7 +52,7 @@ kt_status run_trace(kt_context* ctx, const kt::Frame& f, const kt::OutSoA& out,
   kt_status r = ensure(ctx, (void**)&ctx->d_order, &ctx->order_cap, words * sizeof(uint32_t),
                        "ray order");
   if (r != KT_OK) return r;
-  KT_CUDA(ctx, kt::launch_ring_order(W, H, ctx->d_order + n, ctx->d_order, st), "ray order");
+  KT_CUDA(ctx, kt::launch_ring_order(W, H, 0, ctx->d_order + n, ctx->d_order, st), "ray order");
   const kt::RayList ord = {ctx->d_order, ctx->d_order, nullptr, (uint32_t)n};
   return run_trace_list(ctx, f, out, ord, n_max, st);
 }

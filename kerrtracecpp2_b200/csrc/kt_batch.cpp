@@ -43,6 +43,7 @@ struct Group {
   kt::OutSoA* d_outs = nullptr;
   uint64_t* d_offsets = nullptr;
   uint32_t* d_fb = nullptr;      // groups with a fallback pass only
+  uint32_t* d_order = nullptr;   // the group's rays, each frame in centre-out order
   uint32_t* d_counters = nullptr;
   int variant = 0;
   int refill_min = 1;
@@ -103,7 +104,8 @@ kt::BatchRays group_rays(const Group& g, const uint32_t* list, const uint32_t* n
 cudaError_t enqueue_group(const Group& g, int variant, const kt::LaunchShape& s, int refill_min,
                           const uint32_t* list, uint64_t n, cudaStream_t st) {
   kt::Fallback fb = {g.d_fb, nullptr, g.d_counters + 2};
-  cudaError_t e = kt::launch_batch(g.mode, variant, group_rays(g, list, nullptr, n, refill_min),
+  cudaError_t e = kt::launch_batch(g.mode, variant,
+                                   group_rays(g, list ? list : g.d_order, nullptr, n, refill_min),
                                    g.d_counters, fb, s, st);
   if (e != cudaSuccess) return e;
   if (kt::has_fallback(g.mode))
@@ -322,9 +324,15 @@ kt_status kt_batch_create(kt_context* ctx, const kt_frame_desc* descs, const kt_
   DeviceGuard dg(ctx->device);
   // Device layout.
   size_t bytes = 0;
-  std::vector<size_t> off_frames, off_outs, off_offsets, off_fb;
+  std::vector<size_t> off_frames, off_outs, off_offsets, off_fb, off_order;
+  size_t ring_scratch = 0;
+  for (int i = 0; i < n_frames; ++i)
+    ring_scratch = std::max(ring_scratch,
+                            kt::ring_scratch_words((uint64_t)descs[i].width * (uint64_t)descs[i].height));
   for (const Group& g : b->groups) {
     const size_t nf = g.frames.size();
+    off_order.push_back(bytes);
+    bytes = align256(bytes + g.n_rays * sizeof(uint32_t));
     off_frames.push_back(bytes);
     bytes = align256(bytes + nf * sizeof(kt::Frame));
     off_outs.push_back(bytes);
@@ -337,6 +345,8 @@ kt_status kt_batch_create(kt_context* ctx, const kt_frame_desc* descs, const kt_
   const size_t off_counters = bytes;
   const size_t counters_bytes = b->groups.size() * 4 * sizeof(uint32_t);
   bytes = align256(bytes + counters_bytes);
+  const size_t off_scratch = bytes;
+  bytes = align256(bytes + ring_scratch * sizeof(uint32_t));
   KT_CUDA(ctx, cudaMalloc((void**)&b->d_mem, bytes), "batch buffers");
   uint32_t* d_counters = (uint32_t*)(b->d_mem + off_counters);
   for (size_t gi = 0; gi < b->groups.size(); ++gi) {
@@ -347,6 +357,7 @@ kt_status kt_batch_create(kt_context* ctx, const kt_frame_desc* descs, const kt_
     g.d_offsets = (uint64_t*)(b->d_mem + off_offsets[gi]);
     g.d_fb = kt::has_fallback(g.mode) ? (uint32_t*)(b->d_mem + off_fb[gi]) : nullptr;
     g.d_counters = d_counters + 4 * gi;
+    g.d_order = (uint32_t*)(b->d_mem + off_order[gi]);
     std::vector<kt::Frame> hf(nf);
     std::vector<kt::OutSoA> ho(nf);
     std::vector<uint64_t> hoff(nf + 1, 0);
@@ -362,6 +373,13 @@ kt_status kt_batch_create(kt_context* ctx, const kt_frame_desc* descs, const kt_
             "batch outputs");
     KT_CUDA(ctx, cudaMemcpy(g.d_offsets, hoff.data(), (nf + 1) * sizeof(uint64_t),
                             cudaMemcpyHostToDevice), "batch offsets");
+    for (size_t k = 0; k < nf; ++k) {
+      const kt_frame_desc& dk = descs[g.frames[k]];
+      KT_CUDA(ctx, kt::launch_ring_order(dk.width, dk.height, (uint32_t)hoff[k],
+                                         (uint32_t*)(b->d_mem + off_scratch), g.d_order + hoff[k],
+                                         ctx->stream), "ray order");
+    }
+    KT_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "ray order");
     if (kt::has_fallback(g.mode)) {
       g.fb_variant = default_variant(g.fb_mode);
       KT_CUDA(ctx, kt::batch_shape(g.fb_mode, g.fb_variant, ctx->device, &g.fb_shape), "occupancy query");

@@ -158,10 +158,11 @@ cudaError_t batch_shape_mixed(Mode mode, int variant, int device, LaunchShape* s
 cudaError_t launch_batch_mixed(Mode mode, int variant, const BatchRays& br, uint32_t* queue,
                                const Fallback& fb, const LaunchShape& s, cudaStream_t st);
 
-// Centre-out ray order (kt_kernels.cu): the W x H frame's pixels in rings
-// about the image centre, innermost first, row-major within a ring, into
-// `list` (W*H words); `scratch` holds ring_scratch_words(W*H) words.  Whole
-// frames of at least kOrderMinPixels pixels are traced in this order.
+// Centre-out ray order (kt_kernels.cu): base + the W x H frame's pixels in
+// rings about the image centre, innermost first, row-major within a ring,
+// into `list` (W*H words); `scratch` holds ring_scratch_words(W*H) words.
+// Whole frames of at least kOrderMinPixels pixels are traced in this order,
+// and every frame of a batch (base = the frame's first ray of its group).
 constexpr int kOrderClasses = 512;
 constexpr uint32_t kOrderMinPixels = 1u << 16;
 // pixels per tile of the counting sort: at least 4096, at most 1024 tiles
@@ -174,7 +175,8 @@ inline size_t ring_scratch_words(uint64_t n) {
   const uint32_t tile = ring_tile(n);
   return (size_t)kOrderClasses * (size_t)((n + tile - 1) / tile);
 }
-cudaError_t launch_ring_order(int W, int H, uint32_t* scratch, uint32_t* list, cudaStream_t stream);
+cudaError_t launch_ring_order(int W, int H, uint32_t base, uint32_t* scratch, uint32_t* list,
+                              cudaStream_t stream);
 
 // FP64 throughput probe: n_iter dependent FMA chains per thread.
 cudaError_t launch_fp64_probe(double* out, int n_iter, int grid, int block, cudaStream_t stream);

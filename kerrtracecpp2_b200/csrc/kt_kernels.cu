@@ -323,7 +323,8 @@ __global__ void __launch_bounds__(1024) k_ring_scan(uint32_t* __restrict__ a, ui
 // One warp per tile: the tile's pixels in order, each ring's in consecutive
 // places from that ring's offset for the tile.
 __global__ void k_ring_place(int W, int H, uint32_t tile, uint32_t tiles,
-                             const uint32_t* __restrict__ offsets, uint32_t* __restrict__ list) {
+                             const uint32_t* __restrict__ offsets, uint32_t base,
+                             uint32_t* __restrict__ list) {
   __shared__ uint32_t next[kOrderClasses];
   const uint32_t t = blockIdx.x;
   for (int c = threadIdx.x; c < kOrderClasses; c += 32) next[c] = offsets[(uint32_t)c * tiles + t];
@@ -340,19 +341,20 @@ __global__ void k_ring_place(int W, int H, uint32_t tile, uint32_t tiles,
     if (c >= 0) at = next[c] + (uint32_t)__popc(same & ((1u << lane) - 1u));
     __syncwarp();
     if (c >= 0) {
-      list[at] = p;
+      list[at] = base + p;
       if ((int)lane == __ffs(same) - 1) next[c] += (uint32_t)__popc(same);
     }
     __syncwarp();
   }
 }
 
-cudaError_t launch_ring_order(int W, int H, uint32_t* scratch, uint32_t* list, cudaStream_t stream) {
+cudaError_t launch_ring_order(int W, int H, uint32_t base, uint32_t* scratch, uint32_t* list,
+                              cudaStream_t stream) {
   const uint64_t n = (uint64_t)W * (uint64_t)H;
   const uint32_t tile = ring_tile(n), tiles = (uint32_t)((n + tile - 1) / tile);
   k_ring_count<<<tiles, 256, 0, stream>>>(W, H, tile, tiles, scratch);
   k_ring_scan<<<1, 1024, 0, stream>>>(scratch, (uint32_t)kOrderClasses * tiles);
-  k_ring_place<<<tiles, 32, 0, stream>>>(W, H, tile, tiles, scratch, list);
+  k_ring_place<<<tiles, 32, 0, stream>>>(W, H, tile, tiles, scratch, base, list);
   return cudaGetLastError();
 }
 
