@@ -164,7 +164,10 @@ void kt_frame_desc_defaults(kt_frame_desc* desc);
 void kt_color_params_defaults(kt_color_params* cp);
 
 /* Trace one frame into caller-owned device buffers, asynchronously on
- * `stream` (a cudaStream_t, NULL = legacy default stream). */
+ * `stream` (a cudaStream_t, NULL = legacy default stream).  Frames of at
+ * least 65536 pixels are traced in rings about the image centre, innermost
+ * first (three small kernels build that order on the same stream, in
+ * context scratch); the results are those of any other order, bit for bit. */
 kt_status kt_trace(kt_context* ctx, const kt_frame_desc* desc,
                    const kt_geo_soa* out, void* stream);
 
