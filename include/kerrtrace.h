@@ -182,9 +182,10 @@ kt_status kt_trace_pixels(kt_context* ctx, const kt_frame_desc* desc,
  * frame loop that cannot afford cudaMalloc/cudaFree (they can synchronize
  * the device), passes only its own output buffers: no context, nothing
  * allocated.  The trace kernels' scratch (ray-queue counters, KS fallback
- * list) is a fixed device array inside the library, sized for frames of at
- * most KT_NOALLOC_MAX_PIXELS pixels (8 MiB per GPU, held until the process
- * exits); larger frames return KT_ERR_INVALID_ARGUMENT.  Runs on the
+ * list, the centre-out ray order of whole frames of at least 2^16 pixels, as
+ * kt_trace uses) is a fixed device array inside the library, sized for frames
+ * of at most KT_NOALLOC_MAX_PIXELS pixels (12.5 MiB per GPU, held until the
+ * process exits); larger frames return KT_ERR_INVALID_ARGUMENT.  Runs on the
  * current device, asynchronously on `stream`.  All calls share that array:
  * calls ordered on the device are independent, calls that overlap on the
  * device race.  The first call on a device resolves the array's address for
@@ -196,8 +197,10 @@ kt_status kt_trace_noalloc(const kt_frame_desc* desc, const kt_geo_soa* out, voi
  * the host.  When every given buffer is page-locked and mapped for the
  * context's device (cudaHostAlloc, cudaHostRegister), the kernels write the
  * records into them directly (so they must be writable: not registered
- * with cudaHostRegisterReadOnly); otherwise they go through a device
- * staging area and are copied after the trace. */
+ * with cudaHostRegisterReadOnly, and each must hold width*height entries
+ * inside its page-locked range, as every output buffer must: the kernels
+ * write through the mapping without a bounds check); otherwise they go
+ * through a device staging area and are copied after the trace. */
 kt_status kt_trace_host(kt_context* ctx, const kt_frame_desc* desc,
                         const kt_geo_soa* out_host);
 

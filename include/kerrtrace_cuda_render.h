@@ -15,7 +15,10 @@
 // default controls), with a black background (the call carries none) and
 // returns RGBA packed as 0xFF<<24 | B<<16 | G<<8 | R, as the reference's
 // CUDA kernel does.  Errors throw std::runtime_error, as the reference's
-// CUDA_CHECK does (gpu/cuda/tracer.cu:19-23).
+// CUDA_CHECK does (gpu/cuda/tracer.cu:19-23).  Each calling thread's first
+// call creates a renderer context on device 0 that its later calls reuse
+// (the reference allocates and frees its device buffers on every call); it
+// is destroyed when the thread exits.
 #pragma once
 
 #include <cstdint>

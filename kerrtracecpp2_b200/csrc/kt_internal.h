@@ -166,12 +166,12 @@ cudaError_t launch_batch_mixed(Mode mode, int variant, const BatchRays& br, uint
 constexpr int kOrderClasses = 512;
 constexpr uint32_t kOrderMinPixels = 1u << 16;
 // pixels per tile of the counting sort: at least 4096, at most 1024 tiles
-inline uint32_t ring_tile(uint64_t n) {
+constexpr uint32_t ring_tile(uint64_t n) {
   uint64_t t = (n + 1023) / 1024;
   t = (t + 31) / 32 * 32;
   return (uint32_t)(t < 4096 ? 4096 : t);
 }
-inline size_t ring_scratch_words(uint64_t n) {
+constexpr size_t ring_scratch_words(uint64_t n) {
   const uint32_t tile = ring_tile(n);
   return (size_t)kOrderClasses * (size_t)((n + tile - 1) / tile);
 }

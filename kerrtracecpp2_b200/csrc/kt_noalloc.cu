@@ -8,12 +8,14 @@
 // caller cannot create a kt_context either, because kt_create allocates the
 // context's scratch.  This entry point needs no context.
 //
-// The scratch the trace kernels need -- the ray-queue counters and, in the
-// KS chart, the list of rays handed back to the BL chart -- lives in one
-// file-scope device array below, sized for frames of at most
-// KT_NOALLOC_MAX_PIXELS pixels (8 MiB + 256 bytes).  Every GPU that loads
-// the library holds that array until the process exits.  Larger frames are
-// rejected with KT_ERR_INVALID_ARGUMENT.
+// The scratch the trace kernels need -- the ray-queue counters, in the KS
+// chart the list of rays handed back to the BL chart, and for whole frames
+// of at least 2^16 pixels the centre-out ray order that kt_trace uses (the
+// list and its counting-sort scratch) -- lives in one file-scope device array
+// below, sized for frames of at most KT_NOALLOC_MAX_PIXELS pixels
+// (12.5 MiB + 256 bytes).  Every GPU that loads the library holds that array
+// until the process exits.  Larger frames are rejected with
+// KT_ERR_INVALID_ARGUMENT.
 //
 // All calls share the one array: each call clears the counters on its
 // stream before its kernels run, so calls that are ordered on the device
@@ -35,8 +37,11 @@
 namespace {
 
 constexpr size_t kCounterBytes = 256;  // queue counters, padded to the alignment
+// centre-out order: the ray list (one word per pixel) and the counting sort's scratch
+constexpr size_t kOrderWords =
+    KT_NOALLOC_MAX_PIXELS + kt::ring_scratch_words(KT_NOALLOC_MAX_PIXELS);
 constexpr size_t kScratchBytes =
-    kCounterBytes + 2ull * KT_NOALLOC_MAX_PIXELS * sizeof(uint32_t);
+    kCounterBytes + (2ull * KT_NOALLOC_MAX_PIXELS + kOrderWords) * sizeof(uint32_t);
 
 // The scratch.  In host code `g_noalloc_scratch` only names the symbol; its
 // device address comes from cudaGetSymbolAddress.
@@ -44,7 +49,9 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 constexpr int kMaxDevices = 64;
 std::atomic<unsigned char*> g_scratch_addr[kMaxDevices];
-std::atomic<int> g_shape_ok[kMaxDevices][kt::kNumModes];
+// Launch shapes per (device, mode): state 0 empty, 1 being written by the one
+// thread that claimed it, 2 ready to read.
+std::atomic<int> g_shape_state[kMaxDevices][kt::kNumModes];
 kt::LaunchShape g_shapes[kMaxDevices][kt::kNumModes];
 
 kt_status cuda_status(cudaError_t e) {
@@ -81,14 +88,21 @@ kt::Mode mode_of(const kt::Frame& f) {
 }
 
 kt_status shape(int dev, kt::Mode m, kt::LaunchShape* s) {
-  if (!g_shape_ok[dev][m].load(std::memory_order_acquire)) {
-    kt::LaunchShape t;
-    const cudaError_t e = kt::launch_shape(m, dev, &t);
-    if (e != cudaSuccess) return cuda_status(e);
-    g_shapes[dev][m] = t;
-    g_shape_ok[dev][m].store(1, std::memory_order_release);
+  if (g_shape_state[dev][m].load(std::memory_order_acquire) == 2) {
+    *s = g_shapes[dev][m];
+    return KT_OK;
   }
-  *s = g_shapes[dev][m];
+  kt::LaunchShape t;
+  const cudaError_t e = kt::launch_shape(m, dev, &t);
+  if (e != cudaSuccess) return cuda_status(e);
+  // Publish it once: only the thread that moves the state from 0 to 1 writes
+  // the cache; a thread that finds another writing uses its own copy.
+  int expect = 0;
+  if (g_shape_state[dev][m].compare_exchange_strong(expect, 1, std::memory_order_acq_rel)) {
+    g_shapes[dev][m] = t;
+    g_shape_state[dev][m].store(2, std::memory_order_release);
+  }
+  *s = t;
   return KT_OK;
 }
 
@@ -122,6 +136,7 @@ extern "C" kt_status kt_trace_noalloc(const kt_frame_desc* desc, const kt_geo_so
   uint32_t* counters = reinterpret_cast<uint32_t*>(base);  // [0] queue, [1] fallback queue, [2] fallback count
   uint32_t* fb_pix = reinterpret_cast<uint32_t*>(base + kCounterBytes);
   uint32_t* fb_slot = fb_pix + KT_NOALLOC_MAX_PIXELS;
+  uint32_t* order = fb_slot + KT_NOALLOC_MAX_PIXELS;  // kOrderWords words
   e = cudaMemsetAsync(counters, 0, 4 * sizeof(uint32_t), s);
   if (e != cudaSuccess) return cuda_status(e);
   kt::OutSoA o;
@@ -136,7 +151,16 @@ extern "C" kt_status kt_trace_noalloc(const kt_frame_desc* desc, const kt_geo_so
   o.steps = out->steps;
   o.attempts = out->attempts;
   const uint32_t n = (uint32_t)((int64_t)desc->width * desc->height);
-  const kt::RayList rl = {nullptr, nullptr, nullptr, n};
+  // As kt_trace (run_trace in kt_api.cpp): a whole frame of at least
+  // kOrderMinPixels pixels is traced in centre-out order, each ray written at
+  // its own pixel; smaller frames in row-major order.
+  kt::RayList rl = {nullptr, nullptr, nullptr, n};
+  if (n >= kt::kOrderMinPixels) {
+    if ((size_t)n + kt::ring_scratch_words(n) > kOrderWords) return KT_ERR_INTERNAL;
+    e = kt::launch_ring_order(desc->width, desc->height, 0, order + n, order, s);
+    if (e != cudaSuccess) return cuda_status(e);
+    rl = {order, order, nullptr, n};
+  }
   const kt::Fallback fb = {fb_pix, fb_slot, counters + 2};
   const kt::Mode m = mode_of(f);
   kt::LaunchShape ls;

@@ -13,7 +13,8 @@ gradient's one all-reduce of its few doubles:
   trace_frame_sharded(renderer, desc, group)
                                          each rank traces its tiles
                                          (kt_trace_pixels), rank 0 gathers
-                                         the frame
+                                         the frame (one byte-buffer gather
+                                         of tensors, NCCL on the GPU)
   l2_grad_sharded(renderer, desc, target, w_g, w_r, group)
                                          each rank the gradient of its tiles
                                          (kt_l2_grad_pixels), one all-reduce
@@ -83,35 +84,62 @@ def _dist():
     return dist
 
 
-def trace_frame_sharded(renderer, desc, group=None, tile=16, trace=None, dst=0):
+def _as_tensor(v, device):
+    import torch
+
+    if isinstance(v, torch.Tensor):
+        return v.to(device).contiguous()
+    return torch.from_numpy(np.ascontiguousarray(v)).to(device)
+
+
+def trace_frame_sharded(renderer, desc, group=None, tile=16, trace=None, dst=0, fields=None):
     """Trace one frame split over the ranks of `group` by tiles.  Every rank
     traces its own tiles (kt_trace_pixels on its GPU, or `trace(desc, pix)`
-    returning a dict of numpy arrays per pixel); rank `dst` receives the
-    whole frame as a dict of numpy arrays (the other ranks get None)."""
+    returning a dict of arrays or tensors per pixel); the parts travel to
+    rank `dst` as one byte buffer per rank (each field's bytes, padded to
+    the largest part) in a single gather -- over NCCL for device tensors,
+    gloo for host ones -- and are scattered into the frame there.  Rank
+    `dst` returns the whole frame as a dict of tensors on the parts' device,
+    bit for bit what each rank traced; the other ranks return None.
+    `fields` (default: every field the trace returned) chooses what
+    travels."""
+    import torch
+
     dist = _dist()
     world = dist.get_world_size(group)
     rank = dist.get_rank(group)
-    pix = frame_tiles(desc.width, desc.height, world, rank, tile)
+    parts = [frame_tiles(desc.width, desc.height, world, q, tile) for q in range(world)]
+    pix = parts[rank]
     if trace is None:
-        import torch
-
         dev = torch.device("cuda", renderer.device)
         res = renderer.trace_pixels(desc, torch.from_numpy(pix.astype(np.int32)).to(dev))
-        torch.cuda.synchronize(dev)
-        part = {k: v.cpu().numpy() for k, v in res.items() if v is not None}
     else:
-        part = trace(desc, pix)
-    gathered = [None] * world if rank == dst else None
-    dist.gather_object((pix, part), gathered, dst=dst, group=group)
+        dev = torch.device("cpu")
+        res = trace(desc, pix)
+    keys = sorted(k for k, v in res.items() if v is not None and (fields is None or k in fields))
+    vals = {k: _as_tensor(res[k], dev) for k in keys}
+    m = max(len(p) for p in parts)
+    sizes = {k: vals[k].element_size() for k in keys}
+    row = sum(sizes.values())
+    buf = torch.zeros(m * row, dtype=torch.uint8, device=dev)
+    off = 0
+    for k in keys:
+        nb = len(pix) * sizes[k]
+        buf[off:off + nb] = vals[k].view(torch.uint8)
+        off += m * sizes[k]
+    gathered = [torch.empty_like(buf) for _ in range(world)] if rank == dst else None
+    dist.gather(buf, gathered, dst=dst, group=group)
     if rank != dst:
         return None
     n = desc.width * desc.height
-    frame = {}
-    for p, d in gathered:
-        for k, v in d.items():
-            if k not in frame:
-                frame[k] = np.zeros(n, dtype=v.dtype)
-            frame[k][p] = v
+    frame = {k: torch.zeros(n, dtype=vals[k].dtype, device=dev) for k in keys}
+    for q in range(world):
+        idx = torch.from_numpy(parts[q].astype(np.int64)).to(dev)
+        off = 0
+        for k in keys:
+            nb = len(parts[q]) * sizes[k]
+            frame[k][idx] = gathered[q][off:off + nb].view(vals[k].dtype)
+            off += m * sizes[k]
     return frame
 
 

@@ -22,6 +22,17 @@ geodesic.hpp:326 passes the address of a C99 compound literal,
 `(const double[]){a21}`, which g++ 13 rejects ("taking address of temporary
 array"); it becomes `&a21`, the same value.  Nothing else is edited.
 
+Also, with the reference tree and the renderer's library present:
+  oracle/_ref/kerr_tracer_ref_cuda  the reference's own main.cpp built with
+            -DUSE_CUDA, its CUDA entry point cuda_render (gpu/cuda/tracer.cuh,
+            reached through a forwarding header generated in
+            oracle/_ref/cuda_inc) linked from kerrtracecpp2_b200/libkerrtrace.so
+            instead of gpu/cuda/tracer.cu: the drop-in link check of the
+            replacement library.
+
+The reference tree is found at --reference DIR, else at $KT_REFERENCE_DIR,
+else in a directory named `reference` beside this repository.
+
 Usage: python oracle/build.py [--reference DIR] [--force]
 """
 import argparse
@@ -34,7 +45,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 BUILD = os.path.join(HERE, "_build")
 REF_OUT = os.path.join(HERE, "_ref")
-DEFAULT_REFERENCE = "/root/reference"
+DEFAULT_REFERENCE = os.environ.get("KT_REFERENCE_DIR") or os.path.join(os.path.dirname(ROOT),
+                                                                        "reference")
 
 # Files of the reference tree that main.cpp needs (its own includes).
 REF_FILES = ["main.cpp", "camera.hpp", "geodesic.hpp", "knds_metric.hpp", "ray_bundle.hpp",
@@ -111,7 +123,42 @@ def build_reference(reference, force=False):
     ieee = os.path.join(REF_OUT, "libktref_ieee.so")
     if force or newer(ieee, deps):
         run(["g++"] + common + ["-O3", MARCH, "-shared", "-o", ieee, harness, "-lm"])
+    build_reference_main_cuda(reference, force)
     return strict, stock, ieee
+
+
+REF_CUDA_MAIN = os.path.join(REF_OUT, "kerr_tracer_ref_cuda")
+
+
+def build_reference_main_cuda(reference, force=False):
+    """The reference's main.cpp with -DUSE_CUDA, linked against the
+    replacement library: its render dispatch (main.cpp:2413-2443) calls
+    cuda_render, which the library exports with the reference's signature
+    (include/kerrtrace_cuda_render.h).  Its #include "gpu/cuda/tracer.cuh"
+    resolves to a generated header that includes that restatement.  PNG
+    output goes to the working directory (OUT_DIR ".")."""
+    lib_dir = os.path.join(ROOT, "kerrtracecpp2_b200")
+    lib = os.path.join(lib_dir, "libkerrtrace.so")
+    if not os.path.isdir(reference) or not os.path.exists(lib):
+        return None
+    src_dir = copy_reference(reference)
+    inc = os.path.join(REF_OUT, "cuda_inc", "gpu", "cuda")
+    os.makedirs(inc, exist_ok=True)
+    hdr = os.path.join(inc, "tracer.cuh")
+    text = ('// generated by oracle/build.py: the reference\'s CUDA interface, served by\n'
+            '// the replacement library\n#pragma once\n#include "%s"\n'
+            % os.path.join(ROOT, "include", "kerrtrace_cuda_render.h"))
+    if not os.path.exists(hdr) or open(hdr).read() != text:
+        open(hdr, "w").write(text)
+    deps = [os.path.join(reference, f) for f in REF_FILES] + [hdr, lib,
+                                                             os.path.join(ROOT, "include",
+                                                                          "kerrtrace_cuda_render.h")]
+    if force or newer(REF_CUDA_MAIN, deps):
+        run(["g++", "-std=c++17", "-O2", "-w", "-DUSE_CUDA", "-DOUT_DIR=\".\"",
+             "-I", os.path.join(REF_OUT, "cuda_inc"), "-I", src_dir, "-o", REF_CUDA_MAIN,
+             os.path.join(src_dir, "main.cpp"), "-L", lib_dir, "-lkerrtrace",
+             "-Wl,-rpath," + os.path.relpath(lib_dir, REF_OUT).join(["$ORIGIN/", ""]), "-lm"])
+    return REF_CUDA_MAIN
 
 
 def main():

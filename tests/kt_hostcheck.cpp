@@ -184,13 +184,15 @@ extern "C" int hc_reproject(const kt_frame_desc* d, uint32_t pix, double eps, do
   return done;
 }
 
-extern "C" int hc_trace_pixels(const kt_frame_desc* d, int64_t n, const uint32_t* pix,
-                               uint8_t* outcome, double* r, double* red, double* magnif,
-                               double* phi_disk, double* th_esc, double* ph_esc, uint8_t* status,
-                               uint32_t* steps, uint32_t* attempts) {
+static int trace_pixels(const kt_frame_desc* d, int64_t n, const uint32_t* pix, uint8_t* outcome,
+                        double* r, double* red, double* magnif, double* phi_disk, double* th_esc,
+                        double* ph_esc, uint8_t* status, uint32_t* steps, uint32_t* attempts,
+                        bool fp64_rhs, double tol) {
   Frame f;
   std::string err;
   if (prepare_frame(d, &f, nullptr, &err) != KT_OK) return 1;
+  if (fp64_rhs) f.r_fp32 = INFINITY;
+  if (tol > 0.0) f.tol = tol;
 #pragma omp parallel for schedule(dynamic, 4)
   for (int64_t i = 0; i < n; ++i) {
     const RayResult o = run_ray(f, pix[i]);
@@ -206,6 +208,31 @@ extern "C" int hc_trace_pixels(const kt_frame_desc* d, int64_t n, const uint32_t
     if (attempts) attempts[i] = o.attempts;
   }
   return 0;
+}
+
+extern "C" int hc_trace_pixels(const kt_frame_desc* d, int64_t n, const uint32_t* pix,
+                               uint8_t* outcome, double* r, double* red, double* magnif,
+                               double* phi_disk, double* th_esc, double* ph_esc, uint8_t* status,
+                               uint32_t* steps, uint32_t* attempts) {
+  return trace_pixels(d, n, pix, outcome, r, red, magnif, phi_disk, th_esc, ph_esc, status, steps,
+                      attempts, false, 0.0);
+}
+
+// The mixed tracer (KT_PREC_MIXED frames) with its FP32 right-hand side and
+// constraint reprojection switched off: the analytic FP64 Hamiltonian
+// gradient, on the host with correctly rounded reciprocals and the
+// renderer's sincos, no contraction.  Separates the mixed kernels' own error
+// (FP32, approximate reciprocals and sincos, FMA) from the difference
+// between the analytic gradient and the reference's finite differences.
+// tol > 0 replaces the frame's tolerance after the set-up (which clamps it to
+// 1e-10 as main.cpp:2683-2716 does), for traces tighter than any frame's.
+extern "C" int hc_trace_pixels_fp64_rhs(const kt_frame_desc* d, int64_t n, const uint32_t* pix,
+                                        uint8_t* outcome, double* r, double* red, double* magnif,
+                                        double* phi_disk, double* th_esc, double* ph_esc,
+                                        uint8_t* status, uint32_t* steps, uint32_t* attempts,
+                                        double tol) {
+  return trace_pixels(d, n, pix, outcome, r, red, magnif, phi_disk, th_esc, ph_esc, status, steps,
+                      attempts, true, tol);
 }
 
 // The smooth tracer and its adjoint on the host (kt_smray.cuh compiled by

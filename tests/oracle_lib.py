@@ -252,3 +252,72 @@ def derive_port(desc):
     d = FrameDerived()
     port().orc_frame_derive(ctypes.byref(desc), ctypes.byref(d))
     return d
+
+
+def boundary_distance(outcome, pix, radius=8):
+    """For pixels whose class differs between two renders: the largest, over
+    those pixels, of the distance (in pixels) to the nearest pixel of another
+    class in `outcome` (H x W) -- how far from a class boundary (critical
+    curve, disk edge) a disagreement lies.  None without disagreements;
+    radius + 1 when some lies farther than `radius`."""
+    if len(pix) == 0:
+        return None
+    H, W = outcome.shape
+    worst = 0.0
+    for p in np.asarray(pix, np.int64):
+        y, x = divmod(int(p), W)
+        y0, y1, x0, x1 = max(0, y - radius), min(H, y + radius + 1), max(0, x - radius), min(W, x + radius + 1)
+        yy, xx = np.nonzero(outcome[y0:y1, x0:x1] != outcome[y, x])
+        d = float(np.min(np.hypot(yy + y0 - y, xx + x0 - x))) if yy.size else radius + 1.0
+        worst = max(worst, d)
+    return worst
+
+
+GEO_FIELDS = ("outcome", "r", "redshift", "magnif", "phi_disk", "theta_esc", "phi_esc")
+
+
+def parity_report(got, want, width, height, pix=None, rel=1e-9):
+    """Per-pixel agreement of a GPU frame `got` with the oracle's `want` on
+    the pixels `pix` (all of them by default; `got` holds the whole frame,
+    `want` one entry per pixel of `pix`):
+
+      pixels_bit_different     pixels where any of the seven fields differs
+                               in its bits (the counters too, when both
+                               sides carry them)
+      class_mismatch           pixels whose outcome differs
+      class_mismatch_max_boundary_distance_px
+                               the largest distance of such a pixel from a
+                               class boundary of the GPU frame (None: none)
+      g_rel_gt / r_hit_rel_gt  disk pixels (in both) whose redshift / hit
+                               radius differs by more than `rel` relative
+      g_rel_max / r_hit_rel_max
+    """
+    n = width * height
+    pix = np.arange(n, dtype=np.int64) if pix is None else np.asarray(pix, np.int64)
+    fields = list(GEO_FIELDS) + [f for f in ("steps", "attempts") if f in want and f in got
+                                 and want[f] is not None and got[f] is not None]
+    differ = np.zeros(len(pix), bool)
+    for f in fields:
+        a = np.ascontiguousarray(np.asarray(got[f])[pix])
+        b = np.ascontiguousarray(np.asarray(want[f], dtype=a.dtype))
+        kind = {1: np.uint8, 4: np.uint32, 8: np.uint64}[a.dtype.itemsize]
+        differ |= a.view(kind) != b.view(kind)
+    go, wo = np.asarray(got["outcome"])[pix], np.asarray(want["outcome"])
+    cls = go != wo
+    disk = (go == 1) & (wo == 1)
+
+    def relerr(f):
+        a, b = np.asarray(got[f])[pix][disk], np.asarray(want[f])[disk]
+        return np.abs(a - b) / np.maximum(np.abs(b), 1e-300)
+
+    eg, er = relerr("redshift"), relerr("r")
+    return {"pixels": int(len(pix)), "fields": fields,
+            "pixels_bit_different": int(differ.sum()),
+            "class_mismatch": int(cls.sum()),
+            "class_mismatch_max_boundary_distance_px": boundary_distance(
+                np.asarray(got["outcome"]).reshape(height, width), pix[cls]),
+            "disk_pixels": int(disk.sum()),
+            "rel_threshold": rel,
+            "g_rel_gt": int((eg > rel).sum()), "r_hit_rel_gt": int((er > rel).sum()),
+            "g_rel_max": float(eg.max()) if eg.size else 0.0,
+            "r_hit_rel_max": float(er.max()) if er.size else 0.0}

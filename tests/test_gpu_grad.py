@@ -70,19 +70,18 @@ def test_vjp_gpu_equals_host(renderer, kw):
 def test_config5_l2_gradient_against_central_differences(renderer):
     """512x512, tol 1e-7: kt_l2_grad's loss equals the loss of its own
     forward, and the VJP with the loss's cotangents on the smooth pixels
-    agrees with central differences of that loss to 1e-5 relative.  The
-    differences use the five-point stencil with h = 1e-4 (theta in radians;
-    Lambda: 1e-6), where the stencil's rounding noise (~1e-10 in r_hit over
-    2h) is far below the derivative; a pixel counts as smooth when every
-    stencil render keeps its class, step and attempt counts, its g and r_hit
-    have small second differences and their central differences over h and
-    2h agree (no kink in the first derivative).  The two-point differences
-    at the same h are printed beside them."""
-    import torch
+    agrees with central differences of that loss (tests/grad_lib.py):
+    five-point differences with h = 1e-4 (theta in radians; Lambda 1e-6)
+    to 1e-5 relative, and two-point differences with h = 1e-6 (Lambda 1e-8),
+    the target's check, to 1e-4 relative -- at h = 1e-6 the differences
+    divide the renders' own rounding noise (~1e-12 in the median pixel's g,
+    ~1e-9 at p99, from the step-size controller) by 2h, which sets that
+    floor (measured 1e-5 to 4e-5)."""
+    import grad_lib
 
     base = dict(CFG5, width=512, height=512)
     n = 512 * 512
-    wg, wr = 1.0, 0.01
+    wg, wr = grad_lib.W_G, grad_lib.W_R
     tgt_t = renderer.trace(abi.frame_desc(precision=abi.KT_PREC_SMOOTH, **dict(base, a=0.72, theta_deg=71.0)))
     tgt = to_np(tgt_t)
     out = renderer.alloc(n)
@@ -93,53 +92,17 @@ def test_config5_l2_gradient_against_central_differences(renderer):
                        wr * (b0["r"][m_all] - tgt["r"][m_all]) ** 2)
     assert loss == pytest.approx(want_loss, rel=1e-12)
     assert st["grad_pixels"] == m_all.sum()
-
-    h = 1e-4
-    steps = {"a": h, "Q": h, "Lambda": 1e-6, "theta_deg": np.degrees(h), "r_obs": h}
-    bl0 = smooth_gpu(renderer, dict(base, chart=1))
-    ok = m_all.copy()
-    renders = {}
-    for k, hk in steps.items():
-        o0 = bl0 if k == "Lambda" else b0
-        rs = {j: smooth_gpu(renderer, dict(base, **{k: base[k] + j * hk})) for j in (-2, -1, 1, 2)}
-        renders[k] = (rs, hk)
-        for o in rs.values():
-            ok &= (o0["outcome"] == 1) & (o["outcome"] == 1)
-            for f in ("steps", "attempts"):
-                ok &= o[f] == o0[f]
-        for f in ("redshift", "r"):
-            for j in (1, 2):
-                op, om = rs[j][f], rs[-j][f]
-                ok &= np.abs(op - 2 * o0[f] + om) <= 1e-8 + 0.01 * np.abs(op - om)
-            # the first derivative itself smooth on [-2h, 2h]: the two
-            # central differences agree to O(h^2)
-            d1, d2 = rs[1][f] - rs[-1][f], rs[2][f] - rs[-2][f]
-            ok &= np.abs(d2 - 2 * d1) <= 1e-12 + 1e-4 * np.abs(d1)
-
-    def loss_on(o):
-        return np.sum(wg * (o["redshift"][ok] - tgt["redshift"][ok]) ** 2 +
-                      wr * (o["r"][ok] - tgt["r"][ok]) ** 2)
-
-    def cot(o):
-        return (torch.from_numpy(np.where(ok, 2 * wg * (o["redshift"] - tgt["redshift"]), 0.0)).cuda(),
-                torch.from_numpy(np.where(ok, 2 * wr * (o["r"] - tgt["r"]), 0.0)).cuda())
-
-    d = abi.frame_desc(**base)
-    g, _ = renderer.vjp(d, *cot(b0), flags=abi.KT_GRAD_SKIP_LAMBDA)
-    gl, _ = renderer.vjp(abi.frame_desc(**dict(base, chart=1)), *cot(bl0))
-    adj = {"a": g[0], "Q": g[1], "Lambda": gl[2], "theta_deg": g[3], "r_obs": g[4]}
-    worst = 0.0
-    for k, (rs, hk) in renders.items():
-        L = {j: loss_on(o) for j, o in rs.items()}
-        fd2 = (L[1] - L[-1]) / (2 * hk)
-        fd4 = (L[-2] - 8 * L[-1] + 8 * L[1] - L[2]) / (12 * hk)
-        rel = abs(adj[k] - fd4) / abs(fd4)
-        worst = max(worst, rel)
-        print(f"{k}: adjoint {adj[k]:.10g} five-point {fd4:.10g} rel {rel:.2e} "
-              f"(two-point rel {abs(adj[k] - fd2) / abs(fd2):.2e})")
-    print(f"smooth pixels {ok.sum()} of {m_all.sum()} disk pixels; worst rel {worst:.2e}")
-    assert worst <= 1e-5
     assert grad_l2[abi.GRAD_NAMES.index("disk_out")] == 0.0
+
+    res = grad_lib.fd_check(renderer, base)
+    for name, r in res.items():
+        print(f"{name} h={r['h']:g}: {r['pixels']} of {r['disk_pixels']} disk pixels in the loss")
+        for k, v in r["per_param"].items():
+            print(f"  {k}: adjoint {v['adjoint']:.10g} differences {v['fd']:.10g} rel {v['rel']:.2e}")
+    assert res["five_point"]["worst_rel"] <= 1e-5
+    assert res["two_point"]["worst_rel"] <= 1e-4
+    assert res["five_point"]["pixels"] > 0.3 * res["five_point"]["disk_pixels"]
+    assert res["two_point"]["pixels"] > 0.5 * res["two_point"]["disk_pixels"]
 
 
 def test_pixel_list_gradients_add_up(renderer):

@@ -28,19 +28,73 @@ def trace(renderer, d):
     return {k: v.cpu().numpy() for k, v in out.items()}
 
 
+# Stated bounds of the mixed tracer's error against the FP64 oracle
+# (class-mismatch fraction; relative g error at p50, p99 and max over the
+# disk pixels of both).  Configuration 2 carries the target's g bar at the
+# median.  These errors are almost entirely the difference between the
+# analytic Hamiltonian gradient and the reference's central differences
+# (test_mixed_error_decomposition): it moves the adaptive step sequence,
+# and the reference's disk crossing is the midpoint of an 8 x 8 bisection
+# of the last step (geodesic.hpp:49-140), so two traces whose last steps
+# differ disagree by up to 1/4096 of a step in the hit.
+BOUNDS = {
+    "cfg2_720p_dopri5": dict(cls=1e-4, p50=1e-6, p99=5e-5, mx=0.2),
+    "cfg1_ks_rk4": dict(cls=1e-4, p50=5e-6, p99=1e-4, mx=0.5),
+    "cfg5_ks_rk4": dict(cls=1e-4, p50=5e-6, p99=1e-4, mx=0.5),
+    "cfg2_geometry_rk4": dict(cls=1e-4, p50=5e-6, p99=1e-4, mx=0.5),
+}
+
+
 @pytest.mark.parametrize("name", sorted(FRAMES))
 def test_mixed_against_fp64(renderer, name):
+    import mixed_lib as X
+
     kw = FRAMES[name]
     ref = trace(renderer, abi.frame_desc(**kw))
     got = trace(renderer, abi.frame_desc(precision=abi.KT_PREC_MIXED, **kw))
-    same = got["outcome"] == ref["outcome"]
-    disk = same & (ref["outcome"] == 1)
-    eg = np.abs(got["redshift"][disk] - ref["redshift"][disk]) / np.abs(ref["redshift"][disk])
-    er = np.abs(got["r"][disk] - ref["r"][disk]) / np.abs(ref["r"][disk])
-    print(f"{name}: class mismatch {1 - same.mean():.2e}, g rel err p50 {np.median(eg):.2e} "
-          f"p99 {np.percentile(eg, 99):.2e}, r rel err p50 {np.median(er):.2e}")
-    assert 1 - same.mean() < 1e-4
-    assert np.median(eg) < 5e-6 and np.median(er) < 5e-5
+    s = X.error_stats(got, ref)
+    print(X.fmt(name, s))
+    b = BOUNDS[name]
+    assert s["class_mismatch"] < b["cls"]
+    assert s["g_p50"] <= b["p50"] and s["g_p99"] <= b["p99"] and s["g_max"] <= b["mx"]
+    assert s["r_p50"] < 5e-5
+
+
+@pytest.mark.parametrize("name,tol", [("cfg2_720p_dopri5", 1e-10), ("cfg2_720p_dopri5", 1e-8),
+                                      ("cfg1_ks_rk4", None), ("cfg5_ks_rk4", None)],
+                         ids=["cfg2_tol1e-10", "cfg2_tol1e-8_fp32", "cfg1_fp32", "cfg5_fp32"])
+def test_mixed_error_decomposition(renderer, name, tol):
+    """The mixed frame M against the FP64 oracle F (the exact kernel,
+    bit-identical to the reference) split through A, the same frame traced
+    on the host with the mixed tracer's analytic FP64 gradient alone (exact
+    reciprocals and sincos, no FP32, no contraction): M vs A is the mixed
+    kernel's own error (FP32 right-hand side, approximate reciprocals and
+    sincos, FMA contraction), A vs F the reference's finite-difference
+    gradient against the analytic one.  At tol 1e-10 the FP32 right-hand
+    side is off and M vs A is rounding; with the FP32 right-hand side on
+    (tol >= 1e-8) M vs A is of the size of A vs F."""
+    import mixed_lib as X
+
+    kw = dict(FRAMES[name])
+    if tol is not None:
+        kw["tol"] = tol
+    F = trace(renderer, abi.frame_desc(**kw))
+    dm = abi.frame_desc(precision=abi.KT_PREC_MIXED, **kw)
+    M = trace(renderer, dm)
+    A = X.trace_fp64_rhs(dm)
+    import kerrtracecpp2_b200 as kt
+
+    fp32 = kt.frame_derive(dm).r_fp32 != float("inf")
+    mf, ma, af = X.error_stats(M, F), X.error_stats(M, A), X.error_stats(A, F)
+    print(f"\n{name} tol {kw.get('tol', 1e-7):g} (FP32 right-hand side {'on' if fp32 else 'off'})")
+    for k, v in (("M mixed vs F oracle", mf), ("M mixed vs A analytic FP64", ma),
+                 ("A analytic FP64 vs F oracle", af)):
+        print(X.fmt(k, v))
+    assert mf["class_mismatch"] < 1e-4 and af["class_mismatch"] < 1e-4
+    if not fp32:
+        assert ma["g_p50"] <= 1e-9 and ma["class_mismatch"] < 1e-5
+    else:
+        assert ma["g_p50"] <= 2 * max(af["g_p50"], 1e-6)
 
 
 def test_mixed_bundles_against_fp64(renderer):

@@ -38,7 +38,11 @@ def _np(out):
          fov_deg=30.0, disk_out=20.0, width=160, height=90),   # BL DOPRI5 (queue counters)
     dict(chart=0, a=0.7, Q=0.1, theta_deg=70.0, r_obs=50.0, disk_out=15.0, width=96,
          height=96),                                           # KS (queue + fallback list)
-], ids=["bl_dopri5", "ks_rk4"])
+    dict(chart=0, a=0.7, Q=0.1, theta_deg=0.0, r_obs=50.0, disk_out=15.0, width=48,
+         height=48),                                           # KS, every ray in the fallback list
+    dict(chart=0, a=0.7, Q=0.1, theta_deg=70.0, r_obs=50.0, disk_out=15.0, width=320,
+         height=240),                                          # KS, centre-out order (>= 2^16 pixels)
+], ids=["bl_dopri5", "ks_rk4", "ks_polar_fallback", "ks_centre_out"])
 def test_noalloc_matches_kt_trace_twice(kw):
     import torch
     import kerrtracecpp2_b200 as kt
@@ -57,6 +61,14 @@ def test_noalloc_matches_kt_trace_twice(kw):
         fields = G.FIELDS + ("status", "steps", "attempts")
         for k in fields:
             assert np.array_equal(got[k].view(np.uint8), want[k].view(np.uint8)), k
+    if kw["theta_deg"] == 0.0:
+        # a camera on the axis: the KS initialisation of every ray fails
+        # (main.cpp:1537-1545), so the frame is the BL trace of the same rays
+        # (the fallback launch read every entry of the fallback list)
+        with kt.Renderer(0) as r:
+            bl = _np(r.trace(abi.frame_desc(**dict(kw, chart=1))))
+        for k in G.FIELDS + ("steps", "attempts"):
+            assert np.array_equal(got[k].view(np.uint8), bl[k].view(np.uint8)), k
 
 
 def test_noalloc_rejects_frames_beyond_its_scratch():
