@@ -215,6 +215,92 @@ def cpu_reference_sample(desc, seconds, flavour="ieee", calib_pixels=None):
 ADJOINT_FRAME = dict(chart=0, a=0.7, Q=0.1, Lambda=0.0, theta_deg=70.0, r_obs=50.0, disk_out=15.0,
                      width=512, height=512)
 
+# Secondary legs of the default line run a few steps each (their frames take
+# up to seconds per step).
+LEG_STEPS = 3
+
+
+def _timed_steps(fn, steps, warmup, stream, flush):
+    """Device time (ms) of `steps` calls of fn, L2 flushed before each, after
+    `warmup` untimed calls; one event pair around the whole loop."""
+    import torch
+
+    for _ in range(max(warmup, 1)):
+        flush.fill_(1)
+        fn()
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev[0].record(stream)
+    for _ in range(steps):
+        flush.fill_(1)
+        fn()
+    ev[1].record(stream)
+    torch.cuda.synchronize()
+    return ev[0].elapsed_time(ev[1])
+
+
+def bundles_leg(R, stream, flush):
+    """Config 3: 1920x1080 Jacobi-bundle frame (BL, a=0.998, theta=60, r_obs
+    40, fov 30, disk ISCO-12, RK4 doubling, tol 1e-7), plain FP64
+    (bit-identical to the reference) and mixed (analytic Hessian-vector
+    products), with the mixed frame's error against the FP64 one."""
+    import torch
+    from kerrtracecpp2_b200 import abi
+
+    kw = WORKLOADS["bundles_bl_1080p"]
+    n = kw["width"] * kw["height"]
+    d = abi.frame_desc(**kw)
+    dm = abi.frame_desc(**dict(kw, precision=abi.KT_PREC_MIXED))
+    o, om = R.alloc(n), R.alloc(n)
+    t = _timed_steps(lambda: R.trace(d, o, stream), LEG_STEPS, 1, stream, flush)
+    tm = _timed_steps(lambda: R.trace(dm, om, stream), LEG_STEPS, 1, stream, flush)
+    same = o["outcome"] == om["outcome"]
+    disk = same & (o["outcome"] == 1)
+    eg = ((om["redshift"] - o["redshift"]).abs() / o["redshift"].abs())[disk]
+    em = ((om["magnif"] - o["magnif"]).abs() / o["magnif"].abs())[disk]
+    q = lambda x, p: float(torch.quantile(x.float(), p)) if x.numel() else None  # noqa: E731
+    return {"frame": "1920x1080 Jacobi bundles, BL, a=0.998, theta=60, r_obs=40, fov=30, disk ISCO-12",
+            "steps": LEG_STEPS, "fp64_value": LEG_STEPS * n / (t * 1e-3) / 1e6,
+            "fp64_ms_per_step": t / LEG_STEPS,
+            "mixed_value": LEG_STEPS * n / (tm * 1e-3) / 1e6, "mixed_ms_per_step": tm / LEG_STEPS,
+            "unit": "Mrays/s", "mixed_speedup": t / tm,
+            "mixed_error_vs_fp64": {"class_mismatch_frac": float(1.0 - same.double().mean()),
+                                    "g_rel_p50": q(eg, 0.5), "g_rel_p99": q(eg, 0.99),
+                                    "magnif_rel_p50": q(em, 0.5), "magnif_rel_p99": q(em, 0.99)}}
+
+
+def batch_leg(R, stream, flush, seed=1, frames=64):
+    """Config 4: the 64 seeded parameter sets in one autotuned batch (one
+    CUDA graph launch per step), against one kt_trace per frame."""
+    import time as _t
+
+    import kerrtracecpp2_b200 as kt
+    from kerrtracecpp2_b200 import abi
+
+    descs = kt.random_parameter_sets(frames, seed=seed)
+    n_rays = sum(d.width * d.height for d in descs)
+    t0 = _t.perf_counter()
+    b = R.batch(descs, options=abi.batch_options(autotune=True))
+    tune_s = _t.perf_counter() - t0
+    steps = max(1, LEG_STEPS - 1)
+    tb = _timed_steps(lambda: b.launch(stream), steps, 1, stream, flush)
+
+    def per_frame():
+        for d, o in zip(descs, b.outs):
+            R.trace(d, o, stream)
+
+    tl = _timed_steps(per_frame, steps, 0, stream, flush)
+    groups = [{k: g[k] for k in ("kernel_name", "n_frames", "n_rays", "variant", "block",
+                                 "min_blocks", "refill_min", "best_ms", "default_ms")}
+              for g in b.groups()]
+    b.close()
+    return {"frames": frames, "seed": seed, "rays": n_rays, "steps": steps,
+            "value": steps * n_rays / (tb * 1e-3) / 1e6, "unit": "Mrays/s",
+            "ms_per_step": tb / steps, "autotune_s": tune_s,
+            "per_frame_kt_trace_value": steps * n_rays / (tl * 1e-3) / 1e6,
+            "speedup_vs_per_frame": tl / tb, "groups": groups,
+            "mode": "plain FP64, bit-identical to the reference CPU path"}
+
 
 def adjoint_leg(R, steps, warmup, stream, flush):
     """Config 5: 512x512 KS frame, L2 loss of (g, r_hit) against the smooth
@@ -272,16 +358,21 @@ def adjoint_leg(R, steps, warmup, stream, flush):
             "checkpoint_interval_steps": 32,
             "fd_rel_h1e-4_5pt": fd["five_point"]["worst_rel"],
             "fd_rel_h1e-6": fd["two_point"]["worst_rel"],
+            "fd_rel_h1e-6_loose_mask": fd["two_point_loose"]["worst_rel"],
             "smooth_pixels": fd["five_point"]["pixels"],
             "smooth_pixels_h1e-6": fd["two_point"]["pixels"],
+            "pixels_h1e-6_loose_mask": fd["two_point_loose"]["pixels"],
+            "disk_pixels": fd["five_point"]["disk_pixels"],
             "fd_per_param": {k: {"h1e-4_5pt": fd["five_point"]["per_param"][k]["rel"],
-                                 "h1e-6": fd["two_point"]["per_param"][k]["rel"]}
+                                 "h1e-6": fd["two_point"]["per_param"][k]["rel"],
+                                 "h1e-6_loose_mask": fd["two_point_loose"]["per_param"][k]["rel"]}
                              for k in grad_lib.PARAMS},
             "fd_check": ("worst relative disagreement over (a, Q, Lambda, theta, r_obs) of the "
                          "adjoint with central differences of the same loss over the pixels whose "
                          "stencil renders keep class, step and attempt counts: five-point with "
                          "h = 1e-4 (Lambda 1e-6) on pixels also without second-difference spikes "
-                         "or kinks; two-point with h = 1e-6 (Lambda 1e-8)")}
+                         "or kinks; two-point with h = 1e-6 (Lambda 1e-8) on those pixels, and "
+                         "on every pixel whose class and step sequence survive +-1e-6 (loose)")}
 
 
 def bench_adjoint(args, rank, world, local_rank):
@@ -618,6 +709,8 @@ def main():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-parity", action="store_true")
+    ap.add_argument("--no-legs", action="store_true",
+                    help="skip the config-3 (bundles) and config-4 (batch) legs of the default line")
     ap.add_argument("--split", default="frames", choices=["frames", "tiles"],
                     help="N>1: 'frames' gives every rank its own frame (weak scaling); 'tiles' "
                          "splits one frame over the ranks by interleaved tiles (strong scaling)")
@@ -880,6 +973,12 @@ def main():
     if not args.no_adjoint:
         adjoint = adjoint_leg(R, args.steps, args.warmup, stream, flush)
 
+    # Configs 3 and 4 as legs of the default line (one GPU).
+    bundles = batch64 = None
+    if world == 1 and args.workload == "knds_bl_dopri5_720p" and not args.no_legs:
+        bundles = bundles_leg(R, stream, flush)
+        batch64 = batch_leg(R, stream, flush)
+
     steps_sum = float(out["steps"].to(torch.int64).sum())
     att_sum = float(out["attempts"].to(torch.int64).sum())
     costs = R.op_costs()
@@ -979,6 +1078,7 @@ def main():
             "roofline": roofline, "cpu_baseline": cpu, "parity_vs_strict": parity,
             "mixed_precision": mixed, "mixed_precision_fp32_tol1e-8": mixed_fp32,
             "mixed_batched": mixed_batched, "adjoint": adjoint,
+            "bundles_1080p": bundles, "batch64": batch64,
             "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": ctypes.sizeof(desc),
                     "d2h_bytes_per_step": d2h, "call": "kt_trace_host"},
             "clocks": clocks, "gpu_launches": args.steps * trace_launches(kt.frame_derive(desc), desc)

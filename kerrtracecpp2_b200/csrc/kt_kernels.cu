@@ -81,6 +81,47 @@ struct ModeBundle {
   }
 };
 
+// Bundles with two lanes per ray (k_trace_pair): the right-hand side is
+// split by bundle_rhs_half, the halves swapped with one shuffle each, and
+// bundle_rhs_combine assembles it in bundle_rhs's order (bit-identical); the
+// even lane runs the machine's bookkeeping.
+__device__ __forceinline__ void bundle_rhs_paired(const Metric& g, const double y[4], double pt,
+                                                  double pphi, const double W[8], double k[5],
+                                                  double kW[8], bool odd, unsigned pmask) {
+  BundleHalf me, other;
+  bundle_rhs_half(g, y[0], y[1], y[2], y[3], pt, pphi, odd, &me);
+#pragma unroll
+  for (int t = 0; t < 3; ++t)
+#pragma unroll
+    for (int j = 0; j < 5; ++j) other.h5[t][j] = __shfl_xor_sync(pmask, me.h5[t][j], 1);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) other.h1[i] = __shfl_xor_sync(pmask, me.h1[i], 1);
+  // the even lane's view (the odd lane's result is not used)
+  bundle_rhs_combine(me, other, y[0], y[2], y[3], W, k, kW);
+}
+
+struct ModeBundlePair {
+  using Machine = Bundle;
+  static constexpr int kSlots = Bundle::kSlots;
+  Bundle* m;
+  __device__ __forceinline__ bool needs_k1() const { return m->needs_k1(); }
+  __device__ __forceinline__ bool start(const Frame& f, uint32_t pix, uint32_t, uint32_t, const Fallback&) {
+    m->init(f, (int)(pix % (uint32_t)f.cam.W), (int)(pix / (uint32_t)f.cam.W));
+    return true;
+  }
+  __device__ __forceinline__ bool slot(const Frame& f, int s, RayResult* res, bool odd,
+                                       unsigned pmask) {
+    double y[4], yW[8], k[5], kW[8];
+    m->input(s, y, yW);
+    bundle_rhs_paired(f.g, y, m->pt, m->pphi, yW, k, kW, odd, pmask);
+    __syncwarp(pmask);  // both lanes have read the record
+    int done = 0;
+    if (!odd) done = m->consume(f, s, k, kW, res) ? 1 : 0;
+    __syncwarp(pmask);  // the even lane's updates are visible to the odd lane
+    return __shfl_sync(pmask, done, (int)((threadIdx.x & 31u) & ~1u)) != 0;
+  }
+};
+
 // Separable Kerr (semi-analytic solver): rays that give up are appended to
 // the fallback list for the BL RK4 launch and write no result here.
 struct ModeSepRk4 {
@@ -126,9 +167,26 @@ template <> struct Defers<ModeSepRk4> { static constexpr bool value = true; };
 // outweighs the lanes idling at the end of each group of 32 (KS: 62 against
 // 73 ms, BL RK4: 66 against 68, DOPRI5: equal; bundles best at 16).
 template <> struct Shape<struct ModeBLRk4> { static constexpr int kBlock = 64, kMinBlocks = 9, kRefill = 32; };
-template <> struct Shape<struct ModeBLDopri5> { static constexpr int kBlock = 64, kMinBlocks = 9, kRefill = 32; };
+#ifndef KT_BL_DOPRI5_MINB
+#define KT_BL_DOPRI5_MINB 9
+#endif
+template <> struct Shape<struct ModeBLDopri5> { static constexpr int kBlock = 64, kMinBlocks = KT_BL_DOPRI5_MINB, kRefill = 32; };
 template <> struct Shape<struct ModeKSRk4> { static constexpr int kBlock = 64, kMinBlocks = 9, kRefill = 32; };
 template <> struct Shape<struct ModeBundle> { static constexpr int kBlock = 128, kMinBlocks = 1, kRefill = 16; };
+// Paired bundles: 64 rays per 128-thread block; kRefill counts lanes.
+#ifndef KT_BUNDLE_PAIR_BLOCK
+#define KT_BUNDLE_PAIR_BLOCK 128
+#endif
+#ifndef KT_BUNDLE_PAIR_MINB
+#define KT_BUNDLE_PAIR_MINB 4
+#endif
+#ifndef KT_BUNDLE_PAIR_REFILL
+#define KT_BUNDLE_PAIR_REFILL 16
+#endif
+template <> struct Shape<ModeBundlePair> {
+  static constexpr int kBlock = KT_BUNDLE_PAIR_BLOCK, kMinBlocks = KT_BUNDLE_PAIR_MINB,
+                       kRefill = KT_BUNDLE_PAIR_REFILL;
+};
 
 cudaError_t launch_shape(Mode mode, int device, LaunchShape* shape) {
   if (is_mixed_mode(mode)) return launch_shape_mixed(mode, device, shape);
@@ -136,7 +194,7 @@ cudaError_t launch_shape(Mode mode, int device, LaunchShape* shape) {
     case kModeBLRk4: return shape_for<ModeBLRk4>(device, shape);
     case kModeBLDopri5: return shape_for<ModeBLDopri5>(device, shape);
     case kModeKSRk4: return shape_for<ModeKSRk4>(device, shape);
-    case kModeBundle: return shape_for<ModeBundle>(device, shape);
+    case kModeBundle: return shape_for_pair<ModeBundlePair>(device, shape);
     case kModeSepRk4: return shape_for<ModeSepRk4>(device, shape);
     default: return cudaErrorInvalidValue;
   }
@@ -150,7 +208,7 @@ cudaError_t launch_trace(Mode mode, const Frame& f, const OutSoA& out, const Ray
     case kModeBLRk4: k_trace<ModeBLRk4><<<s.grid, s.block, s.smem, stream>>>(f, out, rl, queue, fb); break;
     case kModeBLDopri5: k_trace<ModeBLDopri5><<<s.grid, s.block, s.smem, stream>>>(f, out, rl, queue, fb); break;
     case kModeKSRk4: k_trace<ModeKSRk4><<<s.grid, s.block, s.smem, stream>>>(f, out, rl, queue, fb); break;
-    case kModeBundle: k_trace<ModeBundle><<<s.grid, s.block, s.smem, stream>>>(f, out, rl, queue, fb); break;
+    case kModeBundle: k_trace_pair<ModeBundlePair><<<s.grid, s.block, s.smem, stream>>>(f, out, rl, queue, fb); break;
     case kModeSepRk4: k_trace<ModeSepRk4><<<s.grid, s.block, s.smem, stream>>>(f, out, rl, queue, fb); break;
     default: return cudaErrorInvalidValue;
   }

@@ -123,6 +123,9 @@ struct Inv {
   double tt, tp, rr, hh, pp;  // g^tt, g^tphi, g^rr, g^thth, g^phiphi
 };
 
+// The quotients over pre (g^tt, g^tphi) and over sig (g^rr, g^thth) share
+// their denominator's correctly rounded reciprocal (ktm_div_rcp: the IEEE
+// quotient in a product and four fma); g^phiphi keeps its division.
 template <bool kD3 = true>
 KT_HD Inv bl_inv(const Metric& g, double r, const Ang& A) {
   const double r_sq = r * r;
@@ -131,11 +134,12 @@ KT_HD Inv bl_inv(const Metric& g, double r, const Ang& A) {
   const double dr = bl_delta_r<kD3>(g, r, r2a2);
   const double dth = A.dth;
   const double pre = (sig * dr) * dth;
+  const double ipre = ktm_rcp(pre), isig = ktm_rcp(sig);
   Inv U;
-  U.tt = ((-g.xi2) * ((dth * r2a2) * r2a2 - ((dr * g.a) * g.a) * A.st2)) / pre;
-  U.tp = (g.axi2 * (dr - dth * r2a2)) / pre;
-  U.rr = dr / sig;
-  U.hh = dth / sig;
+  U.tt = ktm_div_rcp((-g.xi2) * ((dth * r2a2) * r2a2 - ((dr * g.a) * g.a) * A.st2), pre, ipre);
+  U.tp = ktm_div_rcp(g.axi2 * (dr - dth * r2a2), pre, ipre);
+  U.rr = ktm_div_rcp(dr, sig, isig);
+  U.hh = ktm_div_rcp(dth, sig, isig);
   U.pp = (A.st2 > 1e-14) ? (g.xi2 * (dr - ((dth * g.a) * g.a) * A.st2)) / (pre * A.st2) : 0.0;
   return U;
 }
@@ -1008,6 +1012,127 @@ KT_HD void bundle_rhs(const Metric& g, double r, double th, double pr, double pt
   bl_rhs_centre<false>(g, r, th, pr, pth, pt, pphi, k, &A0, &U00);
   double Hs[4][4];
   bundle_hessian(g, r, th, pr, pth, pt, pphi, A0, U00, Hs);
+  double M[4][4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    M[0][j] = Hs[2][j];
+    M[1][j] = Hs[3][j];
+    M[2][j] = -Hs[0][j];
+    M[3][j] = -Hs[1][j];
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      double s = 0.0;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) s += M[i][j] * W[2 * j + c];
+      dW[2 * i + c] = s;
+    }
+}
+
+// The bundle RHS split over the two lanes of a ray (the paired bundle kernel,
+// two threads per ray).  Both lanes run the same instructions on
+// lane-dependent inputs, so the warp never diverges: each evaluates 3 of the
+// 5 angle factors (theta itself on both), 7 of the 13 inverse metrics (the
+// centre's on both) and 19 of the 37 Hamiltonians of bundle_rhs, and
+// bundle_rhs_combine assembles the RHS from the two halves in bundle_rhs's
+// own operation order, so the result is bit-identical to it.
+//
+// Inverse metrics, lane 0 | lane 1 (rp = r + e0, rm = r + (-e0)):
+//   t0 (r, theta) both        t1 (rp | rm, theta)      t2 (r, theta +e1 | +(-e1))
+//   t3 (r + eps_r | r - eps_r, theta)                  t4 (r, theta + eps_th | - eps_th)
+//   t5 (rp, theta +e1 | +(-e1))                        t6 (rm, theta +e1 | +(-e1))
+// Momenta of the Hamiltonians of t0..t2: (pr, pth), (prp, pth), (prm, pth),
+// (pr, pthp), (pr, pthm); at t0 lane 1 takes the four corners (prp, pthp),
+// (prp, pthm), (prm, pthp), (prm, pthm) of the (2,3) cross term instead.
+// t3..t6 take (pr, pth).
+struct BundleHalf {
+  double h5[3][5];  // t0..t2
+  double h1[4];     // t3..t6
+  double k0, k1, k4;  // dr, dtheta, dphi from the centre's g^{mu nu}
+};
+
+KT_HD void bundle_rhs_half(const Metric& g, double r, double th, double pr, double pth, double pt,
+                           double pphi, bool odd, BundleHalf* o) {
+  const double sgn = odd ? -1.0 : 1.0;
+  const double eps_r = 1e-5 * dmax(fabs(r), 0.01);
+  const double eps_th = 1e-6;
+  const double e0 = 1e-5 * (fabs(r) + 0.1);
+  const double e1 = 1e-5;
+  const double e2 = 1e-5 * (fabs(pr) + 1e-3);
+  const double e3 = 1e-5 * (fabs(pth) + 1e-3);
+  const Ang A0 = bl_ang<false>(g, th);
+  const Ang A1 = bl_ang<false>(g, th + sgn * e1);       // theta + e1 | theta + (-e1)
+  const Ang A2 = bl_ang<false>(g, th + sgn * eps_th);   // theta + eps_th | theta - eps_th
+  const double rp = r + e0, rm = r + (-e0);
+  const double prp = pr + e2, prm = pr + (-e2);
+  const double pthp = pth + e3, pthm = pth + (-e3);
+  // t0: the centre; its Hamiltonians: lane 0 H0, the e2 and e3 pairs; lane 1
+  // the (2,3) corners (its fifth value repeats the fourth)
+  {
+    const Inv U = bl_inv<false>(g, r, A0);
+    o->k0 = U.rr * pr;
+    o->k1 = U.hh * pth;
+    o->k4 = U.tp * pt + U.pp * pphi;
+    o->h5[0][0] = bl_ham(U, odd ? prp : pr, odd ? pthp : pth, pt, pphi);
+    o->h5[0][1] = bl_ham(U, prp, odd ? pthm : pth, pt, pphi);
+    o->h5[0][2] = bl_ham(U, prm, odd ? pthp : pth, pt, pphi);
+    o->h5[0][3] = bl_ham(U, odd ? prm : pr, odd ? pthm : pthp, pt, pphi);
+    o->h5[0][4] = bl_ham(U, odd ? prm : pr, pthm, pt, pphi);
+  }
+  // t1, t2: (rp | rm, theta) and (r, theta + e1 | + (-e1)), five momenta each
+  {
+    const Inv U = bl_inv<false>(g, odd ? rm : rp, A0);
+    o->h5[1][0] = bl_ham(U, pr, pth, pt, pphi);
+    o->h5[1][1] = bl_ham(U, prp, pth, pt, pphi);
+    o->h5[1][2] = bl_ham(U, prm, pth, pt, pphi);
+    o->h5[1][3] = bl_ham(U, pr, pthp, pt, pphi);
+    o->h5[1][4] = bl_ham(U, pr, pthm, pt, pphi);
+  }
+  {
+    const Inv U = bl_inv<false>(g, r, A1);
+    o->h5[2][0] = bl_ham(U, pr, pth, pt, pphi);
+    o->h5[2][1] = bl_ham(U, prp, pth, pt, pphi);
+    o->h5[2][2] = bl_ham(U, prm, pth, pt, pphi);
+    o->h5[2][3] = bl_ham(U, pr, pthp, pt, pphi);
+    o->h5[2][4] = bl_ham(U, pr, pthm, pt, pphi);
+  }
+  // t3..t6: one Hamiltonian each
+  o->h1[0] = bl_ham(bl_inv<false>(g, odd ? r - eps_r : r + eps_r, A0), pr, pth, pt, pphi);
+  o->h1[1] = bl_ham(bl_inv<false>(g, r, A2), pr, pth, pt, pphi);
+  o->h1[2] = bl_ham(bl_inv<false>(g, rp, A1), pr, pth, pt, pphi);
+  o->h1[3] = bl_ham(bl_inv<false>(g, rm, A1), pr, pth, pt, pphi);
+}
+
+// The RHS from the two halves (E: lane 0, O: lane 1), bundle_rhs's
+// expressions: k as bl_rhs_centre, Hess(H) as bundle_hessian, dW = J_s Hess W.
+KT_HD void bundle_rhs_combine(const BundleHalf& E, const BundleHalf& O, double r, double pr,
+                              double pth, const double W[8], double k[5], double dW[8]) {
+  const double eps_r = 1e-5 * dmax(fabs(r), 0.01);
+  const double eps_th = 1e-6;
+  k[0] = E.k0;
+  k[1] = E.k1;
+  k[4] = E.k4;
+  k[2] = -(E.h1[0] - O.h1[0]) / (2.0 * eps_r);
+  k[3] = -(E.h1[1] - O.h1[1]) / (2.0 * eps_th);
+  const double e[4] = {1e-5 * (fabs(r) + 0.1), 1e-5, 1e-5 * (fabs(pr) + 1e-3),
+                       1e-5 * (fabs(pth) + 1e-3)};
+  const double H0 = E.h5[0][0];
+  const double vp[4] = {E.h5[1][0], E.h5[2][0], E.h5[0][1], E.h5[0][3]};
+  const double vm[4] = {O.h5[1][0], O.h5[2][0], E.h5[0][2], E.h5[0][4]};
+  double Hs[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a) Hs[a][a] = ((vp[a] - 2.0 * H0) + vm[a]) / (e[a] * e[a]);
+#define KT_CROSS(a, b, pp, pm, mp, mm) \
+  Hs[a][b] = Hs[b][a] = ((((pp) - (pm)) - (mp)) + (mm)) / ((4.0 * e[a]) * e[b])
+  KT_CROSS(0, 1, E.h1[2], O.h1[2], E.h1[3], O.h1[3]);
+  KT_CROSS(0, 2, E.h5[1][1], E.h5[1][2], O.h5[1][1], O.h5[1][2]);
+  KT_CROSS(0, 3, E.h5[1][3], E.h5[1][4], O.h5[1][3], O.h5[1][4]);
+  KT_CROSS(1, 2, E.h5[2][1], E.h5[2][2], O.h5[2][1], O.h5[2][2]);
+  KT_CROSS(1, 3, E.h5[2][3], E.h5[2][4], O.h5[2][3], O.h5[2][4]);
+  KT_CROSS(2, 3, O.h5[0][0], O.h5[0][1], O.h5[0][2], O.h5[0][3]);
+#undef KT_CROSS
   double M[4][4];
 #pragma unroll
   for (int j = 0; j < 4; ++j) {

@@ -83,14 +83,19 @@ KT_HD void sm_stage_of(int t, int* sub, int* s) {
   *s = *sub == 0 ? t + 1 : (*sub == 1 ? t - 2 : t - 6);
 }
 
-// Paths A and B of an attempt (results yA, yB and B's passenger); with
-// `rec`, the stage inputs and slopes are kept.
+// Paths A and B of an attempt (results yA, yB and B's passenger) and their
+// difference dAB = yA - yB formed from the paths' increments,
+// (h/6 sum_A) - ((h/12 sum_B1) + (h/12 sum_B2)): the same quantity as the
+// difference of the two end states, without the rounding of the states
+// themselves, which near-cancel in it -- the error estimate it feeds moves
+// the step sizes, so that rounding would move the trace by ~1e-12 whatever
+// the parameters.  With `rec`, the stage inputs and slopes are kept.
 template <class C>
 KT_HD_CALL void sm_paths(double M, const SmPrm<double>& P, const double* c, const double* y, double pas,
                          const double* k1, double k1p, double hh, double* yA, double* yB, double* pB,
-                         SmStages* rec) {
+                         double* dAB, SmStages* rec) {
   constexpr int n = C::kN;
-  double base[n], kp[n], sum[n], yB1[n], u[n], k[n];
+  double base[n], kp[n], sum[n], yB1[n], u[n], k[n], incA[n], incB1[n];
   double pbase = pas, sump = k1p, pB1 = pas, kk;
   KT_ROLLED
   for (int t = 0; t < 10; ++t) {
@@ -138,10 +143,14 @@ KT_HD_CALL void sm_paths(double M, const SmPrm<double>& P, const double* c, cons
     sump = sump + w * kk;
     if (s == 3) {
       for (int i = 0; i < n; ++i) {
-        const double r = base[i] + hs / 6.0 * sum[i];
+        const double inc = hs / 6.0 * sum[i];
+        const double r = base[i] + inc;
         yA[i] = sub == 0 ? r : yA[i];
         yB1[i] = sub == 1 ? r : yB1[i];
         yB[i] = sub == 2 ? r : yB[i];
+        incA[i] = sub == 0 ? inc : incA[i];
+        incB1[i] = sub == 1 ? inc : incB1[i];
+        dAB[i] = sub == 2 ? incA[i] - (incB1[i] + inc) : dAB[i];
       }
       const double pr = pbase + hs / 6.0 * sump;
       pB1 = sub == 1 ? pr : pB1;
@@ -155,11 +164,11 @@ KT_HD_CALL void sm_paths(double M, const SmPrm<double>& P, const double* c, cons
 template <class C>
 KT_HD int sm_attempt(double M, const SmPrm<double>& P, double tol, const double* c, const double* y,
                      double pas, const double* k1, double k1p, double* h, double* yo, double* paso) {
-  double yA[C::kN], yB[C::kN], pB = 0.0;
-  sm_paths<C>(M, P, c, y, pas, k1, k1p, *h, yA, yB, &pB, nullptr);
+  double yA[C::kN], yB[C::kN], dAB[C::kN], pB = 0.0;
+  sm_paths<C>(M, P, c, y, pas, k1, k1p, *h, yA, yB, &pB, dAB, nullptr);
   double e2 = 0.0;
   for (int i = 0; i < C::kN; ++i) {
-    const double d = yA[i] - yB[i];
+    const double d = dAB[i];
     e2 = e2 + d * d;
   }
   const int res = doubling_update(sqrt(e2) / 15.0, tol, h);
@@ -447,12 +456,9 @@ KT_HD double sm_attempt_bwd(const Frame& f, const SmPrm<double>& P, const double
   const double M = f.g.M;
   double k1[n], k1p, yA[n], yB[n], pB = 0.0;
   sm_rhs<C>(M, P, y, c, k1, &k1p);
-  sm_paths<C>(M, P, c, y, 0.0, k1, k1p, hh, yA, yB, &pB, st);
   double d[n], e2 = 0.0;
-  for (int i = 0; i < n; ++i) {
-    d[i] = yA[i] - yB[i];
-    e2 = e2 + d[i] * d[i];
-  }
+  sm_paths<C>(M, P, c, y, 0.0, k1, k1p, hh, yA, yB, &pB, d, st);
+  for (int i = 0; i < n; ++i) e2 = e2 + d[i] * d[i];
   const double e = sqrt(e2) / 15.0;
   double dh, de;
   sm_ctl_partials(e, f.tol, hh, &dh, &de);
@@ -825,9 +831,10 @@ typedef Dual<1> T1;
 
 template <class C>
 KT_HD_CALL void sm_paths_t(double M, const SmPrm<T1>& P, const T1* c, const T1* y, double pas,
-                           const T1* k1, double k1p, const T1& hh, T1* yA, T1* yB, double* pB) {
+                           const T1* k1, double k1p, const T1& hh, T1* yA, T1* yB, double* pB,
+                           T1* dAB) {
   constexpr int n = C::kN;
-  T1 base[n], kp[n], sum[n], yB1[n], u[n], k[n], kk;
+  T1 base[n], kp[n], sum[n], yB1[n], u[n], k[n], kk, incA[n], incB1[n];
   double pbase = pas, sump = k1p, pB1 = pas;
   KT_ROLLED
   for (int t = 0; t < 10; ++t) {
@@ -870,10 +877,20 @@ KT_HD_CALL void sm_paths_t(double M, const SmPrm<T1>& P, const T1* c, const T1* 
     sump = sump + w * kk.v;
     if (s == 3) {
       for (int i = 0; i < n; ++i) {
-        const T1 r = base[i] + hs / 6.0 * sum[i];
-        if (sub == 0) yA[i] = r;
-        if (sub == 1) yB1[i] = r;
-        if (sub == 2) yB[i] = r;
+        const T1 inc = hs / 6.0 * sum[i];
+        const T1 r = base[i] + inc;
+        if (sub == 0) {
+          yA[i] = r;
+          incA[i] = inc;
+        }
+        if (sub == 1) {
+          yB1[i] = r;
+          incB1[i] = inc;
+        }
+        if (sub == 2) {
+          yB[i] = r;
+          dAB[i] = incA[i] - (incB1[i] + inc);
+        }
       }
       const double pr = pbase + hs.v / 6.0 * sump;
       pB1 = sub == 1 ? pr : pB1;
@@ -921,12 +938,12 @@ KT_HD int sm_update_t(const T1& err, double tol, T1* h) {
 template <class C>
 KT_HD int sm_attempt_t(double M, const SmPrm<T1>& P, double tol, const T1* c, const T1* y, double pas,
                        const T1* k1, double k1p, T1* h, T1* yo, double* paso) {
-  T1 yA[C::kN], yB[C::kN];
+  T1 yA[C::kN], yB[C::kN], dAB[C::kN];
   double pB = 0.0;
-  sm_paths_t<C>(M, P, c, y, pas, k1, k1p, *h, yA, yB, &pB);
+  sm_paths_t<C>(M, P, c, y, pas, k1, k1p, *h, yA, yB, &pB, dAB);
   T1 e2(0.0);
   for (int i = 0; i < C::kN; ++i) {
-    const T1 d = yA[i] - yB[i];
+    const T1 d = dAB[i];
     e2 = e2 + d * d;
   }
   T1 err(sqrt(e2.v) / 15.0);

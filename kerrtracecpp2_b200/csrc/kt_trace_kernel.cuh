@@ -132,6 +132,96 @@ __global__ void __launch_bounds__(Shape<ModeT>::kBlock, Shape<ModeT>::kMinBlocks
   }
 }
 
+// ---- two lanes per ray ------------------------------------------------------
+// Pair modes: lanes 2i and 2i+1 of a warp carry one ray, 16 rays per warp.
+// The mode's slot() splits the right-hand side between the two lanes with
+// the same instructions on lane-dependent inputs (no divergence) and one
+// shuffle exchange; the ray machine (one shared-memory record per pair) is
+// written by the even lane only, with __syncwarp over the slot's lanes
+// between the reads of a slot and the writes of its bookkeeping, and after
+// them.  Both lanes of a pair always share `active`, so idle lanes come in
+// pairs and a pair's two lanes take the same queue index.  As in k_trace,
+// there is no waiting on other warps: the barriers are warp-local.
+template <class ModeT>
+constexpr size_t smem_bytes_pair(int block) {
+  return sizeof(SmemRecord<typename ModeT::Machine>) * (size_t)(block / 2);
+}
+
+template <class ModeT>
+__global__ void __launch_bounds__(Shape<ModeT>::kBlock, Shape<ModeT>::kMinBlocks)
+    k_trace_pair(const __grid_constant__ Frame f, const OutSoA out, const RayList rl,
+                 uint32_t* __restrict__ queue, const Fallback fb) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  using Rec = SmemRecord<typename ModeT::Machine>;
+  ModeT mode;
+  mode.m = &reinterpret_cast<Rec*>(smem)[threadIdx.x >> 1].m;
+  bool active = false;
+  uint32_t out_slot = 0;
+  const uint32_t n = rl.n_dev ? *rl.n_dev : rl.n;
+  const unsigned lane = threadIdx.x & 31u;
+  const bool odd = (lane & 1u) != 0;
+  bool exhausted = false;
+  for (;;) {
+    if (!exhausted) {
+      const unsigned need = __ballot_sync(kFull, !active);
+      if (need && (need == kFull || __popc(need) >= Shape<ModeT>::kRefill)) {
+        const int leader = __ffs(need) - 1;
+        const unsigned cnt = (unsigned)__popc(need) >> 1;  // rays
+        unsigned base = 0;
+        if ((int)lane == leader) base = atomicAdd(queue, cnt);
+        base = __shfl_sync(kFull, base, leader);
+        if (base + cnt >= n) exhausted = true;
+        if (!active) {
+          const unsigned idx = base + ((unsigned)__popc(need & ((1u << lane) - 1u)) >> 1);
+          if (idx < n) {
+            const uint32_t pix = rl.pix ? rl.pix[idx] : idx;
+            out_slot = rl.slot ? rl.slot[idx] : idx;
+            if (!odd) mode.start(f, pix, out_slot, pix, fb);
+            active = true;
+          }
+        }
+      }
+      __syncwarp();  // new records written by the even lanes are visible to their partners
+    }
+    if (!__any_sync(kFull, active)) {
+      if (exhausted) break;
+      continue;
+    }
+    KT_ROLLED
+    for (int s = -1; s < ModeT::kSlots; ++s) {
+      const bool part = active && (s >= 0 || mode.needs_k1());
+      const unsigned pmask = __ballot_sync(kFull, part);
+      if (s < 0 && !pmask) continue;
+      if (part) {
+        RayResult res;
+        if (mode.slot(f, s, &res, odd, pmask)) {
+          if (!odd) write_result(out, out_slot, res);
+          active = false;
+        }
+      }
+    }
+  }
+}
+
+template <class ModeT>
+static cudaError_t shape_for_pair(int device, LaunchShape* shape) {
+  int sms = 0, per_sm = 0;
+  cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  if (e != cudaSuccess) return e;
+  const int block = Shape<ModeT>::kBlock;
+  const size_t smem = smem_bytes_pair<ModeT>(block);
+  e = cudaFuncSetAttribute(k_trace_pair<ModeT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem);
+  if (e != cudaSuccess) return e;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace_pair<ModeT>, block, smem);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) per_sm = 1;
+  shape->block = block;
+  shape->grid = sms * per_sm;
+  shape->smem = smem;
+  return cudaSuccess;
+}
+
 template <class ModeT>
 static cudaError_t shape_for(int device, LaunchShape* shape) {
   int sms = 0, per_sm = 0;

@@ -29,10 +29,13 @@ import numpy as np
 from . import abi
 
 
-def frame_tiles(width, height, world, rank, tile=16):
+def frame_tiles(width, height, world, rank, tile=16, centre_out=False):
     """Pixel indices (py*width + px, uint32, ascending within each tile) of
     the tiles of side `tile` dealt to `rank`: tile k goes to rank k % world,
-    tiles numbered row-major."""
+    tiles numbered row-major.  With centre_out, the same pixels in the
+    renderer's centre-out order (rings 4 pixels wide about the image centre,
+    innermost first, row-major within a ring), so that each rank's longest
+    rays -- by the critical curve, near the centre -- start first."""
     if not (0 <= rank < world):
         raise ValueError("rank out of range")
     tx = (width + tile - 1) // tile
@@ -45,7 +48,17 @@ def frame_tiles(width, height, world, rank, tile=16):
         out.append((ys[:, None] * width + xs[None, :]).ravel())
     if not out:
         return np.zeros(0, np.uint32)
-    return np.concatenate(out).astype(np.uint32)
+    pix = np.concatenate(out)
+    if centre_out:
+        pix = np.sort(pix)
+        cx, cy = np.float32(0.5 * (width - 1)), np.float32(0.5 * (height - 1))
+        rmax = np.sqrt(cx * cx + cy * cy) + np.float32(1.0)
+        inv_w = np.float32(1.0) / np.maximum(np.float32(4.0), rmax / np.float32(512))
+        dx = (pix % width).astype(np.float32) - cx
+        dy = (pix // width).astype(np.float32) - cy
+        ring = np.minimum((np.sqrt(dx * dx + dy * dy) * inv_w).astype(np.int64), 511)
+        pix = pix[np.argsort(ring, kind="stable")]
+    return pix.astype(np.uint32)
 
 
 # Mean adaptive attempts per ray measured on the benchmark frames, by
@@ -84,6 +97,23 @@ def _dist():
     return dist
 
 
+_PLANS = {}
+
+
+def _plan(width, height, world, tile, centre_out, device):
+    """Every rank's tile pixels (host) and their device index tensors for a
+    frame shape, built once per (shape, world, tile, order, device)."""
+    import torch
+
+    key = (width, height, world, tile, centre_out, str(device))
+    if key not in _PLANS:
+        parts = [frame_tiles(width, height, world, q, tile, centre_out) for q in range(world)]
+        _PLANS[key] = (parts,
+                       [torch.from_numpy(p.astype(np.int32)).to(device) for p in parts],
+                       [torch.from_numpy(p.astype(np.int64)).to(device) for p in parts])
+    return _PLANS[key]
+
+
 def _as_tensor(v, device):
     import torch
 
@@ -92,7 +122,8 @@ def _as_tensor(v, device):
     return torch.from_numpy(np.ascontiguousarray(v)).to(device)
 
 
-def trace_frame_sharded(renderer, desc, group=None, tile=16, trace=None, dst=0, fields=None):
+def trace_frame_sharded(renderer, desc, group=None, tile=16, trace=None, dst=0, fields=None,
+                        centre_out=True):
     """Trace one frame split over the ranks of `group` by tiles.  Every rank
     traces its own tiles (kt_trace_pixels on its GPU, or `trace(desc, pix)`
     returning a dict of arrays or tensors per pixel); the parts travel to
@@ -102,20 +133,17 @@ def trace_frame_sharded(renderer, desc, group=None, tile=16, trace=None, dst=0, 
     `dst` returns the whole frame as a dict of tensors on the parts' device,
     bit for bit what each rank traced; the other ranks return None.
     `fields` (default: every field the trace returned) chooses what
-    travels."""
+    travels; each rank traces its pixels in centre-out order unless
+    centre_out is False (the results do not depend on the order)."""
     import torch
 
     dist = _dist()
     world = dist.get_world_size(group)
     rank = dist.get_rank(group)
-    parts = [frame_tiles(desc.width, desc.height, world, q, tile) for q in range(world)]
+    dev = torch.device("cuda", renderer.device) if trace is None else torch.device("cpu")
+    parts, pix32, idx64 = _plan(desc.width, desc.height, world, tile, centre_out, dev)
     pix = parts[rank]
-    if trace is None:
-        dev = torch.device("cuda", renderer.device)
-        res = renderer.trace_pixels(desc, torch.from_numpy(pix.astype(np.int32)).to(dev))
-    else:
-        dev = torch.device("cpu")
-        res = trace(desc, pix)
+    res = renderer.trace_pixels(desc, pix32[rank]) if trace is None else trace(desc, pix)
     keys = sorted(k for k, v in res.items() if v is not None and (fields is None or k in fields))
     vals = {k: _as_tensor(res[k], dev) for k in keys}
     m = max(len(p) for p in parts)
@@ -134,7 +162,7 @@ def trace_frame_sharded(renderer, desc, group=None, tile=16, trace=None, dst=0, 
     n = desc.width * desc.height
     frame = {k: torch.zeros(n, dtype=vals[k].dtype, device=dev) for k in keys}
     for q in range(world):
-        idx = torch.from_numpy(parts[q].astype(np.int64)).to(dev)
+        idx = idx64[q]
         off = 0
         for k in keys:
             nb = len(parts[q]) * sizes[k]

@@ -13,14 +13,15 @@ not of the integrator's derivative):
   five-point, h = 1e-4 (theta in radians; Lambda 1e-6): renders at +-h, +-2h;
       a pixel also needs small second differences of g and r_hit and central
       differences over h and 2h that agree to 1e-4 (no kink);
-  two-point, h = 1e-6 (Lambda 1e-8): renders at +-h; class, step and
-      attempt counts unchanged.
+  two-point, h = 1e-6 (Lambda 1e-8): renders at +-h, on the five-point
+      check's smooth pixels that keep class, step and attempt counts at +-h
+      ("two_point"), and on every pixel that keeps them ("two_point_loose").
 
-The two-point differences at h = 1e-6 are limited by the renders' own noise:
-the step-size controller's error estimate |A - B|/15 is a difference of
-nearly equal states, so its rounding moves the step sizes and g by ~1e-12
-(median pixel) to ~1e-9 (p99) whatever h is, which central differences
-divide by 2h.
+At h = 1e-6 the differences divide the renders' own rounding noise by 2h:
+about 1e-13 in the median pixel's g and 2e-11 at p99 (the smooth tracer
+forms its error estimate from the paths' increments; from the end states it
+was 2e-12 and 8e-10), plus a few pixels whose g jumps at that scale with
+their step sequence unchanged, which only the loose mask keeps.
 """
 import numpy as np
 
@@ -43,9 +44,9 @@ def _np(out):
 
 
 def fd_check(renderer, base=CFG5, h4=1e-4, h2=1e-6):
-    """Returns {"five_point": {...}, "two_point": {...}}, each with the
-    per-parameter adjoint, difference and relative disagreement, the worst
-    of them and the number of pixels in the loss."""
+    """Returns {"five_point": .., "two_point": .., "two_point_loose": ..},
+    each with the per-parameter adjoint, difference and relative
+    disagreement, the worst of them and the number of pixels in the loss."""
     import torch
 
     def smooth(kw):
@@ -102,7 +103,9 @@ def fd_check(renderer, base=CFG5, h4=1e-4, h2=1e-6):
         five["per_param"][k] = {"adjoint": adj[k], "fd": fd4, "rel": abs(adj[k] - fd4) / abs(fd4)}
     five["worst_rel"] = max(v["rel"] for v in five["per_param"].values())
 
-    # two-point, h2
+    # two-point, h2: on the five-point check's smooth pixels (whose stencil
+    # over [-2 h4, 2 h4] contains this one) that keep class and step sequence
+    # at +-h2, and on every pixel that keeps them at +-h2 (loose)
     ok2 = m_all.copy()
     renders2 = {}
     for k in PARAMS:
@@ -112,10 +115,13 @@ def fd_check(renderer, base=CFG5, h4=1e-4, h2=1e-6):
         renders2[k] = (rs, hk)
         for o in rs.values():
             ok2 = same_piece(o0, o, ok2)
-    adj2 = adjoint(ok2)
-    two = {"h": h2, "pixels": int(ok2.sum()), "disk_pixels": int(m_all.sum()), "per_param": {}}
-    for k, (rs, hk) in renders2.items():
-        fd2 = (loss_on(rs[1], ok2) - loss_on(rs[-1], ok2)) / (2 * hk)
-        two["per_param"][k] = {"adjoint": adj2[k], "fd": fd2, "rel": abs(adj2[k] - fd2) / abs(fd2)}
-    two["worst_rel"] = max(v["rel"] for v in two["per_param"].values())
-    return {"five_point": five, "two_point": two}
+    out = {"five_point": five}
+    for name, mask in (("two_point", ok2 & ok), ("two_point_loose", ok2)):
+        adj2 = adjoint(mask)
+        two = {"h": h2, "pixels": int(mask.sum()), "disk_pixels": int(m_all.sum()), "per_param": {}}
+        for k, (rs, hk) in renders2.items():
+            fd2 = (loss_on(rs[1], mask) - loss_on(rs[-1], mask)) / (2 * hk)
+            two["per_param"][k] = {"adjoint": adj2[k], "fd": fd2, "rel": abs(adj2[k] - fd2) / abs(fd2)}
+        two["worst_rel"] = max(v["rel"] for v in two["per_param"].values())
+        out[name] = two
+    return out

@@ -82,6 +82,18 @@ RayResult run_ray(const Frame& f, uint32_t pix) {
   return res;
 }
 
+// Bundle RHS through the two-lane split (bundle_rhs_half for both lanes,
+// then bundle_rhs_combine), as the paired bundle kernel evaluates it.
+bool g_bundle_split = false;
+
+void bundle_rhs_split(const Metric& g, const double y[4], double pt, double pphi,
+                      const double W[8], double k[5], double kW[8]) {
+  BundleHalf E, O;
+  bundle_rhs_half(g, y[0], y[1], y[2], y[3], pt, pphi, false, &E);
+  bundle_rhs_half(g, y[0], y[1], y[2], y[3], pt, pphi, true, &O);
+  bundle_rhs_combine(E, O, y[0], y[2], y[3], W, k, kW);
+}
+
 RayResult run_ray_standard(const Frame& f, uint32_t pix) {
   if (f.bundles) {
     Bundle m;
@@ -94,6 +106,8 @@ RayResult run_ray_standard(const Frame& f, uint32_t pix) {
         m.input(slot, y, yW);
         if (f.precision == KT_PREC_MIXED)
           bundle_rhs_analytic(f.g, y, m.pt, m.pphi, yW, k, kW);
+        else if (g_bundle_split)
+          bundle_rhs_split(f.g, y, m.pt, m.pphi, yW, k, kW);
         else
           bundle_rhs(f.g, y[0], y[1], y[2], y[3], m.pt, m.pphi, yW, k, kW);
         if (m.consume(f, slot, k, kW, &res)) return res;
@@ -209,6 +223,9 @@ static int trace_pixels(const kt_frame_desc* d, int64_t n, const uint32_t* pix, 
   }
   return 0;
 }
+
+// 1: FP64 bundle frames take the two-lane split of the bundle RHS.
+extern "C" void hc_set_bundle_split(int on) { g_bundle_split = on != 0; }
 
 extern "C" int hc_trace_pixels(const kt_frame_desc* d, int64_t n, const uint32_t* pix,
                                uint8_t* outcome, double* r, double* red, double* magnif,

@@ -72,11 +72,10 @@ def test_config5_l2_gradient_against_central_differences(renderer):
     forward, and the VJP with the loss's cotangents on the smooth pixels
     agrees with central differences of that loss (tests/grad_lib.py):
     five-point differences with h = 1e-4 (theta in radians; Lambda 1e-6)
-    to 1e-5 relative, and two-point differences with h = 1e-6 (Lambda 1e-8),
-    the target's check, to 1e-4 relative -- at h = 1e-6 the differences
-    divide the renders' own rounding noise (~1e-12 in the median pixel's g,
-    ~1e-9 at p99, from the step-size controller) by 2h, which sets that
-    floor (measured 1e-5 to 4e-5)."""
+    and two-point differences with h = 1e-6 (Lambda 1e-8), the target's
+    check, on the same smooth pixels, to 1e-5 relative; on the looser mask
+    (every pixel whose class and step sequence survive +-1e-6) the two-point
+    differences are reported and bounded at 1e-4."""
     import grad_lib
 
     base = dict(CFG5, width=512, height=512)
@@ -100,9 +99,11 @@ def test_config5_l2_gradient_against_central_differences(renderer):
         for k, v in r["per_param"].items():
             print(f"  {k}: adjoint {v['adjoint']:.10g} differences {v['fd']:.10g} rel {v['rel']:.2e}")
     assert res["five_point"]["worst_rel"] <= 1e-5
-    assert res["two_point"]["worst_rel"] <= 1e-4
+    assert res["two_point"]["worst_rel"] <= 1e-5
+    assert res["two_point_loose"]["worst_rel"] <= 1e-4
     assert res["five_point"]["pixels"] > 0.3 * res["five_point"]["disk_pixels"]
-    assert res["two_point"]["pixels"] > 0.5 * res["two_point"]["disk_pixels"]
+    assert res["two_point"]["pixels"] > 0.3 * res["two_point"]["disk_pixels"]
+    assert res["two_point_loose"]["pixels"] > 0.5 * res["two_point_loose"]["disk_pixels"]
 
 
 def test_pixel_list_gradients_add_up(renderer):

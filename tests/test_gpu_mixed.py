@@ -37,11 +37,15 @@ def trace(renderer, d):
 # and the reference's disk crossing is the midpoint of an 8 x 8 bisection
 # of the last step (geodesic.hpp:49-140), so two traces whose last steps
 # differ disagree by up to 1/4096 of a step in the hit.
+# Measured on B200 (class, g p50 / p99 / max): config 2 0, 8.5e-7 / 1.7e-5 /
+# 7.1e-2; config 1 0, 2.3e-6 / 2.0e-5 / 8.3e-2; config 5 3.8e-6, 2.0e-6 /
+# 4.3e-5 / 6.6e-2; config 2 geometry with RK4 at tol 1e-7 0, 2.1e-6 / 5.1e-5
+# / 3.2e-2.  The maxima are pixels by the critical curve.
 BOUNDS = {
     "cfg2_720p_dopri5": dict(cls=1e-4, p50=1e-6, p99=5e-5, mx=0.2),
-    "cfg1_ks_rk4": dict(cls=1e-4, p50=5e-6, p99=1e-4, mx=0.5),
-    "cfg5_ks_rk4": dict(cls=1e-4, p50=5e-6, p99=1e-4, mx=0.5),
-    "cfg2_geometry_rk4": dict(cls=1e-4, p50=5e-6, p99=1e-4, mx=0.5),
+    "cfg1_ks_rk4": dict(cls=1e-4, p50=5e-6, p99=5e-5, mx=0.2),
+    "cfg5_ks_rk4": dict(cls=1e-4, p50=5e-6, p99=1e-4, mx=0.2),
+    "cfg2_geometry_rk4": dict(cls=1e-4, p50=5e-6, p99=1e-4, mx=0.2),
 }
 
 
@@ -71,8 +75,9 @@ def test_mixed_error_decomposition(renderer, name, tol):
     kernel's own error (FP32 right-hand side, approximate reciprocals and
     sincos, FMA contraction), A vs F the reference's finite-difference
     gradient against the analytic one.  At tol 1e-10 the FP32 right-hand
-    side is off and M vs A is rounding; with the FP32 right-hand side on
-    (tol >= 1e-8) M vs A is of the size of A vs F."""
+    side is off and M vs A is the rounding of the mixed path's operations
+    (measured p50 9.3e-9, a hundredth of A vs F); with the FP32 right-hand
+    side on (tol >= 1e-8) M vs A is of the size of A vs F (p50 2e-6)."""
     import mixed_lib as X
 
     kw = dict(FRAMES[name])
@@ -92,7 +97,8 @@ def test_mixed_error_decomposition(renderer, name, tol):
         print(X.fmt(k, v))
     assert mf["class_mismatch"] < 1e-4 and af["class_mismatch"] < 1e-4
     if not fp32:
-        assert ma["g_p50"] <= 1e-9 and ma["class_mismatch"] < 1e-5
+        assert ma["g_p50"] <= 5e-8 and ma["g_p50"] < 0.05 * af["g_p50"]
+        assert ma["class_mismatch"] < 1e-5
     else:
         assert ma["g_p50"] <= 2 * max(af["g_p50"], 1e-6)
 

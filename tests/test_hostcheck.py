@@ -67,3 +67,35 @@ def test_pixel_subset_equals_frame(hc):
     sub = run(hc, d, pix)
     for k in G.FIELDS:
         assert np.array_equal(G.bits(sub[k]), G.bits(full[k][pix]))
+
+
+@pytest.mark.parametrize("name", [n for n, kw in sorted(G.cases().items()) if kw.get("bundles")])
+def test_bundle_rhs_split_matches_reference(hc, name):
+    """The bundle RHS split over two lanes (bundle_rhs_half for each lane,
+    bundle_rhs_combine), as the paired bundle kernel evaluates it, traced on
+    the host: bit-identical to the reference's bundle fixtures."""
+    hc.hc_set_bundle_split.argtypes = [ctypes.c_int]
+    hc.hc_set_bundle_split(1)
+    try:
+        got = run(hc, G.desc(name))
+    finally:
+        hc.hc_set_bundle_split(0)
+    assert G.mismatches(got, G.result(name)) == {k: 0 for k in G.FIELDS}
+
+
+def test_bundle_rhs_split_matches_oracle_medium(hc):
+    """Config 3's geometry at 96x54 through the split bundle RHS on the host:
+    all fields and the counters bit-identical to the oracle."""
+    import oracle_lib as O
+    from kerrtracecpp2_b200 import abi
+
+    d = abi.frame_desc(chart=1, bundles=1, a=0.998, theta_deg=60.0, width=96, height=54)
+    hc.hc_set_bundle_split.argtypes = [ctypes.c_int]
+    hc.hc_set_bundle_split(1)
+    try:
+        got = run(hc, d)
+    finally:
+        hc.hc_set_bundle_split(0)
+    want = O.trace_port(d, counters=True)
+    assert G.mismatches(got, want) == {k: 0 for k in G.FIELDS}
+    assert np.array_equal(got["steps"], want["steps"]) and np.array_equal(got["attempts"], want["attempts"])

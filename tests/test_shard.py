@@ -22,6 +22,21 @@ def test_tiles_partition_the_frame(w, h, world, tile):
     assert max(sizes) - min(sizes) <= tile * tile
 
 
+@pytest.mark.parametrize("w,h,world", [(1280, 720, 1), (1280, 720, 3), (45, 29, 2)])
+def test_centre_out_tiles_are_the_same_pixels(w, h, world):
+    """The centre-out order is a permutation of each rank's tile pixels,
+    innermost ring first and row-major within a ring."""
+    for r in range(world):
+        a = S.frame_tiles(w, h, world, r, 16)
+        b = S.frame_tiles(w, h, world, r, 16, centre_out=True)
+        assert np.array_equal(np.sort(a), np.sort(b))
+        x, y = (b % w).astype(float) - 0.5 * (w - 1), (b // w).astype(float) - 0.5 * (h - 1)
+        ring = np.minimum((np.hypot(x, y) / max(4.0, (np.hypot(0.5 * (w - 1), 0.5 * (h - 1)) + 1) / 512)).astype(int), 511)
+        assert np.all(np.diff(ring) >= 0)
+        same = np.diff(ring) == 0
+        assert np.all(np.diff(b.astype(np.int64))[same] > 0)
+
+
 def test_assign_frames_balances_and_covers():
     rng = np.random.default_rng(0)
     costs = list(rng.uniform(1, 100, 64))
