@@ -39,8 +39,9 @@ WORKLOADS = {
     "kerr_ks_rk4_320x180": dict(chart=0, a=0.5, r_obs=40.0, theta_deg=80.0, phi_deg=0.0,
                                 fov_deg=45.0, disk_out=12.0, width=320, height=180),
     "bundles_bl_1080p": dict(chart=1, bundles=1, a=0.998, theta_deg=60.0, width=1920, height=1080),
-    # config 3's geometry at a quarter of the resolution (profiling size)
+    # config 3's geometry at a quarter and at half the resolution (profiling sizes)
     "bundles_bl_480x270": dict(chart=1, bundles=1, a=0.998, theta_deg=60.0, width=480, height=270),
+    "bundles_bl_960x540": dict(chart=1, bundles=1, a=0.998, theta_deg=60.0, width=960, height=540),
     "kn_ks_rk4_512": dict(chart=0, a=0.7, Q=0.1, theta_deg=70.0, r_obs=50.0, disk_out=15.0,
                           width=512, height=512),
     # 64 seeded parameter sets (kerrtracecpp2_b200.random_parameter_sets, seed
@@ -302,19 +303,21 @@ def batch_leg(R, stream, flush, seed=1, frames=64):
             "mode": "plain FP64, bit-identical to the reference CPU path"}
 
 
-def adjoint_leg(R, steps, warmup, stream, flush):
-    """Config 5: 512x512 KS frame, L2 loss of (g, r_hit) against the smooth
-    tracer at a=0.72, theta=71; kt_l2_grad (fused forward + reverse per ray)
-    timed on the device against kt_trace of the same frame (plain FP64, the
-    reference's arithmetic) and the smooth forward alone."""
+def adjoint_leg(R, steps, warmup, stream, flush, frame=None, target=None, fd_check=True):
+    """Config 5 (default): 512x512 KS frame, L2 loss of (g, r_hit) against
+    the smooth tracer at a=0.72, theta=71; kt_l2_grad (fused forward +
+    reverse per ray) timed on the device against kt_trace of the same frame
+    (plain FP64, the reference's arithmetic) and the smooth forward alone.
+    `frame` / `target` give another frame and the target's parameters."""
     import torch
     from kerrtracecpp2_b200 import abi
 
-    n = ADJOINT_FRAME["width"] * ADJOINT_FRAME["height"]
-    d = abi.frame_desc(**ADJOINT_FRAME)
-    ds = abi.frame_desc(precision=abi.KT_PREC_SMOOTH, **ADJOINT_FRAME)
-    tgt = R.trace(abi.frame_desc(precision=abi.KT_PREC_SMOOTH,
-                                 **dict(ADJOINT_FRAME, a=0.72, theta_deg=71.0)))
+    frame = frame or ADJOINT_FRAME
+    target = target or dict(a=0.72, theta_deg=71.0)
+    n = frame["width"] * frame["height"]
+    d = abi.frame_desc(**frame)
+    ds = abi.frame_desc(precision=abi.KT_PREC_SMOOTH, **frame)
+    tgt = R.trace(abi.frame_desc(precision=abi.KT_PREC_SMOOTH, **dict(frame, **target)))
     out = R.alloc(n)
 
     def timed(fn):
@@ -340,6 +343,21 @@ def adjoint_leg(R, steps, warmup, stream, flush):
 
     grad_ms = timed(grad)
     loss, g, st = res["r"]
+    desc_txt = {k: frame[k] for k in ("width", "height", "chart", "a", "Q", "Lambda", "theta_deg",
+                                      "r_obs", "disk_out") if k in frame}
+    desc_txt["integrator"] = "DOPRI5" if frame.get("integrator", 0) == 1 else "RK4-doubling"
+    desc_txt["tol"] = frame.get("tol", 1e-7)
+    leg = {"frame": desc_txt,
+           "loss": "sum over pixels that are disk hits in both frames of (g-g_t)^2 + 0.01 (r-r_t)^2, "
+                   f"target: the same tracer at {target}",
+           "ms_per_frame": grad_ms, "ms_main_pass": st["ms_main"], "ms_lambda_pass": st["ms_lambda"],
+           "forward_fp64_ms": fwd_ms, "forward_smooth_ms": smooth_ms,
+           "ratio_vs_forward_fp64": grad_ms / fwd_ms,
+           "grad": dict(zip(abi.GRAD_NAMES, [float(x) for x in g])), "loss_value": loss,
+           "grad_pixels": st["grad_pixels"], "unrecorded": st["unrecorded"],
+           "checkpoint_interval_steps": 32}
+    if not fd_check:
+        return leg
     # Central differences of the same loss (tests/grad_lib.py): five-point
     # at h = 1e-4 and two-point at h = 1e-6, on the pixels whose stencil
     # renders keep their class and step sequence.
@@ -969,9 +987,14 @@ def main():
         b.close()
         del b
 
-    adjoint = None
+    adjoint = adjoint_dopri5 = None
     if not args.no_adjoint:
         adjoint = adjoint_leg(R, args.steps, args.warmup, stream, flush)
+        if args.workload == "knds_bl_dopri5_720p":
+            # the DOPRI5 adjoint on this run's own frame (configuration 2, 720p)
+            adjoint_dopri5 = adjoint_leg(R, min(args.steps, LEG_STEPS), 1, stream, flush,
+                                         frame=WORKLOADS["knds_bl_dopri5_720p"],
+                                         target=dict(a=0.92, theta_deg=86.0), fd_check=False)
 
     # Configs 3 and 4 as legs of the default line (one GPU).
     bundles = batch64 = None
@@ -1077,7 +1100,7 @@ def main():
             "mode": "plain FP64, bit-identical to the reference CPU path",
             "roofline": roofline, "cpu_baseline": cpu, "parity_vs_strict": parity,
             "mixed_precision": mixed, "mixed_precision_fp32_tol1e-8": mixed_fp32,
-            "mixed_batched": mixed_batched, "adjoint": adjoint,
+            "mixed_batched": mixed_batched, "adjoint": adjoint, "adjoint_dopri5_720p": adjoint_dopri5,
             "bundles_1080p": bundles, "batch64": batch64,
             "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": ctypes.sizeof(desc),
                     "d2h_bytes_per_step": d2h, "call": "kt_trace_host"},

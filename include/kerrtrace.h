@@ -271,7 +271,10 @@ kt_status kt_camera_spp_offsets(int32_t camera_spp, double* xy);
  * Tuning: each group's launch has a block size and register cap (one of
  * KT_BATCH_VARIANTS compiled variants), a persistent grid, and a regroup
  * threshold (idle lanes of a warp take new rays only when at least that many
- * are idle).  Rays per warp is 32: one ray per lane.  With KT_BATCH_AUTOTUNE,
+ * are idle).  Variants 0-2 run one ray per lane (32 rays per warp); variant
+ * 3 runs two lanes per ray (16 rays per warp), which only the FP64 bundle
+ * kernel has -- other groups given variant 3 take their default variant, and
+ * the tuner times it for bundle groups only.  With KT_BATCH_AUTOTUNE,
  * kt_batch_create times every variant x threshold on a sample of the group's
  * rays (tune_fraction of them, in runs of 256 neighbouring pixels) and keeps
  * the fastest; the sample's results are written to the outputs.  Otherwise
@@ -283,14 +286,14 @@ kt_status kt_camera_spp_offsets(int32_t camera_spp, double* xy);
  * different batches are independent. */
 typedef struct kt_batch kt_batch;
 
-#define KT_BATCH_VARIANTS 3
+#define KT_BATCH_VARIANTS 4
 #define KT_BATCH_AUTOTUNE 1u
 
 typedef struct kt_batch_options {
   uint32_t flags;          /* KT_BATCH_AUTOTUNE */
   int32_t variant;         /* -1: per-mode default; else 0..KT_BATCH_VARIANTS-1 */
   int32_t refill_min;      /* 0: per-mode default (the single-frame kernels' threshold:
-                              16 for bundles, 1 for the separable tracer, 32 otherwise);
+                              8 for FP64 bundles, 1 for the separable tracer, 32 otherwise);
                               1..32: idle lanes of a warp take new rays once this many are idle */
   int32_t tune_reps;       /* timed repetitions per candidate (>= 1) */
   double tune_fraction;    /* share of a group's rays in the tuning sample, (0, 1] */

@@ -90,7 +90,7 @@ class ColorParams(ctypes.Structure):
     ]
 
 
-KT_BATCH_VARIANTS = 3
+KT_BATCH_VARIANTS = 4
 KT_BATCH_AUTOTUNE = 1
 
 

@@ -14,6 +14,9 @@
 // fixed order (the sum does not depend on the schedule).  The tangent kernel
 // gives one parameter's entry by forward mode (no recording).
 //
+// BL frames integrated with DOPRI5 have their own pair of kernels (the
+// smooth DOPRI5 attempt and its reverse, kt_smray.cuh).
+//
 // Compiled with --fmad=false: the recorded forward and every replay of it
 // must round identically, which contraction choices made per inlining site
 // would not guarantee.
@@ -29,7 +32,7 @@ constexpr int kSumThreads = 256;
 // Rays: pixels 0..n-1, or list[0..*n_dev) (a count on the device) or
 // list[0..n_list) (on the host).  The KS kernel appends the rays
 // whose KS initialisation fails to fb_pix (count *fb_n) for the BL kernel.
-template <class C, bool kGrad>
+template <class C, bool kGrad, class I>
 __global__ void __launch_bounds__(kSmBlock) k_smooth(const Frame f, const OutSoA out, const SmJob job,
                                                      uint32_t n, const uint32_t* __restrict__ list,
                                                      uint32_t n_list,
@@ -51,7 +54,7 @@ __global__ void __launch_bounds__(kSmBlock) k_smooth(const Frame f, const OutSoA
     if (pix < n) {  // else past the end, or a caller's list index outside the frame
       RayResult o;
       double g[kGSlots];
-      if (!sm_pixel<C, kGrad>(f, pix, job.cot, &o, g, kGrad ? &sc : nullptr)) {
+      if (!sm_pixel<C, kGrad, I>(f, pix, job.cot, &o, g, kGrad ? &sc : nullptr)) {
         fb_pix[atomicAdd(fb_n, 1u)] = pix;
       } else {
         if (out.outcome) write_result(out, pix, o);
@@ -152,7 +155,7 @@ static cudaError_t tangent_launch(const Frame& f, const OutSoA& out, uint32_t n,
   return cudaGetLastError();
 }
 
-template <class C, bool kGrad>
+template <class C, bool kGrad, class I = SmRk4>
 static cudaError_t smooth_launch(const Frame& f, const OutSoA& out, uint32_t n, const SmJob& job,
                                  const uint32_t* list, uint32_t n_list, const uint32_t* n_dev,
                                  uint32_t* queue,
@@ -160,11 +163,11 @@ static cudaError_t smooth_launch(const Frame& f, const OutSoA& out, uint32_t n, 
   int sms = 0, per_sm = 0;
   cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   if (e != cudaSuccess) return e;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_smooth<C, kGrad>, kSmBlock, 0);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_smooth<C, kGrad, I>, kSmBlock, 0);
   if (e != cudaSuccess) return e;
   const int grid = sms * (per_sm < 1 ? 1 : per_sm);
-  k_smooth<C, kGrad><<<grid, kSmBlock, 0, st>>>(f, out, job, n, list, n_list, n_dev, queue, fb_pix,
-                                                 fb_n);
+  k_smooth<C, kGrad, I><<<grid, kSmBlock, 0, st>>>(f, out, job, n, list, n_list, n_dev, queue, fb_pix,
+                                                    fb_n);
   return cudaGetLastError();
 }
 
@@ -174,6 +177,15 @@ cudaError_t launch_smooth(const Frame& f, const OutSoA& out, uint32_t n, const S
   memset(&none, 0, sizeof none);
   const SmJob& jb = job ? *job : none;
   const bool grad = job != nullptr;
+  // BL frames with DOPRI5 (KS frames integrate with RK4, their BL passes too)
+  const bool dp5 = f.intg == 1 && f.chart == 1;  // KT_DOPRI5, KT_CHART_BL
+  if (dp5) {
+    if (grad && job->tangent_dir >= 0) return cudaErrorInvalidValue;  // no DOPRI5 tangent
+    return grad ? smooth_launch<ChartBL, true, SmDp5>(f, out, n, jb, jb.pix, jb.n_pix, nullptr,
+                                                      counters, nullptr, nullptr, device, st)
+                : smooth_launch<ChartBL, false, SmDp5>(f, out, n, jb, jb.pix, jb.n_pix, nullptr,
+                                                       counters, nullptr, nullptr, device, st);
+  }
   if (grad && job->tangent_dir >= 0) {
     if (f.chart == 0 && !job->force_bl) {
       cudaError_t e = tangent_launch<ChartKS>(f, out, n, jb, jb.pix, jb.n_pix, nullptr, counters, fb_pix,

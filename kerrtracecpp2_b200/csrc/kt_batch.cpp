@@ -58,14 +58,16 @@ struct Group {
 };
 
 int default_variant(kt::Mode m) {
-  // The single-frame launch shapes (kt_kernels.cu, kt_mixed.cu): 128 x 1
-  // for the bundle and separable-Kerr kernels, 64 x 9 for the others.
-  return (m == kt::kModeBundle || m == kt::kModeBundleMixed || m == kt::kModeSepRk4) ? 1 : 0;
+  // The single-frame launch shapes (kt_kernels.cu, kt_mixed.cu): two lanes
+  // per ray, 128 x 3, for the FP64 bundle kernel; 128 x 1 for the mixed
+  // bundle and separable-Kerr kernels; 64 x 9 for the others.
+  if (m == kt::kModeBundle) return kt::kBatchPairVariant;
+  return (m == kt::kModeBundleMixed || m == kt::kModeSepRk4) ? 1 : 0;
 }
 
 int default_refill(kt::Mode m) {
-  // ... and their refill thresholds
-  return m == kt::kModeBundle ? 16 : m == kt::kModeSepRk4 ? 1 : 32;
+  // ... and their refill thresholds (in lanes)
+  return m == kt::kModeBundle ? 8 : m == kt::kModeSepRk4 ? 1 : 32;
 }
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -148,6 +150,7 @@ kt_status tune_group(kt_context* ctx, Group& g, const kt_batch_options& opt) {
   KT_CUDA(ctx, cudaEventCreate(&guard.e1), "event");
   kt::LaunchShape shapes[kt::kBatchVariants];
   for (int v = 0; v < kt::kBatchVariants; ++v) {
+    if (!kt::batch_variant_ok(g.mode, v)) continue;
     KT_CUDA(ctx, kt::batch_shape(g.mode, v, ctx->device, &shapes[v]), "occupancy query");
     // Untimed first launch of each variant (module load, caches).
     KT_CUDA(ctx, cudaMemsetAsync(g.d_counters, 0, 4 * sizeof(uint32_t), st), "reset queue");
@@ -158,6 +161,7 @@ kt_status tune_group(kt_context* ctx, Group& g, const kt_batch_options& opt) {
   float best = 1e30f, dflt = -1.f;
   int candidates = 0;
   for (int v = 0; v < kt::kBatchVariants; ++v) {
+    if (!kt::batch_variant_ok(g.mode, v)) continue;
     for (int rm : kRefillCandidates) {
       float t = 1e30f;
       for (int r = 0; r < reps; ++r) {
@@ -384,7 +388,9 @@ kt_status kt_batch_create(kt_context* ctx, const kt_frame_desc* descs, const kt_
       g.fb_variant = default_variant(g.fb_mode);
       KT_CUDA(ctx, kt::batch_shape(g.fb_mode, g.fb_variant, ctx->device, &g.fb_shape), "occupancy query");
     }
-    g.variant = opt.variant >= 0 ? opt.variant : default_variant(g.mode);
+    // a variant the group's kernel lacks (the paired one, outside bundles)
+    // gives the group its default variant
+    g.variant = kt::batch_variant_ok(g.mode, opt.variant) ? opt.variant : default_variant(g.mode);
     g.refill_min = opt.refill_min > 0 ? opt.refill_min : default_refill(g.mode);
     if (opt.flags & KT_BATCH_AUTOTUNE) {
       kt_status r = tune_group(ctx, g, opt);
@@ -401,7 +407,7 @@ kt_status kt_batch_create(kt_context* ctx, const kt_frame_desc* descs, const kt_
     in.min_blocks = kt::kBatchMinBlocks[g.variant];
     in.grid = g.shape.grid;
     in.refill_min = g.refill_min;
-    in.rays_per_warp = 32;
+    in.rays_per_warp = kt::kBatchRaysPerWarp[g.variant];
   }
   kt_status r = capture(ctx, b, counters_bytes, d_counters);
   if (r != KT_OK) return r;

@@ -240,11 +240,6 @@ kt_status prepare_frame(const kt_frame_desc* d, Frame* f, kt_frame_derived* dv, 
     *err = "the smooth tracer has no ray-bundle mode";
     return KT_ERR_UNSUPPORTED;
   }
-  if (d->precision == KT_PREC_SMOOTH && d->integrator == KT_DOPRI5 &&
-      (d->chart == KT_CHART_BL || fabs(d->Lambda) > 1e-15)) {
-    *err = "the smooth tracer integrates with RK4 step doubling only";
-    return KT_ERR_UNSUPPORTED;
-  }
   if ((d->flags & ~(uint32_t)KT_FLAG_ANGLES_RADIANS) != 0) {
     *err = "unknown bits in flags";
     return KT_ERR_INVALID_ARGUMENT;

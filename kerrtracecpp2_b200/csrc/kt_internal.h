@@ -145,9 +145,16 @@ struct BatchRays {
 // block, minimum resident blocks per SM).  The second number sets the
 // register cap: 65536 / (threads x blocks) per thread, rounded down to the
 // allocation granule (112 for 64 x 9, 80 for 64 x 12, none for 128 x 1).
-constexpr int kBatchVariants = 3;
-constexpr int kBatchBlock[kBatchVariants] = {64, 128, 64};
-constexpr int kBatchMinBlocks[kBatchVariants] = {9, 1, 12};
+constexpr int kBatchVariants = 4;
+constexpr int kBatchBlock[kBatchVariants] = {64, 128, 64, 128};
+constexpr int kBatchMinBlocks[kBatchVariants] = {9, 1, 12, 3};
+// Variant 3 runs two lanes per ray (16 rays per warp); only the FP64 bundle
+// kernel has that form.
+constexpr int kBatchPairVariant = 3;
+constexpr int kBatchRaysPerWarp[kBatchVariants] = {32, 32, 32, 16};
+inline bool batch_variant_ok(Mode m, int v) {
+  return v >= 0 && v < kBatchVariants && (v != kBatchPairVariant || m == kModeBundle);
+}
 
 // Shape (grid at full occupancy) and launch of variant `variant` of `mode`.
 // The KS fallback list receives batch ray indices.

@@ -178,10 +178,10 @@ template <> struct Shape<struct ModeBundle> { static constexpr int kBlock = 128,
 #define KT_BUNDLE_PAIR_BLOCK 128
 #endif
 #ifndef KT_BUNDLE_PAIR_MINB
-#define KT_BUNDLE_PAIR_MINB 4
+#define KT_BUNDLE_PAIR_MINB 3
 #endif
 #ifndef KT_BUNDLE_PAIR_REFILL
-#define KT_BUNDLE_PAIR_REFILL 16
+#define KT_BUNDLE_PAIR_REFILL 8
 #endif
 template <> struct Shape<ModeBundlePair> {
   static constexpr int kBlock = KT_BUNDLE_PAIR_BLOCK, kMinBlocks = KT_BUNDLE_PAIR_MINB,
@@ -220,7 +220,11 @@ cudaError_t batch_shape(Mode mode, int variant, int device, LaunchShape* shape) 
     case kModeBLRk4: return batch_shape<ModeBLRk4>(variant, device, shape);
     case kModeBLDopri5: return batch_shape<ModeBLDopri5>(variant, device, shape);
     case kModeKSRk4: return batch_shape<ModeKSRk4>(variant, device, shape);
-    case kModeBundle: return batch_shape<ModeBundle>(variant, device, shape);
+    case kModeBundle:
+      if (variant == kBatchPairVariant)
+        return batch_shape_pair_for<ModeBundlePair, kBatchBlock[kBatchPairVariant],
+                                    kBatchMinBlocks[kBatchPairVariant]>(device, shape);
+      return batch_shape<ModeBundle>(variant, device, shape);
     case kModeSepRk4: return batch_shape<ModeSepRk4>(variant, device, shape);
     default: return batch_shape_mixed(mode, variant, device, shape);
   }
@@ -232,7 +236,14 @@ cudaError_t launch_batch(Mode mode, int variant, const BatchRays& br, uint32_t* 
     case kModeBLRk4: return batch_launch<ModeBLRk4>(variant, br, queue, fb, s, st);
     case kModeBLDopri5: return batch_launch<ModeBLDopri5>(variant, br, queue, fb, s, st);
     case kModeKSRk4: return batch_launch<ModeKSRk4>(variant, br, queue, fb, s, st);
-    case kModeBundle: return batch_launch<ModeBundle>(variant, br, queue, fb, s, st);
+    case kModeBundle:
+      if (variant == kBatchPairVariant) {
+        k_trace_batch_pair<ModeBundlePair, kBatchBlock[kBatchPairVariant],
+                           kBatchMinBlocks[kBatchPairVariant]><<<s.grid, s.block, s.smem, st>>>(
+            br, queue, fb);
+        return cudaGetLastError();
+      }
+      return batch_launch<ModeBundle>(variant, br, queue, fb, s, st);
     case kModeSepRk4: return batch_launch<ModeSepRk4>(variant, br, queue, fb, s, st);
     default: return launch_batch_mixed(mode, variant, br, queue, fb, s, st);
   }

@@ -123,9 +123,6 @@ struct Inv {
   double tt, tp, rr, hh, pp;  // g^tt, g^tphi, g^rr, g^thth, g^phiphi
 };
 
-// The quotients over pre (g^tt, g^tphi) and over sig (g^rr, g^thth) share
-// their denominator's correctly rounded reciprocal (ktm_div_rcp: the IEEE
-// quotient in a product and four fma); g^phiphi keeps its division.
 template <bool kD3 = true>
 KT_HD Inv bl_inv(const Metric& g, double r, const Ang& A) {
   const double r_sq = r * r;
@@ -134,12 +131,11 @@ KT_HD Inv bl_inv(const Metric& g, double r, const Ang& A) {
   const double dr = bl_delta_r<kD3>(g, r, r2a2);
   const double dth = A.dth;
   const double pre = (sig * dr) * dth;
-  const double ipre = ktm_rcp(pre), isig = ktm_rcp(sig);
   Inv U;
-  U.tt = ktm_div_rcp((-g.xi2) * ((dth * r2a2) * r2a2 - ((dr * g.a) * g.a) * A.st2), pre, ipre);
-  U.tp = ktm_div_rcp(g.axi2 * (dr - dth * r2a2), pre, ipre);
-  U.rr = ktm_div_rcp(dr, sig, isig);
-  U.hh = ktm_div_rcp(dth, sig, isig);
+  U.tt = ((-g.xi2) * ((dth * r2a2) * r2a2 - ((dr * g.a) * g.a) * A.st2)) / pre;
+  U.tp = (g.axi2 * (dr - dth * r2a2)) / pre;
+  U.rr = dr / sig;
+  U.hh = dth / sig;
   U.pp = (A.st2 > 1e-14) ? (g.xi2 * (dr - ((dth * g.a) * g.a) * A.st2)) / (pre * A.st2) : 0.0;
   return U;
 }
@@ -1053,8 +1049,65 @@ struct BundleHalf {
   double k0, k1, k4;  // dr, dtheta, dphi from the centre's g^{mu nu}
 };
 
+#ifndef KT_BUNDLE_HALF_ROLLED
+#define KT_BUNDLE_HALF_ROLLED 1
+#endif
+
+// Code shape of the split (kRolled): the angle factors, the three
+// five-Hamiltonian inverse metrics and the four one-Hamiltonian ones in
+// rolled loops (one copy of bl_ang, two of bl_inv, six of bl_ham: the paired
+// kernel's instruction fetch), or everything unrolled.  Same arithmetic.
+template <bool kRolled = (KT_BUNDLE_HALF_ROLLED != 0)>
 KT_HD void bundle_rhs_half(const Metric& g, double r, double th, double pr, double pth, double pt,
-                           double pphi, bool odd, BundleHalf* o) {
+                           double pphi, bool odd, BundleHalf* o);
+
+template <>
+KT_HD void bundle_rhs_half<true>(const Metric& g, double r, double th, double pr, double pth,
+                                 double pt, double pphi, bool odd, BundleHalf* o) {
+  const double sgn = odd ? -1.0 : 1.0;
+  const double eps_r = 1e-5 * dmax(fabs(r), 0.01);
+  const double eps_th = 1e-6;
+  const double e0 = 1e-5 * (fabs(r) + 0.1);
+  const double e1 = 1e-5;
+  const double e2 = 1e-5 * (fabs(pr) + 1e-3);
+  const double e3 = 1e-5 * (fabs(pth) + 1e-3);
+  Ang A[3];  // theta; theta + e1 | + (-e1); theta + eps_th | - eps_th
+  KT_ROLLED
+  for (int j = 0; j < 3; ++j) {
+    const double x = (j == 0) ? th : th + sgn * ((j == 1) ? e1 : eps_th);
+    A[j] = bl_ang<false>(g, x);
+  }
+  const double rp = r + e0, rm = r + (-e0);
+  const double prp = pr + e2, prm = pr + (-e2);
+  const double pthp = pth + e3, pthm = pth + (-e3);
+  // t0..t2: five Hamiltonians each (lane 1 at t0: the (2,3) corners)
+  KT_ROLLED
+  for (int t = 0; t < 3; ++t) {
+    const double rad = (t == 1) ? (odd ? rm : rp) : r;
+    const Inv U = bl_inv<false>(g, rad, A[t == 2 ? 1 : 0]);
+    if (t == 0) {
+      o->k0 = U.rr * pr;
+      o->k1 = U.hh * pth;
+      o->k4 = U.tp * pt + U.pp * pphi;
+    }
+    const bool c23 = (t == 0) && odd;
+    o->h5[t][0] = bl_ham(U, c23 ? prp : pr, c23 ? pthp : pth, pt, pphi);
+    o->h5[t][1] = bl_ham(U, prp, c23 ? pthm : pth, pt, pphi);
+    o->h5[t][2] = bl_ham(U, prm, c23 ? pthp : pth, pt, pphi);
+    o->h5[t][3] = bl_ham(U, c23 ? prm : pr, c23 ? pthm : pthp, pt, pphi);
+    o->h5[t][4] = bl_ham(U, c23 ? prm : pr, pthm, pt, pphi);
+  }
+  // t3..t6: one Hamiltonian each
+  KT_ROLLED
+  for (int t = 0; t < 4; ++t) {
+    const double rad = (t == 0) ? (odd ? r - eps_r : r + eps_r) : (t == 1) ? r : (t == 2) ? rp : rm;
+    o->h1[t] = bl_ham(bl_inv<false>(g, rad, A[t == 1 ? 2 : (t == 0 ? 0 : 1)]), pr, pth, pt, pphi);
+  }
+}
+
+template <>
+KT_HD void bundle_rhs_half<false>(const Metric& g, double r, double th, double pr, double pth,
+                                  double pt, double pphi, bool odd, BundleHalf* o) {
   const double sgn = odd ? -1.0 : 1.0;
   const double eps_r = 1e-5 * dmax(fabs(r), 0.01);
   const double eps_th = 1e-6;

@@ -179,6 +179,113 @@ KT_HD int sm_attempt(double M, const SmPrm<double>& P, double tol, const double*
   return res;
 }
 
+// ---- DOPRI5 (BL chart) ------------------------------------------------------
+// dopri5_adaptive (geodesic.hpp:312-414) for the smooth tracer: stages
+// k2..k6 from the Dormand-Prince tableau, the fifth-order result y5, k7 =
+// f(y5), the error norm sqrt(sum_i (dy_i / (tol (1 + |y_i|)))^2 / 4) with
+// dy = y5 - y4 formed from the stages as h sum_j (b5_j - b4_j) k_j (the same
+// quantity without the rounding of the two states), and the reference's
+// controller.  Phi is not advanced (the reference's `advance` updates r,
+// theta, p_r, p_theta only).  The stage records are u[s] (s = 1..6, u[6] =
+// y5) and k[s] (s = 0..6).
+
+// a_{s j}: stage s = 1..5 (the inputs of k2..k6), s = 6: b5 (y5)
+KT_HD double dp5_a(int s, int j) {
+  const double A[6][6] = {
+      {1.0 / 5.0, 0.0, 0.0, 0.0, 0.0, 0.0},
+      {3.0 / 40.0, 9.0 / 40.0, 0.0, 0.0, 0.0, 0.0},
+      {44.0 / 45.0, -56.0 / 15.0, 32.0 / 9.0, 0.0, 0.0, 0.0},
+      {19372.0 / 6561.0, -25360.0 / 2187.0, 64448.0 / 6561.0, -212.0 / 729.0, 0.0, 0.0},
+      {9017.0 / 3168.0, -355.0 / 33.0, 46732.0 / 5247.0, 49.0 / 176.0, -5103.0 / 18656.0, 0.0},
+      {35.0 / 384.0, 0.0, 500.0 / 1113.0, 125.0 / 192.0, -2187.0 / 6784.0, 11.0 / 84.0}};
+  return A[s - 1][j];
+}
+// b5_j - b4_j, j = 0..6 (the exact rationals, each rounded once)
+KT_HD double dp5_e(int j) {
+  const double E[7] = {71.0 / 57600.0, 0.0, -71.0 / 16695.0, 71.0 / 1920.0, -17253.0 / 339200.0,
+                       22.0 / 525.0, -1.0 / 40.0};
+  return E[j];
+}
+
+template <class C>
+KT_HD_CALL void sm_dp_paths(double M, const SmPrm<double>& P, const double* c, const double* y,
+                            const double* k1, double hh, double* y5, double* dy, SmStages* rec) {
+  constexpr int n = C::kN;
+  double kk[7][n], u[n], fp;
+  for (int i = 0; i < n; ++i) kk[0][i] = k1[i];
+  KT_ROLLED
+  for (int s = 1; s <= 6; ++s) {
+    for (int i = 0; i < n; ++i) u[i] = y[i];
+    for (int j = 0; j < s; ++j) {
+      const double hw = hh * dp5_a(s, j);
+      for (int i = 0; i < n; ++i) u[i] = u[i] + hw * kk[j][i];
+    }
+    sm_rhs<C>(M, P, u, c, kk[s], &fp);
+    if (rec)
+      for (int i = 0; i < n; ++i) rec->u[s][i] = u[i];
+    if (s == 6)
+      for (int i = 0; i < n; ++i) y5[i] = u[i];
+  }
+  for (int i = 0; i < n; ++i) {
+    double d = 0.0;
+    for (int j = 0; j < 7; ++j) d = d + (hh * dp5_e(j)) * kk[j][i];
+    dy[i] = d;
+  }
+  if (rec)
+    for (int j = 0; j < 7; ++j)
+      for (int i = 0; i < n; ++i) rec->k[j][i] = kk[j][i];
+}
+
+KT_HD double sm_dp_err(const double* dy, const double* y, double tol, int n) {
+  double e2 = 0.0;
+  for (int i = 0; i < n; ++i) {
+    const double ratio = dy[i] / (tol * (1.0 + fabs(y[i])));
+    e2 = e2 + ratio * ratio;
+  }
+  return sqrt(e2 / (double)n);
+}
+
+// The controller of dopri5_adaptive (geodesic.hpp:392-413): 1 accepted,
+// 0 rejected, -1 a non-finite error norm (h halved, FSAL dropped).
+KT_HD int dp5_update(double err, double* h) {
+  if (!finite(err)) {
+    *h = (finite(*h) && *h > 1e-10) ? *h * 0.5 : 1e-6;
+    if (*h < 1e-10) *h = 1e-10;
+    return -1;
+  }
+  if (err <= 1.0 || *h < 1e-10) {
+    const double fac = (err > 1e-12) ? 0.9 * ktm_pow(1.0 / err, 0.2) : 4.0;
+    double hnew = *h * fac;
+    if (!finite(hnew)) hnew = *h;
+    if (hnew > 100.0) hnew = 100.0;
+    if (hnew < 1e-10) hnew = 1e-10;
+    *h = hnew;
+    return 1;
+  }
+  double hnew = (*h * 0.9) * ktm_pow(1.0 / err, 0.25);
+  if (!finite(hnew)) hnew = *h * 0.5;
+  *h = dmax(hnew, 1e-10);
+  return 0;
+}
+
+// One DOPRI5 attempt from (y, pas) with k1 = f(y): on acceptance (yo, paso)
+// = (y5, pas).
+template <class C>
+KT_HD int sm_attempt_dp(double M, const SmPrm<double>& P, double tol, const double* c, const double* y,
+                        double pas, const double* k1, double, double* h, double* yo, double* paso) {
+  double y5[C::kN], dy[C::kN];
+  sm_dp_paths<C>(M, P, c, y, k1, *h, y5, dy, nullptr);
+  const int res = dp5_update(sm_dp_err(dy, y, tol, C::kN), h);
+  if (res == 1) {
+    for (int i = 0; i < C::kN; ++i) yo[i] = y5[i];
+    *paso = pas;
+  }
+  return res;
+}
+
+struct SmRk4;
+struct SmDp5;
+
 // Outputs of a stop without event: {ESCAPED, r, 1, theta, phi} of the state.
 template <class C>
 KT_HD void sm_stop(const Frame& f, const double* y, double pas, int status, uint32_t steps,
@@ -201,7 +308,7 @@ KT_HD void sm_stop(const Frame& f, const double* y, double pas, int status, uint
 // (y, dlam, attempts) is kept in ring[m % 32] (the last 32 steps).  On a disk hit `ev` receives the
 // final step; returns the number of accepted steps N (0 if the ray ended
 // otherwise or more than 131072 steps were taken with recording on).
-template <class C>
+template <class C, class I = SmRk4>
 KT_HD int sm_trace(const Frame& f, const SmPrm<double>& P, const double* y_in, const double* c,
                    double pas_in, RayResult* o, SmEvent* ev, SmCk* ck, int* ck_k, int* ck_n,
                    SmSt* ring) {
@@ -252,7 +359,7 @@ KT_HD int sm_trace(const Frame& f, const SmPrm<double>& P, const double* y_in, c
     for (;;) {
       step_used = h;
       ++attempts;
-      if (sm_attempt<C>(M, P, f.tol, c, yp, pasp, kprev, kprevp, &h, y, &pas) == 1) break;
+      if (I::template attempt<C>(M, P, f.tol, c, yp, pasp, kprev, kprevp, &h, y, &pas) == 1) break;
       int status;
       if (reject_cap(h, &rejects, &status)) {
         sm_stop<C>(f, yp, pasp, status, (uint32_t)it, attempts, o);
@@ -344,7 +451,7 @@ KT_HD int sm_trace(const Frame& f, const SmPrm<double>& P, const double* y_in, c
 // Replay `n` accepted steps from checkpoint `ck0` (the controller from its
 // dlam, rejections included).  Stores each step's start (y_n, H_n) and its
 // number of attempts into st[0..n) and/or a checkpoint every k2 steps into ck2.
-template <class C>
+template <class C, class I = SmRk4>
 KT_HD void sm_replay(const Frame& f, const SmPrm<double>& P, const double* c, const SmCk& ck0, int n,
                      SmSt* st, SmCk* ck2, int k2) {
   const double M = f.g.M;
@@ -366,7 +473,7 @@ KT_HD void sm_replay(const Frame& f, const SmPrm<double>& P, const double* c, co
     KT_ROLLED
     for (;;) {
       ++na;
-      if (sm_attempt<C>(M, P, f.tol, c, y, pas, k1, k1p, &h, y1, &pas1) == 1) break;
+      if (I::template attempt<C>(M, P, f.tol, c, y, pas, k1, k1p, &h, y1, &pas1) == 1) break;
       int status;
       if (reject_cap(h, &rejects, &status)) break;  // not reached: the forward accepted
     }
@@ -537,13 +644,139 @@ KT_HD double sm_attempt_bwd(const Frame& f, const SmPrm<double>& P, const double
   return hb;
 }
 
+// Partial derivatives of dp5_update's new step in (h, err) on the branch it
+// takes (zero where a clamp or a constant is chosen).
+KT_HD void sm_dp_ctl_partials(double err, double h, double* dh, double* de) {
+  *dh = 0.0;
+  *de = 0.0;
+  if (!finite(err)) {
+    if (finite(h) && h > 1e-10 && !(h * 0.5 < 1e-10)) *dh = 0.5;
+    return;
+  }
+  if (err <= 1.0 || h < 1e-10) {
+    const double fac = (err > 1e-12) ? 0.9 * ktm_pow(1.0 / err, 0.2) : 4.0;
+    const double hnew = h * fac;
+    if (!finite(hnew)) {
+      if (h > 100.0 || h < 1e-10) return;
+      *dh = 1.0;
+      return;
+    }
+    if (hnew > 100.0 || hnew < 1e-10) return;
+    *dh = fac;
+    if (err > 1e-12) *de = -0.2 * hnew / err;
+    return;
+  }
+  const double hnew = (h * 0.9) * ktm_pow(1.0 / err, 0.25);
+  if (!finite(hnew)) {
+    if (!(h * 0.5 < 1e-10)) *dh = 0.5;
+    return;
+  }
+  if (hnew < 1e-10) return;
+  *dh = hnew / h;
+  *de = -0.25 * hnew / err;
+}
+
+// Reverse of one DOPRI5 attempt (the arguments as sm_attempt_bwd's; the
+// passenger phi is not integrated).  The error norm feeds the controller:
+// its cotangent reaches dy (and the scales' |y_i|), dy = h sum_j e_j k_j
+// reaches every slope; y5 = y + h sum_{j<6} b5_j k_j gets yb_out plus k7's
+// VJP; then the stage inputs u_s = y + h sum_{j<s} a_sj k_j, s = 5..1, walk
+// back (each slope's cotangent complete before its VJP), and k1 = f(y) last.
+template <class C>
+KT_HD double sm_attempt_bwd_dp(const Frame& f, const SmPrm<double>& P, const double* c, const double* y,
+                               double hh, double gout, const double* yb_out, double hbar_extra,
+                               double* ybar, double* cbar, double* pbar, SmStages* st) {
+  constexpr int n = C::kN;
+  const double M = f.g.M;
+  double k1[n], k1p, y5[n], dy[n];
+  sm_rhs<C>(M, P, y, c, k1, &k1p);
+  sm_dp_paths<C>(M, P, c, y, k1, hh, y5, dy, st);
+  const double err = sm_dp_err(dy, y, f.tol, n);
+  double dh, de;
+  sm_dp_ctl_partials(err, hh, &dh, &de);
+  const double eb = gout * de;
+  double hb = gout * dh + hbar_extra;
+  const bool ok = err > 0.0 && finite(err);
+  double dyb[n];
+  for (int i = 0; i < n; ++i) {
+    const double sc = f.tol * (1.0 + fabs(y[i]));
+    const double ratio = dy[i] / sc;
+    const double rb = ok ? eb * ratio / ((double)n * err) : 0.0;  // d err / d ratio_i = ratio_i / (n err)
+    dyb[i] = rb / sc;
+    const double sg = y[i] > 0.0 ? 1.0 : (y[i] < 0.0 ? -1.0 : 0.0);
+    ybar[i] = ybar[i] - rb * ratio * (f.tol * sg) / sc;  // through the scale tol (1 + |y_i|)
+  }
+  double kb[7][n];
+  for (int j = 0; j < 7; ++j) {
+    const double he = hh * dp5_e(j);
+    double dk = 0.0;
+    for (int i = 0; i < n; ++i) {
+      kb[j][i] = he * dyb[i];
+      dk = dk + dyb[i] * st->k[j][i];
+    }
+    hb = hb + dp5_e(j) * dk;
+  }
+  double w[n];
+  sm_vjp_f<C>(M, P, st->u[6], c, kb[6], w, cbar, pbar);  // k7 = f(y5)
+  for (int i = 0; i < n; ++i) w[i] = w[i] + (yb_out ? yb_out[i] : 0.0);
+  KT_ROLLED
+  for (int s = 6; s >= 1; --s) {
+    if (s < 6) sm_vjp_f<C>(M, P, st->u[s], c, kb[s], w, cbar, pbar);  // w = cotangent of u_s
+    for (int i = 0; i < n; ++i) ybar[i] = ybar[i] + w[i];
+    for (int j = 0; j < s; ++j) {
+      const double a = dp5_a(s, j);
+      double dk = 0.0;
+      for (int i = 0; i < n; ++i) {
+        kb[j][i] = kb[j][i] + (hh * a) * w[i];
+        dk = dk + w[i] * st->k[j][i];
+      }
+      hb = hb + a * dk;
+    }
+  }
+  sm_vjp_f<C>(M, P, y, c, kb[0], w, cbar, pbar);  // k1 = f(y)
+  for (int i = 0; i < n; ++i) ybar[i] = ybar[i] + w[i];
+  return hb;
+}
+
+// The integrators of the smooth tracer: an attempt and its reverse.
+struct SmRk4 {
+  template <class C>
+  KT_HD static int attempt(double M, const SmPrm<double>& P, double tol, const double* c, const double* y,
+                           double pas, const double* k1, double k1p, double* h, double* yo,
+                           double* paso) {
+    return sm_attempt<C>(M, P, tol, c, y, pas, k1, k1p, h, yo, paso);
+  }
+  template <class C>
+  KT_HD static double attempt_bwd(const Frame& f, const SmPrm<double>& P, const double* c,
+                                  const double* y, double hh, double gout, const double* yb_out,
+                                  double hbar_extra, double* ybar, double* cbar, double* pbar,
+                                  SmStages* st) {
+    return sm_attempt_bwd<C>(f, P, c, y, hh, gout, yb_out, hbar_extra, ybar, cbar, pbar, st);
+  }
+};
+struct SmDp5 {
+  template <class C>
+  KT_HD static int attempt(double M, const SmPrm<double>& P, double tol, const double* c, const double* y,
+                           double pas, const double* k1, double k1p, double* h, double* yo,
+                           double* paso) {
+    return sm_attempt_dp<C>(M, P, tol, c, y, pas, k1, k1p, h, yo, paso);
+  }
+  template <class C>
+  KT_HD static double attempt_bwd(const Frame& f, const SmPrm<double>& P, const double* c,
+                                  const double* y, double hh, double gout, const double* yb_out,
+                                  double hbar_extra, double* ybar, double* cbar, double* pbar,
+                                  SmStages* st) {
+    return sm_attempt_bwd_dp<C>(f, P, c, y, hh, gout, yb_out, hbar_extra, ybar, cbar, pbar, st);
+  }
+};
+
 constexpr int kSmMaxAttempts = 66;  // reject cap 64 + the accepted attempt
 
 // Reverse of accepted step n from (y_n, H_n, attempts).  In: ybar =
 // cotangent of y_{n+1}, *Hbar = cotangent of H_{n+1}, hbar_acc = extra
 // cotangent of the accepted size (the event's).  Out: ybar = cotangent of
 // y_n, *Hbar = of H_n.
-template <class C>
+template <class C, class I = SmRk4>
 KT_HD void sm_step_bwd(const Frame& f, const SmPrm<double>& P, const double* c, const SmSt& st,
                        double hbar_acc, double* ybar, double* Hbar, double* cbar, double* pbar,
                        SmStages* stg) {
@@ -558,7 +791,7 @@ KT_HD void sm_step_bwd(const Frame& f, const SmPrm<double>& P, const double* c, 
     double h = st.H;
     KT_ROLLED
     for (int j = 0; j + 1 < na; ++j) {
-      sm_attempt<C>(M, P, f.tol, c, st.y, 0.0, k1, k1p, &h, yo, &po);
+      I::template attempt<C>(M, P, f.tol, c, st.y, 0.0, k1, k1p, &h, yo, &po);
       hs[j + 1] = h;
     }
   }
@@ -571,8 +804,8 @@ KT_HD void sm_step_bwd(const Frame& f, const SmPrm<double>& P, const double* c, 
   KT_ROLLED
   for (int j = na - 1; j >= 0; --j) {
     const bool acc = (j == na - 1);
-    gout = sm_attempt_bwd<C>(f, P, c, st.y, hs[j], gout, acc ? yb_out : nullptr, acc ? hbar_acc : 0.0,
-                             ybar, cbar, pbar, stg);
+    gout = I::template attempt_bwd<C>(f, P, c, st.y, hs[j], gout, acc ? yb_out : nullptr,
+                                      acc ? hbar_acc : 0.0, ybar, cbar, pbar, stg);
   }
   *Hbar = gout;
 }
@@ -661,7 +894,7 @@ struct SmScratch {
 // one ending in the disk event `ev`, checkpoints every k1 steps in
 // sc->ck1).  Returns the cotangents of the initial state, the constants
 // and (a, Q, Lambda).  The initial dlam is a constant (step_init).
-template <class C>
+template <class C, class I = SmRk4>
 KT_HD void sm_adjoint(const Frame& f, const SmPrm<double>& P, const double* c, const SmEvent& ev,
                       int N, int k1, double gbar, double rbar, SmScratch* sc, double* ybar,
                       double* cbar, double* pbar) {
@@ -680,7 +913,7 @@ KT_HD void sm_adjoint(const Frame& f, const SmPrm<double>& P, const double* c, c
     const int s0 = sgi * k1;
     const int len = (N - s0 < k1) ? N - s0 : k1;
     const int nsub = (len + kSmCkSteps - 1) / kSmCkSteps;
-    if (nsub > 1) sm_replay<C>(f, P, c, sc->ck1[sgi], len, nullptr, sc->ck2, kSmCkSteps);
+    if (nsub > 1) sm_replay<C, I>(f, P, c, sc->ck1[sgi], len, nullptr, sc->ck2, kSmCkSteps);
     KT_ROLLED
     for (int sub = nsub - 1; sub >= 0; --sub) {
       const int t0 = sub * kSmCkSteps;
@@ -688,11 +921,11 @@ KT_HD void sm_adjoint(const Frame& f, const SmPrm<double>& P, const double* c, c
       // the last sub-segment (steps from a multiple of 32 up to N-1) is still
       // in the forward's ring of step starts
       if (!(sgi == nseg - 1 && sub == nsub - 1))
-        sm_replay<C>(f, P, c, nsub > 1 ? sc->ck2[sub] : sc->ck1[sgi], tl, sc->st, nullptr, 0);
+        sm_replay<C, I>(f, P, c, nsub > 1 ? sc->ck2[sub] : sc->ck1[sgi], tl, sc->st, nullptr, 0);
       KT_ROLLED
       for (int m = tl - 1; m >= 0; --m) {
-        sm_step_bwd<C>(f, P, c, sc->st[m], last ? hbar_ev : 0.0, ybar, &Hbar, cbar, pbar,
-                       &sc->stages);
+        sm_step_bwd<C, I>(f, P, c, sc->st[m], last ? hbar_ev : 0.0, ybar, &Hbar, cbar, pbar,
+                          &sc->stages);
         if (last) {
           for (int i = 0; i < C::kN; ++i) ybar[i] = ybar[i] + yb_direct[i];
           last = false;
@@ -744,7 +977,7 @@ enum : int {
 // into g[kGSlots].  In the KS chart a ray whose KS initialisation fails
 // (init_ks_state, main.cpp:1533-1538) is not traced: returns false, and the
 // caller hands it to the BL chart.
-template <class C, bool kGrad>
+template <class C, bool kGrad, class I = SmRk4>
 KT_HD bool sm_pixel(const Frame& f, uint32_t pix, const SmCot& cot, RayResult* o, double* g,
                     SmScratch* sc) {
   constexpr bool kKS = C::kN == 6;
@@ -767,8 +1000,8 @@ KT_HD bool sm_pixel(const Frame& f, uint32_t pix, const SmCot& cot, RayResult* o
   SmEvent ev;
   int k1 = 0, nck = 0;
   SmCk* ck = kGrad ? sc->ck1 : nullptr;
-  const int N = sm_trace<C>(f, P, y0, c0, kKS ? 0.0 : f.cam.phi_obs, o, &ev, ck, &k1, &nck,
-                            kGrad ? sc->st : nullptr);
+  const int N = sm_trace<C, I>(f, P, y0, c0, kKS ? 0.0 : f.cam.phi_obs, o, &ev, ck, &k1, &nck,
+                               kGrad ? sc->st : nullptr);
   if (!kGrad) return true;
   for (int q = 0; q < kGSlots; ++q) g[q] = 0.0;
   g[kGNumBL] = kKS ? 0.0 : 1.0;
@@ -791,7 +1024,7 @@ KT_HD bool sm_pixel(const Frame& f, uint32_t pix, const SmCot& cot, RayResult* o
   }
   g[kGNumGrad] = 1.0;
   double ybar[C::kN], cbar[C::kC], pbar[kSmPrm];
-  sm_adjoint<C>(f, P, c0, ev, N, k1, gbar, rbar, sc, ybar, cbar, pbar);
+  sm_adjoint<C, I>(f, P, c0, ev, N, k1, gbar, rbar, sc, ybar, cbar, pbar);
   // chain through the camera ray: Dual over (a, Q, Lambda, theta_obs, r_obs)
   typedef Dual<5> D5;
   SmPrm<D5> Pd;

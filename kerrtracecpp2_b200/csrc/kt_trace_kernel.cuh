@@ -314,6 +314,87 @@ __global__ void __launch_bounds__(BLOCK, MINB)
   }
 }
 
+// k_trace_batch with two lanes per ray (pair modes, as k_trace_pair): 16
+// rays per warp; both lanes of a pair take the same batch ray.
+template <class ModeT, int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB)
+    k_trace_batch_pair(const BatchRays br, uint32_t* __restrict__ queue, const Fallback fb) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  using Rec = SmemRecord<typename ModeT::Machine>;
+  ModeT mode;
+  mode.m = &reinterpret_cast<Rec*>(smem)[threadIdx.x >> 1].m;
+  bool active = false;
+  int fi = 0;
+  uint32_t pix = 0;
+  const uint64_t n = br.n_dev ? (uint64_t)*br.n_dev : br.n;
+  const unsigned lane = threadIdx.x & 31u;
+  const bool odd = (lane & 1u) != 0;
+  bool exhausted = false;
+  for (;;) {
+    if (!exhausted) {
+      const unsigned need = __ballot_sync(kFull, !active);
+      const int idle = __popc(need);
+      if (need && (idle >= br.refill_min || need == kFull)) {
+        const int leader = __ffs(need) - 1;
+        const unsigned cnt = (unsigned)idle >> 1;  // rays
+        unsigned base = 0;
+        if ((int)lane == leader) base = atomicAdd(queue, cnt);
+        base = __shfl_sync(kFull, base, leader);
+        if ((uint64_t)base + (uint64_t)cnt >= n) exhausted = true;
+        if (!active) {
+          const uint64_t idx =
+              (uint64_t)base + ((unsigned)__popc(need & ((1u << lane) - 1u)) >> 1);
+          if (idx < n) {
+            const uint32_t g = br.list ? br.list[idx] : (uint32_t)idx;
+            fi = batch_frame_of(br, g);
+            pix = (uint32_t)(g - br.offsets[fi]);
+            if (!odd) mode.start(br.frames[fi], pix, pix, g, fb);
+            active = true;
+          }
+        }
+      }
+      __syncwarp();  // new records written by the even lanes are visible to their partners
+    }
+    if (!__any_sync(kFull, active)) {
+      if (exhausted) break;
+      continue;
+    }
+    const Frame& f = br.frames[fi];
+    KT_ROLLED
+    for (int s = -1; s < ModeT::kSlots; ++s) {
+      const bool part = active && (s >= 0 || mode.needs_k1());
+      const unsigned pmask = __ballot_sync(kFull, part);
+      if (s < 0 && !pmask) continue;
+      if (part) {
+        RayResult res;
+        if (mode.slot(f, s, &res, odd, pmask)) {
+          if (!odd) write_result(br.outs[fi], pix, res);
+          active = false;
+        }
+      }
+    }
+  }
+}
+
+template <class ModeT, int BLOCK, int MINB>
+static cudaError_t batch_shape_pair_for(int device, LaunchShape* shape) {
+  int sms = 0, per_sm = 0;
+  cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  if (e != cudaSuccess) return e;
+  const size_t smem = smem_bytes_pair<ModeT>(BLOCK);
+  e = cudaFuncSetAttribute(k_trace_batch_pair<ModeT, BLOCK, MINB>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace_batch_pair<ModeT, BLOCK, MINB>,
+                                                    BLOCK, smem);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) per_sm = 1;
+  shape->block = BLOCK;
+  shape->grid = sms * per_sm;
+  shape->smem = smem;
+  return cudaSuccess;
+}
+
 template <class ModeT, int BLOCK, int MINB>
 static cudaError_t batch_shape_for(int device, LaunchShape* shape) {
   int sms = 0, per_sm = 0;

@@ -211,42 +211,6 @@ KTM_FN double ktm_div_odd(double x, double b, double y) {
 }
 KTM_FN double ktm_div3(double x) { return ktm_div_odd(x, 3.0, 0x1.5555555555555p-2); }
 
-/* ------------------------------------------- quotients over one denominator */
-
-/* RN(1/b): the correctly rounded reciprocal (CUDA's __drcp_rn on the device,
- * the IEEE division on the host). */
-KTM_FN double ktm_rcp(double b) {
-#if defined(__CUDA_ARCH__)
-  return __drcp_rn(b);
-#else
-  return 1.0 / b;
-#endif
-}
-
-/* a / b, the correctly rounded IEEE quotient, from y = RN(1/b) (ktm_rcp)
- * shared by the numerators over one denominator: a product and four fma
- * instead of a division.  Method: P. Markstein's correction (IBM J. Res.
- * Dev. 34(1), 1990) applied twice.  With u = 2^-53 and y = (1 + e)/b,
- * |e| <= u:
- *   q0 = RN(a y) lies within (2u + u^2)|a/b| of a/b: within two ulp, so
- *   not necessarily a faithful rounding;
- *   r0 = a - b q0 is exact in one fma (q0 a few ulp from a/b, no underflow
- *   in the guarded range), and q0 + r0 y = a/b - e (q0 - a/b) is within
- *   (2u^2 + u^3)|a/b| of a/b, so q1 = RN(q0 + r0 y) is within half an ulp
- *   plus that of a/b: a faithful rounding;
- *   Markstein's theorem -- y within half an ulp of 1/b, q1 faithful,
- *   r1 = a - b q1 exact -- gives RN(q1 + r1 y) = RN(a/b).
- * Arguments whose magnitude is outside [2^-255, 2^257) (zero, subnormal,
- * huge, Inf, NaN), where a quotient or a residual could leave the normal
- * range, take the division. */
-KTM_FN double ktm_div_rcp(double a, double b, double y) {
-  const uint32_t ea = (uint32_t)(ktm_bits(a) >> 52) & 0x7ffu;
-  const uint32_t eb = (uint32_t)(ktm_bits(b) >> 52) & 0x7ffu;
-  if (ea - 768u >= 512u || eb - 768u >= 512u) return a / b;
-  const double q0 = a * y;
-  const double q1 = fma(fma(-b, q0, a), y, q0);
-  return fma(fma(-b, q1, a), y, q1);
-}
 
 /* -------------------------------------------------------------------- exp */
 

@@ -43,7 +43,14 @@ def _np(out):
     return got
 
 
-def fd_check(renderer, base=CFG5, h4=1e-4, h2=1e-6):
+# Configuration 2's geometry with DOPRI5 at tol 1e-10 (the BL DOPRI5 adjoint),
+# its loss against the same tracer at a=0.92, theta=86.
+CFG2_DOPRI5 = dict(chart=1, integrator=1, tol=1e-10, a=0.9, Q=0.3, Lambda=1e-4, r_obs=60.0,
+                   theta_deg=85.0, fov_deg=30.0, disk_out=20.0, width=320, height=180)
+TARGET_CFG2 = dict(a=0.92, theta_deg=86.0)
+
+
+def fd_check(renderer, base=CFG5, h4=1e-4, h2=1e-6, target=None):
     """Returns {"five_point": .., "two_point": .., "two_point_loose": ..},
     each with the per-parameter adjoint, difference and relative
     disagreement, the worst of them and the number of pixels in the loss."""
@@ -52,7 +59,7 @@ def fd_check(renderer, base=CFG5, h4=1e-4, h2=1e-6):
     def smooth(kw):
         return _np(renderer.trace(abi.frame_desc(precision=abi.KT_PREC_SMOOTH, **kw)))
 
-    tgt = smooth(dict(base, a=0.72, theta_deg=71.0))
+    tgt = smooth(dict(base, **(target or dict(a=0.72, theta_deg=71.0))))
     b0 = smooth(base)
     bl0 = smooth(dict(base, chart=1))
     m_all = (b0["outcome"] == 1) & (tgt["outcome"] == 1)

@@ -84,13 +84,18 @@ RayResult run_ray(const Frame& f, uint32_t pix) {
 
 // Bundle RHS through the two-lane split (bundle_rhs_half for both lanes,
 // then bundle_rhs_combine), as the paired bundle kernel evaluates it.
-bool g_bundle_split = false;
+int g_bundle_split = 0;  // 1: the rolled code shape, 2: the unrolled one
 
 void bundle_rhs_split(const Metric& g, const double y[4], double pt, double pphi,
                       const double W[8], double k[5], double kW[8]) {
   BundleHalf E, O;
-  bundle_rhs_half(g, y[0], y[1], y[2], y[3], pt, pphi, false, &E);
-  bundle_rhs_half(g, y[0], y[1], y[2], y[3], pt, pphi, true, &O);
+  if (g_bundle_split == 2) {
+    bundle_rhs_half<false>(g, y[0], y[1], y[2], y[3], pt, pphi, false, &E);
+    bundle_rhs_half<false>(g, y[0], y[1], y[2], y[3], pt, pphi, true, &O);
+  } else {
+    bundle_rhs_half<true>(g, y[0], y[1], y[2], y[3], pt, pphi, false, &E);
+    bundle_rhs_half<true>(g, y[0], y[1], y[2], y[3], pt, pphi, true, &O);
+  }
   bundle_rhs_combine(E, O, y[0], y[2], y[3], W, k, kW);
 }
 
@@ -224,8 +229,9 @@ static int trace_pixels(const kt_frame_desc* d, int64_t n, const uint32_t* pix, 
   return 0;
 }
 
-// 1: FP64 bundle frames take the two-lane split of the bundle RHS.
-extern "C" void hc_set_bundle_split(int on) { g_bundle_split = on != 0; }
+// FP64 bundle frames take the two-lane split of the bundle RHS: 1 in its
+// rolled code shape, 2 unrolled; 0 the single-lane bundle_rhs.
+extern "C" void hc_set_bundle_split(int mode) { g_bundle_split = mode; }
 
 extern "C" int hc_trace_pixels(const kt_frame_desc* d, int64_t n, const uint32_t* pix,
                                uint8_t* outcome, double* r, double* red, double* magnif,
@@ -277,6 +283,10 @@ extern "C" int hc_smooth_pixels(const kt_frame_desc* d, int64_t n, const uint32_
   cot.t_r = t_r;
   cot.w_g = w_g;
   cot.w_r = w_r;
+  // BL frames with DOPRI5 take the smooth DOPRI5 integrator, as the kernels
+  // do (no forward-mode tangent for it)
+  const bool dp5 = f.intg == KT_DOPRI5 && f.chart == KT_CHART_BL;
+  if (dp5 && mode != 0 && tangent_dir >= 0) return 2;
 #pragma omp parallel
   {
     SmScratch* sc = new SmScratch;
@@ -294,10 +304,16 @@ extern "C" int hc_smooth_pixels(const kt_frame_desc* d, int64_t n, const uint32_
         done = mode == 0 ? sm_pixel<ChartKS, false>(f, pix[i], cot, &o, g, nullptr)
                          : sm_pixel<ChartKS, true>(f, pix[i], cot, &o, g, sc);
       if (!done) {
-        if (mode == 0)
+        if (dp5) {
+          if (mode == 0)
+            sm_pixel<ChartBL, false, SmDp5>(f, pix[i], cot, &o, g, nullptr);
+          else
+            sm_pixel<ChartBL, true, SmDp5>(f, pix[i], cot, &o, g, sc);
+        } else if (mode == 0) {
           sm_pixel<ChartBL, false>(f, pix[i], cot, &o, g, nullptr);
-        else
+        } else {
           sm_pixel<ChartBL, true>(f, pix[i], cot, &o, g, sc);
+        }
       }
       outcome[i] = (uint8_t)o.outcome;
       r[i] = o.r;

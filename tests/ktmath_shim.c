@@ -18,44 +18,3 @@ double kts_hypot(double x, double y) { return ktm_hypot(x, y); }
 void kts_div3_n(const double* x, double* q, long n) {
   for (long i = 0; i < n; ++i) q[i] = ktm_div3(x[i]);
 }
-
-/* ktm_div_rcp against the division on n pseudo-random (a, b) pairs
- * (xorshift64*, seed): mode 0 uniform exponents over the guarded range and
- * beyond (|x| in [2^-300, 2^300), either sign, zeros and powers of two
- * mixed in), mode 1 the renderer's range (mantissas uniform, |x| in
- * [2^-40, 2^60)).  Returns the number of quotients whose bits differ. */
-static uint64_t kts_next(uint64_t* s) {
-  *s ^= *s >> 12;
-  *s ^= *s << 25;
-  *s ^= *s >> 27;
-  return *s * 2685821657736338717ULL;
-}
-static double kts_draw(uint64_t* s, int lo, int hi) {
-  const uint64_t u = kts_next(s);
-  const uint64_t man = u & 0xfffffffffffffULL;
-  const int span = hi - lo;
-  const int ex = lo + (int)((kts_next(s) >> 11) % (uint64_t)span);
-  uint64_t bits = ((uint64_t)(ex + 1023) << 52) | man;
-  if ((u >> 52) & 1) bits |= 0x8000000000000000ULL;
-  if (((u >> 53) & 63) == 0) bits &= 0xfff0000000000000ULL;  /* a power of two */
-  double x;
-  memcpy(&x, &bits, 8);
-  if (((u >> 59) & 31) == 0 && lo < 0) x = 0.0;
-  return x;
-}
-long kts_div_rcp_check(uint64_t seed, long n, int mode) {
-  uint64_t s = seed | 1;
-  long bad = 0;
-  const int lo = mode == 0 ? -300 : -40, hi = mode == 0 ? 300 : 60;
-  for (long i = 0; i < n; ++i) {
-    const double a = kts_draw(&s, lo, hi), b = kts_draw(&s, lo, hi);
-    if (b == 0.0) continue;
-    const double q = ktm_div_rcp(a, b, ktm_rcp(b));
-    const double w = a / b;
-    uint64_t qb, wb;
-    memcpy(&qb, &q, 8);
-    memcpy(&wb, &w, 8);
-    bad += (qb != wb) && !(q != q && w != w);
-  }
-  return bad;
-}

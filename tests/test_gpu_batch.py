@@ -68,9 +68,30 @@ def test_variants_match_single_frame(renderer, variant, refill_min):
     ]
     b = renderer.batch(descs, options=abi.batch_options(variant=variant, refill_min=refill_min))
     for g in b.groups():
-        assert g["variant"] == variant and g["refill_min"] == refill_min and g["tuned"] == 0
+        # variant 3 (two lanes per ray) exists for the FP64 bundle kernel
+        # only; other groups given it run their default variant
+        paired = g["kernel_name"] == "bundles"
+        want_v = variant if variant != 3 or paired else (1 if g["kernel_name"] == "separable_kerr" else 0)
+        assert g["variant"] == want_v and g["refill_min"] == refill_min and g["tuned"] == 0
+        assert g["rays_per_warp"] == (16 if want_v == 3 else 32)
     b.launch()
     b.launch()  # the graph resets its queues: a second launch is a full trace again
+    for d, out in zip(descs, b.outs):
+        assert_same(to_np(out), single(renderer, d))
+    b.close()
+
+
+def test_autotuned_bundle_batch_tunes_rays_per_warp(renderer):
+    """A bundle group's autotuner also times the two-lanes-per-ray variant
+    (16 rays per warp): 4 variants x 4 thresholds; results bit-identical to
+    kt_trace whichever wins."""
+    descs = [abi.frame_desc(chart=1, bundles=1, a=0.998, theta_deg=60.0, width=96, height=54),
+             abi.frame_desc(chart=1, bundles=1, a=0.9, theta_deg=75.0, width=64, height=40)]
+    b = renderer.batch(descs, options=abi.batch_options(autotune=True, tune_fraction=0.5))
+    (g,) = b.groups()
+    assert g["kernel_name"] == "bundles" and g["tuned"] == 1 and g["candidates"] == 16
+    assert g["rays_per_warp"] == (16 if g["variant"] == 3 else 32)
+    b.launch()
     for d, out in zip(descs, b.outs):
         assert_same(to_np(out), single(renderer, d))
     b.close()

@@ -33,8 +33,10 @@ def smooth_gpu(renderer, kw):
 
 
 @pytest.mark.parametrize("kw", [dict(CFG5, width=96, height=96), dict(KNDS, width=96, height=54),
-                                dict(CFG5, width=77, height=31, tol=1e-10)],
-                         ids=["cfg5_ks", "knds_bl", "cfg5_tight"])
+                                dict(CFG5, width=77, height=31, tol=1e-10),
+                                dict(KNDS, integrator=abi.KT_DOPRI5, tol=1e-10, fov_deg=30.0,
+                                     width=96, height=54)],
+                         ids=["cfg5_ks", "knds_bl", "cfg5_tight", "knds_bl_dopri5"])
 def test_smooth_trace_gpu_equals_host(renderer, kw):
     got = smooth_gpu(renderer, kw)
     want, _ = S.smooth(abi.frame_desc(**kw))
@@ -42,8 +44,10 @@ def test_smooth_trace_gpu_equals_host(renderer, kw):
         assert np.array_equal(got[f], want[f]), f
 
 
-@pytest.mark.parametrize("kw", [dict(CFG5, width=64, height=64), dict(KNDS, width=64, height=36)],
-                         ids=["ks", "bl"])
+@pytest.mark.parametrize("kw", [dict(CFG5, width=64, height=64), dict(KNDS, width=64, height=36),
+                                dict(KNDS, integrator=abi.KT_DOPRI5, tol=1e-10, fov_deg=30.0,
+                                     width=64, height=36)],
+                         ids=["ks", "bl", "bl_dopri5"])
 def test_vjp_gpu_equals_host(renderer, kw):
     import torch
 
@@ -104,6 +108,25 @@ def test_config5_l2_gradient_against_central_differences(renderer):
     assert res["five_point"]["pixels"] > 0.3 * res["five_point"]["disk_pixels"]
     assert res["two_point"]["pixels"] > 0.3 * res["two_point"]["disk_pixels"]
     assert res["two_point_loose"]["pixels"] > 0.5 * res["two_point_loose"]["disk_pixels"]
+
+
+def test_config2_dopri5_gradient_against_central_differences(renderer):
+    """The DOPRI5 adjoint (the smooth tracer's dopri5_adaptive, its reverse
+    with the embedded error norm and the controller differentiated): config
+    2's geometry at 320x180, tol 1e-10, L2 loss against a=0.92, theta=86;
+    five-point (h = 1e-4) and two-point (h = 1e-6) central differences on the
+    smooth pixels to 1e-5 relative, the loose mask to 1e-4."""
+    import grad_lib
+
+    res = grad_lib.fd_check(renderer, grad_lib.CFG2_DOPRI5, target=grad_lib.TARGET_CFG2)
+    for name, r in res.items():
+        print(f"{name} h={r['h']:g}: {r['pixels']} of {r['disk_pixels']} disk pixels in the loss")
+        for k, v in r["per_param"].items():
+            print(f"  {k}: adjoint {v['adjoint']:.10g} differences {v['fd']:.10g} rel {v['rel']:.2e}")
+    assert res["five_point"]["worst_rel"] <= 1e-5
+    assert res["two_point"]["worst_rel"] <= 1e-5
+    assert res["two_point_loose"]["worst_rel"] <= 1e-4
+    assert res["five_point"]["pixels"] > 0.3 * res["five_point"]["disk_pixels"]
 
 
 def test_pixel_list_gradients_add_up(renderer):

@@ -69,13 +69,15 @@ def test_pixel_subset_equals_frame(hc):
         assert np.array_equal(G.bits(sub[k]), G.bits(full[k][pix]))
 
 
+@pytest.mark.parametrize("shape", [1, 2], ids=["rolled", "unrolled"])
 @pytest.mark.parametrize("name", [n for n, kw in sorted(G.cases().items()) if kw.get("bundles")])
-def test_bundle_rhs_split_matches_reference(hc, name):
+def test_bundle_rhs_split_matches_reference(hc, name, shape):
     """The bundle RHS split over two lanes (bundle_rhs_half for each lane,
-    bundle_rhs_combine), as the paired bundle kernel evaluates it, traced on
-    the host: bit-identical to the reference's bundle fixtures."""
+    in either code shape, and bundle_rhs_combine), as the paired bundle
+    kernel evaluates it, traced on the host: bit-identical to the
+    reference's bundle fixtures."""
     hc.hc_set_bundle_split.argtypes = [ctypes.c_int]
-    hc.hc_set_bundle_split(1)
+    hc.hc_set_bundle_split(shape)
     try:
         got = run(hc, G.desc(name))
     finally:

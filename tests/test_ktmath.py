@@ -120,17 +120,3 @@ def test_div3_is_the_ieee_quotient(L):
         ref = x / 3.0
     same = (q.view(np.uint64) == ref.view(np.uint64)) | (np.isnan(q) & np.isnan(ref))
     assert same.all(), x[~same][:5]
-
-
-@pytest.mark.parametrize("mode,n", [(0, 200_000_000), (1, 200_000_000)],
-                         ids=["exponents_-300_300", "renderer_range"])
-def test_div_rcp_is_the_ieee_quotient(L, mode, n):
-    """ktm_div_rcp(a, b, RN(1/b)) -- two Markstein corrections of a * RN(1/b),
-    the inverse metric's quotients over a shared denominator -- returns the
-    bits of a / b on 2e8 pseudo-random pairs with exponents over
-    [-300, 300) (signs, zeros and powers of two mixed in; arguments outside
-    the guarded range take the division) and on 2e8 over the renderer's
-    range [2^-40, 2^60)."""
-    L.kts_div_rcp_check.restype = ctypes.c_long
-    L.kts_div_rcp_check.argtypes = [ctypes.c_uint64, ctypes.c_long, ctypes.c_int]
-    assert L.kts_div_rcp_check(0x9E3779B97F4A7C15 + mode, n, mode) == 0

@@ -23,8 +23,10 @@ PARAMS = ["a", "Q", "Lambda", "theta_deg", "r_obs"]
 
 
 @pytest.mark.parametrize("kw", [dict(CFG5, width=96, height=96), dict(KNDS, width=96, height=54),
-                                dict(chart=0, a=0.5, fov_deg=45.0, width=160, height=90)],
-                         ids=["cfg5_ks", "knds_bl", "cfg1_ks"])
+                                dict(chart=0, a=0.5, fov_deg=45.0, width=160, height=90),
+                                dict(KNDS, integrator=abi.KT_DOPRI5, tol=1e-10, fov_deg=30.0,
+                                     width=96, height=54)],
+                         ids=["cfg5_ks", "knds_bl", "cfg1_ks", "cfg2_bl_dopri5"])
 def test_smooth_tracer_close_to_reference_path(kw):
     """The smooth tracer changes three numerical details of the reference's
     algorithm; the images agree to the reference's own discretisation
@@ -78,7 +80,8 @@ def smooth_pixels(base, names, h, pix=None):
 @pytest.mark.parametrize("frame,names", [
     (dict(CFG5, width=64, height=64, tol=1e-10), ["a", "Q", "theta_deg", "r_obs"]),
     (dict(KNDS, width=64, height=36, tol=1e-10), PARAMS),
-], ids=["ks", "bl_lambda"])
+    (dict(KNDS, integrator=abi.KT_DOPRI5, tol=1e-10, fov_deg=30.0, width=64, height=36), PARAMS),
+], ids=["ks", "bl_lambda", "bl_dopri5"])
 def test_per_ray_gradients_match_central_differences(frame, names):
     """d g / d theta and d r_hit / d theta of single rays from the adjoint
     (unit cotangents) against central differences with h = 1e-4."""
@@ -182,13 +185,19 @@ def test_smooth_frames_rejected_where_unsupported(L=None):
     lib = kt.load_library()
     out = abi.FrameDerived()
     for kw, st in [(dict(bundles=1), abi.KT_ERR_UNSUPPORTED),
-                   (dict(chart=1, integrator=1), abi.KT_ERR_UNSUPPORTED),
                    (dict(precision=3), abi.KT_ERR_INVALID_ARGUMENT)]:
         d = abi.frame_desc(width=4, height=4, **dict(dict(precision=abi.KT_PREC_SMOOTH), **kw))
         assert lib.kt_frame_derive(ctypes.byref(d), ctypes.byref(out)) == st
-    # the KS chart ignores --dopri5, as the reference does
-    d = abi.frame_desc(width=4, height=4, chart=0, integrator=1, precision=abi.KT_PREC_SMOOTH)
-    assert lib.kt_frame_derive(ctypes.byref(d), ctypes.byref(out)) == abi.KT_OK
+    # DOPRI5 in the BL chart (and KS + Lambda, which runs in BL); the KS
+    # chart ignores --dopri5, as the reference does
+    for kw in (dict(chart=1, integrator=1), dict(chart=0, integrator=1, Lambda=1e-4),
+               dict(chart=0, integrator=1)):
+        d = abi.frame_desc(width=4, height=4, precision=abi.KT_PREC_SMOOTH, **kw)
+        assert lib.kt_frame_derive(ctypes.byref(d), ctypes.byref(out)) == abi.KT_OK
+    # the forward-mode tangent is RK4 only
+    with pytest.raises(ValueError):
+        S.smooth(abi.frame_desc(chart=1, integrator=1, width=4, height=4), mode=1,
+                 cot_g=np.ones(16), cot_r=np.zeros(16), tangent=0)
 
 
 @pytest.mark.parametrize("frame,dirs", [(dict(KNDS, width=48, height=27), [0, 1, 2, 3, 4]),
