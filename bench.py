@@ -42,6 +42,12 @@ WORKLOADS = {
     # config 3's geometry at a quarter and at half the resolution (profiling sizes)
     "bundles_bl_480x270": dict(chart=1, bundles=1, a=0.998, theta_deg=60.0, width=480, height=270),
     "bundles_bl_960x540": dict(chart=1, bundles=1, a=0.998, theta_deg=60.0, width=960, height=540),
+    # configuration 2's geometry in mixed precision at tol 1e-8, where the FP32
+    # right-hand side runs (profiling size)
+    "knds_bl_dopri5_mixed_tol1e-8_640x360": dict(chart=1, integrator=1, tol=1e-8, a=0.9, Q=0.3,
+                                                 Lambda=1e-4, r_obs=60.0, theta_deg=85.0,
+                                                 fov_deg=30.0, disk_out=20.0, width=640,
+                                                 height=360, precision=1),
     "kn_ks_rk4_512": dict(chart=0, a=0.7, Q=0.1, theta_deg=70.0, r_obs=50.0, disk_out=15.0,
                           width=512, height=512),
     # 64 seeded parameter sets (kerrtracecpp2_b200.random_parameter_sets, seed
@@ -148,8 +154,9 @@ def weighted(counts, w):
 def ray_flops(desc, steps, attempts, w=UNIT_WEIGHTS):
     """Algorithmic FP64 flops of one traced frame from the kernel's counters,
     with operation weights w (flops per division, x/3, sqrt, sincos, pow)."""
-    if desc.bundles or desc.chart == 0 and abs(desc.Lambda) <= 1e-15 or desc.solver_mode != 0:
-        return None  # counted only for the standard BL single-ray integrators
+    if (desc.bundles or desc.chart == 0 and abs(desc.Lambda) <= 1e-15 or desc.solver_mode != 0
+            or desc.precision != 0):
+        return None  # counted only for the standard BL single-ray integrators in FP64
     n = desc.width * desc.height
     f_rhs = weighted(RHS_COUNTS, w)
     if desc.integrator == 1:
@@ -1076,7 +1083,8 @@ def main():
     # contraction and with the renderer's libm on every golden fixture),
     # over the whole frame (Jacobi bundles: every 16th pixel).
     parity = None
-    if rank == 0 and world == 1 and not args.no_parity and wl.get("solver_mode", 0) != 1:
+    if (rank == 0 and world == 1 and not args.no_parity and wl.get("solver_mode", 0) != 1
+            and desc.precision == 0):
         import oracle_lib as O  # noqa: E402  (tests/oracle_lib.py)
 
         stride = 16 if desc.bundles else 1
@@ -1097,7 +1105,8 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (procedural camera frame; no dataset)", "config": base_cfg,
-            "mode": "plain FP64, bit-identical to the reference CPU path",
+            "mode": "plain FP64, bit-identical to the reference CPU path" if desc.precision == 0
+            else ["plain FP64", "mixed precision", "smooth tracer"][desc.precision],
             "roofline": roofline, "cpu_baseline": cpu, "parity_vs_strict": parity,
             "mixed_precision": mixed, "mixed_precision_fp32_tol1e-8": mixed_fp32,
             "mixed_batched": mixed_batched, "adjoint": adjoint, "adjoint_dopri5_720p": adjoint_dopri5,

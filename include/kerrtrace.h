@@ -72,8 +72,11 @@ enum { KT_SOLVER_STANDARD = 0, KT_SOLVER_SEMI_ANALYTIC = 1, KT_SOLVER_ELLIPTIC_C
  * (FP64; the Jacobi map and its determinant FP64).
  * SMOOTH: the differentiable tracer (kt_vjp, kt_l2_grad): FP64, analytic
  * Hamiltonian gradient, analytic BL->KS Jacobian, disk crossing solved to
- * convergence, RK4 step doubling only; its outputs are smooth functions of
- * the frame parameters between changes of the accept/reject pattern. */
+ * convergence, error estimate formed from the stages; RK4 step doubling, or
+ * DOPRI5 for frames traced in the BL chart (a KS-chart frame integrates
+ * with RK4, as the reference's KS tracer does); no bundles.  Its outputs
+ * are smooth functions of the frame parameters between changes of the
+ * accept/reject pattern. */
 enum { KT_PREC_FP64 = 0, KT_PREC_MIXED = 1, KT_PREC_SMOOTH = 2 };
 /* kt_frame_desc.flags: theta_deg, phi_deg and fov_deg hold radians (the
  * reference's CameraParams_CUDA carries radians, gpu/cuda/tracer.cuh:16-20). */
@@ -341,7 +344,7 @@ enum {
 };
 /* Point-sampled pixels: g and r_hit of a disk pixel do not depend on the
  * disk's outer radius (it only decides which rays hit), so the
- * KT_GRAD_DISK_OUT entry is 0.  In the KS chart (Lambda = 0 only; any other
+ * KT_GRAD_DISK_OUT entry is 0 by construction.  In the KS chart (Lambda = 0 only; any other
  * Lambda sends the frame to the BL chart, main.cpp:2033-2040) the Lambda
  * entry is the derivative of the BL-chart trace of the same frame, which
  * is what the tracer computes for Lambda != 0; it takes a second pass
