@@ -143,45 +143,6 @@ struct ModeBundleMixed {
   }
 };
 
-// Mixed bundles with two lanes per ray (k_trace_pair): lane 2i+c evaluates
-// the analytic gradient along column c of W (bundle_rhs_analytic_col, one
-// Dual<1> each instead of one Dual<2>), the columns are swapped with one
-// shuffle each, and the even lane runs the machine.
-struct ModeBundleMixedPair {
-  using Machine = Bundle;
-  static constexpr int kSlots = Bundle::kSlots;
-  Bundle* m;
-  __device__ __forceinline__ bool needs_k1() const { return m->needs_k1(); }
-  __device__ __forceinline__ bool start(const Frame& f, uint32_t pix, uint32_t, uint32_t, const Fallback&) {
-    m->init(f, (int)(pix % (uint32_t)f.cam.W), (int)(pix / (uint32_t)f.cam.W));
-    return true;
-  }
-  __device__ __forceinline__ bool slot(const Frame& f, int s, RayResult* res, bool odd,
-                                       unsigned pmask) {
-    double y[4], yW[8], k[5], kW[8], mine[4];
-    m->input(s, y, yW);
-    bundle_rhs_analytic_col(f.g, y, m->pt, m->pphi, yW, odd ? 1 : 0, k, mine);
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const double other = __shfl_xor_sync(pmask, mine[i], 1);
-      kW[2 * i] = mine[i];      // the even lane's view: column 0 its own,
-      kW[2 * i + 1] = other;    // column 1 its partner's
-    }
-    __syncwarp(pmask);  // both lanes have read the record
-    int done = 0;
-    if (!odd) done = m->consume(f, s, k, kW, res) ? 1 : 0;
-    __syncwarp(pmask);  // the even lane's updates are visible to the odd lane
-    return __shfl_sync(pmask, done, (int)((threadIdx.x & 31u) & ~1u)) != 0;
-  }
-};
-
-#ifndef KT_BUNDLE_MIXED_PAIR_MINB
-#define KT_BUNDLE_MIXED_PAIR_MINB 3
-#endif
-template <> struct Shape<ModeBundleMixedPair> {
-  static constexpr int kBlock = 128, kMinBlocks = KT_BUNDLE_MIXED_PAIR_MINB, kRefill = 8;
-};
-
 // Launch shapes, measured on B200 as for the exact kernels: refilling a
 // warp only when all 32 lanes are idle matters more here, since the FP32/FP64
 // choice is made per warp and a warp of neighbouring rays that started
@@ -208,7 +169,7 @@ cudaError_t launch_shape_mixed(Mode mode, int device, LaunchShape* shape) {
     case kModeBLRk4Mixed: return shape_for<ModeBLRk4MixedT<true>>(device, shape);
     case kModeBLDopri5Mixed: return shape_for<ModeBLDopri5MixedT<true>>(device, shape);
     case kModeKSRk4Mixed: return shape_for<ModeKSRk4MixedT<true>>(device, shape);
-    case kModeBundleMixed: return shape_for_pair<ModeBundleMixedPair>(device, shape);
+    case kModeBundleMixed: return shape_for<ModeBundleMixed>(device, shape);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -227,9 +188,7 @@ cudaError_t launch_trace_mixed(Mode mode, const Frame& f, const OutSoA& out, con
     case kModeKSRk4Mixed:
       return fp32 ? launch_one<ModeKSRk4MixedT<true>>(f, out, rl, queue, fb, s, stream)
                   : launch_one<ModeKSRk4MixedT<false>>(f, out, rl, queue, fb, s, stream);
-    case kModeBundleMixed:
-      k_trace_pair<ModeBundleMixedPair><<<s.grid, s.block, s.smem, stream>>>(f, out, rl, queue, fb);
-      return cudaGetLastError();
+    case kModeBundleMixed: return launch_one<ModeBundleMixed>(f, out, rl, queue, fb, s, stream);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -338,35 +338,6 @@ KT_HD void bundle_rhs_analytic(const Metric& g, const double y[4], double pt, do
   }
 }
 
-// bundle_rhs_analytic along one column of W (col 0 or 1): the same gradient
-// of H in Dual<1> (values k, tangents Hess(H) W[:, col]) -- the mixed bundle
-// kernel with two lanes per ray, one column each.
-KT_HD void bundle_rhs_analytic_col(const Metric& g, const double y[4], double pt, double pphi,
-                                   const double W[8], int col, double k[5], double dWc[4]) {
-  typedef Dual<1> D;
-  SmPrm<D> P;
-  P.a = D(g.a);
-  P.Q = D(g.Q);
-  P.L = D(g.L);
-  D yd[4], cd[2], gy[4], gc[2], gp[3];
-  for (int i = 0; i < 4; ++i) {
-    yd[i] = D(y[i]);
-    yd[i].d[0] = W[2 * i + col];
-  }
-  cd[0] = D(pt);
-  cd[1] = D(pphi);
-  ChartBL::grad<D, false, true>(g.M, P, yd, cd, gy, gc, gp);
-  k[0] = gy[2].v;
-  k[1] = gy[3].v;
-  k[2] = -gy[0].v;
-  k[3] = -gy[1].v;
-  k[4] = gc[1].v;
-  dWc[0] = gy[2].d[0];
-  dWc[1] = gy[3].d[0];
-  dWc[2] = -gy[0].d[0];
-  dWc[3] = -gy[1].d[0];
-}
-
 // --------------------------------------------------------------- camera
 // camera.hpp:50-145: the BL photon of pixel angles (alpha, beta) for an
 // observer at (r_obs, theta_obs, phi_obs), in T.  y = (r, theta, pr, ptheta),

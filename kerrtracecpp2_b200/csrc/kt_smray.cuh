@@ -189,23 +189,34 @@ KT_HD int sm_attempt(double M, const SmPrm<double>& P, double tol, const double*
 // theta, p_r, p_theta only).  The stage records are u[s] (s = 1..6, u[6] =
 // y5) and k[s] (s = 0..6).
 
-// a_{s j}: stage s = 1..5 (the inputs of k2..k6), s = 6: b5 (y5)
-KT_HD double dp5_a(int s, int j) {
-  const double A[6][6] = {
-      {1.0 / 5.0, 0.0, 0.0, 0.0, 0.0, 0.0},
-      {3.0 / 40.0, 9.0 / 40.0, 0.0, 0.0, 0.0, 0.0},
-      {44.0 / 45.0, -56.0 / 15.0, 32.0 / 9.0, 0.0, 0.0, 0.0},
-      {19372.0 / 6561.0, -25360.0 / 2187.0, 64448.0 / 6561.0, -212.0 / 729.0, 0.0, 0.0},
-      {9017.0 / 3168.0, -355.0 / 33.0, 46732.0 / 5247.0, 49.0 / 176.0, -5103.0 / 18656.0, 0.0},
-      {35.0 / 384.0, 0.0, 500.0 / 1113.0, 125.0 / 192.0, -2187.0 / 6784.0, 11.0 / 84.0}};
-  return A[s - 1][j];
+// The tableau: a_{s j} for stage s = 1..5 (the inputs of k2..k6) and s = 6
+// (b5, the result y5), row-major 6 x 6, then b5_j - b4_j for j = 0..6 (the
+// exact rationals, each rounded once).  In constant memory on the device (the
+// stage loops are rolled, and all lanes read the same entry).
+#define KT_DP5_TABLEAU                                                                      \
+  {1.0 / 5.0, 0.0, 0.0, 0.0, 0.0, 0.0,                                                       \
+   3.0 / 40.0, 9.0 / 40.0, 0.0, 0.0, 0.0, 0.0,                                               \
+   44.0 / 45.0, -56.0 / 15.0, 32.0 / 9.0, 0.0, 0.0, 0.0,                                     \
+   19372.0 / 6561.0, -25360.0 / 2187.0, 64448.0 / 6561.0, -212.0 / 729.0, 0.0, 0.0,          \
+   9017.0 / 3168.0, -355.0 / 33.0, 46732.0 / 5247.0, 49.0 / 176.0, -5103.0 / 18656.0, 0.0,   \
+   35.0 / 384.0, 0.0, 500.0 / 1113.0, 125.0 / 192.0, -2187.0 / 6784.0, 11.0 / 84.0,          \
+   71.0 / 57600.0, 0.0, -71.0 / 16695.0, 71.0 / 1920.0, -17253.0 / 339200.0, 22.0 / 525.0,   \
+   -1.0 / 40.0}
+#if defined(__CUDACC__)
+static __constant__ double kDp5TabDev[43] = KT_DP5_TABLEAU;
+#endif
+static const double kDp5TabHost[43] = KT_DP5_TABLEAU;
+#undef KT_DP5_TABLEAU
+
+KT_HD double dp5_tab(int i) {
+#if defined(__CUDA_ARCH__)
+  return kDp5TabDev[i];
+#else
+  return kDp5TabHost[i];
+#endif
 }
-// b5_j - b4_j, j = 0..6 (the exact rationals, each rounded once)
-KT_HD double dp5_e(int j) {
-  const double E[7] = {71.0 / 57600.0, 0.0, -71.0 / 16695.0, 71.0 / 1920.0, -17253.0 / 339200.0,
-                       22.0 / 525.0, -1.0 / 40.0};
-  return E[j];
-}
+KT_HD double dp5_a(int s, int j) { return dp5_tab((s - 1) * 6 + j); }
+KT_HD double dp5_e(int j) { return dp5_tab(36 + j); }
 
 template <class C>
 KT_HD_CALL void sm_dp_paths(double M, const SmPrm<double>& P, const double* c, const double* y,
