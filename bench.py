@@ -310,12 +310,13 @@ def batch_leg(R, stream, flush, seed=1, frames=64):
             "mode": "plain FP64, bit-identical to the reference CPU path"}
 
 
-def adjoint_leg(R, steps, warmup, stream, flush, frame=None, target=None, fd_check=True):
+def adjoint_leg(R, steps, warmup, stream, flush, frame=None, target=None, fd_check=True, w_m=0.0):
     """Config 5 (default): 512x512 KS frame, L2 loss of (g, r_hit) against
     the smooth tracer at a=0.72, theta=71; kt_l2_grad (fused forward +
     reverse per ray) timed on the device against kt_trace of the same frame
     (plain FP64, the reference's arithmetic) and the smooth forward alone.
-    `frame` / `target` give another frame and the target's parameters."""
+    `frame` / `target` give another frame and the target's parameters; w_m
+    adds a bundle frame's magnification to the loss."""
     import torch
     from kerrtracecpp2_b200 import abi
 
@@ -346,16 +347,18 @@ def adjoint_leg(R, steps, warmup, stream, flush, frame=None, target=None, fd_che
     res = {}
 
     def grad():
-        res["r"] = R.l2_grad(d, tgt, 1.0, 0.01, out=out, stream=stream)
+        res["r"] = R.l2_grad(d, tgt, 1.0, 0.01, out=out, stream=stream, w_m=w_m)
 
     grad_ms = timed(grad)
     loss, g, st = res["r"]
-    desc_txt = {k: frame[k] for k in ("width", "height", "chart", "a", "Q", "Lambda", "theta_deg",
-                                      "r_obs", "disk_out") if k in frame}
-    desc_txt["integrator"] = "DOPRI5" if frame.get("integrator", 0) == 1 else "RK4-doubling"
+    desc_txt = {k: frame[k] for k in ("width", "height", "chart", "bundles", "a", "Q", "Lambda",
+                                      "theta_deg", "r_obs", "disk_out") if k in frame}
+    desc_txt["integrator"] = ("DOPRI5" if frame.get("integrator", 0) == 1 and not frame.get("bundles")
+                              else "RK4-doubling")
     desc_txt["tol"] = frame.get("tol", 1e-7)
+    mterm = f" + {w_m:g} (magnif-magnif_t)^2" if w_m else ""
     leg = {"frame": desc_txt,
-           "loss": "sum over pixels that are disk hits in both frames of (g-g_t)^2 + 0.01 (r-r_t)^2, "
+           "loss": f"sum over pixels that are disk hits in both frames of (g-g_t)^2 + 0.01 (r-r_t)^2{mterm}, "
                    f"target: the same tracer at {target}",
            "ms_per_frame": grad_ms, "ms_main_pass": st["ms_main"], "ms_lambda_pass": st["ms_lambda"],
            "forward_fp64_ms": fwd_ms, "forward_smooth_ms": smooth_ms,
@@ -994,7 +997,7 @@ def main():
         b.close()
         del b
 
-    adjoint = adjoint_dopri5 = None
+    adjoint = adjoint_dopri5 = adjoint_bundle = None
     if not args.no_adjoint:
         adjoint = adjoint_leg(R, args.steps, args.warmup, stream, flush)
         if args.workload == "knds_bl_dopri5_720p":
@@ -1002,6 +1005,13 @@ def main():
             adjoint_dopri5 = adjoint_leg(R, min(args.steps, LEG_STEPS), 1, stream, flush,
                                          frame=WORKLOADS["knds_bl_dopri5_720p"],
                                          target=dict(a=0.92, theta_deg=86.0), fd_check=False)
+            if not args.no_legs:
+                # the bundle adjoint, magnification in the loss (configuration
+                # 3's geometry at 960x540)
+                adjoint_bundle = adjoint_leg(R, min(args.steps, LEG_STEPS), 1, stream, flush,
+                                             frame=WORKLOADS["bundles_bl_960x540"],
+                                             target=dict(a=0.99, theta_deg=61.0), fd_check=False,
+                                             w_m=0.01)
 
     # Configs 3 and 4 as legs of the default line (one GPU).
     bundles = batch64 = None
@@ -1110,6 +1120,7 @@ def main():
             "roofline": roofline, "cpu_baseline": cpu, "parity_vs_strict": parity,
             "mixed_precision": mixed, "mixed_precision_fp32_tol1e-8": mixed_fp32,
             "mixed_batched": mixed_batched, "adjoint": adjoint, "adjoint_dopri5_720p": adjoint_dopri5,
+            "adjoint_bundles_960x540": adjoint_bundle,
             "bundles_1080p": bundles, "batch64": batch64,
             "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": ctypes.sizeof(desc),
                     "d2h_bytes_per_step": d2h, "call": "kt_trace_host"},

@@ -74,7 +74,8 @@ enum { KT_SOLVER_STANDARD = 0, KT_SOLVER_SEMI_ANALYTIC = 1, KT_SOLVER_ELLIPTIC_C
  * Hamiltonian gradient, analytic BL->KS Jacobian, disk crossing solved to
  * convergence, error estimate formed from the stages; RK4 step doubling, or
  * DOPRI5 for frames traced in the BL chart (a KS-chart frame integrates
- * with RK4, as the reference's KS tracer does); no bundles.  Its outputs
+ * with RK4, as the reference's KS tracer does); bundles with the analytic
+ * Hessian, RK4 step doubling as the reference's bundle tracer.  Its outputs
  * are smooth functions of the frame parameters between changes of the
  * accept/reject pattern. */
 enum { KT_PREC_FP64 = 0, KT_PREC_MIXED = 1, KT_PREC_SMOOTH = 2 };
@@ -390,6 +391,24 @@ kt_status kt_vjp_pixels(kt_context* ctx, const kt_frame_desc* desc, const uint32
 kt_status kt_l2_grad_pixels(kt_context* ctx, const kt_frame_desc* desc, const uint32_t* pix_dev,
                             int64_t n_pix, const kt_geo_soa* target, double w_g, double w_r,
                             const kt_geo_soa* out, uint32_t flags, double* loss,
+                            double grad[KT_GRAD_COUNT], kt_grad_stats* stats, void* stream);
+
+/* The same with the Jacobi bundle's magnification (GeoPixel::magnif of a
+ * bundle frame, ray_bundle.hpp:386-392; the renderer scales a disk pixel's
+ * intensity by clamp(1/magnif, 0.05, 5), main.cpp:1789): kt_vjp_magnif adds
+ * cot_magnif[p] d magnif_p / d theta_k (device array over the frame, or
+ * NULL), kt_l2_grad_magnif adds w_m (magnif - magnif_t)^2 to the loss
+ * (target->magnif must then be set).  pix_dev / n_pix as kt_vjp_pixels
+ * (NULL, 0: every pixel).  On a frame without bundles the magnification is
+ * the constant 1 and these equal kt_vjp_pixels / kt_l2_grad_pixels.  Not in
+ * the reference (which has no gradients). */
+kt_status kt_vjp_magnif(kt_context* ctx, const kt_frame_desc* desc, const uint32_t* pix_dev,
+                        int64_t n_pix, const double* cot_redshift, const double* cot_r,
+                        const double* cot_magnif, const kt_geo_soa* out, uint32_t flags,
+                        double grad[KT_GRAD_COUNT], kt_grad_stats* stats, void* stream);
+kt_status kt_l2_grad_magnif(kt_context* ctx, const kt_frame_desc* desc, const uint32_t* pix_dev,
+                            int64_t n_pix, const kt_geo_soa* target, double w_g, double w_r,
+                            double w_m, const kt_geo_soa* out, uint32_t flags, double* loss,
                             double grad[KT_GRAD_COUNT], kt_grad_stats* stats, void* stream);
 
 /* Measured FP64 FMA throughput of the context's device (GFLOP/s, 2 flops

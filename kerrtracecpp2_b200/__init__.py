@@ -126,6 +126,12 @@ def load_library():
     L.kt_l2_grad_pixels.argtypes = [P, PD, P, ctypes.c_int64, ctypes.POINTER(GeoSoA), D, D,
                                     ctypes.POINTER(GeoSoA), ctypes.c_uint32, PDB, PDB, PG, P]
     L.kt_l2_grad_pixels.restype = ctypes.c_int
+    L.kt_vjp_magnif.argtypes = [P, PD, P, ctypes.c_int64, P, P, P, ctypes.POINTER(GeoSoA),
+                                ctypes.c_uint32, PDB, PG, P]
+    L.kt_vjp_magnif.restype = ctypes.c_int
+    L.kt_l2_grad_magnif.argtypes = [P, PD, P, ctypes.c_int64, ctypes.POINTER(GeoSoA), D, D, D,
+                                    ctypes.POINTER(GeoSoA), ctypes.c_uint32, PDB, PDB, PG, P]
+    L.kt_l2_grad_magnif.restype = ctypes.c_int
     if L.kt_abi_version() != abi.KT_ABI_VERSION:
         raise ImportError("libkerrtrace.so ABI version mismatch")
     _lib = L
@@ -304,34 +310,39 @@ class Renderer:
         _check(self.L.kt_measure_op_costs(self.ctx, ctypes.byref(v)), "kt_measure_op_costs", self.ctx)
         return {f: getattr(v, f) for f, _ in abi.OpCosts._fields_}
 
-    def vjp(self, desc, cot_redshift=None, cot_r=None, out=None, flags=0, stream=None, pix=None):
+    def vjp(self, desc, cot_redshift=None, cot_r=None, out=None, flags=0, stream=None, pix=None,
+            cot_magnif=None):
         """kt_vjp: gradient (numpy, kt_frame_desc units, abi.GRAD_NAMES order)
         of sum(cot_redshift * g + cot_r * r_hit) over the disk pixels of the
         smooth tracer; cotangents are float64 device tensors over the frame.
         With `pix` (an int32 device tensor of pixel indices) only those
-        pixels are traced (kt_vjp_pixels).  Returns (grad, stats dict)."""
+        pixels are traced; `cot_magnif` adds a bundle frame's magnification
+        (kt_vjp_magnif).  Returns (grad, stats dict)."""
         grad = (ctypes.c_double * abi.KT_GRAD_COUNT)()
         st = abi.GradStats()
-        _check(self.L.kt_vjp_pixels(self.ctx, ctypes.byref(desc),
+        _check(self.L.kt_vjp_magnif(self.ctx, ctypes.byref(desc),
                                     _torch_ptr(pix) if pix is not None else None,
                                     int(pix.numel()) if pix is not None else 0,
                                     _torch_ptr(cot_redshift) if cot_redshift is not None else None,
                                     _torch_ptr(cot_r) if cot_r is not None else None,
+                                    _torch_ptr(cot_magnif) if cot_magnif is not None else None,
                                     ctypes.byref(_soa_struct(out, _torch_ptr)) if out is not None else None,
                                     flags, grad, ctypes.byref(st), self._stream(stream)), "kt_vjp", self.ctx)
         return np.array(grad[:]), st.as_dict()
 
-    def l2_grad(self, desc, target, w_g=1.0, w_r=0.0, out=None, flags=0, stream=None, pix=None):
+    def l2_grad(self, desc, target, w_g=1.0, w_r=0.0, out=None, flags=0, stream=None, pix=None,
+                w_m=0.0):
         """kt_l2_grad: (loss, grad, stats) of the L2 loss of (g, r_hit) against
         a target frame (dict of device tensors from a smooth trace); with `pix`,
-        over those pixels only (kt_l2_grad_pixels)."""
+        over those pixels only; w_m weighs a bundle frame's magnification
+        (kt_l2_grad_magnif)."""
         grad = (ctypes.c_double * abi.KT_GRAD_COUNT)()
         loss = ctypes.c_double()
         st = abi.GradStats()
-        _check(self.L.kt_l2_grad_pixels(self.ctx, ctypes.byref(desc),
+        _check(self.L.kt_l2_grad_magnif(self.ctx, ctypes.byref(desc),
                                         _torch_ptr(pix) if pix is not None else None,
                                         int(pix.numel()) if pix is not None else 0,
-                                        ctypes.byref(_soa_struct(target, _torch_ptr)), w_g, w_r,
+                                        ctypes.byref(_soa_struct(target, _torch_ptr)), w_g, w_r, w_m,
                                         ctypes.byref(_soa_struct(out, _torch_ptr)) if out is not None else None,
                                         flags, ctypes.byref(loss), grad, ctypes.byref(st),
                                         self._stream(stream)),

@@ -15,7 +15,9 @@
 // gives one parameter's entry by forward mode (no recording).
 //
 // BL frames integrated with DOPRI5 have their own pair of kernels (the
-// smooth DOPRI5 attempt and its reverse, kt_smray.cuh).
+// smooth DOPRI5 attempt and its reverse, kt_smray.cuh), and so do Jacobi
+// bundles (ChartBLB: the geodesic with its 4x2 Jacobi matrix, ~20 KB of
+// checkpoints per thread).
 //
 // Compiled with --fmad=false: the recorded forward and every replay of it
 // must round identically, which contraction choices made per inlining site
@@ -40,7 +42,7 @@ __global__ void __launch_bounds__(kSmBlock) k_smooth(const Frame f, const OutSoA
                                                      uint32_t* __restrict__ queue,
                                                      uint32_t* __restrict__ fb_pix,
                                                      uint32_t* __restrict__ fb_n) {
-  SmScratch sc;
+  SmScratch<C::kN> sc;
   const uint32_t count = n_dev ? *n_dev : (list ? n_list : n);
   const unsigned lane = threadIdx.x & 31u;
   KT_ROLLED
@@ -177,6 +179,15 @@ cudaError_t launch_smooth(const Frame& f, const OutSoA& out, uint32_t n, const S
   memset(&none, 0, sizeof none);
   const SmJob& jb = job ? *job : none;
   const bool grad = job != nullptr;
+  // Jacobi bundles (BL chart, RK4 step doubling whatever the integrator, as
+  // trace_bundle): no forward-mode tangent (their Lambda comes from the sweep)
+  if (f.bundles) {
+    if (grad && job->tangent_dir >= 0) return cudaErrorInvalidValue;
+    return grad ? smooth_launch<ChartBLB, true>(f, out, n, jb, jb.pix, jb.n_pix, nullptr, counters,
+                                                nullptr, nullptr, device, st)
+                : smooth_launch<ChartBLB, false>(f, out, n, jb, jb.pix, jb.n_pix, nullptr, counters,
+                                                 nullptr, nullptr, device, st);
+  }
   // BL frames with DOPRI5 (KS frames integrate with RK4, their BL passes too)
   const bool dp5 = f.intg == 1 && f.chart == 1;  // KT_DOPRI5, KT_CHART_BL
   if (dp5) {

@@ -180,4 +180,56 @@ KT_HD double sm_abs(double x) { return fabs(x); }
 template <int N>
 KT_HD Dual<N> sm_abs(const Dual<N>& x) { return x.v < 0.0 ? -x : x; }
 
+// Hyper-dual numbers x = v + a e1 + b e2 + c e1 e2 with e1^2 = e2^2 = 0
+// (Fike and Alonso, "The development of hyper-dual numbers for exact
+// second-derivative calculations", AIAA 2011-886): f(x) = f(v) + f'(v) a e1 +
+// f'(v) b e2 + (f'(v) c + f''(v) a b) e1 e2, so evaluating g at x0 + e1 u +
+// e2 w gives g's second directional derivative D^2 g[u, w] in the e1 e2 part.
+// Only the operations of the BL Hamiltonian gradient are defined.  The
+// values follow the primal's operations (comparisons look at v).
+struct HDual {
+  double v, a, b, c;
+  KT_HD HDual() {}
+  KT_HD HDual(double x) : v(x), a(0.0), b(0.0), c(0.0) {}
+  KT_HD HDual(double x, double da, double db, double dc) : v(x), a(da), b(db), c(dc) {}
+};
+KT_HD double val(const HDual& x) { return x.v; }
+KT_HD HDual operator+(const HDual& x, const HDual& y) {
+  return HDual(x.v + y.v, x.a + y.a, x.b + y.b, x.c + y.c);
+}
+KT_HD HDual operator-(const HDual& x, const HDual& y) {
+  return HDual(x.v - y.v, x.a - y.a, x.b - y.b, x.c - y.c);
+}
+KT_HD HDual operator-(const HDual& x) { return HDual(-x.v, -x.a, -x.b, -x.c); }
+KT_HD HDual operator*(const HDual& x, const HDual& y) {
+  return HDual(x.v * y.v, x.a * y.v + x.v * y.a, x.b * y.v + x.v * y.b,
+               x.c * y.v + x.v * y.c + x.a * y.b + x.b * y.a);
+}
+KT_HD HDual operator+(const HDual& x, double y) { return HDual(x.v + y, x.a, x.b, x.c); }
+KT_HD HDual operator+(double x, const HDual& y) { return y + x; }
+KT_HD HDual operator-(const HDual& x, double y) { return HDual(x.v - y, x.a, x.b, x.c); }
+KT_HD HDual operator-(double x, const HDual& y) { return HDual(x - y.v, -y.a, -y.b, -y.c); }
+KT_HD HDual operator*(const HDual& x, double y) { return HDual(x.v * y, x.a * y, x.b * y, x.c * y); }
+KT_HD HDual operator*(double x, const HDual& y) { return y * x; }
+KT_HD HDual operator/(const HDual& x, double y) { return HDual(x.v / y, x.a / y, x.b / y, x.c / y); }
+// x / y: the value x / y.v; f(y) = x / y, f' = -f / y, f'' = -2 f' / y
+KT_HD HDual operator/(double x, const HDual& y) {
+  const double f = x / y.v;
+  const double iy = 1.0 / y.v;
+  const double f1 = -f * iy;
+  const double f2 = -2.0 * f1 * iy;
+  return HDual(f, f1 * y.a, f1 * y.b, f1 * y.c + f2 * y.a * y.b);
+}
+KT_HD bool operator<(const HDual& x, double y) { return x.v < y; }
+KT_HD bool operator>(const HDual& x, double y) { return x.v > y; }
+KT_HD bool operator<=(const HDual& x, double y) { return x.v <= y; }
+KT_HD bool operator>=(const HDual& x, double y) { return x.v >= y; }
+KT_HD void sm_sincos(const HDual& x, HDual* s, HDual* c) {
+  double sv, cv;
+  ktm_sincos(x.v, &sv, &cv);
+  const double ab = x.a * x.b;
+  *s = HDual(sv, cv * x.a, cv * x.b, cv * x.c - sv * ab);
+  *c = HDual(cv, -sv * x.a, -sv * x.b, -sv * x.c - cv * ab);
+}
+
 }  // namespace kt

@@ -236,10 +236,6 @@ kt_status prepare_frame(const kt_frame_desc* d, Frame* f, kt_frame_derived* dv, 
     *err = "precision must be KT_PREC_FP64, KT_PREC_MIXED or KT_PREC_SMOOTH";
     return KT_ERR_INVALID_ARGUMENT;
   }
-  if (d->precision == KT_PREC_SMOOTH && d->bundles) {
-    *err = "the smooth tracer has no ray-bundle mode";
-    return KT_ERR_UNSUPPORTED;
-  }
   if ((d->flags & ~(uint32_t)KT_FLAG_ANGLES_RADIANS) != 0) {
     *err = "unknown bits in flags";
     return KT_ERR_INVALID_ARGUMENT;
@@ -305,12 +301,12 @@ kt_status prepare_frame(const kt_frame_desc* d, Frame* f, kt_frame_derived* dv, 
   fr.r_fp32 = (d->precision == KT_PREC_MIXED && fr.tol >= 1e-8) ? dmax(4.0 * d->M, 2.0 * rh)
                                                                   : ktm_inf();
   fr.turn_frac = 0.05;
-  // Mixed-precision bundles: rays whose step skipped the horizon and escape
-  // tests (near the equator, no crossing found) and that creep onto a
-  // horizon in BL coordinates -- ingoing within 1e-4 r_+ of r_+, or
+  // Mixed-precision and smooth bundles: rays whose step skipped the horizon
+  // and escape tests (near the equator, no crossing found) and that creep
+  // onto a horizon in BL coordinates -- ingoing within 1e-4 r_+ of r_+, or
   // outgoing within 1e-4 r_c of the cosmological horizon -- end as a horizon
   // hit, the record the controller's eventual failure gives them.
-  const bool doom = d->precision == KT_PREC_MIXED && d->bundles;
+  const bool doom = (d->precision == KT_PREC_MIXED || d->precision == KT_PREC_SMOOTH) && d->bundles;
   fr.r_doom = doom ? rh * (1.0 + 1e-4) : -ktm_inf();
   fr.r_cdoom = doom ? host_r_cosmo(fr.g) * (1.0 - 1e-4) : ktm_inf();
   *f = fr;

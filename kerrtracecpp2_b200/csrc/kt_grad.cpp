@@ -1,5 +1,6 @@
-// kt_grad.cpp -- kt_vjp and kt_l2_grad: the discrete adjoint of the smooth
-// tracer behind the C ABI (kernels in kt_adjoint.cu).
+// kt_grad.cpp -- kt_vjp and kt_l2_grad (and their pixel-list and
+// magnification forms): the discrete adjoint of the smooth tracer behind the
+// C ABI (kernels in kt_adjoint.cu).
 #include <cuda_runtime.h>
 #include <string.h>
 
@@ -126,17 +127,26 @@ kt_status grad_run(kt_context* ctx, const kt_frame_desc* desc_in, const uint32_t
 
 extern "C" {
 
-kt_status kt_vjp_pixels(kt_context* ctx, const kt_frame_desc* desc, const uint32_t* pix_dev,
+kt_status kt_vjp_magnif(kt_context* ctx, const kt_frame_desc* desc, const uint32_t* pix_dev,
                         int64_t n_pix, const double* cot_redshift, const double* cot_r,
-                        const kt_geo_soa* out, uint32_t flags, double* grad, kt_grad_stats* stats,
-                        void* stream) {
+                        const double* cot_magnif, const kt_geo_soa* out, uint32_t flags,
+                        double* grad, kt_grad_stats* stats, void* stream) {
   kt::SmCot cot;
   memset(&cot, 0, sizeof cot);
   cot.mode = 1;
   cot.g = cot_redshift;
   cot.r = cot_r;
+  cot.m = cot_magnif;
   return grad_run(ctx, desc, pix_dev, n_pix, cot, out, flags, grad, stats, (cudaStream_t)stream,
                   "kt_vjp");
+}
+
+kt_status kt_vjp_pixels(kt_context* ctx, const kt_frame_desc* desc, const uint32_t* pix_dev,
+                        int64_t n_pix, const double* cot_redshift, const double* cot_r,
+                        const kt_geo_soa* out, uint32_t flags, double* grad, kt_grad_stats* stats,
+                        void* stream) {
+  return kt_vjp_magnif(ctx, desc, pix_dev, n_pix, cot_redshift, cot_r, nullptr, out, flags, grad,
+                       stats, stream);
 }
 
 kt_status kt_vjp(kt_context* ctx, const kt_frame_desc* desc, const double* cot_redshift,
@@ -156,10 +166,19 @@ kt_status kt_l2_grad_pixels(kt_context* ctx, const kt_frame_desc* desc, const ui
                             int64_t n_pix, const kt_geo_soa* target, double w_g, double w_r,
                             const kt_geo_soa* out, uint32_t flags, double* loss, double* grad,
                             kt_grad_stats* stats, void* stream) {
+  return kt_l2_grad_magnif(ctx, desc, pix_dev, n_pix, target, w_g, w_r, 0.0, out, flags, loss, grad,
+                           stats, stream);
+}
+
+kt_status kt_l2_grad_magnif(kt_context* ctx, const kt_frame_desc* desc, const uint32_t* pix_dev,
+                            int64_t n_pix, const kt_geo_soa* target, double w_g, double w_r,
+                            double w_m, const kt_geo_soa* out, uint32_t flags, double* loss,
+                            double* grad, kt_grad_stats* stats, void* stream) {
   if (!ctx) return KT_ERR_INVALID_ARGUMENT;
-  if (!target || !target->outcome || !target->redshift || !target->r || !loss)
+  if (!target || !target->outcome || !target->redshift || !target->r || !loss ||
+      (w_m != 0.0 && !target->magnif))
     return fail(ctx, KT_ERR_INVALID_ARGUMENT, "kt_l2_grad: NULL pointer");
-  if (!kt::finite(w_g) || !kt::finite(w_r))
+  if (!kt::finite(w_g) || !kt::finite(w_r) || !kt::finite(w_m))
     return fail(ctx, KT_ERR_INVALID_ARGUMENT, "kt_l2_grad: non-finite weight");
   kt::SmCot cot;
   memset(&cot, 0, sizeof cot);
@@ -169,6 +188,8 @@ kt_status kt_l2_grad_pixels(kt_context* ctx, const kt_frame_desc* desc, const ui
   cot.t_r = target->r;
   cot.w_g = w_g;
   cot.w_r = w_r;
+  cot.t_m = w_m != 0.0 ? target->magnif : nullptr;
+  cot.w_m = w_m;
   kt_grad_stats st_local;
   kt_grad_stats* sp = stats ? stats : &st_local;
   const kt_status r = grad_run(ctx, desc, pix_dev, n_pix, cot, out, flags, grad, sp, (cudaStream_t)stream,

@@ -105,6 +105,8 @@ struct ChartKS {
   static constexpr int kC = 1;  // constants of motion: p_T
   static constexpr int kEq = 2;  // state index of the equator coordinate (Z)
   static constexpr double kEqTarget = 0.0;
+  static constexpr int kG = 6;            // geodesic components (error norm, events)
+  static constexpr bool kBundle = false;  // no Jacobi matrix in the state
 
   // gy = dH/dy (X, Y, Z, pX, pY, pZ), gc = dH/dp_T, gp = dH/d(a, Q, Lambda)
   // (only with kPrm: the right-hand side needs gy and gc alone).
@@ -198,6 +200,8 @@ struct ChartBL {
   static constexpr int kC = 2;
   static constexpr int kEq = 1;  // theta
   static constexpr double kEqTarget = 1.57079632679489661923;  // M_PI/2 as the reference
+  static constexpr int kG = 4;
+  static constexpr bool kBundle = false;
 
   // x/3 is taken as x * (1/3) (on a Dual, one product per component instead
   // of a division).  kFast (the mixed-precision bundle): reciprocals and
@@ -290,16 +294,68 @@ struct ChartBL {
   KT_HD static T radius(const A&, const T* y) { return y[0]; }
 };
 
-// f = (dH/dp, -dH/dx) and the passenger rate (BL: dphi = dH/dp_phi).
+// ------------------------------------------------------- BL ray bundle
+// The Jacobi bundle of ray_bundle.hpp:117-263 for the smooth tracer: state
+// y = (r, theta, p_r, p_theta, W) with the 4x2 Jacobi matrix W row-major
+// (y[4 + 2 i + k] = W[i][k]), constants (p_t, p_phi), passenger phi.  The
+// geodesic is the BL chart's; dW = J_s Hess(H) W with the analytic Hessian
+// (the reference differences H with steps of 1e-5, whose rounding noise
+// moves the magnification by ~1e-5).  The error norm and the events look at
+// the geodesic (kG = 4 components) only, as bundle_adaptive does.
+struct ChartBLB {
+  static constexpr int kX = 2;
+  static constexpr int kN = 12;
+  static constexpr int kC = 2;
+  static constexpr int kEq = 1;
+  static constexpr double kEqTarget = ChartBL::kEqTarget;
+  static constexpr int kG = 4;
+  static constexpr bool kBundle = true;
+
+  template <class T, class A>
+  KT_HD static T radius(const A&, const T* y) { return y[0]; }
+};
+
+// f = (dH/dp, -dH/dx) and the passenger rate (BL: dphi = dH/dp_phi).  For a
+// bundle, one evaluation of the BL gradient in Dual<2> along W's columns
+// gives the geodesic RHS (the values, bit for bit the BL chart's) and
+// Hess(H) W (the tangents), so dW = J_s Hess(H) W (ray_bundle.hpp:117-156).
 template <class C, class T>
 KT_HD_CALL void sm_rhs(double M, const SmPrm<T>& P, const T* y, const T* c, T* f, T* fpas) {
-  T gy[C::kN], gc[C::kC], gp[kSmPrm];
-  C::template grad<T, false>(M, P, y, c, gy, gc, gp);
-  for (int i = 0; i < C::kX; ++i) {
-    f[i] = gy[C::kX + i];
-    f[C::kX + i] = -gy[i];
+  if constexpr (C::kBundle) {
+    typedef Dual<2> D;
+    SmPrm<D> Pd;
+    Pd.a = D(P.a);
+    Pd.Q = D(P.Q);
+    Pd.L = D(P.L);
+    D yd[4], cd[2], gy[4], gc[2], gp[kSmPrm];
+    for (int i = 0; i < 4; ++i) {
+      yd[i] = D(y[i]);
+      yd[i].d[0] = y[4 + 2 * i];
+      yd[i].d[1] = y[5 + 2 * i];
+    }
+    cd[0] = D(c[0]);
+    cd[1] = D(c[1]);
+    ChartBL::grad<D, false>(M, Pd, yd, cd, gy, gc, gp);
+    f[0] = gy[2].v;
+    f[1] = gy[3].v;
+    f[2] = -gy[0].v;
+    f[3] = -gy[1].v;
+    for (int k = 0; k < 2; ++k) {
+      f[4 + k] = gy[2].d[k];
+      f[6 + k] = gy[3].d[k];
+      f[8 + k] = -gy[0].d[k];
+      f[10 + k] = -gy[1].d[k];
+    }
+    if (fpas) *fpas = gc[1].v;
+  } else {
+    T gy[C::kN], gc[C::kC], gp[kSmPrm];
+    C::template grad<T, false>(M, P, y, c, gy, gc, gp);
+    for (int i = 0; i < C::kX; ++i) {
+      f[i] = gy[C::kX + i];
+      f[C::kX + i] = -gy[i];
+    }
+    if (fpas) *fpas = (C::kC > 1) ? gc[C::kC - 1] : T(0.0);
   }
-  if (fpas) *fpas = (C::kC > 1) ? gc[C::kC - 1] : T(0.0);
 }
 
 // Bundle RHS (bundle_rhs, ray_bundle.hpp:130-156) from one evaluation of
@@ -468,6 +524,43 @@ KT_HD bool sm_redshift(double M, const SmPrm<T>& P, const T& r, const T& pt, con
   *red = sm_sqrt(d2) / dv;
   if (!finite(val(*red))) {
     *red = T(1.0);
+    return false;
+  }
+  return true;
+}
+
+// The bundle's own redshift (ray_bundle.hpp:360-371): sqrt(d2) / (1 - Omega b)
+// where d2 > 0 and |1 - Omega b| > 1e-10, else 1, clamped to [0, 20].
+// Returns false where that is a constant (no derivative).
+template <class T>
+KT_HD bool sm_redshift_bundle(double M, const SmPrm<T>& P, const T& r, const T& pt, const T& pph,
+                              T* red) {
+  const double s = (val(P.a) < 0.0) ? 1.0 : -1.0;
+  const T Meff = M - P.Q * P.Q / (2.0 * r) + P.L * P.a * r * r / 3.0;
+  const T sq = Meff > 0.0 ? sm_sqrt(Meff) : T(0.0);
+  const T den = r * sm_sqrt(r) + s * P.a * sq;
+  const T Om = (sm_abs(den) < 1e-14) ? T(0.0) : s * sq / den;
+  const T b = (-pph) / (-pt);
+  SmBL<T> G;
+  const T one(1.0), zero(0.0);
+  sm_bl_metric<T>(M, P, r, one, zero, &G, (SmBL<T>*)nullptr);
+  const T d2 = -(G.tt + 2.0 * G.tp * Om + G.pp * Om * Om);
+  const T dv = 1.0 - Om * b;
+  if (!(d2 > 0.0 && fabs(val(dv)) > 1e-10)) {
+    *red = T(1.0);
+    return false;
+  }
+  *red = sm_sqrt(d2) / dv;
+  if (!finite(val(*red))) {
+    *red = T(1.0);
+    return false;
+  }
+  if (*red < 0.0) {
+    *red = T(0.0);
+    return false;
+  }
+  if (*red > 20.0) {
+    *red = T(20.0);
     return false;
   }
   return true;

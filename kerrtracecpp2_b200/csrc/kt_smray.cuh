@@ -42,28 +42,33 @@ namespace kt {
 
 constexpr int kSmCkSteps = 32;  // accepted steps between checkpoints
 constexpr int kSmCkCap = 64;    // checkpoints per level
-constexpr int kSmMaxN = 6;
 constexpr int kSmMaxDoublings = 6;  // k up to 32 * 2^6: 131072 accepted steps
 
+// The per-ray records below are sized by the chart's state size N (4 for
+// BL, 6 for KS, 12 for a BL ray bundle).
+template <int N>
 struct SmCk {  // state at the start of an accepted step and dlam before its attempts
-  double y[kSmMaxN];
+  double y[N];
   double h;
 };
 
+template <int N>
 struct SmSt {  // state at the start of an accepted step, dlam before its attempts, attempts
-  double y[kSmMaxN];
+  double y[N];
   double H;
   int na;
 };
 
 // Data of the final (event) step kept for the adjoint.
+template <int N>
 struct SmEvent {
-  double yp[kSmMaxN];  // y_{N-1}
-  double y[kSmMaxN];   // y_N
-  double H;            // dlam before the attempts of step N-1
-  double h;            // accepted step size of step N-1
+  double yp[N];  // y_{N-1}
+  double y[N];   // y_N
+  double H;      // dlam before the attempts of step N-1
+  double h;      // accepted step size of step N-1
   double alpha;
-  int deriv;           // 1: redshift has a derivative (not a constant or clamped)
+  int deriv;     // 1: redshift has a derivative (not a constant or clamped)
+  int mderiv;    // 1: the bundle's magnification has a derivative (not clamped)
 };
 
 // Stages of one adaptive attempt from y with step h, t = 0..9: path A =
@@ -73,9 +78,10 @@ struct SmEvent {
 // base + h/2 k2, base + h k3; result base + h/6 (k1 + 2 k2 + 2 k3 + k4)
 // (rk4_step_ks, main.cpp:1456-1486).  One rolled loop, one RHS call site: the
 // kernel's code stays small enough for the instruction cache.
+template <int N>
 struct SmStages {
-  double u[10][kSmMaxN];  // stage inputs
-  double k[10][kSmMaxN];  // f(u)
+  double u[10][N];  // stage inputs
+  double k[10][N];  // f(u)
 };
 
 KT_HD void sm_stage_of(int t, int* sub, int* s) {
@@ -93,7 +99,7 @@ KT_HD void sm_stage_of(int t, int* sub, int* s) {
 template <class C>
 KT_HD_CALL void sm_paths(double M, const SmPrm<double>& P, const double* c, const double* y, double pas,
                          const double* k1, double k1p, double hh, double* yA, double* yB, double* pB,
-                         double* dAB, SmStages* rec) {
+                         double* dAB, SmStages<C::kN>* rec) {
   constexpr int n = C::kN;
   double base[n], kp[n], sum[n], yB1[n], u[n], k[n], incA[n], incB1[n];
   double pbase = pas, sump = k1p, pB1 = pas, kk;
@@ -167,7 +173,7 @@ KT_HD int sm_attempt(double M, const SmPrm<double>& P, double tol, const double*
   double yA[C::kN], yB[C::kN], dAB[C::kN], pB = 0.0;
   sm_paths<C>(M, P, c, y, pas, k1, k1p, *h, yA, yB, &pB, dAB, nullptr);
   double e2 = 0.0;
-  for (int i = 0; i < C::kN; ++i) {
+  for (int i = 0; i < C::kG; ++i) {
     const double d = dAB[i];
     e2 = e2 + d * d;
   }
@@ -220,7 +226,7 @@ KT_HD double dp5_e(int j) { return dp5_tab(36 + j); }
 
 template <class C>
 KT_HD_CALL void sm_dp_paths(double M, const SmPrm<double>& P, const double* c, const double* y,
-                            const double* k1, double hh, double* y5, double* dy, SmStages* rec) {
+                            const double* k1, double hh, double* y5, double* dy, SmStages<C::kN>* rec) {
   constexpr int n = C::kN;
   double kk[7][n], u[n], fp;
   for (int i = 0; i < n; ++i) kk[0][i] = k1[i];
@@ -311,7 +317,10 @@ KT_HD void sm_stop(const Frame& f, const double* y, double pas, int status, uint
   }
   o->steps = steps;
   o->attempts = attempts;
-  set_result(o, kOutEscaped, status, rr, 1.0, 1.0, tt, pp, 0.0);
+  if (C::kBundle)  // BundleResult{} / {false, r, 1, 1} (ray_bundle.hpp:320, 435)
+    set_result(o, kOutEscaped, status, 0.0, 1.0, 1.0, 0.0, 0.0, 0.0);
+  else
+    set_result(o, kOutEscaped, status, rr, 1.0, 1.0, tt, pp, 0.0);
 }
 
 // Trace one ray from (y, c, pas).  With ck != NULL, checkpoints are recorded
@@ -321,8 +330,8 @@ KT_HD void sm_stop(const Frame& f, const double* y, double pas, int status, uint
 // otherwise or more than 131072 steps were taken with recording on).
 template <class C, class I = SmRk4>
 KT_HD int sm_trace(const Frame& f, const SmPrm<double>& P, const double* y_in, const double* c,
-                   double pas_in, RayResult* o, SmEvent* ev, SmCk* ck, int* ck_k, int* ck_n,
-                   SmSt* ring) {
+                   double pas_in, RayResult* o, SmEvent<C::kN>* ev, SmCk<C::kN>* ck, int* ck_k, int* ck_n,
+                   SmSt<C::kN>* ring) {
   const double M = f.g.M;
   double y[C::kN], yp[C::kN], k1[C::kN], kprev[C::kN];
   double pas = pas_in, pasp, k1p, kprevp;
@@ -383,15 +392,16 @@ KT_HD int sm_trace(const Frame& f, const SmPrm<double>& P, const double* y_in, c
     const double r_now = C::radius(f.g.a, y);
     double best_alpha = 2.0;
     int evt = kEvNone;
-    double disk_r = 0.0, disk_red = 1.0, disk_phi = 0.0;
-    int deriv = 0;
+    double disk_r = 0.0, disk_red = 1.0, disk_phi = 0.0, disk_m = 1.0;
+    int deriv = 0, mderiv = 0;
+    bool skip = false;
     const double q0 = yp[C::kEq] - C::kEqTarget, q1 = y[C::kEq] - C::kEqTarget;
     if (sign_change(q0, q1) || dmin(fabs(q0), fabs(q1)) < 0.35) {
       double alpha = 0.0;
       if (sm_first_crossing(yp[C::kEq], y[C::kEq], kprev[C::kEq], k1[C::kEq], step_used,
                             C::kEqTarget, &alpha)) {
-        double yh[C::kN];
-        for (int i = 0; i < C::kN; ++i) yh[i] = sm_hermite(yp[i], y[i], kprev[i], k1[i], step_used, alpha);
+        double yh[C::kG];
+        for (int i = 0; i < C::kG; ++i) yh[i] = sm_hermite(yp[i], y[i], kprev[i], k1[i], step_used, alpha);
         const double r_hit = C::radius(f.g.a, yh);
         if (r_hit >= f.r_in && r_hit <= f.r_out) {
           double red, pph;
@@ -400,10 +410,22 @@ KT_HD int sm_trace(const Frame& f, const SmPrm<double>& P, const double* y_in, c
           } else {
             pph = c[C::kC - 1];
           }
-          deriv = sm_redshift<double>(M, P, r_hit, c[0], pph, &red) ? 1 : 0;
-          if (!(red > 0.0 && red < 20.0)) deriv = 0;
+          if constexpr (C::kBundle) {
+            // ray_bundle.hpp:360-392: the bundle's redshift, and |det| of
+            // W's (r, theta) rows interpolated linearly to the crossing
+            deriv = sm_redshift_bundle<double>(M, P, r_hit, c[0], pph, &red) ? 1 : 0;
+            disk_red = red;
+            double J[4];
+            for (int m = 0; m < 4; ++m) J[m] = yp[4 + m] + alpha * (y[4 + m] - yp[4 + m]);
+            const double det = fabs(J[0] * J[3] - J[1] * J[2]);
+            mderiv = det < 1e-12 ? 0 : 1;
+            disk_m = det < 1e-12 ? 1e-12 : det;
+          } else {
+            deriv = sm_redshift<double>(M, P, r_hit, c[0], pph, &red) ? 1 : 0;
+            if (!(red > 0.0 && red < 20.0)) deriv = 0;
+            disk_red = dclamp(red, 0.0, 20.0);
+          }
           disk_r = r_hit;
-          disk_red = dclamp(red, 0.0, 20.0);
           if (C::kN == 6) {
             double rr, tt;
             ks_to_bl(f.g, yh[0], yh[1], yh[2], &rr, &tt, &disk_phi);
@@ -413,14 +435,26 @@ KT_HD int sm_trace(const Frame& f, const SmPrm<double>& P, const double* y_in, c
           best_alpha = alpha;
           evt = kEvDisk;
         }
+      } else if (C::kBundle) {
+        skip = true;  // ray_bundle.hpp:352-356 `continue`: no horizon/escape test this step
       }
     }
-    horizon_escape(prev_r, r_now, f.rh_cut, f.r_esc, &best_alpha, &evt);
+    if (C::kBundle && skip &&
+        ((r_now <= f.r_doom && k1[0] < 0.0) || (r_now >= f.r_cdoom && k1[0] > 0.0))) {
+      // a ray creeping onto a horizon in BL coordinates (theta frozen near
+      // the equator, the horizon test skipped) ends with the record the
+      // controller's eventual failure would give it
+      o->steps = (uint32_t)it + 1;
+      o->attempts = attempts;
+      set_result(o, kOutEscaped, kStEvent, 0.0, 1.0, 1.0, 0.0, 0.0, 0.0);
+      return 0;
+    }
+    if (!skip) horizon_escape(prev_r, r_now, f.rh_cut, f.r_esc, &best_alpha, &evt);
     if (evt != kEvNone) {
       o->steps = (uint32_t)it + 1;
       o->attempts = attempts;
       if (evt == kEvDisk) {
-        set_result(o, kOutDisk, kStEvent, disk_r, disk_red, 1.0, disk_phi, 0.0, 0.0);
+        set_result(o, kOutDisk, kStEvent, disk_r, disk_red, disk_m, disk_phi, 0.0, 0.0);
         if (ev) {
           for (int i = 0; i < C::kN; ++i) {
             ev->yp[i] = yp[i];
@@ -430,12 +464,19 @@ KT_HD int sm_trace(const Frame& f, const SmPrm<double>& P, const double* y_in, c
           ev->h = step_used;
           ev->alpha = best_alpha;
           ev->deriv = deriv;
+          ev->mderiv = mderiv;
         }
         if (ck_k) *ck_k = k;
         if (ck_n) *ck_n = nck;
         return (ck == nullptr || rec_ok) ? it + 1 : 0;
       }
-      if (evt == kEvHorizon) {
+      if (C::kBundle) {
+        // trace_bundle's records (ray_bundle.hpp:418-433): a horizon hit is
+        // BundleResult{} (escaped toward (0, 0)); an escape carries theta, phi
+        const double te = evt == kEvHorizon ? 0.0 : yp[1] + best_alpha * (y[1] - yp[1]);
+        const double pe = evt == kEvHorizon ? 0.0 : pasp + best_alpha * (pas - pasp);
+        set_result(o, kOutEscaped, kStEvent, 0.0, 1.0, 1.0, 0.0, te, pe);
+      } else if (evt == kEvHorizon) {
         set_result(o, kOutHorizon, kStEvent, prev_r + best_alpha * (r_now - prev_r), 0.0, 1.0, 0.0,
                    0.0, 0.0);
       } else if (C::kN == 6) {
@@ -463,8 +504,8 @@ KT_HD int sm_trace(const Frame& f, const SmPrm<double>& P, const double* y_in, c
 // dlam, rejections included).  Stores each step's start (y_n, H_n) and its
 // number of attempts into st[0..n) and/or a checkpoint every k2 steps into ck2.
 template <class C, class I = SmRk4>
-KT_HD void sm_replay(const Frame& f, const SmPrm<double>& P, const double* c, const SmCk& ck0, int n,
-                     SmSt* st, SmCk* ck2, int k2) {
+KT_HD void sm_replay(const Frame& f, const SmPrm<double>& P, const double* c, const SmCk<C::kN>& ck0, int n,
+                     SmSt<C::kN>* st, SmCk<C::kN>* ck2, int k2) {
   const double M = f.g.M;
   double y[C::kN], y1[C::kN], k1[C::kN], k1p, pas = 0.0, pas1;
   for (int i = 0; i < C::kN; ++i) y[i] = ck0.y[i];
@@ -532,25 +573,62 @@ KT_HD void sm_ctl_partials(double err, double tol, double h, double* dh, double*
 }
 
 // v^T df/d(y, c, prm) at u: ybar = .., cbar += .., pbar += ..
+//
+// Bundle (u = (z, W), f = (J_s grad H(z), J_s Hess(H)(z) W)): with d = J^T v_z
+// and d_k = J^T v_{W,k} (v_{W,k} the cotangent of W's column k),
+//   v^T f = d . grad H + sum_k d_k^T Hess(H) W_k,
+// so z gets Hess(H) d + sum_k D^3 H[., W_k, d_k], W_k gets Hess(H) d_k, and
+// the constants and (a, Q, Lambda) the matching mixed derivatives: one
+// Dual<1> evaluation of grad H along d, and per column one hyper-dual
+// evaluation at z + e1 W_k + e2 d_k (its e2 part is Hess(H) d_k, its e1 e2
+// part D^3 H[., W_k, d_k]).  A zero column cotangent skips its evaluation.
 template <class C>
 KT_HD_CALL void sm_vjp_f(double M, const SmPrm<double>& P, const double* u, const double* c,
                          const double* v, double* ubar, double* cbar, double* pbar) {
-  Dual<1> yd[C::kN], cd[C::kC], gy[C::kN], gc[C::kC], gp[kSmPrm];
-  for (int i = 0; i < C::kX; ++i) {
-    yd[i] = Dual<1>(u[i]);
-    yd[i].d[0] = -v[C::kX + i];
-    yd[C::kX + i] = Dual<1>(u[C::kX + i]);
-    yd[C::kX + i].d[0] = v[i];
+  if constexpr (C::kBundle) {
+    sm_vjp_f<ChartBL>(M, P, u, c, v, ubar, cbar, pbar);
+    SmPrm<HDual> Ph;
+    Ph.a = HDual(P.a);
+    Ph.Q = HDual(P.Q);
+    Ph.L = HDual(P.L);
+    KT_ROLLED
+    for (int k = 0; k < 2; ++k) {
+      const double w0 = v[4 + k], w1 = v[6 + k], w2 = v[8 + k], w3 = v[10 + k];
+      if (w0 == 0.0 && w1 == 0.0 && w2 == 0.0 && w3 == 0.0) {
+        for (int i = 0; i < 4; ++i) ubar[4 + 2 * i + k] = 0.0;
+        continue;
+      }
+      const double dk[4] = {-w2, -w3, w0, w1};
+      HDual yh[4], ch[2], gy[4], gc[2], gp[kSmPrm];
+      for (int i = 0; i < 4; ++i) yh[i] = HDual(u[i], u[4 + 2 * i + k], dk[i], 0.0);
+      ch[0] = HDual(c[0]);
+      ch[1] = HDual(c[1]);
+      ChartBL::grad<HDual, true>(M, Ph, yh, ch, gy, gc, gp);
+      for (int i = 0; i < 4; ++i) {
+        ubar[i] = ubar[i] + gy[i].c;
+        ubar[4 + 2 * i + k] = gy[i].b;
+      }
+      for (int j = 0; j < 2; ++j) cbar[j] = cbar[j] + gc[j].c;
+      for (int q = 0; q < kSmPrm; ++q) pbar[q] = pbar[q] + gp[q].c;
+    }
+  } else {
+    Dual<1> yd[C::kN], cd[C::kC], gy[C::kN], gc[C::kC], gp[kSmPrm];
+    for (int i = 0; i < C::kX; ++i) {
+      yd[i] = Dual<1>(u[i]);
+      yd[i].d[0] = -v[C::kX + i];
+      yd[C::kX + i] = Dual<1>(u[C::kX + i]);
+      yd[C::kX + i].d[0] = v[i];
+    }
+    for (int j = 0; j < C::kC; ++j) cd[j] = Dual<1>(c[j]);
+    SmPrm<Dual<1>> Pd;
+    Pd.a = Dual<1>(P.a);
+    Pd.Q = Dual<1>(P.Q);
+    Pd.L = Dual<1>(P.L);
+    C::grad(M, Pd, yd, cd, gy, gc, gp);
+    for (int i = 0; i < C::kN; ++i) ubar[i] = gy[i].d[0];
+    for (int j = 0; j < C::kC; ++j) cbar[j] = cbar[j] + gc[j].d[0];
+    for (int q = 0; q < kSmPrm; ++q) pbar[q] = pbar[q] + gp[q].d[0];
   }
-  for (int j = 0; j < C::kC; ++j) cd[j] = Dual<1>(c[j]);
-  SmPrm<Dual<1>> Pd;
-  Pd.a = Dual<1>(P.a);
-  Pd.Q = Dual<1>(P.Q);
-  Pd.L = Dual<1>(P.L);
-  C::grad(M, Pd, yd, cd, gy, gc, gp);
-  for (int i = 0; i < C::kN; ++i) ubar[i] = gy[i].d[0];
-  for (int j = 0; j < C::kC; ++j) cbar[j] = cbar[j] + gc[j].d[0];
-  for (int q = 0; q < kSmPrm; ++q) pbar[q] = pbar[q] + gp[q].d[0];
 }
 
 // Reverse of one attempt from y with size hh.  gout: cotangent of the dlam
@@ -569,14 +647,15 @@ KT_HD_CALL void sm_vjp_f(double M, const SmPrm<double>& P, const double* u, cons
 template <class C>
 KT_HD double sm_attempt_bwd(const Frame& f, const SmPrm<double>& P, const double* c, const double* y,
                             double hh, double gout, const double* yb_out, double hbar_extra,
-                            double* ybar, double* cbar, double* pbar, SmStages* st) {
+                            double* ybar, double* cbar, double* pbar, SmStages<C::kN>* st) {
   constexpr int n = C::kN;
   const double M = f.g.M;
   double k1[n], k1p, yA[n], yB[n], pB = 0.0;
   sm_rhs<C>(M, P, y, c, k1, &k1p);
   double d[n], e2 = 0.0;
   sm_paths<C>(M, P, c, y, 0.0, k1, k1p, hh, yA, yB, &pB, d, st);
-  for (int i = 0; i < n; ++i) e2 = e2 + d[i] * d[i];
+  for (int i = 0; i < C::kG; ++i) e2 = e2 + d[i] * d[i];
+  for (int i = C::kG; i < n; ++i) d[i] = 0.0;  // outside the error norm
   const double e = sqrt(e2) / 15.0;
   double dh, de;
   sm_ctl_partials(e, f.tol, hh, &dh, &de);
@@ -696,7 +775,7 @@ KT_HD void sm_dp_ctl_partials(double err, double h, double* dh, double* de) {
 template <class C>
 KT_HD double sm_attempt_bwd_dp(const Frame& f, const SmPrm<double>& P, const double* c, const double* y,
                                double hh, double gout, const double* yb_out, double hbar_extra,
-                               double* ybar, double* cbar, double* pbar, SmStages* st) {
+                               double* ybar, double* cbar, double* pbar, SmStages<C::kN>* st) {
   constexpr int n = C::kN;
   const double M = f.g.M;
   double k1[n], k1p, y5[n], dy[n];
@@ -761,7 +840,7 @@ struct SmRk4 {
   KT_HD static double attempt_bwd(const Frame& f, const SmPrm<double>& P, const double* c,
                                   const double* y, double hh, double gout, const double* yb_out,
                                   double hbar_extra, double* ybar, double* cbar, double* pbar,
-                                  SmStages* st) {
+                                  SmStages<C::kN>* st) {
     return sm_attempt_bwd<C>(f, P, c, y, hh, gout, yb_out, hbar_extra, ybar, cbar, pbar, st);
   }
 };
@@ -776,7 +855,7 @@ struct SmDp5 {
   KT_HD static double attempt_bwd(const Frame& f, const SmPrm<double>& P, const double* c,
                                   const double* y, double hh, double gout, const double* yb_out,
                                   double hbar_extra, double* ybar, double* cbar, double* pbar,
-                                  SmStages* st) {
+                                  SmStages<C::kN>* st) {
     return sm_attempt_bwd_dp<C>(f, P, c, y, hh, gout, yb_out, hbar_extra, ybar, cbar, pbar, st);
   }
 };
@@ -788,9 +867,9 @@ constexpr int kSmMaxAttempts = 66;  // reject cap 64 + the accepted attempt
 // cotangent of the accepted size (the event's).  Out: ybar = cotangent of
 // y_n, *Hbar = of H_n.
 template <class C, class I = SmRk4>
-KT_HD void sm_step_bwd(const Frame& f, const SmPrm<double>& P, const double* c, const SmSt& st,
+KT_HD void sm_step_bwd(const Frame& f, const SmPrm<double>& P, const double* c, const SmSt<C::kN>& st,
                        double hbar_acc, double* ybar, double* Hbar, double* cbar, double* pbar,
-                       SmStages* stg) {
+                       SmStages<C::kN>* stg) {
   const double M = f.g.M;
   double hs[kSmMaxAttempts];
   const int na = st.na < kSmMaxAttempts ? st.na : kSmMaxAttempts;
@@ -821,19 +900,22 @@ KT_HD void sm_step_bwd(const Frame& f, const SmPrm<double>& P, const double* c, 
   *Hbar = gout;
 }
 
-// Cotangents of the event step's inputs from (gbar, rbar): the hit state
+// Cotangents of the event step's inputs from (gbar, rbar, mbar): the hit state
 // yh = Hermite(y_{N-1}, y_N, f_{N-1}, f_N; h, alpha*) feeds the outputs
 // (r_hit; g through the disk redshift), differentiated in Dual over (yh,
 // constants, a, Q, Lambda); alpha* moves with the inputs as
 // d alpha* = -dq / q'(alpha*) (q the equator coordinate's interpolant minus
 // its target), so the inputs also get lambda dq/dx with lambda = -alphabar/q';
-// f_{N-1}, f_N pass their cotangents on through VJPs of the RHS.
+// f_{N-1}, f_N pass their cotangents on through VJPs of the RHS.  A bundle's
+// magnification |det J|, J = W_{N-1} + alpha* (W_N - W_{N-1}) over W's (r,
+// theta) rows, sends mbar to both W's and to alpha*.
 template <class C>
-KT_HD void sm_event_bwd(const Frame& f, const SmPrm<double>& P, const double* c, const SmEvent& ev,
-                        double gbar, double rbar, double* ybp, double* ybN, double* cbar,
-                        double* pbar, double* hbar) {
+KT_HD void sm_event_bwd(const Frame& f, const SmPrm<double>& P, const double* c, const SmEvent<C::kN>& ev,
+                        double gbar, double rbar, double mbar, double* ybp, double* ybN,
+                        double* cbar, double* pbar, double* hbar) {
   constexpr int n = C::kN;
-  constexpr int ND = n + C::kC + kSmPrm;
+  constexpr int ng = C::kG;
+  constexpr int ND = ng + C::kC + kSmPrm;
   typedef Dual<ND> D;
   const double M = f.g.M;
   double fe[2][n], pp;
@@ -845,40 +927,60 @@ KT_HD void sm_event_bwd(const Frame& f, const SmPrm<double>& P, const double* c,
                b11 = a3 - a2;
   const double d00 = 6.0 * a2 - 6.0 * al, d10 = 3.0 * a2 - 4.0 * al + 1.0, d01 = 6.0 * al - 6.0 * a2,
                d11 = 3.0 * a2 - 2.0 * al;
-  D yh[n], cd[C::kC];
-  for (int i = 0; i < n; ++i)
+  D yh[ng], cd[C::kC];
+  for (int i = 0; i < ng; ++i)
     yh[i] = D::var(b00 * ev.yp[i] + b10 * (h * fe[0][i]) + b01 * ev.y[i] + b11 * (h * fe[1][i]), i);
-  for (int j = 0; j < C::kC; ++j) cd[j] = D::var(c[j], n + j);
+  for (int j = 0; j < C::kC; ++j) cd[j] = D::var(c[j], ng + j);
   SmPrm<D> Pd;
-  Pd.a = D::var(P.a, n + C::kC);
-  Pd.Q = D::var(P.Q, n + C::kC + 1);
-  Pd.L = D::var(P.L, n + C::kC + 2);
+  Pd.a = D::var(P.a, ng + C::kC);
+  Pd.Q = D::var(P.Q, ng + C::kC + 1);
+  Pd.L = D::var(P.L, ng + C::kC + 2);
   const D r = C::radius(Pd.a, yh);
   const D pph = (n == 6) ? yh[0] * yh[4] - yh[1] * yh[3] : cd[C::kC - 1];
   D red;
-  const bool has = sm_redshift<D>(M, Pd, r, cd[0], pph, &red) && ev.deriv;
-  double yhb[n];
-  for (int i = 0; i < n; ++i) yhb[i] = rbar * r.d[i] + (has ? gbar * red.d[i] : 0.0);
-  for (int j = 0; j < C::kC; ++j) cbar[j] = cbar[j] + rbar * r.d[n + j] + (has ? gbar * red.d[n + j] : 0.0);
+  bool has;
+  if constexpr (C::kBundle)
+    has = sm_redshift_bundle<D>(M, Pd, r, cd[0], pph, &red) && ev.deriv;
+  else
+    has = sm_redshift<D>(M, Pd, r, cd[0], pph, &red) && ev.deriv;
+  double yhb[ng];
+  for (int i = 0; i < ng; ++i) yhb[i] = rbar * r.d[i] + (has ? gbar * red.d[i] : 0.0);
+  for (int j = 0; j < C::kC; ++j) cbar[j] = cbar[j] + rbar * r.d[ng + j] + (has ? gbar * red.d[ng + j] : 0.0);
   for (int q = 0; q < kSmPrm; ++q)
-    pbar[q] = pbar[q] + rbar * r.d[n + C::kC + q] + (has ? gbar * red.d[n + C::kC + q] : 0.0);
+    pbar[q] = pbar[q] + rbar * r.d[ng + C::kC + q] + (has ? gbar * red.d[ng + C::kC + q] : 0.0);
   // alpha
   double alb = 0.0;
-  for (int i = 0; i < n; ++i)
+  for (int i = 0; i < ng; ++i)
     alb = alb + yhb[i] * (d00 * ev.yp[i] + d10 * (h * fe[0][i]) + d01 * ev.y[i] + d11 * (h * fe[1][i]));
+  double Jb[4] = {0.0, 0.0, 0.0, 0.0};
+  if (C::kBundle && ev.mderiv && mbar != 0.0) {
+    double J[4];
+    for (int m = 0; m < 4; ++m) J[m] = ev.yp[4 + m] + al * (ev.y[4 + m] - ev.yp[4 + m]);
+    const double sg = (J[0] * J[3] - J[1] * J[2]) < 0.0 ? -mbar : mbar;
+    Jb[0] = sg * J[3];
+    Jb[1] = -sg * J[2];
+    Jb[2] = -sg * J[1];
+    Jb[3] = sg * J[0];
+    for (int m = 0; m < 4; ++m) alb = alb + Jb[m] * (ev.y[4 + m] - ev.yp[4 + m]);
+  }
   const int e = C::kEq;
   const double dqda = d00 * ev.yp[e] + d10 * (h * fe[0][e]) + d01 * ev.y[e] + d11 * (h * fe[1][e]);
   const double lam = -alb / dqda;
   double fb[2][n];
   double hb = 0.0;
   for (int i = 0; i < n; ++i) {
-    const double g = yhb[i] + (i == e ? lam : 0.0);
+    const double g = i < ng ? yhb[i] + (i == e ? lam : 0.0) : 0.0;
     ybp[i] = b00 * g;
     ybN[i] = b01 * g;
     fb[0][i] = b10 * h * g;
     fb[1][i] = b11 * h * g;
     hb = hb + (b10 * fe[0][i] + b11 * fe[1][i]) * g;
   }
+  if (C::kBundle)
+    for (int m = 0; m < 4; ++m) {
+      ybp[4 + m] = ybp[4 + m] + (1.0 - al) * Jb[m];
+      ybN[4 + m] = ybN[4 + m] + al * Jb[m];
+    }
   double ub[n];
   KT_ROLLED
   for (int w = 0; w < 2; ++w) {
@@ -894,11 +996,12 @@ KT_HD void sm_event_bwd(const Frame& f, const SmPrm<double>& P, const double* c,
 }
 
 // Scratch of one ray's adjoint (per thread, local memory).
+template <int N>
 struct SmScratch {
-  SmCk ck1[kSmCkCap];
-  SmCk ck2[kSmCkCap];
-  SmSt st[kSmCkSteps];
-  SmStages stages;
+  SmCk<N> ck1[kSmCkCap];
+  SmCk<N> ck2[kSmCkCap];
+  SmSt<N> st[kSmCkSteps];
+  SmStages<N> stages;
 };
 
 // Reverse sweep of a ray traced with recording (N accepted steps, the last
@@ -906,13 +1009,13 @@ struct SmScratch {
 // sc->ck1).  Returns the cotangents of the initial state, the constants
 // and (a, Q, Lambda).  The initial dlam is a constant (step_init).
 template <class C, class I = SmRk4>
-KT_HD void sm_adjoint(const Frame& f, const SmPrm<double>& P, const double* c, const SmEvent& ev,
-                      int N, int k1, double gbar, double rbar, SmScratch* sc, double* ybar,
-                      double* cbar, double* pbar) {
+KT_HD void sm_adjoint(const Frame& f, const SmPrm<double>& P, const double* c, const SmEvent<C::kN>& ev,
+                      int N, int k1, double gbar, double rbar, double mbar, SmScratch<C::kN>* sc,
+                      double* ybar, double* cbar, double* pbar) {
   double ybN[C::kN], yb_direct[C::kN], hbar_ev = 0.0;
   for (int j = 0; j < C::kC; ++j) cbar[j] = 0.0;
   for (int q = 0; q < kSmPrm; ++q) pbar[q] = 0.0;
-  sm_event_bwd<C>(f, P, c, ev, gbar, rbar, yb_direct, ybN, cbar, pbar, &hbar_ev);
+  sm_event_bwd<C>(f, P, c, ev, gbar, rbar, mbar, yb_direct, ybN, cbar, pbar, &hbar_ev);
   // The walk starts at step N-1 with the cotangent of y_N (H_N unused); the
   // direct seed of y_{N-1} joins after that step.
   for (int i = 0; i < C::kN; ++i) ybar[i] = ybN[i];
@@ -952,13 +1055,16 @@ namespace kt {
 
 // Where a disk-hit pixel's cotangents come from.
 struct SmCot {
-  int mode;  // 0: forward only; 1: arrays g, r; 2: L2 loss against a target frame
+  int mode;  // 0: forward only; 1: arrays g, r (and m); 2: L2 loss against a target frame
   const double* g;
   const double* r;
   const uint8_t* t_out;
   const double* t_g;
   const double* t_r;
   double w_g, w_r;
+  const double* m;    // cotangent of the magnification (mode 1; bundles)
+  const double* t_m;  // target magnification (mode 2; bundles)
+  double w_m;
 };
 
 // A launch of the smooth kernel with gradients: cotangent source, chart
@@ -983,6 +1089,23 @@ enum : int {
   kGNumUnrecorded = 8, kGSlots = 9
 };
 
+// init_bundle (ray_bundle.hpp:278-298): W's columns are the central
+// differences of the camera ray (r, theta, p_r, p_theta) over alpha and beta
+// with the half-pixel step f.bundle_eps, here in T (the camera's own
+// parameters carried as Duals for the chain to theta_obs, r_obs, a, Q, Lambda).
+template <class T>
+KT_HD void sm_bundle_w0(const Frame& f, double M, const SmPrm<T>& P, const T& r_obs, const T& th_obs,
+                        double al, double be, T* W) {
+  const double eps = f.bundle_eps;
+  T yp[4], ym[4], cp[2], cm[2];
+  KT_ROLLED
+  for (int k = 0; k < 2; ++k) {
+    sm_camera<T>(M, P, r_obs, th_obs, k == 0 ? al + eps : al, k == 0 ? be : be + eps, yp, cp);
+    sm_camera<T>(M, P, r_obs, th_obs, k == 0 ? al - eps : al, k == 0 ? be : be - eps, ym, cm);
+    for (int i = 0; i < 4; ++i) W[2 * i + k] = (yp[i] - ym[i]) / (2.0 * eps);
+  }
+}
+
 // One pixel of the smooth tracer in chart C: outputs into *o; with a
 // cotangent source, the pixel's loss, gradient (theta in radians) and counts
 // into g[kGSlots].  In the KS chart a ray whose KS initialisation fails
@@ -990,7 +1113,7 @@ enum : int {
 // caller hands it to the BL chart.
 template <class C, bool kGrad, class I = SmRk4>
 KT_HD bool sm_pixel(const Frame& f, uint32_t pix, const SmCot& cot, RayResult* o, double* g,
-                    SmScratch* sc) {
+                    SmScratch<C::kN>* sc) {
   constexpr bool kKS = C::kN == 6;
   const int px = (int)(pix % (uint32_t)f.cam.W), py = (int)(pix / (uint32_t)f.cam.W);
   double al, be;
@@ -1005,37 +1128,44 @@ KT_HD bool sm_pixel(const Frame& f, uint32_t pix, const SmCot& cot, RayResult* o
     for (int i = 0; i < C::kN; ++i) y0[i] = yk[i];
     c0[0] = ck[0];
   } else {
-    for (int i = 0; i < C::kN; ++i) y0[i] = ybl[i];
+    for (int i = 0; i < 4; ++i) y0[i] = ybl[i];
     for (int j = 0; j < C::kC; ++j) c0[j] = cbl[j];
+    if constexpr (C::kBundle) sm_bundle_w0<double>(f, M, P, f.cam.r_obs, f.cam.theta_obs, al, be, y0 + 4);
   }
-  SmEvent ev;
+  SmEvent<C::kN> ev;
   int k1 = 0, nck = 0;
-  SmCk* ck = kGrad ? sc->ck1 : nullptr;
+  SmCk<C::kN>* ck = kGrad ? sc->ck1 : nullptr;
   const int N = sm_trace<C, I>(f, P, y0, c0, kKS ? 0.0 : f.cam.phi_obs, o, &ev, ck, &k1, &nck,
                                kGrad ? sc->st : nullptr);
   if (!kGrad) return true;
   for (int q = 0; q < kGSlots; ++q) g[q] = 0.0;
   g[kGNumBL] = kKS ? 0.0 : 1.0;
   if (o->outcome != kOutDisk) return true;
-  double gbar = 0.0, rbar = 0.0;
+  double gbar = 0.0, rbar = 0.0, mbar = 0.0;
   if (cot.mode == 1) {
     gbar = cot.g ? cot.g[pix] : 0.0;
     rbar = cot.r ? cot.r[pix] : 0.0;
+    mbar = (C::kBundle && cot.m) ? cot.m[pix] : 0.0;
   } else if (cot.mode == 2) {
     if (cot.t_out[pix] != kOutDisk) return true;
     const double dg = o->red - cot.t_g[pix], dr = o->r - cot.t_r[pix];
     g[kGLoss] = cot.w_g * dg * dg + cot.w_r * dr * dr;
     gbar = 2.0 * cot.w_g * dg;
     rbar = 2.0 * cot.w_r * dr;
+    if (C::kBundle && cot.t_m && cot.w_m != 0.0) {
+      const double dm = o->magnif - cot.t_m[pix];
+      g[kGLoss] = g[kGLoss] + cot.w_m * dm * dm;
+      mbar = 2.0 * cot.w_m * dm;
+    }
   }
-  if (gbar == 0.0 && rbar == 0.0) return true;
+  if (gbar == 0.0 && rbar == 0.0 && mbar == 0.0) return true;
   if (N == 0) {
     g[kGNumUnrecorded] = 1.0;
     return true;
   }
   g[kGNumGrad] = 1.0;
   double ybar[C::kN], cbar[C::kC], pbar[kSmPrm];
-  sm_adjoint<C, I>(f, P, c0, ev, N, k1, gbar, rbar, sc, ybar, cbar, pbar);
+  sm_adjoint<C, I>(f, P, c0, ev, N, k1, gbar, rbar, mbar, sc, ybar, cbar, pbar);
   // chain through the camera ray: Dual over (a, Q, Lambda, theta_obs, r_obs)
   typedef Dual<5> D5;
   SmPrm<D5> Pd;
@@ -1051,8 +1181,9 @@ KT_HD bool sm_pixel(const Frame& f, uint32_t pix, const SmCot& cot, RayResult* o
     for (int i = 0; i < C::kN; ++i) y5[i] = yk[i];
     c5[0] = ck5[0];
   } else {
-    for (int i = 0; i < C::kN; ++i) y5[i] = yb5[i];
+    for (int i = 0; i < 4; ++i) y5[i] = yb5[i];
     for (int j = 0; j < C::kC; ++j) c5[j] = cb5[j];
+    if constexpr (C::kBundle) sm_bundle_w0<D5>(f, M, Pd, rd, thd, al, be, y5 + 4);
   }
   for (int k = 0; k < 5; ++k) {
     double acc = k < kSmPrm ? pbar[k] : 0.0;

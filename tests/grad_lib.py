@@ -49,11 +49,20 @@ CFG2_DOPRI5 = dict(chart=1, integrator=1, tol=1e-10, a=0.9, Q=0.3, Lambda=1e-4, 
                    theta_deg=85.0, fov_deg=30.0, disk_out=20.0, width=320, height=180)
 TARGET_CFG2 = dict(a=0.92, theta_deg=86.0)
 
+# A KNdS Jacobi-bundle frame (BL, RK4 step doubling, tol 1e-9) for the
+# bundle adjoint, its loss with the magnification (weight W_M) against the
+# same tracer at a=0.92, theta=71.
+BUNDLE = dict(chart=1, bundles=1, a=0.9, Q=0.2, Lambda=1e-5, theta_deg=70.0, r_obs=40.0,
+              fov_deg=30.0, disk_out=12.0, tol=1e-9, max_steps=20000, width=320, height=180)
+TARGET_BUNDLE = dict(a=0.92, theta_deg=71.0)
+W_M = 0.01
 
-def fd_check(renderer, base=CFG5, h4=1e-4, h2=1e-6, target=None):
+
+def fd_check(renderer, base=CFG5, h4=1e-4, h2=1e-6, target=None, w_m=0.0):
     """Returns {"five_point": .., "two_point": .., "two_point_loose": ..},
     each with the per-parameter adjoint, difference and relative
-    disagreement, the worst of them and the number of pixels in the loss."""
+    disagreement, the worst of them and the number of pixels in the loss.
+    With w_m, the loss also holds w_m (magnif - magnif_t)^2 (bundles)."""
     import torch
 
     def smooth(kw):
@@ -61,20 +70,32 @@ def fd_check(renderer, base=CFG5, h4=1e-4, h2=1e-6, target=None):
 
     tgt = smooth(dict(base, **(target or dict(a=0.72, theta_deg=71.0))))
     b0 = smooth(base)
-    bl0 = smooth(dict(base, chart=1))
+    bl0 = b0 if base.get("chart", 0) == 1 else smooth(dict(base, chart=1))
     m_all = (b0["outcome"] == 1) & (tgt["outcome"] == 1)
+    fields = ("redshift", "r", "magnif") if w_m else ("redshift", "r")
 
     def loss_on(o, ok):
-        return np.sum(W_G * (o["redshift"][ok] - tgt["redshift"][ok]) ** 2 +
-                      W_R * (o["r"][ok] - tgt["r"][ok]) ** 2)
+        L = np.sum(W_G * (o["redshift"][ok] - tgt["redshift"][ok]) ** 2 +
+                   W_R * (o["r"][ok] - tgt["r"][ok]) ** 2)
+        if w_m:
+            L += np.sum(w_m * (o["magnif"][ok] - tgt["magnif"][ok]) ** 2)
+        return L
 
     def adjoint(ok):
         def cot(o):
-            return (torch.from_numpy(np.where(ok, 2 * W_G * (o["redshift"] - tgt["redshift"]), 0.0)).cuda(),
-                    torch.from_numpy(np.where(ok, 2 * W_R * (o["r"] - tgt["r"]), 0.0)).cuda())
+            c = (torch.from_numpy(np.where(ok, 2 * W_G * (o["redshift"] - tgt["redshift"]), 0.0)).cuda(),
+                 torch.from_numpy(np.where(ok, 2 * W_R * (o["r"] - tgt["r"]), 0.0)).cuda())
+            m = (torch.from_numpy(np.where(ok, 2 * w_m * (o["magnif"] - tgt["magnif"]), 0.0)).cuda()
+                 if w_m else None)
+            return c, m
 
-        g, _ = renderer.vjp(abi.frame_desc(**base), *cot(b0), flags=abi.KT_GRAD_SKIP_LAMBDA)
-        gl, _ = renderer.vjp(abi.frame_desc(**dict(base, chart=1)), *cot(bl0))
+        (cg, cr), cm = cot(b0)
+        if base.get("chart", 0) == 1:  # BL: Lambda from the same reverse sweep
+            g, _ = renderer.vjp(abi.frame_desc(**base), cg, cr, cot_magnif=cm)
+            gl = g
+        else:
+            g, _ = renderer.vjp(abi.frame_desc(**base), cg, cr, flags=abi.KT_GRAD_SKIP_LAMBDA)
+            gl, _ = renderer.vjp(abi.frame_desc(**dict(base, chart=1)), *cot(bl0)[0])
         return {"a": g[0], "Q": g[1], "Lambda": gl[2], "theta_deg": g[3], "r_obs": g[4]}
 
     def stencil(k, hk, js):
@@ -96,7 +117,7 @@ def fd_check(renderer, base=CFG5, h4=1e-4, h2=1e-6, target=None):
         renders[k] = (rs, hk)
         for o in rs.values():
             ok = same_piece(o0, o, ok)
-        for f in ("redshift", "r"):
+        for f in fields:
             for j in (1, 2):
                 op, om = rs[j][f], rs[-j][f]
                 ok &= np.abs(op - 2 * o0[f] + om) <= 1e-8 + 0.01 * np.abs(op - om)

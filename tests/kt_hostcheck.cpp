@@ -262,12 +262,16 @@ extern "C" int hc_trace_pixels_fp64_rhs(const kt_frame_desc* d, int64_t n, const
 // g++ with the kernels' floating-point flags): pixels pix[0..n) of the
 // frame; cotangent mode 0 (forward only), 1 (arrays over the frame's pixels)
 // or 2 (L2 against target arrays); contrib[kGSlots][n] per listed pixel.
-extern "C" int hc_smooth_pixels(const kt_frame_desc* d, int64_t n, const uint32_t* pix, int mode,
-                                int force_bl, int tangent_dir, const double* cot_g, const double* cot_r,
-                                const uint8_t* t_out, const double* t_g, const double* t_r,
-                                double w_g, double w_r, uint8_t* outcome, double* r, double* red,
-                                double* phi_disk, double* th_esc, double* ph_esc, uint32_t* steps,
-                                uint32_t* attempts, double* contrib) {
+// Bundle frames take the bundle tracer (cot_m / t_m, w_m: the
+// magnification's cotangent or target; magnif may be NULL).
+extern "C" int hc_smooth_pixels_m(const kt_frame_desc* d, int64_t n, const uint32_t* pix, int mode,
+                                  int force_bl, int tangent_dir, const double* cot_g,
+                                  const double* cot_r, const double* cot_m, const uint8_t* t_out,
+                                  const double* t_g, const double* t_r, const double* t_m,
+                                  double w_g, double w_r, double w_m, uint8_t* outcome, double* r,
+                                  double* red, double* magnif, double* phi_disk, double* th_esc,
+                                  double* ph_esc, uint32_t* steps, uint32_t* attempts,
+                                  double* contrib) {
   kt_frame_desc dd = *d;
   dd.precision = KT_PREC_SMOOTH;
   Frame f;
@@ -283,41 +287,54 @@ extern "C" int hc_smooth_pixels(const kt_frame_desc* d, int64_t n, const uint32_
   cot.t_r = t_r;
   cot.w_g = w_g;
   cot.w_r = w_r;
-  // BL frames with DOPRI5 take the smooth DOPRI5 integrator, as the kernels
-  // do (no forward-mode tangent for it)
-  const bool dp5 = f.intg == KT_DOPRI5 && f.chart == KT_CHART_BL;
-  if (dp5 && mode != 0 && tangent_dir >= 0) return 2;
+  cot.m = cot_m;
+  cot.t_m = t_m;
+  cot.w_m = w_m;
+  // BL frames with DOPRI5 take the smooth DOPRI5 integrator, bundles the
+  // bundle tracer, as the kernels do (no forward-mode tangent for either)
+  const bool bundle = f.bundles != 0;
+  const bool dp5 = !bundle && f.intg == KT_DOPRI5 && f.chart == KT_CHART_BL;
+  if ((dp5 || bundle) && mode != 0 && tangent_dir >= 0) return 2;
 #pragma omp parallel
   {
-    SmScratch* sc = new SmScratch;
+    SmScratch<6>* sk = new SmScratch<6>;
+    SmScratch<4>* sb = new SmScratch<4>;
+    SmScratch<12>* sw = bundle ? new SmScratch<12> : nullptr;
 #pragma omp for schedule(dynamic, 2)
     for (int64_t i = 0; i < n; ++i) {
       RayResult o;
       double g[kGSlots];
       const bool ks = f.chart == KT_CHART_KS && !force_bl;
       bool done = false;
-      if (mode != 0 && tangent_dir >= 0) {
+      if (bundle) {
+        if (mode == 0)
+          sm_pixel<ChartBLB, false>(f, pix[i], cot, &o, g, nullptr);
+        else
+          sm_pixel<ChartBLB, true>(f, pix[i], cot, &o, g, sw);
+        done = true;
+      } else if (mode != 0 && tangent_dir >= 0) {
         if (ks) done = sm_pixel_tangent<ChartKS>(f, pix[i], tangent_dir, cot, &o, g);
         if (!done) sm_pixel_tangent<ChartBL>(f, pix[i], tangent_dir, cot, &o, g);
         done = true;
       } else if (ks)
         done = mode == 0 ? sm_pixel<ChartKS, false>(f, pix[i], cot, &o, g, nullptr)
-                         : sm_pixel<ChartKS, true>(f, pix[i], cot, &o, g, sc);
+                         : sm_pixel<ChartKS, true>(f, pix[i], cot, &o, g, sk);
       if (!done) {
         if (dp5) {
           if (mode == 0)
             sm_pixel<ChartBL, false, SmDp5>(f, pix[i], cot, &o, g, nullptr);
           else
-            sm_pixel<ChartBL, true, SmDp5>(f, pix[i], cot, &o, g, sc);
+            sm_pixel<ChartBL, true, SmDp5>(f, pix[i], cot, &o, g, sb);
         } else if (mode == 0) {
           sm_pixel<ChartBL, false>(f, pix[i], cot, &o, g, nullptr);
         } else {
-          sm_pixel<ChartBL, true>(f, pix[i], cot, &o, g, sc);
+          sm_pixel<ChartBL, true>(f, pix[i], cot, &o, g, sb);
         }
       }
       outcome[i] = (uint8_t)o.outcome;
       r[i] = o.r;
       red[i] = o.red;
+      if (magnif) magnif[i] = o.magnif;
       phi_disk[i] = o.phi_disk;
       th_esc[i] = o.th_esc;
       ph_esc[i] = o.ph_esc;
@@ -326,7 +343,20 @@ extern "C" int hc_smooth_pixels(const kt_frame_desc* d, int64_t n, const uint32_
       if (mode != 0 && contrib)
         for (int q = 0; q < kGSlots; ++q) contrib[q * n + i] = g[q];
     }
-    delete sc;
+    delete sk;
+    delete sb;
+    delete sw;
   }
   return 0;
+}
+
+extern "C" int hc_smooth_pixels(const kt_frame_desc* d, int64_t n, const uint32_t* pix, int mode,
+                                int force_bl, int tangent_dir, const double* cot_g, const double* cot_r,
+                                const uint8_t* t_out, const double* t_g, const double* t_r,
+                                double w_g, double w_r, uint8_t* outcome, double* r, double* red,
+                                double* phi_disk, double* th_esc, double* ph_esc, uint32_t* steps,
+                                uint32_t* attempts, double* contrib) {
+  return hc_smooth_pixels_m(d, n, pix, mode, force_bl, tangent_dir, cot_g, cot_r, nullptr, t_out, t_g,
+                            t_r, nullptr, w_g, w_r, 0.0, outcome, r, red, nullptr, phi_disk, th_esc,
+                            ph_esc, steps, attempts, contrib);
 }

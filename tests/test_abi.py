@@ -168,7 +168,7 @@ def test_fallback_rules():
     (dict(solver_mode=abi.KT_SOLVER_ELLIPTIC_CLOSED, precision=abi.KT_PREC_MIXED), abi.KT_ERR_UNSUPPORTED),
     (dict(solver_mode=9), abi.KT_ERR_INVALID_ARGUMENT),
     (dict(precision=7), abi.KT_ERR_INVALID_ARGUMENT),
-    (dict(precision=abi.KT_PREC_SMOOTH, bundles=1), abi.KT_ERR_UNSUPPORTED),
+    (dict(solver_mode=abi.KT_SOLVER_ELLIPTIC_CLOSED, precision=abi.KT_PREC_SMOOTH), abi.KT_ERR_UNSUPPORTED),
     (dict(r_obs=-1.0), abi.KT_ERR_INVALID_ARGUMENT),
     (dict(flags=8), abi.KT_ERR_INVALID_ARGUMENT),
 ])

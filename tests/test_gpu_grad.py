@@ -15,7 +15,13 @@ pytestmark = pytest.mark.gpu
 
 CFG5 = dict(chart=0, a=0.7, Q=0.1, Lambda=0.0, theta_deg=70.0, r_obs=50.0, disk_out=15.0)
 KNDS = dict(chart=1, a=0.9, Q=0.3, Lambda=1e-4, r_obs=60.0, theta_deg=85.0, disk_out=20.0)
-FIELDS = ["outcome", "r", "redshift", "phi_disk", "theta_esc", "phi_esc", "steps", "attempts"]
+# Jacobi bundles: configuration 3's geometry, and a KNdS bundle frame
+CFG3 = dict(chart=1, bundles=1, a=0.998, theta_deg=60.0, r_obs=40.0, fov_deg=30.0, disk_out=12.0,
+            max_steps=20000)
+BUNDLE = dict(chart=1, bundles=1, a=0.9, Q=0.2, Lambda=1e-5, theta_deg=70.0, r_obs=40.0,
+              fov_deg=30.0, disk_out=12.0, max_steps=20000)
+FIELDS = ["outcome", "r", "redshift", "magnif", "phi_disk", "theta_esc", "phi_esc", "steps",
+          "attempts"]
 
 
 def to_np(out):
@@ -35,8 +41,10 @@ def smooth_gpu(renderer, kw):
 @pytest.mark.parametrize("kw", [dict(CFG5, width=96, height=96), dict(KNDS, width=96, height=54),
                                 dict(CFG5, width=77, height=31, tol=1e-10),
                                 dict(KNDS, integrator=abi.KT_DOPRI5, tol=1e-10, fov_deg=30.0,
-                                     width=96, height=54)],
-                         ids=["cfg5_ks", "knds_bl", "cfg5_tight", "knds_bl_dopri5"])
+                                     width=96, height=54),
+                                dict(CFG3, width=96, height=54), dict(BUNDLE, width=96, height=54)],
+                         ids=["cfg5_ks", "knds_bl", "cfg5_tight", "knds_bl_dopri5", "cfg3_bundle",
+                              "knds_bundle"])
 def test_smooth_trace_gpu_equals_host(renderer, kw):
     got = smooth_gpu(renderer, kw)
     want, _ = S.smooth(abi.frame_desc(**kw))
@@ -46,8 +54,9 @@ def test_smooth_trace_gpu_equals_host(renderer, kw):
 
 @pytest.mark.parametrize("kw", [dict(CFG5, width=64, height=64), dict(KNDS, width=64, height=36),
                                 dict(KNDS, integrator=abi.KT_DOPRI5, tol=1e-10, fov_deg=30.0,
-                                     width=64, height=36)],
-                         ids=["ks", "bl", "bl_dopri5"])
+                                     width=64, height=36),
+                                dict(BUNDLE, width=64, height=36)],
+                         ids=["ks", "bl", "bl_dopri5", "bundle"])
 def test_vjp_gpu_equals_host(renderer, kw):
     import torch
 
@@ -55,9 +64,11 @@ def test_vjp_gpu_equals_host(renderer, kw):
     n = d.width * d.height
     rng = np.random.default_rng(7)
     cg, cr = rng.normal(size=n), rng.normal(size=n)
+    cm = rng.normal(size=n) if kw.get("bundles") else None
     out = renderer.alloc(n)
-    grad, st = renderer.vjp(d, torch.from_numpy(cg).cuda(), torch.from_numpy(cr).cuda(), out=out)
-    fwd, c = S.smooth(d, mode=1, cot_g=cg, cot_r=cr)
+    grad, st = renderer.vjp(d, torch.from_numpy(cg).cuda(), torch.from_numpy(cr).cuda(), out=out,
+                            cot_magnif=torch.from_numpy(cm).cuda() if cm is not None else None)
+    fwd, c = S.smooth(d, mode=1, cot_g=cg, cot_r=cr, cot_m=cm)
     got = to_np(out)
     for f in FIELDS:
         assert np.array_equal(got[f], fwd[f]), f
@@ -126,6 +137,28 @@ def test_config2_dopri5_gradient_against_central_differences(renderer):
     assert res["five_point"]["worst_rel"] <= 1e-5
     assert res["two_point"]["worst_rel"] <= 1e-5
     assert res["two_point_loose"]["worst_rel"] <= 1e-4
+    assert res["five_point"]["pixels"] > 0.3 * res["five_point"]["disk_pixels"]
+
+
+def test_bundle_gradient_against_central_differences(renderer):
+    """The bundle adjoint (the Jacobi matrix's equation differentiated with
+    third derivatives of H by hyper-dual numbers, the magnification's
+    dependence on W and on the crossing): a KNdS bundle frame at 320x180,
+    tol 1e-9, L2 loss of (g, r_hit, magnification) against a=0.92,
+    theta=71: five-point (h = 1e-4) central differences on the smooth
+    pixels to 1e-5 relative, two-point (h = 1e-6) on the same pixels to
+    1e-4 (the magnification's rounding noise over 2h), the loose mask
+    reported and bounded at 1e-3."""
+    import grad_lib
+
+    res = grad_lib.fd_check(renderer, grad_lib.BUNDLE, target=grad_lib.TARGET_BUNDLE, w_m=grad_lib.W_M)
+    for name, r in res.items():
+        print(f"{name} h={r['h']:g}: {r['pixels']} of {r['disk_pixels']} disk pixels in the loss")
+        for k, v in r["per_param"].items():
+            print(f"  {k}: adjoint {v['adjoint']:.10g} differences {v['fd']:.10g} rel {v['rel']:.2e}")
+    assert res["five_point"]["worst_rel"] <= 1e-5
+    assert res["two_point"]["worst_rel"] <= 1e-4
+    assert res["two_point_loose"]["worst_rel"] <= 1e-3
     assert res["five_point"]["pixels"] > 0.3 * res["five_point"]["disk_pixels"]
 
 

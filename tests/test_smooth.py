@@ -184,20 +184,21 @@ def test_smooth_frames_rejected_where_unsupported(L=None):
 
     lib = kt.load_library()
     out = abi.FrameDerived()
-    for kw, st in [(dict(bundles=1), abi.KT_ERR_UNSUPPORTED),
-                   (dict(precision=3), abi.KT_ERR_INVALID_ARGUMENT)]:
+    for kw, st in [(dict(precision=3), abi.KT_ERR_INVALID_ARGUMENT),
+                   (dict(bundles=2), abi.KT_ERR_INVALID_ARGUMENT)]:
         d = abi.frame_desc(width=4, height=4, **dict(dict(precision=abi.KT_PREC_SMOOTH), **kw))
         assert lib.kt_frame_derive(ctypes.byref(d), ctypes.byref(out)) == st
     # DOPRI5 in the BL chart (and KS + Lambda, which runs in BL); the KS
-    # chart ignores --dopri5, as the reference does
+    # chart ignores --dopri5, as the reference does; bundles (BL chart, RK4)
     for kw in (dict(chart=1, integrator=1), dict(chart=0, integrator=1, Lambda=1e-4),
-               dict(chart=0, integrator=1)):
+               dict(chart=0, integrator=1), dict(bundles=1), dict(bundles=1, integrator=1)):
         d = abi.frame_desc(width=4, height=4, precision=abi.KT_PREC_SMOOTH, **kw)
         assert lib.kt_frame_derive(ctypes.byref(d), ctypes.byref(out)) == abi.KT_OK
-    # the forward-mode tangent is RK4 only
-    with pytest.raises(ValueError):
-        S.smooth(abi.frame_desc(chart=1, integrator=1, width=4, height=4), mode=1,
-                 cot_g=np.ones(16), cot_r=np.zeros(16), tangent=0)
+    # the forward-mode tangent is RK4 without bundles only
+    for kw in (dict(chart=1, integrator=1), dict(chart=1, bundles=1)):
+        with pytest.raises(ValueError):
+            S.smooth(abi.frame_desc(width=4, height=4, **kw), mode=1,
+                     cot_g=np.ones(16), cot_r=np.zeros(16), tangent=0)
 
 
 @pytest.mark.parametrize("frame,dirs", [(dict(KNDS, width=48, height=27), [0, 1, 2, 3, 4]),
@@ -221,6 +222,126 @@ def test_tangent_equals_adjoint(frame, dirs):
         others = [q for q in range(5) if q != k]
         assert not ct[others].any()
         assert np.array_equal(ct[6], ca[6])  # the same pixels get a derivative
+
+
+# Jacobi bundles: configuration 3's geometry (BL, a = 0.998, theta = 60,
+# r_obs = 40, fov 30, disk ISCO-12), and a KNdS bundle frame for gradients
+# (Q = 0 would make dL/dQ vanish).
+CFG3 = dict(chart=1, bundles=1, a=0.998, theta_deg=60.0, r_obs=40.0, fov_deg=30.0, disk_out=12.0)
+BUNDLE = dict(chart=1, bundles=1, a=0.9, Q=0.2, Lambda=1e-5, theta_deg=70.0, r_obs=40.0,
+              fov_deg=30.0, disk_out=12.0)
+
+
+def test_smooth_bundle_close_to_reference_bundle():
+    """The smooth bundle tracer (analytic Hessian in place of the reference's
+    33-point finite differences, ray_bundle.hpp:56-108) against the
+    reference's bundle trace (the oracle): every pixel's class, g and r_hit
+    to the reference's own noise; the magnification, whose finite-difference
+    Hessian carries ~1e-5 relative rounding noise, to 2e-4 at the median
+    (larger near the critical curve, where W is ill-conditioned)."""
+    d = abi.frame_desc(**dict(CFG3, width=64, height=36, max_steps=20000))
+    sm, _ = S.smooth(d)
+    ex = O.trace_port(d)
+    assert np.array_equal(sm["outcome"], ex["outcome"])
+    disk = ex["outcome"] == 1
+    assert disk.sum() > 1500
+    rel = {f: np.abs(sm[f][disk] - ex[f][disk]) / np.abs(ex[f][disk]) for f in ("r", "redshift", "magnif")}
+    print({f: (np.median(v), np.percentile(v, 99), v.max()) for f, v in rel.items()})
+    assert np.median(rel["r"]) < 2e-5 and rel["r"].max() < 1e-4
+    assert np.median(rel["redshift"]) < 1e-5 and np.percentile(rel["redshift"], 99) < 1e-3
+    assert np.median(rel["magnif"]) < 2e-4
+    esc = ex["outcome"] == 0
+    assert np.abs(sm["theta_esc"][esc] - ex["theta_esc"][esc]).max() < 1e-4
+
+
+def test_bundle_per_ray_gradients_match_central_differences():
+    """Per-ray derivatives of g, r_hit (two-point, h = 1e-5) and of the
+    magnification (five-point, h = 1e-3, Lambda 1e-7: its rounding noise,
+    ~1e-11 relative, dominates smaller steps) on the pixels whose stencil
+    keeps class and step sequence, and, for the magnification, stays in its
+    linear range (near a caustic, where det J passes close to 0, a step of
+    1e-3 does not)."""
+    base = dict(BUNDLE, width=64, height=36, max_steps=20000, tol=1e-10)
+    n = base["width"] * base["height"]
+    pix = np.arange(0, n, 3, dtype=np.uint32)
+    d = abi.frame_desc(**base)
+    b0, _ = S.smooth(d, pix=pix)
+    one, zero = np.ones(n), np.zeros(n)
+    cots = {f: S.smooth(d, pix=pix, mode=1, cot_g=one if f == "redshift" else zero,
+                        cot_r=one if f == "r" else zero, cot_m=one if f == "magnif" else zero)[1]
+            for f in ("redshift", "r", "magnif")}
+    steps = {"a": 1e-5, "Q": 1e-5, "Lambda": 1e-8, "theta_deg": np.degrees(1e-5), "r_obs": 1e-4}
+    for q, (k, hk) in enumerate(steps.items()):
+        hm = (10 if k == "Lambda" else 100) * hk
+        for f, h, js in (("redshift", hk, (-1, 1)), ("r", hk, (-1, 1)), ("magnif", hm, (-2, -1, 1, 2))):
+            rs = {j: S.smooth(abi.frame_desc(**dict(base, **{k: base[k] + j * h})), pix=pix)[0] for j in js}
+            ok = b0["outcome"] == 1
+            for o in rs.values():
+                ok &= (o["outcome"] == 1) & (o["steps"] == b0["steps"]) & (o["attempts"] == b0["attempts"])
+            assert ok.sum() >= 300, (k, f)
+            if len(js) == 2:
+                fd = (rs[1][f] - rs[-1][f]) / (2 * h)
+            else:
+                fd = (rs[-2][f] - 8 * rs[-1][f] + 8 * rs[1][f] - rs[2][f]) / (12 * h)
+                # within the linear range: differences over h and 2h agree
+                d1, d2 = rs[1][f] - rs[-1][f], rs[2][f] - rs[-2][f]
+                ok &= np.abs(d2 - 2 * d1) <= 1e-3 * np.abs(d1)
+                assert ok.sum() >= 300, (k, f)
+            adj = cots[f][q] * (np.pi / 180 if k == "theta_deg" else 1.0)
+            fd, adj = fd[ok], adj[ok]
+            rel = np.abs(adj - fd) / (np.abs(fd) + 1e-3 * np.abs(fd).max())
+            assert rel.max() < (1e-4 if f == "magnif" else 1e-5), (k, f, rel.max())
+
+
+def test_bundle_l2_gradient_matches_central_differences():
+    """The L2 loss of (g, r_hit, magnification) of a 96x54 KNdS bundle frame
+    against the same tracer at a = 0.92, theta = 71, restricted to the
+    pixels whose five-point stencil keeps class and step sequence: the
+    adjoint against five-point differences with h = 1e-4 (Lambda 1e-6) to
+    1e-5, and two-point differences with h = 1e-6 (Lambda 1e-8) on the same
+    pixels to 1e-4 (the magnification's rounding noise over 2h)."""
+    base = dict(BUNDLE, width=96, height=54, max_steps=20000, tol=1e-9)
+    wg, wr, wm = 1.0, 0.01, 0.01
+    tgt, _ = S.smooth(abi.frame_desc(**dict(base, a=0.92, theta_deg=71.0)))
+    b0, _ = S.smooth(abi.frame_desc(**base))
+    ok = (b0["outcome"] == 1) & (tgt["outcome"] == 1)
+
+    def step(k, h):
+        return 1e-2 * h if k == "Lambda" else (np.degrees(h) if k == "theta_deg" else h)
+
+    R = {}
+    for h, js in ((1e-4, (-2, -1, 1, 2)), (1e-6, (-1, 1))):
+        for k in PARAMS:
+            rs = {j: S.smooth(abi.frame_desc(**dict(base, **{k: base[k] + j * step(k, h)})))[0] for j in js}
+            R[h, k] = rs
+            for o in rs.values():
+                ok &= (o["outcome"] == 1) & (o["steps"] == b0["steps"]) & (o["attempts"] == b0["attempts"])
+    assert ok.sum() > 2500
+
+    def loss(o):
+        return np.sum(wg * (o["redshift"][ok] - tgt["redshift"][ok]) ** 2 +
+                      wr * (o["r"][ok] - tgt["r"][ok]) ** 2 + wm * (o["magnif"][ok] - tgt["magnif"][ok]) ** 2)
+
+    cg = np.where(ok, 2 * wg * (b0["redshift"] - tgt["redshift"]), 0.0)
+    cr = np.where(ok, 2 * wr * (b0["r"] - tgt["r"]), 0.0)
+    cm = np.where(ok, 2 * wm * (b0["magnif"] - tgt["magnif"]), 0.0)
+    _, c = S.smooth(abi.frame_desc(**base), mode=1, cot_g=cg, cot_r=cr, cot_m=cm)
+    grad = c.sum(axis=1)
+    # the fused L2 form gives the same loss over its own (both-disk) pixels
+    o2, c2 = S.smooth(abi.frame_desc(**base), mode=2, target=tgt, w_g=wg, w_r=wr, w_m=wm)
+    m2 = (o2["outcome"] == 1) & (tgt["outcome"] == 1)
+    assert c2[5].sum() == pytest.approx(np.sum(wg * (o2["redshift"][m2] - tgt["redshift"][m2]) ** 2 +
+                                              wr * (o2["r"][m2] - tgt["r"][m2]) ** 2 +
+                                              wm * (o2["magnif"][m2] - tgt["magnif"][m2]) ** 2), rel=1e-12)
+    for q, k in enumerate(PARAMS):
+        adj = grad[q] * (np.pi / 180 if k == "theta_deg" else 1.0)
+        L = {j: loss(o) for j, o in R[1e-4, k].items()}
+        fd4 = (L[-2] - 8 * L[-1] + 8 * L[1] - L[2]) / (12 * step(k, 1e-4))
+        L2 = {j: loss(o) for j, o in R[1e-6, k].items()}
+        fd2 = (L2[1] - L2[-1]) / (2 * step(k, 1e-6))
+        print(k, adj, fd4, fd2)
+        assert abs(adj - fd4) <= 1e-5 * abs(fd4), (k, adj, fd4)
+        assert abs(adj - fd2) <= 1e-4 * abs(fd2), (k, adj, fd2)
 
 
 @pytest.mark.skipif(not O.ref_available("strict"), reason="reference tree not built here")
