@@ -250,18 +250,27 @@ def _timed_steps(fn, steps, warmup, stream, flush):
 def bundles_leg(R, stream, flush):
     """Config 3: 1920x1080 Jacobi-bundle frame (BL, a=0.998, theta=60, r_obs
     40, fov 30, disk ISCO-12, RK4 doubling, tol 1e-7), plain FP64
-    (bit-identical to the reference) and mixed (analytic Hessian-vector
-    products), with the mixed frame's error against the FP64 one."""
+    (bit-identical to the reference's records; rays creeping onto the
+    horizon stop with the record their end gives) and, for the reference's
+    counters as well, with KT_FLAG_BUNDLE_FULL_CREEP; mixed (analytic
+    Hessian-vector products), with the mixed frame's error against the
+    FP64 one."""
     import torch
     from kerrtracecpp2_b200 import abi
 
     kw = WORKLOADS["bundles_bl_1080p"]
     n = kw["width"] * kw["height"]
     d = abi.frame_desc(**kw)
+    df = abi.frame_desc(**dict(kw, flags=abi.KT_FLAG_BUNDLE_FULL_CREEP))
     dm = abi.frame_desc(**dict(kw, precision=abi.KT_PREC_MIXED))
-    o, om = R.alloc(n), R.alloc(n)
+    o, of, om = R.alloc(n), R.alloc(n), R.alloc(n)
     t = _timed_steps(lambda: R.trace(d, o, stream), LEG_STEPS, 1, stream, flush)
+    tf = _timed_steps(lambda: R.trace(df, of, stream), LEG_STEPS, 1, stream, flush)
     tm = _timed_steps(lambda: R.trace(dm, om, stream), LEG_STEPS, 1, stream, flush)
+    torch.cuda.synchronize()
+    rec_same = all(torch.equal(o[k], of[k]) for k in ("outcome", "r", "redshift", "magnif", "phi_disk",
+                                                     "theta_esc", "phi_esc"))
+    creep = int((o["status"] == abi.KT_RAY_CREEP).sum())
     same = o["outcome"] == om["outcome"]
     disk = same & (o["outcome"] == 1)
     eg = ((om["redshift"] - o["redshift"]).abs() / o["redshift"].abs())[disk]
@@ -269,7 +278,10 @@ def bundles_leg(R, stream, flush):
     q = lambda x, p: float(torch.quantile(x.float(), p)) if x.numel() else None  # noqa: E731
     return {"frame": "1920x1080 Jacobi bundles, BL, a=0.998, theta=60, r_obs=40, fov=30, disk ISCO-12",
             "steps": LEG_STEPS, "fp64_value": LEG_STEPS * n / (t * 1e-3) / 1e6,
-            "fp64_ms_per_step": t / LEG_STEPS,
+            "fp64_ms_per_step": t / LEG_STEPS, "fp64_creeping_rays_stopped": creep,
+            "fp64_full_creep_value": LEG_STEPS * n / (tf * 1e-3) / 1e6,
+            "fp64_full_creep_ms_per_step": tf / LEG_STEPS,
+            "fp64_records_equal_full_creep": rec_same,
             "mixed_value": LEG_STEPS * n / (tm * 1e-3) / 1e6, "mixed_ms_per_step": tm / LEG_STEPS,
             "unit": "Mrays/s", "mixed_speedup": t / tm,
             "mixed_error_vs_fp64": {"class_mismatch_frac": float(1.0 - same.double().mean()),

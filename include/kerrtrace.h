@@ -82,6 +82,13 @@ enum { KT_PREC_FP64 = 0, KT_PREC_MIXED = 1, KT_PREC_SMOOTH = 2 };
 /* kt_frame_desc.flags: theta_deg, phi_deg and fov_deg hold radians (the
  * reference's CameraParams_CUDA carries radians, gpu/cuda/tracer.cuh:16-20). */
 #define KT_FLAG_ANGLES_RADIANS 1u
+/* kt_frame_desc.flags: bundle rays that creep onto the horizon (ingoing
+ * within 1e-4 r_+ of r_+ with the horizon test skipped near the equator,
+ * ray_bundle.hpp:352-356) are traced on until the reference's reject or
+ * step cap, so that their steps and attempts equal the reference's.
+ * Without the flag they stop there with status KT_RAY_CREEP and the same
+ * record (every way such a ray can end gives BundleResult{}). */
+#define KT_FLAG_BUNDLE_FULL_CREEP 2u
 
 /* Per-pixel outcome codes (GeoPixel::outcome, main.cpp:85). */
 enum { KT_OUT_ESCAPED = 0, KT_OUT_DISK = 1, KT_OUT_HORIZON = 2 };
@@ -90,7 +97,9 @@ enum {
   KT_RAY_EVENT = 0,      /* stopped at a disk / horizon / escape event */
   KT_RAY_STEP_CAP = 1,   /* max_steps accepted steps without an event */
   KT_RAY_REJECT_CAP = 2, /* more than 64 consecutive rejected attempts */
-  KT_RAY_NONFINITE = 3   /* step size became non-finite */
+  KT_RAY_NONFINITE = 3,  /* step size became non-finite */
+  KT_RAY_CREEP = 4       /* bundle ray creeping onto a horizon: the record of
+                          * its eventual end (KT_FLAG_BUNDLE_FULL_CREEP) */
 };
 
 typedef struct kt_frame_desc {

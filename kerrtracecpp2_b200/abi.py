@@ -36,6 +36,9 @@ KT_RAY_EVENT = 0
 KT_RAY_STEP_CAP = 1
 KT_RAY_REJECT_CAP = 2
 KT_RAY_NONFINITE = 3
+KT_RAY_CREEP = 4
+KT_FLAG_ANGLES_RADIANS = 1
+KT_FLAG_BUNDLE_FULL_CREEP = 2
 
 
 class FrameDesc(ctypes.Structure):

@@ -236,7 +236,7 @@ kt_status prepare_frame(const kt_frame_desc* d, Frame* f, kt_frame_derived* dv, 
     *err = "precision must be KT_PREC_FP64, KT_PREC_MIXED or KT_PREC_SMOOTH";
     return KT_ERR_INVALID_ARGUMENT;
   }
-  if ((d->flags & ~(uint32_t)KT_FLAG_ANGLES_RADIANS) != 0) {
+  if ((d->flags & ~(uint32_t)(KT_FLAG_ANGLES_RADIANS | KT_FLAG_BUNDLE_FULL_CREEP)) != 0) {
     *err = "unknown bits in flags";
     return KT_ERR_INVALID_ARGUMENT;
   }
@@ -301,14 +301,23 @@ kt_status prepare_frame(const kt_frame_desc* d, Frame* f, kt_frame_derived* dv, 
   fr.r_fp32 = (d->precision == KT_PREC_MIXED && fr.tol >= 1e-8) ? dmax(4.0 * d->M, 2.0 * rh)
                                                                   : ktm_inf();
   fr.turn_frac = 0.05;
-  // Mixed-precision and smooth bundles: rays whose step skipped the horizon
-  // and escape tests (near the equator, no crossing found) and that creep
-  // onto a horizon in BL coordinates -- ingoing within 1e-4 r_+ of r_+, or
-  // outgoing within 1e-4 r_c of the cosmological horizon -- end as a horizon
-  // hit, the record the controller's eventual failure gives them.
-  const bool doom = (d->precision == KT_PREC_MIXED || d->precision == KT_PREC_SMOOTH) && d->bundles;
-  fr.r_doom = doom ? rh * (1.0 + 1e-4) : -ktm_inf();
-  fr.r_cdoom = doom ? host_r_cosmo(fr.g) * (1.0 - 1e-4) : ktm_inf();
+  // Bundles: rays whose step skipped the horizon and escape tests (near the
+  // equator, no crossing found) and that creep onto a horizon in BL
+  // coordinates end with the record the controller's eventual failure gives
+  // them (status KT_RAY_CREEP).  Ingoing within 1e-4 r_+ of r_+, in every
+  // precision: r decreases monotonically there (inside every photon orbit),
+  // below rh_cut and -- checked here, with a margin for the Hermite
+  // interpolant -- below the disk's inner edge, so no ending of the ray can
+  // be a disk hit or an escape and its record is BundleResult{}'s whatever
+  // it does next.  Outgoing within 1e-4 r_c of the cosmological horizon:
+  // mixed and smooth only (an FP64 ray there may still leave the band
+  // beyond r_escape and record an escape).  KT_FLAG_BUNDLE_FULL_CREEP traces
+  // them on, as the reference does, for its step and attempt counts.
+  const double r_doom = rh * (1.0 + 1e-4);
+  const bool creep_end = d->bundles && !(d->flags & KT_FLAG_BUNDLE_FULL_CREEP);
+  fr.r_doom = (creep_end && r_isco > 1.01 * r_doom) ? r_doom : -ktm_inf();
+  fr.r_cdoom = (creep_end && d->precision != KT_PREC_FP64) ? host_r_cosmo(fr.g) * (1.0 - 1e-4)
+                                                          : ktm_inf();
   *f = fr;
   if (dv) {
     memset(dv, 0, sizeof *dv);

@@ -28,7 +28,7 @@
 namespace kt {
 
 enum : int { kOutEscaped = 0, kOutDisk = 1, kOutHorizon = 2 };
-enum : int { kStEvent = 0, kStStepCap = 1, kStRejectCap = 2, kStNonfinite = 3 };
+enum : int { kStEvent = 0, kStStepCap = 1, kStRejectCap = 2, kStNonfinite = 3, kStCreep = 4 };
 enum : int { kEvNone = 0, kEvDisk = 1, kEvHorizon = 2, kEvEscape = 3 };
 
 struct Frame {
@@ -40,8 +40,8 @@ struct Frame {
   double bundle_eps;
   double r_fp32;     // mixed precision: FP32 RHS beyond this radius (inf: never)
   double turn_frac;  // mixed precision: FP64 when |p_r| or |p_th|/r < turn_frac |p_t|
-  double r_doom;     // mixed-precision bundles: a ray ingoing below r_doom or
-  double r_cdoom;    // outgoing beyond r_cdoom ends as a horizon hit (+-inf: never)
+  double r_doom;     // bundles: a ray creeping ingoing below r_doom, or (mixed and
+  double r_cdoom;    // smooth) outgoing beyond r_cdoom, ends as a horizon hit (+-inf: never)
   int max_steps;
   int chart, intg, bundles;
   int precision;     // KT_PREC_FP64 / KT_PREC_MIXED
@@ -821,16 +821,20 @@ struct Bundle {
       }
     }
     if (skip && ((r <= f.r_doom && k1[0] < 0.0) || (r >= f.r_cdoom && k1[0] > 0.0))) {
-      // Mixed precision only (r_doom = -inf, r_cdoom = +inf otherwise): the
-      // step near the equator skipped the horizon and escape tests, and the
-      // ray is ingoing within 1e-4 r_+ of the outer horizon (inside every
-      // photon orbit) or outgoing within 1e-4 r_c of the cosmological one:
-      // it can only creep onto that horizon in BL coordinates, theta frozen,
-      // until the controller gives up, which ends it with the same record
-      // as a horizon hit.
+      // The step near the equator skipped the horizon and escape tests, and
+      // the ray is ingoing within 1e-4 r_+ of the outer horizon (inside every
+      // photon orbit, below the disk's inner edge and rh_cut), or (mixed
+      // precision only) outgoing within 1e-4 r_c of the cosmological one: it
+      // can only creep onto that horizon in BL coordinates, theta frozen,
+      // until the controller gives up (the reference's reject cap, or its
+      // step cap), or leave the band and meet the horizon test at once --
+      // every ending gives the record BundleResult{} gives (trace_bundle,
+      // ray_bundle.hpp:320, 418-435; the frame loop writes r = 0 for every
+      // ray that misses the disk, main.cpp:2103-2110).  It ends here with
+      // that record and status kStCreep; its counters stop here.
       o->steps = (uint32_t)it + 1;
       o->attempts = attempts;
-      set_result(o, kOutEscaped, kStEvent, 0.0, 1.0, 1.0, 0.0, 0.0, 0.0);
+      set_result(o, kOutEscaped, kStCreep, 0.0, 1.0, 1.0, 0.0, 0.0, 0.0);
       return true;
     }
     if (!skip) {

@@ -446,7 +446,7 @@ KT_HD int sm_trace(const Frame& f, const SmPrm<double>& P, const double* y_in, c
       // controller's eventual failure would give it
       o->steps = (uint32_t)it + 1;
       o->attempts = attempts;
-      set_result(o, kOutEscaped, kStEvent, 0.0, 1.0, 1.0, 0.0, 0.0, 0.0);
+      set_result(o, kOutEscaped, kStCreep, 0.0, 1.0, 1.0, 0.0, 0.0, 0.0);
       return 0;
     }
     if (!skip) horizon_escape(prev_r, r_now, f.rh_cut, f.r_esc, &best_alpha, &evt);

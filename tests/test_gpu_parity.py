@@ -44,12 +44,34 @@ def test_kernel_matches_reference_fixtures(renderer, name):
          height=128),                                                           # config 5 at 1/16
 ], ids=["cfg1_full", "cfg2_160x90", "cfg3_96x54", "cfg5_128"])
 def test_kernel_matches_oracle_medium(renderer, kw):
+    """Every field bit-identical to the oracle; the step and attempt counters
+    too, except on bundle rays stopped while creeping onto the horizon
+    (status KT_RAY_CREEP), whose counters stop early."""
     d = abi.frame_desc(**kw)
+    got = trace(renderer, d)
+    want = O.trace_port(d, counters=True)
+    assert G.mismatches(got, want) == {k: 0 for k in G.FIELDS}
+    ok, creeping = O.counters_agree(got, want)
+    assert ok
+    assert (creeping > 0) == bool(kw.get("bundles"))
+
+
+def test_bundle_full_creep_counters_match_oracle(renderer):
+    """With KT_FLAG_BUNDLE_FULL_CREEP the bundle rays creeping onto the
+    horizon are traced on to the reference's reject or step cap: config 3's
+    geometry at 96x54, records and counters bit-identical to the oracle, and
+    the records equal to the default trace's (which stops those rays early)."""
+    kw = dict(chart=1, bundles=1, a=0.998, theta_deg=60.0, width=96, height=54)
+    d = abi.frame_desc(flags=abi.KT_FLAG_BUNDLE_FULL_CREEP, **kw)
     got = trace(renderer, d)
     want = O.trace_port(d, counters=True)
     assert G.mismatches(got, want) == {k: 0 for k in G.FIELDS}
     assert np.array_equal(got["steps"], want["steps"])
     assert np.array_equal(got["attempts"], want["attempts"])
+    assert not np.any(got["status"] == abi.KT_RAY_CREEP)
+    early = trace(renderer, abi.frame_desc(**kw))
+    assert G.mismatches(early, got) == {k: 0 for k in G.FIELDS}
+    assert np.any(early["status"] == abi.KT_RAY_CREEP)
 
 
 CFG2_720P = dict(chart=1, integrator=1, tol=1e-10, a=0.9, Q=0.3, Lambda=1e-4, r_obs=60.0,
@@ -87,7 +109,8 @@ def test_full_720p_frame_against_oracle(renderer):
 def test_full_size_frames_against_oracle(renderer, kw, stride):
     """Config 5 at full size, every pixel, and config 3 (Jacobi bundles) at
     full size on every 16th pixel (129,600 bundle rays): all fields and the
-    counters bit-identical to the oracle."""
+    counters bit-identical to the oracle (on bundle rays stopped while
+    creeping onto the horizon, counters no larger)."""
     d = abi.frame_desc(**kw)
     a = trace(renderer, d)
     pix = np.arange(0, d.width * d.height, stride, dtype=np.uint32)

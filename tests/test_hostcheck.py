@@ -85,13 +85,17 @@ def test_bundle_rhs_split_matches_reference(hc, name, shape):
     assert G.mismatches(got, G.result(name)) == {k: 0 for k in G.FIELDS}
 
 
-def test_bundle_rhs_split_matches_oracle_medium(hc):
+@pytest.mark.parametrize("full_creep", [False, True], ids=["creep_end", "full_creep"])
+def test_bundle_rhs_split_matches_oracle_medium(hc, full_creep):
     """Config 3's geometry at 96x54 through the split bundle RHS on the host:
-    all fields and the counters bit-identical to the oracle."""
+    all fields bit-identical to the oracle; the counters too, but for the
+    rays stopped while creeping onto the horizon (status KT_RAY_CREEP, whose
+    counters stop early), and for every ray with KT_FLAG_BUNDLE_FULL_CREEP."""
     import oracle_lib as O
     from kerrtracecpp2_b200 import abi
 
-    d = abi.frame_desc(chart=1, bundles=1, a=0.998, theta_deg=60.0, width=96, height=54)
+    d = abi.frame_desc(chart=1, bundles=1, a=0.998, theta_deg=60.0, width=96, height=54,
+                       flags=abi.KT_FLAG_BUNDLE_FULL_CREEP if full_creep else 0)
     hc.hc_set_bundle_split.argtypes = [ctypes.c_int]
     hc.hc_set_bundle_split(1)
     try:
@@ -100,4 +104,14 @@ def test_bundle_rhs_split_matches_oracle_medium(hc):
         hc.hc_set_bundle_split(0)
     want = O.trace_port(d, counters=True)
     assert G.mismatches(got, want) == {k: 0 for k in G.FIELDS}
-    assert np.array_equal(got["steps"], want["steps"]) and np.array_equal(got["attempts"], want["attempts"])
+    ok, creeping = O.counters_agree(got, want)
+    assert ok
+    if full_creep:
+        assert creeping == 0
+        assert np.array_equal(got["steps"], want["steps"]) and np.array_equal(got["attempts"], want["attempts"])
+    else:
+        assert creeping > 0  # this frame has rays plunging near the equator
+        creep = got["status"] == abi.KT_RAY_CREEP
+        assert np.all(got["outcome"][creep] == 0) and np.all(got["r"][creep] == 0.0)
+        print(f"{creeping} creeping rays; attempts {got['attempts'].sum()} against the "
+              f"oracle's {want['attempts'].sum()}")
