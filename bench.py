@@ -1117,6 +1117,7 @@ def main():
         got = {k: out[k].cpu().numpy() for k in O.GEO_FIELDS}
         got["steps"] = out["steps"].cpu().numpy().view(np.uint32)
         got["attempts"] = out["attempts"].cpu().numpy().view(np.uint32)
+        got["status"] = out["status"].cpu().numpy()  # creeping bundle rays: counters stop early
         parity = dict(O.parity_report(got, want, desc.width, desc.height, pix=pix),
                       oracle="oracle/kt_oracle.c (strict: no contraction, the renderer's libm; "
                              "bit-identical to the reference built that way on every golden fixture)",
