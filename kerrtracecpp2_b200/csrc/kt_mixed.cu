@@ -150,7 +150,20 @@ struct ModeBundleMixed {
 // RK4: 25.2 against 41.1; KS RK4: 22.3 against 52.1; 1080p bundles: 224
 // against 243).
 template <bool B> struct Shape<ModeBLRk4MixedT<B>> { static constexpr int kBlock = 64, kMinBlocks = 9, kRefill = 32; };
-template <bool B> struct Shape<ModeBLDopri5MixedT<B>> { static constexpr int kBlock = 64, kMinBlocks = 9, kRefill = 32; };
+#ifndef KT_MIXED32_DOPRI5_BLOCK
+#define KT_MIXED32_DOPRI5_BLOCK 64
+#endif
+#ifndef KT_MIXED32_DOPRI5_MINB
+#define KT_MIXED32_DOPRI5_MINB 9
+#endif
+#ifndef KT_MIXED32_DOPRI5_REFILL
+#define KT_MIXED32_DOPRI5_REFILL 32
+#endif
+template <bool B> struct Shape<ModeBLDopri5MixedT<B>> {
+  static constexpr int kBlock = B ? KT_MIXED32_DOPRI5_BLOCK : 64,
+                       kMinBlocks = B ? KT_MIXED32_DOPRI5_MINB : 9,
+                       kRefill = B ? KT_MIXED32_DOPRI5_REFILL : 32;
+};
 template <bool B> struct Shape<ModeKSRk4MixedT<B>> { static constexpr int kBlock = 64, kMinBlocks = 9, kRefill = 32; };
 template <> struct Shape<ModeBundleMixed> { static constexpr int kBlock = 128, kMinBlocks = 1, kRefill = 32; };
 
