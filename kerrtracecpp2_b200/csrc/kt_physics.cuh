@@ -341,17 +341,9 @@ KT_HD Inv bl_inv_mx(const Metric& g, double r, double th) {
 // dR/dr = 2r(1 - L r^2/3) - (2L r/3) A - 2M, dS/dth = -2a^2 s c,
 // dT/dth = -(2 L a^2/3) s c, d(s2)/dth = 2 s c.  One evaluation, four
 // reciprocals; T is float (far field) or double.  k as bl_rhs.
-#ifndef KT_MIXED_RHS_INLINE
-#define KT_MIXED_RHS_INLINE 1
-#endif
-#if KT_MIXED_RHS_INLINE
-#define KT_MIXED_RHS KT_HD
-#else
-#define KT_MIXED_RHS KT_HD_CALL
-#endif
 template <class T>
-KT_MIXED_RHS void bl_rhs_analytic(const Metric& g, double r_, double th_, double pr_, double pth_,
-                                  double pt_, double pphi_, double k[5]) {
+KT_HD void bl_rhs_analytic(const Metric& g, double r_, double th_, double pr_, double pth_,
+                           double pt_, double pphi_, double k[5]) {
   const T r = (T)r_, pr = (T)pr_, pth = (T)pth_, pt = (T)pt_, pphi = (T)pphi_;
   const T a = (T)g.a, a2 = (T)g.a2, L = (T)g.L, M = (T)g.M, Q2 = (T)g.Q2, xi2 = (T)g.xi2;
   T sn, c;
