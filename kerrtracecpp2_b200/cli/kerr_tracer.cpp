@@ -167,6 +167,9 @@ int main(int argc, char** argv) {
       return argv[++i];
     };
     if (a == "--bundles") d.bundles = 1;
+    // extension: trace bundle rays creeping onto the horizon to the
+    // reference's reject or step cap (its step counts; same image either way)
+    else if (a == "--bundle-full-creep") d.flags |= KT_FLAG_BUNDLE_FULL_CREEP;
     else if (a == "--dopri5") d.integrator = KT_DOPRI5;
     else if (a == "--max-steps") d.max_steps = std::max(1, atoi(next()));
     else if (a == "--step-init" || a == "--step-size") d.step_init = atof(next());
