@@ -170,7 +170,12 @@ template <> struct Shape<struct ModeBLRk4> { static constexpr int kBlock = 64, k
 #ifndef KT_BL_DOPRI5_MINB
 #define KT_BL_DOPRI5_MINB 9
 #endif
-template <> struct Shape<struct ModeBLDopri5> { static constexpr int kBlock = 64, kMinBlocks = KT_BL_DOPRI5_MINB, kRefill = 32; };
+#ifndef KT_BL_DOPRI5_REFILL
+#define KT_BL_DOPRI5_REFILL 32
+#endif
+template <> struct Shape<struct ModeBLDopri5> {
+  static constexpr int kBlock = 64, kMinBlocks = KT_BL_DOPRI5_MINB, kRefill = KT_BL_DOPRI5_REFILL;
+};
 template <> struct Shape<struct ModeKSRk4> { static constexpr int kBlock = 64, kMinBlocks = 9, kRefill = 32; };
 template <> struct Shape<struct ModeBundle> { static constexpr int kBlock = 128, kMinBlocks = 1, kRefill = 16; };
 // Paired bundles: 64 rays per 128-thread block; kRefill counts lanes.
