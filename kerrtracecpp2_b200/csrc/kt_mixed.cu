@@ -150,11 +150,13 @@ struct ModeBundleMixed {
 // RK4: 25.2 against 41.1; KS RK4: 22.3 against 52.1; 1080p bundles: 224
 // against 243).
 template <bool B> struct Shape<ModeBLRk4MixedT<B>> { static constexpr int kBlock = 64, kMinBlocks = 9, kRefill = 32; };
-// With the FP32 right-hand side on, a warp refills once 16 lanes are idle
-// (measured at 720p, tol 1e-8: 21.2 ms against 22.3 with 32; block and
-// minimum blocks are shared by both instantiations, see launch_shape_mixed).
+// A warp refills once all 32 lanes are idle, so its rays are always the same
+// 32 consecutive rays of the queue and the per-warp FP32 choice does not
+// depend on the schedule (refilling at 16 idle lanes measured 21.2 ms
+// against 22.3 at 720p, tol 1e-8, but mixes the groups).  Block and minimum
+// blocks are shared by both instantiations (see launch_shape_mixed).
 #ifndef KT_MIXED32_DOPRI5_REFILL
-#define KT_MIXED32_DOPRI5_REFILL 16
+#define KT_MIXED32_DOPRI5_REFILL 32
 #endif
 template <bool B> struct Shape<ModeBLDopri5MixedT<B>> {
   static constexpr int kBlock = 64, kMinBlocks = 9, kRefill = B ? KT_MIXED32_DOPRI5_REFILL : 32;
