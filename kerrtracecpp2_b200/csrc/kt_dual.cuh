@@ -232,140 +232,4 @@ KT_HD void sm_sincos(const HDual& x, HDual* s, HDual* c) {
   *c = HDual(cv, -sv * x.a, -sv * x.b, -sv * x.c - cv * ab);
 }
 
-// One evaluation carrying a Dual<1> (tangent d) and two hyper-duals (pairs
-// a[k], b[k] with cross part c[k], k = 0, 1) that share a value:
-//   x = v + d e + sum_k (a_k e1k + b_k e2k + c_k e1k e2k),
-// products of different infinitesimals dropped.  Each part follows, operation
-// for operation, the rule of the type it stands for (the d part Dual<1>'s,
-// the others HDual's), so its results equal those of the three separate
-// evaluations bit for bit, at the cost of one value and one reciprocal.
-struct BDual {
-  double v, d, a[2], b[2], c[2];
-  KT_HD BDual() {}
-  KT_HD BDual(double x) : v(x), d(0.0) {
-    for (int k = 0; k < 2; ++k) a[k] = b[k] = c[k] = 0.0;
-  }
-};
-KT_HD double val(const BDual& x) { return x.v; }
-KT_HD BDual operator+(const BDual& x, const BDual& y) {
-  BDual r;
-  r.v = x.v + y.v;
-  r.d = x.d + y.d;
-  for (int k = 0; k < 2; ++k) {
-    r.a[k] = x.a[k] + y.a[k];
-    r.b[k] = x.b[k] + y.b[k];
-    r.c[k] = x.c[k] + y.c[k];
-  }
-  return r;
-}
-KT_HD BDual operator-(const BDual& x, const BDual& y) {
-  BDual r;
-  r.v = x.v - y.v;
-  r.d = x.d - y.d;
-  for (int k = 0; k < 2; ++k) {
-    r.a[k] = x.a[k] - y.a[k];
-    r.b[k] = x.b[k] - y.b[k];
-    r.c[k] = x.c[k] - y.c[k];
-  }
-  return r;
-}
-KT_HD BDual operator-(const BDual& x) {
-  BDual r;
-  r.v = -x.v;
-  r.d = -x.d;
-  for (int k = 0; k < 2; ++k) {
-    r.a[k] = -x.a[k];
-    r.b[k] = -x.b[k];
-    r.c[k] = -x.c[k];
-  }
-  return r;
-}
-KT_HD BDual operator*(const BDual& x, const BDual& y) {
-  BDual r;
-  r.v = x.v * y.v;
-  r.d = x.d * y.v + x.v * y.d;
-  for (int k = 0; k < 2; ++k) {
-    r.a[k] = x.a[k] * y.v + x.v * y.a[k];
-    r.b[k] = x.b[k] * y.v + x.v * y.b[k];
-    r.c[k] = x.c[k] * y.v + x.v * y.c[k] + x.a[k] * y.b[k] + x.b[k] * y.a[k];
-  }
-  return r;
-}
-KT_HD BDual operator+(const BDual& x, double y) {
-  BDual r = x;
-  r.v = x.v + y;
-  return r;
-}
-KT_HD BDual operator+(double x, const BDual& y) { return y + x; }
-KT_HD BDual operator-(const BDual& x, double y) {
-  BDual r = x;
-  r.v = x.v - y;
-  return r;
-}
-KT_HD BDual operator-(double x, const BDual& y) {
-  BDual r = -y;
-  r.v = x - y.v;
-  return r;
-}
-KT_HD BDual operator*(const BDual& x, double y) {
-  BDual r;
-  r.v = x.v * y;
-  r.d = x.d * y;
-  for (int k = 0; k < 2; ++k) {
-    r.a[k] = x.a[k] * y;
-    r.b[k] = x.b[k] * y;
-    r.c[k] = x.c[k] * y;
-  }
-  return r;
-}
-KT_HD BDual operator*(double x, const BDual& y) { return y * x; }
-KT_HD BDual operator/(const BDual& x, double y) {
-  BDual r;
-  r.v = x.v / y;
-  r.d = x.d / y;
-  for (int k = 0; k < 2; ++k) {
-    r.a[k] = x.a[k] / y;
-    r.b[k] = x.b[k] / y;
-    r.c[k] = x.c[k] / y;
-  }
-  return r;
-}
-// x / y: the d part as Dual<1>'s division, the pairs as HDual's
-KT_HD BDual operator/(double x, const BDual& y) {
-  BDual r;
-  r.v = x / y.v;
-  const double s = (x == 1.0) ? -(r.v * r.v) : -r.v / y.v;
-  r.d = s * y.d;
-  const double iy = 1.0 / y.v;
-  const double f1 = -r.v * iy;
-  const double f2 = -2.0 * f1 * iy;
-  for (int k = 0; k < 2; ++k) {
-    r.a[k] = f1 * y.a[k];
-    r.b[k] = f1 * y.b[k];
-    r.c[k] = f1 * y.c[k] + f2 * y.a[k] * y.b[k];
-  }
-  return r;
-}
-KT_HD bool operator<(const BDual& x, double y) { return x.v < y; }
-KT_HD bool operator>(const BDual& x, double y) { return x.v > y; }
-KT_HD bool operator<=(const BDual& x, double y) { return x.v <= y; }
-KT_HD bool operator>=(const BDual& x, double y) { return x.v >= y; }
-KT_HD void sm_sincos(const BDual& x, BDual* s, BDual* c) {
-  double sv, cv;
-  ktm_sincos(x.v, &sv, &cv);
-  s->v = sv;
-  c->v = cv;
-  s->d = cv * x.d;
-  c->d = -sv * x.d;
-  for (int k = 0; k < 2; ++k) {
-    const double ab = x.a[k] * x.b[k];
-    s->a[k] = cv * x.a[k];
-    s->b[k] = cv * x.b[k];
-    s->c[k] = cv * x.c[k] - sv * ab;
-    c->a[k] = -sv * x.a[k];
-    c->b[k] = -sv * x.b[k];
-    c->c[k] = -sv * x.c[k] - cv * ab;
-  }
-}
-
 }  // namespace kt

@@ -581,59 +581,35 @@ KT_HD void sm_ctl_partials(double err, double tol, double h, double* dh, double*
 // the constants and (a, Q, Lambda) the matching mixed derivatives: one
 // Dual<1> evaluation of grad H along d, and per column one hyper-dual
 // evaluation at z + e1 W_k + e2 d_k (its e2 part is Hess(H) d_k, its e1 e2
-// part D^3 H[., W_k, d_k]), carried together in one BDual evaluation.  A
-// zero column cotangent contributes nothing.
+// part D^3 H[., W_k, d_k]).  A zero column cotangent skips its evaluation.
 template <class C>
 KT_HD_CALL void sm_vjp_f(double M, const SmPrm<double>& P, const double* u, const double* c,
                          const double* v, double* ubar, double* cbar, double* pbar) {
   if constexpr (C::kBundle) {
-    bool use[2];
-    double dk[2][4];
+    sm_vjp_f<ChartBL>(M, P, u, c, v, ubar, cbar, pbar);
+    SmPrm<HDual> Ph;
+    Ph.a = HDual(P.a);
+    Ph.Q = HDual(P.Q);
+    Ph.L = HDual(P.L);
+    KT_ROLLED
     for (int k = 0; k < 2; ++k) {
       const double w0 = v[4 + k], w1 = v[6 + k], w2 = v[8 + k], w3 = v[10 + k];
-      use[k] = !(w0 == 0.0 && w1 == 0.0 && w2 == 0.0 && w3 == 0.0);
-      dk[k][0] = -w2;
-      dk[k][1] = -w3;
-      dk[k][2] = w0;
-      dk[k][3] = w1;
-    }
-    if (!use[0] && !use[1]) {
-      sm_vjp_f<ChartBL>(M, P, u, c, v, ubar, cbar, pbar);
-      for (int i = 0; i < 8; ++i) ubar[4 + i] = 0.0;
-      return;
-    }
-    // the three evaluations in one (BDual: the Dual<1> along d and the two
-    // hyper-duals share the value and the reciprocals), bit for bit the same
-    BDual yb[4], cb[2], gy[4], gc[2], gp[kSmPrm];
-    SmPrm<BDual> Pb;
-    Pb.a = BDual(P.a);
-    Pb.Q = BDual(P.Q);
-    Pb.L = BDual(P.L);
-    for (int i = 0; i < 4; ++i) {
-      yb[i] = BDual(u[i]);
-      yb[i].d = i < 2 ? -v[2 + i] : v[i - 2];
-      for (int k = 0; k < 2; ++k) {
-        yb[i].a[k] = u[4 + 2 * i + k];
-        yb[i].b[k] = use[k] ? dk[k][i] : 0.0;
-      }
-    }
-    cb[0] = BDual(c[0]);
-    cb[1] = BDual(c[1]);
-    ChartBL::grad<BDual, true>(M, Pb, yb, cb, gy, gc, gp);
-    for (int i = 0; i < 4; ++i) ubar[i] = gy[i].d;
-    for (int j = 0; j < 2; ++j) cbar[j] = cbar[j] + gc[j].d;
-    for (int q = 0; q < kSmPrm; ++q) pbar[q] = pbar[q] + gp[q].d;
-    for (int k = 0; k < 2; ++k) {
-      if (!use[k]) {
+      if (w0 == 0.0 && w1 == 0.0 && w2 == 0.0 && w3 == 0.0) {
         for (int i = 0; i < 4; ++i) ubar[4 + 2 * i + k] = 0.0;
         continue;
       }
+      const double dk[4] = {-w2, -w3, w0, w1};
+      HDual yh[4], ch[2], gy[4], gc[2], gp[kSmPrm];
+      for (int i = 0; i < 4; ++i) yh[i] = HDual(u[i], u[4 + 2 * i + k], dk[i], 0.0);
+      ch[0] = HDual(c[0]);
+      ch[1] = HDual(c[1]);
+      ChartBL::grad<HDual, true>(M, Ph, yh, ch, gy, gc, gp);
       for (int i = 0; i < 4; ++i) {
-        ubar[i] = ubar[i] + gy[i].c[k];
-        ubar[4 + 2 * i + k] = gy[i].b[k];
+        ubar[i] = ubar[i] + gy[i].c;
+        ubar[4 + 2 * i + k] = gy[i].b;
       }
-      for (int j = 0; j < 2; ++j) cbar[j] = cbar[j] + gc[j].c[k];
-      for (int q = 0; q < kSmPrm; ++q) pbar[q] = pbar[q] + gp[q].c[k];
+      for (int j = 0; j < 2; ++j) cbar[j] = cbar[j] + gc[j].c;
+      for (int q = 0; q < kSmPrm; ++q) pbar[q] = pbar[q] + gp[q].c;
     }
   } else {
     Dual<1> yd[C::kN], cd[C::kC], gy[C::kN], gc[C::kC], gp[kSmPrm];

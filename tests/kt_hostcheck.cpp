@@ -360,83 +360,3 @@ extern "C" int hc_smooth_pixels(const kt_frame_desc* d, int64_t n, const uint32_
                             t_r, nullptr, w_g, w_r, 0.0, outcome, r, red, nullptr, phi_disk, th_esc,
                             ph_esc, steps, attempts, contrib);
 }
-
-// The bundle VJP of the right-hand side as three separate evaluations (a
-// Dual<1> along d = J^T v_z and one HDual per column of W), the form that
-// sm_vjp_f<ChartBLB> carries in a single BDual evaluation: n random states
-// (r, theta, p_r, p_theta, W), constants and cotangents (a column's
-// cotangent zeroed on some of them); returns the number of differing bits
-// patterns between the two forms over all outputs.
-namespace {
-void vjp_bundle_separate(double M, const SmPrm<double>& P, const double* u, const double* c,
-                         const double* v, double* ubar, double* cbar, double* pbar) {
-  sm_vjp_f<ChartBL>(M, P, u, c, v, ubar, cbar, pbar);
-  SmPrm<HDual> Ph;
-  Ph.a = HDual(P.a);
-  Ph.Q = HDual(P.Q);
-  Ph.L = HDual(P.L);
-  for (int k = 0; k < 2; ++k) {
-    const double w0 = v[4 + k], w1 = v[6 + k], w2 = v[8 + k], w3 = v[10 + k];
-    if (w0 == 0.0 && w1 == 0.0 && w2 == 0.0 && w3 == 0.0) {
-      for (int i = 0; i < 4; ++i) ubar[4 + 2 * i + k] = 0.0;
-      continue;
-    }
-    const double dk[4] = {-w2, -w3, w0, w1};
-    HDual yh[4], ch[2], gy[4], gc[2], gp[kSmPrm];
-    for (int i = 0; i < 4; ++i) yh[i] = HDual(u[i], u[4 + 2 * i + k], dk[i], 0.0);
-    ch[0] = HDual(c[0]);
-    ch[1] = HDual(c[1]);
-    ChartBL::grad<HDual, true>(M, Ph, yh, ch, gy, gc, gp);
-    for (int i = 0; i < 4; ++i) {
-      ubar[i] = ubar[i] + gy[i].c;
-      ubar[4 + 2 * i + k] = gy[i].b;
-    }
-    for (int j = 0; j < 2; ++j) cbar[j] = cbar[j] + gc[j].c;
-    for (int q = 0; q < kSmPrm; ++q) pbar[q] = pbar[q] + gp[q].c;
-  }
-}
-
-uint64_t bits_of(double x) {
-  uint64_t b;
-  memcpy(&b, &x, sizeof b);
-  return b;
-}
-}  // namespace
-
-extern "C" int64_t hc_bundle_vjp_compare(int64_t n, uint64_t seed) {
-  uint64_t s = seed * 6364136223846793005ULL + 1442695040888963407ULL;
-  auto uni = [&s](double lo, double hi) {
-    s = s * 6364136223846793005ULL + 1442695040888963407ULL;
-    return lo + (hi - lo) * ((double)(s >> 11) * (1.0 / 9007199254740992.0));
-  };
-  int64_t bad = 0;
-  for (int64_t t = 0; t < n; ++t) {
-    const double M = 1.0;
-    SmPrm<double> P;
-    P.a = uni(0.0, 0.998);
-    P.Q = uni(0.0, 0.3);
-    P.L = uni(0.0, 1e-4);
-    double u[12], c[2], v[12];
-    u[0] = uni(2.0, 60.0);
-    u[1] = uni(0.2, 2.9);
-    u[2] = uni(-2.0, 2.0);
-    u[3] = uni(-10.0, 10.0);
-    for (int i = 4; i < 12; ++i) u[i] = uni(-5.0, 5.0);
-    c[0] = -1.0;
-    c[1] = uni(-5.0, 5.0);
-    for (int i = 0; i < 12; ++i) v[i] = uni(-1.0, 1.0);
-    const int zero = (int)(t % 4);  // 0: none, 1: column 0, 2: column 1, 3: both
-    for (int i = 0; i < 4; ++i) {
-      if (zero & 1) v[4 + 2 * i] = 0.0;
-      if (zero & 2) v[5 + 2 * i] = 0.0;
-    }
-    double ua[12], ca[2] = {0.1, 0.2}, pa[3] = {0.3, 0.4, 0.5};
-    double ub[12], cb[2] = {0.1, 0.2}, pb[3] = {0.3, 0.4, 0.5};
-    sm_vjp_f<ChartBLB>(M, P, u, c, v, ua, ca, pa);
-    vjp_bundle_separate(M, P, u, c, v, ub, cb, pb);
-    for (int i = 0; i < 12; ++i) bad += bits_of(ua[i]) != bits_of(ub[i]);
-    for (int j = 0; j < 2; ++j) bad += bits_of(ca[j]) != bits_of(cb[j]);
-    for (int q = 0; q < 3; ++q) bad += bits_of(pa[q]) != bits_of(pb[q]);
-  }
-  return bad;
-}

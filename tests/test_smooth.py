@@ -383,19 +383,3 @@ def test_gradient_against_reference_renderer_differences():
         rel = abs(adj[k] - slope) / abs(slope)
         print(f"{k}: adjoint {adj[k]:.6g} reference slope {slope:.6g} rel {rel:.1e}")
         assert rel < 0.5
-
-
-def test_bundle_vjp_single_evaluation_equals_three():
-    """The bundle right-hand side's VJP carries the Dual<1> of the geodesic
-    part and the two hyper-duals of W's columns in one BDual evaluation; on
-    40,000 random states, constants and cotangents (columns zeroed in turn)
-    every output equals the three separate evaluations bit for bit."""
-    import ctypes
-
-    import testlibs
-
-    L = ctypes.CDLL(testlibs.HOSTCHECK)
-    L.hc_bundle_vjp_compare.argtypes = [ctypes.c_int64, ctypes.c_uint64]
-    L.hc_bundle_vjp_compare.restype = ctypes.c_int64
-    assert L.hc_bundle_vjp_compare(20000, 1) == 0
-    assert L.hc_bundle_vjp_compare(20000, 7) == 0
