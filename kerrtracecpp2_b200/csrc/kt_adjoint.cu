@@ -34,8 +34,15 @@ constexpr int kSumThreads = 256;
 // Rays: pixels 0..n-1, or list[0..*n_dev) (a count on the device) or
 // list[0..n_list) (on the host).  The KS kernel appends the rays
 // whose KS initialisation fails to fb_pix (count *fb_n) for the BL kernel.
+// Minimum blocks per SM of the gradient kernels, measured (ms per gradient,
+// unconstrained / 6 / 8 blocks of 64 threads): config 5 48 / 58 / 80, the
+// 720p DOPRI5 frame 156 / 195 / 233, the 960x540 bundle frame 623 / 596 /
+// 657.  Only the bundle kernel takes the bound.
+template <class C, bool kGrad>
+constexpr int sm_min_blocks() { return (kGrad && C::kBundle) ? 6 : 1; }
+
 template <class C, bool kGrad, class I>
-__global__ void __launch_bounds__(kSmBlock) k_smooth(const Frame f, const OutSoA out, const SmJob job,
+__global__ void __launch_bounds__(kSmBlock, (sm_min_blocks<C, kGrad>())) k_smooth(const Frame f, const OutSoA out, const SmJob job,
                                                      uint32_t n, const uint32_t* __restrict__ list,
                                                      uint32_t n_list,
                                                      const uint32_t* __restrict__ n_dev,
