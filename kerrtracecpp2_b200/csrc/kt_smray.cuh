@@ -405,7 +405,7 @@ KT_HD int sm_trace(const Frame& f, const SmPrm<double>& P, const double* y_in, c
         const double r_hit = C::radius(f.g.a, yh);
         if (r_hit >= f.r_in && r_hit <= f.r_out) {
           double red, pph;
-          if (C::kN == 6) {
+          if constexpr (C::kN == 6) {
             pph = yh[0] * yh[4] - yh[1] * yh[3];
           } else {
             pph = c[C::kC - 1];
@@ -936,7 +936,11 @@ KT_HD void sm_event_bwd(const Frame& f, const SmPrm<double>& P, const double* c,
   Pd.Q = D::var(P.Q, ng + C::kC + 1);
   Pd.L = D::var(P.L, ng + C::kC + 2);
   const D r = C::radius(Pd.a, yh);
-  const D pph = (n == 6) ? yh[0] * yh[4] - yh[1] * yh[3] : cd[C::kC - 1];
+  D pph;
+  if constexpr (n == 6)
+    pph = yh[0] * yh[4] - yh[1] * yh[3];  // KS: L_z = X p_Y - Y p_X
+  else
+    pph = cd[C::kC - 1];
   D red;
   bool has;
   if constexpr (C::kBundle)
@@ -1396,7 +1400,11 @@ KT_HD bool sm_trace_t(const Frame& f, const SmPrm<T1>& P, const T1* y_in, const 
         for (int i = 0; i < C::kN; ++i) yh[i] = sm_hermite_h(yp[i], y[i], kprev[i], k1[i], step_used, al);
         const T1 r_hit = C::radius(P.a, yh);
         if (r_hit.v >= f.r_in && r_hit.v <= f.r_out) {
-          const T1 pph = (C::kN == 6) ? yh[0] * yh[4] - yh[1] * yh[3] : c[C::kC - 1];
+          T1 pph;
+          if constexpr (C::kN == 6)
+            pph = yh[0] * yh[4] - yh[1] * yh[3];
+          else
+            pph = c[C::kC - 1];
           T1 red;
           deriv = sm_redshift<T1>(M, P, r_hit, c[0], pph, &red) ? 1 : 0;
           if (!(red.v > 0.0 && red.v < 20.0)) deriv = 0;
