@@ -10,6 +10,7 @@
 #include "kt_adjoint.h"
 #include "kt_context.h"
 #include "kt_frame.h"
+#include "kt_internal.h"
 
 using namespace ktc;
 
@@ -29,8 +30,8 @@ struct EventPair {
 // force_bl: trace every ray in the BL chart; tangent_dir >= 0: forward-mode
 // tangent along that parameter instead of the reverse sweep.
 kt_status grad_pass(kt_context* ctx, const kt::Frame& f, const kt::OutSoA& out, uint32_t n,
-                    const uint32_t* pix, uint32_t n_pix, const kt::SmCot& cot, bool force_bl,
-                    int tangent_dir, cudaStream_t st, double* sums, float* ms) {
+                    const uint32_t* pix, uint32_t n_pix, bool whole, const kt::SmCot& cot,
+                    bool force_bl, int tangent_dir, cudaStream_t st, double* sums, float* ms) {
   kt::SmJob job;
   job.cot = cot;
   job.force_bl = force_bl ? 1 : 0;
@@ -44,7 +45,8 @@ kt_status grad_pass(kt_context* ctx, const kt::Frame& f, const kt::OutSoA& out, 
   KT_CUDA(ctx, cudaMemsetAsync(ctx->d_counters, 0, 4 * sizeof(uint32_t), st), "reset queue");
   KT_CUDA(ctx, cudaEventRecord(ev.a, st), "event");
   // with a pixel list only the listed pixels' contributions are written
-  if (pix)
+  // (a whole frame in centre-out order writes every pixel's)
+  if (pix && !whole)
     KT_CUDA(ctx, cudaMemsetAsync(ctx->d_grad, 0, (size_t)n * kt::kGSlots * sizeof(double), st),
             "clear contributions");
   KT_CUDA(ctx, kt::launch_smooth(f, out, n, &job, ctx->d_counters, ctx->d_fb, ctx->device, st),
@@ -87,9 +89,23 @@ kt_status grad_run(kt_context* ctx, const kt_frame_desc* desc_in, const uint32_t
   kt::OutSoA out;
   memset(&out, 0, sizeof out);
   if (out_soa) out = to_out(out_soa);
+  // a whole frame of at least kOrderMinPixels pixels in centre-out order, as
+  // kt_trace traces it (the expensive rays by the critical curve first); the
+  // contributions are per pixel and summed in pixel order either way
+  bool whole = false;
+  if (!pix && n >= kt::kOrderMinPixels) {
+    const size_t words = (size_t)n + kt::ring_scratch_words((uint32_t)n);
+    r = ensure(ctx, (void**)&ctx->d_order, &ctx->order_cap, words * sizeof(uint32_t), "ray order");
+    if (r != KT_OK) return r;
+    KT_CUDA(ctx, kt::launch_ring_order(desc.width, desc.height, 0, ctx->d_order + n, ctx->d_order, st),
+            "ray order");
+    pix = ctx->d_order;
+    n_pix = (int64_t)n;
+    whole = true;
+  }
   double s[kt::kGSlots], sl[kt::kGSlots];
   float ms = 0.f, ms_l = 0.f;
-  r = grad_pass(ctx, f, out, (uint32_t)n, pix, (uint32_t)n_pix, cot, false, -1, st, s, &ms);
+  r = grad_pass(ctx, f, out, (uint32_t)n, pix, (uint32_t)n_pix, whole, cot, false, -1, st, s, &ms);
   if (r != KT_OK) return r;
   double lambda = s[kt::kGLambda];
   if (f.chart == KT_CHART_KS) {
@@ -98,7 +114,7 @@ kt_status grad_run(kt_context* ctx, const kt_frame_desc* desc_in, const uint32_t
       kt::OutSoA none;
       memset(&none, 0, sizeof none);
       // one derivative in the BL chart: forward-mode tangent along Lambda
-      r = grad_pass(ctx, f, none, (uint32_t)n, pix, (uint32_t)n_pix, cot, true, kt::kGLambda, st,
+      r = grad_pass(ctx, f, none, (uint32_t)n, pix, (uint32_t)n_pix, whole, cot, true, kt::kGLambda, st,
                     sl, &ms_l);
       if (r != KT_OK) return r;
       lambda = sl[kt::kGLambda];
