@@ -1,10 +1,12 @@
-"""Central-difference check of the config-5 gradient on the GPU (shared by
+"""Central-difference check of a gradient on the GPU (shared by
 tests/test_gpu_grad.py and bench.py's adjoint leg).
 
-The frame: 512x512 KS, a=0.7, Q=0.1, theta=70, r_obs=50, disk ISCO-15,
-tol 1e-7; the loss: sum over the disk pixels of both frames of
+The default frame (config 5): 512x512 KS, a=0.7, Q=0.1, theta=70, r_obs=50,
+disk ISCO-15, tol 1e-7; the loss: sum over the disk pixels of both frames of
 w_g (g - g_t)^2 + w_r (r_hit - r_t)^2 against the smooth tracer at a=0.72,
-theta=71.  The adjoint (kt_vjp with the loss's cotangents) is compared with
+theta=71.  CFG2_DOPRI5 (the DOPRI5 adjoint) and BUNDLE (the Jacobi-bundle
+adjoint, its loss with w_m (magnif - magnif_t)^2 as well) use the same
+check.  The adjoint (kt_vjp with the loss's cotangents) is compared with
 central differences of the same loss, restricted to the pixels on which the
 stencil renders lie on one smooth piece of the point-sampled image (a pixel
 that changes class, step or attempt count is a discontinuity of the image,
