@@ -74,6 +74,27 @@ def test_bundle_full_creep_counters_match_oracle(renderer):
     assert np.any(early["status"] == abi.KT_RAY_CREEP)
 
 
+@pytest.mark.parametrize("kw", [
+    dict(chart=1, bundles=1, a=0.998, theta_deg=60.0, width=960, height=540),   # config 3, 1/4
+    dict(chart=1, bundles=1, a=0.9, Q=0.2, Lambda=1e-5, theta_deg=70.0, width=480, height=270),
+], ids=["cfg3_960x540", "knds_480x270"])
+def test_bundle_creep_end_keeps_every_record(renderer, kw):
+    """Whole bundle frames traced with and without KT_FLAG_BUNDLE_FULL_CREEP:
+    every record bit-identical; the rays stopped early carry status
+    KT_RAY_CREEP and no more steps or attempts than the full trace."""
+    full = trace(renderer, abi.frame_desc(flags=abi.KT_FLAG_BUNDLE_FULL_CREEP, **kw))
+    early = trace(renderer, abi.frame_desc(**kw))
+    assert G.mismatches(early, full) == {k: 0 for k in G.FIELDS}
+    creep = early["status"] == abi.KT_RAY_CREEP
+    print(f"{int(creep.sum())} of {creep.size} rays stopped creeping; attempts "
+          f"{int(early['attempts'].astype(np.int64).sum())} against {int(full['attempts'].astype(np.int64).sum())}")
+    assert creep.any()
+    assert np.all(early["steps"][creep] <= full["steps"][creep])
+    assert np.all(early["attempts"][creep] <= full["attempts"][creep])
+    for f in ("steps", "attempts", "status"):
+        assert np.array_equal(early[f][~creep], full[f][~creep]), f
+
+
 CFG2_720P = dict(chart=1, integrator=1, tol=1e-10, a=0.9, Q=0.3, Lambda=1e-4, r_obs=60.0,
                  theta_deg=85.0, fov_deg=30.0, disk_out=20.0, width=1280, height=720)
 
