@@ -41,6 +41,11 @@
 namespace kt {
 
 constexpr int kSmCkSteps = 32;  // accepted steps between checkpoints
+// Step starts the forward keeps (the last kSmRing of them): a ray of at most
+// that many accepted steps needs no replay in its reverse sweep.  A multiple
+// of kSmCkSteps; smaller for the bundle's 12-double state.
+template <int N>
+constexpr int sm_ring_steps() { return N >= 12 ? 128 : 256; }
 constexpr int kSmCkCap = 64;    // checkpoints per level
 constexpr int kSmMaxDoublings = 6;  // k up to 32 * 2^6: 131072 accepted steps
 
@@ -325,7 +330,8 @@ KT_HD void sm_stop(const Frame& f, const double* y, double pas, int status, uint
 
 // Trace one ray from (y, c, pas).  With ck != NULL, checkpoints are recorded
 // (*ck_k = final interval, *ck_n = count); with ring != NULL, step m's start
-// (y, dlam, attempts) is kept in ring[m % 32] (the last 32 steps).  On a disk hit `ev` receives the
+// (y, dlam, attempts) is kept in ring[m % R], R = sm_ring_steps (the last R
+// steps).  On a disk hit `ev` receives the
 // final step; returns the number of accepted steps N (0 if the ray ended
 // otherwise or more than 131072 steps were taken with recording on).
 template <class C, class I = SmRk4>
@@ -369,9 +375,10 @@ KT_HD int sm_trace(const Frame& f, const SmPrm<double>& P, const double* y_in, c
     kprevp = k1p;
     const double H_start = h;
     const uint32_t att0 = attempts;
+    constexpr int R = sm_ring_steps<C::kN>();
     if (ring) {
-      for (int i = 0; i < C::kN; ++i) ring[it % kSmCkSteps].y[i] = y[i];
-      ring[it % kSmCkSteps].H = h;
+      for (int i = 0; i < C::kN; ++i) ring[it % R].y[i] = y[i];
+      ring[it % R].H = h;
     }
     double step_used = h;
     int rejects = 0;
@@ -386,7 +393,7 @@ KT_HD int sm_trace(const Frame& f, const SmPrm<double>& P, const double* y_in, c
         return 0;
       }
     }
-    if (ring) ring[it % kSmCkSteps].na = (int)(attempts - att0);
+    if (ring) ring[it % R].na = (int)(attempts - att0);
     sm_rhs<C>(M, P, y, c, k1, &k1p);
     // events (main.cpp:1570-1657, 364-433)
     const double r_now = C::radius(f.g.a, y);
@@ -1004,7 +1011,7 @@ template <int N>
 struct SmScratch {
   SmCk<N> ck1[kSmCkCap];
   SmCk<N> ck2[kSmCkCap];
-  SmSt<N> st[kSmCkSteps];
+  SmSt<N> st[sm_ring_steps<N>()];  // the forward's ring; replays reuse st[0..31]
   SmStages<N> stages;
 };
 
@@ -1025,24 +1032,32 @@ KT_HD void sm_adjoint(const Frame& f, const SmPrm<double>& P, const double* c, c
   for (int i = 0; i < C::kN; ++i) ybar[i] = ybN[i];
   double Hbar = 0.0;
   bool last = true;
+  // Steps from N - R on are still in the forward's ring (step t at st[t % R];
+  // a sub-segment starts at a multiple of 32, so its entries are contiguous).
+  // Older sub-segments are replayed into st[0..31]: the reverse reaches them
+  // only after every ring entry has been used.
+  constexpr int R = sm_ring_steps<C::kN>();
+  const int in_ring = N - R;
   const int nseg = (N + k1 - 1) / k1;
   KT_ROLLED
   for (int sgi = nseg - 1; sgi >= 0; --sgi) {
     const int s0 = sgi * k1;
     const int len = (N - s0 < k1) ? N - s0 : k1;
     const int nsub = (len + kSmCkSteps - 1) / kSmCkSteps;
-    if (nsub > 1) sm_replay<C, I>(f, P, c, sc->ck1[sgi], len, nullptr, sc->ck2, kSmCkSteps);
+    if (nsub > 1 && s0 < in_ring)
+      sm_replay<C, I>(f, P, c, sc->ck1[sgi], len, nullptr, sc->ck2, kSmCkSteps);
     KT_ROLLED
     for (int sub = nsub - 1; sub >= 0; --sub) {
       const int t0 = sub * kSmCkSteps;
       const int tl = (len - t0 < kSmCkSteps) ? len - t0 : kSmCkSteps;
-      // the last sub-segment (steps from a multiple of 32 up to N-1) is still
-      // in the forward's ring of step starts
-      if (!(sgi == nseg - 1 && sub == nsub - 1))
+      const SmSt<C::kN>* st = sc->st;
+      if (s0 + t0 >= in_ring)
+        st = sc->st + (s0 + t0) % R;
+      else
         sm_replay<C, I>(f, P, c, nsub > 1 ? sc->ck2[sub] : sc->ck1[sgi], tl, sc->st, nullptr, 0);
       KT_ROLLED
       for (int m = tl - 1; m >= 0; --m) {
-        sm_step_bwd<C, I>(f, P, c, sc->st[m], last ? hbar_ev : 0.0, ybar, &Hbar, cbar, pbar,
+        sm_step_bwd<C, I>(f, P, c, st[m], last ? hbar_ev : 0.0, ybar, &Hbar, cbar, pbar,
                           &sc->stages);
         if (last) {
           for (int i = 0; i < C::kN; ++i) ybar[i] = ybar[i] + yb_direct[i];
