@@ -28,8 +28,9 @@
 //   * states come back from the checkpoints: a segment of k steps is replayed
 //     from its checkpoint (same controller, same rejections, so the same
 //     accepted steps); segments longer than 32 steps are replayed once into
-//     inner checkpoints every 32 steps.  The last 32 step starts are kept
-//     by the forward itself, so the final sub-segment needs no replay.
+//     inner checkpoints every 32 steps.  The last sm_ring_steps (256; 128
+//     for bundles) step starts are kept by the forward itself, so a ray of
+//     at most that many steps needs no replay at all.
 // VJP of the RHS f = J grad_y H (J = [[0, I], [-I, 0]]): v^T df/dy =
 // H_yy (J^T v) and v^T df/dc = d/dc (grad_y H) . (J^T v) = the derivative of
 // dH/dc along J^T v, so one Dual<1> evaluation of the full gradient of H along
@@ -44,8 +45,14 @@ constexpr int kSmCkSteps = 32;  // accepted steps between checkpoints
 // Step starts the forward keeps (the last kSmRing of them): a ray of at most
 // that many accepted steps needs no replay in its reverse sweep.  A multiple
 // of kSmCkSteps; smaller for the bundle's 12-double state.
+#ifndef KT_SM_RING
+#define KT_SM_RING 256
+#endif
+#ifndef KT_SM_RING_BUNDLE
+#define KT_SM_RING_BUNDLE 128
+#endif
 template <int N>
-constexpr int sm_ring_steps() { return N >= 12 ? 128 : 256; }
+constexpr int sm_ring_steps() { return N >= 12 ? KT_SM_RING_BUNDLE : KT_SM_RING; }
 constexpr int kSmCkCap = 64;    // checkpoints per level
 constexpr int kSmMaxDoublings = 6;  // k up to 32 * 2^6: 131072 accepted steps
 
