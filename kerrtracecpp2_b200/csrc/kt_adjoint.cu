@@ -98,7 +98,8 @@ __global__ void __launch_bounds__(kSmBlock) k_smooth_tangent(const Frame f, cons
     if (pix < n) {
       RayResult o;
       double g[kGSlots];
-      if (!sm_pixel_tangent<C>(f, pix, job.tangent_dir, job.cot, &o, g)) {
+      // without outputs, pixels whose cotangent is zero are not traced
+      if (!sm_pixel_tangent<C>(f, pix, job.tangent_dir, job.cot, &o, g, out.outcome != nullptr)) {
         fb_pix[atomicAdd(fb_n, 1u)] = pix;
       } else {
         if (out.outcome) write_result(out, pix, o);

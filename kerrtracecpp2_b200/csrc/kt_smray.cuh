@@ -1484,8 +1484,19 @@ KT_HD bool sm_trace_t(const Frame& f, const SmPrm<T1>& P, const T1* y_in, const 
 // derivatives.  Returns false where the KS initialisation fails (KS chart).
 template <class C>
 KT_HD bool sm_pixel_tangent(const Frame& f, uint32_t pix, int dir, const SmCot& cot, RayResult* o,
-                            double* g) {
+                            double* g, bool need_out = true) {
   constexpr bool kKS = C::kN == 6;
+  if (!need_out) {
+    // a pixel whose cotangent is zero whatever its trace gives contributes
+    // nothing: a target pixel off the disk, or zero cotangent entries
+    const bool zero = cot.mode == 2 ? cot.t_out[pix] != kOutDisk
+                                    : (!cot.g || cot.g[pix] == 0.0) && (!cot.r || cot.r[pix] == 0.0);
+    if (zero) {
+      for (int q = 0; q < kGSlots; ++q) g[q] = 0.0;
+      g[kGNumBL] = kKS ? 0.0 : 1.0;
+      return true;
+    }
+  }
   const int px = (int)(pix % (uint32_t)f.cam.W), py = (int)(pix / (uint32_t)f.cam.W);
   double al, be;
   pixel_angles(f.cam, px, py, &al, &be);
