@@ -166,8 +166,9 @@ cudaError_t launch_batch_mixed(Mode mode, int variant, const BatchRays& br, uint
                                const Fallback& fb, const LaunchShape& s, cudaStream_t st);
 
 // Centre-out ray order (kt_kernels.cu): base + the W x H frame's pixels in
-// rings about the image centre, innermost first, row-major within a ring,
-// into `list` (W*H words); `scratch` holds ring_scratch_words(W*H) words.
+// rings about the image centre, innermost first, in blocks of 8 x 4 pixels
+// within a ring, into `list` (W*H words); `scratch` holds
+// ring_scratch_words(W*H) words.
 // Whole frames of at least kOrderMinPixels pixels are traced in this order,
 // and every frame of a batch (base = the frame's first ray of its group).
 constexpr int kOrderClasses = 512;
@@ -184,6 +185,71 @@ constexpr size_t ring_scratch_words(uint64_t n) {
 }
 cudaError_t launch_ring_order(int W, int H, uint32_t base, uint32_t* scratch, uint32_t* list,
                               cudaStream_t stream);
+
+// The order's geometry and its input order (ring_item), shared by the sort
+// kernels and their host check.
+struct RingGeom {
+  float cx, cy, inv_w;
+  int W, H, Wt, Ht;   // frame; the top-left region covered by whole 8 x 4 blocks
+  uint32_t n_int;     // its pixels, Wt * Ht
+};
+
+KT_HD RingGeom ring_geom(int W, int H) {
+  RingGeom g;
+  g.cx = 0.5f * (float)(W - 1);
+  g.cy = 0.5f * (float)(H - 1);
+  const float rmax = sqrtf(g.cx * g.cx + g.cy * g.cy) + 1.0f;
+  const float w = fmaxf(4.0f, rmax / (float)kOrderClasses);
+  g.inv_w = 1.0f / w;
+  g.W = W;
+  g.H = H;
+  g.Wt = W / 8 * 8;
+  g.Ht = H / 4 * 4;
+  g.n_int = (uint32_t)g.Wt * (uint32_t)g.Ht;
+  return g;
+}
+
+KT_HD int ring_of(const RingGeom& g, float x, float y) {
+  const float dx = x - g.cx, dy = y - g.cy;
+  const int c = (int)(sqrtf(dx * dx + dy * dy) * g.inv_w);
+  return c < kOrderClasses - 1 ? c : kOrderClasses - 1;
+}
+
+// Item e (0 <= e < W*H) of the sort's input order, a one-to-one map onto
+// the pixels: the 8 x 4 blocks of the top-left Wt x Ht region block by block
+// (row-major over blocks, each block's 32 pixels row-major), a block in the
+// ring of its centre, so that a warp's 32 rays are one compact block; then
+// the right strip (x >= Wt, every row) and the bottom strip (y >= Ht,
+// x < Wt) pixel by pixel, each pixel in its own ring.  Measured on the 720p
+// headline frame: 54.4 ms against 58.2 with single pixels placed in the
+// rings in row-major order (8 x 8 blocks 54.3, 4 x 8 54.7, 16 x 2 55.1;
+// pixels sorted by angle within each ring 54.6; row-major order 64.5).
+KT_HD void ring_item(const RingGeom& g, uint32_t e, uint32_t* p, int* c) {
+  if (e < g.n_int) {
+    const uint32_t bw = (uint32_t)g.Wt / 8u;
+    const uint32_t blk = e >> 5, j = e & 31u;
+    const uint32_t bx = blk % bw, by = blk / bw;
+    const uint32_t x = bx * 8u + (j & 7u), y = by * 4u + (j >> 3);
+    *p = y * (uint32_t)g.W + x;
+    *c = ring_of(g, (float)(bx * 8u) + 3.5f, (float)(by * 4u) + 1.5f);
+    return;
+  }
+  const uint32_t r = e - g.n_int;
+  const uint32_t wr = (uint32_t)(g.W - g.Wt);
+  const uint32_t n_right = wr * (uint32_t)g.H;
+  uint32_t x, y;
+  if (r < n_right) {
+    y = r / wr;
+    x = (uint32_t)g.Wt + r % wr;
+  } else {
+    const uint32_t r2 = r - n_right;
+    y = (uint32_t)g.Ht + r2 / (uint32_t)g.Wt;
+    x = r2 % (uint32_t)g.Wt;
+  }
+  *p = y * (uint32_t)g.W + x;
+  *c = ring_of(g, (float)x, (float)y);
+}
+
 
 // FP64 throughput probe: n_iter dependent FMA chains per thread.
 cudaError_t launch_fp64_probe(double* out, int n_iter, int grid, int block, cudaStream_t stream);

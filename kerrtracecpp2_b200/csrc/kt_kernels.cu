@@ -315,34 +315,15 @@ cudaError_t launch_elliptic(const Frame& f, const OutSoA& out, const RayList& rl
 // The camera looks at the black hole, so the image centre holds the shadow
 // and the critical curve, whose rays are the longest, and the edges hold
 // short escaping rays.  A whole frame is traced in rings about the image
-// centre, innermost first, row-major within a ring: the long rays start
-// early and the persistent kernel's tail is short, while a warp's rays stay
-// neighbours (each ring crosses a row in runs of adjacent pixels).  Each
-// ray's arithmetic does not depend on when or beside which rays it runs, so
-// the results are bit for bit those of the row-major trace.  Rings are 4
+// centre, innermost first, in blocks of 8 x 4 pixels (ring_item): the long
+// rays start early and the persistent kernel's tail is short, while a
+// warp's 32 rays are one compact block of neighbours.  Each ray's
+// arithmetic does not depend on when or beside which rays it runs, so the
+// results are bit for bit those of the row-major trace.  Rings are 4
 // pixels wide, wider where the frame needs more than kOrderClasses of them.
-// The list is a stable counting sort: per-tile ring counts, one exclusive
-// scan in (ring, tile) order, then each tile scattered in pixel order.
-
-struct RingGeom {
-  float cx, cy, inv_w;
-};
-
-__host__ __device__ inline RingGeom ring_geom(int W, int H) {
-  RingGeom g;
-  g.cx = 0.5f * (float)(W - 1);
-  g.cy = 0.5f * (float)(H - 1);
-  const float rmax = sqrtf(g.cx * g.cx + g.cy * g.cy) + 1.0f;
-  const float w = fmaxf(4.0f, rmax / (float)kOrderClasses);
-  g.inv_w = 1.0f / w;
-  return g;
-}
-
-__device__ __forceinline__ int ring_class(const RingGeom& g, int W, uint32_t p) {
-  const int y = (int)(p / (uint32_t)W), x = (int)(p - (uint32_t)y * (uint32_t)W);
-  const float dx = (float)x - g.cx, dy = (float)y - g.cy;
-  return min((int)(sqrtf(dx * dx + dy * dy) * g.inv_w), kOrderClasses - 1);
-}
+// The list is a stable counting sort of ring_item's order: per-tile ring
+// counts, one exclusive scan in (ring, tile) order, then each tile scattered
+// in item order (a "tile" here is the sort's chunk of items).
 
 // counts[c * tiles + t]: pixels of ring c in tile t (tile = `tile` pixels)
 __global__ void k_ring_count(int W, int H, uint32_t tile, uint32_t tiles, uint32_t* __restrict__ counts) {
@@ -353,7 +334,12 @@ __global__ void k_ring_count(int W, int H, uint32_t tile, uint32_t tiles, uint32
   const uint32_t n = (uint32_t)W * (uint32_t)H;
   const uint32_t t = blockIdx.x;
   const uint32_t end = min(n, (t + 1) * tile);
-  for (uint32_t p = t * tile + threadIdx.x; p < end; p += blockDim.x) atomicAdd(&h[ring_class(g, W, p)], 1u);
+  for (uint32_t e = t * tile + threadIdx.x; e < end; e += blockDim.x) {
+    uint32_t p;
+    int c;
+    ring_item(g, e, &p, &c);
+    atomicAdd(&h[c], 1u);
+  }
   __syncthreads();
   for (int c = threadIdx.x; c < kOrderClasses; c += blockDim.x) counts[(uint32_t)c * tiles + t] = h[c];
 }
@@ -407,9 +393,11 @@ __global__ void k_ring_place(int W, int H, uint32_t tile, uint32_t tiles,
   const uint32_t n = (uint32_t)W * (uint32_t)H;
   const uint32_t end = min(n, (t + 1) * tile);
   const unsigned lane = threadIdx.x;
-  for (uint32_t p0 = t * tile; p0 < end; p0 += 32) {
-    const uint32_t p = p0 + lane;
-    const int c = (p < end) ? ring_class(g, W, p) : -1;
+  for (uint32_t e0 = t * tile; e0 < end; e0 += 32) {
+    const uint32_t e = e0 + lane;
+    uint32_t p = 0;
+    int c = -1;
+    if (e < end) ring_item(g, e, &p, &c);
     const unsigned same = __match_any_sync(kFull, c);
     uint32_t at = 0;
     if (c >= 0) at = next[c] + (uint32_t)__popc(same & ((1u << lane) - 1u));

@@ -12,6 +12,7 @@
 
 #include "../include/kerrtrace.h"
 #include "../kerrtracecpp2_b200/csrc/kt_frame.h"
+#include "../kerrtracecpp2_b200/csrc/kt_internal.h"
 #include "../kerrtracecpp2_b200/csrc/kt_elliptic.cuh"
 #include "../kerrtracecpp2_b200/csrc/kt_smray.cuh"
 
@@ -359,4 +360,16 @@ extern "C" int hc_smooth_pixels(const kt_frame_desc* d, int64_t n, const uint32_
   return hc_smooth_pixels_m(d, n, pix, mode, force_bl, tangent_dir, cot_g, cot_r, nullptr, t_out, t_g,
                             t_r, nullptr, w_g, w_r, 0.0, outcome, r, red, nullptr, phi_disk, th_esc,
                             ph_esc, steps, attempts, contrib);
+}
+
+// The centre-out order's input map (ring_item, kt_internal.h) on the host:
+// for every item e of a W x H frame, its pixel p[e] and ring c[e].
+extern "C" void hc_ring_items(int W, int H, uint32_t* p, int32_t* c) {
+  const RingGeom g = ring_geom(W, H);
+  const uint32_t n = (uint32_t)W * (uint32_t)H;
+  for (uint32_t e = 0; e < n; ++e) {
+    int cc;
+    ring_item(g, e, &p[e], &cc);
+    c[e] = cc;
+  }
 }

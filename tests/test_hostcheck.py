@@ -115,3 +115,31 @@ def test_bundle_rhs_split_matches_oracle_medium(hc, full_creep):
         assert np.all(got["outcome"][creep] == 0) and np.all(got["r"][creep] == 0.0)
         print(f"{creeping} creeping rays; attempts {got['attempts'].sum()} against the "
               f"oracle's {want['attempts'].sum()}")
+
+
+@pytest.mark.parametrize("wh", [(1280, 720), (1920, 1080), (1283, 721), (77, 31), (7, 10000), (1, 70000),
+                                (8, 4), (512, 512)])
+def test_centre_out_order_input_map(hc, wh):
+    """ring_item, the input order of the centre-out sort, maps the items
+    0..W*H-1 one to one onto the pixels: 8 x 4 blocks of the top-left region
+    whose 32 pixels share one ring, then the strips row-major."""
+    W, H = wh
+    n = W * H
+    p = np.zeros(n, np.uint32)
+    c = np.zeros(n, np.int32)
+    hc.hc_ring_items.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    hc.hc_ring_items(W, H, p.ctypes.data_as(ctypes.c_void_p), c.ctypes.data_as(ctypes.c_void_p))
+    assert np.array_equal(np.sort(p), np.arange(n, dtype=np.uint32))
+    assert c.min() >= 0 and c.max() < 512
+    n_int = (W // 8 * 8) * (H // 4 * 4)
+    if n_int:
+        blocks = p[:n_int].reshape(-1, 32)
+        x, y = blocks % W, blocks // W
+        assert np.all(x.max(1) - x.min(1) == 7) and np.all(y.max(1) - y.min(1) == 3)
+        assert np.all(c[:n_int].reshape(-1, 32) == c[:n_int].reshape(-1, 32)[:, :1])
+    # the rings grow outward: the sorted order starts at the image centre
+    order = p[np.argsort(c, kind="stable")]
+    cx, cy = (W - 1) / 2, (H - 1) / 2
+    d0 = np.hypot(order[:32] % W - cx, order[:32] // W - cy).max()
+    ring_w = max(4.0, (np.hypot(cx, cy) + 1) / 512)
+    assert d0 <= ring_w + 9.0
