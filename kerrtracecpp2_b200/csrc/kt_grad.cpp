@@ -92,11 +92,11 @@ kt_status grad_run(kt_context* ctx, const kt_frame_desc* desc_in, const uint32_t
   // a whole frame of at least kOrderMinPixels pixels in centre-out order, as
   // kt_trace traces it (the expensive rays by the critical curve first); the
   // contributions are per pixel and summed in pixel order either way.
-  // Measured per gradient, row-major against centre-out: config 5 48 / 44 ms,
-  // the 720p DOPRI5 frame 156 / 158, the 960x540 bundle frame 596 / 635, so
-  // bundle frames keep the row-major order.
+  // Measured per gradient, row-major against centre-out in 8 x 4 blocks:
+  // config 5 48 / 32 ms (the later changes included), the 960x540 bundle
+  // frame 559 / 488.
   bool whole = false;
-  if (!pix && n >= kt::kOrderMinPixels && !f.bundles) {
+  if (!pix && n >= kt::kOrderMinPixels) {
     const size_t words = (size_t)n + kt::ring_scratch_words((uint32_t)n);
     r = ensure(ctx, (void**)&ctx->d_order, &ctx->order_cap, words * sizeof(uint32_t), "ray order");
     if (r != KT_OK) return r;
