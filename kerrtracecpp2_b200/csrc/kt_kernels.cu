@@ -173,8 +173,12 @@ template <> struct Shape<struct ModeBLRk4> { static constexpr int kBlock = 64, k
 #ifndef KT_BL_DOPRI5_REFILL
 #define KT_BL_DOPRI5_REFILL 32
 #endif
+#ifndef KT_BL_DOPRI5_BLOCK
+#define KT_BL_DOPRI5_BLOCK 64
+#endif
 template <> struct Shape<struct ModeBLDopri5> {
-  static constexpr int kBlock = 64, kMinBlocks = KT_BL_DOPRI5_MINB, kRefill = KT_BL_DOPRI5_REFILL;
+  static constexpr int kBlock = KT_BL_DOPRI5_BLOCK, kMinBlocks = KT_BL_DOPRI5_MINB,
+                       kRefill = KT_BL_DOPRI5_REFILL;
 };
 template <> struct Shape<struct ModeKSRk4> { static constexpr int kBlock = 64, kMinBlocks = 9, kRefill = 32; };
 template <> struct Shape<struct ModeBundle> { static constexpr int kBlock = 128, kMinBlocks = 1, kRefill = 16; };
