@@ -158,8 +158,12 @@ template <bool B> struct Shape<ModeBLRk4MixedT<B>> { static constexpr int kBlock
 #ifndef KT_MIXED32_DOPRI5_REFILL
 #define KT_MIXED32_DOPRI5_REFILL 32
 #endif
+#ifndef KT_MIXED_DOPRI5_MINB
+#define KT_MIXED_DOPRI5_MINB 9
+#endif
 template <bool B> struct Shape<ModeBLDopri5MixedT<B>> {
-  static constexpr int kBlock = 64, kMinBlocks = 9, kRefill = B ? KT_MIXED32_DOPRI5_REFILL : 32;
+  static constexpr int kBlock = 64, kMinBlocks = KT_MIXED_DOPRI5_MINB,
+                       kRefill = B ? KT_MIXED32_DOPRI5_REFILL : 32;
 };
 template <bool B> struct Shape<ModeKSRk4MixedT<B>> { static constexpr int kBlock = 64, kMinBlocks = 9, kRefill = 32; };
 // Mixed bundles: 64-thread blocks, at least 6 per SM (168 registers, no
