@@ -182,9 +182,12 @@ static cudaError_t smooth_launch(const Frame& f, const OutSoA& out, uint32_t n, 
 }
 
 cudaError_t launch_smooth(const Frame& f, const OutSoA& out, uint32_t n, const SmJob* job,
-                          uint32_t* counters, uint32_t* fb_pix, int device, cudaStream_t st) {
+                          uint32_t* counters, uint32_t* fb_pix, int device, cudaStream_t st,
+                          const uint32_t* order) {
   SmJob none;
   memset(&none, 0, sizeof none);
+  none.pix = order;
+  none.n_pix = order ? n : 0;
   const SmJob& jb = job ? *job : none;
   const bool grad = job != nullptr;
   // Jacobi bundles (BL chart, RK4 step doubling whatever the integrator, as

@@ -37,22 +37,31 @@ kt_status shape(kt_context* ctx, kt::Mode m, kt::LaunchShape* s) {
 static kt_status run_trace_list(kt_context* ctx, const kt::Frame& f, const kt::OutSoA& out,
                                 const kt::RayList& rl, uint64_t n_max, cudaStream_t st);
 
-// A whole frame of at least kOrderMinPixels pixels (not the smooth tracer)
-// is traced in centre-out order (kt_kernels.cu, launch_ring_order: three
-// small launches on the same stream before the trace), each ray written at
-// its own pixel.  Smaller frames and pixel lists take the row-major order.
+// A whole frame of at least kOrderMinPixels pixels is traced in centre-out
+// order (kt_kernels.cu, launch_ring_order: three small launches on the same
+// stream before the trace), each ray written at its own pixel.  Smaller
+// frames and pixel lists take the row-major order.
 kt_status run_trace(kt_context* ctx, const kt::Frame& f, const kt::OutSoA& out,
                     const kt::RayList& rl, uint64_t n_max, cudaStream_t st) {
   const int W = f.cam.W, H = f.cam.H;
   const uint64_t n = (uint64_t)W * (uint64_t)H;
-  if (rl.pix || rl.slot || rl.n_dev || rl.n != n || n < kt::kOrderMinPixels ||
-      f.precision == KT_PREC_SMOOTH)
+  if (rl.pix || rl.slot || rl.n_dev || rl.n != n || n < kt::kOrderMinPixels)
     return run_trace_list(ctx, f, out, rl, n_max, st);
   const size_t words = (size_t)n + kt::ring_scratch_words(n);
   kt_status r = ensure(ctx, (void**)&ctx->d_order, &ctx->order_cap, words * sizeof(uint32_t),
                        "ray order");
   if (r != KT_OK) return r;
   KT_CUDA(ctx, kt::launch_ring_order(W, H, 0, ctx->d_order + n, ctx->d_order, st), "ray order");
+  if (f.precision == KT_PREC_SMOOTH) {
+    // the smooth tracer takes the order as its list of rays
+    r = ensure(ctx, (void**)&ctx->d_fb, &ctx->fb_cap, 2 * n_max * sizeof(uint32_t), "fallback list");
+    if (r != KT_OK) return r;
+    KT_CUDA(ctx, cudaMemsetAsync(ctx->d_counters, 0, 4 * sizeof(uint32_t), st), "reset queue");
+    KT_CUDA(ctx, kt::launch_smooth(f, out, (uint32_t)n, nullptr, ctx->d_counters, ctx->d_fb, ctx->device,
+                                   st, ctx->d_order),
+            "smooth kernel launch");
+    return KT_OK;
+  }
   const kt::RayList ord = {ctx->d_order, ctx->d_order, nullptr, (uint32_t)n};
   return run_trace_list(ctx, f, out, ord, n_max, st);
 }
